@@ -1,0 +1,202 @@
+/*
+ * mpgpu.h -- C ABI of the B200 (sm_100a) realignment engine.
+ *
+ * The engine runs MarginPolish's anchored, banded 3-state pair-HMM
+ * forward / backward / posterior pass (match, gap-x and gap-y posteriors,
+ * run-length repeat-count emissions included) for batches of reads on one
+ * GPU. Every entry point takes plain pointers and sizes and returns an
+ * mp_status; mp_last_error() gives a thread-local message for the last
+ * failure. There is no CPU fallback: without a usable sm_100 device every
+ * compute call fails with MP_ERR_CUDA.
+ *
+ * Reference interfaces replaced (paths within the MarginPolish tree):
+ *  - mp_realign_batch                 the per-read calls of
+ *        getAlignedPairsWithIndelsUsingAnchors (impl/pairwiseAligner.c:1105-1130)
+ *        made by getAlignedPairsWithIndelsCroppingReference
+ *        (impl/polisher.c:605-654) inside poa_realign (impl/polisher.c:656-703),
+ *        batched over all reads of all chunks;
+ *  - mp_model_create                  the StateMachine built by
+ *        hmm_getStateMachine + rleNucleotideEmissions_construct
+ *        (impl/stateMachine.c:676-689, :724-736; impl/parser.c:235-245, :391-401),
+ *        lowered to flat tables;
+ *  - mp_params                        PairwiseAlignmentParameters
+ *        (inc/pairwiseAligner.h:28-39);
+ *  - mp_band / mp_split_points        band_constructDynamic / band_construct and
+ *        getSplitPoints (impl/pairwiseAligner.c:120-226, :899-926).
+ * The reference's own signatures (stList / StateMachine based) are exported
+ * by the drop-in layer declared in mpgpu_dropin.h.
+ */
+#ifndef MPGPU_H_
+#define MPGPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    MP_OK = 0,
+    MP_ERR_ARGUMENT = 1,   /* malformed input (anchors, lengths, parameters, symbols) */
+    MP_ERR_CUDA = 2,       /* CUDA runtime / device failure, or no usable device */
+    MP_ERR_MEMORY = 3,     /* host or device allocation failed */
+    MP_ERR_OVERFLOW = 4,   /* an internal bound was exceeded (reported, never silent) */
+    MP_ERR_STATE = 5       /* call order / handle misuse */
+} mp_status;
+
+#define MP_MAX_REPEAT 51           /* repeat-count table dimension (inc/margin.h:123) */
+#define MP_PROB_ONE 10000000       /* integer probability one (inc/pairwiseAligner.h:26) */
+
+/* Lowered state machine for one read strand. States: 0 match, 1 gap-x, 2 gap-y.
+ * All probabilities are natural-log values, -INFINITY for zero. */
+typedef struct {
+    double log_transitions[9];     /* index from*3+to */
+    double log_start[3];
+    double log_ragged_start[3];
+    double log_end[3];
+    double log_ragged_end[3];
+    double log_match[25];          /* by base [x*5+y]; base 4 = 'N' */
+    double log_gap_x[5];
+    double log_gap_y[5];
+    int32_t run_length;            /* 1: symbols carry repeat counts (base = sym & 255, count = sym >> 8) */
+    int32_t strand;                /* strand flag of the repeat table lookup (1 forward) */
+    int32_t max_repeat;            /* table dimension, MP_MAX_REPEAT */
+    int32_t reserved;
+    double repeat_scale;           /* multiplier on the log10 table (2.3025 in the reference) */
+    const double *repeat_log10;    /* [4][max_repeat][max_repeat] = [base][underlying][observed]; NULL if !run_length */
+} mp_model_desc;
+
+typedef struct {
+    double threshold;                       /* minimum posterior emitted */
+    int64_t min_diags_between_traceback;
+    int64_t traceback_diagonals;
+    int64_t diagonal_expansion;
+    int64_t constraint_diagonal_trim;       /* carried, unused on this path (as in the reference) */
+    int64_t split_matrix_bigger_than_this;
+    int32_t dynamic_anchor_expansion;
+    int32_t reserved;
+    double gap_gamma;                       /* carried, unused on this path */
+} mp_params;
+
+/* A batch of alignment jobs in HOST memory. Job j aligns sequence Y =
+ * y_symbols[y_offsets[j] .. y_offsets[j+1]) (the read) against sequence X =
+ * x_symbols[x_begin[j] .. x_end[j]) (the template; jobs may share one template
+ * buffer), with anchors in those coordinates. Anchors are int32 triples
+ * (x, y, expansion), strictly increasing in x and y, with 0 <= x < len(X),
+ * 0 <= y < len(Y), expansion even and >= 0. */
+typedef struct {
+    int64_t n_jobs;
+    const int64_t *x_begin;         /* n_jobs */
+    const int64_t *x_end;           /* n_jobs */
+    int64_t x_symbols_length;       /* length of x_symbols */
+    const uint16_t *x_symbols;
+    const int64_t *y_offsets;       /* n_jobs+1 */
+    const uint16_t *y_symbols;
+    const int64_t *anchor_offsets;  /* n_jobs+1, in triples */
+    const int32_t *anchors;         /* 3 int32 per anchor */
+    const uint8_t *strand;          /* 1 forward (model 0), 0 reverse (model 1) */
+    const uint8_t *ragged_left;     /* NULL: all 0 */
+    const uint8_t *ragged_right;    /* NULL: all 0 */
+    const int64_t *x_shift;         /* NULL: 0. Added to output x (the crop start of the reference) */
+} mp_batch;
+
+typedef struct mp_engine mp_engine;
+typedef struct mp_model mp_model;
+typedef struct mp_result mp_result;
+
+/* Result view: host arrays owned by the mp_result. For list k (0 match, 1 gap-x,
+ * 2 gap-y), job j's tuples are [offsets[k][j], offsets[k][j+1]) of
+ * weight[k], x[k], y[k], in the reference's output order. */
+typedef struct {
+    int64_t n_jobs;
+    const int64_t *offsets[3];
+    const int32_t *weight[3];
+    const int32_t *x[3];
+    const int32_t *y[3];
+    const double *log_likelihood;   /* per job: sum over split sub-problems of the final segment's log total */
+    const int64_t *cells;           /* per job: sum of band widths (cell updates counted by the metric) */
+    int64_t total_cells;
+    double device_ms;               /* device time of the posterior kernels for this call */
+} mp_result_view;
+
+const char *mp_last_error(void);
+const char *mp_version(void);
+
+/* Engine bound to one CUDA device (one process per GPU). */
+mp_status mp_engine_create(int device, mp_engine **out);
+void mp_engine_destroy(mp_engine *e);
+/* Query: SM count, and whether the device is sm_100. */
+mp_status mp_engine_info(const mp_engine *e, int *sm_count, int *cc_major, int *cc_minor);
+
+/* Lowered models for forward-strand (fwd) and reverse-strand (rev) reads. */
+mp_status mp_model_create(mp_engine *e, const mp_model_desc *fwd, const mp_model_desc *rev, mp_model **out);
+void mp_model_destroy(mp_model *m);
+
+/* Tuning: slots are assigned in lanes of `slots_per_lane` (0 = automatic),
+ * checkpoint stride in anti-diagonals (0 = automatic), warps per block (0 = automatic). */
+typedef struct {
+    int32_t checkpoint_stride;
+    int32_t warps_per_block;
+    int32_t blocks_per_sm;
+    int32_t reserved;
+} mp_tuning;
+mp_status mp_engine_set_tuning(mp_engine *e, const mp_tuning *t);
+
+/* Full posterior pass over a batch of jobs held in host memory: host->device copies,
+ * band construction, the persistent length-sorted posterior kernel, compaction and
+ * device->host copies of the tuples. */
+mp_status mp_realign_batch(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
+                           mp_result **out);
+mp_status mp_result_view_get(const mp_result *r, mp_result_view *v);
+void mp_result_destroy(mp_result *r);
+
+/* ---- device-resident path (inputs already in HBM; used for kernel timing) ---- */
+typedef struct mp_device_batch mp_device_batch;
+/* Copies a host batch to the device once and plans it (splits, band, queue order). */
+mp_status mp_device_batch_create(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
+                                 mp_device_batch **out);
+/* Runs the posterior kernel(s) on the resident batch; outputs stay on the device.
+ * If kernel_ms is non-NULL it receives the CUDA-event time of the posterior kernel(s). */
+mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, float *kernel_ms);
+/* Copies the last run's results to the host. */
+mp_status mp_device_batch_fetch(mp_engine *e, mp_device_batch *db, mp_result **out);
+/* Totals of the resident batch (cells = sum of band widths; launches per run). */
+mp_status mp_device_batch_stats(const mp_device_batch *db, int64_t *total_cells, int64_t *n_tasks,
+                                int32_t *kernel_launches_per_run);
+void mp_device_batch_destroy(mp_device_batch *db);
+
+/* ---- geometry helpers (host, integer-exact restatements used by the planner) ---- */
+/* Band of one sub-problem: (xay, xmyL, xmyR) for d = 0..lX+lY into out[3*(lX+lY+1)]. */
+mp_status mp_band(const int32_t *anchors, int64_t n_anchors, int64_t lx, int64_t ly, int64_t expansion,
+                  int dynamic, int64_t *out);
+/* Split rectangles (x1, y1, x2, y2); *n_out receives the count, at most cap are written. */
+mp_status mp_split_points(const int32_t *anchors, int64_t n_anchors, int64_t lx, int64_t ly,
+                          int64_t max_matrix_size, int ragged_left, int ragged_right, int64_t *out, int64_t cap,
+                          int64_t *n_out);
+/* Reference crop of getAlignedPairsWithIndelsCroppingReference (impl/polisher.c:613-628):
+ * [*start, *end) of the template given the first/last anchor and the read length. */
+mp_status mp_crop_range(const int32_t *anchors, int64_t n_anchors, int64_t template_length, int64_t read_length,
+                        int64_t *start, int64_t *end);
+
+/* ---- run-length encoding and anchors (host, integer-exact) ---- */
+/* rleString_construct (impl/polisher.c:1357-1389): runs of identical characters.
+ * run_chars / run_counts need room for n entries; *n_runs receives the run count. */
+mp_status mp_rle_encode(const char *s, int64_t n, char *run_chars, uint32_t *run_counts, int64_t *n_runs);
+/* rleString_constructSymbolString (impl/stateMachine.c:133-146) with the nucleotide
+ * alphabet (impl/stateMachine.c:25-42): symbol = (min(count, max_exclusive-1) << 8) | base
+ * when include_counts, else base. */
+mp_status mp_rle_symbols(const char *run_chars, const uint32_t *run_counts, int64_t n, int include_counts,
+                         uint32_t max_repeat_exclusive, uint16_t *out);
+/* runLengthEncodeAlignment (impl/polisher.c:1732-1750): maps base-level aligned pairs
+ * (x, y, expansion) through the non-RLE -> RLE coordinate maps of X and Y
+ * (rleString_getNonRleToRleCoordinateMap, :1718-1730, built from the run counts)
+ * and keeps the strictly increasing ones. out needs room for 3*n int32; returns the count. */
+mp_status mp_rle_anchors(const int64_t *pairs, int64_t n, const uint32_t *x_run_counts, int64_t x_runs,
+                         const uint32_t *y_run_counts, int64_t y_runs, int32_t *out, int64_t *n_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

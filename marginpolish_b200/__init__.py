@@ -1,0 +1,14 @@
+"""B200-native (sm_100a) realignment engine for MarginPolish's banded pair-HMM
+posterior pass. The compute path is the in-tree CUDA library libmpgpu.so
+(C ABI in include/mpgpu.h); this package is its host-side interface."""
+from . import _lib
+from .params import AlignmentParams, PolishModel, StateModel, build_state_model, load_polish_model
+from .realign import (DeviceBatch, Engine, Jobs, Model, Pairs, get_aligned_pairs_using_anchors,
+                      get_aligned_pairs_with_indels_using_anchors, realign_batch)
+from .rle import RleString, crop_range, rle_anchors
+
+__all__ = [
+    "AlignmentParams", "PolishModel", "StateModel", "build_state_model", "load_polish_model", "DeviceBatch",
+    "Engine", "Jobs", "Model", "Pairs", "get_aligned_pairs_using_anchors",
+    "get_aligned_pairs_with_indels_using_anchors", "realign_batch", "RleString", "crop_range", "rle_anchors",
+]

@@ -1,0 +1,179 @@
+"""ctypes binding of the in-tree CUDA library ``libmpgpu.so`` (C ABI in include/mpgpu.h).
+
+The library is the product; this module only declares its entry points. It is
+loaded from the package directory and fails loudly when it is missing: there
+is no CPU fallback for the realignment pass.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import (POINTER, Structure, c_char, c_char_p, c_double, c_float, c_int, c_int32, c_int64, c_uint8,
+                    c_uint16, c_uint32, c_void_p)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmpgpu.so")
+
+MP_OK = 0
+MP_ERR_ARGUMENT = 1
+MP_ERR_CUDA = 2
+MP_ERR_MEMORY = 3
+MP_ERR_OVERFLOW = 4
+MP_ERR_STATE = 5
+MP_MAX_REPEAT = 51
+MP_PROB_ONE = 10000000
+
+STATUS_NAMES = {0: "MP_OK", 1: "MP_ERR_ARGUMENT", 2: "MP_ERR_CUDA", 3: "MP_ERR_MEMORY", 4: "MP_ERR_OVERFLOW",
+                5: "MP_ERR_STATE"}
+
+
+class MpError(RuntimeError):
+    """Error status returned by the C ABI, with the library's message."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class ModelDesc(Structure):
+    _fields_ = [
+        ("log_transitions", c_double * 9),
+        ("log_start", c_double * 3),
+        ("log_ragged_start", c_double * 3),
+        ("log_end", c_double * 3),
+        ("log_ragged_end", c_double * 3),
+        ("log_match", c_double * 25),
+        ("log_gap_x", c_double * 5),
+        ("log_gap_y", c_double * 5),
+        ("run_length", c_int32),
+        ("strand", c_int32),
+        ("max_repeat", c_int32),
+        ("reserved", c_int32),
+        ("repeat_scale", c_double),
+        ("repeat_log10", POINTER(c_double)),
+    ]
+
+
+class Params(Structure):
+    _fields_ = [
+        ("threshold", c_double),
+        ("min_diags_between_traceback", c_int64),
+        ("traceback_diagonals", c_int64),
+        ("diagonal_expansion", c_int64),
+        ("constraint_diagonal_trim", c_int64),
+        ("split_matrix_bigger_than_this", c_int64),
+        ("dynamic_anchor_expansion", c_int32),
+        ("reserved", c_int32),
+        ("gap_gamma", c_double),
+    ]
+
+
+class Batch(Structure):
+    _fields_ = [
+        ("n_jobs", c_int64),
+        ("x_begin", POINTER(c_int64)),
+        ("x_end", POINTER(c_int64)),
+        ("x_symbols_length", c_int64),
+        ("x_symbols", POINTER(c_uint16)),
+        ("y_offsets", POINTER(c_int64)),
+        ("y_symbols", POINTER(c_uint16)),
+        ("anchor_offsets", POINTER(c_int64)),
+        ("anchors", POINTER(c_int32)),
+        ("strand", POINTER(c_uint8)),
+        ("ragged_left", POINTER(c_uint8)),
+        ("ragged_right", POINTER(c_uint8)),
+        ("x_shift", POINTER(c_int64)),
+    ]
+
+
+class ResultView(Structure):
+    _fields_ = [
+        ("n_jobs", c_int64),
+        ("offsets", POINTER(c_int64) * 3),
+        ("weight", POINTER(c_int32) * 3),
+        ("x", POINTER(c_int32) * 3),
+        ("y", POINTER(c_int32) * 3),
+        ("log_likelihood", POINTER(c_double)),
+        ("cells", POINTER(c_int64)),
+        ("total_cells", c_int64),
+        ("device_ms", c_double),
+    ]
+
+
+class Tuning(Structure):
+    _fields_ = [
+        ("checkpoint_stride", c_int32),
+        ("warps_per_block", c_int32),
+        ("blocks_per_sm", c_int32),
+        ("reserved", c_int32),
+    ]
+
+
+# Every symbol include/mpgpu.h declares (checked by the CPU tests).
+EXPORTED = [
+    "mp_last_error", "mp_version", "mp_engine_create", "mp_engine_destroy", "mp_engine_info",
+    "mp_model_create", "mp_model_destroy", "mp_engine_set_tuning", "mp_realign_batch", "mp_result_view_get",
+    "mp_result_destroy", "mp_device_batch_create", "mp_device_batch_run", "mp_device_batch_fetch",
+    "mp_device_batch_stats", "mp_device_batch_destroy", "mp_band", "mp_split_points", "mp_crop_range",
+    "mp_rle_encode", "mp_rle_symbols", "mp_rle_anchors",
+]
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Loads libmpgpu.so from the package directory (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with marginpolish_b200.build.build() "
+                          "(nvcc, sm_100a); there is no CPU fallback")
+    lib = ctypes.CDLL(LIB_PATH)
+    P = POINTER
+    sig = {
+        "mp_last_error": (c_char_p, []),
+        "mp_version": (c_char_p, []),
+        "mp_engine_create": (c_int, [c_int, P(c_void_p)]),
+        "mp_engine_destroy": (None, [c_void_p]),
+        "mp_engine_info": (c_int, [c_void_p, P(c_int), P(c_int), P(c_int)]),
+        "mp_engine_set_tuning": (c_int, [c_void_p, P(Tuning)]),
+        "mp_model_create": (c_int, [c_void_p, P(ModelDesc), P(ModelDesc), P(c_void_p)]),
+        "mp_model_destroy": (None, [c_void_p]),
+        "mp_realign_batch": (c_int, [c_void_p, c_void_p, P(Params), P(Batch), P(c_void_p)]),
+        "mp_result_view_get": (c_int, [c_void_p, P(ResultView)]),
+        "mp_result_destroy": (None, [c_void_p]),
+        "mp_device_batch_create": (c_int, [c_void_p, c_void_p, P(Params), P(Batch), P(c_void_p)]),
+        "mp_device_batch_run": (c_int, [c_void_p, c_void_p, P(c_float)]),
+        "mp_device_batch_fetch": (c_int, [c_void_p, c_void_p, P(c_void_p)]),
+        "mp_device_batch_stats": (c_int, [c_void_p, P(c_int64), P(c_int64), P(c_int32)]),
+        "mp_device_batch_destroy": (None, [c_void_p]),
+        "mp_band": (c_int, [P(c_int32), c_int64, c_int64, c_int64, c_int64, c_int, P(c_int64)]),
+        "mp_split_points": (c_int, [P(c_int32), c_int64, c_int64, c_int64, c_int64, c_int, c_int, P(c_int64),
+                                    c_int64, P(c_int64)]),
+        "mp_crop_range": (c_int, [P(c_int32), c_int64, c_int64, c_int64, P(c_int64), P(c_int64)]),
+        "mp_rle_encode": (c_int, [c_char_p, c_int64, P(c_char), P(c_uint32), P(c_int64)]),
+        "mp_rle_symbols": (c_int, [P(c_char), P(c_uint32), c_int64, c_int, c_uint32, P(c_uint16)]),
+        "mp_rle_anchors": (c_int, [P(c_int64), c_int64, P(c_uint32), c_int64, P(c_uint32), c_int64, P(c_int32),
+                                   P(c_int64)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(status: int) -> None:
+    """Raises MpError with the library's message for a non-OK status."""
+    if status != MP_OK:
+        msg = load().mp_last_error()
+        raise MpError(status, msg.decode() if msg else "")
+
+
+def ptr(arr, ctype):
+    """ctypes pointer to a contiguous numpy array (None -> NULL)."""
+    if arr is None:
+        return None
+    return arr.ctypes.data_as(POINTER(ctype))

@@ -1,0 +1,993 @@
+// C ABI of the realignment engine: model lowering, batch planning (splits,
+// slot classes, length-sorted queues), device memory and launches.
+//
+// Reference behaviour restated here (integer logic, bit-exact):
+//  * split rectangles  -- getSplitPoints / getSplitPointsP (impl/pairwiseAligner.c:875-926)
+//  * anchor re-basing  -- getPosteriorProbsWithBandingSplittingAlignmentsByLargeGaps (:942-991)
+//  * band geometry     -- band_constructDynamic / band_construct (:96-226), mirrored by the band kernel
+//  * crop range        -- getAlignedPairsWithIndelsCroppingReference (impl/polisher.c:613-628)
+#include "../../include/mpgpu.h"
+#include "mp_internal.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace mp {
+cudaError_t launchPosterior(int C, const DpArgs &a, int blocks, int warps, cudaStream_t s);
+size_t posteriorSmemBytes(int C, int warps);
+int classStride(int C);
+int classMaxWarps(int C);
+cudaError_t launchBand(const BandArgs &a, cudaStream_t s);
+cudaError_t launchCompact(const Task *tasks, const TaskOut *out, int nTasks, const int64_t *dst0,
+                          const int64_t *dst1, const int64_t *dst2, int32_t *const *srcW, int32_t *const *srcX,
+                          int32_t *const *srcY, int32_t *const *dstW, int32_t *const *dstX, int32_t *const *dstY,
+                          cudaStream_t s);
+}  // namespace mp
+
+using namespace mp;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+
+static thread_local std::string g_lastError;
+
+static mp_status failf(mp_status s, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_lastError = buf;
+    return s;
+}
+
+#define CUDA_TRY(expr)                                                                              \
+    do {                                                                                            \
+        cudaError_t _e = (expr);                                                                    \
+        if (_e != cudaSuccess) return failf(MP_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(_e)); \
+    } while (0)
+
+#define MP_TRY(expr)                   \
+    do {                               \
+        mp_status _s = (expr);         \
+        if (_s != MP_OK) return _s;    \
+    } while (0)
+
+extern "C" const char *mp_last_error(void) {
+    return g_lastError.c_str();
+}
+
+extern "C" const char *mp_version(void) {
+    return "mpgpu 0.1 (sm_100a)";
+}
+
+// ---------------------------------------------------------------------------
+// device buffers
+// ---------------------------------------------------------------------------
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    mp_status reserve(size_t n) {
+        if (n <= bytes && p) return MP_OK;
+        release();
+        size_t want = n > 0 ? n : 16;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return failf(MP_ERR_MEMORY, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
+        }
+        bytes = want;
+        return MP_OK;
+    }
+    template <class T>
+    T *as() const { return static_cast<T *>(p); }
+};
+
+// ---------------------------------------------------------------------------
+// engine and model
+// ---------------------------------------------------------------------------
+
+struct mp_engine {
+    int device = 0;
+    int smCount = 0;
+    int ccMajor = 0, ccMinor = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    mp_tuning tuning{};
+};
+
+struct mp_model {
+    mp_engine *engine = nullptr;
+    DevModel host[2];
+    DevBuf models;   // DevModel[2]
+    DevBuf repeat;   // float [2][kRepTable]
+};
+
+extern "C" mp_status mp_engine_create(int device, mp_engine **out) {
+    if (!out) return failf(MP_ERR_ARGUMENT, "mp_engine_create: out is NULL");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        return failf(MP_ERR_CUDA, "no CUDA device available (%s)", e != cudaSuccess ? cudaGetErrorString(e) : "0 devices");
+    }
+    if (device < 0 || device >= n) return failf(MP_ERR_ARGUMENT, "device %d out of range (%d devices)", device, n);
+    CUDA_TRY(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) {
+        return failf(MP_ERR_CUDA, "device %d is sm_%d%d; this library is built for sm_100a only", device, prop.major,
+                     prop.minor);
+    }
+    mp_engine *eng = new mp_engine();
+    eng->device = device;
+    eng->smCount = prop.multiProcessorCount;
+    eng->ccMajor = prop.major;
+    eng->ccMinor = prop.minor;
+    e = cudaStreamCreateWithFlags(&eng->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&eng->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&eng->ev1);
+    if (e != cudaSuccess) {
+        delete eng;
+        return failf(MP_ERR_CUDA, "stream/event creation failed: %s", cudaGetErrorString(e));
+    }
+    *out = eng;
+    return MP_OK;
+}
+
+extern "C" void mp_engine_destroy(mp_engine *e) {
+    if (!e) return;
+    cudaSetDevice(e->device);
+    if (e->ev0) cudaEventDestroy(e->ev0);
+    if (e->ev1) cudaEventDestroy(e->ev1);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+extern "C" mp_status mp_engine_info(const mp_engine *e, int *sm, int *ma, int *mi) {
+    if (!e) return failf(MP_ERR_ARGUMENT, "engine is NULL");
+    if (sm) *sm = e->smCount;
+    if (ma) *ma = e->ccMajor;
+    if (mi) *mi = e->ccMinor;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_engine_set_tuning(mp_engine *e, const mp_tuning *t) {
+    if (!e || !t) return failf(MP_ERR_ARGUMENT, "engine or tuning is NULL");
+    e->tuning = *t;
+    return MP_OK;
+}
+
+static float probOf(double logp) {
+    return (float) std::exp(logp);
+}
+
+static mp_status lowerModel(const mp_model_desc *d, DevModel &m, float *rp) {
+    if (!d) return failf(MP_ERR_ARGUMENT, "model description is NULL");
+    for (int k = 0; k < 9; k++) {
+        if (std::isnan(d->log_transitions[k]) || d->log_transitions[k] > 1e-9)
+            return failf(MP_ERR_ARGUMENT, "log transition %d is not a log probability (%g)", k, d->log_transitions[k]);
+        m.t[k] = probOf(d->log_transitions[k]);
+    }
+    for (int k = 0; k < 3; k++) {
+        m.start[k] = probOf(d->log_start[k]);
+        m.raggedStart[k] = probOf(d->log_ragged_start[k]);
+        m.end[k] = probOf(d->log_end[k]);
+        m.raggedEnd[k] = probOf(d->log_ragged_end[k]);
+    }
+    for (int k = 0; k < 25; k++) {
+        if (std::isnan(d->log_match[k])) return failf(MP_ERR_ARGUMENT, "log match emission %d is NaN", k);
+        m.match[k] = probOf(d->log_match[k]);
+    }
+    for (int k = 0; k < 5; k++) {
+        m.gapX[k] = probOf(d->log_gap_x[k]);
+        m.gapY[k] = probOf(d->log_gap_y[k]);
+    }
+    m.runLength = d->run_length ? 1 : 0;
+    m.strand = d->strand ? 1 : 0;
+    if (m.runLength) {
+        if (d->max_repeat != kMaxRepeat)
+            return failf(MP_ERR_ARGUMENT, "max_repeat must be %d (got %d)", kMaxRepeat, d->max_repeat);
+        if (!d->repeat_log10) return failf(MP_ERR_ARGUMENT, "run-length model needs repeat_log10");
+        for (int i = 0; i < kRepTable; i++) {
+            double v = d->repeat_log10[i];
+            if (std::isnan(v)) return failf(MP_ERR_ARGUMENT, "repeat table entry %d is NaN", i);
+            rp[i] = (float) std::exp(d->repeat_scale * v);
+        }
+    } else {
+        for (int i = 0; i < kRepTable; i++) rp[i] = 1.0f;
+    }
+    return MP_OK;
+}
+
+extern "C" mp_status mp_model_create(mp_engine *e, const mp_model_desc *fwd, const mp_model_desc *rev,
+                                     mp_model **out) {
+    if (!e || !out) return failf(MP_ERR_ARGUMENT, "engine or out is NULL");
+    *out = nullptr;
+    mp_model *m = new mp_model();
+    m->engine = e;
+    std::vector<float> rp(2 * kRepTable);
+    mp_status s = lowerModel(fwd, m->host[0], rp.data());
+    if (s == MP_OK) s = lowerModel(rev, m->host[1], rp.data() + kRepTable);
+    if (s == MP_OK) {
+        cudaSetDevice(e->device);
+        s = m->models.reserve(sizeof(DevModel) * 2);
+        if (s == MP_OK) s = m->repeat.reserve(sizeof(float) * 2 * kRepTable);
+        if (s == MP_OK) {
+            cudaError_t ce = cudaMemcpy(m->models.p, m->host, sizeof(DevModel) * 2, cudaMemcpyHostToDevice);
+            if (ce == cudaSuccess) ce = cudaMemcpy(m->repeat.p, rp.data(), sizeof(float) * 2 * kRepTable, cudaMemcpyHostToDevice);
+            if (ce != cudaSuccess) s = failf(MP_ERR_CUDA, "model upload failed: %s", cudaGetErrorString(ce));
+        }
+    }
+    if (s != MP_OK) {
+        delete m;
+        return s;
+    }
+    *out = m;
+    return MP_OK;
+}
+
+extern "C" void mp_model_destroy(mp_model *m) {
+    if (!m) return;
+    if (m->engine) cudaSetDevice(m->engine->device);
+    delete m;
+}
+
+// ---------------------------------------------------------------------------
+// geometry helpers (host)
+// ---------------------------------------------------------------------------
+
+static int64_t clampCoord(int64_t z, int64_t lz) {
+    return z < 0 ? 0 : (z > lz ? lz : z);
+}
+
+static bool boxDiagonalHost(int64_t d, int64_t xL, int64_t yL, int64_t xU, int64_t yU, int64_t &lo, int64_t &hi) {
+    int64_t l = xL - yL, h = xU - yU;
+    if ((d + l) & 1) l++;
+    if ((d + h) & 1) h++;
+    int64_t x = (d + l) / 2;
+    if (x < xL) l += 2 * (xL - x);
+    int64_t y = (d - l) / 2;
+    if (yL < y) l += 2 * (y - yL);
+    x = (d + h) / 2;
+    if (xU < x) h -= 2 * (x - xU);
+    y = (d - h) / 2;
+    if (y < yU) h -= 2 * (yU - y);
+    lo = l;
+    hi = h;
+    return l <= h;
+}
+
+extern "C" mp_status mp_band(const int32_t *anchors, int64_t nA, int64_t lx, int64_t ly, int64_t expansion,
+                             int dynamic, int64_t *out) {
+    if (lx < 0 || ly < 0 || (!anchors && nA > 0) || !out) return failf(MP_ERR_ARGUMENT, "mp_band: bad arguments");
+    int64_t xL = 0, yL = 0, xU = 0, yU = 0, e = dynamic ? 0 : expansion, nx = 0, ny = 0, k = 0;
+    for (int64_t d = 0; d <= lx + ly; d++) {
+        int64_t lo, hi;
+        if (!boxDiagonalHost(d, xL, yL, xU, yU, lo, hi))
+            return failf(MP_ERR_ARGUMENT, "invalid diagonal %lld (xmyL %lld > xmyR %lld)", (long long) d,
+                         (long long) lo, (long long) hi);
+        out[3 * d] = d;
+        out[3 * d + 1] = lo;
+        out[3 * d + 2] = hi;
+        if (d == nx + ny) {
+            int64_t px = nx, py = ny;
+            if (k < nA) {
+                nx = anchors[3 * k] + 1;
+                ny = anchors[3 * k + 1] + 1;
+                if (dynamic) e = anchors[3 * k + 2];
+                k++;
+            } else {
+                nx = lx;
+                ny = ly;
+            }
+            int64_t pxay = px + py, pxmy = px - py, nxay = nx + ny, nxmy = nx - ny;
+            xL = clampCoord((pxay + (pxmy - e)) / 2, lx);
+            yL = clampCoord((nxay - (nxmy - e)) / 2, ly);
+            xU = clampCoord((nxay + (nxmy + e)) / 2, lx);
+            yU = clampCoord((pxay - (pxmy + e)) / 2, ly);
+        }
+    }
+    return MP_OK;
+}
+
+struct SplitRect {
+    int64_t x1, y1, x2, y2;
+};
+
+static bool splitGap(int64_t &x1, int64_t &y1, int64_t x2, int64_t y2, int64_t x3, int64_t y3, int64_t maxSize,
+                     bool skip, std::vector<SplitRect> &out) {
+    int64_t gx = x3 - x2, gy = y3 - y2;
+    if (gx * gy > maxSize) {
+        int64_t side = (int64_t) std::sqrt((double) maxSize);
+        int64_t hX = gx / 2 > side ? side : gx / 2;
+        int64_t hY = gy / 2 > side ? side : gy / 2;
+        if (!skip) out.push_back({x1, y1, x2 + hX, y2 + hY});
+        x1 = x3 - hX;
+        y1 = y3 - hY;
+        return true;
+    }
+    return false;
+}
+
+static void splitPoints(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, int64_t maxSize, bool raggedL,
+                        bool raggedR, std::vector<SplitRect> &out) {
+    int64_t x1 = 0, y1 = 0, x2 = 0, y2 = 0;
+    for (int64_t i = 0; i < nA; i++) {
+        int64_t x3 = an[3 * i], y3 = an[3 * i + 1];
+        splitGap(x1, y1, x2, y2, x3, y3, maxSize, raggedL && i == 0, out);
+        x2 = x3 + 1;
+        y2 = y3 + 1;
+    }
+    bool split = splitGap(x1, y1, x2, y2, lx, ly, maxSize, raggedL && nA == 0, out);
+    if (!split || !raggedR) out.push_back({x1, y1, lx, ly});
+}
+
+extern "C" mp_status mp_split_points(const int32_t *anchors, int64_t nA, int64_t lx, int64_t ly, int64_t maxSize,
+                                     int raggedL, int raggedR, int64_t *out, int64_t cap, int64_t *nOut) {
+    if (lx < 0 || ly < 0 || (!anchors && nA > 0)) return failf(MP_ERR_ARGUMENT, "mp_split_points: bad arguments");
+    std::vector<SplitRect> r;
+    splitPoints(anchors, nA, lx, ly, maxSize, raggedL != 0, raggedR != 0, r);
+    for (size_t i = 0; i < r.size() && (int64_t) i < cap; i++) {
+        out[4 * i] = r[i].x1;
+        out[4 * i + 1] = r[i].y1;
+        out[4 * i + 2] = r[i].x2;
+        out[4 * i + 3] = r[i].y2;
+    }
+    if (nOut) *nOut = (int64_t) r.size();
+    return MP_OK;
+}
+
+extern "C" mp_status mp_crop_range(const int32_t *anchors, int64_t nA, int64_t tlen, int64_t rlen, int64_t *start,
+                                   int64_t *end) {
+    if (!start || !end) return failf(MP_ERR_ARGUMENT, "mp_crop_range: NULL output");
+    int64_t s = 0, e = tlen;
+    if (nA > 0) {
+        s = (int64_t) anchors[0] - anchors[1];
+        s = s < 0 ? 0 : s;
+        e = 1 + (int64_t) anchors[3 * (nA - 1)] + (rlen - anchors[3 * (nA - 1) + 1]);
+        e = e > tlen ? tlen : e;
+    }
+    if (s < 0 || s >= tlen || e < 0 || e > tlen)
+        return failf(MP_ERR_ARGUMENT, "crop range [%lld, %lld) outside template of length %lld", (long long) s,
+                     (long long) e, (long long) tlen);
+    *start = s;
+    *end = e;
+    return MP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// planning
+// ---------------------------------------------------------------------------
+
+static const int kClasses[] = {2, 3, 4, 6, 8};
+static const int kNumClasses = 5;
+
+// Upper bound (in window slots) of the hull of 5 consecutive anti-diagonal bands:
+// the union of up to three consecutive anchor boxes, clipped to the matrix.
+static int64_t hullSlotBound(const int32_t *an, int64_t nA, int64_t x1, int64_t y1, int64_t lx, int64_t ly,
+                             bool dynamic, int64_t fixedExp) {
+    int64_t best = 1;
+    int64_t lo1 = 0, hi1 = 0, lo2 = 0, hi2 = 0;  // previous two boxes (diagonal 0 seeds them)
+    for (int64_t k = 0; k <= nA; k++) {
+        int64_t px = 0, py = 0, nx, ny, e;
+        if (k > 0) {
+            px = an[3 * (k - 1)] - x1 + 1;
+            py = an[3 * (k - 1) + 1] - y1 + 1;
+        }
+        if (k < nA) {
+            nx = an[3 * k] - x1 + 1;
+            ny = an[3 * k + 1] - y1 + 1;
+            e = dynamic ? an[3 * k + 2] : fixedExp;
+        } else {
+            nx = lx;
+            ny = ly;
+            e = dynamic ? (nA > 0 ? an[3 * (nA - 1) + 2] : 0) : fixedExp;
+        }
+        int64_t lo = std::max(px - ny - e, -ly), hi = std::min(nx - py + e, lx);
+        int64_t L = std::min(lo, std::min(lo1, lo2)), H = std::max(hi, std::max(hi1, hi2));
+        int64_t span = ((H >> 1) - (L >> 1)) + 1;
+        best = std::max(best, span);
+        lo2 = lo1;
+        hi2 = hi1;
+        lo1 = lo;
+        hi1 = hi;
+    }
+    return best;
+}
+
+static int classFor(int64_t slots) {
+    for (int i = 0; i < kNumClasses; i++) {
+        int C = kClasses[i];
+        if (slots <= 32 * C - 2 * C) return C;
+    }
+    return 0;
+}
+
+struct PlannedTask {
+    Task t;
+    int cls;
+};
+
+struct mp_device_batch {
+    mp_engine *e = nullptr;
+    const mp_model *m = nullptr;
+    mp_params p{};
+    int64_t nJobs = 0;
+    std::vector<Task> tasks;
+    std::vector<int> cls;
+    std::vector<int64_t> jobFirstTask;  // n_jobs+1
+    int64_t totalDiags = 0;
+    int64_t outCap[3] = {0, 0, 0};
+    // device
+    DevBuf xs, ys, anchors, dTasks, band, dOut, outW[3], outX[3], outY[3];
+    DevBuf orders, queue, scratch, scratchScal, resume;
+    std::vector<int> classOrderOff;  // per class offset into orders
+    std::vector<int> classCount;
+    std::vector<int64_t> classMaxN;
+    std::vector<TaskOut> hostOut;
+    int launchesPerRun = 0;
+    bool ran = false;
+};
+
+static mp_status validateJob(const mp_batch *b, int64_t j, const mp_params *p) {
+    int64_t lx = b->x_end[j] - b->x_begin[j];
+    int64_t ly = b->y_offsets[j + 1] - b->y_offsets[j];
+    if (b->x_begin[j] < 0 || b->x_end[j] > b->x_symbols_length || lx < 0)
+        return failf(MP_ERR_ARGUMENT, "job %lld: template range [%lld, %lld) invalid", (long long) j,
+                     (long long) b->x_begin[j], (long long) b->x_end[j]);
+    if (ly < 0) return failf(MP_ERR_ARGUMENT, "job %lld: negative read length", (long long) j);
+    if (lx + ly > (int64_t) 1 << 30) return failf(MP_ERR_ARGUMENT, "job %lld: sequences too long", (long long) j);
+    int64_t a0 = b->anchor_offsets[j], a1 = b->anchor_offsets[j + 1];
+    if (a1 < a0) return failf(MP_ERR_ARGUMENT, "job %lld: anchor offsets decrease", (long long) j);
+    int64_t px = -1, py = -1;
+    for (int64_t i = a0; i < a1; i++) {
+        int64_t x = b->anchors[3 * i], y = b->anchors[3 * i + 1], ex = b->anchors[3 * i + 2];
+        if (x <= px || y <= py || x >= lx || y >= ly)
+            return failf(MP_ERR_ARGUMENT, "job %lld: anchor %lld (%lld, %lld) not strictly increasing / in range",
+                         (long long) j, (long long) (i - a0), (long long) x, (long long) y);
+        if (p->dynamic_anchor_expansion && (ex < 0 || (ex & 1)))
+            return failf(MP_ERR_ARGUMENT, "job %lld: anchor %lld expansion %lld must be even and >= 0",
+                         (long long) j, (long long) (i - a0), (long long) ex);
+        px = x;
+        py = y;
+    }
+    return MP_OK;
+}
+
+static mp_status validateParams(const mp_params *p) {
+    if (!p) return failf(MP_ERR_ARGUMENT, "params is NULL");
+    if (!(p->threshold >= 0.0 && p->threshold <= 1.0))
+        return failf(MP_ERR_ARGUMENT, "threshold %g outside [0, 1]", p->threshold);
+    if (p->threshold <= 0.0) return failf(MP_ERR_ARGUMENT, "threshold 0 (emit every cell) is not supported");
+    if (p->traceback_diagonals < 1) return failf(MP_ERR_ARGUMENT, "traceback_diagonals must be >= 1");
+    if (p->diagonal_expansion < 0 || (p->diagonal_expansion & 1))
+        return failf(MP_ERR_ARGUMENT, "diagonal_expansion must be even and >= 0");
+    if (p->min_diags_between_traceback < 2) return failf(MP_ERR_ARGUMENT, "min_diags_between_traceback must be >= 2");
+    if (p->traceback_diagonals + 1 >= p->min_diags_between_traceback)
+        return failf(MP_ERR_ARGUMENT, "traceback_diagonals + 1 must be < min_diags_between_traceback");
+    return MP_OK;
+}
+
+static mp_status planBatch(mp_device_batch *db, const mp_batch *b) {
+    const int64_t nJobs = b->n_jobs;
+    const mp_params *p = &db->p;
+    unsigned nThreads = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+    if (nJobs < 64) nThreads = 1;
+    std::vector<std::vector<PlannedTask>> perThread(nThreads);
+    std::vector<std::vector<int64_t>> perThreadJobCount(nThreads);
+    std::vector<mp_status> statuses(nThreads, MP_OK);
+    std::vector<std::string> errors(nThreads);
+    int64_t chunk = (nJobs + nThreads - 1) / nThreads;
+    auto work = [&](unsigned t) {
+        int64_t j0 = t * chunk, j1 = std::min(nJobs, j0 + chunk);
+        std::vector<SplitRect> rects;
+        for (int64_t j = j0; j < j1; j++) {
+            mp_status s = validateJob(b, j, p);
+            if (s != MP_OK) {
+                statuses[t] = s;
+                errors[t] = g_lastError;
+                return;
+            }
+            int64_t lx = b->x_end[j] - b->x_begin[j];
+            int64_t ly = b->y_offsets[j + 1] - b->y_offsets[j];
+            const int32_t *an = b->anchors + 3 * b->anchor_offsets[j];
+            int64_t nA = b->anchor_offsets[j + 1] - b->anchor_offsets[j];
+            bool rL = b->ragged_left ? b->ragged_left[j] != 0 : false;
+            bool rR = b->ragged_right ? b->ragged_right[j] != 0 : false;
+            rects.clear();
+            splitPoints(an, nA, lx, ly, p->split_matrix_bigger_than_this, rL, rR, rects);
+            int64_t ai = 0;
+            int64_t count = 0;
+            for (size_t i = 0; i < rects.size(); i++) {
+                const SplitRect &r = rects[i];
+                int64_t first = ai;
+                while (ai < nA) {
+                    int64_t x = an[3 * ai], y = an[3 * ai + 1];
+                    if (x + y >= r.x2 + r.y2) break;
+                    ai++;
+                }
+                PlannedTask pt;
+                memset(&pt, 0, sizeof(pt));
+                Task &tk = pt.t;
+                tk.lx = (int32_t) (r.x2 - r.x1);
+                tk.ly = (int32_t) (r.y2 - r.y1);
+                tk.xOff = b->x_begin[j] + r.x1;
+                tk.yOff = b->y_offsets[j] + r.y1;
+                tk.anchorOff = b->anchor_offsets[j] + first;
+                tk.nAnchors = (int32_t) (ai - first);
+                tk.x1 = (int32_t) r.x1;
+                tk.y1 = (int32_t) r.y1;
+                tk.xShift = b->x_shift ? (int32_t) b->x_shift[j] : 0;
+                bool tl = rL || i > 0, tr = rR || i + 1 < rects.size();
+                tk.flags = (tl ? 1 : 0) | (tr ? 2 : 0) | ((b->strand && b->strand[j]) ? 4 : 0) |
+                           (p->dynamic_anchor_expansion ? 8 : 0);
+                tk.job = (int32_t) j;
+                tk.expansion = (int32_t) p->diagonal_expansion;
+                int64_t slots = hullSlotBound(an + 3 * first, tk.nAnchors, r.x1, r.y1, tk.lx, tk.ly,
+                                              p->dynamic_anchor_expansion != 0, p->diagonal_expansion);
+                pt.cls = classFor(slots);
+                if (pt.cls == 0) {
+                    statuses[t] = failf(MP_ERR_OVERFLOW,
+                                        "job %lld: band hull of %lld slots exceeds the widest slot class (%d)",
+                                        (long long) j, (long long) slots, 32 * 8 - 16);
+                    errors[t] = g_lastError;
+                    return;
+                }
+                perThread[t].push_back(pt);
+                count++;
+            }
+            perThreadJobCount[t].push_back(count);
+        }
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nThreads; t++) th.emplace_back(work, t);
+    work(0);
+    for (auto &x : th) x.join();
+    for (unsigned t = 0; t < nThreads; t++) {
+        if (statuses[t] != MP_OK) {
+            g_lastError = errors[t];
+            return statuses[t];
+        }
+    }
+    // assemble in job order
+    db->tasks.clear();
+    db->cls.clear();
+    db->jobFirstTask.assign(1, 0);
+    for (unsigned t = 0; t < nThreads; t++) {
+        for (auto &pt : perThread[t]) {
+            db->tasks.push_back(pt.t);
+            db->cls.push_back(pt.cls);
+        }
+        for (int64_t c : perThreadJobCount[t]) db->jobFirstTask.push_back(db->jobFirstTask.back() + c);
+    }
+    // band / output offsets
+    int64_t bandOff = 0;
+    int64_t outOff[3] = {0, 0, 0};
+    for (auto &tk : db->tasks) {
+        int64_t N = (int64_t) tk.lx + tk.ly;
+        tk.bandOff = bandOff;
+        bandOff += N + 1;
+        // capacity: measured densities are ~0.75 match and ~0.45 gap tuples per anti-diagonal at
+        // threshold 0.01; overflowing tasks are re-run with their exact counts
+        int32_t capM = (int32_t) (N + N / 8 + 64), capX = (int32_t) (N * 3 / 4 + 64), capY = (int32_t) (N * 3 / 4 + 64);
+        int32_t caps[3] = {capM, capX, capY};
+        for (int k = 0; k < 3; k++) {
+            tk.cap[k] = caps[k];
+            tk.outOff[k] = outOff[k];
+            outOff[k] += caps[k];
+        }
+    }
+    db->totalDiags = bandOff;
+    for (int k = 0; k < 3; k++) db->outCap[k] = outOff[k];
+    return MP_OK;
+}
+
+// Builds the per-class length-sorted queues for the tasks in `subset`.
+static void buildQueues(mp_device_batch *db, const std::vector<int32_t> &subset, std::vector<int32_t> &orderHost) {
+    db->classOrderOff.assign(kNumClasses + 1, 0);
+    db->classCount.assign(kNumClasses, 0);
+    db->classMaxN.assign(kNumClasses, 0);
+    std::vector<std::vector<int32_t>> per(kNumClasses);
+    for (int32_t t : subset) {
+        int ci = 0;
+        while (kClasses[ci] != db->cls[t]) ci++;
+        per[ci].push_back(t);
+        int64_t N = (int64_t) db->tasks[t].lx + db->tasks[t].ly;
+        db->classMaxN[ci] = std::max(db->classMaxN[ci], N);
+    }
+    orderHost.clear();
+    for (int ci = 0; ci < kNumClasses; ci++) {
+        auto &v = per[ci];
+        std::stable_sort(v.begin(), v.end(), [&](int32_t a, int32_t b) {
+            return (db->tasks[a].lx + db->tasks[a].ly) > (db->tasks[b].lx + db->tasks[b].ly);
+        });
+        db->classOrderOff[ci] = (int) orderHost.size();
+        db->classCount[ci] = (int) v.size();
+        orderHost.insert(orderHost.end(), v.begin(), v.end());
+    }
+    db->classOrderOff[kNumClasses] = (int) orderHost.size();
+}
+
+static mp_status upload(DevBuf &buf, const void *src, size_t bytes, cudaStream_t s) {
+    MP_TRY(buf.reserve(bytes));
+    if (bytes) CUDA_TRY(cudaMemcpyAsync(buf.p, src, bytes, cudaMemcpyHostToDevice, s));
+    return MP_OK;
+}
+
+extern "C" mp_status mp_device_batch_create(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
+                                            mp_device_batch **out) {
+    if (!e || !m || !b || !out) return failf(MP_ERR_ARGUMENT, "mp_device_batch_create: NULL argument");
+    *out = nullptr;
+    MP_TRY(validateParams(p));
+    if (b->n_jobs < 0) return failf(MP_ERR_ARGUMENT, "negative job count");
+    if (b->n_jobs > 0 && (!b->x_begin || !b->x_end || !b->y_offsets || !b->anchor_offsets || !b->strand))
+        return failf(MP_ERR_ARGUMENT, "batch arrays missing");
+    CUDA_TRY(cudaSetDevice(e->device));
+    mp_device_batch *db = new mp_device_batch();
+    db->e = e;
+    db->m = m;
+    db->p = *p;
+    db->nJobs = b->n_jobs;
+    mp_status s = planBatch(db, b);
+    if (s != MP_OK) {
+        delete db;
+        return s;
+    }
+    cudaStream_t st = e->stream;
+    int64_t ny = b->n_jobs > 0 ? b->y_offsets[b->n_jobs] : 0;
+    int64_t na = b->n_jobs > 0 ? b->anchor_offsets[b->n_jobs] : 0;
+    s = upload(db->xs, b->x_symbols, sizeof(uint16_t) * b->x_symbols_length, st);
+    if (s == MP_OK) s = upload(db->ys, b->y_symbols, sizeof(uint16_t) * ny, st);
+    if (s == MP_OK) s = upload(db->anchors, b->anchors, sizeof(int32_t) * 3 * na, st);
+    if (s == MP_OK) s = upload(db->dTasks, db->tasks.data(), sizeof(Task) * db->tasks.size(), st);
+    if (s == MP_OK) s = db->band.reserve(sizeof(int4) * std::max<int64_t>(db->totalDiags, 1));
+    if (s == MP_OK) s = db->dOut.reserve(sizeof(TaskOut) * std::max<size_t>(db->tasks.size(), 1));
+    for (int k = 0; k < 3 && s == MP_OK; k++) {
+        size_t n = sizeof(int32_t) * std::max<int64_t>(db->outCap[k], 1);
+        s = db->outW[k].reserve(n);
+        if (s == MP_OK) s = db->outX[k].reserve(n);
+        if (s == MP_OK) s = db->outY[k].reserve(n);
+    }
+    if (s == MP_OK) s = db->queue.reserve(sizeof(int32_t) * kNumClasses);
+    if (s == MP_OK) {
+        cudaError_t ce = cudaStreamSynchronize(st);
+        if (ce != cudaSuccess) s = failf(MP_ERR_CUDA, "upload failed: %s", cudaGetErrorString(ce));
+    }
+    if (s != MP_OK) {
+        delete db;
+        return s;
+    }
+    *out = db;
+    return MP_OK;
+}
+
+static mp_status ensureScratch(mp_device_batch *db, int C, int64_t maxN, int warpsTotal, int &scratchBlocks) {
+    int K = classStride(C);
+    scratchBlocks = (int) (maxN / K + 2);
+    size_t perWarp = (size_t) scratchBlocks * C * 32 * sizeof(float4);
+    MP_TRY(db->scratch.reserve(perWarp * warpsTotal));
+    MP_TRY(db->scratchScal.reserve(sizeof(int2) * (size_t) scratchBlocks * warpsTotal));
+    MP_TRY(db->resume.reserve(sizeof(float4) * C * 32 * (size_t) warpsTotal));
+    return MP_OK;
+}
+
+// Launches the posterior kernels for the current queues.
+static mp_status launchQueues(mp_device_batch *db) {
+    mp_engine *e = db->e;
+    cudaStream_t st = e->stream;
+    CUDA_TRY(cudaMemsetAsync(db->queue.p, 0, sizeof(int32_t) * kNumClasses, st));
+    for (int ci = 0; ci < kNumClasses; ci++) {
+        if (db->classCount[ci] == 0) continue;
+        int C = kClasses[ci];
+        int warps = e->tuning.warps_per_block > 0 ? e->tuning.warps_per_block : classMaxWarps(C);
+        warps = std::min(warps, classMaxWarps(C));
+        int blocksPerSm = e->tuning.blocks_per_sm > 0 ? e->tuning.blocks_per_sm : 1;
+        int blocks = e->smCount * blocksPerSm;
+        // do not launch more warps than tasks
+        int maxBlocks = (db->classCount[ci] + warps - 1) / warps;
+        blocks = std::max(1, std::min(blocks, maxBlocks));
+        int scratchBlocks = 0;
+        MP_TRY(ensureScratch(db, C, db->classMaxN[ci], blocks * warps, scratchBlocks));
+        DpArgs a;
+        memset(&a, 0, sizeof(a));
+        a.tasks = db->dTasks.as<Task>();
+        a.order = db->orders.as<int32_t>() + db->classOrderOff[ci];
+        a.nTasks = db->classCount[ci];
+        a.scratchBlocks = scratchBlocks;
+        a.queue = db->queue.as<int32_t>() + ci;
+        a.xs = db->xs.as<uint16_t>();
+        a.ys = db->ys.as<uint16_t>();
+        a.band = db->band.as<int2>();
+        a.models = db->m->models.as<DevModel>();
+        a.repeatProb = db->m->repeat.as<float>();
+        a.scratch = db->scratch.as<float4>();
+        a.scratchScalars = db->scratchScal.as<int2>();
+        a.resume = db->resume.as<float4>();
+        for (int k = 0; k < 3; k++) {
+            a.outW[k] = db->outW[k].as<int32_t>();
+            a.outX[k] = db->outX[k].as<int32_t>();
+            a.outY[k] = db->outY[k].as<int32_t>();
+        }
+        a.out = db->dOut.as<TaskOut>();
+        a.threshold = (float) db->p.threshold;
+        a.minDiagsBetweenTraceBack = (int32_t) std::min<int64_t>(db->p.min_diags_between_traceback, 1 << 30);
+        a.traceBackDiagonals = (int32_t) db->p.traceback_diagonals;
+        a.diagonalExpansion = (int32_t) std::min<int64_t>(db->p.diagonal_expansion, 1 << 29);
+        CUDA_TRY(launchPosterior(C, a, blocks, warps, st));
+        db->launchesPerRun++;
+    }
+    return MP_OK;
+}
+
+extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, float *kernelMs) {
+    if (!e || !db) return failf(MP_ERR_ARGUMENT, "mp_device_batch_run: NULL argument");
+    CUDA_TRY(cudaSetDevice(e->device));
+    cudaStream_t st = e->stream;
+    const int nTasks = (int) db->tasks.size();
+    db->launchesPerRun = 0;
+    std::vector<int32_t> all(nTasks), orderHost;
+    for (int i = 0; i < nTasks; i++) all[i] = i;
+    buildQueues(db, all, orderHost);
+    MP_TRY(upload(db->orders, orderHost.data(), sizeof(int32_t) * std::max<size_t>(orderHost.size(), 1), st));
+    CUDA_TRY(cudaEventRecord(e->ev0, st));
+    BandArgs ba;
+    ba.tasks = db->dTasks.as<Task>();
+    ba.nTasks = nTasks;
+    ba.anchors = db->anchors.as<int32_t>();
+    ba.band = db->band.as<int2>();
+    ba.out = db->dOut.as<TaskOut>();
+    CUDA_TRY(launchBand(ba, st));
+    db->launchesPerRun += nTasks > 0 ? 2 : 0;
+    MP_TRY(launchQueues(db));
+    CUDA_TRY(cudaEventRecord(e->ev1, st));
+    // statuses
+    db->hostOut.resize(nTasks);
+    if (nTasks) CUDA_TRY(cudaMemcpyAsync(db->hostOut.data(), db->dOut.p, sizeof(TaskOut) * nTasks, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    float ms = 0.0f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+    // retries: capacity overflows (exact counts known), window overflows (next class), scratch
+    for (int round = 0; round < 4; round++) {
+        std::vector<int32_t> retry;
+        bool changed = false;
+        for (int t = 0; t < nTasks; t++) {
+            TaskOut &o = db->hostOut[t];
+            if (o.status & kTaskBand) {
+                return failf(MP_ERR_ARGUMENT, "job %d: invalid band diagonal (anchors inconsistent with lengths)",
+                             db->tasks[t].job);
+            }
+            if (o.status & (kTaskCapacity | kTaskWindow | kTaskScratch)) {
+                if (o.status & kTaskWindow) {
+                    int ci = 0;
+                    while (kClasses[ci] != db->cls[t]) ci++;
+                    if (ci + 1 >= kNumClasses)
+                        return failf(MP_ERR_OVERFLOW, "job %d: band wider than the widest slot class", db->tasks[t].job);
+                    db->cls[t] = kClasses[ci + 1];
+                }
+                if (o.status & kTaskCapacity) {
+                    for (int k = 0; k < 3; k++) {
+                        if (o.count[k] > db->tasks[t].cap[k]) {
+                            // new region at the end of the list buffer
+                            db->tasks[t].cap[k] = o.count[k] + 16;
+                            db->tasks[t].outOff[k] = db->outCap[k];
+                            db->outCap[k] += db->tasks[t].cap[k];
+                        }
+                    }
+                }
+                retry.push_back(t);
+                changed = true;
+            }
+        }
+        if (!changed) break;
+        // grow output buffers (preserving contents)
+        for (int k = 0; k < 3; k++) {
+            size_t need = sizeof(int32_t) * db->outCap[k];
+            if (need > db->outW[k].bytes) {
+                DevBuf *bufs[3] = {&db->outW[k], &db->outX[k], &db->outY[k]};
+                for (DevBuf *bb : bufs) {
+                    void *np = nullptr;
+                    CUDA_TRY(cudaMalloc(&np, need));
+                    CUDA_TRY(cudaMemcpyAsync(np, bb->p, bb->bytes, cudaMemcpyDeviceToDevice, st));
+                    CUDA_TRY(cudaStreamSynchronize(st));
+                    cudaFree(bb->p);
+                    bb->p = np;
+                    bb->bytes = need;
+                }
+            }
+        }
+        MP_TRY(upload(db->dTasks, db->tasks.data(), sizeof(Task) * nTasks, st));
+        // reset statuses of retried tasks (band flags stay valid)
+        for (int32_t t : retry) db->hostOut[t].status = 0;
+        CUDA_TRY(cudaMemcpyAsync(db->dOut.p, db->hostOut.data(), sizeof(TaskOut) * nTasks, cudaMemcpyHostToDevice, st));
+        buildQueues(db, retry, orderHost);
+        MP_TRY(upload(db->orders, orderHost.data(), sizeof(int32_t) * std::max<size_t>(orderHost.size(), 1), st));
+        CUDA_TRY(cudaEventRecord(e->ev0, st));
+        MP_TRY(launchQueues(db));
+        CUDA_TRY(cudaEventRecord(e->ev1, st));
+        CUDA_TRY(cudaMemcpyAsync(db->hostOut.data(), db->dOut.p, sizeof(TaskOut) * nTasks, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        float ms2 = 0.0f;
+        CUDA_TRY(cudaEventElapsedTime(&ms2, e->ev0, e->ev1));
+        ms += ms2;
+    }
+    for (int t = 0; t < nTasks; t++) {
+        if (db->hostOut[t].status != 0)
+            return failf(MP_ERR_OVERFLOW, "job %d: task status %d after retries", db->tasks[t].job, db->hostOut[t].status);
+    }
+    if (kernelMs) *kernelMs = ms;
+    db->ran = true;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_device_batch_stats(const mp_device_batch *db, int64_t *cells, int64_t *nTasks,
+                                           int32_t *launches) {
+    if (!db) return failf(MP_ERR_ARGUMENT, "batch is NULL");
+    int64_t c = 0;
+    for (auto &o : db->hostOut) c += o.cells;
+    if (cells) *cells = c;
+    if (nTasks) *nTasks = (int64_t) db->tasks.size();
+    if (launches) *launches = db->launchesPerRun;
+    return MP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// results
+// ---------------------------------------------------------------------------
+
+struct mp_result {
+    int64_t nJobs = 0;
+    std::vector<int64_t> off[3];
+    std::vector<int32_t> w[3], x[3], y[3];
+    std::vector<double> logLik;
+    std::vector<int64_t> cells;
+    int64_t totalCells = 0;
+    double deviceMs = 0.0;
+};
+
+extern "C" mp_status mp_device_batch_fetch(mp_engine *e, mp_device_batch *db, mp_result **out) {
+    if (!e || !db || !out) return failf(MP_ERR_ARGUMENT, "mp_device_batch_fetch: NULL argument");
+    if (!db->ran) return failf(MP_ERR_STATE, "mp_device_batch_fetch before a successful run");
+    CUDA_TRY(cudaSetDevice(e->device));
+    cudaStream_t st = e->stream;
+    const int nTasks = (int) db->tasks.size();
+    mp_result *r = new mp_result();
+    r->nJobs = db->nJobs;
+    std::vector<int64_t> dst[3];
+    int64_t total[3] = {0, 0, 0};
+    for (int k = 0; k < 3; k++) {
+        dst[k].resize(std::max(nTasks, 1));
+        r->off[k].assign(db->nJobs + 1, 0);
+    }
+    r->logLik.assign(db->nJobs, 0.0);
+    r->cells.assign(db->nJobs, 0);
+    for (int64_t j = 0; j < db->nJobs; j++) {
+        for (int64_t t = db->jobFirstTask[j]; t < db->jobFirstTask[j + 1]; t++) {
+            const TaskOut &o = db->hostOut[t];
+            for (int k = 0; k < 3; k++) {
+                dst[k][t] = total[k];
+                total[k] += o.count[k];
+            }
+            r->logLik[j] += o.logLik;
+            r->cells[j] += o.cells;
+        }
+        for (int k = 0; k < 3; k++) r->off[k][j + 1] = total[k];
+        r->totalCells += r->cells[j];
+    }
+    DevBuf dDst[3], fW[3], fX[3], fY[3], ptrs;
+    mp_status s = MP_OK;
+    for (int k = 0; k < 3 && s == MP_OK; k++) {
+        s = upload(dDst[k], dst[k].data(), sizeof(int64_t) * dst[k].size(), st);
+        size_t n = sizeof(int32_t) * std::max<int64_t>(total[k], 1);
+        if (s == MP_OK) s = fW[k].reserve(n);
+        if (s == MP_OK) s = fX[k].reserve(n);
+        if (s == MP_OK) s = fY[k].reserve(n);
+    }
+    int32_t *hp[12];
+    for (int k = 0; k < 3; k++) {
+        hp[k] = db->outW[k].as<int32_t>();
+        hp[3 + k] = db->outX[k].as<int32_t>();
+        hp[6 + k] = db->outY[k].as<int32_t>();
+    }
+    int32_t *fp[9];
+    for (int k = 0; k < 3; k++) {
+        fp[k] = fW[k].as<int32_t>();
+        fp[3 + k] = fX[k].as<int32_t>();
+        fp[6 + k] = fY[k].as<int32_t>();
+    }
+    if (s == MP_OK) s = ptrs.reserve(sizeof(int32_t *) * 18);
+    if (s == MP_OK) {
+        int32_t *all[18];
+        for (int i = 0; i < 9; i++) all[i] = hp[i];
+        for (int i = 0; i < 9; i++) all[9 + i] = fp[i];
+        cudaError_t ce = cudaMemcpyAsync(ptrs.p, all, sizeof(all), cudaMemcpyHostToDevice, st);
+        if (ce != cudaSuccess) s = failf(MP_ERR_CUDA, "pointer upload failed: %s", cudaGetErrorString(ce));
+    }
+    if (s == MP_OK) {
+        int32_t *const *dp = ptrs.as<int32_t *>();
+        cudaError_t ce = launchCompact(db->dTasks.as<Task>(), db->dOut.as<TaskOut>(), nTasks, dDst[0].as<int64_t>(),
+                                       dDst[1].as<int64_t>(), dDst[2].as<int64_t>(), dp, dp + 3, dp + 6, dp + 9,
+                                       dp + 12, dp + 15, st);
+        if (ce != cudaSuccess) s = failf(MP_ERR_CUDA, "compaction launch failed: %s", cudaGetErrorString(ce));
+    }
+    for (int k = 0; k < 3 && s == MP_OK; k++) {
+        r->w[k].resize(total[k]);
+        r->x[k].resize(total[k]);
+        r->y[k].resize(total[k]);
+        if (total[k]) {
+            cudaError_t ce = cudaMemcpyAsync(r->w[k].data(), fW[k].p, sizeof(int32_t) * total[k], cudaMemcpyDeviceToHost, st);
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(r->x[k].data(), fX[k].p, sizeof(int32_t) * total[k], cudaMemcpyDeviceToHost, st);
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(r->y[k].data(), fY[k].p, sizeof(int32_t) * total[k], cudaMemcpyDeviceToHost, st);
+            if (ce != cudaSuccess) s = failf(MP_ERR_CUDA, "result download failed: %s", cudaGetErrorString(ce));
+        }
+    }
+    if (s == MP_OK) {
+        cudaError_t ce = cudaStreamSynchronize(st);
+        if (ce != cudaSuccess) s = failf(MP_ERR_CUDA, "fetch failed: %s", cudaGetErrorString(ce));
+    }
+    if (s != MP_OK) {
+        delete r;
+        return s;
+    }
+    *out = r;
+    return MP_OK;
+}
+
+extern "C" void mp_device_batch_destroy(mp_device_batch *db) {
+    if (!db) return;
+    if (db->e) cudaSetDevice(db->e->device);
+    delete db;
+}
+
+extern "C" mp_status mp_result_view_get(const mp_result *r, mp_result_view *v) {
+    if (!r || !v) return failf(MP_ERR_ARGUMENT, "mp_result_view_get: NULL argument");
+    v->n_jobs = r->nJobs;
+    for (int k = 0; k < 3; k++) {
+        v->offsets[k] = r->off[k].data();
+        v->weight[k] = r->w[k].data();
+        v->x[k] = r->x[k].data();
+        v->y[k] = r->y[k].data();
+    }
+    v->log_likelihood = r->logLik.data();
+    v->cells = r->cells.data();
+    v->total_cells = r->totalCells;
+    v->device_ms = r->deviceMs;
+    return MP_OK;
+}
+
+extern "C" void mp_result_destroy(mp_result *r) {
+    delete r;
+}
+
+extern "C" mp_status mp_realign_batch(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
+                                      mp_result **out) {
+    if (!out) return failf(MP_ERR_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    mp_device_batch *db = nullptr;
+    MP_TRY(mp_device_batch_create(e, m, p, b, &db));
+    float ms = 0.0f;
+    mp_status s = mp_device_batch_run(e, db, &ms);
+    if (s == MP_OK) s = mp_device_batch_fetch(e, db, out);
+    if (s == MP_OK) (*out)->deviceMs = ms;
+    mp_device_batch_destroy(db);
+    return s;
+}

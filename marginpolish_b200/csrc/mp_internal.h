@@ -1,0 +1,95 @@
+// Internal definitions shared by the host planner (mp_api.cu) and the device
+// kernels (mp_kernels.cu) of the realignment engine.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mp {
+
+constexpr int kMaxRepeat = 51;                       // inc/margin.h:123
+constexpr int kRepTable = 4 * kMaxRepeat * kMaxRepeat; // one strand's run-length table
+constexpr int kProbOne = 10000000;                   // inc/pairwiseAligner.h:26
+
+// Lowered state machine of one read strand in probability space (FP32).
+struct DevModel {
+    float t[9];            // transitions from*3+to (0 match, 1 gap-x, 2 gap-y)
+    float start[3];
+    float raggedStart[3];
+    float end[3];
+    float raggedEnd[3];
+    float match[25];       // [xbase*5 + ybase], base 4 = 'N'
+    float gapX[5];
+    float gapY[5];
+    int32_t runLength;     // symbols carry repeat counts
+    int32_t strand;        // repeat-table strand flag (row = strand ? base : 3 - base)
+    int32_t pad[2];
+};
+
+// One banded sub-problem (one split rectangle of one job).
+struct Task {
+    int64_t xOff;          // first X symbol of the sub-problem (device symbol buffer index)
+    int64_t yOff;          // first Y symbol
+    int64_t bandOff;       // first diagonal record in the band buffer (N+1 records)
+    int64_t anchorOff;     // first anchor triple of the sub-problem (original coordinates)
+    int64_t outOff[3];     // start of this task's output region per list
+    int32_t cap[3];        // capacity per list (tuples)
+    int32_t nAnchors;
+    int32_t lx, ly;        // sub-problem lengths
+    int32_t x1, y1;        // split origin (subtracted from anchors, added to outputs)
+    int32_t xShift;        // job-level x shift added to outputs (reference crop start)
+    int32_t flags;         // bit0 ragged left, bit1 ragged right, bit2 forward strand, bit3 dynamic expansion
+    int32_t job;
+    int32_t expansion;     // fixed expansion when not dynamic
+    int32_t pad[2];
+};
+
+enum TaskStatus : int32_t {
+    kTaskOk = 0,
+    kTaskCapacity = 1,     // an output list needed more than its capacity (counts are exact)
+    kTaskWindow = 2,       // band hull wider than the slot window of the class
+    kTaskBand = 4,         // invalid diagonal (reference: exception)
+    kTaskScratch = 8       // checkpoint scratch too small
+};
+
+struct TaskOut {
+    int32_t count[3];
+    int32_t status;
+    double logLik;         // natural log of the final segment's total probability
+    int64_t cells;         // sum of band widths
+};
+
+// Kernel-wide parameters of a posterior launch.
+struct DpArgs {
+    const Task *tasks;
+    const int32_t *order;       // task indices in queue order (longest first)
+    int32_t nTasks;
+    int32_t scratchBlocks;      // checkpoints available per warp
+    int32_t *queue;             // global work counter
+    const uint16_t *xs;
+    const uint16_t *ys;
+    const int2 *band;           // (xmyL, xmyR) per diagonal
+    const DevModel *models;     // [0] forward strand, [1] reverse strand
+    const float *repeatProb;    // [2][4][51][51] exp(scale*log10 table), per model
+    float4 *scratch;            // per-warp checkpoints
+    int2 *scratchScalars;       // per-warp (exponent, window) per checkpoint
+    float4 *resume;             // per-warp forward state saved across a traceback walk
+    int32_t *outW[3];
+    int32_t *outX[3];
+    int32_t *outY[3];
+    TaskOut *out;
+    float threshold;
+    int32_t minDiagsBetweenTraceBack;
+    int32_t traceBackDiagonals;
+    int32_t diagonalExpansion;
+};
+
+struct BandArgs {
+    const Task *tasks;
+    int32_t nTasks;
+    const int32_t *anchors;     // triples, original job coordinates
+    int2 *band;
+    TaskOut *out;
+};
+
+}  // namespace mp

@@ -1,0 +1,259 @@
+"""Host-side interface of the realignment pass, mirroring the reference's
+operator API for this path:
+
+* ``get_aligned_pairs_with_indels_using_anchors`` -- getAlignedPairsWithIndelsUsingAnchors
+  (impl/pairwiseAligner.c:1105-1130): match, gap-x and gap-y posterior tuples
+  (weight, x, y) of one read, in the reference's output order;
+* ``get_aligned_pairs_using_anchors`` -- getAlignedPairsUsingAnchors (:1088-1103);
+* ``get_aligned_pairs_with_indels_cropping_reference`` -- the per-read call of
+  poa_realign (impl/polisher.c:605-654), including the reference crop and the
+  gap-x -> deletes / gap-y -> inserts naming;
+* ``realign_batch`` -- all reads of all chunks in one call (the batched form
+  poa_realignAll's per-read loop maps onto).
+
+Every call goes through the CUDA library (libmpgpu.so); errors of the C ABI
+are raised as MpError.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import c_float, c_int32, c_int64, c_uint8, c_uint16, c_void_p
+from .params import AlignmentParams, PolishModel, StateModel
+
+
+class Engine:
+    """One CUDA device (one process per GPU)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = _lib.load()
+        h = c_void_p()
+        _lib.check(self._lib.mp_engine_create(device, ctypes.byref(h)))
+        self.handle = h
+        sm, ma, mi = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.check(self._lib.mp_engine_info(h, sm, ma, mi))
+        self.sm_count, self.cc = sm.value, (ma.value, mi.value)
+
+    def set_tuning(self, warps_per_block: int = 0, blocks_per_sm: int = 0) -> None:
+        t = _lib.Tuning(0, warps_per_block, blocks_per_sm, 0)
+        _lib.check(self._lib.mp_engine_set_tuning(self.handle, ctypes.byref(t)))
+
+    def close(self) -> None:
+        if self.handle:
+            self._lib.mp_engine_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Model:
+    """Forward- and reverse-strand machines resident on the device."""
+
+    def __init__(self, engine: Engine, forward: StateModel, reverse: StateModel):
+        self.engine = engine
+        self._fd, self._rd = forward.desc(), reverse.desc()
+        self._keep = (forward, reverse)
+        h = c_void_p()
+        _lib.check(engine._lib.mp_model_create(engine.handle, ctypes.byref(self._fd), ctypes.byref(self._rd),
+                                               ctypes.byref(h)))
+        self.handle = h
+
+    @classmethod
+    def from_polish(cls, engine: Engine, pm: PolishModel) -> "Model":
+        return cls(engine, pm.forward, pm.reverse)
+
+    def close(self) -> None:
+        if self.handle:
+            self.engine._lib.mp_model_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class Jobs:
+    """A batch of alignment jobs (host arrays). Job j aligns
+    y_symbols[y_offsets[j]:y_offsets[j+1]] against x_symbols[x_begin[j]:x_end[j]]."""
+
+    x_symbols: np.ndarray
+    x_begin: np.ndarray
+    x_end: np.ndarray
+    y_symbols: np.ndarray
+    y_offsets: np.ndarray
+    anchors: np.ndarray          # (n, 3) int32 in job coordinates
+    anchor_offsets: np.ndarray
+    strand: np.ndarray           # uint8, 1 forward
+    ragged_left: Optional[np.ndarray] = None
+    ragged_right: Optional[np.ndarray] = None
+    x_shift: Optional[np.ndarray] = None
+    _keep: list = field(default_factory=list, repr=False)
+
+    def __post_init__(self):
+        self.x_symbols = np.ascontiguousarray(self.x_symbols, dtype=np.uint16)
+        self.x_begin = np.ascontiguousarray(self.x_begin, dtype=np.int64)
+        self.x_end = np.ascontiguousarray(self.x_end, dtype=np.int64)
+        self.y_symbols = np.ascontiguousarray(self.y_symbols, dtype=np.uint16)
+        self.y_offsets = np.ascontiguousarray(self.y_offsets, dtype=np.int64)
+        self.anchors = np.ascontiguousarray(np.asarray(self.anchors, dtype=np.int32).reshape(-1, 3))
+        self.anchor_offsets = np.ascontiguousarray(self.anchor_offsets, dtype=np.int64)
+        self.strand = np.ascontiguousarray(self.strand, dtype=np.uint8)
+        for name in ("ragged_left", "ragged_right"):
+            v = getattr(self, name)
+            if v is not None:
+                setattr(self, name, np.ascontiguousarray(v, dtype=np.uint8))
+        if self.x_shift is not None:
+            self.x_shift = np.ascontiguousarray(self.x_shift, dtype=np.int64)
+
+    @property
+    def n_jobs(self) -> int:
+        return int(self.x_begin.shape[0])
+
+    def struct(self) -> _lib.Batch:
+        b = _lib.Batch()
+        b.n_jobs = self.n_jobs
+        b.x_begin = _lib.ptr(self.x_begin, c_int64)
+        b.x_end = _lib.ptr(self.x_end, c_int64)
+        b.x_symbols_length = int(self.x_symbols.shape[0])
+        xs = self.x_symbols if self.x_symbols.size else np.zeros(1, np.uint16)
+        ys = self.y_symbols if self.y_symbols.size else np.zeros(1, np.uint16)
+        an = self.anchors if self.anchors.size else np.zeros((1, 3), np.int32)
+        self._keep = [xs, ys, an]
+        b.x_symbols = _lib.ptr(xs, c_uint16)
+        b.y_offsets = _lib.ptr(self.y_offsets, c_int64)
+        b.y_symbols = _lib.ptr(ys, c_uint16)
+        b.anchor_offsets = _lib.ptr(self.anchor_offsets, c_int64)
+        b.anchors = _lib.ptr(an, c_int32)
+        b.strand = _lib.ptr(self.strand, c_uint8)
+        b.ragged_left = _lib.ptr(self.ragged_left, c_uint8)
+        b.ragged_right = _lib.ptr(self.ragged_right, c_uint8)
+        b.x_shift = _lib.ptr(self.x_shift, c_int64)
+        return b
+
+    @classmethod
+    def single(cls, sx, sy, anchors, strand: int = 1, ragged_left: bool = False, ragged_right: bool = False,
+               x_shift: int = 0) -> "Jobs":
+        sx = np.asarray(sx, dtype=np.uint16)
+        sy = np.asarray(sy, dtype=np.uint16)
+        a = np.asarray(anchors, dtype=np.int32).reshape(-1, 3)
+        return cls(sx, np.array([0]), np.array([sx.size]), sy, np.array([0, sy.size]), a,
+                   np.array([0, a.shape[0]]), np.array([strand]), np.array([int(ragged_left)]),
+                   np.array([int(ragged_right)]), np.array([x_shift]))
+
+
+@dataclass
+class Pairs:
+    """Posterior tuples of a batch: for list k (0 match, 1 gap-x, 2 gap-y), job j owns
+    rows offsets[k][j]:offsets[k][j+1] of weight/x/y."""
+
+    offsets: list
+    weight: list
+    x: list
+    y: list
+    log_likelihood: np.ndarray
+    cells: np.ndarray
+    total_cells: int
+    device_ms: float
+
+    def job(self, j: int, k: int) -> np.ndarray:
+        a, b = self.offsets[k][j], self.offsets[k][j + 1]
+        return np.stack([self.weight[k][a:b], self.x[k][a:b], self.y[k][a:b]], axis=1)
+
+
+def _copy_view(lib, res) -> Pairs:
+    v = _lib.ResultView()
+    _lib.check(lib.mp_result_view_get(res, ctypes.byref(v)))
+    n = v.n_jobs
+    offsets, w, x, y = [], [], [], []
+    for k in range(3):
+        off = np.ctypeslib.as_array(v.offsets[k], shape=(n + 1,)).copy() if n >= 0 else np.zeros(1, np.int64)
+        tot = int(off[-1]) if n > 0 else 0
+        offsets.append(off)
+        for dst, src in ((w, v.weight[k]), (x, v.x[k]), (y, v.y[k])):
+            dst.append(np.ctypeslib.as_array(src, shape=(tot,)).copy() if tot else np.zeros(0, np.int32))
+    ll = np.ctypeslib.as_array(v.log_likelihood, shape=(n,)).copy() if n else np.zeros(0)
+    cells = np.ctypeslib.as_array(v.cells, shape=(n,)).copy() if n else np.zeros(0, np.int64)
+    return Pairs(offsets, w, x, y, ll, cells, int(v.total_cells), float(v.device_ms))
+
+
+def realign_batch(engine: Engine, model: Model, params: AlignmentParams, jobs: Jobs) -> Pairs:
+    """Full posterior pass over a batch held in host memory (H2D, kernels, D2H inside)."""
+    lib = engine._lib
+    ps = params.struct()
+    bs = jobs.struct()
+    res = c_void_p()
+    _lib.check(lib.mp_realign_batch(engine.handle, model.handle, ctypes.byref(ps), ctypes.byref(bs),
+                                    ctypes.byref(res)))
+    try:
+        return _copy_view(lib, res)
+    finally:
+        lib.mp_result_destroy(res)
+
+
+class DeviceBatch:
+    """A batch resident in HBM; ``run`` times only the device work (band + posterior kernels)."""
+
+    def __init__(self, engine: Engine, model: Model, params: AlignmentParams, jobs: Jobs):
+        self.engine, self.model, self.params, self.jobs = engine, model, params, jobs
+        self._ps = params.struct()
+        self._bs = jobs.struct()
+        h = c_void_p()
+        _lib.check(engine._lib.mp_device_batch_create(engine.handle, model.handle, ctypes.byref(self._ps),
+                                                      ctypes.byref(self._bs), ctypes.byref(h)))
+        self.handle = h
+
+    def run(self) -> float:
+        ms = c_float(0.0)
+        _lib.check(self.engine._lib.mp_device_batch_run(self.engine.handle, self.handle, ctypes.byref(ms)))
+        return float(ms.value)
+
+    def fetch(self) -> Pairs:
+        lib = self.engine._lib
+        res = c_void_p()
+        _lib.check(lib.mp_device_batch_fetch(self.engine.handle, self.handle, ctypes.byref(res)))
+        try:
+            return _copy_view(lib, res)
+        finally:
+            lib.mp_result_destroy(res)
+
+    def stats(self):
+        cells, tasks, launches = c_int64(), c_int64(), ctypes.c_int32()
+        _lib.check(self.engine._lib.mp_device_batch_stats(self.handle, cells, tasks, launches))
+        return cells.value, tasks.value, launches.value
+
+    def close(self) -> None:
+        if self.handle:
+            self.engine._lib.mp_device_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def get_aligned_pairs_with_indels_using_anchors(engine: Engine, model: Model, sx, sy, anchors,
+                                                params: AlignmentParams, strand: int = 1,
+                                                ragged_left: bool = False, ragged_right: bool = False):
+    """(matches, gap_x, gap_y) as (n, 3) int arrays of (weight, x, y) for one read."""
+    r = realign_batch(engine, model, params, Jobs.single(sx, sy, anchors, strand, ragged_left, ragged_right))
+    return r.job(0, 0), r.job(0, 1), r.job(0, 2)
+
+
+def get_aligned_pairs_using_anchors(engine: Engine, model: Model, sx, sy, anchors, params: AlignmentParams,
+                                    strand: int = 1, ragged_left: bool = False, ragged_right: bool = False):
+    return get_aligned_pairs_with_indels_using_anchors(engine, model, sx, sy, anchors, params, strand,
+                                                       ragged_left, ragged_right)[0]

@@ -1,0 +1,308 @@
+"""ctypes bindings of the two CPU oracles -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, bench.py's CPU-baseline leg and __graft_entry__.smoke() import
+this module, and only as the checker of the CUDA library.
+
+* ``RefOracle``  (Oracle A): the reference's own impl/pairwiseAligner.c and
+  impl/stateMachine.c compiled unmodified (oracle/_ref/libref_oracle.so).
+* ``ExactOracle`` (Oracle B): the FP64 restatement in oracle/phmm_oracle.c
+  (oracle/libmp_oracle.so); with the reference's logAdd plugged in it must
+  reproduce Oracle A bit for bit.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, Structure, c_double, c_int, c_int64, c_uint8, c_uint16, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "_ref", "libref_oracle.so")
+REF_LIB_CHECKED = os.path.join(HERE, "_ref", "libref_oracle_checked.so")
+EXACT_LIB = os.path.join(HERE, "libmp_oracle.so")
+SHIM_LIB = os.path.join(HERE, "libsonlib_shim.so")
+
+
+def _p(a, t):
+    return a.ctypes.data_as(POINTER(t)) if a is not None else None
+
+
+class OracleParams(Structure):
+    """Layout shared by RefoParams (ref_harness.c) and MpoParams (phmm_oracle.h)."""
+
+    _fields_ = [
+        ("threshold", c_double),
+        ("minDiagsBetweenTraceBack", c_int64),
+        ("traceBackDiagonals", c_int64),
+        ("diagonalExpansion", c_int64),
+        ("constraintDiagonalTrim", c_int64),
+        ("splitMatrixBiggerThanThis", c_int64),
+        ("dynamicAnchorExpansion", c_int64),
+        ("gapGamma", c_double),
+    ]
+
+    @classmethod
+    def from_alignment(cls, ap) -> "OracleParams":
+        return cls(ap.threshold, ap.min_diags_between_traceback, ap.traceback_diagonals, ap.diagonal_expansion,
+                   ap.constraint_diagonal_trim, ap.split_matrix_bigger_than_this,
+                   1 if ap.dynamic_anchor_expansion else 0, ap.gap_gamma)
+
+
+class _Pairs(Structure):
+    _fields_ = [("n", c_int64 * 3), ("t", POINTER(c_int64) * 3)]
+
+
+class _MpoResult(Structure):
+    _fields_ = [("n", c_int64 * 3), ("t", POINTER(c_int64) * 3), ("logLikelihood", c_double), ("cells", c_int64),
+                ("nDense", c_int64), ("dense", POINTER(c_double))]
+
+
+class MpoModel(Structure):
+    _fields_ = [
+        ("trans", c_double * 9), ("start", c_double * 3), ("raggedStart", c_double * 3), ("end", c_double * 3),
+        ("raggedEnd", c_double * 3), ("match", c_double * 25), ("gapX", c_double * 5), ("gapY", c_double * 5),
+        ("runLength", c_int64), ("strand", c_int64), ("maxRepeat", c_int64), ("repeatScale", c_double),
+        ("repeat10", POINTER(c_double)),
+    ]
+
+    @classmethod
+    def from_state_model(cls, sm) -> "MpoModel":
+        m = cls()
+        m.trans[:] = list(map(float, sm.log_transitions))
+        m.start[:] = list(map(float, sm.log_start))
+        m.raggedStart[:] = list(map(float, sm.log_ragged_start))
+        m.end[:] = list(map(float, sm.log_end))
+        m.raggedEnd[:] = list(map(float, sm.log_ragged_end))
+        m.match[:] = list(map(float, sm.log_match))
+        m.gapX[:] = list(map(float, sm.log_gap_x))
+        m.gapY[:] = list(map(float, sm.log_gap_y))
+        m.runLength = 1 if sm.run_length else 0
+        m.strand = int(sm.strand)
+        m.maxRepeat = 51
+        m.repeatScale = float(sm.repeat_scale)
+        if sm.run_length:
+            tab = np.ascontiguousarray(sm.repeat_log10, dtype=np.float64).reshape(-1)
+            m._keep = tab
+            m.repeat10 = _p(tab, c_double)
+        return m
+
+
+def _tuples(ptr, n):
+    if n == 0:
+        return np.zeros((0, 3), dtype=np.int64)
+    return np.ctypeslib.as_array(ptr, shape=(n * 3,)).reshape(n, 3).copy()
+
+
+def available_reference() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+class RefOracle:
+    """Oracle A: the reference's own code."""
+
+    def __init__(self, checked: bool = False):
+        path = REF_LIB_CHECKED if checked else REF_LIB
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: build with `make -C oracle reference`")
+        lib = ctypes.CDLL(path)
+        P = POINTER
+        lib.refo_model_create.restype = c_void_p
+        lib.refo_model_create.argtypes = [c_int, P(c_double), P(c_double), c_int, P(c_double), c_int]
+        lib.refo_model_create_default.restype = c_void_p
+        lib.refo_model_destroy.argtypes = [c_void_p]
+        for f in ("refo_model_match_emission",):
+            getattr(lib, f).restype = c_double
+            getattr(lib, f).argtypes = [c_void_p, c_int, c_int]
+        for f in ("refo_model_gap_x_emission", "refo_model_gap_y_emission"):
+            getattr(lib, f).restype = c_double
+            getattr(lib, f).argtypes = [c_void_p, c_int]
+        lib.refo_model_boundary.restype = c_double
+        lib.refo_model_boundary.argtypes = [c_void_p, c_int, c_int]
+        lib.refo_model_transitions.argtypes = [c_void_p, P(c_double)]
+        job = [c_void_p, P(c_uint16), c_int64, P(c_uint16), c_int64, P(c_int64), c_int64, P(OracleParams), c_int, c_int]
+        for f in ("refo_align_with_indels", "refo_align"):
+            getattr(lib, f).restype = P(_Pairs)
+            getattr(lib, f).argtypes = job
+        lib.refo_pairs_free.argtypes = [P(_Pairs)]
+        lib.refo_align_batch.restype = c_int64
+        lib.refo_align_batch.argtypes = [c_void_p, c_void_p, c_int64, P(c_int64), P(c_uint16), P(c_int64),
+                                         P(c_uint16), P(c_int64), P(c_int64), P(c_uint8), P(OracleParams), c_int,
+                                         P(c_int64), c_void_p]
+        lib.refo_band.argtypes = [P(c_int64), c_int64, c_int64, c_int64, c_int64, c_int, P(c_int64)]
+        lib.refo_split_points.restype = c_int64
+        lib.refo_split_points.argtypes = [P(c_int64), c_int64, c_int64, c_int64, c_int64, c_int, c_int, P(c_int64),
+                                          c_int64]
+        lib.refo_logadd.restype = c_double
+        lib.refo_logadd.argtypes = [c_double, c_double]
+        lib.refo_forward_probability.restype = c_double
+        lib.refo_forward_probability.argtypes = job
+        lib.refo_expectations.argtypes = [c_void_p, c_int, P(c_uint16), c_int64, P(c_uint16), c_int64, P(c_int64),
+                                          c_int64, P(OracleParams), c_int, c_int, P(c_double), P(c_double)]
+        lib.refo_mea.restype = c_int64
+        lib.refo_mea.argtypes = [P(c_int64), c_int64, P(c_int64), c_int64, P(c_int64), c_int64, c_int64, c_int64,
+                                 c_double, P(c_double), P(c_int64), c_int64]
+        self.lib = lib
+
+    # ---- models ----
+    def model(self, hmm_type, transitions, emissions, reverse_complement, repeat_log10=None, strand=1):
+        t = np.ascontiguousarray(transitions, dtype=np.float64)
+        e = np.ascontiguousarray(emissions, dtype=np.float64)
+        r = None if repeat_log10 is None else np.ascontiguousarray(repeat_log10, dtype=np.float64).reshape(-1)
+        h = self.lib.refo_model_create(hmm_type, _p(t, c_double), _p(e, c_double), 1 if reverse_complement else 0,
+                                       _p(r, c_double), 1 if strand else 0)
+        return h
+
+    def default_model(self):
+        return self.lib.refo_model_create_default()
+
+    def free_model(self, h):
+        self.lib.refo_model_destroy(h)
+
+    def transitions(self, h) -> np.ndarray:
+        out = np.zeros(9)
+        self.lib.refo_model_transitions(h, _p(out, c_double))
+        return out
+
+    def match_emission(self, h, cx, cy):
+        return self.lib.refo_model_match_emission(h, cx, cy)
+
+    def gap_emissions(self, h, c):
+        return self.lib.refo_model_gap_x_emission(h, c), self.lib.refo_model_gap_y_emission(h, c)
+
+    def boundary(self, h, which):
+        return np.array([self.lib.refo_model_boundary(h, which, s) for s in range(3)])
+
+    # ---- alignment ----
+    def align_with_indels(self, h, sx, sy, anchors, params, ragged_left=False, ragged_right=False):
+        sx = np.ascontiguousarray(sx, dtype=np.uint16)
+        sy = np.ascontiguousarray(sy, dtype=np.uint16)
+        a = np.ascontiguousarray(np.asarray(anchors, dtype=np.int64).reshape(-1, 3))
+        op = OracleParams.from_alignment(params)
+        r = self.lib.refo_align_with_indels(h, _p(sx, c_uint16), sx.size, _p(sy, c_uint16), sy.size,
+                                            _p(a, c_int64), a.shape[0], ctypes.byref(op), int(ragged_left),
+                                            int(ragged_right))
+        out = tuple(_tuples(r.contents.t[k], r.contents.n[k]) for k in range(3))
+        self.lib.refo_pairs_free(r)
+        return out
+
+    def align_batch(self, hf, hr, jobs, params, n_threads=0):
+        """OpenMP over jobs; returns per-job tuple counts (n, 3)."""
+        n = jobs.n_jobs
+        xoff_b = np.ascontiguousarray(jobs.x_begin, dtype=np.int64)
+        # the harness takes x offsets as (begin, next); build contiguous copies per job
+        xs, xo = _gather_x(jobs)
+        op = OracleParams.from_alignment(params)
+        counts = np.zeros((n, 3), dtype=np.int64)
+        an = np.ascontiguousarray(jobs.anchors, dtype=np.int64)
+        self.lib.refo_align_batch(hf, hr, n, _p(xo, c_int64), _p(xs, c_uint16), _p(jobs.y_offsets, c_int64),
+                                  _p(jobs.y_symbols, c_uint16), _p(jobs.anchor_offsets, c_int64), _p(an, c_int64),
+                                  _p(jobs.strand, c_uint8), ctypes.byref(op), n_threads, _p(counts, c_int64), None)
+        del xoff_b
+        return counts
+
+    def band(self, anchors, lx, ly, expansion, dynamic):
+        a = np.ascontiguousarray(np.asarray(anchors, dtype=np.int64).reshape(-1, 3))
+        out = np.zeros((lx + ly + 1, 3), dtype=np.int64)
+        self.lib.refo_band(_p(a, c_int64), a.shape[0], lx, ly, expansion, int(dynamic), _p(out, c_int64))
+        return out
+
+    def split_points(self, anchors, lx, ly, max_size, ragged_left, ragged_right):
+        a = np.ascontiguousarray(np.asarray(anchors, dtype=np.int64).reshape(-1, 3))
+        n = self.lib.refo_split_points(_p(a, c_int64), a.shape[0], lx, ly, max_size, int(ragged_left),
+                                       int(ragged_right), None, 0)
+        out = np.zeros((max(n, 1), 4), dtype=np.int64)
+        self.lib.refo_split_points(_p(a, c_int64), a.shape[0], lx, ly, max_size, int(ragged_left),
+                                   int(ragged_right), _p(out, c_int64), n)
+        return out[:n]
+
+    def logadd_address(self) -> int:
+        return ctypes.cast(self.lib.refo_logadd, c_void_p).value
+
+
+def _gather_x(jobs):
+    """Per-job contiguous X symbols and monotone offsets (the oracle harness layout)."""
+    parts = [jobs.x_symbols[b:e] for b, e in zip(jobs.x_begin, jobs.x_end)]
+    xo = np.zeros(len(parts) + 1, dtype=np.int64)
+    xo[1:] = np.cumsum([p.size for p in parts])
+    xs = np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros(1, np.uint16), dtype=np.uint16)
+    return xs, xo
+
+
+class ExactOracle:
+    """Oracle B: FP64 restatement (exact log-sum unless a logAdd function pointer is given)."""
+
+    def __init__(self):
+        if not os.path.exists(EXACT_LIB):
+            raise FileNotFoundError(f"{EXACT_LIB} missing: build with `make -C oracle oracle-b`")
+        lib = ctypes.CDLL(EXACT_LIB)
+        P = POINTER
+        lib.mpo_align_with_indels.restype = P(_MpoResult)
+        lib.mpo_align_with_indels.argtypes = [P(MpoModel), P(c_uint16), c_int64, P(c_uint16), c_int64, P(c_int64),
+                                              c_int64, P(OracleParams), c_int, c_int, c_void_p, c_int]
+        lib.mpo_result_free.argtypes = [P(_MpoResult)]
+        lib.mpo_band.restype = c_int
+        lib.mpo_band.argtypes = [P(c_int64), c_int64, c_int64, c_int64, c_int64, c_int, P(c_int64)]
+        lib.mpo_split_points.restype = c_int64
+        lib.mpo_split_points.argtypes = [P(c_int64), c_int64, c_int64, c_int64, c_int64, c_int, c_int, P(c_int64),
+                                         c_int64]
+        lib.mpo_match_emission.restype = c_double
+        lib.mpo_match_emission.argtypes = [P(MpoModel), c_uint16, c_uint16]
+        lib.mpo_gap_x_emission.restype = c_double
+        lib.mpo_gap_x_emission.argtypes = [P(MpoModel), c_uint16]
+        lib.mpo_gap_y_emission.restype = c_double
+        lib.mpo_gap_y_emission.argtypes = [P(MpoModel), c_uint16]
+        lib.mpo_align_batch.restype = c_int64
+        lib.mpo_align_batch.argtypes = [P(MpoModel), P(MpoModel), c_int64, P(c_int64), P(c_uint16), P(c_int64),
+                                        P(c_uint16), P(c_int64), P(c_int64), P(c_uint8), P(OracleParams), c_int,
+                                        P(c_int64), P(c_double)]
+        self.lib = lib
+
+    def align_with_indels(self, model: MpoModel, sx, sy, anchors, params, ragged_left=False, ragged_right=False,
+                          logadd=None, dense=False):
+        sx = np.ascontiguousarray(sx, dtype=np.uint16)
+        sy = np.ascontiguousarray(sy, dtype=np.uint16)
+        a = np.ascontiguousarray(np.asarray(anchors, dtype=np.int64).reshape(-1, 3))
+        op = OracleParams.from_alignment(params)
+        r = self.lib.mpo_align_with_indels(ctypes.byref(model), _p(sx, c_uint16), sx.size, _p(sy, c_uint16), sy.size,
+                                           _p(a, c_int64), a.shape[0], ctypes.byref(op), int(ragged_left),
+                                           int(ragged_right), logadd, 1 if dense else 0)
+        rc = r.contents
+        out = {
+            "pairs": tuple(_tuples(rc.t[k], rc.n[k]) for k in range(3)),
+            "log_likelihood": rc.logLikelihood,
+            "cells": rc.cells,
+        }
+        if dense:
+            out["dense"] = (np.ctypeslib.as_array(rc.dense, shape=(rc.nDense * 5,)).reshape(-1, 5).copy()
+                            if rc.nDense else np.zeros((0, 5)))
+        self.lib.mpo_result_free(r)
+        return out
+
+    def align_batch(self, mf: MpoModel, mr: MpoModel, jobs, params, n_threads=0):
+        n = jobs.n_jobs
+        xs, xo = _gather_x(jobs)
+        op = OracleParams.from_alignment(params)
+        counts = np.zeros((n, 3), dtype=np.int64)
+        ll = np.zeros(n)
+        an = np.ascontiguousarray(jobs.anchors, dtype=np.int64)
+        self.lib.mpo_align_batch(ctypes.byref(mf), ctypes.byref(mr), n, _p(xo, c_int64), _p(xs, c_uint16),
+                                 _p(jobs.y_offsets, c_int64), _p(jobs.y_symbols, c_uint16),
+                                 _p(jobs.anchor_offsets, c_int64), _p(an, c_int64), _p(jobs.strand, c_uint8),
+                                 ctypes.byref(op), n_threads, _p(counts, c_int64), _p(ll, c_double))
+        return counts, ll
+
+    def band(self, anchors, lx, ly, expansion, dynamic):
+        a = np.ascontiguousarray(np.asarray(anchors, dtype=np.int64).reshape(-1, 3))
+        out = np.zeros((lx + ly + 1, 3), dtype=np.int64)
+        rc = self.lib.mpo_band(_p(a, c_int64), a.shape[0], lx, ly, expansion, int(dynamic), _p(out, c_int64))
+        return out if rc == 0 else None
+
+    def split_points(self, anchors, lx, ly, max_size, ragged_left, ragged_right):
+        a = np.ascontiguousarray(np.asarray(anchors, dtype=np.int64).reshape(-1, 3))
+        n = self.lib.mpo_split_points(_p(a, c_int64), a.shape[0], lx, ly, max_size, int(ragged_left),
+                                      int(ragged_right), None, 0)
+        out = np.zeros((max(n, 1), 4), dtype=np.int64)
+        self.lib.mpo_split_points(_p(a, c_int64), a.shape[0], lx, ly, max_size, int(ragged_left),
+                                  int(ragged_right), _p(out, c_int64), n)
+        return out[:n]

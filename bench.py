@@ -1,0 +1,377 @@
+#!/usr/bin/env python3
+"""Throughput of the banded pair-HMM forward/backward/posterior pass (GCUPS) on B200.
+
+Workload (default): the batched uneven-reads configuration -- 256 chunks of a
+10 kb homopolymer-enriched synthetic template (GC 0.41, run lengths geometric
+p=0.55 capped at 20), 30x coverage, log-normal read lengths (median 6 kb,
+sigma 0.6) truncated to the chunk, nanopore-like errors, band half-width 25,
+the shipped run-length model; all reads of all chunks in one persistent launch.
+A step is one full posterior pass over the batch. Cells = sum of anti-diagonal
+band widths (the reference's band). Inputs are larger than L2 (126 MB).
+
+value: cells / device time (band + posterior kernels, CUDA events) with inputs
+resident in HBM. e2e: the same pass through mp_realign_batch with host
+buffers in pinned memory (host->device copies, planning, kernels, compaction
+and device->host copies of every tuple inside the timed region).
+
+--impl reference: the reference's own C implementation (pairwiseAligner.c /
+stateMachine.c compiled unmodified, OpenMP over reads on all host cores) on a
+bounded sample of the same workload.
+
+Multi-GPU: one process per GPU (torchrun); reads are independent, so every rank
+runs its own full workload (weak scaling, no data-path collective); value is
+the sum of cells over ranks divided by the max device time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FLOP_PER_CELL = 48  # 30 FP32 FMA-pipe instructions per cell (forward 12, backward 12, posterior 6)
+METRIC = "GCUPS fwd+bwd+posterior (batched FP32 vs plain GPU, ≤1e-4 vs FP64); CPU ref"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=["batched", "small"], default="batched")
+    ap.add_argument("--chunks", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work per baseline sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([s.strip() for s in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(s[1]) for s in self.samples if len(s) >= 9 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) >= 9 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            if len(s) < 9:
+                continue
+            for i, n in enumerate(names):
+                if s[5 + i].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def load_model():
+    from marginpolish_b200 import params
+    return params.polish_model_from_npz(os.path.join(ROOT, "tests", "golden", "model_np.npz"))
+
+
+def make_workload(args, rank):
+    from marginpolish_b200 import synth
+    if args.config == "small":
+        return synth.config_small(seed=args.seed + rank)
+    return synth.config_batched(seed=args.seed + rank, n_chunks=args.chunks)
+
+
+def cpu_sample(jobs, cells, target_cells):
+    """First jobs whose cells add up to about target_cells (a bounded sample of the workload)."""
+    import numpy as np
+    from marginpolish_b200 import Jobs
+    c = np.cumsum(cells)
+    n = int(np.searchsorted(c, target_cells)) + 1
+    n = max(1, min(n, jobs.n_jobs))
+    a0, a1 = int(jobs.anchor_offsets[0]), int(jobs.anchor_offsets[n])
+    sub = Jobs(jobs.x_symbols, jobs.x_begin[:n], jobs.x_end[:n], jobs.y_symbols[:int(jobs.y_offsets[n])],
+               jobs.y_offsets[:n + 1], jobs.anchors[a0:a1], jobs.anchor_offsets[:n + 1], jobs.strand[:n])
+    return sub, int(c[n - 1])
+
+
+def reference_models(ref, pm):
+    import numpy as np
+    z = np.load(os.path.join(ROOT, "tests", "golden", "model_np.npz"))
+    hf = ref.model(int(z["hmm_type"]), z["transitions"], z["emissions"], False, z["repeat_log10"], 1)
+    hr = ref.model(int(z["hmm_type"]), z["transitions"], z["emissions"], True, z["repeat_log10"], 0)
+    return hf, hr
+
+
+def time_reference(jobs, cells, pm, seconds, steps=1, warmup=0):
+    """Oracle A (the reference's own code) with OpenMP over reads on all host cores."""
+    from oracle.bindings import RefOracle
+    ref = RefOracle()
+    hf, hr = reference_models(ref, pm)
+    cores = os.cpu_count() or 1
+    # calibrate the sample size on a short run
+    probe, probe_cells = cpu_sample(jobs, cells, 4e6 * cores * 0.25)
+    t = time.perf_counter()
+    ref.align_batch(hf, hr, probe, pm.alignment, cores)
+    rate = probe_cells / max(time.perf_counter() - t, 1e-3)
+    sample, sample_cells = cpu_sample(jobs, cells, rate * seconds)
+    for _ in range(warmup):
+        ref.align_batch(hf, hr, sample, pm.alignment, cores)
+    times = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        ref.align_batch(hf, hr, sample, pm.alignment, cores)
+        times.append(time.perf_counter() - t)
+    ref.free_model(hf)
+    ref.free_model(hr)
+    return {"gcups": sample_cells / statistics.median(times) / 1e9, "cores": cores, "reads": sample.n_jobs,
+            "cells": sample_cells, "seconds": statistics.median(times)}
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    from oracle.bindings import available_reference
+    if not available_reference():
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libref_oracle.so missing"}))
+        return
+    import numpy as np
+    from marginpolish_b200 import Engine, Model, realign_batch  # noqa: F401
+    pm = load_model()
+    wl = make_workload(args, 0)
+    jobs = wl.jobs()
+    # cells per job from the band (the oracle counts them identically)
+    from oracle.bindings import ExactOracle
+    cells = band_cells(jobs, pm)
+    r = time_reference(jobs, cells, pm, args.cpu_seconds, steps=args.steps, warmup=args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["gcups"], "unit": "GCUPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["seconds"] * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"{args.config}: {wl.meta}", "reads_in_sample": r["reads"],
+                   "cells_per_step": r["cells"]},
+        "cpu_baseline": {"value": r["gcups"], "unit": "GCUPS", "cores": r["cores"], "kind": "reference",
+                         "sample": f"first {r['reads']} reads of the workload ({r['cells']} cells) per step"},
+        "e2e": {"value": r["gcups"], "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    del np, ExactOracle
+    print(json.dumps(line), flush=True)
+
+
+def band_cells(jobs, pm):
+    """Cells per job from the library's host band restatement (integer-exact)."""
+    import ctypes
+
+    import numpy as np
+    from marginpolish_b200 import _lib
+    lib = _lib.load()
+    out = np.zeros(jobs.n_jobs, dtype=np.int64)
+    ap = pm.alignment
+    for j in range(jobs.n_jobs):
+        lx = int(jobs.x_end[j] - jobs.x_begin[j])
+        ly = int(jobs.y_offsets[j + 1] - jobs.y_offsets[j])
+        a = np.ascontiguousarray(jobs.anchors[jobs.anchor_offsets[j]:jobs.anchor_offsets[j + 1]])
+        b = np.zeros((lx + ly + 1, 3), dtype=np.int64)
+        _lib.check(lib.mp_band(_lib.ptr(a, ctypes.c_int32) if a.size else None, a.shape[0], lx, ly,
+                               ap.diagonal_expansion, 1 if ap.dynamic_anchor_expansion else 0,
+                               _lib.ptr(b, ctypes.c_int64)))
+        out[j] = int(((b[:, 2] - b[:, 1]) // 2 + 1).sum()) if lx + ly > 0 else 0
+    return out
+
+
+def pinned_jobs(jobs):
+    """Copy of a batch whose arrays live in page-locked host memory."""
+    import torch
+    from marginpolish_b200 import Jobs
+
+    def pin(a):
+        t = torch.from_numpy(a.copy()).pin_memory()
+        return t.numpy(), t
+
+    keep = []
+    arrs = {}
+    for name in ("x_symbols", "x_begin", "x_end", "y_symbols", "y_offsets", "anchors", "anchor_offsets", "strand",
+                 "x_shift"):
+        v = getattr(jobs, name)
+        if v is None:
+            arrs[name] = None
+            continue
+        arr, t = pin(v)
+        keep.append(t)
+        arrs[name] = arr
+    pj = Jobs(arrs["x_symbols"], arrs["x_begin"], arrs["x_end"], arrs["y_symbols"], arrs["y_offsets"],
+              arrs["anchors"], arrs["anchor_offsets"], arrs["strand"], None, None, arrs["x_shift"])
+    pj._pinned = keep
+    return pj
+
+
+def run_ours(args, rank, world, local):
+    import numpy as np
+    import torch
+
+    from marginpolish_b200 import DeviceBatch, Engine, Model, realign_batch
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    pm = load_model()
+    t0 = time.perf_counter()
+    wl = make_workload(args, rank)
+    jobs = wl.jobs()
+    gen_s = time.perf_counter() - t0
+    engine = Engine(local)
+    model = Model.from_polish(engine, pm)
+    db = DeviceBatch(engine, model, pm.alignment, jobs)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+
+    for _ in range(args.warmup):
+        db.run()
+    cells, n_tasks, launches = db.stats()
+    sampler = ClockSampler(local) if rank == 0 else None
+    barrier()
+    if sampler:
+        sampler.start()
+        time.sleep(0.4)
+    dev_ms, post_ms, band_ms = [], [], []
+    wall0 = time.perf_counter()
+    for _ in range(args.steps):
+        ms = db.run()
+        b, p = db.timing()
+        dev_ms.append(ms)
+        post_ms.append(p)
+        band_ms.append(b)
+    barrier()
+    wall = time.perf_counter() - wall0
+    clocks = sampler.stop() if sampler else None
+    total_ms = float(sum(dev_ms))
+    if dist is not None:
+        t = torch.tensor([total_ms, float(cells)], dtype=torch.float64, device=f"cuda:{local}")
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = t.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        max_ms, all_cells = float(mx[0]), float(sm[1])
+    else:
+        max_ms, all_cells = total_ms, float(cells)
+    value = all_cells * args.steps / (max_ms * 1e-3) / 1e9
+
+    # end-to-end through the public API with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        pj = pinned_jobs(jobs)
+        realign_batch(engine, model, pm.alignment, pj)  # warm
+        e2e_times = []
+        h2d = int(pj.x_symbols.nbytes + pj.y_symbols.nbytes + pj.anchors.nbytes + pj.x_begin.nbytes * 2 +
+                  pj.y_offsets.nbytes + pj.anchor_offsets.nbytes + pj.strand.nbytes + pj.x_shift.nbytes)
+        d2h = 0
+        steps_e2e = max(1, min(args.steps, 3))
+        for _ in range(steps_e2e):
+            barrier()
+            t = time.perf_counter()
+            r = realign_batch(engine, model, pm.alignment, pj)
+            torch.cuda.synchronize(local)
+            e2e_times.append(time.perf_counter() - t)
+            d2h = int(sum(r.offsets[k][-1] for k in range(3)) * 12 + n_tasks * 32)
+        e2e_t = max(e2e_times) if dist is None else e2e_times
+        tt = float(np.median(e2e_times))
+        if dist is not None:
+            t = torch.tensor([tt], dtype=torch.float64, device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            tt = float(t[0])
+        e2e = {"value": all_cells / tt / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": tt * 1e3}
+        del e2e_t
+
+    peak = engine.fp32_peak_tflops()
+    post = float(np.median(post_ms))
+    achieved = cells * FLOP_PER_CELL / (post * 1e-3) / 1e12
+    line = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu and world == 1:
+            from oracle.bindings import available_reference
+            if available_reference():
+                cpc = band_cells(jobs, pm)
+                r = time_reference(jobs, cpc, pm, args.cpu_seconds)
+                cpu = {"value": r["gcups"], "unit": "GCUPS", "cores": r["cores"], "kind": "reference",
+                       "sample": f"first {r['reads']} reads of the workload ({r['cells']} cells), "
+                                 f"OpenMP over reads on {r['cores']} threads"}
+        line = {
+            "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, shipped run-length model)",
+            "config": {"workload": f"{args.config}: {wl.meta}", "reads": jobs.n_jobs, "cells_per_gpu_step": cells,
+                       "tasks": n_tasks, "l2": "inputs and band/scratch/output buffers exceed the 126 MB L2",
+                       "generation_s": round(gen_s, 1), "band_ms": float(np.median(band_ms)),
+                       "posterior_ms": post, "wall_s_timed": wall},
+            "e2e": e2e,
+            "gpu_launches": launches * args.steps,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "note": f"{FLOP_PER_CELL} flop per cell x cells / posterior-kernel event time; "
+                                 "peak = FP32 FMA throughput measured live on this GPU (mp_measure_fp32_peak)"},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    db.close()
+    model.close()
+    engine.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+    else:
+        run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

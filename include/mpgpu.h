@@ -165,6 +165,14 @@ mp_status mp_device_batch_fetch(mp_engine *e, mp_device_batch *db, mp_result **o
 mp_status mp_device_batch_stats(const mp_device_batch *db, int64_t *total_cells, int64_t *n_tasks,
                                 int32_t *kernel_launches_per_run);
 void mp_device_batch_destroy(mp_device_batch *db);
+/* CUDA-event times of the last run: band kernels and posterior kernels (ms). */
+mp_status mp_device_batch_timing(const mp_device_batch *db, float *band_ms, float *posterior_ms);
+
+/* ---- measurement ---- */
+/* FP32 FMA throughput of the device measured with a dependent-chain-free FMA loop
+ * (TFLOP/s, FMA = 2 flops), timed with CUDA events; the roofline denominator of the
+ * posterior kernel, whose bound is the FP32 pipe. */
+mp_status mp_measure_fp32_peak(mp_engine *e, double *tflops);
 
 /* ---- geometry helpers (host, integer-exact restatements used by the planner) ---- */
 /* Band of one sub-problem: (xay, xmyL, xmyR) for d = 0..lX+lY into out[3*(lX+lY+1)]. */

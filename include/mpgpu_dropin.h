@@ -1,0 +1,126 @@
+/*
+ * mpgpu_dropin.h -- drop-in replacements for MarginPolish's pair-HMM entry points.
+ *
+ * libmpgpu_dropin.so exports the reference's own signatures so that a MarginPolish
+ * build can link it in place of impl/pairwiseAligner.c's posterior functions:
+ *
+ *   getAlignedPairsWithIndelsUsingAnchors   inc/pairwiseAligner.h:75-77 (impl/pairwiseAligner.c:1105-1130)
+ *   getAlignedPairsUsingAnchors             inc/pairwiseAligner.h:73    (impl/pairwiseAligner.c:1088-1103)
+ *   getAlignedPairsWithIndels               inc/pairwiseAligner.h:67-69 (impl/pairwiseAligner.c:1141-1149)
+ *   getAlignedPairs                         inc/pairwiseAligner.h:60-61 (impl/pairwiseAligner.c:1132-1139)
+ *
+ * The type declarations below restate the reference's public layouts
+ * (inc/stateMachine.h:13-22, :40-48, :65-75, :101-124; inc/pairwiseAligner.h:28-39)
+ * so that objects built by the caller are read correctly. stList / stIntTuple
+ * are the caller's sonLib; the library resolves stList_* / stIntTuple_* from the
+ * host application at load time. The StateMachine is lowered to flat tables
+ * through its public function pointers (cellCalculate, emission, boundary
+ * probabilities), once per machine, and cached.
+ *
+ * Semantics: identical argument meaning and output order as the reference;
+ * returned lists are newly allocated, own their stIntTuple elements and are
+ * destroyed by the caller. Failures (no sm_100 device, malformed anchors,
+ * unsupported machines) print the library's message and call exit(1), which
+ * matches the reference's st_errAbort behaviour. Calls are serialised by an
+ * internal mutex (the reference calls them from OpenMP threads).
+ */
+#ifndef MPGPU_DROPIN_H_
+#define MPGPU_DROPIN_H_
+
+#include <stdbool.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "mpgpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct _stList stList;
+typedef int64_t stIntTuple;
+
+typedef struct _alphabet Alphabet;
+typedef struct _emissions Emissions;
+typedef uint16_t Symbol;
+
+typedef struct _symbolString {
+    Alphabet *alphabet;
+    Symbol *sequence;
+    int64_t length;
+} SymbolString;
+
+struct _alphabet {
+    uint64_t alphabetSize;
+    Symbol (*convertCharToSymbol)(char i);
+    char (*convertSymbolToChar)(Symbol i);
+    bool (*symbolsEqual)(Symbol, Symbol);
+};
+
+struct _emissions {
+    Alphabet *alphabet;
+    double (*emission)(Emissions *e, Symbol cX, Symbol cY);
+    double (*gapEmissionX)(Emissions *e, Symbol cX);
+    double (*gapEmissionY)(Emissions *e, Symbol cY);
+    void (*printFn)(Emissions *e, FILE *f);
+};
+
+typedef enum { threeState = 2, threeStateAsymmetric = 3 } StateMachineType;
+
+typedef struct _stateMachine StateMachine;
+
+struct _stateMachine {
+    StateMachineType type;
+    int64_t stateNumber;
+    int64_t matchState;
+    int64_t gapXState;
+    int64_t gapYState;
+    Emissions *emissions;
+    double (*startStateProb)(StateMachine *sM, int64_t state);
+    double (*endStateProb)(StateMachine *sM, int64_t state);
+    double (*raggedEndStateProb)(StateMachine *sM, int64_t state);
+    double (*raggedStartStateProb)(StateMachine *sM, int64_t state);
+    void (*cellCalculate)(StateMachine *sM, double *current, double *lower, double *middle, double *upper,
+                          Symbol cX, Symbol cY, void (*doTransition)(double *, double *, int64_t, int64_t, double,
+                                                                     double, void *),
+                          void *extraArgs);
+    void (*printFn)(StateMachine *e, FILE *f);
+};
+
+typedef struct _pairwiseAlignmentBandingParameters {
+    double threshold;
+    int64_t minDiagsBetweenTraceBack;
+    int64_t traceBackDiagonals;
+    int64_t diagonalExpansion;
+    int64_t constraintDiagonalTrim;
+    int64_t splitMatrixBiggerThanThis;
+    bool alignAmbiguityCharacters;
+    float gapGamma;
+    bool dynamicAnchorExpansion;
+} PairwiseAlignmentParameters;
+
+/* Reference signatures (see the file comment for the lines they replace). */
+void getAlignedPairsWithIndelsUsingAnchors(StateMachine *sM, SymbolString sX, SymbolString sY, stList *anchorPairs,
+                                           PairwiseAlignmentParameters *p, stList **alignedPairs, stList **gapXPairs,
+                                           stList **gapYPairs, bool alignmentHasRaggedLeftEnd,
+                                           bool alignmentHasRaggedRightEnd);
+stList *getAlignedPairsUsingAnchors(StateMachine *sM, SymbolString sX, SymbolString sY, stList *anchorPairs,
+                                    PairwiseAlignmentParameters *p, bool alignmentHasRaggedLeftEnd,
+                                    bool alignmentHasRaggedRightEnd);
+void getAlignedPairsWithIndels(StateMachine *sM, SymbolString sX, SymbolString sY, PairwiseAlignmentParameters *p,
+                               stList **alignedPairs, stList **gapXPairs, stList **gapYPairs,
+                               bool alignmentHasRaggedLeftEnd, bool alignmentHasRaggedRightEnd);
+stList *getAlignedPairs(StateMachine *sM, SymbolString sX, SymbolString sY, PairwiseAlignmentParameters *p,
+                        bool alignmentHasRaggedLeftEnd, bool alignmentHasRaggedRightEnd);
+
+/* Lowering of a caller's StateMachine to the flat description mp_model_create takes
+ * (no device needed). repeat_out must hold 4*51*51 doubles; desc->repeat_log10 is set
+ * to point at it when the machine carries run-length emissions. Returns MP_OK or
+ * MP_ERR_ARGUMENT when the machine's emissions are not of the reference's form. */
+mp_status mpd_lower_state_machine(StateMachine *sM, mp_model_desc *desc, double *repeat_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -115,7 +115,7 @@ EXPORTED = [
     "mp_model_create", "mp_model_destroy", "mp_engine_set_tuning", "mp_realign_batch", "mp_result_view_get",
     "mp_result_destroy", "mp_device_batch_create", "mp_device_batch_run", "mp_device_batch_fetch",
     "mp_device_batch_stats", "mp_device_batch_destroy", "mp_band", "mp_split_points", "mp_crop_range",
-    "mp_rle_encode", "mp_rle_symbols", "mp_rle_anchors",
+    "mp_rle_encode", "mp_rle_symbols", "mp_rle_anchors", "mp_device_batch_timing", "mp_measure_fp32_peak",
 ]
 
 _lib = None
@@ -148,6 +148,8 @@ def load() -> ctypes.CDLL:
         "mp_device_batch_fetch": (c_int, [c_void_p, c_void_p, P(c_void_p)]),
         "mp_device_batch_stats": (c_int, [c_void_p, P(c_int64), P(c_int64), P(c_int32)]),
         "mp_device_batch_destroy": (None, [c_void_p]),
+        "mp_device_batch_timing": (c_int, [c_void_p, P(c_float), P(c_float)]),
+        "mp_measure_fp32_peak": (c_int, [c_void_p, P(c_double)]),
         "mp_band": (c_int, [P(c_int32), c_int64, c_int64, c_int64, c_int64, c_int, P(c_int64)]),
         "mp_split_points": (c_int, [P(c_int32), c_int64, c_int64, c_int64, c_int64, c_int, c_int, P(c_int64),
                                     c_int64, P(c_int64)]),

@@ -447,6 +447,11 @@ struct mp_device_batch {
     std::vector<TaskOut> hostOut;
     int launchesPerRun = 0;
     bool ran = false;
+    float bandMs = 0.0f, posteriorMs = 0.0f;
+    cudaEvent_t evBand = nullptr;
+    ~mp_device_batch() {
+        if (evBand) cudaEventDestroy(evBand);
+    }
 };
 
 static mp_status validateJob(const mp_batch *b, int64_t j, const mp_params *p) {
@@ -681,39 +686,49 @@ extern "C" mp_status mp_device_batch_create(mp_engine *e, const mp_model *m, con
     return MP_OK;
 }
 
-static mp_status ensureScratch(mp_device_batch *db, int C, int64_t maxN, int warpsTotal, int &scratchBlocks) {
-    int K = classStride(C);
-    scratchBlocks = (int) (maxN / K + 2);
-    size_t perWarp = (size_t) scratchBlocks * C * 32 * sizeof(float4);
-    MP_TRY(db->scratch.reserve(perWarp * warpsTotal));
-    MP_TRY(db->scratchScal.reserve(sizeof(int2) * (size_t) scratchBlocks * warpsTotal));
-    MP_TRY(db->resume.reserve(sizeof(float4) * C * 32 * (size_t) warpsTotal));
-    return MP_OK;
-}
-
-// Launches the posterior kernels for the current queues.
+// Launches the posterior kernels for the current queues (one persistent launch per
+// slot class with tasks). Scratch for all classes is reserved before the first launch.
 static mp_status launchQueues(mp_device_batch *db) {
     mp_engine *e = db->e;
     cudaStream_t st = e->stream;
-    CUDA_TRY(cudaMemsetAsync(db->queue.p, 0, sizeof(int32_t) * kNumClasses, st));
+    int blocksOf[kNumClasses], warpsOf[kNumClasses], scratchBlocksOf[kNumClasses];
+    size_t needScratch = 0, needScal = 0, needResume = 0;
     for (int ci = 0; ci < kNumClasses; ci++) {
+        blocksOf[ci] = warpsOf[ci] = scratchBlocksOf[ci] = 0;
         if (db->classCount[ci] == 0) continue;
         int C = kClasses[ci];
         int warps = e->tuning.warps_per_block > 0 ? e->tuning.warps_per_block : classMaxWarps(C);
         warps = std::min(warps, classMaxWarps(C));
         int blocksPerSm = e->tuning.blocks_per_sm > 0 ? e->tuning.blocks_per_sm : 1;
         int blocks = e->smCount * blocksPerSm;
-        // do not launch more warps than tasks
-        int maxBlocks = (db->classCount[ci] + warps - 1) / warps;
+        int maxBlocks = (db->classCount[ci] + warps - 1) / warps;  // no more warps than tasks
         blocks = std::max(1, std::min(blocks, maxBlocks));
-        int scratchBlocks = 0;
-        MP_TRY(ensureScratch(db, C, db->classMaxN[ci], blocks * warps, scratchBlocks));
+        int K = classStride(C);
+        int scratchBlocks = (int) (db->classMaxN[ci] / K + 2);
+        size_t wt = (size_t) blocks * warps;
+        needScratch = std::max(needScratch, (size_t) scratchBlocks * C * 32 * sizeof(float4) * wt);
+        needScal = std::max(needScal, sizeof(int2) * (size_t) scratchBlocks * wt);
+        needResume = std::max(needResume, sizeof(float4) * C * 32 * wt);
+        blocksOf[ci] = blocks;
+        warpsOf[ci] = warps;
+        scratchBlocksOf[ci] = scratchBlocks;
+    }
+    if (needScratch > db->scratch.bytes || needScal > db->scratchScal.bytes || needResume > db->resume.bytes) {
+        CUDA_TRY(cudaStreamSynchronize(st));
+        MP_TRY(db->scratch.reserve(needScratch));
+        MP_TRY(db->scratchScal.reserve(needScal));
+        MP_TRY(db->resume.reserve(needResume));
+    }
+    CUDA_TRY(cudaMemsetAsync(db->queue.p, 0, sizeof(int32_t) * kNumClasses, st));
+    for (int ci = 0; ci < kNumClasses; ci++) {
+        if (db->classCount[ci] == 0) continue;
+        int C = kClasses[ci];
         DpArgs a;
         memset(&a, 0, sizeof(a));
         a.tasks = db->dTasks.as<Task>();
         a.order = db->orders.as<int32_t>() + db->classOrderOff[ci];
         a.nTasks = db->classCount[ci];
-        a.scratchBlocks = scratchBlocks;
+        a.scratchBlocks = scratchBlocksOf[ci];
         a.queue = db->queue.as<int32_t>() + ci;
         a.xs = db->xs.as<uint16_t>();
         a.ys = db->ys.as<uint16_t>();
@@ -733,7 +748,7 @@ static mp_status launchQueues(mp_device_batch *db) {
         a.minDiagsBetweenTraceBack = (int32_t) std::min<int64_t>(db->p.min_diags_between_traceback, 1 << 30);
         a.traceBackDiagonals = (int32_t) db->p.traceback_diagonals;
         a.diagonalExpansion = (int32_t) std::min<int64_t>(db->p.diagonal_expansion, 1 << 29);
-        CUDA_TRY(launchPosterior(C, a, blocks, warps, st));
+        CUDA_TRY(launchPosterior(C, a, blocksOf[ci], warpsOf[ci], st));
         db->launchesPerRun++;
     }
     return MP_OK;
@@ -749,6 +764,7 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
     for (int i = 0; i < nTasks; i++) all[i] = i;
     buildQueues(db, all, orderHost);
     MP_TRY(upload(db->orders, orderHost.data(), sizeof(int32_t) * std::max<size_t>(orderHost.size(), 1), st));
+    if (!db->evBand) CUDA_TRY(cudaEventCreate(&db->evBand));
     CUDA_TRY(cudaEventRecord(e->ev0, st));
     BandArgs ba;
     ba.tasks = db->dTasks.as<Task>();
@@ -758,6 +774,7 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
     ba.out = db->dOut.as<TaskOut>();
     CUDA_TRY(launchBand(ba, st));
     db->launchesPerRun += nTasks > 0 ? 2 : 0;
+    CUDA_TRY(cudaEventRecord(db->evBand, st));
     MP_TRY(launchQueues(db));
     CUDA_TRY(cudaEventRecord(e->ev1, st));
     // statuses
@@ -766,6 +783,8 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
     CUDA_TRY(cudaStreamSynchronize(st));
     float ms = 0.0f;
     CUDA_TRY(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+    CUDA_TRY(cudaEventElapsedTime(&db->bandMs, e->ev0, db->evBand));
+    CUDA_TRY(cudaEventElapsedTime(&db->posteriorMs, db->evBand, e->ev1));
     // retries: capacity overflows (exact counts known), window overflows (next class), scratch
     for (int round = 0; round < 4; round++) {
         std::vector<int32_t> retry;
@@ -775,6 +794,10 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
             if (o.status & kTaskBand) {
                 return failf(MP_ERR_ARGUMENT, "job %d: invalid band diagonal (anchors inconsistent with lengths)",
                              db->tasks[t].job);
+            }
+            if (o.status & kTaskSymbol) {
+                return failf(MP_ERR_ARGUMENT, "job %d: a symbol's repeat count is >= %d", db->tasks[t].job,
+                             kMaxRepeat);
             }
             if (o.status & (kTaskCapacity | kTaskWindow | kTaskScratch)) {
                 if (o.status & kTaskWindow) {
@@ -829,6 +852,7 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
         float ms2 = 0.0f;
         CUDA_TRY(cudaEventElapsedTime(&ms2, e->ev0, e->ev1));
         ms += ms2;
+        db->posteriorMs += ms2;
     }
     for (int t = 0; t < nTasks; t++) {
         if (db->hostOut[t].status != 0)
@@ -836,6 +860,42 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
     }
     if (kernelMs) *kernelMs = ms;
     db->ran = true;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_device_batch_timing(const mp_device_batch *db, float *bandMs, float *posteriorMs) {
+    if (!db) return failf(MP_ERR_ARGUMENT, "batch is NULL");
+    if (bandMs) *bandMs = db->bandMs;
+    if (posteriorMs) *posteriorMs = db->posteriorMs;
+    return MP_OK;
+}
+
+namespace mp {
+cudaError_t launchFmaProbe(float *out, int blocks, int threads, int iters, cudaStream_t s);
+}
+
+extern "C" mp_status mp_measure_fp32_peak(mp_engine *e, double *tflops) {
+    if (!e || !tflops) return failf(MP_ERR_ARGUMENT, "mp_measure_fp32_peak: NULL argument");
+    CUDA_TRY(cudaSetDevice(e->device));
+    DevBuf out;
+    const int threads = 512, blocksPerSm = 4, iters = 4096;
+    const int blocks = e->smCount * blocksPerSm;
+    MP_TRY(out.reserve(sizeof(float) * blocks * threads));
+    cudaStream_t st = e->stream;
+    for (int w = 0; w < 3; w++) CUDA_TRY(launchFmaProbe(out.as<float>(), blocks, threads, iters, st));
+    float best = 1e30f;
+    for (int r = 0; r < 5; r++) {
+        CUDA_TRY(cudaEventRecord(e->ev0, st));
+        CUDA_TRY(launchFmaProbe(out.as<float>(), blocks, threads, iters, st));
+        CUDA_TRY(cudaEventRecord(e->ev1, st));
+        CUDA_TRY(cudaEventSynchronize(e->ev1));
+        float ms = 0.0f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+        best = std::min(best, ms);
+    }
+    // 16 independent FMA chains per thread, `iters` rounds each
+    double flops = 2.0 * 16.0 * iters * (double) blocks * threads;
+    *tflops = flops / (best * 1e-3) / 1e12;
     return MP_OK;
 }
 

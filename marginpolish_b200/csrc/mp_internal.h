@@ -49,7 +49,8 @@ enum TaskStatus : int32_t {
     kTaskCapacity = 1,     // an output list needed more than its capacity (counts are exact)
     kTaskWindow = 2,       // band hull wider than the slot window of the class
     kTaskBand = 4,         // invalid diagonal (reference: exception)
-    kTaskScratch = 8       // checkpoint scratch too small
+    kTaskScratch = 8,      // checkpoint scratch too small
+    kTaskSymbol = 16       // a symbol's repeat count is >= kMaxRepeat
 };
 
 struct TaskOut {

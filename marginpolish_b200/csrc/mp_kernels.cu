@@ -84,7 +84,7 @@ struct TaskCtx {
 };
 
 // Decoded X symbol: packed (repeat-table byte offset | match-row byte offset << 17), gap-x emission.
-__device__ __forceinline__ uint2 decodeX(const TaskCtx &c, int pos) {
+__device__ __forceinline__ uint2 decodeX(const TaskCtx &c, int pos, int &bad) {
     int b = 4, rc = 0;
     if (pos >= 0 && pos < c.lx) {
         uint32_t s = c.xs[pos];
@@ -95,6 +95,10 @@ __device__ __forceinline__ uint2 decodeX(const TaskCtx &c, int pos) {
             b = (int) s;
         }
         b = b > 4 ? 4 : b;
+        if (rc >= kMaxRepeat) {  // keeps the table lookup in bounds; reported as an argument error
+            rc = kMaxRepeat - 1;
+            bad = 1;
+        }
     }
     int bb = b == 4 ? 0 : b;  // 'N' reads the A row of the repeat table
     int row = c.strandFwd ? bb : 3 - bb;
@@ -104,7 +108,7 @@ __device__ __forceinline__ uint2 decodeX(const TaskCtx &c, int pos) {
 }
 
 // Decoded Y symbol: packed (repeat column byte offset | match-column byte offset << 17), gap-y emission.
-__device__ __forceinline__ uint2 decodeY(const TaskCtx &c, int pos) {
+__device__ __forceinline__ uint2 decodeY(const TaskCtx &c, int pos, int &bad) {
     int b = 4, rc = 0;
     if (pos >= 0 && pos < c.ly) {
         uint32_t s = c.ys[pos];
@@ -115,6 +119,10 @@ __device__ __forceinline__ uint2 decodeY(const TaskCtx &c, int pos) {
             b = (int) s;
         }
         b = b > 4 ? 4 : b;
+        if (rc >= kMaxRepeat) {
+            rc = kMaxRepeat - 1;
+            bad = 1;
+        }
     }
     uint32_t pk = (uint32_t) (rc * 4) | ((uint32_t) (b * 4) << 17);
     return make_uint2(pk, __float_as_uint(c.gyS[b]));
@@ -135,17 +143,20 @@ __device__ __forceinline__ float matchEmission(const TaskCtx &c, const char *rpB
 template <int R>
 struct Ring {
     uint2 *buf;
-    int lo;  // first cached position (uniform)
+    int lo;   // first cached position (uniform)
+    int bad;  // sticky: a decoded symbol had a repeat count >= kMaxRepeat (clamped)
 };
 
 template <int R, bool IS_X>
 __device__ __forceinline__ void ringFill(const TaskCtx &c, Ring<R> &r, int newLo) {
     r.lo = newLo;
+    int bad = 0;
 #pragma unroll
     for (int k = 0; k < R / 32; k++) {
         int p = newLo + k * 32 + c.lane;
-        r.buf[p & (R - 1)] = IS_X ? decodeX(c, p) : decodeY(c, p);
+        r.buf[p & (R - 1)] = IS_X ? decodeX(c, p, bad) : decodeY(c, p, bad);
     }
+    if (__any_sync(FULL_MASK, bad)) r.bad = 1;
     __syncwarp();
 }
 
@@ -551,6 +562,9 @@ __device__ void runTask(const DpArgs &a, const SharedTables &tab, int taskIndex,
     double logLik = 0.0;
     bool bad = false;
 
+    rx.bad = 0;
+    ry.bad = 0;
+
     // ------------------------------------------------------------------
     // Forward sweep
     // ------------------------------------------------------------------
@@ -872,6 +886,7 @@ __device__ void runTask(const DpArgs &a, const SharedTables &tab, int taskIndex,
     if (lane == 0) {
         int s = status;
         if (bad) s |= kTaskWindow;
+        if (rx.bad | ry.bad) s |= kTaskSymbol;
         for (int k = 0; k < 3; k++) {
             to->count[k] = bad ? 0 : oc.written[k];
             if (!bad && oc.written[k] > oc.top[k]) s |= kTaskCapacity;
@@ -903,8 +918,8 @@ __global__ void __launch_bounds__(MAXT, 1) posteriorKernel(DpArgs a, int warpsPe
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int gwarp = blockIdx.x * warpsPerBlock + warp;
-    Ring<R> rx{rings + (size_t) warp * 2 * R, 0};
-    Ring<R> ry{rings + (size_t) warp * 2 * R + R, 0};
+    Ring<R> rx{rings + (size_t) warp * 2 * R, 0, 0};
+    Ring<R> ry{rings + (size_t) warp * 2 * R + R, 0, 0};
     float4 *chkBase = a.scratch + (size_t) gwarp * a.scratchBlocks * (C * 32);
     int2 *chkScal = a.scratchScalars + (size_t) gwarp * a.scratchBlocks;
     float4 *resumeBase = a.resume + (size_t) gwarp * (C * 32);
@@ -960,7 +975,7 @@ __global__ void bandKernel(BandArgs a) {
     bool ok = true;
     if (lane == 0) {
         band[0] = make_int2(0, 0);
-        cells += 1;
+        cells += N > 0 ? 1 : 0;  // an empty sub-problem computes nothing (impl/pairwiseAligner.c:698-701)
     }
     for (int k0 = 0; k0 <= nA; k0 += 32) {
         int k = k0 + lane;
@@ -1052,6 +1067,30 @@ __global__ void compactKernel(const Task *tasks, const TaskOut *out, int nTasks,
         dstX[k][to + i] = srcX[k][from + i];
         dstY[k][to + i] = srcY[k][from + i];
     }
+}
+
+// ---------------------------------------------------------------------------
+// FP32 FMA throughput probe: 16 independent FMA chains per thread.
+// ---------------------------------------------------------------------------
+
+__global__ void fmaProbeKernel(float *out, int iters) {
+    float a[16];
+    const float m = 1.0000001f, c = 1e-7f;
+#pragma unroll
+    for (int k = 0; k < 16; k++) a[k] = (float) (threadIdx.x + k) * 1e-3f;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 16; k++) a[k] = __fmaf_rn(a[k], m, c);
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 16; k++) s += a[k];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+cudaError_t launchFmaProbe(float *out, int blocks, int threads, int iters, cudaStream_t s) {
+    fmaProbeKernel<<<blocks, threads, 0, s>>>(out, iters);
+    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------

@@ -252,3 +252,34 @@ def load_polish_model(path: str) -> PolishModel:
     rev = build_state_model(int(hmm["type"]), hmm["transitions"], hmm["emissions"], True,
                             rep if use_rc else None, strand=0)
     return PolishModel(fwd, rev, ap, use_rle, use_rc, rep, raw=pol)
+
+
+def polish_model_from_tables(hmm_type: int, transitions, emissions, repeat_log10, alignment: AlignmentParams,
+                             use_repeat_counts: bool = True) -> PolishModel:
+    """PolishModel from raw tables (the HMM probabilities and the log10 repeat table)."""
+    rep = np.asarray(repeat_log10, dtype=np.float64) if use_repeat_counts else None
+    fwd = build_state_model(int(hmm_type), transitions, emissions, False, rep, strand=1)
+    rev = build_state_model(int(hmm_type), transitions, emissions, True, rep, strand=0)
+    return PolishModel(fwd, rev, alignment, True, use_repeat_counts, rep)
+
+
+def polish_model_from_npz(path: str) -> PolishModel:
+    """Reads a model fixture written by tests/golden/make_golden.py."""
+    z = np.load(path)
+    ap = AlignmentParams(threshold=float(z["threshold"]), min_diags_between_traceback=int(z["min_diags"]),
+                         traceback_diagonals=int(z["traceback_diags"]), diagonal_expansion=int(z["diagonal_expansion"]),
+                         constraint_diagonal_trim=int(z["constraint_trim"]),
+                         split_matrix_bigger_than_this=int(z["split"]), dynamic_anchor_expansion=bool(z["dynamic"]),
+                         gap_gamma=float(z["gap_gamma"]))
+    return polish_model_from_tables(int(z["hmm_type"]), z["transitions"], z["emissions"], z["repeat_log10"], ap,
+                                    bool(z["use_repeat_counts"]))
+
+
+def default_state_model(transitions, match, gap, boundary) -> StateModel:
+    """StateModel from tables of the reference's code-default machine (impl/stateMachine.c:598-630),
+    as probed from the reference build: 9 log transitions, 25 log match emissions, 5x2 log gap emissions,
+    4x3 boundary vectors (start, ragged start, end, ragged end)."""
+    gap = np.asarray(gap, dtype=np.float64).reshape(5, 2)
+    b = np.asarray(boundary, dtype=np.float64).reshape(4, 3)
+    return StateModel(np.asarray(transitions, dtype=np.float64), b[0], b[1], b[2], b[3],
+                      np.asarray(match, dtype=np.float64), gap[:, 0].copy(), gap[:, 1].copy(), run_length=False)

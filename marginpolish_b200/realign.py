@@ -43,6 +43,12 @@ class Engine:
         t = _lib.Tuning(0, warps_per_block, blocks_per_sm, 0)
         _lib.check(self._lib.mp_engine_set_tuning(self.handle, ctypes.byref(t)))
 
+    def fp32_peak_tflops(self) -> float:
+        """Measured FP32 FMA throughput of this device (TFLOP/s)."""
+        v = ctypes.c_double()
+        _lib.check(self._lib.mp_measure_fp32_peak(self.handle, v))
+        return float(v.value)
+
     def close(self) -> None:
         if self.handle:
             self._lib.mp_engine_destroy(self.handle)
@@ -227,6 +233,12 @@ class DeviceBatch:
             return _copy_view(lib, res)
         finally:
             lib.mp_result_destroy(res)
+
+    def timing(self):
+        """(band_ms, posterior_ms) CUDA-event times of the last run."""
+        b, q = c_float(), c_float()
+        _lib.check(self.engine._lib.mp_device_batch_timing(self.handle, b, q))
+        return float(b.value), float(q.value)
 
     def stats(self):
         cells, tasks, launches = c_int64(), c_int64(), ctypes.c_int32()

@@ -1,0 +1,125 @@
+"""GPU parity of the posterior pass against the FP64 oracle (Oracle B) and the
+reference's own code (Oracle A): posteriors within 1e-4 absolute, tuple sets
+equal outside the threshold tie band, reference output order, log-likelihood."""
+import numpy as np
+import pytest
+
+from marginpolish_b200 import AlignmentParams, Jobs, Model, realign_batch, synth
+from oracle.bindings import MpoModel
+from oracle.compare import check_job, check_loglik, set_diff_against_reference
+
+pytestmark = pytest.mark.gpu
+
+
+def _run_and_check(engine, gpu_model, mpo_models, jobs, params, ref=None, ref_models=None):
+    res = realign_batch(engine, gpu_model, params, jobs)
+    from oracle.bindings import ExactOracle
+    eo = ExactOracle()
+    worst = 0.0
+    for j in range(jobs.n_jobs):
+        sx = jobs.x_symbols[jobs.x_begin[j]:jobs.x_end[j]]
+        sy = jobs.y_symbols[jobs.y_offsets[j]:jobs.y_offsets[j + 1]]
+        a = jobs.anchors[jobs.anchor_offsets[j]:jobs.anchor_offsets[j + 1]]
+        rl = bool(jobs.ragged_left[j]) if jobs.ragged_left is not None else False
+        rr = bool(jobs.ragged_right[j]) if jobs.ragged_right is not None else False
+        m = mpo_models[0] if jobs.strand[j] else mpo_models[1]
+        o = eo.align_with_indels(m, sx, sy, a, params, rl, rr, dense=True)
+        shift = int(jobs.x_shift[j]) if jobs.x_shift is not None else 0
+        g = [res.job(j, k).copy() for k in range(3)]
+        for k in range(3):
+            g[k][:, 1] -= shift
+        rep = check_job(g, o, params.threshold)
+        worst = max(worst, rep["max_abs_posterior_error"])
+        if o["cells"] > 0:
+            check_loglik(res.log_likelihood[j], o["log_likelihood"])
+        assert res.cells[j] == o["cells"]
+        if ref is not None:
+            h = ref_models[0] if jobs.strand[j] else ref_models[1]
+            rlists = ref.align_with_indels(h, sx, sy, a, params, rl, rr)
+            set_diff_against_reference(g, rlists, o, params.threshold)
+    return res, worst
+
+
+def test_small_workload_matches_fp64_and_reference(engine, polish_model, ref_oracle):
+    wl = synth.config_small(seed=1)
+    jobs = wl.jobs()
+    gm = Model.from_polish(engine, polish_model)
+    mpo = (MpoModel.from_state_model(polish_model.forward), MpoModel.from_state_model(polish_model.reverse))
+    hmm_t, hmm_tr, hmm_em = 2, None, None
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "model_np.npz"))
+    hf = ref_oracle.model(int(z["hmm_type"]), z["transitions"], z["emissions"], False, z["repeat_log10"], 1)
+    hr = ref_oracle.model(int(z["hmm_type"]), z["transitions"], z["emissions"], True, z["repeat_log10"], 0)
+    res, worst = _run_and_check(engine, gm, mpo, jobs, polish_model.alignment, ref_oracle, (hf, hr))
+    assert worst <= 1e-4
+    assert res.total_cells > 2_000_000
+
+
+def test_known_answer_agcg(engine, default_model):
+    """tests/pairwiseAlignerTest.c:256-339: X=AGCG, Y=AGTTCG, default machine, threshold 0.2
+    -> match pairs exactly {(0,0),(1,1),(2,4),(3,5)}."""
+    conv = {"A": 0, "C": 1, "G": 2, "T": 3}
+    sx = np.array([conv[c] for c in "AGCG"], dtype=np.uint16)
+    sy = np.array([conv[c] for c in "AGTTCG"], dtype=np.uint16)
+    p = AlignmentParams(threshold=0.2, diagonal_expansion=2)
+    gm = Model(engine, default_model, default_model)
+    res = realign_batch(engine, gm, p, Jobs.single(sx, sy, np.zeros((0, 3), np.int32)))
+    pairs = {(int(x), int(y)) for _, x, y in res.job(0, 0)}
+    assert pairs == {(0, 0), (1, 1), (2, 4), (3, 5)}
+
+
+def _random_case(rng, n_max=100):
+    lx = int(rng.integers(0, n_max))
+    sx = rng.integers(0, 4, size=lx).astype(np.uint16)
+    # evolve: substitutions and indels
+    out = []
+    for c in sx:
+        u = rng.random()
+        if u < 0.1:
+            continue
+        out.append(int(rng.integers(0, 4)) if u < 0.2 else int(c))
+        if rng.random() < 0.1:
+            out.append(int(rng.integers(0, 4)))
+    sy = np.array(out, dtype=np.uint16)
+    return sx, sy
+
+
+def _random_anchors(rng, lx, ly):
+    """getRandomAnchorPairs (tests/pairwiseAlignerTest.c:341-357)."""
+    a, x, y = [], -1, -1
+    while True:
+        x += int(rng.integers(1, 20))
+        y += int(rng.integers(1, 20))
+        e = 2 * int(rng.integers(0, 5))
+        if x >= lx or y >= ly:
+            break
+        a.append((x, y, e))
+    return np.array(a, dtype=np.int32).reshape(-1, 3)
+
+
+@pytest.mark.parametrize("seed", list(range(6)))
+def test_random_banding_segments_and_splits(engine, default_model, seed):
+    """tests/pairwiseAlignerTest.c:418-455 style: random anchors, traceback parameters small enough to
+    force several traceback segments, dynamic expansion on or off, occasional ragged ends and splits."""
+    rng = np.random.default_rng(100 + seed)
+    gm = Model(engine, default_model, default_model)
+    mpo = (MpoModel.from_state_model(default_model), MpoModel.from_state_model(default_model))
+    for case in range(12):
+        sx, sy = _random_case(rng, 120)
+        tb = int(rng.integers(1, 10))
+        p = AlignmentParams(threshold=0.01, traceback_diagonals=tb, min_diags_between_traceback=tb + int(rng.integers(2, 10)),
+                            diagonal_expansion=2 * int(rng.integers(0, 10)), dynamic_anchor_expansion=bool(rng.random() > 0.5),
+                            split_matrix_bigger_than_this=int(rng.choice([3000 * 3000, 400, 900])))
+        a = _random_anchors(rng, sx.size, sy.size)
+        rl, rr = bool(rng.random() < 0.3), bool(rng.random() < 0.3)
+        jobs = Jobs.single(sx, sy, a, 1, rl, rr)
+        _run_and_check(engine, gm, mpo, jobs, p)
+
+
+def test_empty_and_tiny_sequences(engine, default_model):
+    gm = Model(engine, default_model, default_model)
+    mpo = (MpoModel.from_state_model(default_model), MpoModel.from_state_model(default_model))
+    p = AlignmentParams()
+    for sx, sy in [([], []), ([0, 1, 2], []), ([], [3, 3]), ([1], [1]), ([0, 4, 2], [0, 2])]:
+        jobs = Jobs.single(np.array(sx, np.uint16), np.array(sy, np.uint16), np.zeros((0, 3), np.int32))
+        _run_and_check(engine, gm, mpo, jobs, p)

@@ -24,7 +24,7 @@ namespace mp {
 cudaError_t launchPosterior(int C, const DpArgs &a, int blocks, int warps, cudaStream_t s);
 size_t posteriorSmemBytes(int C, int warps);
 int classStride(int C);
-int classMaxWarps(int C);
+int classMaxWarps(int C, int nTables);
 cudaError_t launchBand(const BandArgs &a, cudaStream_t s);
 cudaError_t launchCompact(const Task *tasks, const TaskOut *out, int nTasks, const int64_t *dst0,
                           const int64_t *dst1, const int64_t *dst2, int32_t *const *srcW, int32_t *const *srcX,
@@ -117,6 +117,7 @@ struct mp_engine {
 
 struct mp_model {
     mp_engine *engine = nullptr;
+    int sharedRepeat = 0;  // the two strands' repeat tables are identical
     DevModel host[2];
     DevBuf models;   // DevModel[2]
     DevBuf repeat;   // float [2][kRepTable]
@@ -229,6 +230,7 @@ extern "C" mp_status mp_model_create(mp_engine *e, const mp_model_desc *fwd, con
     mp_status s = lowerModel(fwd, m->host[0], rp.data());
     if (s == MP_OK) s = lowerModel(rev, m->host[1], rp.data() + kRepTable);
     if (s == MP_OK) {
+        m->sharedRepeat = memcmp(rp.data(), rp.data() + kRepTable, sizeof(float) * kRepTable) == 0 ? 1 : 0;
         cudaSetDevice(e->device);
         s = m->models.reserve(sizeof(DevModel) * 2);
         if (s == MP_OK) s = m->repeat.reserve(sizeof(float) * 2 * kRepTable);
@@ -697,8 +699,8 @@ static mp_status launchQueues(mp_device_batch *db) {
         blocksOf[ci] = warpsOf[ci] = scratchBlocksOf[ci] = 0;
         if (db->classCount[ci] == 0) continue;
         int C = kClasses[ci];
-        int warps = e->tuning.warps_per_block > 0 ? e->tuning.warps_per_block : classMaxWarps(C);
-        warps = std::min(warps, classMaxWarps(C));
+        int maxW = classMaxWarps(C, db->m->sharedRepeat ? 1 : 2);
+        int warps = e->tuning.warps_per_block > 0 ? std::min(e->tuning.warps_per_block, maxW) : maxW;
         int blocksPerSm = e->tuning.blocks_per_sm > 0 ? e->tuning.blocks_per_sm : 1;
         int blocks = e->smCount * blocksPerSm;
         int maxBlocks = (db->classCount[ci] + warps - 1) / warps;  // no more warps than tasks
@@ -748,6 +750,7 @@ static mp_status launchQueues(mp_device_batch *db) {
         a.minDiagsBetweenTraceBack = (int32_t) std::min<int64_t>(db->p.min_diags_between_traceback, 1 << 30);
         a.traceBackDiagonals = (int32_t) db->p.traceback_diagonals;
         a.diagonalExpansion = (int32_t) std::min<int64_t>(db->p.diagonal_expansion, 1 << 29);
+        a.sharedRepeat = db->m->sharedRepeat;
         CUDA_TRY(launchPosterior(C, a, blocksOf[ci], warpsOf[ci], st));
         db->launchesPerRun++;
     }

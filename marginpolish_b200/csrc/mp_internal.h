@@ -83,6 +83,7 @@ struct DpArgs {
     int32_t minDiagsBetweenTraceBack;
     int32_t traceBackDiagonals;
     int32_t diagonalExpansion;
+    int32_t sharedRepeat;       // both models use repeat table 0
 };
 
 struct BandArgs {

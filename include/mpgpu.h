@@ -187,6 +187,34 @@ mp_status mp_split_points(const int32_t *anchors, int64_t n_anchors, int64_t lx,
 mp_status mp_crop_range(const int32_t *anchors, int64_t n_anchors, int64_t template_length, int64_t read_length,
                         int64_t *start, int64_t *end);
 
+/* ---- single read without any memory allocation ----
+ * No counterpart in the reference. For callers that cannot allocate device memory
+ * (their framework's pool owns the GPU, or allocation is not allowed where they
+ * run): the pass uses only a fixed device array inside this library (8 MiB on
+ * every GPU that loads it, held until exit) plus the caller's own host buffers.
+ * Limits: lx + ly < MP_NOALLOC_MAX_DIAGONALS, one split rectangle, a band hull
+ * of at most 60 window slots; beyond them MP_ERR_ARGUMENT. The first call on a
+ * device looks the array up with cudaGetSymbolAddress (make it before any stream
+ * capture). Calls share the array and serialise internally; two calls running on
+ * the GPU at the same time would race. Output lists: the caller's host arrays of
+ * `capacity` entries; `count` receives the tuple counts (MP_ERR_OVERFLOW when a
+ * count exceeds its capacity), in the same order as mp_realign_batch. */
+#define MP_NOALLOC_MAX_DIAGONALS 32768
+#define MP_NOALLOC_SCRATCH_BYTES (8u << 20)
+typedef struct {
+    int32_t *weight[3];   /* list 0 match, 1 gap-x, 2 gap-y */
+    int32_t *x[3];
+    int32_t *y[3];
+    int64_t capacity[3];
+    int64_t count[3];     /* out */
+    double log_likelihood; /* out */
+    int64_t cells;        /* out */
+} mp_noalloc_output;
+mp_status mp_realign_single_noalloc(mp_engine *e, const mp_model *m, const mp_params *p, const uint16_t *x,
+                                    int64_t lx, const uint16_t *y, int64_t ly, const int32_t *anchors,
+                                    int64_t n_anchors, int strand, int ragged_left, int ragged_right,
+                                    mp_noalloc_output *out);
+
 /* ---- run-length encoding and anchors (host, integer-exact) ---- */
 /* rleString_construct (impl/polisher.c:1357-1389): runs of identical characters.
  * run_chars / run_counts need room for n entries; *n_runs receives the run count. */

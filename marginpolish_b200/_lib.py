@@ -100,6 +100,18 @@ class ResultView(Structure):
     ]
 
 
+class NoallocOutput(Structure):
+    _fields_ = [
+        ("weight", POINTER(c_int32) * 3),
+        ("x", POINTER(c_int32) * 3),
+        ("y", POINTER(c_int32) * 3),
+        ("capacity", c_int64 * 3),
+        ("count", c_int64 * 3),
+        ("log_likelihood", c_double),
+        ("cells", c_int64),
+    ]
+
+
 class Tuning(Structure):
     _fields_ = [
         ("checkpoint_stride", c_int32),
@@ -116,6 +128,7 @@ EXPORTED = [
     "mp_result_destroy", "mp_device_batch_create", "mp_device_batch_run", "mp_device_batch_fetch",
     "mp_device_batch_stats", "mp_device_batch_destroy", "mp_band", "mp_split_points", "mp_crop_range",
     "mp_rle_encode", "mp_rle_symbols", "mp_rle_anchors", "mp_device_batch_timing", "mp_measure_fp32_peak",
+    "mp_realign_single_noalloc",
 ]
 
 _lib = None
@@ -150,6 +163,8 @@ def load() -> ctypes.CDLL:
         "mp_device_batch_destroy": (None, [c_void_p]),
         "mp_device_batch_timing": (c_int, [c_void_p, P(c_float), P(c_float)]),
         "mp_measure_fp32_peak": (c_int, [c_void_p, P(c_double)]),
+        "mp_realign_single_noalloc": (c_int, [c_void_p, c_void_p, P(Params), P(c_uint16), c_int64, P(c_uint16),
+                                              c_int64, P(c_int32), c_int64, c_int, c_int, c_int, P(NoallocOutput)]),
         "mp_band": (c_int, [P(c_int32), c_int64, c_int64, c_int64, c_int64, c_int, P(c_int64)]),
         "mp_split_points": (c_int, [P(c_int32), c_int64, c_int64, c_int64, c_int64, c_int, c_int, P(c_int64),
                                     c_int64, P(c_int64)]),

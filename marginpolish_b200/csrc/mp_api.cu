@@ -8,6 +8,7 @@
 //  * crop range        -- getAlignedPairsWithIndelsCroppingReference (impl/polisher.c:613-628)
 #include "../../include/mpgpu.h"
 #include "mp_internal.h"
+#include "mp_host.h"
 
 #include <algorithm>
 #include <atomic>
@@ -62,6 +63,16 @@ static mp_status failf(mp_status s, const char *fmt, ...) {
         if (_s != MP_OK) return _s;    \
     } while (0)
 
+mp_status mp_fail(mp_status s, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_lastError = buf;
+    return s;
+}
+
 extern "C" const char *mp_last_error(void) {
     return g_lastError.c_str();
 }
@@ -69,59 +80,6 @@ extern "C" const char *mp_last_error(void) {
 extern "C" const char *mp_version(void) {
     return "mpgpu 0.1 (sm_100a)";
 }
-
-// ---------------------------------------------------------------------------
-// device buffers
-// ---------------------------------------------------------------------------
-
-struct DevBuf {
-    void *p = nullptr;
-    size_t bytes = 0;
-    DevBuf() = default;
-    DevBuf(const DevBuf &) = delete;
-    DevBuf &operator=(const DevBuf &) = delete;
-    ~DevBuf() { release(); }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-    }
-    mp_status reserve(size_t n) {
-        if (n <= bytes && p) return MP_OK;
-        release();
-        size_t want = n > 0 ? n : 16;
-        cudaError_t e = cudaMalloc(&p, want);
-        if (e != cudaSuccess) {
-            p = nullptr;
-            return failf(MP_ERR_MEMORY, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
-        }
-        bytes = want;
-        return MP_OK;
-    }
-    template <class T>
-    T *as() const { return static_cast<T *>(p); }
-};
-
-// ---------------------------------------------------------------------------
-// engine and model
-// ---------------------------------------------------------------------------
-
-struct mp_engine {
-    int device = 0;
-    int smCount = 0;
-    int ccMajor = 0, ccMinor = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    mp_tuning tuning{};
-};
-
-struct mp_model {
-    mp_engine *engine = nullptr;
-    int sharedRepeat = 0;  // the two strands' repeat tables are identical
-    DevModel host[2];
-    DevBuf models;   // DevModel[2]
-    DevBuf repeat;   // float [2][kRepTable]
-};
 
 extern "C" mp_status mp_engine_create(int device, mp_engine **out) {
     if (!out) return failf(MP_ERR_ARGUMENT, "mp_engine_create: out is NULL");
@@ -425,6 +383,18 @@ static int classFor(int64_t slots) {
     return 0;
 }
 
+namespace mp {
+int64_t splitCount(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, int64_t maxSize, bool raggedL, bool raggedR) {
+    std::vector<SplitRect> r;
+    splitPoints(an, nA, lx, ly, maxSize, raggedL, raggedR, r);
+    return (int64_t) r.size();
+}
+
+int64_t hullSlots(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, bool dynamic, int64_t fixedExp) {
+    return hullSlotBound(an, nA, 0, 0, lx, ly, dynamic, fixedExp);
+}
+}  // namespace mp
+
 struct PlannedTask {
     Task t;
     int cls;
@@ -481,6 +451,24 @@ static mp_status validateJob(const mp_batch *b, int64_t j, const mp_params *p) {
     return MP_OK;
 }
 
+namespace mp {
+mp_status validateAnchors(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, bool dynamic, int64_t job) {
+    int64_t px = -1, py = -1;
+    for (int64_t i = 0; i < nA; i++) {
+        int64_t x = an[3 * i], y = an[3 * i + 1], ex = an[3 * i + 2];
+        if (x <= px || y <= py || x >= lx || y >= ly)
+            return failf(MP_ERR_ARGUMENT, "job %lld: anchor %lld (%lld, %lld) not strictly increasing / in range",
+                         (long long) job, (long long) i, (long long) x, (long long) y);
+        if (dynamic && (ex < 0 || (ex & 1)))
+            return failf(MP_ERR_ARGUMENT, "job %lld: anchor %lld expansion %lld must be even and >= 0",
+                         (long long) job, (long long) i, (long long) ex);
+        px = x;
+        py = y;
+    }
+    return MP_OK;
+}
+}  // namespace mp
+
 static mp_status validateParams(const mp_params *p) {
     if (!p) return failf(MP_ERR_ARGUMENT, "params is NULL");
     if (!(p->threshold >= 0.0 && p->threshold <= 1.0))
@@ -494,6 +482,12 @@ static mp_status validateParams(const mp_params *p) {
         return failf(MP_ERR_ARGUMENT, "traceback_diagonals + 1 must be < min_diags_between_traceback");
     return MP_OK;
 }
+
+namespace mp {
+mp_status validateParamsStruct(const mp_params *p) {
+    return validateParams(p);
+}
+}  // namespace mp
 
 static mp_status planBatch(mp_device_batch *db, const mp_batch *b) {
     const int64_t nJobs = b->n_jobs;

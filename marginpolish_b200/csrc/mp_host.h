@@ -1,0 +1,79 @@
+// Host-side objects shared by the C ABI translation units (internal).
+#pragma once
+
+#include "../../include/mpgpu.h"
+#include "mp_internal.h"
+
+#include <cstdint>
+#include <string>
+
+// Records the thread-local error message of the C ABI and returns s.
+mp_status mp_fail(mp_status s, const char *fmt, ...);
+
+// Reference restatements used by the planner (defined in mp_api.cu).
+namespace mp {
+struct SplitRectH {
+    int64_t x1, y1, x2, y2;
+};
+// Number of split rectangles of one job (getSplitPoints, impl/pairwiseAligner.c:899-926).
+int64_t splitCount(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, int64_t maxSize, bool raggedL, bool raggedR);
+// Upper bound of the 5-diagonal band hull in window slots.
+int64_t hullSlots(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, bool dynamic, int64_t fixedExp);
+// Checks anchor order / range / expansion parity of one job.
+mp_status validateAnchors(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, bool dynamic, int64_t job);
+mp_status validateParamsStruct(const mp_params *p);
+}  // namespace mp
+
+// ---------------------------------------------------------------------------
+// device buffers
+// ---------------------------------------------------------------------------
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    mp_status reserve(size_t n) {
+        if (n <= bytes && p) return MP_OK;
+        release();
+        size_t want = n > 0 ? n : 16;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return mp_fail(MP_ERR_MEMORY, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
+        }
+        bytes = want;
+        return MP_OK;
+    }
+    template <class T>
+    T *as() const { return static_cast<T *>(p); }
+};
+
+// ---------------------------------------------------------------------------
+// engine and model
+// ---------------------------------------------------------------------------
+
+struct mp_engine {
+    int device = 0;
+    int smCount = 0;
+    int ccMajor = 0, ccMinor = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    mp_tuning tuning{};
+};
+
+struct mp_model {
+    mp_engine *engine = nullptr;
+    int sharedRepeat = 0;  // the two strands' repeat tables are identical
+    mp::DevModel host[2];
+    DevBuf models;   // DevModel[2]
+    DevBuf repeat;   // float [2][kRepTable]
+};
+

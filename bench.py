@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work per baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--lanes", type=int, default=0, choices=[0, 8, 16, 32],
+                    help="lanes per banded sub-problem (0 = the engine's automatic choice)")
+    ap.add_argument("--warps", type=int, default=0, help="warps per block of the posterior kernel (0 = automatic)")
     return ap.parse_args()
 
 
@@ -256,6 +259,7 @@ def run_ours(args, rank, world, local):
     jobs = wl.jobs()
     gen_s = time.perf_counter() - t0
     engine = Engine(local)
+    engine.set_tuning(warps_per_block=args.warps, lanes_per_task=args.lanes)
     model = Model.from_polish(engine, pm)
     db = DeviceBatch(engine, model, pm.alignment, jobs)
 
@@ -343,7 +347,8 @@ def run_ours(args, rank, world, local):
             "config": {"workload": f"{args.config}: {wl.meta}", "reads": jobs.n_jobs, "cells_per_gpu_step": cells,
                        "tasks": n_tasks, "l2": "inputs and band/scratch/output buffers exceed the 126 MB L2",
                        "generation_s": round(gen_s, 1), "band_ms": float(np.median(band_ms)),
-                       "posterior_ms": post, "wall_s_timed": wall},
+                       "posterior_ms": post, "wall_s_timed": wall,
+                       "tuning": {"lanes_per_task": args.lanes or "auto", "warps_per_block": args.warps or "auto"}},
             "e2e": e2e,
             "gpu_launches": launches * args.steps,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

@@ -133,13 +133,17 @@ mp_status mp_engine_info(const mp_engine *e, int *sm_count, int *cc_major, int *
 mp_status mp_model_create(mp_engine *e, const mp_model_desc *fwd, const mp_model_desc *rev, mp_model **out);
 void mp_model_destroy(mp_model *m);
 
-/* Tuning: slots are assigned in lanes of `slots_per_lane` (0 = automatic),
- * checkpoint stride in anti-diagonals (0 = automatic), warps per block (0 = automatic). */
+/* Tuning of the posterior kernel (0 = automatic everywhere):
+ *   checkpoint_stride  unused (each kernel variant has a fixed stride), kept for layout;
+ *   warps_per_block    resident warps per block, capped by the variant's shared memory;
+ *   blocks_per_sm      persistent blocks per SM;
+ *   lanes_per_task     32, 16 or 8: lanes that carry one banded sub-problem. With 16 or 8,
+ *                      a warp advances 2 or 4 sub-problems of similar length in lockstep. */
 typedef struct {
     int32_t checkpoint_stride;
     int32_t warps_per_block;
     int32_t blocks_per_sm;
-    int32_t reserved;
+    int32_t lanes_per_task;
 } mp_tuning;
 mp_status mp_engine_set_tuning(mp_engine *e, const mp_tuning *t);
 

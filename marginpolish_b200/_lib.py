@@ -117,7 +117,7 @@ class Tuning(Structure):
         ("checkpoint_stride", c_int32),
         ("warps_per_block", c_int32),
         ("blocks_per_sm", c_int32),
-        ("reserved", c_int32),
+        ("lanes_per_task", c_int32),
     ]
 
 

@@ -1,5 +1,5 @@
 // C ABI of the realignment engine: model lowering, batch planning (splits,
-// slot classes, length-sorted queues), device memory and launches.
+// kernel variants, length-sorted queues), device memory and launches.
 //
 // Reference behaviour restated here (integer logic, bit-exact):
 //  * split rectangles  -- getSplitPoints / getSplitPointsP (impl/pairwiseAligner.c:875-926)
@@ -22,10 +22,10 @@
 #include <vector>
 
 namespace mp {
-cudaError_t launchPosterior(int C, const DpArgs &a, int blocks, int warps, cudaStream_t s);
-size_t posteriorSmemBytes(int C, int warps);
-int classStride(int C);
-int classMaxWarps(int C, int nTables);
+int variantCount();
+bool variantShape(int v, int *C, int *L, int *K);
+int variantMaxWarps(int v, int nTables);
+cudaError_t launchVariant(int v, const DpArgs &a, int blocks, int warps, cudaStream_t s);
 cudaError_t launchBand(const BandArgs &a, cudaStream_t s);
 cudaError_t launchCompact(const Task *tasks, const TaskOut *out, int nTasks, const int64_t *dst0,
                           const int64_t *dst1, const int64_t *dst2, int32_t *const *srcW, int32_t *const *srcX,
@@ -132,6 +132,10 @@ extern "C" mp_status mp_engine_info(const mp_engine *e, int *sm, int *ma, int *m
 
 extern "C" mp_status mp_engine_set_tuning(mp_engine *e, const mp_tuning *t) {
     if (!e || !t) return failf(MP_ERR_ARGUMENT, "engine or tuning is NULL");
+    if (t->lanes_per_task != 0 && t->lanes_per_task != 32 && t->lanes_per_task != 16 && t->lanes_per_task != 8)
+        return failf(MP_ERR_ARGUMENT, "lanes_per_task must be 0, 32, 16 or 8 (got %d)", t->lanes_per_task);
+    if (t->warps_per_block < 0 || t->blocks_per_sm < 0)
+        return failf(MP_ERR_ARGUMENT, "negative tuning value");
     e->tuning = *t;
     return MP_OK;
 }
@@ -339,8 +343,40 @@ extern "C" mp_status mp_crop_range(const int32_t *anchors, int64_t nA, int64_t t
 // planning
 // ---------------------------------------------------------------------------
 
-static const int kClasses[] = {2, 3, 4, 6, 8};
-static const int kNumClasses = 5;
+// Kernel variants (C slots per lane, L lanes per task; see mp_posterior.cu). A task
+// runs in the first variant of the engine's preference list whose window holds its
+// band hull: S - 2C >= hull slots, S = L*C. Every list has ascending capacities.
+static const int kPrefAuto[] = {0, 3, 4, 5, 6};  // measured fastest on the batched workload
+static const int kPref32[] = {0, 3, 4, 5, 6};
+static const int kPref16[] = {1, 0, 3, 4, 5, 6};
+static const int kPref8[] = {2, 1, 0, 3, 4, 5, 6};
+static const int kMaxHullSlots = 8 * 32 - 2 * 8;  // widest variant
+
+static int variantCapacity(int v) {
+    int C = 0, L = 0, K = 0;
+    if (!variantShape(v, &C, &L, &K)) return 0;
+    return L * C - 2 * C;
+}
+
+// Variant for a task needing `slots` window slots under lane preference `lanes`
+// (32, 16, 8 or 0 = automatic); -1 when none is wide enough.
+static int pickVariant(int lanes, int64_t slots) {
+    const int *list = kPrefAuto;
+    int n = (int) (sizeof(kPrefAuto) / sizeof(int));
+    if (lanes == 32) {
+        list = kPref32;
+        n = (int) (sizeof(kPref32) / sizeof(int));
+    } else if (lanes == 16) {
+        list = kPref16;
+        n = (int) (sizeof(kPref16) / sizeof(int));
+    } else if (lanes == 8) {
+        list = kPref8;
+        n = (int) (sizeof(kPref8) / sizeof(int));
+    }
+    for (int i = 0; i < n; i++)
+        if (slots <= variantCapacity(list[i])) return list[i];
+    return -1;
+}
 
 // Upper bound (in window slots) of the hull of 5 consecutive anti-diagonal bands:
 // the union of up to three consecutive anchor boxes, clipped to the matrix.
@@ -375,14 +411,6 @@ static int64_t hullSlotBound(const int32_t *an, int64_t nA, int64_t x1, int64_t 
     return best;
 }
 
-static int classFor(int64_t slots) {
-    for (int i = 0; i < kNumClasses; i++) {
-        int C = kClasses[i];
-        if (slots <= 32 * C - 2 * C) return C;
-    }
-    return 0;
-}
-
 namespace mp {
 int64_t splitCount(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, int64_t maxSize, bool raggedL, bool raggedR) {
     std::vector<SplitRect> r;
@@ -397,7 +425,7 @@ int64_t hullSlots(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, bool dy
 
 struct PlannedTask {
     Task t;
-    int cls;
+    int32_t hull;  // window slots the band hull needs
 };
 
 struct mp_device_batch {
@@ -406,16 +434,17 @@ struct mp_device_batch {
     mp_params p{};
     int64_t nJobs = 0;
     std::vector<Task> tasks;
-    std::vector<int> cls;
+    std::vector<int32_t> hull;          // per task: window slots needed (raised by window retries)
+    std::vector<int> var;               // per task: kernel variant of the current run
     std::vector<int64_t> jobFirstTask;  // n_jobs+1
     int64_t totalDiags = 0;
     int64_t outCap[3] = {0, 0, 0};
     // device
     DevBuf xs, ys, anchors, dTasks, band, dOut, outW[3], outX[3], outY[3];
-    DevBuf orders, queue, scratch, scratchScal, resume;
-    std::vector<int> classOrderOff;  // per class offset into orders
-    std::vector<int> classCount;
-    std::vector<int64_t> classMaxN;
+    DevBuf orders, queue, scratch, scratchScal;
+    std::vector<int> varOrderOff;  // per variant offset into orders
+    std::vector<int> varCount;
+    std::vector<int64_t> varMaxN;
     std::vector<TaskOut> hostOut;
     int launchesPerRun = 0;
     bool ran = false;
@@ -546,11 +575,11 @@ static mp_status planBatch(mp_device_batch *db, const mp_batch *b) {
                 tk.expansion = (int32_t) p->diagonal_expansion;
                 int64_t slots = hullSlotBound(an + 3 * first, tk.nAnchors, r.x1, r.y1, tk.lx, tk.ly,
                                               p->dynamic_anchor_expansion != 0, p->diagonal_expansion);
-                pt.cls = classFor(slots);
-                if (pt.cls == 0) {
+                pt.hull = (int32_t) std::min<int64_t>(slots, 1 << 30);
+                if (slots > kMaxHullSlots) {
                     statuses[t] = failf(MP_ERR_OVERFLOW,
-                                        "job %lld: band hull of %lld slots exceeds the widest slot class (%d)",
-                                        (long long) j, (long long) slots, 32 * 8 - 16);
+                                        "job %lld: band hull of %lld slots exceeds the widest kernel window (%d)",
+                                        (long long) j, (long long) slots, kMaxHullSlots);
                     errors[t] = g_lastError;
                     return;
                 }
@@ -572,12 +601,12 @@ static mp_status planBatch(mp_device_batch *db, const mp_batch *b) {
     }
     // assemble in job order
     db->tasks.clear();
-    db->cls.clear();
+    db->hull.clear();
     db->jobFirstTask.assign(1, 0);
     for (unsigned t = 0; t < nThreads; t++) {
         for (auto &pt : perThread[t]) {
             db->tasks.push_back(pt.t);
-            db->cls.push_back(pt.cls);
+            db->hull.push_back(pt.hull);
         }
         for (int64_t c : perThreadJobCount[t]) db->jobFirstTask.push_back(db->jobFirstTask.back() + c);
     }
@@ -603,30 +632,36 @@ static mp_status planBatch(mp_device_batch *db, const mp_batch *b) {
     return MP_OK;
 }
 
-// Builds the per-class length-sorted queues for the tasks in `subset`.
-static void buildQueues(mp_device_batch *db, const std::vector<int32_t> &subset, std::vector<int32_t> &orderHost) {
-    db->classOrderOff.assign(kNumClasses + 1, 0);
-    db->classCount.assign(kNumClasses, 0);
-    db->classMaxN.assign(kNumClasses, 0);
-    std::vector<std::vector<int32_t>> per(kNumClasses);
+// Picks each task's kernel variant under the engine's tuning and builds the
+// per-variant length-sorted queues for the tasks in `subset`.
+static mp_status buildQueues(mp_device_batch *db, const std::vector<int32_t> &subset, std::vector<int32_t> &orderHost) {
+    const int nV = variantCount();
+    db->varOrderOff.assign(nV + 1, 0);
+    db->varCount.assign(nV, 0);
+    db->varMaxN.assign(nV, 0);
+    db->var.resize(db->tasks.size(), -1);
+    std::vector<std::vector<int32_t>> per(nV);
     for (int32_t t : subset) {
-        int ci = 0;
-        while (kClasses[ci] != db->cls[t]) ci++;
-        per[ci].push_back(t);
+        const int v = pickVariant(db->e->tuning.lanes_per_task, db->hull[t]);
+        if (v < 0)
+            return failf(MP_ERR_OVERFLOW, "job %d: band wider than the widest kernel window", db->tasks[t].job);
+        db->var[t] = v;
+        per[v].push_back(t);
         int64_t N = (int64_t) db->tasks[t].lx + db->tasks[t].ly;
-        db->classMaxN[ci] = std::max(db->classMaxN[ci], N);
+        db->varMaxN[v] = std::max(db->varMaxN[v], N);
     }
     orderHost.clear();
-    for (int ci = 0; ci < kNumClasses; ci++) {
-        auto &v = per[ci];
-        std::stable_sort(v.begin(), v.end(), [&](int32_t a, int32_t b) {
-            return (db->tasks[a].lx + db->tasks[a].ly) > (db->tasks[b].lx + db->tasks[b].ly);
+    for (int v = 0; v < nV; v++) {
+        auto &q = per[v];
+        std::stable_sort(q.begin(), q.end(), [&](int32_t x, int32_t y) {
+            return (db->tasks[x].lx + db->tasks[x].ly) > (db->tasks[y].lx + db->tasks[y].ly);
         });
-        db->classOrderOff[ci] = (int) orderHost.size();
-        db->classCount[ci] = (int) v.size();
-        orderHost.insert(orderHost.end(), v.begin(), v.end());
+        db->varOrderOff[v] = (int) orderHost.size();
+        db->varCount[v] = (int) q.size();
+        orderHost.insert(orderHost.end(), q.begin(), q.end());
     }
-    db->classOrderOff[kNumClasses] = (int) orderHost.size();
+    db->varOrderOff[nV] = (int) orderHost.size();
+    return MP_OK;
 }
 
 static mp_status upload(DevBuf &buf, const void *src, size_t bytes, cudaStream_t s) {
@@ -669,7 +704,7 @@ extern "C" mp_status mp_device_batch_create(mp_engine *e, const mp_model *m, con
         if (s == MP_OK) s = db->outX[k].reserve(n);
         if (s == MP_OK) s = db->outY[k].reserve(n);
     }
-    if (s == MP_OK) s = db->queue.reserve(sizeof(int32_t) * kNumClasses);
+    if (s == MP_OK) s = db->queue.reserve(sizeof(int32_t) * variantCount());
     if (s == MP_OK) {
         cudaError_t ce = cudaStreamSynchronize(st);
         if (ce != cudaSuccess) s = failf(MP_ERR_CUDA, "upload failed: %s", cudaGetErrorString(ce));
@@ -683,49 +718,48 @@ extern "C" mp_status mp_device_batch_create(mp_engine *e, const mp_model *m, con
 }
 
 // Launches the posterior kernels for the current queues (one persistent launch per
-// slot class with tasks). Scratch for all classes is reserved before the first launch.
+// variant with tasks). Scratch for all variants is reserved before the first launch:
+// every task slot (warp x tasks per warp) owns checkpoints for the longest task.
 static mp_status launchQueues(mp_device_batch *db) {
     mp_engine *e = db->e;
     cudaStream_t st = e->stream;
-    int blocksOf[kNumClasses], warpsOf[kNumClasses], scratchBlocksOf[kNumClasses];
-    size_t needScratch = 0, needScal = 0, needResume = 0;
-    for (int ci = 0; ci < kNumClasses; ci++) {
-        blocksOf[ci] = warpsOf[ci] = scratchBlocksOf[ci] = 0;
-        if (db->classCount[ci] == 0) continue;
-        int C = kClasses[ci];
-        int maxW = classMaxWarps(C, db->m->sharedRepeat ? 1 : 2);
-        int warps = e->tuning.warps_per_block > 0 ? std::min(e->tuning.warps_per_block, maxW) : maxW;
-        int blocksPerSm = e->tuning.blocks_per_sm > 0 ? e->tuning.blocks_per_sm : 1;
-        int blocks = e->smCount * blocksPerSm;
-        int maxBlocks = (db->classCount[ci] + warps - 1) / warps;  // no more warps than tasks
-        blocks = std::max(1, std::min(blocks, maxBlocks));
-        int K = classStride(C);
-        int scratchBlocks = (int) (db->classMaxN[ci] / K + 2);
-        size_t wt = (size_t) blocks * warps;
-        needScratch = std::max(needScratch, (size_t) scratchBlocks * C * 32 * sizeof(float4) * wt);
-        needScal = std::max(needScal, sizeof(int2) * (size_t) scratchBlocks * wt);
-        needResume = std::max(needResume, sizeof(float4) * C * 32 * wt);
-        blocksOf[ci] = blocks;
-        warpsOf[ci] = warps;
-        scratchBlocksOf[ci] = scratchBlocks;
+    const int nV = variantCount();
+    std::vector<int> blocksOf(nV, 0), warpsOf(nV, 0), scratchBlocksOf(nV, 0);
+    size_t needScratch = 0, needScal = 0;
+    for (int v = 0; v < nV; v++) {
+        if (db->varCount[v] == 0) continue;
+        int C = 0, L = 0, K = 0;
+        variantShape(v, &C, &L, &K);
+        const int G = 32 / L;
+        const int maxW = variantMaxWarps(v, db->m->sharedRepeat ? 1 : 2);
+        const int warps = e->tuning.warps_per_block > 0 ? std::min(e->tuning.warps_per_block, maxW) : maxW;
+        const int blocksPerSm = e->tuning.blocks_per_sm > 0 ? e->tuning.blocks_per_sm : 1;
+        const int loads = (db->varCount[v] + G - 1) / G;  // warp-loads of G tasks
+        const int maxBlocks = (loads + warps - 1) / warps;  // no more warps than loads
+        const int blocks = std::max(1, std::min(e->smCount * blocksPerSm, maxBlocks));
+        const int scratchBlocks = (int) (db->varMaxN[v] / K + 2);
+        const size_t slots = (size_t) blocks * warps * G;
+        needScratch = std::max(needScratch, (size_t) scratchBlocks * (size_t) (C * L) * sizeof(float4) * slots);
+        needScal = std::max(needScal, sizeof(int2) * (size_t) scratchBlocks * slots);
+        blocksOf[v] = blocks;
+        warpsOf[v] = warps;
+        scratchBlocksOf[v] = scratchBlocks;
     }
-    if (needScratch > db->scratch.bytes || needScal > db->scratchScal.bytes || needResume > db->resume.bytes) {
+    if (needScratch > db->scratch.bytes || needScal > db->scratchScal.bytes) {
         CUDA_TRY(cudaStreamSynchronize(st));
         MP_TRY(db->scratch.reserve(needScratch));
         MP_TRY(db->scratchScal.reserve(needScal));
-        MP_TRY(db->resume.reserve(needResume));
     }
-    CUDA_TRY(cudaMemsetAsync(db->queue.p, 0, sizeof(int32_t) * kNumClasses, st));
-    for (int ci = 0; ci < kNumClasses; ci++) {
-        if (db->classCount[ci] == 0) continue;
-        int C = kClasses[ci];
+    CUDA_TRY(cudaMemsetAsync(db->queue.p, 0, sizeof(int32_t) * nV, st));
+    for (int v = 0; v < nV; v++) {
+        if (db->varCount[v] == 0) continue;
         DpArgs a;
         memset(&a, 0, sizeof(a));
         a.tasks = db->dTasks.as<Task>();
-        a.order = db->orders.as<int32_t>() + db->classOrderOff[ci];
-        a.nTasks = db->classCount[ci];
-        a.scratchBlocks = scratchBlocksOf[ci];
-        a.queue = db->queue.as<int32_t>() + ci;
+        a.order = db->orders.as<int32_t>() + db->varOrderOff[v];
+        a.nTasks = db->varCount[v];
+        a.scratchBlocks = scratchBlocksOf[v];
+        a.queue = db->queue.as<int32_t>() + v;
         a.xs = db->xs.as<uint16_t>();
         a.ys = db->ys.as<uint16_t>();
         a.band = db->band.as<int2>();
@@ -733,7 +767,6 @@ static mp_status launchQueues(mp_device_batch *db) {
         a.repeatProb = db->m->repeat.as<float>();
         a.scratch = db->scratch.as<float4>();
         a.scratchScalars = db->scratchScal.as<int2>();
-        a.resume = db->resume.as<float4>();
         for (int k = 0; k < 3; k++) {
             a.outW[k] = db->outW[k].as<int32_t>();
             a.outX[k] = db->outX[k].as<int32_t>();
@@ -745,7 +778,7 @@ static mp_status launchQueues(mp_device_batch *db) {
         a.traceBackDiagonals = (int32_t) db->p.traceback_diagonals;
         a.diagonalExpansion = (int32_t) std::min<int64_t>(db->p.diagonal_expansion, 1 << 29);
         a.sharedRepeat = db->m->sharedRepeat;
-        CUDA_TRY(launchPosterior(C, a, blocksOf[ci], warpsOf[ci], st));
+        CUDA_TRY(launchVariant(v, a, blocksOf[v], warpsOf[v], st));
         db->launchesPerRun++;
     }
     return MP_OK;
@@ -759,7 +792,7 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
     db->launchesPerRun = 0;
     std::vector<int32_t> all(nTasks), orderHost;
     for (int i = 0; i < nTasks; i++) all[i] = i;
-    buildQueues(db, all, orderHost);
+    MP_TRY(buildQueues(db, all, orderHost));
     MP_TRY(upload(db->orders, orderHost.data(), sizeof(int32_t) * std::max<size_t>(orderHost.size(), 1), st));
     if (!db->evBand) CUDA_TRY(cudaEventCreate(&db->evBand));
     CUDA_TRY(cudaEventRecord(e->ev0, st));
@@ -782,7 +815,7 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
     CUDA_TRY(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
     CUDA_TRY(cudaEventElapsedTime(&db->bandMs, e->ev0, db->evBand));
     CUDA_TRY(cudaEventElapsedTime(&db->posteriorMs, db->evBand, e->ev1));
-    // retries: capacity overflows (exact counts known), window overflows (next class), scratch
+    // retries: capacity overflows (exact counts known), window overflows (next wider variant), scratch
     for (int round = 0; round < 4; round++) {
         std::vector<int32_t> retry;
         bool changed = false;
@@ -798,11 +831,10 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
             }
             if (o.status & (kTaskCapacity | kTaskWindow | kTaskScratch)) {
                 if (o.status & kTaskWindow) {
-                    int ci = 0;
-                    while (kClasses[ci] != db->cls[t]) ci++;
-                    if (ci + 1 >= kNumClasses)
-                        return failf(MP_ERR_OVERFLOW, "job %d: band wider than the widest slot class", db->tasks[t].job);
-                    db->cls[t] = kClasses[ci + 1];
+                    const int cap = variantCapacity(db->var[t]);
+                    if (cap >= kMaxHullSlots)
+                        return failf(MP_ERR_OVERFLOW, "job %d: band wider than the widest kernel window", db->tasks[t].job);
+                    db->hull[t] = std::max(db->hull[t], cap + 1);
                 }
                 if (o.status & kTaskCapacity) {
                     for (int k = 0; k < 3; k++) {
@@ -839,7 +871,7 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
         // reset statuses of retried tasks (band flags stay valid)
         for (int32_t t : retry) db->hostOut[t].status = 0;
         CUDA_TRY(cudaMemcpyAsync(db->dOut.p, db->hostOut.data(), sizeof(TaskOut) * nTasks, cudaMemcpyHostToDevice, st));
-        buildQueues(db, retry, orderHost);
+        MP_TRY(buildQueues(db, retry, orderHost));
         MP_TRY(upload(db->orders, orderHost.data(), sizeof(int32_t) * std::max<size_t>(orderHost.size(), 1), st));
         CUDA_TRY(cudaEventRecord(e->ev0, st));
         MP_TRY(launchQueues(db));

@@ -65,16 +65,15 @@ struct DpArgs {
     const Task *tasks;
     const int32_t *order;       // task indices in queue order (longest first)
     int32_t nTasks;
-    int32_t scratchBlocks;      // checkpoints available per warp
+    int32_t scratchBlocks;      // checkpoints available per task slot
     int32_t *queue;             // global work counter
     const uint16_t *xs;
     const uint16_t *ys;
     const int2 *band;           // (xmyL, xmyR) per diagonal
     const DevModel *models;     // [0] forward strand, [1] reverse strand
     const float *repeatProb;    // [2][4][51][51] exp(scale*log10 table), per model
-    float4 *scratch;            // per-warp checkpoints
-    int2 *scratchScalars;       // per-warp (exponent, window) per checkpoint
-    float4 *resume;             // per-warp forward state saved across a traceback walk
+    float4 *scratch;            // per task slot: checkpoints [block][window slot]
+    int2 *scratchScalars;       // per task slot: (exponent, window) per checkpoint
     int32_t *outW[3];
     int32_t *outX[3];
     int32_t *outY[3];

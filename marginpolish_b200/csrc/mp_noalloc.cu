@@ -29,7 +29,7 @@
 #include <mutex>
 
 namespace mp {
-cudaError_t launchPosterior(int C, const DpArgs &a, int blocks, int warps, cudaStream_t s);
+cudaError_t launchVariant(int v, const DpArgs &a, int blocks, int warps, cudaStream_t s);
 cudaError_t launchBand(const BandArgs &a, cudaStream_t s);
 }  // namespace mp
 
@@ -38,8 +38,9 @@ using namespace mp;
 namespace {
 
 constexpr int64_t kMaxDiag = MP_NOALLOC_MAX_DIAGONALS;  // anti-diagonals 0..N with N < kMaxDiag
-constexpr int kC = 2;                                      // slot class used (window of 64 slots)
-constexpr int kK = 8;                                      // its checkpoint stride
+constexpr int kVariant = 0;                                // kernel variant used: one task per warp,
+constexpr int kC = 2;                                      // 2 slots per lane (window of 64 slots),
+constexpr int kK = 8;                                      // checkpoint stride 8
 constexpr int64_t kBlocks = kMaxDiag / kK + 2;
 constexpr int64_t kCapM = kMaxDiag + kMaxDiag / 8 + 64;
 constexpr int64_t kCapG = kMaxDiag * 3 / 4 + 64;
@@ -58,8 +59,7 @@ constexpr size_t kOffAnchors = align256(kOffYs + kMaxDiag * sizeof(uint16_t));
 constexpr size_t kOffBand = align256(kOffAnchors + (kMaxDiag / 2 + 1) * 3 * sizeof(int32_t));
 constexpr size_t kOffChk = align256(kOffBand + (kMaxDiag + 1) * sizeof(int4));
 constexpr size_t kOffScal = align256(kOffChk + kBlocks * kC * 32 * sizeof(float4));
-constexpr size_t kOffResume = align256(kOffScal + kBlocks * sizeof(int2));
-constexpr size_t kOffOut = align256(kOffResume + kC * 32 * sizeof(float4));
+constexpr size_t kOffOut = align256(kOffScal + kBlocks * sizeof(int2));
 constexpr size_t kOutListBytes[3] = {kCapM * sizeof(int32_t), kCapG * sizeof(int32_t), kCapG * sizeof(int32_t)};
 constexpr size_t kOffOutList(int k, int field) {  // field 0 weight, 1 x, 2 y
     size_t off = kOffOut;
@@ -178,7 +178,6 @@ extern "C" mp_status mp_realign_single_noalloc(mp_engine *e, const mp_model *m, 
     a.repeatProb = m->repeat.as<float>();
     a.scratch = reinterpret_cast<float4 *>(base + kOffChk);
     a.scratchScalars = reinterpret_cast<int2 *>(base + kOffScal);
-    a.resume = reinterpret_cast<float4 *>(base + kOffResume);
     for (int k = 0; k < 3; k++) {
         a.outW[k] = reinterpret_cast<int32_t *>(base + kOffOutList(k, 0));
         a.outX[k] = reinterpret_cast<int32_t *>(base + kOffOutList(k, 1));
@@ -190,7 +189,7 @@ extern "C" mp_status mp_realign_single_noalloc(mp_engine *e, const mp_model *m, 
     a.traceBackDiagonals = (int32_t) p->traceback_diagonals;
     a.diagonalExpansion = (int32_t) std::min<int64_t>(p->diagonal_expansion, 1 << 29);
     a.sharedRepeat = m->sharedRepeat;
-    NA_TRY(launchPosterior(kC, a, 1, 1, s));
+    NA_TRY(launchVariant(kVariant, a, 1, 1, s));
 
     TaskOut res;
     NA_TRY(cudaMemcpyAsync(&res, dOut, sizeof(res), cudaMemcpyDeviceToHost, s));

@@ -4,30 +4,37 @@
 // posterior pass of MarginPolish (getPosteriorProbsWithBanding,
 // impl/pairwiseAligner.c:687-808, over the split rectangles of :942-991; cell
 // recurrence impl/stateMachine.c:559-581; posterior rules
-// impl/pairwiseAligner.c:586-664), re-designed for one warp per banded
-// sub-problem ("task"), persistent, fed from a length-sorted queue:
+// impl/pairwiseAligner.c:586-664), re-designed for warps that carry G = 32/L
+// banded sub-problems ("tasks"), one per group of L lanes, persistent, fed
+// from a length-sorted queue:
 //
-//  * The cells of anti-diagonal d live in a window of S = 32*C slots, C
-//    consecutive slots per lane; slot i holds x-y = 2(Q+i) + (d&1). The
+//  * The cells of anti-diagonal d of a task live in a window of S = L*C slots,
+//    C consecutive slots per lane; slot i holds x-y = 2(Q+i) + (d&1). The
 //    window origin Q moves only by whole lanes, when the 5-diagonal band hull
-//    leaves it, so the exchange between diagonals is one shuffle per lane.
+//    leaves it, so a diagonal step needs one shuffle per lane.
+//  * The G tasks of a warp (neighbours in the length-sorted queue) run in
+//    lockstep over anti-diagonals: the per-diagonal bookkeeping is issued once
+//    for G tasks and every lane carries C independent cells. A group whose task
+//    has ended is masked by predicates until the warp's longest task ends.
 //  * FP32 probabilities (not logs), in push form: each cell sends its three
-//    outgoing sums (to gap-x, gap-y and match successors); the receiving
-//    cell multiplies by its emission. Emissions are zeroed outside the band,
-//    which also masks every product built on them. Values are rescaled by
-//    exact powers of two every K diagonals and the integer exponents are
-//    tracked per block, so no log / exp is evaluated per cell; the FP64
-//    log-likelihood is ln(mantissa) + exponent*ln2 once per segment.
+//    outgoing sums (to gap-x, gap-y and match successors); the receiving cell
+//    multiplies by its emission. Emissions are zeroed outside the band, which
+//    also masks every product built on them. Values are rescaled by exact
+//    powers of two every K diagonals and the integer exponents are tracked per
+//    block, so no log / exp is evaluated per cell; the FP64 log-likelihood is
+//    ln(mantissa) + exponent*ln2 once per segment.
 //  * The forward sweep stores one float4 per slot every K diagonals (the
-//    checkpoint: outgoing gap sums of d-1 and match sums of d-1, d-2). A
-//    traceback walk (at the end, or at the reference's intermediate traceback
-//    points) recomputes each block of K diagonals into shared memory and runs
-//    the backward recurrence and the posteriors over it, top block first,
+//    checkpoint: outgoing gap sums of d-1 and match sums of d-1, d-2). The
+//    forward values never depend on a traceback, so the reference's traceback
+//    segments (intermediate points of impl/pairwiseAligner.c:722-737, then the
+//    end) are all walked after the sweep, in the reference's order. A walk
+//    recomputes each block of K diagonals into shared memory and runs the
+//    backward recurrence and the posteriors over it, top block first,
 //    prefetching the next block's checkpoint and band records into registers.
-//  * Posterior tuples are ranked in the warp (packed prefix sum) and written
-//    from the top of the task's output region downwards: the region then
-//    reads in the reference's order (ascending anti-diagonal, descending x-y,
-//    later traceback segments first).
+//  * Posterior tuples are ranked within the group (packed prefix sum) and
+//    written from the top of the task's output region downwards: the region
+//    then reads in the reference's order (ascending anti-diagonal, descending
+//    x-y, later traceback segments first).
 #include "mp_internal.h"
 
 #include <algorithm>
@@ -37,9 +44,8 @@ namespace mp {
 
 #define FULL_MASK 0xffffffffu
 
-template <int C>
-struct Geo {
-    static constexpr int S = 32 * C;
+template <int S>
+struct RingSize {
     static constexpr int R = (S + 64 <= 128) ? 128 : ((S + 64 <= 256) ? 256 : 512);
 };
 
@@ -51,16 +57,45 @@ __device__ __forceinline__ int exponentOf(float m) {  // floor(log2 m) for norma
     return ((__float_as_int(m) >> 23) & 0xff) - 127;
 }
 
-__device__ __forceinline__ float warpMax(float v) {
+// Reductions within an aligned group of L lanes.
+template <int L>
+__device__ __forceinline__ float groupMax(float v) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(FULL_MASK, v, o));
+    for (int o = L / 2; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(FULL_MASK, v, o));
     return v;
 }
 
-__device__ __forceinline__ float warpSum(float v) {
+template <int L>
+__device__ __forceinline__ float groupSum(float v) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL_MASK, v, o);
+    for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(FULL_MASK, v, o);
     return v;
+}
+
+__device__ __forceinline__ int warpMaxInt(int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(FULL_MASK, v, o));
+    return v;
+}
+
+// Value held by lane gl+1 of the group (0 past the group's last lane).
+template <int L>
+__device__ __forceinline__ float fromNext(float v, int gl) {
+    const float r = __shfl_down_sync(FULL_MASK, v, 1, L);
+    return gl == L - 1 ? 0.0f : r;
+}
+
+// Value held by lane gl-1 of the group (0 before the group's first lane).
+template <int L>
+__device__ __forceinline__ float fromPrev(float v, int gl) {
+    const float r = __shfl_up_sync(FULL_MASK, v, 1, L);
+    return gl == 0 ? 0.0f : r;
+}
+
+// This group's bits of a warp ballot, shifted down to bit 0.
+template <int L>
+__device__ __forceinline__ unsigned groupBits(unsigned ballot, int g) {
+    return L == 32 ? ballot : (ballot >> (g * L)) & ((1u << L) - 1u);
 }
 
 __device__ __forceinline__ void cpAsync16(void *smem, const void *gmem) {
@@ -77,11 +112,12 @@ __device__ __forceinline__ void cpAsyncWaitAllButOne() {
 }
 
 // ---------------------------------------------------------------------------
-// Task context (uniform over the warp)
+// Task context (identical over the lanes of a group)
 // ---------------------------------------------------------------------------
 
 struct Ctx {
-    int lane;
+    int gl;                 // lane within the group
+    int g;                  // group within the warp
     int lx, ly, N;
     const uint16_t *xs;
     const uint16_t *ys;
@@ -96,6 +132,8 @@ struct Ctx {
 };
 
 // Decoded symbols: packed (repeat-table byte offset | match-table byte offset << 17) and gap emission.
+// Positions outside the sequence decode to 'N' with repeat count 0, so every ring entry is a valid
+// table offset.
 __device__ __forceinline__ uint2 decodeX(const Ctx &c, int pos, int &bad) {
     int b = 4, rc = 0;
     if (pos >= 0 && pos < c.lx) {
@@ -137,7 +175,7 @@ __device__ __forceinline__ float matchEmission(const Ctx &c, uint32_t xpk, uint3
     return r * m;
 }
 
-// Decoded symbols of a span of positions in shared memory (one ring per sequence).
+// Decoded symbols of a span of positions in shared memory (one ring per sequence and group).
 template <int R>
 struct Ring {
     uint2 *buf;
@@ -145,31 +183,32 @@ struct Ring {
     int bad;
 };
 
-// Decodes positions [newLo, newLo+R) into the ring; returns 1 if a symbol was out of range.
-template <int R, bool IS_X>
-__device__ __noinline__ int ringFillRaw(Ctx c, uint2 *buf, int newLo) {
+// Decodes positions [newLo, newLo+R) into the group's ring where `doFill`; returns 1 if a
+// symbol of this group's fill was out of range. Called by every lane of the warp.
+template <int R, int L, bool IS_X>
+__device__ __noinline__ int ringFillRaw(Ctx c, uint2 *buf, int newLo, int doFill) {
     int bad = 0;
+    if (doFill) {
 #pragma unroll 4
-    for (int k = 0; k < R / 32; k++) {
-        int p = newLo + k * 32 + c.lane;
-        buf[p & (R - 1)] = IS_X ? decodeX(c, p, bad) : decodeY(c, p, bad);
+        for (int k = 0; k < R / L; k++) {
+            int p = newLo + k * L + c.gl;
+            buf[p & (R - 1)] = IS_X ? decodeX(c, p, bad) : decodeY(c, p, bad);
+        }
     }
-    bad = __any_sync(FULL_MASK, bad) ? 1 : 0;
+    const unsigned b = __ballot_sync(FULL_MASK, bad);
     __syncwarp();
-    return bad;
+    return groupBits<L>(b, c.g) ? 1 : 0;
 }
 
-template <int R, bool IS_X>
-__device__ __forceinline__ void ringFill(const Ctx &c, Ring<R> &r, int newLo) {
-    r.lo = newLo;
-    r.bad |= ringFillRaw<R, IS_X>(c, r.buf, newLo);
-}
-
-template <int R, bool IS_X>
-__device__ __forceinline__ void ringEnsure(const Ctx &c, Ring<R> &r, int needLo, int needHi, bool up) {
-    if (needLo < r.lo || needHi >= r.lo + R) {
-        int slack = R - (needHi - needLo + 1);
-        ringFill<R, IS_X>(c, r, up ? needLo - slack / 8 : needLo - (slack - slack / 8));
+// Makes positions [needLo, needHi] resident for the groups where `active`.
+template <int R, int L, bool IS_X>
+__device__ __forceinline__ void ringEnsure(const Ctx &c, Ring<R> &r, int needLo, int needHi, bool up, bool active) {
+    const bool need = active && (needLo < r.lo || needHi >= r.lo + R);
+    if (__any_sync(FULL_MASK, need)) {
+        const int slack = R - (needHi - needLo + 1);
+        const int newLo = up ? needLo - slack / 8 : needLo - (slack - slack / 8);
+        r.bad |= ringFillRaw<R, L, IS_X>(c, r.buf, newLo, need ? 1 : 0);
+        if (need) r.lo = newLo;
     }
 }
 
@@ -187,14 +226,13 @@ __device__ __forceinline__ int slotX0(int d, int Q) {
 }
 
 template <int C, int R>
-__device__ __forceinline__ void loadSlots(const Ctx &c, const Ring<R> &rx, const Ring<R> &ry, int d, int Q,
-                                          Slots<C> &s) {
-    int x0 = slotX0(d, Q), y0 = d - x0;
+__device__ __forceinline__ void loadSlots(int gl, const Ring<R> &rx, const Ring<R> &ry, int d, int Q, Slots<C> &s) {
+    const int x0 = slotX0(d, Q), y0 = d - x0;
 #pragma unroll
     for (int j = 0; j < C; j++) {
-        int i = c.lane * C + j;
-        uint2 vx = rx.buf[(x0 + i - 1) & (R - 1)];
-        uint2 vy = ry.buf[(y0 - i - 1) & (R - 1)];
+        const int i = gl * C + j;
+        const uint2 vx = rx.buf[(x0 + i - 1) & (R - 1)];
+        const uint2 vy = ry.buf[(y0 - i - 1) & (R - 1)];
         s.xpk[j] = vx.x;
         s.ex[j] = __uint_as_float(vx.y);
         s.ypk[j] = vy.x;
@@ -204,15 +242,14 @@ __device__ __forceinline__ void loadSlots(const Ctx &c, const Ring<R> &rx, const
 
 // Slot symbols from diagonal d-1 to d (window unchanged): entering odd d the x of
 // every slot grows by one, entering even d the y of every slot grows by one.
-template <int C, int R, int PAR>
-__device__ __forceinline__ void stepSlots(const Ctx &c, const Ring<R> &rx, const Ring<R> &ry, int d, int Q,
-                                          Slots<C> &s) {
-    constexpr int S = 32 * C;
+template <int C, int L, int R, int PAR>
+__device__ __forceinline__ void stepSlots(int gl, const Ring<R> &rx, const Ring<R> &ry, int d, int Q, Slots<C> &s) {
+    constexpr int S = L * C;
     if (PAR) {
-        uint2 fresh = rx.buf[(slotX0(d, Q) + S - 2) & (R - 1)];
-        uint32_t npk = __shfl_down_sync(FULL_MASK, s.xpk[0], 1);
-        float ne = __shfl_down_sync(FULL_MASK, s.ex[0], 1);
-        if (c.lane == 31) {
+        const uint2 fresh = rx.buf[(slotX0(d, Q) + S - 2) & (R - 1)];
+        uint32_t npk = __shfl_down_sync(FULL_MASK, s.xpk[0], 1, L);
+        float ne = __shfl_down_sync(FULL_MASK, s.ex[0], 1, L);
+        if (gl == L - 1) {
             npk = fresh.x;
             ne = __uint_as_float(fresh.y);
         }
@@ -224,10 +261,10 @@ __device__ __forceinline__ void stepSlots(const Ctx &c, const Ring<R> &rx, const
         s.xpk[C - 1] = npk;
         s.ex[C - 1] = ne;
     } else {
-        uint2 fresh = ry.buf[(d - slotX0(d, Q) - 1) & (R - 1)];
-        uint32_t npk = __shfl_up_sync(FULL_MASK, s.ypk[C - 1], 1);
-        float ne = __shfl_up_sync(FULL_MASK, s.ey[C - 1], 1);
-        if (c.lane == 0) {
+        const uint2 fresh = ry.buf[(d - slotX0(d, Q) - 1) & (R - 1)];
+        uint32_t npk = __shfl_up_sync(FULL_MASK, s.ypk[C - 1], 1, L);
+        float ne = __shfl_up_sync(FULL_MASK, s.ey[C - 1], 1, L);
+        if (gl == 0) {
             npk = fresh.x;
             ne = __uint_as_float(fresh.y);
         }
@@ -248,78 +285,74 @@ struct Fwd {
     float ox[C], oy[C], mA[C], mB[C];
 };
 
-// New lane l takes old lane l+dl (values leaving the warp become zero).
-template <int C>
-__device__ __forceinline__ void laneShift(float (&v)[C], int dl, int lane) {
-    int src = lane + dl;
-    bool ok = src >= 0 && src < 32;
+// New lane gl takes old lane gl+dl of the group (values leaving the group become zero).
+template <int C, int L>
+__device__ __forceinline__ void laneShift(float (&v)[C], int dl, int gl) {
+    const int src = gl + dl;
+    const bool ok = src >= 0 && src < L;
 #pragma unroll
     for (int j = 0; j < C; j++) {
-        float w = __shfl_sync(FULL_MASK, v[j], src & 31);
+        const float w = __shfl_sync(FULL_MASK, v[j], src & (L - 1), L);
         v[j] = ok ? w : 0.0f;
     }
 }
 
-template <int C>
-__device__ __forceinline__ void shiftFwd(Fwd<C> &f, int dl, int lane) {
-    laneShift<C>(f.ox, dl, lane);
-    laneShift<C>(f.oy, dl, lane);
-    laneShift<C>(f.mA, dl, lane);
-    laneShift<C>(f.mB, dl, lane);
+template <int C, int L>
+__device__ __forceinline__ void shiftFwd(Fwd<C> &f, int dl, int gl) {
+    laneShift<C, L>(f.ox, dl, gl);
+    laneShift<C, L>(f.oy, dl, gl);
+    laneShift<C, L>(f.mA, dl, gl);
+    laneShift<C, L>(f.mB, dl, gl);
 }
 
 // The window must contain the hull of the bands of d-2..d+2; returns the lane
 // shift (new Q = Q + C*shift). Shared by the sweep and the recompute, so both
-// take the same decisions. Sets *bad when the hull does not fit the class.
-template <int C>
+// take the same decisions. Sets `bad` when the hull does not fit the window.
+template <int C, int S>
 __device__ __forceinline__ int windowShift(int Q, int hullLo, int hullHi, bool &bad) {
-    constexpr int S = 32 * C;
-    int needLo = hullLo >> 1, needHi = hullHi >> 1;
+    const int needLo = hullLo >> 1, needHi = hullHi >> 1;
     if (needLo >= Q && needHi <= Q + S - 1) return 0;
-    int span = needHi - needLo + 1;
+    const int span = needHi - needLo + 1;
     if (span > S - 2 * C) {
         bad = true;
         return 0;
     }
-    int diff = needLo - (S - span) / 2 - Q;
+    const int diff = needLo - (S - span) / 2 - Q;
     int dl = diff >= 0 ? diff / C : -((-diff + C - 1) / C);
     if (Q + C * dl + S - 1 < needHi) dl++;
     if (Q + C * dl > needLo) bad = true;
     return dl;
 }
 
-template <int C>
+template <int S>
 __device__ __forceinline__ int initialWindow(int hullLo, int hullHi) {
-    constexpr int S = 32 * C;
-    int needLo = hullLo >> 1, needHi = hullHi >> 1;
+    const int needLo = hullLo >> 1, needHi = hullHi >> 1;
     return needLo - (S - (needHi - needLo + 1)) / 2;
 }
 
 // One forward anti-diagonal (PAR = d & 1). Emissions are zeroed outside the band
 // [sLo, sHi], which zeroes the cell. With CACHE, the cell values and the masked
-// emissions are written to the block cache (slot-major, lane-minor).
-template <int C, int PAR, bool CACHE>
+// emissions are written to the block cache at [j][gl].
+template <int C, int L, int PAR, bool CACHE>
 __device__ __forceinline__ void forwardDiagonal(const Ctx &c, Fwd<C> &st, const Slots<C> &sy, int sLo, int sHi,
                                                 float4 *cacheA, float2 *cacheB) {
     float inX[C], inY[C];
     if (PAR) {  // odd d: gap-x source slot i, gap-y source slot i+1
-        float nb = __shfl_down_sync(FULL_MASK, st.oy[0], 1);
-        if (c.lane == 31) nb = 0.0f;
+        const float nb = fromNext<L>(st.oy[0], c.gl);
 #pragma unroll
         for (int j = 0; j < C; j++) {
             inX[j] = st.ox[j];
             inY[j] = (j < C - 1) ? st.oy[j + 1] : nb;
         }
     } else {  // even d: gap-x source slot i-1, gap-y source slot i
-        float nb = __shfl_up_sync(FULL_MASK, st.ox[C - 1], 1);
-        if (c.lane == 0) nb = 0.0f;
+        const float nb = fromPrev<L>(st.ox[C - 1], c.gl);
 #pragma unroll
         for (int j = 0; j < C; j++) {
             inX[j] = (j > 0) ? st.ox[j - 1] : nb;
             inY[j] = st.oy[j];
         }
     }
-    const int base = c.lane * C - sLo;
+    const int base = c.gl * C - sLo;
     const unsigned span = (unsigned) (sHi - sLo);
 #pragma unroll
     for (int j = 0; j < C; j++) {
@@ -337,19 +370,19 @@ __device__ __forceinline__ void forwardDiagonal(const Ctx &c, Fwd<C> &st, const 
         st.ox[j] = nx;
         st.oy[j] = ny;
         if (CACHE) {
-            cacheA[j * 32 + c.lane] = make_float4(fM, fX, fY, eM);
-            cacheB[j * 32 + c.lane] = make_float2(eX, eY);
+            cacheA[j * L + c.gl] = make_float4(fM, fX, fY, eM);
+            cacheB[j * L + c.gl] = make_float2(eX, eY);
         }
     }
 }
 
 // Diagonal 0: the start cell (x-y = 0) holds the start (or ragged-start) probabilities.
-template <int C, bool CACHE>
+template <int C, int L, bool CACHE>
 __device__ __forceinline__ void forwardOrigin(const Ctx &c, const float *startP, int Q, Fwd<C> &st, float4 *cacheA,
                                               float2 *cacheB) {
 #pragma unroll
     for (int j = 0; j < C; j++) {
-        const bool here = c.lane * C + j == -Q;
+        const bool here = c.gl * C + j == -Q;
         const float fM = here ? startP[0] : 0.0f;
         const float fX = here ? startP[1] : 0.0f;
         const float fY = here ? startP[2] : 0.0f;
@@ -358,18 +391,19 @@ __device__ __forceinline__ void forwardOrigin(const Ctx &c, const float *startP,
         st.oy[j] = __fmaf_rn(c.t[1 * 3 + 2], fX, __fmaf_rn(c.t[2 * 3 + 2], fY, c.t[0 * 3 + 2] * fM));
         st.mB[j] = 0.0f;
         if (CACHE) {
-            cacheA[j * 32 + c.lane] = make_float4(fM, fX, fY, 0.0f);
-            cacheB[j * 32 + c.lane] = make_float2(0.0f, 0.0f);
+            cacheA[j * L + c.gl] = make_float4(fM, fX, fY, 0.0f);
+            cacheB[j * L + c.gl] = make_float2(0.0f, 0.0f);
         }
     }
 }
 
-template <int C>
+// Rescales the carried forward state by a power of two; returns the exponent removed.
+template <int C, int L>
 __device__ __forceinline__ int rescaleFwd(Fwd<C> &st) {
     float m = 0.0f;
 #pragma unroll
     for (int j = 0; j < C; j++) m = fmaxf(m, fmaxf(fmaxf(st.ox[j], st.oy[j]), fmaxf(st.mA[j], st.mB[j])));
-    m = warpMax(m);
+    m = groupMax<L>(m);
     if (!(m > 0.0f)) return 0;
     const int k = exponentOf(m);
     const float sc = pow2f(-k);
@@ -384,7 +418,7 @@ __device__ __forceinline__ int rescaleFwd(Fwd<C> &st) {
 }
 
 // ---------------------------------------------------------------------------
-// Output: ordered warp compaction of one diagonal's tuples.
+// Output: ordered group compaction of one diagonal's tuples.
 // ---------------------------------------------------------------------------
 
 struct Out {
@@ -396,77 +430,70 @@ struct Out {
     int xShift, yShift;
 };
 
-template <int C>
-__device__ __forceinline__ void emitDiagonal(int lane, Out &o, const float (&p)[3][C], float thr, int x0, int d) {
-    uint32_t mask = 0;  // bit k*C+j: list k, slot j
+// Called by every lane of the warp; groups with `active` false emit nothing. The
+// (list, slot) pairs are unrolled at compile time, so each tuple is written through a
+// fixed list pointer and the warp skips a pair no lane holds.
+template <int C, int L>
+__device__ __forceinline__ void emitDiagonal(int gl, Out &o, const float (&p)[3][C], float thr, int x0, int d,
+                                             bool active) {
+    uint32_t m[3];  // bit j: slot j of list k passes the threshold
 #pragma unroll
     for (int k = 0; k < 3; k++) {
+        m[k] = 0;
 #pragma unroll
-        for (int j = 0; j < C; j++) mask |= (p[k][j] >= thr ? 1u : 0u) << (k * C + j);
+        for (int j = 0; j < C; j++) m[k] |= (p[k][j] >= thr ? 1u : 0u) << j;
+        m[k] = active ? m[k] : 0u;
     }
-    if (__ballot_sync(FULL_MASK, mask != 0) == 0) return;
-    constexpr uint32_t listBits = (1u << C) - 1u;
-    const uint32_t cnt = (uint32_t) __popc(mask & listBits) | ((uint32_t) __popc(mask & (listBits << C)) << 10) |
-                         ((uint32_t) __popc(mask & (listBits << (2 * C))) << 20);
+    if (__ballot_sync(FULL_MASK, (m[0] | m[1] | m[2]) != 0) == 0) return;
+    const uint32_t cnt = (uint32_t) __popc(m[0]) | ((uint32_t) __popc(m[1]) << 10) | ((uint32_t) __popc(m[2]) << 20);
     uint32_t incl = cnt;
 #pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        uint32_t v = __shfl_up_sync(FULL_MASK, incl, off);
-        if (lane >= off) incl += v;
+    for (int off = 1; off < L; off <<= 1) {
+        const uint32_t v = __shfl_up_sync(FULL_MASK, incl, off, L);
+        if (gl >= off) incl += v;
     }
-    const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
-    uint32_t rank = incl - cnt;  // packed exclusive ranks, advanced as this lane writes
-    while (mask) {
-        const int bit = __ffs(mask) - 1;
-        mask &= mask - 1;
-        const int k = bit / C, j = bit - k * C;
-        const int r = o.written[k] + (int) ((rank >> (10 * k)) & 1023u);
-        rank += 1u << (10 * k);
-        const int pos = o.top[k] - 1 - r;
-        if (pos >= 0) {
-            const int x = x0 + lane * C + j;
-            float v = 0.0f;
+    const uint32_t total = __shfl_sync(FULL_MASK, incl, L - 1, L);
+    const uint32_t excl = incl - cnt;  // packed ranks of this lane's first tuple in each list
+    const int xl = x0 + gl * C;
 #pragma unroll
-            for (int kk = 0; kk < 3; kk++) {
+    for (int k = 0; k < 3; k++) {
+        int pos = o.top[k] - 1 - o.written[k] - (int) ((excl >> (10 * k)) & 1023u);
 #pragma unroll
-                for (int jj = 0; jj < C; jj++) v = bit == kk * C + jj ? p[kk][jj] : v;
+        for (int j = 0; j < C; j++) {
+            if (m[k] & (1u << j)) {
+                if (pos >= 0) {
+                    const int x = xl + j;
+                    o.w[k][pos] = (int32_t) floorf(fminf(p[k][j], 1.0f) * (float) kProbOne);
+                    o.x[k][pos] = x - 1 + o.xShift;
+                    o.y[k][pos] = d - x - 1 + o.yShift;
+                }
+                pos--;
             }
-            v = fminf(v, 1.0f);
-            o.w[k][pos] = (int32_t) floorf(v * (float) kProbOne);
-            o.x[k][pos] = x - 1 + o.xShift;
-            o.y[k][pos] = d - x - 1 + o.yShift;
         }
+        o.written[k] += (int) ((total >> (10 * k)) & 1023u);
     }
-#pragma unroll
-    for (int k = 0; k < 3; k++) o.written[k] += (int) ((total >> (10 * k)) & 1023u);
 }
 
 // ---------------------------------------------------------------------------
-// Per-warp shared workspace
+// Shared workspace of one group
 // ---------------------------------------------------------------------------
 
-template <int C, int K>
-struct WarpSmem {
-    static constexpr int R = Geo<C>::R;
+template <int C, int L, int K>
+struct GroupSmem {
+    static constexpr int S = L * C;
+    static constexpr int R = RingSize<S>::R;
     static constexpr size_t ringBytes = 2 * R * sizeof(uint2);
     static constexpr size_t bandRingBytes = 64 * sizeof(int4);
     static constexpr size_t walkBandBytes = K * sizeof(int4);
-    static constexpr size_t cacheABytes = (size_t) K * C * 32 * sizeof(float4);
-    static constexpr size_t cacheBBytes = (size_t) K * C * 32 * sizeof(float2);
+    static constexpr size_t cacheABytes = (size_t) K * S * sizeof(float4);
+    static constexpr size_t cacheBBytes = (size_t) K * S * sizeof(float2);
     static constexpr size_t infoBytes = K * sizeof(int2);
     static constexpr size_t bytes = ringBytes + bandRingBytes + walkBandBytes + cacheABytes + cacheBBytes + infoBytes;
 };
 
-struct Scratch {
-    float4 *chk;      // checkpoints of this warp: [block][C][32]
-    int2 *scal;       // (exponent, window) per checkpoint
-    float4 *resume;   // sweep state across an intermediate walk
-    int blocks;
-};
-
-template <int C, int K>
-struct WarpMem {
-    Ring<Geo<C>::R> rx, ry;
+template <int C, int L, int K>
+struct GroupMem {
+    Ring<RingSize<L * C>::R> rx, ry;
     int4 *bandRing;
     int4 *walkBand;
     float4 *cacheA;
@@ -474,10 +501,16 @@ struct WarpMem {
     int2 *info;
 };
 
-template <int C>
-__device__ __forceinline__ void storeFwd(float4 *p, int lane, const Fwd<C> &st) {
+struct Scratch {
+    float4 *chk;      // checkpoints of the group's task: [block][C][L]
+    int2 *scal;       // (exponent, window) per checkpoint
+    int blocks;
+};
+
+template <int C, int L>
+__device__ __forceinline__ void storeFwd(float4 *p, int gl, const Fwd<C> &st) {
 #pragma unroll
-    for (int j = 0; j < C; j++) p[j * 32 + lane] = make_float4(st.ox[j], st.oy[j], st.mA[j], st.mB[j]);
+    for (int j = 0; j < C; j++) p[j * L + gl] = make_float4(st.ox[j], st.oy[j], st.mA[j], st.mB[j]);
 }
 
 template <int C>
@@ -492,208 +525,222 @@ __device__ __forceinline__ void loadFwd(const float4 (&v)[C], Fwd<C> &st) {
 }
 
 // ---------------------------------------------------------------------------
-// Traceback walk over (tbTo, D]: recompute each block of K diagonals into the
-// shared cache, then the backward recurrence and posteriors over it.
+// Traceback walk over (tbTo, D] of every active group's task, in lockstep:
+// iteration w processes block D/K - w of each group; every block is recomputed
+// into the shared cache, then the backward recurrence and posteriors run over it.
+// Block starts are multiples of K (even), so the parity of a block position is
+// the same in every group.
 // ---------------------------------------------------------------------------
 
-struct WalkArgs {
-    int D, tbTo, tbFrom, atEnd;
+struct Walk {
+    int D, tbTo, tbFrom, atEnd, active;
     const float *startP;
     const float *endP;
-    float thr;
 };
 
-template <int C, int K>
-__device__ __forceinline__ void walkSegment(const Ctx &c, WarpMem<C, K> &wm, const Scratch &sc, const WalkArgs &wa,
-                                            Out &o, double &logLik, bool &bad) {
-    constexpr int S = 32 * C;
-    constexpr int R = Geo<C>::R;
-    const int lane = c.lane;
-    int untilRefresh = 0;
+template <int C, int L, int K>
+__device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm, const Scratch &sc, const Walk &wk,
+                                            float thr, Out &o, double &logLik, bool &bad) {
+    static_assert(K <= L && (K % 2) == 0, "band records of a block are held one per lane");
+    constexpr int S = L * C;
+    constexpr int R = RingSize<S>::R;
+    const int gl = c.gl;
     float gX[C], gY[C], gA[C], gB[C];  // backward u-values: gap-x / gap-y of d+1, match (even d in A, odd in B)
 #pragma unroll
     for (int j = 0; j < C; j++) gX[j] = gY[j] = gA[j] = gB[j] = 0.0f;
-    int Eb = 0, posts = 0, ET = 0;
+    int Eb = 0, posts = 0, ET = 0, untilRefresh = 0;
     float Tm = 0.0f;
-    const int D = wa.D;
-    const int bTop = D / K, bBot = (wa.tbTo + 1) / K;
+    const float endM = wk.endP[0], endX = wk.endP[1], endY = wk.endP[2];
+    const int bTop = wk.active ? wk.D / K : -1;
+    const int bBot = wk.active ? (wk.tbTo + 1) / K : 0;
+    const int nIter = warpMaxInt(wk.active ? bTop - bBot + 1 : 0);
 
     // register prefetch of a block's checkpoint and band records
     float4 pchk[C];
+#pragma unroll
+    for (int j = 0; j < C; j++) pchk[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     int2 pscal = make_int2(0, 0);
     int4 pband = make_int4(0, 0, 0, 0);
-    auto prefetch = [&](int b) {
-        if (b > 0) {
+    auto prefetch = [&](int b, bool ok) {
+        if (ok && b > 0) {
 #pragma unroll
-            for (int j = 0; j < C; j++) pchk[j] = sc.chk[((size_t) b * C + j) * 32 + lane];
+            for (int j = 0; j < C; j++) pchk[j] = sc.chk[((size_t) b * C + j) * L + gl];
             pscal = sc.scal[b];
         }
-        const int dd = b * K + lane;
-        if (lane < K && dd <= c.N) pband = c.band[dd];
+        const int dd = b * K + gl;
+        if (ok && gl < K && dd <= c.N) pband = c.band[dd];
     };
-    prefetch(bTop);
+    prefetch(bTop, bTop >= bBot);
 
-    for (int b = bTop; b >= bBot; b--) {
+    for (int w = 0; w < nIter; w++) {
+        const int b = bTop - w;
+        const bool blockOn = b >= bBot;
         const int dStart = b * K;
-        const int dEnd = min(dStart + K - 1, D);
+        const int dEnd = min(dStart + K - 1, wk.D);
         Fwd<C> rs;
         float4 cchk[C];
 #pragma unroll
         for (int j = 0; j < C; j++) cchk[j] = pchk[j];
         const int2 cscal = pscal;
-        if (lane < K) wm.walkBand[lane] = pband;
+        if (blockOn && gl < K) gm.walkBand[gl] = pband;
         __syncwarp();
-        if (b > bBot) prefetch(b - 1);
+        prefetch(b - 1, blockOn && b - 1 >= bBot);
 
         // ---------------- recompute the block ----------------
-        int Q, Ef;
+        int Q;
+        int Ef;
         float chkSM[C];
-        if (b == 0) {
-            const int4 b0 = wm.walkBand[0];
-            Q = initialWindow<C>(b0.z, b0.w);
+        loadFwd<C>(cchk, rs);
+        Ef = cscal.x;
+        Q = cscal.y;
+#pragma unroll
+        for (int j = 0; j < C; j++) chkSM[j] = rs.mB[j];
+        if (blockOn && b == 0) {
+            const int4 b0 = gm.walkBand[0];
+            Q = initialWindow<S>(b0.z, b0.w);
             Ef = 0;
 #pragma unroll
             for (int j = 0; j < C; j++) chkSM[j] = 0.0f;
-        } else {
-            loadFwd<C>(cchk, rs);
-            Ef = cscal.x;
-            Q = cscal.y;
-#pragma unroll
-            for (int j = 0; j < C; j++) chkSM[j] = rs.mB[j];
         }
         Slots<C> sy;
         bool have = false;
-        for (int k = 0; k <= dEnd - dStart; k++) {
-            const int d = dStart + k;
-            const int4 bd = wm.walkBand[k];
-            int dl = 0;
-            if (d == 0) {
-                int x0 = slotX0(0, Q);
-                ringEnsure<R, true>(c, wm.rx, x0 - 1, x0 + S - 2, false);
-                ringEnsure<R, false>(c, wm.ry, -x0 - S, -x0 - 1, false);
-                loadSlots<C, R>(c, wm.rx, wm.ry, 0, Q, sy);
-                have = true;
-                forwardOrigin<C, true>(c, wa.startP, Q, rs, wm.cacheA, wm.cacheB);
-            } else {
-                dl = windowShift<C>(Q, bd.z, bd.w, bad);
-                if (dl != 0) {
-                    shiftFwd<C>(rs, dl, lane);
-                    Q += C * dl;
-                    have = false;
+#pragma unroll 1
+        for (int k = 0; k < K; k += 2) {
+#pragma unroll
+            for (int par = 0; par < 2; par++) {
+                const int kk = k + par;
+                const int d = dStart + kk;
+                const bool on = blockOn && d <= dEnd;
+                const int4 bd = gm.walkBand[kk];
+                const int dl = (on && d > 0) ? windowShift<C, S>(Q, bd.z, bd.w, bad) : 0;
+                if (__any_sync(FULL_MASK, dl != 0)) {
+                    shiftFwd<C, L>(rs, dl, gl);
+                    if (dl != 0) {
+                        Q += C * dl;
+                        have = false;
+                    }
                 }
                 const int x0 = slotX0(d, Q), y0 = d - x0;
-                ringEnsure<R, true>(c, wm.rx, x0 - 1, x0 + S - 2, false);
-                ringEnsure<R, false>(c, wm.ry, y0 - S, y0 - 1, false);
+                ringEnsure<R, L, true>(c, gm.rx, x0 - 1, x0 + S - 2, false, on);
+                ringEnsure<R, L, false>(c, gm.ry, y0 - S, y0 - 1, false, on);
                 const int sLo = (bd.x >> 1) - Q, sHi = (bd.y >> 1) - Q;
-                float4 *ca = wm.cacheA + (size_t) k * C * 32;
-                float2 *cb = wm.cacheB + (size_t) k * C * 32;
-                if (d & 1) {
-                    if (have) stepSlots<C, R, 1>(c, wm.rx, wm.ry, d, Q, sy); else loadSlots<C, R>(c, wm.rx, wm.ry, d, Q, sy);
-                    forwardDiagonal<C, 1, true>(c, rs, sy, sLo, sHi, ca, cb);
+                float4 *ca = gm.cacheA + (size_t) kk * S;
+                float2 *cb = gm.cacheB + (size_t) kk * S;
+                if (par) {
+                    stepSlots<C, L, R, 1>(gl, gm.rx, gm.ry, d, Q, sy);
+                    if (!have) loadSlots<C, R>(gl, gm.rx, gm.ry, d, Q, sy);
+                    forwardDiagonal<C, L, 1, true>(c, rs, sy, sLo, sHi, ca, cb);
                 } else {
-                    if (have) stepSlots<C, R, 0>(c, wm.rx, wm.ry, d, Q, sy); else loadSlots<C, R>(c, wm.rx, wm.ry, d, Q, sy);
-                    forwardDiagonal<C, 0, true>(c, rs, sy, sLo, sHi, ca, cb);
+                    stepSlots<C, L, R, 0>(gl, gm.rx, gm.ry, d, Q, sy);
+                    if (!have) loadSlots<C, R>(gl, gm.rx, gm.ry, d, Q, sy);
+                    forwardDiagonal<C, L, 0, true>(c, rs, sy, sLo, sHi, ca, cb);
+                    if (d == 0) forwardOrigin<C, L, true>(c, wk.startP, Q, rs, ca, cb);
                 }
                 have = true;
+                if (gl == 0) gm.info[kk] = make_int2(Q, dl);
             }
-            if (lane == 0) wm.info[k] = make_int2(Q, dl);
         }
         __syncwarp();
-        if (bad) break;
 
         // ---------------- backward over the block ----------------
-        const int kLow = max(dStart, wa.tbTo + 1) - dStart;
-        for (int k = dEnd - dStart; k >= kLow; k--) {
-            const int d = dStart + k;
-            const int2 inf = wm.info[k];
-            const float4 *ca = wm.cacheA + (size_t) k * C * 32;
-            const float2 *cb = wm.cacheB + (size_t) k * C * 32;
-            float4 f[C];
-            float2 e[C];
+#pragma unroll 1
+        for (int k = K - 2; k >= 0; k -= 2) {
 #pragma unroll
-            for (int j = 0; j < C; j++) {
-                f[j] = ca[j * 32 + lane];
-                e[j] = cb[j * 32 + lane];
-            }
-            float bM[C], bX[C], bY[C];
-            if (d == D) {
+            for (int par = 1; par >= 0; par--) {
+                const int kk = k + par;
+                const int d = dStart + kk;
+                const bool on = blockOn && d <= dEnd && d > wk.tbTo;
+                const int2 inf = gm.info[kk];
+                const float4 *ca = gm.cacheA + (size_t) kk * S;
+                const float2 *cb = gm.cacheB + (size_t) kk * S;
+                float4 f[C];
+                float2 e[C];
 #pragma unroll
                 for (int j = 0; j < C; j++) {
-                    bM[j] = wa.endP[0];
-                    bX[j] = wa.endP[1];
-                    bY[j] = wa.endP[2];
+                    f[j] = ca[j * L + gl];
+                    e[j] = cb[j * L + gl];
                 }
-            } else {
-                float sX[C], sY[C];
-                if (d & 1) {
-                    float nb = __shfl_down_sync(FULL_MASK, gX[0], 1);
-                    if (lane == 31) nb = 0.0f;
-#pragma unroll
-                    for (int j = 0; j < C; j++) {
-                        sX[j] = (j < C - 1) ? gX[j + 1] : nb;
-                        sY[j] = gY[j];
-                    }
-                } else {
-                    float nb = __shfl_up_sync(FULL_MASK, gY[C - 1], 1);
-                    if (lane == 0) nb = 0.0f;
-#pragma unroll
-                    for (int j = 0; j < C; j++) {
-                        sX[j] = gX[j];
-                        sY[j] = (j > 0) ? gY[j - 1] : nb;
-                    }
-                }
-#pragma unroll
-                for (int j = 0; j < C; j++) {
-                    const float s2 = (d & 1) ? gB[j] : gA[j];
-                    bM[j] = __fmaf_rn(c.t[0 * 3 + 0], s2, __fmaf_rn(c.t[0 * 3 + 2], sY[j], c.t[0 * 3 + 1] * sX[j]));
-                    bX[j] = __fmaf_rn(c.t[1 * 3 + 0], s2, __fmaf_rn(c.t[1 * 3 + 2], sY[j], c.t[1 * 3 + 1] * sX[j]));
-                    bY[j] = __fmaf_rn(c.t[2 * 3 + 0], s2, __fmaf_rn(c.t[2 * 3 + 2], sY[j], c.t[2 * 3 + 1] * sX[j]));
-                }
-            }
-            if (d <= wa.tbFrom) {
-                if (untilRefresh == 0) {
-                    untilRefresh = 10;
-                    // total: cells of d plus the match transitions crossing d (impl/pairwiseAligner.c:567-584)
-                    float sM1[C];
-                    if (k > 0) {
-                        const float4 *cp = wm.cacheA + (size_t) (k - 1) * C * 32;
+                float bM[C], bX[C], bY[C];
+                {
+                    float sX[C], sY[C];
+                    if (par) {  // odd d: gap-x successor slot i+1, gap-y successor slot i
+                        const float nb = fromNext<L>(gX[0], gl);
 #pragma unroll
                         for (int j = 0; j < C; j++) {
-                            const float4 q = cp[j * 32 + lane];
+                            sX[j] = (j < C - 1) ? gX[j + 1] : nb;
+                            sY[j] = gY[j];
+                        }
+                    } else {  // even d: gap-x successor slot i, gap-y successor slot i-1
+                        const float nb = fromPrev<L>(gY[C - 1], gl);
+#pragma unroll
+                        for (int j = 0; j < C; j++) {
+                            sX[j] = gX[j];
+                            sY[j] = (j > 0) ? gY[j - 1] : nb;
+                        }
+                    }
+                    const bool top = d == wk.D;  // the walk's first diagonal holds the end probabilities
+#pragma unroll
+                    for (int j = 0; j < C; j++) {
+                        const float s2 = par ? gB[j] : gA[j];
+                        const float m_ = __fmaf_rn(c.t[0 * 3 + 0], s2, __fmaf_rn(c.t[0 * 3 + 2], sY[j], c.t[0 * 3 + 1] * sX[j]));
+                        const float x_ = __fmaf_rn(c.t[1 * 3 + 0], s2, __fmaf_rn(c.t[1 * 3 + 2], sY[j], c.t[1 * 3 + 1] * sX[j]));
+                        const float y_ = __fmaf_rn(c.t[2 * 3 + 0], s2, __fmaf_rn(c.t[2 * 3 + 2], sY[j], c.t[2 * 3 + 1] * sX[j]));
+                        bM[j] = top ? endM : m_;
+                        bX[j] = top ? endX : x_;
+                        bY[j] = top ? endY : y_;
+                    }
+                }
+                const bool post = on && d <= wk.tbFrom;
+                // total probability refresh: 1st, 11th, 21st ... posterior diagonal of the walk
+                const bool refresh = post && untilRefresh == 0;
+                if (__any_sync(FULL_MASK, refresh)) {
+                    // cells of d plus the match transitions crossing d (impl/pairwiseAligner.c:567-584)
+                    float sM1[C];
+                    if (kk > 0) {
+                        const float4 *cp = gm.cacheA + (size_t) (kk - 1) * S;
+#pragma unroll
+                        for (int j = 0; j < C; j++) {
+                            const float4 q = cp[j * L + gl];
                             sM1[j] = __fmaf_rn(c.t[2 * 3 + 0], q.z, __fmaf_rn(c.t[1 * 3 + 0], q.y, c.t[0 * 3 + 0] * q.x));
                         }
                     } else {
 #pragma unroll
                         for (int j = 0; j < C; j++) sM1[j] = chkSM[j];
                     }
-                    if (inf.y != 0) laneShift<C>(sM1, inf.y, lane);
+                    laneShift<C, L>(sM1, on ? inf.y : 0, gl);
                     float part = 0.0f;
 #pragma unroll
                     for (int j = 0; j < C; j++) {
-                        const float uMn = (d & 1) ? gA[j] : gB[j];  // match u of d+1
+                        const float uMn = par ? gA[j] : gB[j];  // match u of d+1
                         part = __fmaf_rn(f[j].x, bM[j], part);
                         part = __fmaf_rn(f[j].y, bX[j], part);
                         part = __fmaf_rn(f[j].z, bY[j], part);
                         part = __fmaf_rn(uMn, sM1[j], part);
                     }
-                    const float T = warpSum(part);
-                    if (T > 0.0f) {
-                        const int ex = exponentOf(T);
-                        Tm = T * pow2f(-ex);
-                        ET = Ef + Eb + ex;
-                    } else {
-                        Tm = 0.0f;
-                        ET = 0;
-                    }
-                    if (wa.atEnd && posts == 0) {
-                        logLik += Tm > 0.0f ? log((double) Tm) + (double) ET * 0.69314718055994530942 : -INFINITY;
+                    const float T = groupSum<L>(part);
+                    if (refresh) {
+                        untilRefresh = 10;
+                        if (T > 0.0f) {
+                            const int ex = exponentOf(T);
+                            Tm = T * pow2f(-ex);
+                            ET = Ef + Eb + ex;
+                        } else {
+                            Tm = 0.0f;
+                            ET = 0;
+                        }
+                        if (wk.atEnd && posts == 0) {
+                            logLik += Tm > 0.0f ? log((double) Tm) + (double) ET * 0.69314718055994530942 : -INFINITY;
+                        }
                     }
                 }
-                posts++;
-                untilRefresh--;
-                if (Tm > 0.0f) {
+                if (post) {
+                    posts++;
+                    untilRefresh--;
+                }
+                const bool emit = post && Tm > 0.0f;
+                if (__any_sync(FULL_MASK, emit)) {
                     const int ex = max(-126, min(127, Ef + Eb - ET));
-                    const float scale = __fdividef(pow2f(ex), Tm);
+                    const float scale = emit ? __fdividef(pow2f(ex), Tm) : 0.0f;
                     float p[3][C];
 #pragma unroll
                     for (int j = 0; j < C; j++) {
@@ -701,23 +748,24 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, WarpMem<C, K> &wm, con
                         p[1][j] = (f[j].y * bX[j]) * scale;
                         p[2][j] = (f[j].z * bY[j]) * scale;
                     }
-                    emitDiagonal<C>(lane, o, p, wa.thr, slotX0(d, inf.x), d);
+                    emitDiagonal<C, L>(gl, o, p, thr, slotX0(d, inf.x), d, emit);
                 }
-            }
-            // u-values of d (emissions are zero outside the band)
+                // u-values of d (emissions are zero outside the band); kept when the diagonal is off
 #pragma unroll
-            for (int j = 0; j < C; j++) {
-                gX[j] = e[j].x * bX[j];
-                gY[j] = e[j].y * bY[j];
-                const float uM = f[j].w * bM[j];
-                if (d & 1) gB[j] = uM; else gA[j] = uM;
-            }
-            // moving below d crosses the window shift met when entering d
-            if (inf.y != 0) {
-                laneShift<C>(gX, -inf.y, lane);
-                laneShift<C>(gY, -inf.y, lane);
-                laneShift<C>(gA, -inf.y, lane);
-                laneShift<C>(gB, -inf.y, lane);
+                for (int j = 0; j < C; j++) {
+                    const float ux = e[j].x * bX[j], uy = e[j].y * bY[j], um = f[j].w * bM[j];
+                    gX[j] = on ? ux : gX[j];
+                    gY[j] = on ? uy : gY[j];
+                    if (par) gB[j] = on ? um : gB[j]; else gA[j] = on ? um : gA[j];
+                }
+                // moving below d crosses the window shift met when entering d
+                const int back = on ? -inf.y : 0;
+                if (__any_sync(FULL_MASK, back != 0)) {
+                    laneShift<C, L>(gX, back, gl);
+                    laneShift<C, L>(gY, back, gl);
+                    laneShift<C, L>(gA, back, gl);
+                    laneShift<C, L>(gB, back, gl);
+                }
             }
         }
         // rescale the carried backward state at the block boundary
@@ -725,8 +773,8 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, WarpMem<C, K> &wm, con
             float m = 0.0f;
 #pragma unroll
             for (int j = 0; j < C; j++) m = fmaxf(m, fmaxf(fmaxf(gX[j], gY[j]), fmaxf(gA[j], gB[j])));
-            m = warpMax(m);
-            if (m > 0.0f) {
+            m = groupMax<L>(m);
+            if (blockOn && m > 0.0f) {
                 const int kx = exponentOf(m);
                 const float s = pow2f(-kx);
 #pragma unroll
@@ -743,27 +791,59 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, WarpMem<C, K> &wm, con
     }
 }
 
+// Next traceback point of a group's task: the first anti-diagonal d in [from, N) whose band
+// is at most 2*diagonalExpansion+1 cells wide (impl/pairwiseAligner.c:722-724), else N.
+// Called by every lane of the warp; groups with `searching` false return N.
+template <int L>
+__device__ __forceinline__ int nextTracePoint(const Ctx &c, int from, int maxWidth, bool searching) {
+    int D = c.N;
+    int pos = from;
+    bool look = searching && pos < c.N;
+    while (__any_sync(FULL_MASK, look)) {
+        const int d = pos + c.gl;
+        bool ok = false;
+        if (look && d < c.N) {
+            const int2 bd = *reinterpret_cast<const int2 *>(c.band + d);
+            ok = ((bd.y - bd.x) >> 1) + 1 <= maxWidth;
+        }
+        const unsigned bits = groupBits<L>(__ballot_sync(FULL_MASK, ok), c.g);
+        if (look) {
+            if (bits) {
+                D = pos + __ffs(bits) - 1;
+                look = false;
+            } else {
+                pos += L;
+                look = pos < c.N;
+            }
+        }
+    }
+    return D;
+}
+
 // ---------------------------------------------------------------------------
-// One task: forward sweep with checkpoints, walks at traceback points and end.
+// One warp-load of G tasks: forward sweep with checkpoints, then the walks.
 // ---------------------------------------------------------------------------
 
-template <int C, int K>
-__device__ __forceinline__ void runTask(const DpArgs &a, const float *rpAll, const float *smAll, const float *gxAll,
-                                        const float *gyAll, int taskIndex, WarpMem<C, K> &wm, const Scratch &sc) {
-    constexpr int S = 32 * C;
-    constexpr int R = Geo<C>::R;
+template <int C, int L, int K>
+__device__ __forceinline__ void runGroup(const DpArgs &a, const float *rpAll, const float *smAll, const float *gxAll,
+                                         const float *gyAll, int taskIndex, GroupMem<C, L, K> &gm, const Scratch &sc) {
+    constexpr int S = L * C;
+    constexpr int R = RingSize<S>::R;
     const int lane = threadIdx.x & 31;
-    const Task &tk = a.tasks[taskIndex];
-    TaskOut *to = a.out + taskIndex;
+    const bool has = taskIndex >= 0;
+    const Task *tk = a.tasks + (has ? taskIndex : 0);
+    TaskOut *to = a.out + (has ? taskIndex : 0);
     Ctx c;
-    c.lane = lane;
-    c.lx = tk.lx;
-    c.ly = tk.ly;
-    c.N = tk.lx + tk.ly;
-    c.xs = a.xs + tk.xOff;
-    c.ys = a.ys + tk.yOff;
-    c.band = reinterpret_cast<const int4 *>(a.band) + tk.bandOff;
-    const int model = (tk.flags & 4) ? 0 : 1;
+    c.gl = lane & (L - 1);
+    c.g = lane / L;
+    c.lx = has ? tk->lx : 0;
+    c.ly = has ? tk->ly : 0;
+    c.N = c.lx + c.ly;
+    c.xs = a.xs + tk->xOff;
+    c.ys = a.ys + tk->yOff;
+    c.band = reinterpret_cast<const int4 *>(a.band) + tk->bandOff;
+    const int flags = has ? tk->flags : 0;
+    const int model = (flags & 4) ? 0 : 1;
     const DevModel &dm = a.models[model];
 #pragma unroll
     for (int k = 0; k < 9; k++) c.t[k] = dm.t[k];
@@ -773,44 +853,45 @@ __device__ __forceinline__ void runTask(const DpArgs &a, const float *rpAll, con
     c.gy = gyAll + model * 5;
     c.rle = dm.runLength;
     c.strandFwd = dm.strand;
-    const int status0 = to->status;
-    if (c.N == 0 || (status0 & kTaskBand)) {
-        if (lane == 0) {
-            to->count[0] = to->count[1] = to->count[2] = 0;
-            to->logLik = 0.0;
-        }
-        return;
+    const int status0 = has ? to->status : 0;
+    const bool tooLong = has && c.N / K + 1 > sc.blocks;
+    const bool live = has && c.N > 0 && (status0 & kTaskBand) == 0 && !tooLong;
+    if (has && !live && c.gl == 0) {
+        to->count[0] = to->count[1] = to->count[2] = 0;
+        to->logLik = 0.0;
+        if (tooLong) to->status = status0 | kTaskScratch;
     }
-    if (c.N / K + 1 > sc.blocks) {
-        if (lane == 0) {
-            to->status = status0 | kTaskScratch;
-            to->count[0] = to->count[1] = to->count[2] = 0;
-        }
-        return;
-    }
+    const int myN = live ? c.N : 0;
+    const int Nmax = warpMaxInt(myN);
+    if (Nmax <= 0) return;
+
     Out o;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        o.w[k] = a.outW[k] + tk.outOff[k];
-        o.x[k] = a.outX[k] + tk.outOff[k];
-        o.y[k] = a.outY[k] + tk.outOff[k];
-        o.top[k] = tk.cap[k];
+        o.w[k] = a.outW[k] + tk->outOff[k];
+        o.x[k] = a.outX[k] + tk->outOff[k];
+        o.y[k] = a.outY[k] + tk->outOff[k];
+        o.top[k] = tk->cap[k];
         o.written[k] = 0;
     }
-    o.xShift = tk.x1 + tk.xShift;
-    o.yShift = tk.y1;
-    WalkArgs wa;
-    wa.startP = (tk.flags & 1) ? dm.raggedStart : dm.start;
-    wa.thr = a.threshold;
+    o.xShift = tk->x1 + tk->xShift;
+    o.yShift = tk->y1;
+    Walk wk;
+    wk.startP = (flags & 1) ? dm.raggedStart : dm.start;
     double logLik = 0.0;
     bool bad = false;
-    wm.rx.bad = 0;
-    wm.ry.bad = 0;
+    gm.rx.bad = 0;
+    gm.ry.bad = 0;
+    gm.rx.lo = 1 << 30;  // nothing resident
+    gm.ry.lo = 1 << 30;
 
-    // band records: 32-diagonal chunks through cp.async into the warp's ring of 64
+    // band records: 32-diagonal chunks through cp.async into the group's ring of 64
     auto issueChunk = [&](int chunk) {
-        const int dd = chunk * 32 + lane;
-        if (dd <= c.N) cpAsync16(&wm.bandRing[dd & 63], &c.band[dd]);
+#pragma unroll
+        for (int q = c.gl; q < 32; q += L) {
+            const int dd = chunk * 32 + q;
+            if (live && dd <= myN) cpAsync16(&gm.bandRing[dd & 63], &c.band[dd]);
+        }
         cpAsyncCommit();
     };
     issueChunk(0);
@@ -820,75 +901,91 @@ __device__ __forceinline__ void runTask(const DpArgs &a, const float *rpAll, con
 
     Fwd<C> st;
     Slots<C> sy;
-    const int4 b0 = wm.bandRing[0];
-    int Q = initialWindow<C>(b0.z, b0.w);
+    int Q = 0;
+    if (live) {
+        const int4 b0 = gm.bandRing[0];
+        Q = initialWindow<S>(b0.z, b0.w);
+    }
     int Ef = 0;
     {
+        // every group fills its rings once, so that every entry is a valid decoded symbol
         const int x0 = slotX0(0, Q);
-        ringFill<R, true>(c, wm.rx, x0 - 1 - 8);
-        ringFill<R, false>(c, wm.ry, -x0 - S - 8);
-        forwardOrigin<C, false>(c, wa.startP, Q, st, nullptr, nullptr);
+        ringEnsure<R, L, true>(c, gm.rx, x0 - 1 - 8, x0 + S - 2, true, true);
+        ringEnsure<R, L, false>(c, gm.ry, -x0 - S - 8, -x0 - 1, true, true);
+        forwardOrigin<C, L, false>(c, wk.startP, Q, st, nullptr, nullptr);
     }
     bool have = false;
-    int tracedBackTo = 0;
-    for (int d = 1; d <= c.N; d++) {
+    for (int d = 1; d <= Nmax; d++) {
+        const bool on = d <= myN;
         if ((d & 31) == 0) {
             issueChunk((d >> 5) + 1);
             cpAsyncWaitAllButOne();
             __syncwarp();
         }
         if ((d & (K - 1)) == 0) {
-            Ef += rescaleFwd<C>(st);
-            const int b = d / K;
-            storeFwd<C>(sc.chk + (size_t) b * C * 32, lane, st);
-            if (lane == 0) sc.scal[b] = make_int2(Ef, Q);
+            Ef += rescaleFwd<C, L>(st);
+            if (on) {
+                const int b = d / K;
+                storeFwd<C, L>(sc.chk + (size_t) b * S, c.gl, st);
+                if (c.gl == 0) sc.scal[b] = make_int2(Ef, Q);
+            }
         }
-        const int4 bd = wm.bandRing[d & 63];
-        const int dl = windowShift<C>(Q, bd.z, bd.w, bad);
-        if (bad) break;
-        if (dl != 0) {
-            shiftFwd<C>(st, dl, lane);
-            Q += C * dl;
-            have = false;
+        const int4 bd = gm.bandRing[d & 63];
+        const int dl = on ? windowShift<C, S>(Q, bd.z, bd.w, bad) : 0;
+        if (__any_sync(FULL_MASK, dl != 0)) {
+            shiftFwd<C, L>(st, dl, c.gl);
+            if (dl != 0) {
+                Q += C * dl;
+                have = false;
+            }
         }
         const int x0 = slotX0(d, Q), y0 = d - x0;
-        ringEnsure<R, true>(c, wm.rx, x0 - 1, x0 + S - 2, true);
-        ringEnsure<R, false>(c, wm.ry, y0 - S, y0 - 1, true);
+        ringEnsure<R, L, true>(c, gm.rx, x0 - 1, x0 + S - 2, true, on);
+        ringEnsure<R, L, false>(c, gm.ry, y0 - S, y0 - 1, true, on);
         const int sLo = (bd.x >> 1) - Q, sHi = (bd.y >> 1) - Q;
         if (d & 1) {
-            if (have) stepSlots<C, R, 1>(c, wm.rx, wm.ry, d, Q, sy); else loadSlots<C, R>(c, wm.rx, wm.ry, d, Q, sy);
-            forwardDiagonal<C, 1, false>(c, st, sy, sLo, sHi, nullptr, nullptr);
+            stepSlots<C, L, R, 1>(c.gl, gm.rx, gm.ry, d, Q, sy);
+            if (!have) loadSlots<C, R>(c.gl, gm.rx, gm.ry, d, Q, sy);
+            forwardDiagonal<C, L, 1, false>(c, st, sy, sLo, sHi, nullptr, nullptr);
         } else {
-            if (have) stepSlots<C, R, 0>(c, wm.rx, wm.ry, d, Q, sy); else loadSlots<C, R>(c, wm.rx, wm.ry, d, Q, sy);
-            forwardDiagonal<C, 0, false>(c, st, sy, sLo, sHi, nullptr, nullptr);
+            stepSlots<C, L, R, 0>(c.gl, gm.rx, gm.ry, d, Q, sy);
+            if (!have) loadSlots<C, R>(c.gl, gm.rx, gm.ry, d, Q, sy);
+            forwardDiagonal<C, L, 0, false>(c, st, sy, sLo, sHi, nullptr, nullptr);
         }
         have = true;
-        const bool atEnd = d == c.N;
-        const int width = ((bd.y - bd.x) >> 1) + 1;
-        if (atEnd || (d >= tracedBackTo + a.minDiagsBetweenTraceBack && width <= 2 * a.diagonalExpansion + 1)) {
-            if (!atEnd) storeFwd<C>(sc.resume, lane, st);
-            wa.D = d;
-            wa.tbTo = tracedBackTo;
-            wa.tbFrom = atEnd ? d : d - (a.traceBackDiagonals + 1);
-            wa.atEnd = atEnd ? 1 : 0;
-            wa.endP = (atEnd && (tk.flags & 2)) ? dm.raggedEnd : dm.end;
-            walkSegment<C, K>(c, wm, sc, wa, o, logLik, bad);
-            tracedBackTo = wa.tbFrom;
-            if (bad || atEnd) break;
-            float4 v[C];
-#pragma unroll
-            for (int j = 0; j < C; j++) v[j] = sc.resume[j * 32 + lane];
-            loadFwd<C>(v, st);
-            have = false;
-        }
     }
-    // drain the band prefetch group before the ring is reused
+    // drain the band prefetch groups before the ring is reused
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncwarp();
-    if (lane == 0) {
+
+    // Traceback segments in the reference's order: an intermediate point D is the first
+    // anti-diagonal after the previous point with D >= tracedBackTo + minDiagsBetweenTraceBack
+    // and a narrow band; its posteriors cover (tracedBackTo, D - traceBackDiagonals - 1].
+    // The last segment ends at N and covers (tracedBackTo, N].
+    const int maxWidth = 2 * a.diagonalExpansion + 1;
+    int prevD = 0, tb = 0;
+    bool more = live;
+    while (__any_sync(FULL_MASK, more)) {
+        const int from = max(prevD + 1, tb + a.minDiagsBetweenTraceBack);
+        const int D = nextTracePoint<L>(c, from, maxWidth, more);
+        const bool atEnd = D >= c.N;
+        wk.D = c.N < D ? c.N : D;
+        wk.tbTo = tb;
+        wk.tbFrom = atEnd ? wk.D : wk.D - (a.traceBackDiagonals + 1);
+        wk.atEnd = atEnd ? 1 : 0;
+        wk.active = more ? 1 : 0;
+        wk.endP = (atEnd && (flags & 2)) ? dm.raggedEnd : dm.end;
+        walkSegment<C, L, K>(c, gm, sc, wk, a.threshold, o, logLik, bad);
+        if (more) {
+            tb = wk.tbFrom;
+            prevD = wk.D;
+            more = !atEnd;
+        }
+    }
+    if (live && c.gl == 0) {
         int s = status0;
         if (bad) s |= kTaskWindow;
-        if (wm.rx.bad | wm.ry.bad) s |= kTaskSymbol;
+        if (gm.rx.bad | gm.ry.bad) s |= kTaskSymbol;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             to->count[k] = bad ? 0 : o.written[k];
@@ -899,10 +996,11 @@ __device__ __forceinline__ void runTask(const DpArgs &a, const float *rpAll, con
     }
 }
 
-template <int C, int K, int MAXW>
+template <int C, int L, int K, int MAXW>
 __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
-    using WS = WarpSmem<C, K>;
-    constexpr int R = Geo<C>::R;
+    using GS = GroupSmem<C, L, K>;
+    constexpr int G = 32 / L;
+    constexpr int R = RingSize<L * C>::R;
     extern __shared__ __align__(16) unsigned char smemRaw[];
     const int nTables = a.sharedRepeat ? 1 : 2;
     float *rp = reinterpret_cast<float *>(smemRaw);
@@ -921,30 +1019,33 @@ __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
+    const int g = lane / L;
     const int gwarp = blockIdx.x * (blockDim.x >> 5) + warp;
-    unsigned char *mine = warpBase + (size_t) warp * WS::bytes;
-    WarpMem<C, K> wm;
-    wm.rx = Ring<R>{reinterpret_cast<uint2 *>(mine), 0, 0};
-    wm.ry = Ring<R>{reinterpret_cast<uint2 *>(mine) + R, 0, 0};
-    wm.bandRing = reinterpret_cast<int4 *>(mine + WS::ringBytes);
-    wm.walkBand = reinterpret_cast<int4 *>(mine + WS::ringBytes + WS::bandRingBytes);
-    wm.cacheA = reinterpret_cast<float4 *>(mine + WS::ringBytes + WS::bandRingBytes + WS::walkBandBytes);
-    wm.cacheB = reinterpret_cast<float2 *>(mine + WS::ringBytes + WS::bandRingBytes + WS::walkBandBytes +
-                                           WS::cacheABytes);
-    wm.info = reinterpret_cast<int2 *>(mine + WS::ringBytes + WS::bandRingBytes + WS::walkBandBytes +
-                                       WS::cacheABytes + WS::cacheBBytes);
+    unsigned char *mine = warpBase + ((size_t) warp * G + g) * GS::bytes;
+    GroupMem<C, L, K> gm;
+    gm.rx = Ring<R>{reinterpret_cast<uint2 *>(mine), 0, 0};
+    gm.ry = Ring<R>{reinterpret_cast<uint2 *>(mine) + R, 0, 0};
+    gm.bandRing = reinterpret_cast<int4 *>(mine + GS::ringBytes);
+    gm.walkBand = reinterpret_cast<int4 *>(mine + GS::ringBytes + GS::bandRingBytes);
+    gm.cacheA = reinterpret_cast<float4 *>(mine + GS::ringBytes + GS::bandRingBytes + GS::walkBandBytes);
+    gm.cacheB = reinterpret_cast<float2 *>(mine + GS::ringBytes + GS::bandRingBytes + GS::walkBandBytes +
+                                           GS::cacheABytes);
+    gm.info = reinterpret_cast<int2 *>(mine + GS::ringBytes + GS::bandRingBytes + GS::walkBandBytes +
+                                       GS::cacheABytes + GS::cacheBBytes);
     Scratch sc;
     sc.blocks = a.scratchBlocks;
-    sc.chk = a.scratch + (size_t) gwarp * a.scratchBlocks * (C * 32);
-    sc.scal = a.scratchScalars + (size_t) gwarp * a.scratchBlocks;
-    sc.resume = a.resume + (size_t) gwarp * (C * 32);
+    const size_t slot = (size_t) gwarp * G + g;  // one checkpoint area per task slot
+    sc.chk = a.scratch + slot * a.scratchBlocks * (size_t) (C * L);
+    sc.scal = a.scratchScalars + slot * a.scratchBlocks;
 
+    const int nLoads = (a.nTasks + G - 1) / G;
     while (true) {
-        int t = 0;
-        if (lane == 0) t = atomicAdd(a.queue, 1);
-        t = __shfl_sync(FULL_MASK, t, 0);
-        if (t >= a.nTasks) break;
-        runTask<C, K>(a, rp, sm, gx, gy, a.order[t], wm, sc);
+        int q = 0;
+        if (lane == 0) q = atomicAdd(a.queue, 1);
+        q = __shfl_sync(FULL_MASK, q, 0);
+        if (q >= nLoads) break;
+        const int t = q * G + g;
+        runGroup<C, L, K>(a, rp, sm, gx, gy, t < a.nTasks ? a.order[t] : -1, gm, sc);
         __syncwarp();
     }
 }
@@ -957,63 +1058,70 @@ size_t tableBytes(int nTables) {
     return (((size_t) (nTables * kRepTable + 2 * 25 + 2 * 5 + 2 * 5) * sizeof(float) + 15) & ~(size_t) 15);
 }
 
-template <int C, int K>
+template <int C, int L, int K>
 static size_t smemFor(int warps, int nTables) {
-    return tableBytes(nTables) + (size_t) warps * WarpSmem<C, K>::bytes;
+    return tableBytes(nTables) + (size_t) warps * (32 / L) * GroupSmem<C, L, K>::bytes;
 }
 
-template <int C, int K, int MAXW>
+template <int C, int L, int K, int MAXW>
 static cudaError_t launchT(const DpArgs &a, int blocks, int warps, cudaStream_t s) {
     if (warps > MAXW || warps < 1) return cudaErrorInvalidValue;
-    const size_t smem = smemFor<C, K>(warps, a.sharedRepeat ? 1 : 2);
-    cudaError_t e = cudaFuncSetAttribute(posteriorKernel<C, K, MAXW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int) smem);
+    const size_t smem = smemFor<C, L, K>(warps, a.sharedRepeat ? 1 : 2);
+    cudaError_t e = cudaFuncSetAttribute(posteriorKernel<C, L, K, MAXW>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     if (e != cudaSuccess) return e;
-    posteriorKernel<C, K, MAXW><<<blocks, warps * 32, smem, s>>>(a);
+    posteriorKernel<C, L, K, MAXW><<<blocks, warps * 32, smem, s>>>(a);
     return cudaGetLastError();
 }
 
-// Slot classes: C slots per lane (window S = 32*C), checkpoint stride K.
-int classStride(int C) {
-    return C <= 3 ? 8 : 4;
+// Kernel variants: (C slots per lane, L lanes per task, K checkpoint stride,
+// maximum warps per block = launch bound). The window is S = L*C slots, a warp
+// carries 32/L tasks and a task fits when its band hull spans at most S - 2C slots.
+#define MP_VARIANTS(X) \
+    X(0, 2, 32, 8, 12) \
+    X(1, 4, 16, 4, 8)  \
+    X(2, 8, 8, 4, 5)   \
+    X(3, 3, 32, 8, 8)  \
+    X(4, 4, 32, 4, 10) \
+    X(5, 6, 32, 4, 8)  \
+    X(6, 8, 32, 4, 5)
+
+int variantCount() {
+    return 7;
 }
 
-static int maxWarpsFor(int C, int nTables) {
-    // as many warps as the 227 KB of shared memory per block allows, at most 16
-    const size_t limit = 227 * 1024;
-    int w = 16;
-    while (w > 1) {
-        size_t need = 0;
-        switch (C) {
-            case 2: need = smemFor<2, 8>(w, nTables); break;
-            case 3: need = smemFor<3, 8>(w, nTables); break;
-            case 4: need = smemFor<4, 4>(w, nTables); break;
-            case 6: need = smemFor<6, 4>(w, nTables); break;
-            case 8: need = smemFor<8, 4>(w, nTables); break;
-            default: need = limit + 1;
-        }
-        if (need <= limit) break;
-        w--;
+bool variantShape(int v, int *C, int *L, int *K) {
+    switch (v) {
+#define MP_SHAPE(i, c_, l_, k_, w_) \
+    case i: *C = c_; *L = l_; *K = k_; return true;
+        MP_VARIANTS(MP_SHAPE)
+#undef MP_SHAPE
+        default: return false;
     }
-    return w;
 }
 
-// Upper bounds on warps per block per class (shared-memory limited with one table);
-// they are the kernels' launch bounds, so the compiler may use 65536/(32*MAXW) registers.
-constexpr int kMaxW2 = 12, kMaxW3 = 8, kMaxW4 = 10, kMaxW6 = 8, kMaxW8 = 5;
-
-int classMaxWarps(int C, int nTables) {
-    int cap = C == 2 ? kMaxW2 : C == 3 ? kMaxW3 : C == 4 ? kMaxW4 : C == 6 ? kMaxW6 : kMaxW8;
-    return std::min(cap, maxWarpsFor(C, nTables));
+// As many warps as the kernel's bound and 227 KB of shared memory per block allow.
+int variantMaxWarps(int v, int nTables) {
+    const size_t limit = 227 * 1024;
+    switch (v) {
+#define MP_MAXW(i, c_, l_, k_, w_)                                            \
+    case i: {                                                                 \
+        int w = w_;                                                           \
+        while (w > 1 && smemFor<c_, l_, k_>(w, nTables) > limit) w--;         \
+        return w;                                                             \
+    }
+        MP_VARIANTS(MP_MAXW)
+#undef MP_MAXW
+        default: return 0;
+    }
 }
 
-cudaError_t launchPosterior(int C, const DpArgs &a, int blocks, int warps, cudaStream_t s) {
-    switch (C) {
-        case 2: return launchT<2, 8, kMaxW2>(a, blocks, warps, s);
-        case 3: return launchT<3, 8, kMaxW3>(a, blocks, warps, s);
-        case 4: return launchT<4, 4, kMaxW4>(a, blocks, warps, s);
-        case 6: return launchT<6, 4, kMaxW6>(a, blocks, warps, s);
-        case 8: return launchT<8, 4, kMaxW8>(a, blocks, warps, s);
+cudaError_t launchVariant(int v, const DpArgs &a, int blocks, int warps, cudaStream_t s) {
+    switch (v) {
+#define MP_LAUNCH(i, c_, l_, k_, w_) \
+    case i: return launchT<c_, l_, k_, w_>(a, blocks, warps, s);
+        MP_VARIANTS(MP_LAUNCH)
+#undef MP_LAUNCH
         default: return cudaErrorInvalidValue;
     }
 }

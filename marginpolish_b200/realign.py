@@ -39,8 +39,10 @@ class Engine:
         _lib.check(self._lib.mp_engine_info(h, sm, ma, mi))
         self.sm_count, self.cc = sm.value, (ma.value, mi.value)
 
-    def set_tuning(self, warps_per_block: int = 0, blocks_per_sm: int = 0) -> None:
-        t = _lib.Tuning(0, warps_per_block, blocks_per_sm, 0)
+    def set_tuning(self, warps_per_block: int = 0, blocks_per_sm: int = 0, lanes_per_task: int = 0) -> None:
+        """Posterior-kernel tuning (0 = automatic): resident warps per block, persistent blocks
+        per SM, and lanes per banded sub-problem (32, 16 or 8)."""
+        t = _lib.Tuning(0, warps_per_block, blocks_per_sm, lanes_per_task)
         _lib.check(self._lib.mp_engine_set_tuning(self.handle, ctypes.byref(t)))
 
     def fp32_peak_tflops(self) -> float:
@@ -157,6 +159,34 @@ class Jobs:
         return cls(sx, np.array([0]), np.array([sx.size]), sy, np.array([0, sy.size]), a,
                    np.array([0, a.shape[0]]), np.array([strand]), np.array([int(ragged_left)]),
                    np.array([int(ragged_right)]), np.array([x_shift]))
+
+    @classmethod
+    def concat(cls, parts: "list[Jobs]") -> "Jobs":
+        """One batch holding the jobs of `parts` in order (templates are laid end to end)."""
+        xs, xb, xe, ys, yo, an, ao, st, rl, rr, sh = [], [], [], [], [0], [], [0], [], [], [], []
+        x_base = 0
+        for p in parts:
+            n = p.n_jobs
+            xs.append(p.x_symbols)
+            xb.append(p.x_begin + x_base)
+            xe.append(p.x_end + x_base)
+            x_base += p.x_symbols.size
+            ys.append(p.y_symbols)
+            yo.extend((p.y_offsets[1:] + yo[-1]).tolist())
+            an.append(p.anchors)
+            ao.extend((p.anchor_offsets[1:] + ao[-1]).tolist())
+            st.append(p.strand)
+            rl.append(p.ragged_left if p.ragged_left is not None else np.zeros(n, np.uint8))
+            rr.append(p.ragged_right if p.ragged_right is not None else np.zeros(n, np.uint8))
+            sh.append(p.x_shift if p.x_shift is not None else np.zeros(n, np.int64))
+
+        def cat(v, dt):
+            return np.concatenate(v).astype(dt) if v else np.zeros(0, dt)
+
+        return cls(cat(xs, np.uint16), cat(xb, np.int64), cat(xe, np.int64), cat(ys, np.uint16),
+                   np.asarray(yo, np.int64), np.concatenate(an) if an else np.zeros((0, 3), np.int32),
+                   np.asarray(ao, np.int64), cat(st, np.uint8), cat(rl, np.uint8), cat(rr, np.uint8),
+                   cat(sh, np.int64))
 
 
 @dataclass

@@ -116,6 +116,44 @@ def test_random_banding_segments_and_splits(engine, default_model, seed):
         _run_and_check(engine, gm, mpo, jobs, p)
 
 
+@pytest.fixture
+def lanes(engine, request):
+    """Runs a test under one lanes-per-task setting and restores the automatic choice."""
+    engine.set_tuning(lanes_per_task=request.param)
+    yield request.param
+    engine.set_tuning()
+
+
+@pytest.mark.parametrize("lanes", [32, 16, 8], indirect=True)
+def test_batched_random_jobs_every_variant(engine, default_model, lanes):
+    """Many random jobs in one batch, so tasks of different lengths, traceback segments,
+    ragged ends and splits share warps (2 or 4 tasks per warp for 16 or 8 lanes), including
+    empty jobs; every job is checked against the FP64 oracle."""
+    rng = np.random.default_rng(7 + lanes)
+    gm = Model(engine, default_model, default_model)
+    mpo = (MpoModel.from_state_model(default_model), MpoModel.from_state_model(default_model))
+    p = AlignmentParams(threshold=0.01, traceback_diagonals=5, min_diags_between_traceback=14,
+                        diagonal_expansion=6, dynamic_anchor_expansion=True, split_matrix_bigger_than_this=2500)
+    parts = []
+    for case in range(48):
+        sx, sy = _random_case(rng, 160)
+        a = _random_anchors(rng, sx.size, sy.size)
+        parts.append(Jobs.single(sx, sy, a, int(rng.random() < 0.5), bool(rng.random() < 0.3),
+                                 bool(rng.random() < 0.3)))
+    parts.append(Jobs.single(np.zeros(0, np.uint16), np.zeros(0, np.uint16), np.zeros((0, 3), np.int32)))
+    _run_and_check(engine, gm, mpo, Jobs.concat(parts), p)
+
+
+@pytest.mark.parametrize("lanes", [32, 16, 8], indirect=True)
+def test_polish_workload_every_variant(engine, polish_model, lanes):
+    """Run-length reads of the small polishing workload under each lanes-per-task setting."""
+    jobs = synth.config_small(seed=3, n_reads=8).jobs()
+    gm = Model.from_polish(engine, polish_model)
+    mpo = (MpoModel.from_state_model(polish_model.forward), MpoModel.from_state_model(polish_model.reverse))
+    res, worst = _run_and_check(engine, gm, mpo, jobs, polish_model.alignment)
+    assert worst <= 1e-4
+
+
 def test_empty_and_tiny_sequences(engine, default_model):
     gm = Model(engine, default_model, default_model)
     mpo = (MpoModel.from_state_model(default_model), MpoModel.from_state_model(default_model))

@@ -212,6 +212,22 @@ __device__ __forceinline__ void ringEnsure(const Ctx &c, Ring<R> &r, int needLo,
     }
 }
 
+// Makes the symbols of diagonal d resident in both rings (window Q) and returns the first
+// diagonal after d whose symbols may leave them. While the window does not move, the x
+// range [x0-1, x0+S-2] with x0 = Q + (d+1)/2 and the y range [y0-S, y0-1] with
+// y0 = d/2 - Q only grow, so the rings stay valid until x0+S-2 or y0-1 passes the ring's
+// top; a window shift forces a new check. Called by every lane of the warp.
+template <int R, int L, int S>
+__device__ __forceinline__ int ensureRings(const Ctx &c, Ring<R> &rx, Ring<R> &ry, int d, int Q, bool up,
+                                           bool active) {
+    const int x0 = Q + ((d + 1) >> 1), y0 = d - x0;
+    ringEnsure<R, L, true>(c, rx, x0 - 1, x0 + S - 2, up, active);
+    ringEnsure<R, L, false>(c, ry, y0 - S, y0 - 1, up, active);
+    // x valid while (d'+1)/2 <= rx.lo + R + 1 - S - Q, y valid while d'/2 <= ry.lo + R + Q
+    const int a = min(rx.lo + R + 1 - S - Q, 1 << 28), b = min(ry.lo + R + Q, 1 << 28);
+    return min(2 * a, 2 * b + 1) + 1;
+}
+
 template <int C>
 struct Slots {
     uint32_t xpk[C];
@@ -604,6 +620,7 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
         }
         Slots<C> sy;
         bool have = false;
+        int checkAt = dStart;  // rings are checked again at the start of every block
 #pragma unroll 1
         for (int k = 0; k < K; k += 2) {
 #pragma unroll
@@ -618,11 +635,11 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
                     if (dl != 0) {
                         Q += C * dl;
                         have = false;
+                        checkAt = d;
                     }
                 }
-                const int x0 = slotX0(d, Q), y0 = d - x0;
-                ringEnsure<R, L, true>(c, gm.rx, x0 - 1, x0 + S - 2, false, on);
-                ringEnsure<R, L, false>(c, gm.ry, y0 - S, y0 - 1, false, on);
+                if (__any_sync(FULL_MASK, on && d >= checkAt))
+                    checkAt = ensureRings<R, L, S>(c, gm.rx, gm.ry, d, Q, false, on);
                 const int sLo = (bd.x >> 1) - Q, sHi = (bd.y >> 1) - Q;
                 float4 *ca = gm.cacheA + (size_t) kk * S;
                 float2 *cb = gm.cacheB + (size_t) kk * S;
@@ -915,6 +932,7 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, const float *rpAll, co
         forwardOrigin<C, L, false>(c, wk.startP, Q, st, nullptr, nullptr);
     }
     bool have = false;
+    int checkAt = 1;
     for (int d = 1; d <= Nmax; d++) {
         const bool on = d <= myN;
         if ((d & 31) == 0) {
@@ -937,11 +955,10 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, const float *rpAll, co
             if (dl != 0) {
                 Q += C * dl;
                 have = false;
+                checkAt = d;
             }
         }
-        const int x0 = slotX0(d, Q), y0 = d - x0;
-        ringEnsure<R, L, true>(c, gm.rx, x0 - 1, x0 + S - 2, true, on);
-        ringEnsure<R, L, false>(c, gm.ry, y0 - S, y0 - 1, true, on);
+        if (__any_sync(FULL_MASK, on && d >= checkAt)) checkAt = ensureRings<R, L, S>(c, gm.rx, gm.ry, d, Q, true, on);
         const int sLo = (bd.x >> 1) - Q, sHi = (bd.y >> 1) - Q;
         if (d & 1) {
             stepSlots<C, L, R, 1>(c.gl, gm.rx, gm.ry, d, Q, sy);

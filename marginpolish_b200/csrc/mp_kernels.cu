@@ -102,8 +102,11 @@ __global__ void bandKernel(BandArgs a) {
     }
 }
 
-// Hull of the bands of d-2..d+2 (clamped to the task), written into the second
-// pair of each diagonal record. One warp per task, lanes stride over diagonals.
+// Hull of the bands of d-2..d+2 (clamped to the task), then every record is
+// converted to window-slot units: x-y = 2*slot + (d&1), so slot = (x-y) >> 1 (floor)
+// for both the band and the hull of the diagonal. One warp per task, lanes stride
+// over diagonals; the raw bands of the two diagonals below each 32-diagonal chunk
+// are carried in registers because the chunk before has already been converted.
 __global__ void hullKernel(BandArgs a) {
     const int lane = threadIdx.x & 31;
     const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -111,17 +114,41 @@ __global__ void hullKernel(BandArgs a) {
     const Task &tk = a.tasks[t];
     const int N = tk.lx + tk.ly;
     int2 *band = a.band + 2 * tk.bandOff;
-    for (int d = lane; d <= N; d += 32) {
-        int lo = INT_MAX, hi = INT_MIN;
+    const int2 none = make_int2(INT_MAX, INT_MIN);
+    int2 below1 = none, below2 = none;  // raw bands of base-1 and base-2
+    for (int base = 0; base <= N; base += 32) {
+        const int d = base + lane;
+        const int2 v = d <= N ? band[2 * d] : none;
+        // the two diagonals above the chunk are not converted yet
+        const int2 above = (lane < 2 && base + 32 + lane <= N) ? band[2 * (base + 32 + lane)] : none;
+        int2 n[4];  // bands of d-2, d-1, d+1, d+2
+        const int offs[4] = {-2, -1, 1, 2};
 #pragma unroll
-        for (int k = -2; k <= 2; k++) {
-            int e = d + k;
-            if (e < 0 || e > N) continue;
-            int2 v = band[2 * e];
-            lo = min(lo, v.x);
-            hi = max(hi, v.y);
+        for (int q = 0; q < 4; q++) {
+            const int src = lane + offs[q];
+            int2 w;
+            w.x = __shfl_sync(FULL_MASK, v.x, src & 31);
+            w.y = __shfl_sync(FULL_MASK, v.y, src & 31);
+            const int2 ab = make_int2(__shfl_sync(FULL_MASK, above.x, src & 1),
+                                      __shfl_sync(FULL_MASK, above.y, src & 1));
+            if (src < 0) w = src == -1 ? below1 : below2;
+            if (src > 31) w = ab;
+            const int e = d + offs[q];
+            n[q] = (e < 0 || e > N) ? none : w;
         }
-        band[2 * d + 1] = make_int2(lo, hi);
+        int lo = v.x, hi = v.y;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            lo = min(lo, n[q].x);
+            hi = max(hi, n[q].y);
+        }
+        below1 = make_int2(__shfl_sync(FULL_MASK, v.x, 31), __shfl_sync(FULL_MASK, v.y, 31));
+        below2 = make_int2(__shfl_sync(FULL_MASK, v.x, 30), __shfl_sync(FULL_MASK, v.y, 30));
+        __syncwarp();
+        if (d <= N) {
+            band[2 * d] = make_int2(v.x >> 1, v.y >> 1);
+            band[2 * d + 1] = make_int2(lo >> 1, hi >> 1);
+        }
     }
 }
 

@@ -39,10 +39,41 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <type_traits>
 
 namespace mp {
 
 #define FULL_MASK 0xffffffffu
+
+// Dynamic shared memory of a posterior block. Fixed layout at the start:
+//   [0, 200)    match emission tables, [model][x base][y base] (5 x 5 floats each)
+//   [200, 240)  gap-x emissions [model][base]
+//   [240, 280)  gap-y emissions [model][base]
+//   [kRepBase)  run-length repeat tables, one per model (one when both strands share it)
+// then the per-group workspaces. Table reads use byte offsets from the array start, so a
+// lookup is one shared load with an immediate base.
+extern __shared__ __align__(16) unsigned char mpSmem[];
+constexpr uint32_t kMatchOff = 0, kGapXOff = 200, kGapYOff = 240, kRepBase = 384;
+
+// Bytes of the table area (the per-group workspaces start 16-byte aligned after it).
+__host__ __device__ constexpr size_t tableBytes(int nTables) {
+    return ((size_t) kRepBase + (size_t) nTables * kRepTable * sizeof(float) + 15) & ~(size_t) 15;
+}
+
+__device__ __forceinline__ float ldsF(uint32_t off) {
+    return *reinterpret_cast<const float *>(mpSmem + off);
+}
+
+// Shared-memory load / store at a byte offset from the start of the dynamic array.
+template <typename T>
+__device__ __forceinline__ T lds(uint32_t off) {
+    return *reinterpret_cast<const T *>(mpSmem + off);
+}
+
+template <typename T>
+__device__ __forceinline__ void sts(uint32_t off, const T &v) {
+    *reinterpret_cast<T *>(mpSmem + off) = v;
+}
 
 template <int S>
 struct RingSize {
@@ -98,8 +129,9 @@ __device__ __forceinline__ unsigned groupBits(unsigned ballot, int g) {
     return L == 32 ? ballot : (ballot >> (g * L)) & ((1u << L) - 1u);
 }
 
-__device__ __forceinline__ void cpAsync16(void *smem, const void *gmem) {
-    unsigned s = (unsigned) __cvta_generic_to_shared(smem);
+// 16-byte asynchronous copy into the dynamic shared array at byte offset `off`.
+__device__ __forceinline__ void cpAsync16(uint32_t off, const void *gmem) {
+    const unsigned s = (unsigned) __cvta_generic_to_shared(mpSmem) + off;
     asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
@@ -121,19 +153,20 @@ struct Ctx {
     int lx, ly, N;
     const uint16_t *xs;
     const uint16_t *ys;
-    const int4 *band;       // (xmyL, xmyR, hullL, hullR) of d = 0..N
+    const int4 *band;       // (band lo, band hi, hull lo, hull hi) of d = 0..N, in window slots
     float t[9];
-    const char *rp;         // shared repeat-probability table of the task's model
-    const float *sm;        // shared match table [25] of the model
-    const float *gx;        // shared gap-x [5]
-    const float *gy;        // shared gap-y [5]
+    uint32_t repOff;        // byte offset of the task's repeat table in shared memory
+    uint32_t model;         // 0 forward strand, 1 reverse strand
     int rle;
     int strandFwd;
 };
 
-// Decoded symbols: packed (repeat-table byte offset | match-table byte offset << 17) and gap emission.
-// Positions outside the sequence decode to 'N' with repeat count 0, so every ring entry is a valid
-// table offset.
+// Decoded symbols: packed shared-memory byte offsets and the gap emission. For x, the low 17
+// bits hold the offset of the repeat-table row (table, x base row, x repeat count) and the high
+// bits the offset of the match-table row (model, x base); for y, the y repeat count and y base
+// columns. The sum of an x and a y symbol therefore holds both cell offsets (the low part stays
+// below 2^17, so it never carries). Positions outside the sequence decode to 'N' with repeat
+// count 0, so every ring entry is a valid table offset.
 __device__ __forceinline__ uint2 decodeX(const Ctx &c, int pos, int &bad) {
     int b = 4, rc = 0;
     if (pos >= 0 && pos < c.lx) {
@@ -148,8 +181,9 @@ __device__ __forceinline__ uint2 decodeX(const Ctx &c, int pos, int &bad) {
     }
     int bb = b == 4 ? 0 : b;  // 'N' reads the A row of the repeat table (impl/polisher.c:1758)
     int row = c.strandFwd ? bb : 3 - bb;
-    uint32_t pk = (uint32_t) ((row * (kMaxRepeat * kMaxRepeat) + rc * kMaxRepeat) * 4) | ((uint32_t) (b * 20) << 17);
-    return make_uint2(pk, __float_as_uint(c.gx[b]));
+    uint32_t pk = (c.repOff + (uint32_t) ((row * (kMaxRepeat * kMaxRepeat) + rc * kMaxRepeat) * 4)) |
+                  ((kMatchOff + c.model * 100u + (uint32_t) (b * 20)) << 17);
+    return make_uint2(pk, __float_as_uint(ldsF(kGapXOff + c.model * 20u + (uint32_t) b * 4u)));
 }
 
 __device__ __forceinline__ uint2 decodeY(const Ctx &c, int pos, int &bad) {
@@ -165,34 +199,34 @@ __device__ __forceinline__ uint2 decodeY(const Ctx &c, int pos, int &bad) {
         }
     }
     uint32_t pk = (uint32_t) (rc * 4) | ((uint32_t) (b * 4) << 17);
-    return make_uint2(pk, __float_as_uint(c.gy[b]));
+    return make_uint2(pk, __float_as_uint(ldsF(kGapYOff + c.model * 20u + (uint32_t) b * 4u)));
 }
 
-__device__ __forceinline__ float matchEmission(const Ctx &c, uint32_t xpk, uint32_t ypk) {
-    uint32_t s = xpk + ypk;
-    float r = *reinterpret_cast<const float *>(c.rp + (s & 0x1ffffu));
-    float m = *reinterpret_cast<const float *>(reinterpret_cast<const char *>(c.sm) + (s >> 17));
-    return r * m;
+__device__ __forceinline__ float matchEmission(uint32_t xpk, uint32_t ypk) {
+    const uint32_t s = xpk + ypk;
+    return ldsF(s & 0x1ffffu) * ldsF(s >> 17);
 }
 
 // Decoded symbols of a span of positions in shared memory (one ring per sequence and group).
 template <int R>
 struct Ring {
-    uint2 *buf;
+    uint32_t base;  // byte offset of the ring (R entries of 8 bytes)
     int lo;
     int bad;
+    __device__ __forceinline__ uint32_t at(int pos) const { return base + ((uint32_t) (pos & (R - 1)) << 3); }
+    __device__ __forceinline__ uint2 get(int pos) const { return lds<uint2>(at(pos)); }
 };
 
 // Decodes positions [newLo, newLo+R) into the group's ring where `doFill`; returns 1 if a
 // symbol of this group's fill was out of range. Called by every lane of the warp.
 template <int R, int L, bool IS_X>
-__device__ __noinline__ int ringFillRaw(Ctx c, uint2 *buf, int newLo, int doFill) {
+__device__ __noinline__ int ringFillRaw(Ctx c, uint32_t base, int newLo, int doFill) {
     int bad = 0;
     if (doFill) {
 #pragma unroll 4
         for (int k = 0; k < R / L; k++) {
             int p = newLo + k * L + c.gl;
-            buf[p & (R - 1)] = IS_X ? decodeX(c, p, bad) : decodeY(c, p, bad);
+            sts<uint2>(base + ((uint32_t) (p & (R - 1)) << 3), IS_X ? decodeX(c, p, bad) : decodeY(c, p, bad));
         }
     }
     const unsigned b = __ballot_sync(FULL_MASK, bad);
@@ -207,7 +241,7 @@ __device__ __forceinline__ void ringEnsure(const Ctx &c, Ring<R> &r, int needLo,
     if (__any_sync(FULL_MASK, need)) {
         const int slack = R - (needHi - needLo + 1);
         const int newLo = up ? needLo - slack / 8 : needLo - (slack - slack / 8);
-        r.bad |= ringFillRaw<R, L, IS_X>(c, r.buf, newLo, need ? 1 : 0);
+        r.bad |= ringFillRaw<R, L, IS_X>(c, r.base, newLo, need ? 1 : 0);
         if (need) r.lo = newLo;
     }
 }
@@ -247,8 +281,8 @@ __device__ __forceinline__ void loadSlots(int gl, const Ring<R> &rx, const Ring<
 #pragma unroll
     for (int j = 0; j < C; j++) {
         const int i = gl * C + j;
-        const uint2 vx = rx.buf[(x0 + i - 1) & (R - 1)];
-        const uint2 vy = ry.buf[(y0 - i - 1) & (R - 1)];
+        const uint2 vx = rx.get(x0 + i - 1);
+        const uint2 vy = ry.get(y0 - i - 1);
         s.xpk[j] = vx.x;
         s.ex[j] = __uint_as_float(vx.y);
         s.ypk[j] = vy.x;
@@ -262,7 +296,7 @@ template <int C, int L, int R, int PAR>
 __device__ __forceinline__ void stepSlots(int gl, const Ring<R> &rx, const Ring<R> &ry, int d, int Q, Slots<C> &s) {
     constexpr int S = L * C;
     if (PAR) {
-        const uint2 fresh = rx.buf[(slotX0(d, Q) + S - 2) & (R - 1)];
+        const uint2 fresh = rx.get(slotX0(d, Q) + S - 2);
         uint32_t npk = __shfl_down_sync(FULL_MASK, s.xpk[0], 1, L);
         float ne = __shfl_down_sync(FULL_MASK, s.ex[0], 1, L);
         if (gl == L - 1) {
@@ -277,7 +311,7 @@ __device__ __forceinline__ void stepSlots(int gl, const Ring<R> &rx, const Ring<
         s.xpk[C - 1] = npk;
         s.ex[C - 1] = ne;
     } else {
-        const uint2 fresh = ry.buf[(d - slotX0(d, Q) - 1) & (R - 1)];
+        const uint2 fresh = ry.get(d - slotX0(d, Q) - 1);
         uint32_t npk = __shfl_up_sync(FULL_MASK, s.ypk[C - 1], 1, L);
         float ne = __shfl_up_sync(FULL_MASK, s.ey[C - 1], 1, L);
         if (gl == 0) {
@@ -321,12 +355,11 @@ __device__ __forceinline__ void shiftFwd(Fwd<C> &f, int dl, int gl) {
     laneShift<C, L>(f.mB, dl, gl);
 }
 
-// The window must contain the hull of the bands of d-2..d+2; returns the lane
-// shift (new Q = Q + C*shift). Shared by the sweep and the recompute, so both
+// The window must contain the hull (in slots) of the bands of d-2..d+2; returns the
+// lane shift (new Q = Q + C*shift). Shared by the sweep and the recompute, so both
 // take the same decisions. Sets `bad` when the hull does not fit the window.
 template <int C, int S>
-__device__ __forceinline__ int windowShift(int Q, int hullLo, int hullHi, bool &bad) {
-    const int needLo = hullLo >> 1, needHi = hullHi >> 1;
+__device__ __forceinline__ int windowShift(int Q, int needLo, int needHi, bool &bad) {
     if (needLo >= Q && needHi <= Q + S - 1) return 0;
     const int span = needHi - needLo + 1;
     if (span > S - 2 * C) {
@@ -341,17 +374,17 @@ __device__ __forceinline__ int windowShift(int Q, int hullLo, int hullHi, bool &
 }
 
 template <int S>
-__device__ __forceinline__ int initialWindow(int hullLo, int hullHi) {
-    const int needLo = hullLo >> 1, needHi = hullHi >> 1;
+__device__ __forceinline__ int initialWindow(int needLo, int needHi) {
     return needLo - (S - (needHi - needLo + 1)) / 2;
 }
 
 // One forward anti-diagonal (PAR = d & 1). Emissions are zeroed outside the band
 // [sLo, sHi], which zeroes the cell. With CACHE, the cell values and the masked
-// emissions are written to the block cache at [j][gl].
+// emissions are written to the block cache: rowA / rowB are the byte offsets of this
+// lane's slot 0 in the diagonal's rows, slot j follows at j*L entries.
 template <int C, int L, int PAR, bool CACHE>
 __device__ __forceinline__ void forwardDiagonal(const Ctx &c, Fwd<C> &st, const Slots<C> &sy, int sLo, int sHi,
-                                                float4 *cacheA, float2 *cacheB) {
+                                                uint32_t rowA, uint32_t rowB) {
     float inX[C], inY[C];
     if (PAR) {  // odd d: gap-x source slot i, gap-y source slot i+1
         const float nb = fromNext<L>(st.oy[0], c.gl);
@@ -373,7 +406,7 @@ __device__ __forceinline__ void forwardDiagonal(const Ctx &c, Fwd<C> &st, const 
 #pragma unroll
     for (int j = 0; j < C; j++) {
         const bool in = (unsigned) (base + j) <= span;
-        const float eM = in ? matchEmission(c, sy.xpk[j], sy.ypk[j]) : 0.0f;
+        const float eM = in ? matchEmission(sy.xpk[j], sy.ypk[j]) : 0.0f;
         const float eX = in ? sy.ex[j] : 0.0f;
         const float eY = in ? sy.ey[j] : 0.0f;
         const float fM = eM * (PAR ? st.mB[j] : st.mA[j]);
@@ -386,16 +419,16 @@ __device__ __forceinline__ void forwardDiagonal(const Ctx &c, Fwd<C> &st, const 
         st.ox[j] = nx;
         st.oy[j] = ny;
         if (CACHE) {
-            cacheA[j * L + c.gl] = make_float4(fM, fX, fY, eM);
-            cacheB[j * L + c.gl] = make_float2(eX, eY);
+            sts<float4>(rowA + j * L * 16, make_float4(fM, fX, fY, eM));
+            sts<float2>(rowB + j * L * 8, make_float2(eX, eY));
         }
     }
 }
 
 // Diagonal 0: the start cell (x-y = 0) holds the start (or ragged-start) probabilities.
 template <int C, int L, bool CACHE>
-__device__ __forceinline__ void forwardOrigin(const Ctx &c, const float *startP, int Q, Fwd<C> &st, float4 *cacheA,
-                                              float2 *cacheB) {
+__device__ __forceinline__ void forwardOrigin(const Ctx &c, const float *startP, int Q, Fwd<C> &st, uint32_t rowA,
+                                              uint32_t rowB) {
 #pragma unroll
     for (int j = 0; j < C; j++) {
         const bool here = c.gl * C + j == -Q;
@@ -407,8 +440,8 @@ __device__ __forceinline__ void forwardOrigin(const Ctx &c, const float *startP,
         st.oy[j] = __fmaf_rn(c.t[1 * 3 + 2], fX, __fmaf_rn(c.t[2 * 3 + 2], fY, c.t[0 * 3 + 2] * fM));
         st.mB[j] = 0.0f;
         if (CACHE) {
-            cacheA[j * L + c.gl] = make_float4(fM, fX, fY, 0.0f);
-            cacheB[j * L + c.gl] = make_float2(0.0f, 0.0f);
+            sts<float4>(rowA + j * L * 16, make_float4(fM, fX, fY, 0.0f));
+            sts<float2>(rowB + j * L * 8, make_float2(0.0f, 0.0f));
         }
     }
 }
@@ -490,6 +523,53 @@ __device__ __forceinline__ void emitDiagonal(int gl, Out &o, const float (&p)[3]
     }
 }
 
+// Stores three 32-bit values under a predicate, without a branch.
+__device__ __forceinline__ void storeIf(bool p, int32_t *a, int32_t va, int32_t *b, int32_t vb, int32_t *c,
+                                        int32_t vc) {
+    asm volatile(
+        "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %0, 0;\n\t@q st.global.b32 [%1], %2;\n\t"
+        "@q st.global.b32 [%3], %4;\n\t@q st.global.b32 [%5], %6;\n}" ::"r"((unsigned) p),
+        "l"(a), "r"(va), "l"(b), "r"(vb), "l"(c), "r"(vc));
+}
+
+// emitDiagonal without branches: the same ranks and tuples, written with predicated stores.
+template <int C, int L>
+__device__ __forceinline__ void emitDiagonalFlat(int gl, Out &o, const float (&p)[3][C], float thr, int x0, int d,
+                                                 bool active) {
+    uint32_t m[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        m[k] = 0;
+#pragma unroll
+        for (int j = 0; j < C; j++) m[k] |= (p[k][j] >= thr ? 1u : 0u) << j;
+        m[k] = active ? m[k] : 0u;
+    }
+    const uint32_t cnt = (uint32_t) __popc(m[0]) | ((uint32_t) __popc(m[1]) << 10) | ((uint32_t) __popc(m[2]) << 20);
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int off = 1; off < L; off <<= 1) {
+        const uint32_t v = __shfl_up_sync(FULL_MASK, incl, off, L);
+        incl += gl >= off ? v : 0u;
+    }
+    const uint32_t total = __shfl_sync(FULL_MASK, incl, L - 1, L);
+    const uint32_t excl = incl - cnt;
+    const int xl = x0 + gl * C;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        int pos = o.top[k] - 1 - o.written[k] - (int) ((excl >> (10 * k)) & 1023u);
+#pragma unroll
+        for (int j = 0; j < C; j++) {
+            const bool sel = (m[k] >> j) & 1u;
+            const int x = xl + j;
+            const int q = max(pos, 0);
+            storeIf(sel && pos >= 0, o.w[k] + q, (int32_t) floorf(fminf(p[k][j], 1.0f) * (float) kProbOne), o.x[k] + q,
+                    x - 1 + o.xShift, o.y[k] + q, d - x - 1 + o.yShift);
+            pos -= sel ? 1 : 0;
+        }
+        o.written[k] += (int) ((total >> (10 * k)) & 1023u);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Shared workspace of one group
 // ---------------------------------------------------------------------------
@@ -510,11 +590,11 @@ struct GroupSmem {
 template <int C, int L, int K>
 struct GroupMem {
     Ring<RingSize<L * C>::R> rx, ry;
-    int4 *bandRing;
-    int4 *walkBand;
-    float4 *cacheA;
-    float2 *cacheB;
-    int2 *info;
+    uint32_t bandRing;  // byte offsets in shared memory: 64 band records (int4)
+    uint32_t walkBand;  // K band records of the block being walked
+    uint32_t cacheA;    // [K][S] float4: fM, fX, fY, eM
+    uint32_t cacheB;    // [K][S] float2: eX, eY
+    uint32_t info;      // [K] int2: window, shift
 };
 
 struct Scratch {
@@ -566,6 +646,9 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
     for (int j = 0; j < C; j++) gX[j] = gY[j] = gA[j] = gB[j] = 0.0f;
     int Eb = 0, posts = 0, ET = 0, untilRefresh = 0;
     float Tm = 0.0f;
+    float llTm = 0.0f;  // total of the first posterior diagonal of the final segment: the likelihood
+    int llET = 0;
+    bool llSet = false;
     const float endM = wk.endP[0], endX = wk.endP[1], endY = wk.endP[2];
     const int bTop = wk.active ? wk.D / K : -1;
     const int bBot = wk.active ? (wk.tbTo + 1) / K : 0;
@@ -587,6 +670,7 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
         if (ok && gl < K && dd <= c.N) pband = c.band[dd];
     };
     prefetch(bTop, bTop >= bBot);
+    const uint32_t laneA = gm.cacheA + (uint32_t) gl * 16, laneB = gm.cacheB + (uint32_t) gl * 8;
 
     for (int w = 0; w < nIter; w++) {
         const int b = bTop - w;
@@ -598,7 +682,7 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
 #pragma unroll
         for (int j = 0; j < C; j++) cchk[j] = pchk[j];
         const int2 cscal = pscal;
-        if (blockOn && gl < K) gm.walkBand[gl] = pband;
+        if (blockOn && gl < K) sts<int4>(gm.walkBand + gl * 16, pband);
         __syncwarp();
         prefetch(b - 1, blockOn && b - 1 >= bBot);
 
@@ -612,177 +696,213 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
 #pragma unroll
         for (int j = 0; j < C; j++) chkSM[j] = rs.mB[j];
         if (blockOn && b == 0) {
-            const int4 b0 = gm.walkBand[0];
+            const int4 b0 = lds<int4>(gm.walkBand);
             Q = initialWindow<S>(b0.z, b0.w);
             Ef = 0;
 #pragma unroll
             for (int j = 0; j < C; j++) chkSM[j] = 0.0f;
         }
         Slots<C> sy;
-        bool have = false;
-        int checkAt = dStart;  // rings are checked again at the start of every block
+        // A whole block past diagonal 0 whose window does not move and whose symbols stay in
+        // the rings is recomputed without checks or branches.
+        const bool full = blockOn && b > 0 && dEnd == dStart + K - 1;
+        // the slots of diagonal dStart-1 (window of the checkpoint) seed the block's first step
+        int checkAt = ensureRings<R, L, S>(c, gm.rx, gm.ry, dStart - 1, Q, false, full);
+        bool clear = full && dEnd < checkAt;
+        if (gl < K) {
+            const int4 bd = lds<int4>(gm.walkBand + gl * 16);
+            clear = clear && bd.z >= Q && bd.w <= Q + S - 1;
+        }
+        const bool flat = __all_sync(FULL_MASK, clear);
+        if (flat) {
+            loadSlots<C, R>(gl, gm.rx, gm.ry, dStart - 1, Q, sy);
 #pragma unroll 1
-        for (int k = 0; k < K; k += 2) {
-#pragma unroll
-            for (int par = 0; par < 2; par++) {
-                const int kk = k + par;
+            for (int kk = 0; kk < K; kk += 2) {
                 const int d = dStart + kk;
-                const bool on = blockOn && d <= dEnd;
-                const int4 bd = gm.walkBand[kk];
-                const int dl = (on && d > 0) ? windowShift<C, S>(Q, bd.z, bd.w, bad) : 0;
-                if (__any_sync(FULL_MASK, dl != 0)) {
-                    shiftFwd<C, L>(rs, dl, gl);
-                    if (dl != 0) {
-                        Q += C * dl;
-                        have = false;
-                        checkAt = d;
+                const int2 b0 = lds<int2>(gm.walkBand + kk * 16);
+                const int2 b1 = lds<int2>(gm.walkBand + (kk + 1) * 16);
+                const uint32_t rowA = laneA + (uint32_t) (kk * S * 16), rowB = laneB + (uint32_t) (kk * S * 8);
+                stepSlots<C, L, R, 0>(gl, gm.rx, gm.ry, d, Q, sy);
+                forwardDiagonal<C, L, 0, true>(c, rs, sy, b0.x - Q, b0.y - Q, rowA, rowB);
+                stepSlots<C, L, R, 1>(gl, gm.rx, gm.ry, d + 1, Q, sy);
+                forwardDiagonal<C, L, 1, true>(c, rs, sy, b1.x - Q, b1.y - Q, rowA + S * 16, rowB + S * 8);
+            }
+            if (gl < K) sts<int2>(gm.info + gl * 8, make_int2(Q, 0));
+        } else {
+            checkAt = dStart;  // the rings are checked, and the slots loaded, at the block's first diagonal
+#pragma unroll 1
+            for (int k = 0; k < K; k += 2) {
+#pragma unroll
+                for (int par = 0; par < 2; par++) {
+                    const int kk = k + par;
+                    const int d = dStart + kk;
+                    const bool on = blockOn && d <= dEnd;
+                    const int4 bd = lds<int4>(gm.walkBand + kk * 16);
+                    const bool move = on && d > 0 && (bd.z < Q || bd.w > Q + S - 1);
+                    int dl = 0;
+                    bool reload = kk == 0;
+                    const bool rare = __any_sync(FULL_MASK, move || (on && d >= checkAt));
+                    if (rare) {
+                        dl = move ? windowShift<C, S>(Q, bd.z, bd.w, bad) : 0;
+                        if (__any_sync(FULL_MASK, dl != 0)) {
+                            shiftFwd<C, L>(rs, dl, gl);
+                            if (dl != 0) {
+                                Q += C * dl;
+                                reload = true;
+                            }
+                        }
+                        checkAt = ensureRings<R, L, S>(c, gm.rx, gm.ry, d, Q, false, on);
                     }
+                    const int sLo = bd.x - Q, sHi = bd.y - Q;
+                    const uint32_t rowA = laneA + (uint32_t) (kk * S * 16), rowB = laneB + (uint32_t) (kk * S * 8);
+                    if (par) {
+                        stepSlots<C, L, R, 1>(gl, gm.rx, gm.ry, d, Q, sy);
+                        if (rare && reload) loadSlots<C, R>(gl, gm.rx, gm.ry, d, Q, sy);
+                        forwardDiagonal<C, L, 1, true>(c, rs, sy, sLo, sHi, rowA, rowB);
+                    } else {
+                        stepSlots<C, L, R, 0>(gl, gm.rx, gm.ry, d, Q, sy);
+                        if (rare && reload) loadSlots<C, R>(gl, gm.rx, gm.ry, d, Q, sy);
+                        forwardDiagonal<C, L, 0, true>(c, rs, sy, sLo, sHi, rowA, rowB);
+                        if (d == 0) forwardOrigin<C, L, true>(c, wk.startP, Q, rs, rowA, rowB);
+                    }
+                    if (gl == 0) sts<int2>(gm.info + kk * 8, make_int2(Q, dl));
                 }
-                if (__any_sync(FULL_MASK, on && d >= checkAt))
-                    checkAt = ensureRings<R, L, S>(c, gm.rx, gm.ry, d, Q, false, on);
-                const int sLo = (bd.x >> 1) - Q, sHi = (bd.y >> 1) - Q;
-                float4 *ca = gm.cacheA + (size_t) kk * S;
-                float2 *cb = gm.cacheB + (size_t) kk * S;
-                if (par) {
-                    stepSlots<C, L, R, 1>(gl, gm.rx, gm.ry, d, Q, sy);
-                    if (!have) loadSlots<C, R>(gl, gm.rx, gm.ry, d, Q, sy);
-                    forwardDiagonal<C, L, 1, true>(c, rs, sy, sLo, sHi, ca, cb);
-                } else {
-                    stepSlots<C, L, R, 0>(gl, gm.rx, gm.ry, d, Q, sy);
-                    if (!have) loadSlots<C, R>(gl, gm.rx, gm.ry, d, Q, sy);
-                    forwardDiagonal<C, L, 0, true>(c, rs, sy, sLo, sHi, ca, cb);
-                    if (d == 0) forwardOrigin<C, L, true>(c, wk.startP, Q, rs, ca, cb);
-                }
-                have = true;
-                if (gl == 0) gm.info[kk] = make_int2(Q, dl);
             }
         }
         __syncwarp();
 
         // ---------------- backward over the block ----------------
-#pragma unroll 1
-        for (int k = K - 2; k >= 0; k -= 2) {
+        // One diagonal (PAR = d & 1). FLAT: every diagonal of the block is on and no window
+        // shift occurs, so the step has no votes or branches (the total is refreshed by
+        // selection and tuples are written with predicated stores).
+        auto back = [&](auto parity, auto flatTag, int kk) {
+            constexpr int PAR = decltype(parity)::value;
+            constexpr bool FLAT = decltype(flatTag)::value;
+            const int d = dStart + kk;
+            const bool on = FLAT || (blockOn && d <= dEnd && d > wk.tbTo);
+            const int2 inf = FLAT ? make_int2(Q, 0) : lds<int2>(gm.info + kk * 8);
+            float4 f[C];
+            float2 e[C];
 #pragma unroll
-            for (int par = 1; par >= 0; par--) {
-                const int kk = k + par;
-                const int d = dStart + kk;
-                const bool on = blockOn && d <= dEnd && d > wk.tbTo;
-                const int2 inf = gm.info[kk];
-                const float4 *ca = gm.cacheA + (size_t) kk * S;
-                const float2 *cb = gm.cacheB + (size_t) kk * S;
-                float4 f[C];
-                float2 e[C];
+            for (int j = 0; j < C; j++) {
+                f[j] = lds<float4>(laneA + (uint32_t) ((kk * S + j * L) * 16));
+                e[j] = lds<float2>(laneB + (uint32_t) ((kk * S + j * L) * 8));
+            }
+            float bM[C], bX[C], bY[C];
+            {
+                float sX[C], sY[C];
+                if (PAR) {  // odd d: gap-x successor slot i+1, gap-y successor slot i
+                    const float nb = fromNext<L>(gX[0], gl);
+#pragma unroll
+                    for (int j = 0; j < C; j++) {
+                        sX[j] = (j < C - 1) ? gX[j + 1] : nb;
+                        sY[j] = gY[j];
+                    }
+                } else {  // even d: gap-x successor slot i, gap-y successor slot i-1
+                    const float nb = fromPrev<L>(gY[C - 1], gl);
+#pragma unroll
+                    for (int j = 0; j < C; j++) {
+                        sX[j] = gX[j];
+                        sY[j] = (j > 0) ? gY[j - 1] : nb;
+                    }
+                }
+                const bool top = d == wk.D;  // the walk's first diagonal holds the end probabilities
 #pragma unroll
                 for (int j = 0; j < C; j++) {
-                    f[j] = ca[j * L + gl];
-                    e[j] = cb[j * L + gl];
+                    const float s2 = PAR ? gB[j] : gA[j];
+                    const float m_ = __fmaf_rn(c.t[0 * 3 + 0], s2, __fmaf_rn(c.t[0 * 3 + 2], sY[j], c.t[0 * 3 + 1] * sX[j]));
+                    const float x_ = __fmaf_rn(c.t[1 * 3 + 0], s2, __fmaf_rn(c.t[1 * 3 + 2], sY[j], c.t[1 * 3 + 1] * sX[j]));
+                    const float y_ = __fmaf_rn(c.t[2 * 3 + 0], s2, __fmaf_rn(c.t[2 * 3 + 2], sY[j], c.t[2 * 3 + 1] * sX[j]));
+                    bM[j] = top ? endM : m_;
+                    bX[j] = top ? endX : x_;
+                    bY[j] = top ? endY : y_;
                 }
-                float bM[C], bX[C], bY[C];
-                {
-                    float sX[C], sY[C];
-                    if (par) {  // odd d: gap-x successor slot i+1, gap-y successor slot i
-                        const float nb = fromNext<L>(gX[0], gl);
-#pragma unroll
-                        for (int j = 0; j < C; j++) {
-                            sX[j] = (j < C - 1) ? gX[j + 1] : nb;
-                            sY[j] = gY[j];
-                        }
-                    } else {  // even d: gap-x successor slot i, gap-y successor slot i-1
-                        const float nb = fromPrev<L>(gY[C - 1], gl);
-#pragma unroll
-                        for (int j = 0; j < C; j++) {
-                            sX[j] = gX[j];
-                            sY[j] = (j > 0) ? gY[j - 1] : nb;
-                        }
-                    }
-                    const bool top = d == wk.D;  // the walk's first diagonal holds the end probabilities
+            }
+            const bool post = on && d <= wk.tbFrom;
+            // total probability refresh: 1st, 11th, 21st ... posterior diagonal of the walk
+            const bool refresh = post && untilRefresh == 0;
+            if (FLAT || __any_sync(FULL_MASK, refresh)) {
+                // cells of d plus the match transitions crossing d (impl/pairwiseAligner.c:567-584)
+                float sM1[C];
+                if (kk > 0) {
 #pragma unroll
                     for (int j = 0; j < C; j++) {
-                        const float s2 = par ? gB[j] : gA[j];
-                        const float m_ = __fmaf_rn(c.t[0 * 3 + 0], s2, __fmaf_rn(c.t[0 * 3 + 2], sY[j], c.t[0 * 3 + 1] * sX[j]));
-                        const float x_ = __fmaf_rn(c.t[1 * 3 + 0], s2, __fmaf_rn(c.t[1 * 3 + 2], sY[j], c.t[1 * 3 + 1] * sX[j]));
-                        const float y_ = __fmaf_rn(c.t[2 * 3 + 0], s2, __fmaf_rn(c.t[2 * 3 + 2], sY[j], c.t[2 * 3 + 1] * sX[j]));
-                        bM[j] = top ? endM : m_;
-                        bX[j] = top ? endX : x_;
-                        bY[j] = top ? endY : y_;
+                        const float4 q = lds<float4>(laneA + (uint32_t) (((kk - 1) * S + j * L) * 16));
+                        sM1[j] = __fmaf_rn(c.t[2 * 3 + 0], q.z, __fmaf_rn(c.t[1 * 3 + 0], q.y, c.t[0 * 3 + 0] * q.x));
                     }
-                }
-                const bool post = on && d <= wk.tbFrom;
-                // total probability refresh: 1st, 11th, 21st ... posterior diagonal of the walk
-                const bool refresh = post && untilRefresh == 0;
-                if (__any_sync(FULL_MASK, refresh)) {
-                    // cells of d plus the match transitions crossing d (impl/pairwiseAligner.c:567-584)
-                    float sM1[C];
-                    if (kk > 0) {
-                        const float4 *cp = gm.cacheA + (size_t) (kk - 1) * S;
+                } else {
 #pragma unroll
-                        for (int j = 0; j < C; j++) {
-                            const float4 q = cp[j * L + gl];
-                            sM1[j] = __fmaf_rn(c.t[2 * 3 + 0], q.z, __fmaf_rn(c.t[1 * 3 + 0], q.y, c.t[0 * 3 + 0] * q.x));
-                        }
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < C; j++) sM1[j] = chkSM[j];
-                    }
-                    laneShift<C, L>(sM1, on ? inf.y : 0, gl);
-                    float part = 0.0f;
-#pragma unroll
-                    for (int j = 0; j < C; j++) {
-                        const float uMn = par ? gA[j] : gB[j];  // match u of d+1
-                        part = __fmaf_rn(f[j].x, bM[j], part);
-                        part = __fmaf_rn(f[j].y, bX[j], part);
-                        part = __fmaf_rn(f[j].z, bY[j], part);
-                        part = __fmaf_rn(uMn, sM1[j], part);
-                    }
-                    const float T = groupSum<L>(part);
-                    if (refresh) {
-                        untilRefresh = 10;
-                        if (T > 0.0f) {
-                            const int ex = exponentOf(T);
-                            Tm = T * pow2f(-ex);
-                            ET = Ef + Eb + ex;
-                        } else {
-                            Tm = 0.0f;
-                            ET = 0;
-                        }
-                        if (wk.atEnd && posts == 0) {
-                            logLik += Tm > 0.0f ? log((double) Tm) + (double) ET * 0.69314718055994530942 : -INFINITY;
-                        }
-                    }
+                    for (int j = 0; j < C; j++) sM1[j] = chkSM[j];
                 }
-                if (post) {
-                    posts++;
-                    untilRefresh--;
-                }
-                const bool emit = post && Tm > 0.0f;
-                if (__any_sync(FULL_MASK, emit)) {
-                    const int ex = max(-126, min(127, Ef + Eb - ET));
-                    const float scale = emit ? __fdividef(pow2f(ex), Tm) : 0.0f;
-                    float p[3][C];
-#pragma unroll
-                    for (int j = 0; j < C; j++) {
-                        p[0][j] = (f[j].x * bM[j]) * scale;
-                        p[1][j] = (f[j].y * bX[j]) * scale;
-                        p[2][j] = (f[j].z * bY[j]) * scale;
-                    }
-                    emitDiagonal<C, L>(gl, o, p, thr, slotX0(d, inf.x), d, emit);
-                }
-                // u-values of d (emissions are zero outside the band); kept when the diagonal is off
+                if (!FLAT) laneShift<C, L>(sM1, on ? inf.y : 0, gl);
+                float part = 0.0f;
 #pragma unroll
                 for (int j = 0; j < C; j++) {
-                    const float ux = e[j].x * bX[j], uy = e[j].y * bY[j], um = f[j].w * bM[j];
-                    gX[j] = on ? ux : gX[j];
-                    gY[j] = on ? uy : gY[j];
-                    if (par) gB[j] = on ? um : gB[j]; else gA[j] = on ? um : gA[j];
+                    const float uMn = PAR ? gA[j] : gB[j];  // match u of d+1
+                    part = __fmaf_rn(f[j].x, bM[j], part);
+                    part = __fmaf_rn(f[j].y, bX[j], part);
+                    part = __fmaf_rn(f[j].z, bY[j], part);
+                    part = __fmaf_rn(uMn, sM1[j], part);
                 }
+                const float T = groupSum<L>(part);
+                const int ex = exponentOf(T);
+                const float tm = T > 0.0f ? T * pow2f(-ex) : 0.0f;
+                const int et = T > 0.0f ? Ef + Eb + ex : 0;
+                const bool first = refresh && wk.atEnd && posts == 0;
+                llTm = first ? tm : llTm;
+                llET = first ? et : llET;
+                llSet = llSet || first;
+                Tm = refresh ? tm : Tm;
+                ET = refresh ? et : ET;
+            }
+            untilRefresh = refresh ? 9 : untilRefresh - (post ? 1 : 0);
+            posts += post ? 1 : 0;
+            const bool emit = post && Tm > 0.0f;
+            if (FLAT || __any_sync(FULL_MASK, emit)) {
+                const int ex = max(-126, min(127, Ef + Eb - ET));
+                const float scale = emit ? __fdividef(pow2f(ex), Tm) : 0.0f;
+                float p[3][C];
+#pragma unroll
+                for (int j = 0; j < C; j++) {
+                    p[0][j] = (f[j].x * bM[j]) * scale;
+                    p[1][j] = (f[j].y * bX[j]) * scale;
+                    p[2][j] = (f[j].z * bY[j]) * scale;
+                }
+                if (FLAT) emitDiagonalFlat<C, L>(gl, o, p, thr, slotX0(d, inf.x), d, emit);
+                else emitDiagonal<C, L>(gl, o, p, thr, slotX0(d, inf.x), d, emit);
+            }
+            // u-values of d (emissions are zero outside the band); kept when the diagonal is off
+#pragma unroll
+            for (int j = 0; j < C; j++) {
+                const float ux = e[j].x * bX[j], uy = e[j].y * bY[j], um = f[j].w * bM[j];
+                gX[j] = on ? ux : gX[j];
+                gY[j] = on ? uy : gY[j];
+                if (PAR) gB[j] = on ? um : gB[j]; else gA[j] = on ? um : gA[j];
+            }
+            if (!FLAT) {
                 // moving below d crosses the window shift met when entering d
-                const int back = on ? -inf.y : 0;
-                if (__any_sync(FULL_MASK, back != 0)) {
-                    laneShift<C, L>(gX, back, gl);
-                    laneShift<C, L>(gY, back, gl);
-                    laneShift<C, L>(gA, back, gl);
-                    laneShift<C, L>(gB, back, gl);
+                const int backShift = on ? -inf.y : 0;
+                if (__any_sync(FULL_MASK, backShift != 0)) {
+                    laneShift<C, L>(gX, backShift, gl);
+                    laneShift<C, L>(gY, backShift, gl);
+                    laneShift<C, L>(gA, backShift, gl);
+                    laneShift<C, L>(gB, backShift, gl);
                 }
+            }
+        };
+        const auto odd = std::integral_constant<int, 1>{};
+        const auto even = std::integral_constant<int, 0>{};
+        if (flat && __all_sync(FULL_MASK, dStart > wk.tbTo)) {
+#pragma unroll 1
+            for (int k = K - 2; k >= 0; k -= 2) {
+                back(odd, std::true_type{}, k + 1);
+                back(even, std::true_type{}, k);
+            }
+        } else {
+#pragma unroll 1
+            for (int k = K - 2; k >= 0; k -= 2) {
+                back(odd, std::false_type{}, k + 1);
+                back(even, std::false_type{}, k);
             }
         }
         // rescale the carried backward state at the block boundary
@@ -806,6 +926,7 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
         }
         __syncwarp();
     }
+    if (llSet) logLik += llTm > 0.0f ? log((double) llTm) + (double) llET * 0.69314718055994530942 : -INFINITY;
 }
 
 // Next traceback point of a group's task: the first anti-diagonal d in [from, N) whose band
@@ -821,7 +942,7 @@ __device__ __forceinline__ int nextTracePoint(const Ctx &c, int from, int maxWid
         bool ok = false;
         if (look && d < c.N) {
             const int2 bd = *reinterpret_cast<const int2 *>(c.band + d);
-            ok = ((bd.y - bd.x) >> 1) + 1 <= maxWidth;
+            ok = bd.y - bd.x + 1 <= maxWidth;
         }
         const unsigned bits = groupBits<L>(__ballot_sync(FULL_MASK, ok), c.g);
         if (look) {
@@ -842,10 +963,10 @@ __device__ __forceinline__ int nextTracePoint(const Ctx &c, int from, int maxWid
 // ---------------------------------------------------------------------------
 
 template <int C, int L, int K>
-__device__ __forceinline__ void runGroup(const DpArgs &a, const float *rpAll, const float *smAll, const float *gxAll,
-                                         const float *gyAll, int taskIndex, GroupMem<C, L, K> &gm, const Scratch &sc) {
+__device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMem<C, L, K> &gm, const Scratch &sc) {
     constexpr int S = L * C;
     constexpr int R = RingSize<S>::R;
+    constexpr bool kSolo = L == 32;  // one task per warp: every lane is always on
     const int lane = threadIdx.x & 31;
     const bool has = taskIndex >= 0;
     const Task *tk = a.tasks + (has ? taskIndex : 0);
@@ -864,10 +985,8 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, const float *rpAll, co
     const DevModel &dm = a.models[model];
 #pragma unroll
     for (int k = 0; k < 9; k++) c.t[k] = dm.t[k];
-    c.rp = reinterpret_cast<const char *>(rpAll + (a.sharedRepeat ? 0 : model * kRepTable));
-    c.sm = smAll + model * 25;
-    c.gx = gxAll + model * 5;
-    c.gy = gyAll + model * 5;
+    c.model = (uint32_t) model;
+    c.repOff = kRepBase + (a.sharedRepeat ? 0u : (uint32_t) model * (uint32_t) (kRepTable * sizeof(float)));
     c.rle = dm.runLength;
     c.strandFwd = dm.strand;
     const int status0 = has ? to->status : 0;
@@ -907,7 +1026,7 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, const float *rpAll, co
 #pragma unroll
         for (int q = c.gl; q < 32; q += L) {
             const int dd = chunk * 32 + q;
-            if (live && dd <= myN) cpAsync16(&gm.bandRing[dd & 63], &c.band[dd]);
+            if (live && dd <= myN) cpAsync16(gm.bandRing + ((dd & 63) << 4), &c.band[dd]);
         }
         cpAsyncCommit();
     };
@@ -920,7 +1039,7 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, const float *rpAll, co
     Slots<C> sy;
     int Q = 0;
     if (live) {
-        const int4 b0 = gm.bandRing[0];
+        const int4 b0 = lds<int4>(gm.bandRing);
         Q = initialWindow<S>(b0.z, b0.w);
     }
     int Ef = 0;
@@ -929,47 +1048,80 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, const float *rpAll, co
         const int x0 = slotX0(0, Q);
         ringEnsure<R, L, true>(c, gm.rx, x0 - 1 - 8, x0 + S - 2, true, true);
         ringEnsure<R, L, false>(c, gm.ry, -x0 - S - 8, -x0 - 1, true, true);
-        forwardOrigin<C, L, false>(c, wk.startP, Q, st, nullptr, nullptr);
+        forwardOrigin<C, L, false>(c, wk.startP, Q, st, 0, 0);
+        loadSlots<C, R>(c.gl, gm.rx, gm.ry, 0, Q, sy);
     }
-    bool have = false;
     int checkAt = 1;
-    for (int d = 1; d <= Nmax; d++) {
-        const bool on = d <= myN;
-        if ((d & 31) == 0) {
-            issueChunk((d >> 5) + 1);
+    // One anti-diagonal of the sweep; the parity is a compile-time constant, and the band
+    // chunk and checkpoint boundaries (multiples of 32 and of K) fall on even diagonals.
+    // One anti-diagonal with the window and ring checks (PAR = d & 1).
+    auto checkedStep = [&](auto parity, int d) {
+        constexpr int PAR = decltype(parity)::value;
+        const bool on = kSolo || d <= myN;
+        const int4 bd = lds<int4>(gm.bandRing + ((d & 63) << 4));
+        const bool move = on && (bd.z < Q || bd.w > Q + S - 1);
+        const bool rare = __any_sync(FULL_MASK, move || (on && d >= checkAt));
+        bool reload = false;
+        if (rare) {
+            const int dl = move ? windowShift<C, S>(Q, bd.z, bd.w, bad) : 0;
+            if (__any_sync(FULL_MASK, dl != 0)) {
+                shiftFwd<C, L>(st, dl, c.gl);
+                if (dl != 0) {
+                    Q += C * dl;
+                    reload = true;
+                }
+            }
+            checkAt = ensureRings<R, L, S>(c, gm.rx, gm.ry, d, Q, true, on);
+        }
+        stepSlots<C, L, R, PAR>(c.gl, gm.rx, gm.ry, d, Q, sy);
+        if (rare && reload) loadSlots<C, R>(c.gl, gm.rx, gm.ry, d, Q, sy);
+        forwardDiagonal<C, L, PAR, false>(c, st, sy, bd.x - Q, bd.y - Q, 0, 0);
+    };
+    const auto odd = std::integral_constant<int, 1>{};
+    const auto even = std::integral_constant<int, 0>{};
+    // diagonals 1 .. K-1
+    for (int d = 1; d < K && d <= Nmax; d++) {
+        if (d & 1) checkedStep(odd, d); else checkedStep(even, d);
+    }
+    // Checkpoint blocks [d0, d0+K-1]. A block where no group's window moves, no ring runs
+    // out and every group is on runs without checks or branches, so the diagonals' symbol
+    // and emission loads overlap the previous diagonals' arithmetic.
+    for (int d0 = K; d0 <= Nmax; d0 += K) {
+        if ((d0 & 31) == 0) {
+            issueChunk((d0 >> 5) + 1);
             cpAsyncWaitAllButOne();
             __syncwarp();
         }
-        if ((d & (K - 1)) == 0) {
-            Ef += rescaleFwd<C, L>(st);
-            if (on) {
-                const int b = d / K;
-                storeFwd<C, L>(sc.chk + (size_t) b * S, c.gl, st);
-                if (c.gl == 0) sc.scal[b] = make_int2(Ef, Q);
-            }
+        Ef += rescaleFwd<C, L>(st);
+        if (kSolo || d0 <= myN) {
+            storeFwd<C, L>(sc.chk + (size_t) (d0 / K) * S, c.gl, st);
+            if (c.gl == 0) sc.scal[d0 / K] = make_int2(Ef, Q);
         }
-        const int4 bd = gm.bandRing[d & 63];
-        const int dl = on ? windowShift<C, S>(Q, bd.z, bd.w, bad) : 0;
-        if (__any_sync(FULL_MASK, dl != 0)) {
-            shiftFwd<C, L>(st, dl, c.gl);
-            if (dl != 0) {
-                Q += C * dl;
-                have = false;
-                checkAt = d;
-            }
+        const int dLast = d0 + K - 1;
+        bool clear = dLast <= myN && dLast < checkAt;
+        if (c.gl < K) {
+            const int4 bd = lds<int4>(gm.bandRing + (((d0 + c.gl) & 63) << 4));
+            clear = clear && bd.z >= Q && bd.w <= Q + S - 1;
         }
-        if (__any_sync(FULL_MASK, on && d >= checkAt)) checkAt = ensureRings<R, L, S>(c, gm.rx, gm.ry, d, Q, true, on);
-        const int sLo = (bd.x >> 1) - Q, sHi = (bd.y >> 1) - Q;
-        if (d & 1) {
-            stepSlots<C, L, R, 1>(c.gl, gm.rx, gm.ry, d, Q, sy);
-            if (!have) loadSlots<C, R>(c.gl, gm.rx, gm.ry, d, Q, sy);
-            forwardDiagonal<C, L, 1, false>(c, st, sy, sLo, sHi, nullptr, nullptr);
+        if (__all_sync(FULL_MASK, clear)) {
+            // pairs (even, odd): one small loop body keeps the hot code in the instruction cache
+#pragma unroll 1
+            for (int d = d0; d < d0 + K; d += 2) {
+                const int2 b0 = lds<int2>(gm.bandRing + ((d & 63) << 4));
+                const int2 b1 = lds<int2>(gm.bandRing + (((d + 1) & 63) << 4));
+                stepSlots<C, L, R, 0>(c.gl, gm.rx, gm.ry, d, Q, sy);
+                forwardDiagonal<C, L, 0, false>(c, st, sy, b0.x - Q, b0.y - Q, 0, 0);
+                stepSlots<C, L, R, 1>(c.gl, gm.rx, gm.ry, d + 1, Q, sy);
+                forwardDiagonal<C, L, 1, false>(c, st, sy, b1.x - Q, b1.y - Q, 0, 0);
+            }
         } else {
-            stepSlots<C, L, R, 0>(c.gl, gm.rx, gm.ry, d, Q, sy);
-            if (!have) loadSlots<C, R>(c.gl, gm.rx, gm.ry, d, Q, sy);
-            forwardDiagonal<C, L, 0, false>(c, st, sy, sLo, sHi, nullptr, nullptr);
+            for (int kk = 0; kk < K; kk += 2) {
+                if (d0 + kk > Nmax) break;
+                checkedStep(even, d0 + kk);
+                if (d0 + kk + 1 > Nmax) break;
+                checkedStep(odd, d0 + kk + 1);
+            }
         }
-        have = true;
     }
     // drain the band prefetch groups before the ring is reused
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -1018,14 +1170,11 @@ __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
     using GS = GroupSmem<C, L, K>;
     constexpr int G = 32 / L;
     constexpr int R = RingSize<L * C>::R;
-    extern __shared__ __align__(16) unsigned char smemRaw[];
     const int nTables = a.sharedRepeat ? 1 : 2;
-    float *rp = reinterpret_cast<float *>(smemRaw);
-    float *sm = rp + nTables * kRepTable;
-    float *gx = sm + 2 * 25;
-    float *gy = gx + 2 * 5;
-    unsigned char *warpBase =
-        smemRaw + (((size_t) (nTables * kRepTable + 2 * 25 + 2 * 5 + 2 * 5) * sizeof(float) + 15) & ~(size_t) 15);
+    float *sm = reinterpret_cast<float *>(mpSmem + kMatchOff);
+    float *gx = reinterpret_cast<float *>(mpSmem + kGapXOff);
+    float *gy = reinterpret_cast<float *>(mpSmem + kGapYOff);
+    float *rp = reinterpret_cast<float *>(mpSmem + kRepBase);
     for (int i = threadIdx.x; i < nTables * kRepTable; i += blockDim.x) rp[i] = a.repeatProb[i];
     for (int i = threadIdx.x; i < 2 * 25; i += blockDim.x) sm[i] = a.models[i / 25].match[i % 25];
     for (int i = threadIdx.x; i < 2 * 5; i += blockDim.x) {
@@ -1038,17 +1187,15 @@ __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
     const int lane = threadIdx.x & 31;
     const int g = lane / L;
     const int gwarp = blockIdx.x * (blockDim.x >> 5) + warp;
-    unsigned char *mine = warpBase + ((size_t) warp * G + g) * GS::bytes;
+    const uint32_t mine = (uint32_t) tableBytes(nTables) + (uint32_t) ((warp * G + g) * GS::bytes);
     GroupMem<C, L, K> gm;
-    gm.rx = Ring<R>{reinterpret_cast<uint2 *>(mine), 0, 0};
-    gm.ry = Ring<R>{reinterpret_cast<uint2 *>(mine) + R, 0, 0};
-    gm.bandRing = reinterpret_cast<int4 *>(mine + GS::ringBytes);
-    gm.walkBand = reinterpret_cast<int4 *>(mine + GS::ringBytes + GS::bandRingBytes);
-    gm.cacheA = reinterpret_cast<float4 *>(mine + GS::ringBytes + GS::bandRingBytes + GS::walkBandBytes);
-    gm.cacheB = reinterpret_cast<float2 *>(mine + GS::ringBytes + GS::bandRingBytes + GS::walkBandBytes +
-                                           GS::cacheABytes);
-    gm.info = reinterpret_cast<int2 *>(mine + GS::ringBytes + GS::bandRingBytes + GS::walkBandBytes +
-                                       GS::cacheABytes + GS::cacheBBytes);
+    gm.rx = Ring<R>{mine, 0, 0};
+    gm.ry = Ring<R>{mine + (uint32_t) (R * sizeof(uint2)), 0, 0};
+    gm.bandRing = mine + (uint32_t) GS::ringBytes;
+    gm.walkBand = gm.bandRing + (uint32_t) GS::bandRingBytes;
+    gm.cacheA = gm.walkBand + (uint32_t) GS::walkBandBytes;
+    gm.cacheB = gm.cacheA + (uint32_t) GS::cacheABytes;
+    gm.info = gm.cacheB + (uint32_t) GS::cacheBBytes;
     Scratch sc;
     sc.blocks = a.scratchBlocks;
     const size_t slot = (size_t) gwarp * G + g;  // one checkpoint area per task slot
@@ -1062,7 +1209,7 @@ __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
         q = __shfl_sync(FULL_MASK, q, 0);
         if (q >= nLoads) break;
         const int t = q * G + g;
-        runGroup<C, L, K>(a, rp, sm, gx, gy, t < a.nTasks ? a.order[t] : -1, gm, sc);
+        runGroup<C, L, K>(a, t < a.nTasks ? a.order[t] : -1, gm, sc);
         __syncwarp();
     }
 }
@@ -1071,9 +1218,6 @@ __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
 // Launch wrappers
 // ---------------------------------------------------------------------------
 
-size_t tableBytes(int nTables) {
-    return (((size_t) (nTables * kRepTable + 2 * 25 + 2 * 5 + 2 * 5) * sizeof(float) + 15) & ~(size_t) 15);
-}
 
 template <int C, int L, int K>
 static size_t smemFor(int warps, int nTables) {
@@ -1099,7 +1243,7 @@ static cudaError_t launchT(const DpArgs &a, int blocks, int warps, cudaStream_t 
     X(1, 4, 16, 4, 8)  \
     X(2, 8, 8, 4, 5)   \
     X(3, 3, 32, 8, 8)  \
-    X(4, 4, 32, 4, 10) \
+    X(4, 4, 32, 4, 8)  \
     X(5, 6, 32, 4, 8)  \
     X(6, 8, 32, 4, 5)
 

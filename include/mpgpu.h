@@ -149,7 +149,9 @@ mp_status mp_engine_set_tuning(mp_engine *e, const mp_tuning *t);
 
 /* Full posterior pass over a batch of jobs held in host memory: host->device copies,
  * band construction, the persistent length-sorted posterior kernel, compaction and
- * device->host copies of the tuples. */
+ * device->host copies of the tuples. The engine keeps the device buffers of its last
+ * one-shot batch, so repeated calls of similar size allocate no device memory; calls on
+ * one engine are serialised. */
 mp_status mp_realign_batch(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
                            mp_result **out);
 mp_status mp_result_view_get(const mp_result *r, mp_result_view *v);
@@ -163,8 +165,29 @@ mp_status mp_device_batch_create(mp_engine *e, const mp_model *m, const mp_param
 /* Runs the posterior kernel(s) on the resident batch; outputs stay on the device.
  * If kernel_ms is non-NULL it receives the CUDA-event time of the posterior kernel(s). */
 mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, float *kernel_ms);
+/* Replaces the batch's jobs (and parameters), reusing its device buffers. */
+mp_status mp_device_batch_reset(mp_engine *e, mp_device_batch *db, const mp_params *p, const mp_batch *b);
 /* Copies the last run's results to the host. */
 mp_status mp_device_batch_fetch(mp_engine *e, mp_device_batch *db, mp_result **out);
+/* Caller-owned host arrays that receive a batch's results (mp_device_batch_fetch_into):
+ * offsets[k] has n_jobs + 1 entries, weight/x/y[k] have totals[k] entries, log_likelihood
+ * and cells have n_jobs entries. Any pointer except the tuple arrays of a non-empty list
+ * may be NULL. Page-locked arrays (mp_host_alloc) are filled by DMA at full link speed. */
+typedef struct {
+    int64_t *offsets[3];
+    int32_t *weight[3];
+    int32_t *x[3];
+    int32_t *y[3];
+    double *log_likelihood;
+    int64_t *cells;
+} mp_output;
+/* Tuples of each list produced by the last run. */
+mp_status mp_device_batch_counts(const mp_device_batch *db, int64_t totals[3]);
+/* Copies the last run's results into caller-owned host arrays (no allocation on the host). */
+mp_status mp_device_batch_fetch_into(mp_engine *e, mp_device_batch *db, const mp_output *out);
+/* Page-locked host memory for inputs and outputs (cudaHostAlloc / cudaFreeHost). */
+mp_status mp_host_alloc(size_t bytes, void **out);
+void mp_host_free(void *p);
 /* Totals of the resident batch (cells = sum of band widths; launches per run). */
 mp_status mp_device_batch_stats(const mp_device_batch *db, int64_t *total_cells, int64_t *n_tasks,
                                 int32_t *kernel_launches_per_run);

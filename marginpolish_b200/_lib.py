@@ -100,6 +100,17 @@ class ResultView(Structure):
     ]
 
 
+class Output(Structure):
+    _fields_ = [
+        ("offsets", POINTER(c_int64) * 3),
+        ("weight", POINTER(c_int32) * 3),
+        ("x", POINTER(c_int32) * 3),
+        ("y", POINTER(c_int32) * 3),
+        ("log_likelihood", POINTER(c_double)),
+        ("cells", POINTER(c_int64)),
+    ]
+
+
 class NoallocOutput(Structure):
     _fields_ = [
         ("weight", POINTER(c_int32) * 3),
@@ -128,7 +139,8 @@ EXPORTED = [
     "mp_result_destroy", "mp_device_batch_create", "mp_device_batch_run", "mp_device_batch_fetch",
     "mp_device_batch_stats", "mp_device_batch_destroy", "mp_band", "mp_split_points", "mp_crop_range",
     "mp_rle_encode", "mp_rle_symbols", "mp_rle_anchors", "mp_device_batch_timing", "mp_measure_fp32_peak",
-    "mp_realign_single_noalloc",
+    "mp_realign_single_noalloc", "mp_device_batch_reset", "mp_device_batch_counts", "mp_device_batch_fetch_into",
+    "mp_host_alloc", "mp_host_free",
 ]
 
 _lib = None
@@ -161,6 +173,11 @@ def load() -> ctypes.CDLL:
         "mp_device_batch_fetch": (c_int, [c_void_p, c_void_p, P(c_void_p)]),
         "mp_device_batch_stats": (c_int, [c_void_p, P(c_int64), P(c_int64), P(c_int32)]),
         "mp_device_batch_destroy": (None, [c_void_p]),
+        "mp_device_batch_reset": (c_int, [c_void_p, c_void_p, P(Params), P(Batch)]),
+        "mp_device_batch_counts": (c_int, [c_void_p, P(c_int64)]),
+        "mp_device_batch_fetch_into": (c_int, [c_void_p, c_void_p, P(Output)]),
+        "mp_host_alloc": (c_int, [ctypes.c_size_t, P(c_void_p)]),
+        "mp_host_free": (None, [c_void_p]),
         "mp_device_batch_timing": (c_int, [c_void_p, P(c_float), P(c_float)]),
         "mp_measure_fp32_peak": (c_int, [c_void_p, P(c_double)]),
         "mp_realign_single_noalloc": (c_int, [c_void_p, c_void_p, P(Params), P(c_uint16), c_int64, P(c_uint16),

@@ -17,6 +17,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -118,6 +120,8 @@ extern "C" void mp_engine_destroy(mp_engine *e) {
     cudaSetDevice(e->device);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
+    mp_device_batch_destroy(e->oneShot);
+    e->oneShot = nullptr;
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }
@@ -430,6 +434,7 @@ struct PlannedTask {
 
 struct mp_device_batch {
     mp_engine *e = nullptr;
+    int device = -1;
     const mp_model *m = nullptr;
     mp_params p{};
     int64_t nJobs = 0;
@@ -442,6 +447,7 @@ struct mp_device_batch {
     // device
     DevBuf xs, ys, anchors, dTasks, band, dOut, outW[3], outX[3], outY[3];
     DevBuf orders, queue, scratch, scratchScal;
+    DevBuf fetchDst[3], fetchW[3], fetchX[3], fetchY[3], fetchPtrs;  // compaction staging (reused)
     std::vector<int> varOrderOff;  // per variant offset into orders
     std::vector<int> varCount;
     std::vector<int64_t> varMaxN;
@@ -670,51 +676,61 @@ static mp_status upload(DevBuf &buf, const void *src, size_t bytes, cudaStream_t
     return MP_OK;
 }
 
-extern "C" mp_status mp_device_batch_create(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
-                                            mp_device_batch **out) {
-    if (!e || !m || !b || !out) return failf(MP_ERR_ARGUMENT, "mp_device_batch_create: NULL argument");
-    *out = nullptr;
+// Plans a batch into `db` and uploads it, reusing the device buffers db already holds
+// (they only grow).
+static mp_status batchReset(mp_engine *e, mp_device_batch *db, const mp_model *m, const mp_params *p,
+                            const mp_batch *b) {
     MP_TRY(validateParams(p));
     if (b->n_jobs < 0) return failf(MP_ERR_ARGUMENT, "negative job count");
     if (b->n_jobs > 0 && (!b->x_begin || !b->x_end || !b->y_offsets || !b->anchor_offsets || !b->strand))
         return failf(MP_ERR_ARGUMENT, "batch arrays missing");
     CUDA_TRY(cudaSetDevice(e->device));
-    mp_device_batch *db = new mp_device_batch();
     db->e = e;
+    db->device = e->device;
     db->m = m;
     db->p = *p;
     db->nJobs = b->n_jobs;
-    mp_status s = planBatch(db, b);
-    if (s != MP_OK) {
-        delete db;
-        return s;
-    }
+    db->ran = false;
+    db->hostOut.clear();
+    MP_TRY(planBatch(db, b));
     cudaStream_t st = e->stream;
     int64_t ny = b->n_jobs > 0 ? b->y_offsets[b->n_jobs] : 0;
     int64_t na = b->n_jobs > 0 ? b->anchor_offsets[b->n_jobs] : 0;
-    s = upload(db->xs, b->x_symbols, sizeof(uint16_t) * b->x_symbols_length, st);
-    if (s == MP_OK) s = upload(db->ys, b->y_symbols, sizeof(uint16_t) * ny, st);
-    if (s == MP_OK) s = upload(db->anchors, b->anchors, sizeof(int32_t) * 3 * na, st);
-    if (s == MP_OK) s = upload(db->dTasks, db->tasks.data(), sizeof(Task) * db->tasks.size(), st);
-    if (s == MP_OK) s = db->band.reserve(sizeof(int4) * std::max<int64_t>(db->totalDiags, 1));
-    if (s == MP_OK) s = db->dOut.reserve(sizeof(TaskOut) * std::max<size_t>(db->tasks.size(), 1));
-    for (int k = 0; k < 3 && s == MP_OK; k++) {
+    MP_TRY(upload(db->xs, b->x_symbols, sizeof(uint16_t) * b->x_symbols_length, st));
+    MP_TRY(upload(db->ys, b->y_symbols, sizeof(uint16_t) * ny, st));
+    MP_TRY(upload(db->anchors, b->anchors, sizeof(int32_t) * 3 * na, st));
+    MP_TRY(upload(db->dTasks, db->tasks.data(), sizeof(Task) * db->tasks.size(), st));
+    MP_TRY(db->band.reserve(sizeof(int4) * std::max<int64_t>(db->totalDiags, 1)));
+    MP_TRY(db->dOut.reserve(sizeof(TaskOut) * std::max<size_t>(db->tasks.size(), 1)));
+    for (int k = 0; k < 3; k++) {
         size_t n = sizeof(int32_t) * std::max<int64_t>(db->outCap[k], 1);
-        s = db->outW[k].reserve(n);
-        if (s == MP_OK) s = db->outX[k].reserve(n);
-        if (s == MP_OK) s = db->outY[k].reserve(n);
+        MP_TRY(db->outW[k].reserve(n));
+        MP_TRY(db->outX[k].reserve(n));
+        MP_TRY(db->outY[k].reserve(n));
     }
-    if (s == MP_OK) s = db->queue.reserve(sizeof(int32_t) * variantCount());
-    if (s == MP_OK) {
-        cudaError_t ce = cudaStreamSynchronize(st);
-        if (ce != cudaSuccess) s = failf(MP_ERR_CUDA, "upload failed: %s", cudaGetErrorString(ce));
-    }
+    MP_TRY(db->queue.reserve(sizeof(int32_t) * variantCount()));
+    // the caller's host arrays may be reused as soon as this returns
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return MP_OK;
+}
+
+extern "C" mp_status mp_device_batch_create(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
+                                            mp_device_batch **out) {
+    if (!e || !m || !p || !b || !out) return failf(MP_ERR_ARGUMENT, "mp_device_batch_create: NULL argument");
+    *out = nullptr;
+    mp_device_batch *db = new mp_device_batch();
+    mp_status s = batchReset(e, db, m, p, b);
     if (s != MP_OK) {
         delete db;
         return s;
     }
     *out = db;
     return MP_OK;
+}
+
+extern "C" mp_status mp_device_batch_reset(mp_engine *e, mp_device_batch *db, const mp_params *p, const mp_batch *b) {
+    if (!e || !db || !p || !b) return failf(MP_ERR_ARGUMENT, "mp_device_batch_reset: NULL argument");
+    return batchReset(e, db, db->m, p, b);
 }
 
 // Launches the posterior kernels for the current queues (one persistent launch per
@@ -946,104 +962,138 @@ extern "C" mp_status mp_device_batch_stats(const mp_device_batch *db, int64_t *c
 struct mp_result {
     int64_t nJobs = 0;
     std::vector<int64_t> off[3];
-    std::vector<int32_t> w[3], x[3], y[3];
+    int64_t n[3] = {0, 0, 0};
+    std::unique_ptr<int32_t[]> w[3], x[3], y[3];
     std::vector<double> logLik;
     std::vector<int64_t> cells;
     int64_t totalCells = 0;
     double deviceMs = 0.0;
 };
 
-extern "C" mp_status mp_device_batch_fetch(mp_engine *e, mp_device_batch *db, mp_result **out) {
-    if (!e || !db || !out) return failf(MP_ERR_ARGUMENT, "mp_device_batch_fetch: NULL argument");
-    if (!db->ran) return failf(MP_ERR_STATE, "mp_device_batch_fetch before a successful run");
-    CUDA_TRY(cudaSetDevice(e->device));
-    cudaStream_t st = e->stream;
+// Per-job offsets of the compacted tuple lists and the per-task destinations.
+static void fetchLayout(const mp_device_batch *db, int64_t total[3], std::vector<int64_t> dst[3],
+                        int64_t *const off[3], double *logLik, int64_t *cells) {
     const int nTasks = (int) db->tasks.size();
-    mp_result *r = new mp_result();
-    r->nJobs = db->nJobs;
-    std::vector<int64_t> dst[3];
-    int64_t total[3] = {0, 0, 0};
     for (int k = 0; k < 3; k++) {
+        total[k] = 0;
         dst[k].resize(std::max(nTasks, 1));
-        r->off[k].assign(db->nJobs + 1, 0);
+        if (off[k]) off[k][0] = 0;
     }
-    r->logLik.assign(db->nJobs, 0.0);
-    r->cells.assign(db->nJobs, 0);
     for (int64_t j = 0; j < db->nJobs; j++) {
+        double ll = 0.0;
+        int64_t c = 0;
         for (int64_t t = db->jobFirstTask[j]; t < db->jobFirstTask[j + 1]; t++) {
             const TaskOut &o = db->hostOut[t];
             for (int k = 0; k < 3; k++) {
                 dst[k][t] = total[k];
                 total[k] += o.count[k];
             }
-            r->logLik[j] += o.logLik;
-            r->cells[j] += o.cells;
+            ll += o.logLik;
+            c += o.cells;
         }
-        for (int k = 0; k < 3; k++) r->off[k][j + 1] = total[k];
-        r->totalCells += r->cells[j];
+        for (int k = 0; k < 3; k++)
+            if (off[k]) off[k][j + 1] = total[k];
+        if (logLik) logLik[j] = ll;
+        if (cells) cells[j] = c;
     }
-    DevBuf dDst[3], fW[3], fX[3], fY[3], ptrs;
-    mp_status s = MP_OK;
-    for (int k = 0; k < 3 && s == MP_OK; k++) {
-        s = upload(dDst[k], dst[k].data(), sizeof(int64_t) * dst[k].size(), st);
-        size_t n = sizeof(int32_t) * std::max<int64_t>(total[k], 1);
-        if (s == MP_OK) s = fW[k].reserve(n);
-        if (s == MP_OK) s = fX[k].reserve(n);
-        if (s == MP_OK) s = fY[k].reserve(n);
-    }
-    int32_t *hp[12];
+}
+
+// Compacts every task's tuples into the batch's staging lists and copies them into the
+// caller's host arrays (page-locked ones are copied by DMA at full link speed).
+static mp_status fetchInto(mp_engine *e, mp_device_batch *db, const mp_output *out) {
+    if (!db->ran) return failf(MP_ERR_STATE, "fetch before a successful run");
+    CUDA_TRY(cudaSetDevice(e->device));
+    cudaStream_t st = e->stream;
+    const int nTasks = (int) db->tasks.size();
+    int64_t total[3];
+    std::vector<int64_t> dst[3];
+    fetchLayout(db, total, dst, out->offsets, out->log_likelihood, out->cells);
     for (int k = 0; k < 3; k++) {
-        hp[k] = db->outW[k].as<int32_t>();
-        hp[3 + k] = db->outX[k].as<int32_t>();
-        hp[6 + k] = db->outY[k].as<int32_t>();
+        if (total[k] > 0 && (!out->weight[k] || !out->x[k] || !out->y[k]))
+            return failf(MP_ERR_ARGUMENT, "output arrays of list %d missing", k);
+        MP_TRY(upload(db->fetchDst[k], dst[k].data(), sizeof(int64_t) * dst[k].size(), st));
+        const size_t n = sizeof(int32_t) * std::max<int64_t>(total[k], 1);
+        MP_TRY(db->fetchW[k].reserve(n));
+        MP_TRY(db->fetchX[k].reserve(n));
+        MP_TRY(db->fetchY[k].reserve(n));
     }
-    int32_t *fp[9];
+    int32_t *all[18];
     for (int k = 0; k < 3; k++) {
-        fp[k] = fW[k].as<int32_t>();
-        fp[3 + k] = fX[k].as<int32_t>();
-        fp[6 + k] = fY[k].as<int32_t>();
+        all[k] = db->outW[k].as<int32_t>();
+        all[3 + k] = db->outX[k].as<int32_t>();
+        all[6 + k] = db->outY[k].as<int32_t>();
+        all[9 + k] = db->fetchW[k].as<int32_t>();
+        all[12 + k] = db->fetchX[k].as<int32_t>();
+        all[15 + k] = db->fetchY[k].as<int32_t>();
     }
-    if (s == MP_OK) s = ptrs.reserve(sizeof(int32_t *) * 18);
-    if (s == MP_OK) {
-        int32_t *all[18];
-        for (int i = 0; i < 9; i++) all[i] = hp[i];
-        for (int i = 0; i < 9; i++) all[9 + i] = fp[i];
-        cudaError_t ce = cudaMemcpyAsync(ptrs.p, all, sizeof(all), cudaMemcpyHostToDevice, st);
-        if (ce != cudaSuccess) s = failf(MP_ERR_CUDA, "pointer upload failed: %s", cudaGetErrorString(ce));
+    MP_TRY(upload(db->fetchPtrs, all, sizeof(all), st));
+    if (nTasks > 0) {
+        int32_t *const *dp = db->fetchPtrs.as<int32_t *>();
+        CUDA_TRY(launchCompact(db->dTasks.as<Task>(), db->dOut.as<TaskOut>(), nTasks, db->fetchDst[0].as<int64_t>(),
+                               db->fetchDst[1].as<int64_t>(), db->fetchDst[2].as<int64_t>(), dp, dp + 3, dp + 6,
+                               dp + 9, dp + 12, dp + 15, st));
     }
-    if (s == MP_OK) {
-        int32_t *const *dp = ptrs.as<int32_t *>();
-        cudaError_t ce = launchCompact(db->dTasks.as<Task>(), db->dOut.as<TaskOut>(), nTasks, dDst[0].as<int64_t>(),
-                                       dDst[1].as<int64_t>(), dDst[2].as<int64_t>(), dp, dp + 3, dp + 6, dp + 9,
-                                       dp + 12, dp + 15, st);
-        if (ce != cudaSuccess) s = failf(MP_ERR_CUDA, "compaction launch failed: %s", cudaGetErrorString(ce));
+    for (int k = 0; k < 3; k++) {
+        if (!total[k]) continue;
+        const size_t n = sizeof(int32_t) * total[k];
+        CUDA_TRY(cudaMemcpyAsync(out->weight[k], db->fetchW[k].p, n, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(out->x[k], db->fetchX[k].p, n, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(out->y[k], db->fetchY[k].p, n, cudaMemcpyDeviceToHost, st));
     }
-    for (int k = 0; k < 3 && s == MP_OK; k++) {
-        r->w[k].resize(total[k]);
-        r->x[k].resize(total[k]);
-        r->y[k].resize(total[k]);
-        if (total[k]) {
-            cudaError_t ce = cudaMemcpyAsync(r->w[k].data(), fW[k].p, sizeof(int32_t) * total[k], cudaMemcpyDeviceToHost, st);
-            if (ce == cudaSuccess) ce = cudaMemcpyAsync(r->x[k].data(), fX[k].p, sizeof(int32_t) * total[k], cudaMemcpyDeviceToHost, st);
-            if (ce == cudaSuccess) ce = cudaMemcpyAsync(r->y[k].data(), fY[k].p, sizeof(int32_t) * total[k], cudaMemcpyDeviceToHost, st);
-            if (ce != cudaSuccess) s = failf(MP_ERR_CUDA, "result download failed: %s", cudaGetErrorString(ce));
-        }
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return MP_OK;
+}
+
+extern "C" mp_status mp_device_batch_counts(const mp_device_batch *db, int64_t totals[3]) {
+    if (!db || !totals) return failf(MP_ERR_ARGUMENT, "mp_device_batch_counts: NULL argument");
+    if (!db->ran) return failf(MP_ERR_STATE, "counts before a successful run");
+    totals[0] = totals[1] = totals[2] = 0;
+    for (const TaskOut &o : db->hostOut)
+        for (int k = 0; k < 3; k++) totals[k] += o.count[k];
+    return MP_OK;
+}
+
+extern "C" mp_status mp_device_batch_fetch_into(mp_engine *e, mp_device_batch *db, const mp_output *out) {
+    if (!e || !db || !out) return failf(MP_ERR_ARGUMENT, "mp_device_batch_fetch_into: NULL argument");
+    return fetchInto(e, db, out);
+}
+
+extern "C" mp_status mp_device_batch_fetch(mp_engine *e, mp_device_batch *db, mp_result **out) {
+    if (!e || !db || !out) return failf(MP_ERR_ARGUMENT, "mp_device_batch_fetch: NULL argument");
+    *out = nullptr;
+    int64_t totals[3];
+    MP_TRY(mp_device_batch_counts(db, totals));
+    mp_result *r = new mp_result();
+    r->nJobs = db->nJobs;
+    mp_output o;
+    for (int k = 0; k < 3; k++) {
+        r->off[k].assign(db->nJobs + 1, 0);
+        r->n[k] = totals[k];
+        r->w[k].reset(new int32_t[std::max<int64_t>(totals[k], 1)]);  // filled by the copy, not zeroed
+        r->x[k].reset(new int32_t[std::max<int64_t>(totals[k], 1)]);
+        r->y[k].reset(new int32_t[std::max<int64_t>(totals[k], 1)]);
+        o.offsets[k] = r->off[k].data();
+        o.weight[k] = r->w[k].get();
+        o.x[k] = r->x[k].get();
+        o.y[k] = r->y[k].get();
     }
-    if (s == MP_OK) {
-        cudaError_t ce = cudaStreamSynchronize(st);
-        if (ce != cudaSuccess) s = failf(MP_ERR_CUDA, "fetch failed: %s", cudaGetErrorString(ce));
-    }
+    r->logLik.assign(db->nJobs, 0.0);
+    r->cells.assign(db->nJobs, 0);
+    o.log_likelihood = r->logLik.data();
+    o.cells = r->cells.data();
+    mp_status s = fetchInto(e, db, &o);
     if (s != MP_OK) {
         delete r;
         return s;
     }
+    for (int64_t c : r->cells) r->totalCells += c;
     *out = r;
     return MP_OK;
 }
 
 extern "C" void mp_device_batch_destroy(mp_device_batch *db) {
     if (!db) return;
-    if (db->e) cudaSetDevice(db->e->device);
+    if (db->device >= 0) cudaSetDevice(db->device);  // the engine may already be gone
     delete db;
 }
 
@@ -1052,9 +1102,9 @@ extern "C" mp_status mp_result_view_get(const mp_result *r, mp_result_view *v) {
     v->n_jobs = r->nJobs;
     for (int k = 0; k < 3; k++) {
         v->offsets[k] = r->off[k].data();
-        v->weight[k] = r->w[k].data();
-        v->x[k] = r->x[k].data();
-        v->y[k] = r->y[k].data();
+        v->weight[k] = r->w[k].get();
+        v->x[k] = r->x[k].get();
+        v->y[k] = r->y[k].get();
     }
     v->log_likelihood = r->logLik.data();
     v->cells = r->cells.data();
@@ -1067,16 +1117,31 @@ extern "C" void mp_result_destroy(mp_result *r) {
     delete r;
 }
 
+// One-shot calls reuse a batch cached in the engine, so repeated calls of similar size
+// allocate no device memory after the first.
 extern "C" mp_status mp_realign_batch(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
                                       mp_result **out) {
     if (!out) return failf(MP_ERR_ARGUMENT, "out is NULL");
     *out = nullptr;
-    mp_device_batch *db = nullptr;
-    MP_TRY(mp_device_batch_create(e, m, p, b, &db));
+    if (!e || !m || !p || !b) return failf(MP_ERR_ARGUMENT, "mp_realign_batch: NULL argument");
+    std::lock_guard<std::mutex> guard(e->oneShotLock);
+    if (!e->oneShot) e->oneShot = new mp_device_batch();
+    mp_device_batch *db = e->oneShot;
+    MP_TRY(batchReset(e, db, m, p, b));
     float ms = 0.0f;
-    mp_status s = mp_device_batch_run(e, db, &ms);
-    if (s == MP_OK) s = mp_device_batch_fetch(e, db, out);
-    if (s == MP_OK) (*out)->deviceMs = ms;
-    mp_device_batch_destroy(db);
-    return s;
+    MP_TRY(mp_device_batch_run(e, db, &ms));
+    MP_TRY(mp_device_batch_fetch(e, db, out));
+    (*out)->deviceMs = ms;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_host_alloc(size_t bytes, void **out) {
+    if (!out) return failf(MP_ERR_ARGUMENT, "mp_host_alloc: out is NULL");
+    *out = nullptr;
+    CUDA_TRY(cudaHostAlloc(out, bytes > 0 ? bytes : 1, cudaHostAllocPortable));
+    return MP_OK;
+}
+
+extern "C" void mp_host_free(void *p) {
+    if (p) cudaFreeHost(p);
 }

@@ -5,6 +5,7 @@
 #include "mp_internal.h"
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 
 // Records the thread-local error message of the C ABI and returns s.
@@ -67,6 +68,8 @@ struct mp_engine {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     mp_tuning tuning{};
+    struct mp_device_batch *oneShot = nullptr;  // reused by the one-shot calls (mp_realign_batch*)
+    std::mutex oneShotLock;
 };
 
 struct mp_model {

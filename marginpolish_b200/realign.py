@@ -17,6 +17,7 @@ are raised as MpError.
 from __future__ import annotations
 
 import ctypes
+import weakref
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
@@ -52,6 +53,10 @@ class Engine:
         return float(v.value)
 
     def close(self) -> None:
+        db = getattr(self, "_one_shot", None)
+        if db is not None:
+            db.close()
+            self._one_shot = None
         if self.handle:
             self._lib.mp_engine_destroy(self.handle)
             self.handle = None
@@ -224,18 +229,85 @@ def _copy_view(lib, res) -> Pairs:
     return Pairs(offsets, w, x, y, ll, cells, int(v.total_cells), float(v.device_ms))
 
 
-def realign_batch(engine: Engine, model: Model, params: AlignmentParams, jobs: Jobs) -> Pairs:
-    """Full posterior pass over a batch held in host memory (H2D, kernels, D2H inside)."""
-    lib = engine._lib
-    ps = params.struct()
-    bs = jobs.struct()
-    res = c_void_p()
-    _lib.check(lib.mp_realign_batch(engine.handle, model.handle, ctypes.byref(ps), ctypes.byref(bs),
-                                    ctypes.byref(res)))
-    try:
-        return _copy_view(lib, res)
-    finally:
-        lib.mp_result_destroy(res)
+def pinned_empty(shape, dtype) -> np.ndarray:
+    """An uninitialised numpy array in page-locked host memory (freed with the array); copies
+    between it and the device run by DMA at full link speed."""
+    lib = _lib.load()
+    dtype = np.dtype(dtype)
+    n = int(np.prod(shape)) * dtype.itemsize
+    p = c_void_p()
+    _lib.check(lib.mp_host_alloc(max(n, 1), ctypes.byref(p)))
+    buf = (ctypes.c_char * max(n, 1)).from_address(p.value)
+    arr = np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
+    weakref.finalize(buf, lib.mp_host_free, c_void_p(p.value))
+    return arr
+
+
+class OutputBuffer:
+    """Reusable host arrays for the results of batches (page-locked by default). A call that
+    writes into the buffer returns Pairs whose arrays are views of it, valid until the buffer
+    is used again."""
+
+    def __init__(self, pinned: bool = True):
+        self.pinned = pinned
+        self._tuples = [None, None, None]  # per list: (3, capacity) int32 rows weight, x, y
+        self._jobs = None                  # (offsets (3, n+1) int64, log_likelihood (n,), cells (n,))
+        self._n = -1
+
+    def _alloc(self, shape, dtype):
+        return pinned_empty(shape, dtype) if self.pinned else np.empty(shape, dtype)
+
+    def ensure(self, n_jobs: int, totals) -> None:
+        if self._n < n_jobs:
+            cap = max(n_jobs, int(self._n * 1.25) if self._n > 0 else 0)
+            self._jobs = (self._alloc((3, cap + 1), np.int64), self._alloc((cap,), np.float64),
+                          self._alloc((cap,), np.int64))
+            self._n = cap
+        for k in range(3):
+            need = int(totals[k])
+            t = self._tuples[k]
+            if t is None or t.shape[1] < need:
+                self._tuples[k] = self._alloc((3, max(need + need // 8, 1)), np.int32)
+
+    def struct(self) -> "_lib.Output":
+        o = _lib.Output()
+        offs, ll, cells = self._jobs
+        for k in range(3):
+            o.offsets[k] = _lib.ptr(offs[k], c_int64)
+            t = self._tuples[k]
+            o.weight[k] = _lib.ptr(t[0], c_int32)
+            o.x[k] = _lib.ptr(t[1], c_int32)
+            o.y[k] = _lib.ptr(t[2], c_int32)
+        o.log_likelihood = _lib.ptr(ll, ctypes.c_double)
+        o.cells = _lib.ptr(cells, c_int64)
+        return o
+
+    def pairs(self, n_jobs: int, totals, device_ms: float) -> Pairs:
+        offs, ll, cells = self._jobs
+        offsets = [offs[k, :n_jobs + 1] for k in range(3)]
+        w = [self._tuples[k][0, :int(totals[k])] for k in range(3)]
+        x = [self._tuples[k][1, :int(totals[k])] for k in range(3)]
+        y = [self._tuples[k][2, :int(totals[k])] for k in range(3)]
+        c = cells[:n_jobs]
+        return Pairs(offsets, w, x, y, ll[:n_jobs], c, int(c.sum()), device_ms)
+
+
+def realign_batch(engine: Engine, model: Model, params: AlignmentParams, jobs: Jobs,
+                  out: Optional[OutputBuffer] = None) -> Pairs:
+    """Full posterior pass over a batch held in host memory (H2D, kernels, D2H inside).
+
+    The engine keeps the device batch of its last call and reuses its buffers. Results go into
+    `out` when given (views valid until `out` is reused), else into new numpy arrays."""
+    db = getattr(engine, "_one_shot", None)
+    if db is None or db.model is not model:
+        if db is not None:
+            db.close()
+        db = DeviceBatch(engine, model, params, jobs)
+        engine._one_shot = db
+    else:
+        db.reset(jobs, params)
+    ms = db.run()
+    return db.fetch_into(out if out is not None else OutputBuffer(pinned=False), ms)
 
 
 class DeviceBatch:
@@ -263,6 +335,31 @@ class DeviceBatch:
             return _copy_view(lib, res)
         finally:
             lib.mp_result_destroy(res)
+
+    def reset(self, jobs: Jobs, params: Optional[AlignmentParams] = None) -> None:
+        """Replaces the jobs (and parameters), reusing the batch's device buffers."""
+        if params is not None:
+            self.params = params
+            self._ps = params.struct()
+        self.jobs = jobs
+        self._bs = jobs.struct()
+        _lib.check(self.engine._lib.mp_device_batch_reset(self.engine.handle, self.handle, ctypes.byref(self._ps),
+                                                          ctypes.byref(self._bs)))
+
+    def counts(self):
+        t = (c_int64 * 3)()
+        _lib.check(self.engine._lib.mp_device_batch_counts(self.handle, t))
+        return [int(t[0]), int(t[1]), int(t[2])]
+
+    def fetch_into(self, out: OutputBuffer, device_ms: float = 0.0) -> Pairs:
+        """Copies the last run's results into `out` (no host allocation when it is large
+        enough) and returns them as views of it."""
+        totals = self.counts()
+        n = self.jobs.n_jobs
+        out.ensure(n, totals)
+        o = out.struct()
+        _lib.check(self.engine._lib.mp_device_batch_fetch_into(self.engine.handle, self.handle, ctypes.byref(o)))
+        return out.pairs(n, totals, device_ms)
 
     def timing(self):
         """(band_ms, posterior_ms) CUDA-event times of the last run."""

@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work per baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--plain-reads", type=int, default=96, help="reads timed in the plain one-read-per-launch form")
     ap.add_argument("--lanes", type=int, default=0, choices=[0, 8, 16, 32],
                     help="lanes per banded sub-problem (0 = the engine's automatic choice)")
     ap.add_argument("--warps", type=int, default=0, help="warps per block of the posterior kernel (0 = automatic)")
@@ -158,10 +160,16 @@ def time_reference(jobs, cells, pm, seconds, steps=1, warmup=0):
         t = time.perf_counter()
         ref.align_batch(hf, hr, sample, pm.alignment, cores)
         times.append(time.perf_counter() - t)
+    # one core, on a sample of about a fifth of the time
+    one, one_cells = cpu_sample(jobs, cells, rate / cores * seconds * 0.2)
+    t = time.perf_counter()
+    ref.align_batch(hf, hr, one, pm.alignment, 1)
+    t1 = time.perf_counter() - t
     ref.free_model(hf)
     ref.free_model(hr)
     return {"gcups": sample_cells / statistics.median(times) / 1e9, "cores": cores, "reads": sample.n_jobs,
-            "cells": sample_cells, "seconds": statistics.median(times)}
+            "cells": sample_cells, "seconds": statistics.median(times),
+            "gcups_1core": one_cells / max(t1, 1e-9) / 1e9, "reads_1core": one.n_jobs}
 
 
 def run_reference_arm(args, rank, world):
@@ -322,6 +330,13 @@ def run_ours(args, rank, world, local):
                "ms_per_step": tt * 1e3}
         del e2e_t
 
+    # the plain one-read-per-launch form of the same kernel on the first reads of the batch
+    plain = None
+    if not args.no_plain and rank == 0:
+        p_ms, p_cells = db.run_plain(args.plain_reads)
+        plain = {"value": p_cells / (p_ms * 1e-3) / 1e9, "unit": "GCUPS", "reads": min(args.plain_reads, n_tasks),
+                 "cells": p_cells, "ms": p_ms, "form": "one launch of one warp per read, same kernel and accuracy",
+                 "batched_over_plain": (value / world) / (p_cells / (p_ms * 1e-3) / 1e9)}
     peak = engine.fp32_peak_tflops()
     post = float(np.median(post_ms))
     achieved = cells * FLOP_PER_CELL / (post * 1e-3) / 1e12
@@ -335,7 +350,8 @@ def run_ours(args, rank, world, local):
                 r = time_reference(jobs, cpc, pm, args.cpu_seconds)
                 cpu = {"value": r["gcups"], "unit": "GCUPS", "cores": r["cores"], "kind": "reference",
                        "sample": f"first {r['reads']} reads of the workload ({r['cells']} cells), "
-                                 f"OpenMP over reads on {r['cores']} threads"}
+                                 f"OpenMP over reads on {r['cores']} threads",
+                       "value_1core": r["gcups_1core"], "sample_1core": f"first {r['reads_1core']} reads, 1 thread"}
         line = {
             "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -352,6 +368,7 @@ def run_ours(args, rank, world, local):
                          "note": f"{FLOP_PER_CELL} flop per cell x cells / posterior-kernel event time; "
                                  "peak = FP32 FMA throughput measured live on this GPU (mp_measure_fp32_peak)"},
             "cpu_baseline": cpu,
+            "plain_gpu": plain,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

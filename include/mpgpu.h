@@ -196,6 +196,12 @@ void mp_device_batch_destroy(mp_device_batch *db);
 mp_status mp_device_batch_timing(const mp_device_batch *db, float *band_ms, float *posterior_ms);
 
 /* ---- measurement ---- */
+/* The plain one-read-per-launch form of the same kernel, for comparison with the batched
+ * launch: the first max_tasks sub-problems of the batch, each in its own launch of one warp,
+ * in batch order. kernel_ms receives the CUDA-event time of those launches and cells their
+ * band cells. The batch must be run again before its results are fetched. */
+mp_status mp_device_batch_run_plain(mp_engine *e, mp_device_batch *db, int64_t max_tasks, float *kernel_ms,
+                                    int64_t *cells);
 /* FP32 FMA throughput of the device measured with a dependent-chain-free FMA loop
  * (TFLOP/s, FMA = 2 flops), timed with CUDA events; the roofline denominator of the
  * posterior kernel, whose bound is the FP32 pipe. */

@@ -140,7 +140,7 @@ EXPORTED = [
     "mp_device_batch_stats", "mp_device_batch_destroy", "mp_band", "mp_split_points", "mp_crop_range",
     "mp_rle_encode", "mp_rle_symbols", "mp_rle_anchors", "mp_device_batch_timing", "mp_measure_fp32_peak",
     "mp_realign_single_noalloc", "mp_device_batch_reset", "mp_device_batch_counts", "mp_device_batch_fetch_into",
-    "mp_host_alloc", "mp_host_free",
+    "mp_host_alloc", "mp_host_free", "mp_device_batch_run_plain",
 ]
 
 _lib = None
@@ -178,6 +178,7 @@ def load() -> ctypes.CDLL:
         "mp_device_batch_fetch_into": (c_int, [c_void_p, c_void_p, P(Output)]),
         "mp_host_alloc": (c_int, [ctypes.c_size_t, P(c_void_p)]),
         "mp_host_free": (None, [c_void_p]),
+        "mp_device_batch_run_plain": (c_int, [c_void_p, c_void_p, c_int64, P(c_float), P(c_int64)]),
         "mp_device_batch_timing": (c_int, [c_void_p, P(c_float), P(c_float)]),
         "mp_measure_fp32_peak": (c_int, [c_void_p, P(c_double)]),
         "mp_realign_single_noalloc": (c_int, [c_void_p, c_void_p, P(Params), P(c_uint16), c_int64, P(c_uint16),

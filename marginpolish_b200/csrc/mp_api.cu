@@ -908,6 +908,95 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
     return MP_OK;
 }
 
+// The plain form of the same computation, for comparison: band kernels for the batch,
+// then one posterior launch per task (one block of one warp, no persistent queue), in
+// batch order, for the first max_tasks tasks. Returns the CUDA-event time of the
+// posterior launches and the cells of the tasks run.
+extern "C" mp_status mp_device_batch_run_plain(mp_engine *e, mp_device_batch *db, int64_t max_tasks, float *kernel_ms,
+                                               int64_t *cells) {
+    if (!e || !db) return failf(MP_ERR_ARGUMENT, "mp_device_batch_run_plain: NULL argument");
+    CUDA_TRY(cudaSetDevice(e->device));
+    cudaStream_t st = e->stream;
+    const int nTasks = (int) db->tasks.size();
+    const int n = (int) std::max<int64_t>(0, std::min<int64_t>(max_tasks, nTasks));
+    std::vector<int32_t> all(nTasks), orderHost;
+    for (int i = 0; i < nTasks; i++) all[i] = i;
+    MP_TRY(buildQueues(db, all, orderHost));
+    std::vector<int32_t> ident(std::max(nTasks, 1));
+    for (int i = 0; i < nTasks; i++) ident[i] = i;
+    MP_TRY(upload(db->orders, ident.data(), sizeof(int32_t) * ident.size(), st));
+    BandArgs ba;
+    ba.tasks = db->dTasks.as<Task>();
+    ba.nTasks = nTasks;
+    ba.anchors = db->anchors.as<int32_t>();
+    ba.band = db->band.as<int2>();
+    ba.out = db->dOut.as<TaskOut>();
+    if (nTasks) CUDA_TRY(launchBand(ba, st));
+    // scratch for one warp, sized for the longest task run
+    size_t needScratch = 0, needScal = 0;
+    int64_t maxN = 0;
+    for (int t = 0; t < n; t++) maxN = std::max<int64_t>(maxN, (int64_t) db->tasks[t].lx + db->tasks[t].ly);
+    for (int v = 0; v < variantCount(); v++) {
+        int C = 0, L = 0, K = 0;
+        variantShape(v, &C, &L, &K);
+        needScratch = std::max(needScratch, (size_t) (maxN / K + 2) * (size_t) (C * L) * sizeof(float4) * (32 / L));
+        needScal = std::max(needScal, sizeof(int2) * (size_t) (maxN / K + 2) * (32 / L));
+    }
+    CUDA_TRY(cudaStreamSynchronize(st));
+    MP_TRY(db->scratch.reserve(needScratch));
+    MP_TRY(db->scratchScal.reserve(needScal));
+    MP_TRY(db->queue.reserve(sizeof(int32_t) * std::max(n, 1)));
+    CUDA_TRY(cudaMemsetAsync(db->queue.p, 0, sizeof(int32_t) * std::max(n, 1), st));
+    CUDA_TRY(cudaEventRecord(e->ev0, st));
+    for (int t = 0; t < n; t++) {
+        int C = 0, L = 0, K = 0;
+        const int v = db->var[t];
+        variantShape(v, &C, &L, &K);
+        DpArgs a;
+        memset(&a, 0, sizeof(a));
+        a.tasks = db->dTasks.as<Task>();
+        a.order = db->orders.as<int32_t>() + t;
+        a.nTasks = 1;
+        a.scratchBlocks = (int32_t) (maxN / K + 2);
+        a.queue = db->queue.as<int32_t>() + t;
+        a.xs = db->xs.as<uint16_t>();
+        a.ys = db->ys.as<uint16_t>();
+        a.band = db->band.as<int2>();
+        a.models = db->m->models.as<DevModel>();
+        a.repeatProb = db->m->repeat.as<float>();
+        a.scratch = db->scratch.as<float4>();
+        a.scratchScalars = db->scratchScal.as<int2>();
+        for (int k = 0; k < 3; k++) {
+            a.outW[k] = db->outW[k].as<int32_t>();
+            a.outX[k] = db->outX[k].as<int32_t>();
+            a.outY[k] = db->outY[k].as<int32_t>();
+        }
+        a.out = db->dOut.as<TaskOut>();
+        a.threshold = (float) db->p.threshold;
+        a.minDiagsBetweenTraceBack = (int32_t) std::min<int64_t>(db->p.min_diags_between_traceback, 1 << 30);
+        a.traceBackDiagonals = (int32_t) db->p.traceback_diagonals;
+        a.diagonalExpansion = (int32_t) std::min<int64_t>(db->p.diagonal_expansion, 1 << 29);
+        a.sharedRepeat = db->m->sharedRepeat;
+        CUDA_TRY(launchVariant(v, a, 1, 1, st));
+    }
+    CUDA_TRY(cudaEventRecord(e->ev1, st));
+    std::vector<TaskOut> host(std::max(nTasks, 1));
+    if (nTasks) CUDA_TRY(cudaMemcpyAsync(host.data(), db->dOut.p, sizeof(TaskOut) * nTasks, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    float ms = 0.0f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+    int64_t c = 0;
+    for (int t = 0; t < n; t++) {
+        if (host[t].status != 0)
+            return failf(MP_ERR_OVERFLOW, "job %d: task status %d in the plain run", db->tasks[t].job, host[t].status);
+        c += host[t].cells;
+    }
+    db->ran = false;  // the batch's results now hold only the plain run's tasks
+    if (kernel_ms) *kernel_ms = ms;
+    if (cells) *cells = c;
+    return MP_OK;
+}
+
 extern "C" mp_status mp_device_batch_timing(const mp_device_batch *db, float *bandMs, float *posteriorMs) {
     if (!db) return failf(MP_ERR_ARGUMENT, "batch is NULL");
     if (bandMs) *bandMs = db->bandMs;

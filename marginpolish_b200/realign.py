@@ -346,6 +346,14 @@ class DeviceBatch:
         _lib.check(self.engine._lib.mp_device_batch_reset(self.engine.handle, self.handle, ctypes.byref(self._ps),
                                                           ctypes.byref(self._bs)))
 
+    def run_plain(self, max_tasks: int):
+        """The plain form: one launch of one warp per sub-problem for the first `max_tasks`
+        sub-problems. Returns (posterior-kernel ms, cells run)."""
+        ms, cells = c_float(0.0), c_int64(0)
+        _lib.check(self.engine._lib.mp_device_batch_run_plain(self.engine.handle, self.handle, int(max_tasks),
+                                                              ctypes.byref(ms), ctypes.byref(cells)))
+        return float(ms.value), int(cells.value)
+
     def counts(self):
         t = (c_int64 * 3)()
         _lib.check(self.engine._lib.mp_device_batch_counts(self.handle, t))

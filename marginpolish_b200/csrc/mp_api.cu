@@ -29,10 +29,7 @@ bool variantShape(int v, int *C, int *L, int *K);
 int variantMaxWarps(int v, int nTables);
 cudaError_t launchVariant(int v, const DpArgs &a, int blocks, int warps, cudaStream_t s);
 cudaError_t launchBand(const BandArgs &a, cudaStream_t s);
-cudaError_t launchCompact(const Task *tasks, const TaskOut *out, int nTasks, const int64_t *dst0,
-                          const int64_t *dst1, const int64_t *dst2, int32_t *const *srcW, int32_t *const *srcX,
-                          int32_t *const *srcY, int32_t *const *dstW, int32_t *const *dstX, int32_t *const *dstY,
-                          cudaStream_t s);
+cudaError_t launchCompact(const CompactArgs &a, cudaStream_t s);
 }  // namespace mp
 
 using namespace mp;
@@ -445,9 +442,9 @@ struct mp_device_batch {
     int64_t totalDiags = 0;
     int64_t outCap[3] = {0, 0, 0};
     // device
-    DevBuf xs, ys, anchors, dTasks, band, dOut, outW[3], outX[3], outY[3];
+    DevBuf xs, ys, anchors, dTasks, band, dOut, outT[3];  // outT: staged tuples per list
     DevBuf orders, queue, scratch, scratchScal;
-    DevBuf fetchDst[3], fetchW[3], fetchX[3], fetchY[3], fetchPtrs;  // compaction staging (reused)
+    DevBuf fetchDst[3], fetchW[3], fetchX[3], fetchY[3];  // compaction staging (reused)
     std::vector<int> varOrderOff;  // per variant offset into orders
     std::vector<int> varCount;
     std::vector<int64_t> varMaxN;
@@ -703,10 +700,7 @@ static mp_status batchReset(mp_engine *e, mp_device_batch *db, const mp_model *m
     MP_TRY(db->band.reserve(sizeof(int4) * std::max<int64_t>(db->totalDiags, 1)));
     MP_TRY(db->dOut.reserve(sizeof(TaskOut) * std::max<size_t>(db->tasks.size(), 1)));
     for (int k = 0; k < 3; k++) {
-        size_t n = sizeof(int32_t) * std::max<int64_t>(db->outCap[k], 1);
-        MP_TRY(db->outW[k].reserve(n));
-        MP_TRY(db->outX[k].reserve(n));
-        MP_TRY(db->outY[k].reserve(n));
+        MP_TRY(db->outT[k].reserve(sizeof(int4) * std::max<int64_t>(db->outCap[k], 1)));
     }
     MP_TRY(db->queue.reserve(sizeof(int32_t) * variantCount()));
     // the caller's host arrays may be reused as soon as this returns
@@ -783,11 +777,7 @@ static mp_status launchQueues(mp_device_batch *db) {
         a.repeatProb = db->m->repeat.as<float>();
         a.scratch = db->scratch.as<float4>();
         a.scratchScalars = db->scratchScal.as<int2>();
-        for (int k = 0; k < 3; k++) {
-            a.outW[k] = db->outW[k].as<int32_t>();
-            a.outX[k] = db->outX[k].as<int32_t>();
-            a.outY[k] = db->outY[k].as<int32_t>();
-        }
+        for (int k = 0; k < 3; k++) a.outT[k] = db->outT[k].as<int4>();
         a.out = db->dOut.as<TaskOut>();
         a.threshold = (float) db->p.threshold;
         a.minDiagsBetweenTraceBack = (int32_t) std::min<int64_t>(db->p.min_diags_between_traceback, 1 << 30);
@@ -869,18 +859,16 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
         if (!changed) break;
         // grow output buffers (preserving contents)
         for (int k = 0; k < 3; k++) {
-            size_t need = sizeof(int32_t) * db->outCap[k];
-            if (need > db->outW[k].bytes) {
-                DevBuf *bufs[3] = {&db->outW[k], &db->outX[k], &db->outY[k]};
-                for (DevBuf *bb : bufs) {
-                    void *np = nullptr;
-                    CUDA_TRY(cudaMalloc(&np, need));
-                    CUDA_TRY(cudaMemcpyAsync(np, bb->p, bb->bytes, cudaMemcpyDeviceToDevice, st));
-                    CUDA_TRY(cudaStreamSynchronize(st));
-                    cudaFree(bb->p);
-                    bb->p = np;
-                    bb->bytes = need;
-                }
+            size_t need = sizeof(int4) * db->outCap[k];
+            if (need > db->outT[k].bytes) {
+                DevBuf *bb = &db->outT[k];
+                void *np = nullptr;
+                CUDA_TRY(cudaMalloc(&np, need));
+                CUDA_TRY(cudaMemcpyAsync(np, bb->p, bb->bytes, cudaMemcpyDeviceToDevice, st));
+                CUDA_TRY(cudaStreamSynchronize(st));
+                cudaFree(bb->p);
+                bb->p = np;
+                bb->bytes = need;
             }
         }
         MP_TRY(upload(db->dTasks, db->tasks.data(), sizeof(Task) * nTasks, st));
@@ -966,11 +954,7 @@ extern "C" mp_status mp_device_batch_run_plain(mp_engine *e, mp_device_batch *db
         a.repeatProb = db->m->repeat.as<float>();
         a.scratch = db->scratch.as<float4>();
         a.scratchScalars = db->scratchScal.as<int2>();
-        for (int k = 0; k < 3; k++) {
-            a.outW[k] = db->outW[k].as<int32_t>();
-            a.outX[k] = db->outX[k].as<int32_t>();
-            a.outY[k] = db->outY[k].as<int32_t>();
-        }
+        for (int k = 0; k < 3; k++) a.outT[k] = db->outT[k].as<int4>();
         a.out = db->dOut.as<TaskOut>();
         a.threshold = (float) db->p.threshold;
         a.minDiagsBetweenTraceBack = (int32_t) std::min<int64_t>(db->p.min_diags_between_traceback, 1 << 30);
@@ -1106,21 +1090,19 @@ static mp_status fetchInto(mp_engine *e, mp_device_batch *db, const mp_output *o
         MP_TRY(db->fetchX[k].reserve(n));
         MP_TRY(db->fetchY[k].reserve(n));
     }
-    int32_t *all[18];
-    for (int k = 0; k < 3; k++) {
-        all[k] = db->outW[k].as<int32_t>();
-        all[3 + k] = db->outX[k].as<int32_t>();
-        all[6 + k] = db->outY[k].as<int32_t>();
-        all[9 + k] = db->fetchW[k].as<int32_t>();
-        all[12 + k] = db->fetchX[k].as<int32_t>();
-        all[15 + k] = db->fetchY[k].as<int32_t>();
-    }
-    MP_TRY(upload(db->fetchPtrs, all, sizeof(all), st));
     if (nTasks > 0) {
-        int32_t *const *dp = db->fetchPtrs.as<int32_t *>();
-        CUDA_TRY(launchCompact(db->dTasks.as<Task>(), db->dOut.as<TaskOut>(), nTasks, db->fetchDst[0].as<int64_t>(),
-                               db->fetchDst[1].as<int64_t>(), db->fetchDst[2].as<int64_t>(), dp, dp + 3, dp + 6,
-                               dp + 9, dp + 12, dp + 15, st));
+        CompactArgs ca;
+        ca.tasks = db->dTasks.as<Task>();
+        ca.out = db->dOut.as<TaskOut>();
+        ca.nTasks = nTasks;
+        for (int k = 0; k < 3; k++) {
+            ca.dst[k] = db->fetchDst[k].as<int64_t>();
+            ca.src[k] = db->outT[k].as<int4>();
+            ca.w[k] = db->fetchW[k].as<int32_t>();
+            ca.x[k] = db->fetchX[k].as<int32_t>();
+            ca.y[k] = db->fetchY[k].as<int32_t>();
+        }
+        CUDA_TRY(launchCompact(ca, st));
     }
     for (int k = 0; k < 3; k++) {
         if (!total[k]) continue;

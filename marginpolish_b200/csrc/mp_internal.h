@@ -74,15 +74,25 @@ struct DpArgs {
     const float *repeatProb;    // [2][4][51][51] exp(scale*log10 table), per model
     float4 *scratch;            // per task slot: checkpoints [block][window slot]
     int2 *scratchScalars;       // per task slot: (exponent, window) per checkpoint
-    int32_t *outW[3];
-    int32_t *outX[3];
-    int32_t *outY[3];
+    int4 *outT[3];              // per list: staged tuples (weight, x, y, 0) in per-task regions
     TaskOut *out;
     float threshold;
     int32_t minDiagsBetweenTraceBack;
     int32_t traceBackDiagonals;
     int32_t diagonalExpansion;
     int32_t sharedRepeat;       // both models use repeat table 0
+};
+
+// Compaction: task regions of the staged tuples -> per-job final lists.
+struct CompactArgs {
+    const Task *tasks;
+    const TaskOut *out;
+    int32_t nTasks;
+    const int64_t *dst[3];      // per list: first destination index of each task (NULL: 0)
+    const int4 *src[3];         // staged tuples (DpArgs::outT)
+    int32_t *w[3];
+    int32_t *x[3];
+    int32_t *y[3];
 };
 
 struct BandArgs {

@@ -157,22 +157,21 @@ __global__ void hullKernel(BandArgs a) {
 // per-job layout (tasks of a job are consecutive, in split order).
 // ---------------------------------------------------------------------------
 
-__global__ void compactKernel(const Task *tasks, const TaskOut *out, int nTasks, const int64_t *dst0,
-                              const int64_t *dst1, const int64_t *dst2, int32_t *const *srcW, int32_t *const *srcX,
-                              int32_t *const *srcY, int32_t *const *dstW, int32_t *const *dstX,
-                              int32_t *const *dstY) {
+__global__ void compactKernel(CompactArgs a) {
     const int k = blockIdx.y;
     const int t = blockIdx.x;
-    if (t >= nTasks) return;
-    const Task &tk = tasks[t];
-    const int n = out[t].count[k];
-    const int64_t *dst = k == 0 ? dst0 : (k == 1 ? dst1 : dst2);
+    if (t >= a.nTasks) return;
+    const Task &tk = a.tasks[t];
+    const int n = a.out[t].count[k];
     const int64_t from = tk.outOff[k] + tk.cap[k] - n;
-    const int64_t to = dst[t];
+    const int64_t to = a.dst[k] ? a.dst[k][t] : 0;
+    const int4 *src = a.src[k] + from;
+    int32_t *w = a.w[k] + to, *x = a.x[k] + to, *y = a.y[k] + to;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        dstW[k][to + i] = srcW[k][from + i];
-        dstX[k][to + i] = srcX[k][from + i];
-        dstY[k][to + i] = srcY[k][from + i];
+        const int4 v = src[i];
+        w[i] = v.x;
+        x[i] = v.y;
+        y[i] = v.z;
     }
 }
 
@@ -215,13 +214,10 @@ cudaError_t launchBand(const BandArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launchCompact(const Task *tasks, const TaskOut *out, int nTasks, const int64_t *dst0,
-                          const int64_t *dst1, const int64_t *dst2, int32_t *const *srcW, int32_t *const *srcX,
-                          int32_t *const *srcY, int32_t *const *dstW, int32_t *const *dstX, int32_t *const *dstY,
-                          cudaStream_t s) {
-    if (nTasks == 0) return cudaSuccess;
-    dim3 grid(nTasks, 3);
-    compactKernel<<<grid, 128, 0, s>>>(tasks, out, nTasks, dst0, dst1, dst2, srcW, srcX, srcY, dstW, dstX, dstY);
+cudaError_t launchCompact(const CompactArgs &a, cudaStream_t s) {
+    if (a.nTasks == 0) return cudaSuccess;
+    dim3 grid(a.nTasks, 3);
+    compactKernel<<<grid, 128, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -31,6 +31,7 @@
 namespace mp {
 cudaError_t launchVariant(int v, const DpArgs &a, int blocks, int warps, cudaStream_t s);
 cudaError_t launchBand(const BandArgs &a, cudaStream_t s);
+cudaError_t launchCompact(const CompactArgs &a, cudaStream_t s);
 }  // namespace mp
 
 using namespace mp;
@@ -59,14 +60,20 @@ constexpr size_t kOffAnchors = align256(kOffYs + kMaxDiag * sizeof(uint16_t));
 constexpr size_t kOffBand = align256(kOffAnchors + (kMaxDiag / 2 + 1) * 3 * sizeof(int32_t));
 constexpr size_t kOffChk = align256(kOffBand + (kMaxDiag + 1) * sizeof(int4));
 constexpr size_t kOffScal = align256(kOffChk + kBlocks * kC * 32 * sizeof(float4));
-constexpr size_t kOffOut = align256(kOffScal + kBlocks * sizeof(int2));
-constexpr size_t kOutListBytes[3] = {kCapM * sizeof(int32_t), kCapG * sizeof(int32_t), kCapG * sizeof(int32_t)};
-constexpr size_t kOffOutList(int k, int field) {  // field 0 weight, 1 x, 2 y
-    size_t off = kOffOut;
-    for (int i = 0; i < k; i++) off += 3 * align256(kOutListBytes[i]);
-    return off + (size_t) field * align256(kOutListBytes[k]);
+constexpr size_t kOffStage = align256(kOffScal + kBlocks * sizeof(int2));
+constexpr int64_t kCap[3] = {kCapM, kCapG, kCapG};
+constexpr size_t kOffStageList(int k) {  // staged tuples (weight, x, y, 0) of list k
+    size_t off = kOffStage;
+    for (int i = 0; i < k; i++) off += align256(kCap[i] * sizeof(int4));
+    return off;
 }
-constexpr size_t kUsed = kOffOutList(2, 2) + align256(kOutListBytes[2]);
+constexpr size_t kOffOut = kOffStageList(2) + align256(kCap[2] * sizeof(int4));
+constexpr size_t kOffOutList(int k, int field) {  // compacted lists; field 0 weight, 1 x, 2 y
+    size_t off = kOffOut;
+    for (int i = 0; i < k; i++) off += 3 * align256(kCap[i] * sizeof(int32_t));
+    return off + (size_t) field * align256(kCap[k] * sizeof(int32_t));
+}
+constexpr size_t kUsed = kOffOutList(2, 2) + align256(kCap[2] * sizeof(int32_t));
 
 }  // namespace
 
@@ -178,11 +185,7 @@ extern "C" mp_status mp_realign_single_noalloc(mp_engine *e, const mp_model *m, 
     a.repeatProb = m->repeat.as<float>();
     a.scratch = reinterpret_cast<float4 *>(base + kOffChk);
     a.scratchScalars = reinterpret_cast<int2 *>(base + kOffScal);
-    for (int k = 0; k < 3; k++) {
-        a.outW[k] = reinterpret_cast<int32_t *>(base + kOffOutList(k, 0));
-        a.outX[k] = reinterpret_cast<int32_t *>(base + kOffOutList(k, 1));
-        a.outY[k] = reinterpret_cast<int32_t *>(base + kOffOutList(k, 2));
-    }
+    for (int k = 0; k < 3; k++) a.outT[k] = reinterpret_cast<int4 *>(base + kOffStageList(k));
     a.out = dOut;
     a.threshold = (float) p->threshold;
     a.minDiagsBetweenTraceBack = (int32_t) std::min<int64_t>(p->min_diags_between_traceback, 1 << 30);
@@ -209,15 +212,25 @@ extern "C" mp_status mp_realign_single_noalloc(mp_engine *e, const mp_model *m, 
         if (res.count[k] > out->capacity[k]) tooSmall = true;
     }
     if (tooSmall) return mp_fail(MP_ERR_OVERFLOW, "an output list is smaller than its tuple count (see count)");
+    // staged records -> three arrays per list (inside the same static array), then to the host
+    CompactArgs ca;
+    ca.tasks = dTask;
+    ca.out = dOut;
+    ca.nTasks = 1;
     for (int k = 0; k < 3; k++) {
-        const int64_t n = res.count[k], from = tk.cap[k] - n;
+        ca.dst[k] = nullptr;
+        ca.src[k] = a.outT[k];
+        ca.w[k] = reinterpret_cast<int32_t *>(base + kOffOutList(k, 0));
+        ca.x[k] = reinterpret_cast<int32_t *>(base + kOffOutList(k, 1));
+        ca.y[k] = reinterpret_cast<int32_t *>(base + kOffOutList(k, 2));
+    }
+    NA_TRY(launchCompact(ca, s));
+    for (int k = 0; k < 3; k++) {
+        const int64_t n = res.count[k];
         if (n == 0) continue;
-        NA_TRY(cudaMemcpyAsync(out->weight[k], base + kOffOutList(k, 0) + sizeof(int32_t) * from,
-                               sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
-        NA_TRY(cudaMemcpyAsync(out->x[k], base + kOffOutList(k, 1) + sizeof(int32_t) * from, sizeof(int32_t) * n,
-                               cudaMemcpyDeviceToHost, s));
-        NA_TRY(cudaMemcpyAsync(out->y[k], base + kOffOutList(k, 2) + sizeof(int32_t) * from, sizeof(int32_t) * n,
-                               cudaMemcpyDeviceToHost, s));
+        NA_TRY(cudaMemcpyAsync(out->weight[k], ca.w[k], sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+        NA_TRY(cudaMemcpyAsync(out->x[k], ca.x[k], sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+        NA_TRY(cudaMemcpyAsync(out->y[k], ca.y[k], sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
     }
     NA_TRY(cudaStreamSynchronize(s));
 #undef NA_TRY

@@ -471,9 +471,7 @@ __device__ __forceinline__ int rescaleFwd(Fwd<C> &st) {
 // ---------------------------------------------------------------------------
 
 struct Out {
-    int32_t *w[3];
-    int32_t *x[3];
-    int32_t *y[3];
+    int4 *t[3];   // the task's staging region of each list: (weight, x, y, 0)
     int top[3];
     int written[3];
     int xShift, yShift;
@@ -481,92 +479,46 @@ struct Out {
 
 // Called by every lane of the warp; groups with `active` false emit nothing. The
 // (list, slot) pairs are unrolled at compile time, so each tuple is written through a
-// fixed list pointer and the warp skips a pair no lane holds.
+// fixed list pointer.
 template <int C, int L>
 __device__ __forceinline__ void emitDiagonal(int gl, Out &o, const float (&p)[3][C], float thr, int x0, int d,
                                              bool active) {
-    uint32_t m[3];  // bit j: slot j of list k passes the threshold
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        m[k] = 0;
-#pragma unroll
-        for (int j = 0; j < C; j++) m[k] |= (p[k][j] >= thr ? 1u : 0u) << j;
-        m[k] = active ? m[k] : 0u;
-    }
-    if (__ballot_sync(FULL_MASK, (m[0] | m[1] | m[2]) != 0) == 0) return;
-    const uint32_t cnt = (uint32_t) __popc(m[0]) | ((uint32_t) __popc(m[1]) << 10) | ((uint32_t) __popc(m[2]) << 20);
-    uint32_t incl = cnt;
-#pragma unroll
-    for (int off = 1; off < L; off <<= 1) {
-        const uint32_t v = __shfl_up_sync(FULL_MASK, incl, off, L);
-        if (gl >= off) incl += v;
-    }
-    const uint32_t total = __shfl_sync(FULL_MASK, incl, L - 1, L);
-    const uint32_t excl = incl - cnt;  // packed ranks of this lane's first tuple in each list
+    // Ranks come from one ballot per (list, slot): a tuple's rank within its group's
+    // diagonal is the number of passing slots of lower index (lower lanes, then lower
+    // slots of the same lane). A list no lane holds is skipped by the whole warp.
+    const int lane = threadIdx.x & 31;
+    const unsigned below = ((1u << gl) - 1u) << (lane - gl);           // lower lanes of the group
+    const unsigned group = (L == 32 ? FULL_MASK : ((1u << L) - 1u)) << (lane - gl);
     const int xl = x0 + gl * C;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        int pos = o.top[k] - 1 - o.written[k] - (int) ((excl >> (10 * k)) & 1023u);
+        unsigned b[C];
+        unsigned any = 0;
 #pragma unroll
         for (int j = 0; j < C; j++) {
-            if (m[k] & (1u << j)) {
+            b[j] = __ballot_sync(FULL_MASK, active && p[k][j] >= thr);
+            any |= b[j];
+        }
+        if (any == 0) continue;
+        int before = 0, total = 0;
+#pragma unroll
+        for (int j = 0; j < C; j++) {
+            before += __popc(b[j] & below);
+            total += L == 32 ? __popc(b[j]) : __popc(b[j] & group);
+        }
+        int pos = o.top[k] - 1 - o.written[k] - before;
+#pragma unroll
+        for (int j = 0; j < C; j++) {
+            if ((b[j] >> lane) & 1u) {
                 if (pos >= 0) {
                     const int x = xl + j;
-                    o.w[k][pos] = (int32_t) floorf(fminf(p[k][j], 1.0f) * (float) kProbOne);
-                    o.x[k][pos] = x - 1 + o.xShift;
-                    o.y[k][pos] = d - x - 1 + o.yShift;
+                    o.t[k][pos] = make_int4((int32_t) floorf(fminf(p[k][j], 1.0f) * (float) kProbOne),
+                                            x - 1 + o.xShift, d - x - 1 + o.yShift, 0);
                 }
                 pos--;
             }
         }
-        o.written[k] += (int) ((total >> (10 * k)) & 1023u);
-    }
-}
-
-// Stores three 32-bit values under a predicate, without a branch.
-__device__ __forceinline__ void storeIf(bool p, int32_t *a, int32_t va, int32_t *b, int32_t vb, int32_t *c,
-                                        int32_t vc) {
-    asm volatile(
-        "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %0, 0;\n\t@q st.global.b32 [%1], %2;\n\t"
-        "@q st.global.b32 [%3], %4;\n\t@q st.global.b32 [%5], %6;\n}" ::"r"((unsigned) p),
-        "l"(a), "r"(va), "l"(b), "r"(vb), "l"(c), "r"(vc));
-}
-
-// emitDiagonal without branches: the same ranks and tuples, written with predicated stores.
-template <int C, int L>
-__device__ __forceinline__ void emitDiagonalFlat(int gl, Out &o, const float (&p)[3][C], float thr, int x0, int d,
-                                                 bool active) {
-    uint32_t m[3];
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        m[k] = 0;
-#pragma unroll
-        for (int j = 0; j < C; j++) m[k] |= (p[k][j] >= thr ? 1u : 0u) << j;
-        m[k] = active ? m[k] : 0u;
-    }
-    const uint32_t cnt = (uint32_t) __popc(m[0]) | ((uint32_t) __popc(m[1]) << 10) | ((uint32_t) __popc(m[2]) << 20);
-    uint32_t incl = cnt;
-#pragma unroll
-    for (int off = 1; off < L; off <<= 1) {
-        const uint32_t v = __shfl_up_sync(FULL_MASK, incl, off, L);
-        incl += gl >= off ? v : 0u;
-    }
-    const uint32_t total = __shfl_sync(FULL_MASK, incl, L - 1, L);
-    const uint32_t excl = incl - cnt;
-    const int xl = x0 + gl * C;
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        int pos = o.top[k] - 1 - o.written[k] - (int) ((excl >> (10 * k)) & 1023u);
-#pragma unroll
-        for (int j = 0; j < C; j++) {
-            const bool sel = (m[k] >> j) & 1u;
-            const int x = xl + j;
-            const int q = max(pos, 0);
-            storeIf(sel && pos >= 0, o.w[k] + q, (int32_t) floorf(fminf(p[k][j], 1.0f) * (float) kProbOne), o.x[k] + q,
-                    x - 1 + o.xShift, o.y[k] + q, d - x - 1 + o.yShift);
-            pos -= sel ? 1 : 0;
-        }
-        o.written[k] += (int) ((total >> (10 * k)) & 1023u);
+        o.written[k] += total;
     }
 }
 
@@ -806,7 +758,8 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
                         sY[j] = (j > 0) ? gY[j - 1] : nb;
                     }
                 }
-                const bool top = d == wk.D;  // the walk's first diagonal holds the end probabilities
+                // the walk's first diagonal holds the end probabilities (never inside a flat block)
+                const bool top = !FLAT && d == wk.D;
 #pragma unroll
                 for (int j = 0; j < C; j++) {
                     const float s2 = PAR ? gB[j] : gA[j];
@@ -821,7 +774,7 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
             const bool post = on && d <= wk.tbFrom;
             // total probability refresh: 1st, 11th, 21st ... posterior diagonal of the walk
             const bool refresh = post && untilRefresh == 0;
-            if (FLAT || __any_sync(FULL_MASK, refresh)) {
+            if (__any_sync(FULL_MASK, refresh)) {
                 // cells of d plus the match transitions crossing d (impl/pairwiseAligner.c:567-584)
                 float sM1[C];
                 if (kk > 0) {
@@ -868,8 +821,7 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
                     p[1][j] = (f[j].y * bX[j]) * scale;
                     p[2][j] = (f[j].z * bY[j]) * scale;
                 }
-                if (FLAT) emitDiagonalFlat<C, L>(gl, o, p, thr, slotX0(d, inf.x), d, emit);
-                else emitDiagonal<C, L>(gl, o, p, thr, slotX0(d, inf.x), d, emit);
+                emitDiagonal<C, L>(gl, o, p, thr, slotX0(d, inf.x), d, emit);
             }
             // u-values of d (emissions are zero outside the band); kept when the diagonal is off
 #pragma unroll
@@ -892,7 +844,7 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
         };
         const auto odd = std::integral_constant<int, 1>{};
         const auto even = std::integral_constant<int, 0>{};
-        if (flat && __all_sync(FULL_MASK, dStart > wk.tbTo)) {
+        if (flat && __all_sync(FULL_MASK, dStart > wk.tbTo && dEnd < wk.D)) {
 #pragma unroll 1
             for (int k = K - 2; k >= 0; k -= 2) {
                 back(odd, std::true_type{}, k + 1);
@@ -1004,9 +956,7 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
     Out o;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        o.w[k] = a.outW[k] + tk->outOff[k];
-        o.x[k] = a.outX[k] + tk->outOff[k];
-        o.y[k] = a.outY[k] + tk->outOff[k];
+        o.t[k] = a.outT[k] + tk->outOff[k];
         o.top[k] = tk->cap[k];
         o.written[k] = 0;
     }

@@ -220,6 +220,49 @@ mp_status mp_split_points(const int32_t *anchors, int64_t n_anchors, int64_t lx,
 mp_status mp_crop_range(const int32_t *anchors, int64_t n_anchors, int64_t template_length, int64_t read_length,
                         int64_t *start, int64_t *end);
 
+/* ---- forward likelihood: computeForwardProbability (impl/pairwiseAligner.c:813-865) ----
+ * log_prob[j] receives ln P(X_j, Y_j): the forward total at the last anti-diagonal with
+ * the (ragged) end probabilities, over the band of band_construct
+ * (impl/pairwiseAligner.c:175-226: every anchor box widened by p->diagonal_expansion; the
+ * anchors' own expansions are ignored), with no split rectangles and no traceback
+ * segments, as in the reference. Jobs with lx + ly = 0 give 0 (LOG_ONE). The band hull
+ * must fit the widest kernel window (240 slots), else MP_ERR_OVERFLOW. The bubble-graph
+ * callers (impl/bubbleGraph.c:924) pass no anchors: the band is then the whole matrix. */
+mp_status mp_forward_batch(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
+                           double *log_prob);
+
+/* ---- adjoint: expected counts = gradient of the summed log-likelihood ----
+ * For the FP32 scaled-probability DP over each job's band (the posterior pass's band,
+ * splits and ragged ends, but one walk over the whole lattice: no traceback segments), the
+ * kernel accumulates, divided by each sub-problem's total P:
+ *   transitions[m][i*3+j]  sum over cells of f_i(cell) * t_ij * e_j(next) * b_j(next)
+ *                          = d ln P / d ln t_ij  (the Baum-Welch transition counts of
+ *                          getExpectationsUsingAnchors, impl/pairwiseAligner.c:347-357,
+ *                          :1151-1156, which the reference only has for transitions);
+ *   match[m][xb*5+yb]      posterior of the match state at cells with bases (xb, yb)
+ *                          = d ln P / d ln (match emission xb, yb);
+ *   gap_x[m][xb], gap_y[m][yb]  posteriors of the gap states by base;
+ *   repeat[table][row][i][j]    match posteriors by the run-length table entry used
+ *                          (impl/polisher.c:1756-1775), = d ln P / d ln R[row][i][j];
+ *                          when both strands share one table all counts are in table 0;
+ *   start[m][s], end[m][s]  state posteriors at the first / last cell = d ln P / d ln of
+ *                          the (ragged) start / end probability of state s (these vectors
+ *                          are functions of the transitions, impl/stateMachine.c:518-557).
+ * m is the model of the read's strand (0 forward, 1 reverse). log_lik (optional, n_jobs)
+ * receives each job's ln P; log_likelihood their sum. Band hulls up to 120 slots. */
+typedef struct {
+    double transitions[2][9];
+    double match[2][25];
+    double gap_x[2][5];
+    double gap_y[2][5];
+    double start[2][3];
+    double end[2][3];
+    double repeat[2][4 * MP_MAX_REPEAT * MP_MAX_REPEAT];
+    double log_likelihood;
+} mp_expectations;
+mp_status mp_expectations_batch(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
+                                mp_expectations *out, double *log_lik);
+
 /* ---- single read without any memory allocation ----
  * No counterpart in the reference. For callers that cannot allocate device memory
  * (their framework's pool owns the GPU, or allocation is not allowed where they

@@ -3,7 +3,8 @@ posterior pass. The compute path is the in-tree CUDA library libmpgpu.so
 (C ABI in include/mpgpu.h); this package is its host-side interface."""
 from . import _lib
 from .params import AlignmentParams, PolishModel, StateModel, build_state_model, load_polish_model
-from .realign import (DeviceBatch, Engine, Jobs, Model, Pairs, get_aligned_pairs_using_anchors,
+from .realign import (DeviceBatch, Engine, Expectations, Jobs, Model, Pairs, compute_forward_probability,
+                      expectations_batch, forward_batch, get_aligned_pairs_using_anchors,
                       get_aligned_pairs_with_indels_using_anchors, realign_batch)
 from .rle import RleString, crop_range, rle_anchors
 
@@ -11,4 +12,5 @@ __all__ = [
     "AlignmentParams", "PolishModel", "StateModel", "build_state_model", "load_polish_model", "DeviceBatch",
     "Engine", "Jobs", "Model", "Pairs", "get_aligned_pairs_using_anchors",
     "get_aligned_pairs_with_indels_using_anchors", "realign_batch", "RleString", "crop_range", "rle_anchors",
+    "compute_forward_probability", "forward_batch", "expectations_batch", "Expectations",
 ]

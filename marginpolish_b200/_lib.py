@@ -123,6 +123,19 @@ class NoallocOutput(Structure):
     ]
 
 
+class Expectations(Structure):
+    _fields_ = [
+        ("transitions", (c_double * 9) * 2),
+        ("match", (c_double * 25) * 2),
+        ("gap_x", (c_double * 5) * 2),
+        ("gap_y", (c_double * 5) * 2),
+        ("start", (c_double * 3) * 2),
+        ("end", (c_double * 3) * 2),
+        ("repeat", (c_double * (4 * MP_MAX_REPEAT * MP_MAX_REPEAT)) * 2),
+        ("log_likelihood", c_double),
+    ]
+
+
 class Tuning(Structure):
     _fields_ = [
         ("checkpoint_stride", c_int32),
@@ -140,7 +153,7 @@ EXPORTED = [
     "mp_device_batch_stats", "mp_device_batch_destroy", "mp_band", "mp_split_points", "mp_crop_range",
     "mp_rle_encode", "mp_rle_symbols", "mp_rle_anchors", "mp_device_batch_timing", "mp_measure_fp32_peak",
     "mp_realign_single_noalloc", "mp_device_batch_reset", "mp_device_batch_counts", "mp_device_batch_fetch_into",
-    "mp_host_alloc", "mp_host_free", "mp_device_batch_run_plain",
+    "mp_host_alloc", "mp_host_free", "mp_device_batch_run_plain", "mp_forward_batch", "mp_expectations_batch",
 ]
 
 _lib = None
@@ -183,6 +196,8 @@ def load() -> ctypes.CDLL:
         "mp_measure_fp32_peak": (c_int, [c_void_p, P(c_double)]),
         "mp_realign_single_noalloc": (c_int, [c_void_p, c_void_p, P(Params), P(c_uint16), c_int64, P(c_uint16),
                                               c_int64, P(c_int32), c_int64, c_int, c_int, c_int, P(NoallocOutput)]),
+        "mp_forward_batch": (c_int, [c_void_p, c_void_p, P(Params), P(Batch), P(c_double)]),
+        "mp_expectations_batch": (c_int, [c_void_p, c_void_p, P(Params), P(Batch), P(Expectations), P(c_double)]),
         "mp_band": (c_int, [P(c_int32), c_int64, c_int64, c_int64, c_int64, c_int, P(c_int64)]),
         "mp_split_points": (c_int, [P(c_int32), c_int64, c_int64, c_int64, c_int64, c_int, c_int, P(c_int64),
                                     c_int64, P(c_int64)]),

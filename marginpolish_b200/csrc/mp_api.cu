@@ -28,6 +28,10 @@ int variantCount();
 bool variantShape(int v, int *C, int *L, int *K);
 int variantMaxWarps(int v, int nTables);
 cudaError_t launchVariant(int v, const DpArgs &a, int blocks, int warps, cudaStream_t s);
+int adjointVariantCount();
+bool adjointVariantShape(int v, int *C, int *L, int *K);
+int adjointVariantMaxWarps(int v, int nTables);
+cudaError_t launchAdjointVariant(int v, const DpArgs &a, int blocks, int warps, cudaStream_t s);
 cudaError_t launchBand(const BandArgs &a, cudaStream_t s);
 cudaError_t launchCompact(const CompactArgs &a, cudaStream_t s);
 }  // namespace mp
@@ -118,7 +122,9 @@ extern "C" void mp_engine_destroy(mp_engine *e) {
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
     mp_device_batch_destroy(e->oneShot);
-    e->oneShot = nullptr;
+    mp_device_batch_destroy(e->forwardShot);
+    mp_device_batch_destroy(e->adjointShot);
+    e->oneShot = e->forwardShot = e->adjointShot = nullptr;
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }
@@ -192,6 +198,12 @@ extern "C" mp_status mp_model_create(mp_engine *e, const mp_model_desc *fwd, con
     std::vector<float> rp(2 * kRepTable);
     mp_status s = lowerModel(fwd, m->host[0], rp.data());
     if (s == MP_OK) s = lowerModel(rev, m->host[1], rp.data() + kRepTable);
+    if (s == MP_OK) {
+        for (int k = 0; k < 9; k++) {
+            m->logT[0][k] = fwd->log_transitions[k];
+            m->logT[1][k] = rev->log_transitions[k];
+        }
+    }
     if (s == MP_OK) {
         m->sharedRepeat = memcmp(rp.data(), rp.data() + kRepTable, sizeof(float) * kRepTable) == 0 ? 1 : 0;
         cudaSetDevice(e->device);
@@ -379,6 +391,22 @@ static int pickVariant(int lanes, int64_t slots) {
     return -1;
 }
 
+// Adjoint variants (one task per warp), narrowest window that holds the hull; -1 if none.
+static int pickAdjointVariant(int64_t slots) {
+    for (int v = 0; v < adjointVariantCount(); v++) {
+        int C = 0, L = 0, K = 0;
+        adjointVariantShape(v, &C, &L, &K);
+        if (slots <= L * C - 2 * C) return v;
+    }
+    return -1;
+}
+
+static int adjointMaxHull() {
+    int C = 0, L = 0, K = 0;
+    adjointVariantShape(adjointVariantCount() - 1, &C, &L, &K);
+    return L * C - 2 * C;
+}
+
 // Upper bound (in window slots) of the hull of 5 consecutive anti-diagonal bands:
 // the union of up to three consecutive anchor boxes, clipped to the matrix.
 static int64_t hullSlotBound(const int32_t *an, int64_t nA, int64_t x1, int64_t y1, int64_t lx, int64_t ly,
@@ -429,7 +457,12 @@ struct PlannedTask {
     int32_t hull;  // window slots the band hull needs
 };
 
+// What a batch computes: the posterior pass (tuples), the forward likelihood only
+// (computeForwardProbability), or the adjoint (expected counts).
+enum BatchMode { kModePosterior = 0, kModeForward = 1, kModeAdjoint = 2 };
+
 struct mp_device_batch {
+    int mode = kModePosterior;
     mp_engine *e = nullptr;
     int device = -1;
     const mp_model *m = nullptr;
@@ -444,6 +477,7 @@ struct mp_device_batch {
     // device
     DevBuf xs, ys, anchors, dTasks, band, dOut, outT[3];  // outT: staged tuples per list
     DevBuf orders, queue, scratch, scratchScal;
+    DevBuf expect, expectRep;  // adjoint accumulators (FP64)
     DevBuf fetchDst[3], fetchW[3], fetchX[3], fetchY[3];  // compaction staging (reused)
     std::vector<int> varOrderOff;  // per variant offset into orders
     std::vector<int> varCount;
@@ -458,7 +492,7 @@ struct mp_device_batch {
     }
 };
 
-static mp_status validateJob(const mp_batch *b, int64_t j, const mp_params *p) {
+static mp_status validateJob(const mp_batch *b, int64_t j, const mp_params *p, bool dynamic) {
     int64_t lx = b->x_end[j] - b->x_begin[j];
     int64_t ly = b->y_offsets[j + 1] - b->y_offsets[j];
     if (b->x_begin[j] < 0 || b->x_end[j] > b->x_symbols_length || lx < 0)
@@ -474,12 +508,13 @@ static mp_status validateJob(const mp_batch *b, int64_t j, const mp_params *p) {
         if (x <= px || y <= py || x >= lx || y >= ly)
             return failf(MP_ERR_ARGUMENT, "job %lld: anchor %lld (%lld, %lld) not strictly increasing / in range",
                          (long long) j, (long long) (i - a0), (long long) x, (long long) y);
-        if (p->dynamic_anchor_expansion && (ex < 0 || (ex & 1)))
+        if (dynamic && (ex < 0 || (ex & 1)))
             return failf(MP_ERR_ARGUMENT, "job %lld: anchor %lld expansion %lld must be even and >= 0",
                          (long long) j, (long long) (i - a0), (long long) ex);
         px = x;
         py = y;
     }
+    (void) p;
     return MP_OK;
 }
 
@@ -531,11 +566,14 @@ static mp_status planBatch(mp_device_batch *db, const mp_batch *b) {
     std::vector<mp_status> statuses(nThreads, MP_OK);
     std::vector<std::string> errors(nThreads);
     int64_t chunk = (nJobs + nThreads - 1) / nThreads;
+    // the forward likelihood uses band_construct (fixed expansion, no splits)
+    const bool forward = db->mode == kModeForward;
+    const bool dynamic = !forward && p->dynamic_anchor_expansion != 0;
     auto work = [&](unsigned t) {
         int64_t j0 = t * chunk, j1 = std::min(nJobs, j0 + chunk);
         std::vector<SplitRect> rects;
         for (int64_t j = j0; j < j1; j++) {
-            mp_status s = validateJob(b, j, p);
+            mp_status s = validateJob(b, j, p, dynamic);
             if (s != MP_OK) {
                 statuses[t] = s;
                 errors[t] = g_lastError;
@@ -548,7 +586,8 @@ static mp_status planBatch(mp_device_batch *db, const mp_batch *b) {
             bool rL = b->ragged_left ? b->ragged_left[j] != 0 : false;
             bool rR = b->ragged_right ? b->ragged_right[j] != 0 : false;
             rects.clear();
-            splitPoints(an, nA, lx, ly, p->split_matrix_bigger_than_this, rL, rR, rects);
+            if (forward) rects.push_back(SplitRect{0, 0, lx, ly});
+            else splitPoints(an, nA, lx, ly, p->split_matrix_bigger_than_this, rL, rR, rects);
             int64_t ai = 0;
             int64_t count = 0;
             for (size_t i = 0; i < rects.size(); i++) {
@@ -572,17 +611,19 @@ static mp_status planBatch(mp_device_batch *db, const mp_batch *b) {
                 tk.y1 = (int32_t) r.y1;
                 tk.xShift = b->x_shift ? (int32_t) b->x_shift[j] : 0;
                 bool tl = rL || i > 0, tr = rR || i + 1 < rects.size();
-                tk.flags = (tl ? 1 : 0) | (tr ? 2 : 0) | ((b->strand && b->strand[j]) ? 4 : 0) |
-                           (p->dynamic_anchor_expansion ? 8 : 0);
+                tk.flags = (tl ? kFlagRaggedLeft : 0) | (tr ? kFlagRaggedRight : 0) |
+                           ((b->strand && b->strand[j]) ? kFlagForward : 0) | (dynamic ? kFlagDynamic : 0) |
+                           (forward ? kFlagForwardOnly : 0);
                 tk.job = (int32_t) j;
                 tk.expansion = (int32_t) p->diagonal_expansion;
-                int64_t slots = hullSlotBound(an + 3 * first, tk.nAnchors, r.x1, r.y1, tk.lx, tk.ly,
-                                              p->dynamic_anchor_expansion != 0, p->diagonal_expansion);
+                int64_t slots = hullSlotBound(an + 3 * first, tk.nAnchors, r.x1, r.y1, tk.lx, tk.ly, dynamic,
+                                              p->diagonal_expansion);
                 pt.hull = (int32_t) std::min<int64_t>(slots, 1 << 30);
-                if (slots > kMaxHullSlots) {
+                const int64_t maxHull = db->mode == kModeAdjoint ? adjointMaxHull() : kMaxHullSlots;
+                if (slots > maxHull) {
                     statuses[t] = failf(MP_ERR_OVERFLOW,
-                                        "job %lld: band hull of %lld slots exceeds the widest kernel window (%d)",
-                                        (long long) j, (long long) slots, kMaxHullSlots);
+                                        "job %lld: band hull of %lld slots exceeds the widest kernel window (%lld)",
+                                        (long long) j, (long long) slots, (long long) maxHull);
                     errors[t] = g_lastError;
                     return;
                 }
@@ -624,6 +665,7 @@ static mp_status planBatch(mp_device_batch *db, const mp_batch *b) {
         // threshold 0.01; overflowing tasks are re-run with their exact counts
         int32_t capM = (int32_t) (N + N / 8 + 64), capX = (int32_t) (N * 3 / 4 + 64), capY = (int32_t) (N * 3 / 4 + 64);
         int32_t caps[3] = {capM, capX, capY};
+        if (db->mode != kModePosterior) caps[0] = caps[1] = caps[2] = 0;  // no tuples
         for (int k = 0; k < 3; k++) {
             tk.cap[k] = caps[k];
             tk.outOff[k] = outOff[k];
@@ -635,17 +677,46 @@ static mp_status planBatch(mp_device_batch *db, const mp_batch *b) {
     return MP_OK;
 }
 
+static int modeVariantCapacity(const mp_device_batch *db, int v) {
+    if (db->mode != kModeAdjoint) return variantCapacity(v);
+    int C = 0, L = 0, K = 0;
+    if (!adjointVariantShape(v, &C, &L, &K)) return 0;
+    return L * C - 2 * C;
+}
+
+static int modeMaxHullSlots(const mp_device_batch *db) {
+    return db->mode == kModeAdjoint ? adjointMaxHull() : kMaxHullSlots;
+}
+
+// Zeroes the adjoint's FP64 accumulators (2 models' small tables, then the repeat tables).
+static mp_status zeroExpectations(mp_device_batch *db) {
+    MP_TRY(db->expect.reserve(sizeof(double) * 2 * kExpPerModel));
+    MP_TRY(db->expectRep.reserve(sizeof(double) * 2 * kRepTable));
+    CUDA_TRY(cudaMemsetAsync(db->expect.p, 0, sizeof(double) * 2 * kExpPerModel, db->e->stream));
+    CUDA_TRY(cudaMemsetAsync(db->expectRep.p, 0, sizeof(double) * 2 * kRepTable, db->e->stream));
+    return MP_OK;
+}
+
 // Picks each task's kernel variant under the engine's tuning and builds the
 // per-variant length-sorted queues for the tasks in `subset`.
+static int modeVariantCount(const mp_device_batch *db) {
+    return db->mode == kModeAdjoint ? adjointVariantCount() : variantCount();
+}
+
+static bool modeVariantShape(const mp_device_batch *db, int v, int *C, int *L, int *K) {
+    return db->mode == kModeAdjoint ? adjointVariantShape(v, C, L, K) : variantShape(v, C, L, K);
+}
+
 static mp_status buildQueues(mp_device_batch *db, const std::vector<int32_t> &subset, std::vector<int32_t> &orderHost) {
-    const int nV = variantCount();
+    const int nV = modeVariantCount(db);
     db->varOrderOff.assign(nV + 1, 0);
     db->varCount.assign(nV, 0);
     db->varMaxN.assign(nV, 0);
     db->var.resize(db->tasks.size(), -1);
     std::vector<std::vector<int32_t>> per(nV);
     for (int32_t t : subset) {
-        const int v = pickVariant(db->e->tuning.lanes_per_task, db->hull[t]);
+        const int v = db->mode == kModeAdjoint ? pickAdjointVariant(db->hull[t])
+                                               : pickVariant(db->e->tuning.lanes_per_task, db->hull[t]);
         if (v < 0)
             return failf(MP_ERR_OVERFLOW, "job %d: band wider than the widest kernel window", db->tasks[t].job);
         db->var[t] = v;
@@ -733,15 +804,18 @@ extern "C" mp_status mp_device_batch_reset(mp_engine *e, mp_device_batch *db, co
 static mp_status launchQueues(mp_device_batch *db) {
     mp_engine *e = db->e;
     cudaStream_t st = e->stream;
-    const int nV = variantCount();
+    const int nV = modeVariantCount(db);
+    const bool adj = db->mode == kModeAdjoint;
     std::vector<int> blocksOf(nV, 0), warpsOf(nV, 0), scratchBlocksOf(nV, 0);
     size_t needScratch = 0, needScal = 0;
     for (int v = 0; v < nV; v++) {
         if (db->varCount[v] == 0) continue;
         int C = 0, L = 0, K = 0;
-        variantShape(v, &C, &L, &K);
+        modeVariantShape(db, v, &C, &L, &K);
         const int G = 32 / L;
-        const int maxW = variantMaxWarps(v, db->m->sharedRepeat ? 1 : 2);
+        const int nTables = db->m->sharedRepeat ? 1 : 2;
+        const int maxW = adj ? adjointVariantMaxWarps(v, nTables) : variantMaxWarps(v, nTables);
+        if (maxW < 1) return failf(MP_ERR_OVERFLOW, "kernel variant %d does not fit in shared memory", v);
         const int warps = e->tuning.warps_per_block > 0 ? std::min(e->tuning.warps_per_block, maxW) : maxW;
         const int blocksPerSm = e->tuning.blocks_per_sm > 0 ? e->tuning.blocks_per_sm : 1;
         const int loads = (db->varCount[v] + G - 1) / G;  // warp-loads of G tasks
@@ -784,7 +858,10 @@ static mp_status launchQueues(mp_device_batch *db) {
         a.traceBackDiagonals = (int32_t) db->p.traceback_diagonals;
         a.diagonalExpansion = (int32_t) std::min<int64_t>(db->p.diagonal_expansion, 1 << 29);
         a.sharedRepeat = db->m->sharedRepeat;
-        CUDA_TRY(launchVariant(v, a, blocksOf[v], warpsOf[v], st));
+        a.expect = db->expect.as<double>();
+        a.expectRep = db->expectRep.as<double>();
+        if (adj) CUDA_TRY(launchAdjointVariant(v, a, blocksOf[v], warpsOf[v], st));
+        else CUDA_TRY(launchVariant(v, a, blocksOf[v], warpsOf[v], st));
         db->launchesPerRun++;
     }
     return MP_OK;
@@ -811,6 +888,7 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
     CUDA_TRY(launchBand(ba, st));
     db->launchesPerRun += nTasks > 0 ? 2 : 0;
     CUDA_TRY(cudaEventRecord(db->evBand, st));
+    if (db->mode == kModeAdjoint) MP_TRY(zeroExpectations(db));
     MP_TRY(launchQueues(db));
     CUDA_TRY(cudaEventRecord(e->ev1, st));
     // statuses
@@ -837,8 +915,8 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
             }
             if (o.status & (kTaskCapacity | kTaskWindow | kTaskScratch)) {
                 if (o.status & kTaskWindow) {
-                    const int cap = variantCapacity(db->var[t]);
-                    if (cap >= kMaxHullSlots)
+                    const int cap = modeVariantCapacity(db, db->var[t]);
+                    if (cap >= modeMaxHullSlots(db))
                         return failf(MP_ERR_OVERFLOW, "job %d: band wider than the widest kernel window", db->tasks[t].job);
                     db->hull[t] = std::max(db->hull[t], cap + 1);
                 }
@@ -857,6 +935,12 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
             }
         }
         if (!changed) break;
+        if (db->mode == kModeAdjoint) {
+            // the accumulators already hold the failed tasks' partial sums: run every task again
+            retry.clear();
+            for (int t = 0; t < nTasks; t++) retry.push_back(t);
+            MP_TRY(zeroExpectations(db));
+        }
         // grow output buffers (preserving contents)
         for (int k = 0; k < 3; k++) {
             size_t need = sizeof(int4) * db->outCap[k];
@@ -1203,6 +1287,76 @@ extern "C" mp_status mp_realign_batch(mp_engine *e, const mp_model *m, const mp_
     MP_TRY(mp_device_batch_run(e, db, &ms));
     MP_TRY(mp_device_batch_fetch(e, db, out));
     (*out)->deviceMs = ms;
+    return MP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// forward likelihood (computeForwardProbability) and the adjoint (expected counts)
+// ---------------------------------------------------------------------------
+
+// Runs a batch in `mode` on the engine's cached batch of that mode.
+static mp_status runMode(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b, int mode,
+                         mp_device_batch **slot, mp_device_batch **ran) {
+    if (!*slot) *slot = new mp_device_batch();
+    mp_device_batch *db = *slot;
+    db->mode = mode;
+    MP_TRY(batchReset(e, db, m, p, b));
+    MP_TRY(mp_device_batch_run(e, db, nullptr));
+    *ran = db;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_forward_batch(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
+                                      double *log_prob) {
+    if (!e || !m || !p || !b || (b->n_jobs > 0 && !log_prob))
+        return failf(MP_ERR_ARGUMENT, "mp_forward_batch: NULL argument");
+    std::lock_guard<std::mutex> guard(e->oneShotLock);
+    mp_device_batch *db = nullptr;
+    MP_TRY(runMode(e, m, p, b, kModeForward, &e->forwardShot, &db));
+    for (int64_t j = 0; j < db->nJobs; j++) {
+        double ll = 0.0;
+        for (int64_t t = db->jobFirstTask[j]; t < db->jobFirstTask[j + 1]; t++) ll += db->hostOut[t].logLik;
+        log_prob[j] = ll;
+    }
+    return MP_OK;
+}
+
+extern "C" mp_status mp_expectations_batch(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
+                                           mp_expectations *out, double *log_lik) {
+    if (!e || !m || !p || !b || !out) return failf(MP_ERR_ARGUMENT, "mp_expectations_batch: NULL argument");
+    std::lock_guard<std::mutex> guard(e->oneShotLock);
+    mp_device_batch *db = nullptr;
+    MP_TRY(runMode(e, m, p, b, kModeAdjoint, &e->adjointShot, &db));
+    std::vector<double> small(2 * kExpPerModel, 0.0), rep(2 * kRepTable, 0.0);
+    if (!db->tasks.empty()) {
+        MP_TRY(db->expect.reserve(sizeof(double) * 2 * kExpPerModel));
+        MP_TRY(db->expectRep.reserve(sizeof(double) * 2 * kRepTable));
+        CUDA_TRY(cudaMemcpy(small.data(), db->expect.p, sizeof(double) * small.size(), cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(rep.data(), db->expectRep.p, sizeof(double) * rep.size(), cudaMemcpyDeviceToHost));
+    }
+    memset(out, 0, sizeof(*out));
+    for (int md = 0; md < 2; md++) {
+        const double *g = small.data() + md * kExpPerModel;
+        for (int k = 0; k < 9; k++) out->transitions[md][k] = g[kExpTrans + k] * std::exp(m->logT[md][k]);
+        for (int k = 0; k < 25; k++) out->match[md][k] = g[kExpMatch + k];
+        for (int k = 0; k < 5; k++) {
+            out->gap_x[md][k] = g[kExpGapX + k];
+            out->gap_y[md][k] = g[kExpGapY + k];
+        }
+        for (int k = 0; k < 3; k++) {
+            out->start[md][k] = g[kExpStart + k];
+            out->end[md][k] = g[kExpEnd + k];
+        }
+        for (int k = 0; k < kRepTable; k++) out->repeat[md][k] = rep[(size_t) md * kRepTable + k];
+    }
+    double total = 0.0;
+    for (int64_t j = 0; j < db->nJobs; j++) {
+        double ll = 0.0;
+        for (int64_t t = db->jobFirstTask[j]; t < db->jobFirstTask[j + 1]; t++) ll += db->hostOut[t].logLik;
+        if (log_lik) log_lik[j] = ll;
+        total += ll;
+    }
+    out->log_likelihood = total;
     return MP_OK;
 }
 

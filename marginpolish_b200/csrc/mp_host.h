@@ -69,6 +69,8 @@ struct mp_engine {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     mp_tuning tuning{};
     struct mp_device_batch *oneShot = nullptr;  // reused by the one-shot calls (mp_realign_batch*)
+    struct mp_device_batch *forwardShot = nullptr;  // reused by mp_forward_batch
+    struct mp_device_batch *adjointShot = nullptr;  // reused by mp_expectations_batch
     std::mutex oneShotLock;
 };
 
@@ -76,6 +78,7 @@ struct mp_model {
     mp_engine *engine = nullptr;
     int sharedRepeat = 0;  // the two strands' repeat tables are identical
     mp::DevModel host[2];
+    double logT[2][9];   // log transitions as given (the adjoint scales its sums by exp(logT))
     DevBuf models;   // DevModel[2]
     DevBuf repeat;   // float [2][kRepTable]
 };

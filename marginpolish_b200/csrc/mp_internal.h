@@ -44,6 +44,19 @@ struct Task {
     int32_t pad[2];
 };
 
+// Task flags.
+constexpr int32_t kFlagRaggedLeft = 1, kFlagRaggedRight = 2, kFlagForward = 4, kFlagDynamic = 8,
+                  kFlagForwardOnly = 16;  // likelihood only: one walk of the top block, no tuples
+
+// Expected counts (adjoint) in global memory, per model m (0 forward strand, 1 reverse):
+// [m*kExpPerModel + kExpTrans + from*3+to]   sum over cells of f_from * u_to / P (times t on the host)
+// [m*kExpPerModel + kExpMatch + xb*5+yb]     posterior of the match state by (x base, y base)
+// [m*kExpPerModel + kExpGapX + xb], [.. + kExpGapY + yb]
+// [m*kExpPerModel + kExpStart + s], [.. + kExpEnd + s]  state posteriors at the first / last cell
+// and, separately, [table][4][51][51] posteriors of the match state by repeat-table entry.
+constexpr int kExpTrans = 0, kExpMatch = 9, kExpGapX = 34, kExpGapY = 39, kExpStart = 44, kExpEnd = 47,
+              kExpPerModel = 50;
+
 enum TaskStatus : int32_t {
     kTaskOk = 0,
     kTaskCapacity = 1,     // an output list needed more than its capacity (counts are exact)
@@ -81,6 +94,8 @@ struct DpArgs {
     int32_t traceBackDiagonals;
     int32_t diagonalExpansion;
     int32_t sharedRepeat;       // both models use repeat table 0
+    double *expect;             // adjoint only: [2][kExpPerModel]
+    double *expectRep;          // adjoint only: [tables][kRepTable]
 };
 
 // Compaction: task regions of the staged tuples -> per-job final lists.

@@ -159,6 +159,7 @@ struct Ctx {
     uint32_t model;         // 0 forward strand, 1 reverse strand
     int rle;
     int strandFwd;
+    int nTables;            // repeat tables in shared memory (1 when both strands share one)
 };
 
 // Decoded symbols: packed shared-memory byte offsets and the gap emission. For x, the low 17
@@ -382,9 +383,9 @@ __device__ __forceinline__ int initialWindow(int needLo, int needHi) {
 // [sLo, sHi], which zeroes the cell. With CACHE, the cell values and the masked
 // emissions are written to the block cache: rowA / rowB are the byte offsets of this
 // lane's slot 0 in the diagonal's rows, slot j follows at j*L entries.
-template <int C, int L, int PAR, bool CACHE>
+template <int C, int L, int PAR, bool CACHE, bool SYM = false>
 __device__ __forceinline__ void forwardDiagonal(const Ctx &c, Fwd<C> &st, const Slots<C> &sy, int sLo, int sHi,
-                                                uint32_t rowA, uint32_t rowB) {
+                                                uint32_t rowA, uint32_t rowB, uint32_t rowC = 0) {
     float inX[C], inY[C];
     if (PAR) {  // odd d: gap-x source slot i, gap-y source slot i+1
         const float nb = fromNext<L>(st.oy[0], c.gl);
@@ -422,6 +423,8 @@ __device__ __forceinline__ void forwardDiagonal(const Ctx &c, Fwd<C> &st, const 
             sts<float4>(rowA + j * L * 16, make_float4(fM, fX, fY, eM));
             sts<float2>(rowB + j * L * 8, make_float2(eX, eY));
         }
+        // the cell's table offsets (repeat | match << 17), for the adjoint's histograms
+        if (SYM) sts<uint32_t>(rowC + j * L * 4, in ? sy.xpk[j] + sy.ypk[j] : 0xffffffffu);
     }
 }
 
@@ -526,7 +529,7 @@ __device__ __forceinline__ void emitDiagonal(int gl, Out &o, const float (&p)[3]
 // Shared workspace of one group
 // ---------------------------------------------------------------------------
 
-template <int C, int L, int K>
+template <int C, int L, int K, bool ADJ = false>
 struct GroupSmem {
     static constexpr int S = L * C;
     static constexpr int R = RingSize<S>::R;
@@ -535,8 +538,10 @@ struct GroupSmem {
     static constexpr size_t walkBandBytes = K * sizeof(int4);
     static constexpr size_t cacheABytes = (size_t) K * S * sizeof(float4);
     static constexpr size_t cacheBBytes = (size_t) K * S * sizeof(float2);
+    static constexpr size_t cacheCBytes = ADJ ? (size_t) K * S * sizeof(uint32_t) : 0;
     static constexpr size_t infoBytes = K * sizeof(int2);
-    static constexpr size_t bytes = ringBytes + bandRingBytes + walkBandBytes + cacheABytes + cacheBBytes + infoBytes;
+    static constexpr size_t bytes =
+        ringBytes + bandRingBytes + walkBandBytes + cacheABytes + cacheBBytes + cacheCBytes + infoBytes;
 };
 
 template <int C, int L, int K>
@@ -546,8 +551,28 @@ struct GroupMem {
     uint32_t walkBand;  // K band records of the block being walked
     uint32_t cacheA;    // [K][S] float4: fM, fX, fY, eM
     uint32_t cacheB;    // [K][S] float2: eX, eY
+    uint32_t cacheC;    // adjoint only: [K][S] uint32 table offsets of the cell
     uint32_t info;      // [K] int2: window, shift
+    uint32_t hist;      // adjoint only: the block's histograms (small tables, then repeat tables)
 };
+
+// Adjoint histograms in shared memory (floats): match posteriors by (model, x base, y base),
+// gap-x by (model, x base), gap-y by (model, y base), state posteriors at the first and the
+// last cell by (model, state), then the repeat tables.
+constexpr int kHistMatch = 0, kHistGapX = 50, kHistGapY = 60, kHistStart = 70, kHistEnd = 76, kHistSmall = 82;
+
+__host__ __device__ constexpr size_t histBytes(int nTables) {
+    return ((size_t) (kHistSmall + nTables * kRepTable) * sizeof(float) + 15) & ~(size_t) 15;
+}
+
+// Global slot of small-histogram bin i (see kExp* in mp_internal.h).
+__device__ __forceinline__ int expectSlot(int i) {
+    if (i < kHistGapX) return (i / 25) * kExpPerModel + kExpMatch + i % 25;
+    if (i < kHistGapY) return ((i - kHistGapX) / 5) * kExpPerModel + kExpGapX + (i - kHistGapX) % 5;
+    if (i < kHistStart) return ((i - kHistGapY) / 5) * kExpPerModel + kExpGapY + (i - kHistGapY) % 5;
+    if (i < kHistEnd) return ((i - kHistStart) / 3) * kExpPerModel + kExpStart + (i - kHistStart) % 3;
+    return ((i - kHistEnd) / 3) * kExpPerModel + kExpEnd + (i - kHistEnd) % 3;
+}
 
 struct Scratch {
     float4 *chk;      // checkpoints of the group's task: [block][C][L]
@@ -581,14 +606,16 @@ __device__ __forceinline__ void loadFwd(const float4 (&v)[C], Fwd<C> &st) {
 // ---------------------------------------------------------------------------
 
 struct Walk {
-    int D, tbTo, tbFrom, atEnd, active;
+    int D, tbTo, tbFrom, atEnd, active, emit;
     const float *startP;
     const float *endP;
 };
 
-template <int C, int L, int K>
+template <int C, int L, int K, bool ADJ>
 __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm, const Scratch &sc, const Walk &wk,
-                                            float thr, Out &o, double &logLik, bool &bad) {
+                                            float thr, Out &o, double &logLik, bool &bad, double (&accD)[9],
+                                            double *expect) {
+    static_assert(!ADJ || L == 32, "the adjoint runs one task per warp");
     static_assert(K <= L && (K % 2) == 0, "band records of a block are held one per lane");
     constexpr int S = L * C;
     constexpr int R = RingSize<S>::R;
@@ -623,6 +650,7 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
     };
     prefetch(bTop, bTop >= bBot);
     const uint32_t laneA = gm.cacheA + (uint32_t) gl * 16, laneB = gm.cacheB + (uint32_t) gl * 8;
+    const uint32_t laneC = gm.cacheC + (uint32_t) gl * 4;
 
     for (int w = 0; w < nIter; w++) {
         const int b = bTop - w;
@@ -638,6 +666,9 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
         __syncwarp();
         prefetch(b - 1, blockOn && b - 1 >= bBot);
 
+        float ta[9];  // adjoint: this block's transition sums
+#pragma unroll
+        for (int i = 0; i < 9; i++) ta[i] = 0.0f;
         // ---------------- recompute the block ----------------
         int Q;
         int Ef;
@@ -674,10 +705,12 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
                 const int2 b0 = lds<int2>(gm.walkBand + kk * 16);
                 const int2 b1 = lds<int2>(gm.walkBand + (kk + 1) * 16);
                 const uint32_t rowA = laneA + (uint32_t) (kk * S * 16), rowB = laneB + (uint32_t) (kk * S * 8);
+                const uint32_t rowC = laneC + (uint32_t) (kk * S * 4);
                 stepSlots<C, L, R, 0>(gl, gm.rx, gm.ry, d, Q, sy);
-                forwardDiagonal<C, L, 0, true>(c, rs, sy, b0.x - Q, b0.y - Q, rowA, rowB);
+                forwardDiagonal<C, L, 0, true, ADJ>(c, rs, sy, b0.x - Q, b0.y - Q, rowA, rowB, rowC);
                 stepSlots<C, L, R, 1>(gl, gm.rx, gm.ry, d + 1, Q, sy);
-                forwardDiagonal<C, L, 1, true>(c, rs, sy, b1.x - Q, b1.y - Q, rowA + S * 16, rowB + S * 8);
+                forwardDiagonal<C, L, 1, true, ADJ>(c, rs, sy, b1.x - Q, b1.y - Q, rowA + S * 16, rowB + S * 8,
+                                                    rowC + S * 4);
             }
             if (gl < K) sts<int2>(gm.info + gl * 8, make_int2(Q, 0));
         } else {
@@ -707,14 +740,15 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
                     }
                     const int sLo = bd.x - Q, sHi = bd.y - Q;
                     const uint32_t rowA = laneA + (uint32_t) (kk * S * 16), rowB = laneB + (uint32_t) (kk * S * 8);
+                    const uint32_t rowC = laneC + (uint32_t) (kk * S * 4);
                     if (par) {
                         stepSlots<C, L, R, 1>(gl, gm.rx, gm.ry, d, Q, sy);
                         if (rare && reload) loadSlots<C, R>(gl, gm.rx, gm.ry, d, Q, sy);
-                        forwardDiagonal<C, L, 1, true>(c, rs, sy, sLo, sHi, rowA, rowB);
+                        forwardDiagonal<C, L, 1, true, ADJ>(c, rs, sy, sLo, sHi, rowA, rowB, rowC);
                     } else {
                         stepSlots<C, L, R, 0>(gl, gm.rx, gm.ry, d, Q, sy);
                         if (rare && reload) loadSlots<C, R>(gl, gm.rx, gm.ry, d, Q, sy);
-                        forwardDiagonal<C, L, 0, true>(c, rs, sy, sLo, sHi, rowA, rowB);
+                        forwardDiagonal<C, L, 0, true, ADJ>(c, rs, sy, sLo, sHi, rowA, rowB, rowC);
                         if (d == 0) forwardOrigin<C, L, true>(c, wk.startP, Q, rs, rowA, rowB);
                     }
                     if (gl == 0) sts<int2>(gm.info + kk * 8, make_int2(Q, dl));
@@ -741,8 +775,8 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
                 e[j] = lds<float2>(laneB + (uint32_t) ((kk * S + j * L) * 8));
             }
             float bM[C], bX[C], bY[C];
+            float sX[C], sY[C], sM2[C];  // u-values of the gap-x, gap-y and match successors
             {
-                float sX[C], sY[C];
                 if (PAR) {  // odd d: gap-x successor slot i+1, gap-y successor slot i
                     const float nb = fromNext<L>(gX[0], gl);
 #pragma unroll
@@ -763,6 +797,7 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
 #pragma unroll
                 for (int j = 0; j < C; j++) {
                     const float s2 = PAR ? gB[j] : gA[j];
+                    sM2[j] = s2;
                     const float m_ = __fmaf_rn(c.t[0 * 3 + 0], s2, __fmaf_rn(c.t[0 * 3 + 2], sY[j], c.t[0 * 3 + 1] * sX[j]));
                     const float x_ = __fmaf_rn(c.t[1 * 3 + 0], s2, __fmaf_rn(c.t[1 * 3 + 2], sY[j], c.t[1 * 3 + 1] * sX[j]));
                     const float y_ = __fmaf_rn(c.t[2 * 3 + 0], s2, __fmaf_rn(c.t[2 * 3 + 2], sY[j], c.t[2 * 3 + 1] * sX[j]));
@@ -810,7 +845,7 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
             }
             untilRefresh = refresh ? 9 : untilRefresh - (post ? 1 : 0);
             posts += post ? 1 : 0;
-            const bool emit = post && Tm > 0.0f;
+            const bool emit = post && Tm > 0.0f && wk.emit;
             if (FLAT || __any_sync(FULL_MASK, emit)) {
                 const int ex = max(-126, min(127, Ef + Eb - ET));
                 const float scale = emit ? __fdividef(pow2f(ex), Tm) : 0.0f;
@@ -822,6 +857,50 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
                     p[2][j] = (f[j].z * bY[j]) * scale;
                 }
                 emitDiagonal<C, L>(gl, o, p, thr, slotX0(d, inf.x), d, emit);
+            }
+            if constexpr (ADJ) {
+                // expected counts: transitions out of the cells of d (f_from * u_to, scaled by 1/P)
+                // and the emission posteriors of each state, binned by the cell's table entries
+                const bool acc = post && Tm > 0.0f;
+                if (FLAT || __any_sync(FULL_MASK, acc)) {
+                    const int ex = max(-126, min(127, Ef + Eb - ET));
+                    const float scale = acc ? __fdividef(pow2f(ex), Tm) : 0.0f;
+                    const int xl = slotX0(d, inf.x) + gl * C;
+                    float *hs = reinterpret_cast<float *>(mpSmem + gm.hist);
+#pragma unroll
+                    for (int j = 0; j < C; j++) {
+                        const float fm = f[j].x * scale, fx = f[j].y * scale, fy = f[j].z * scale;
+                        ta[0] = __fmaf_rn(fm, sM2[j], ta[0]);
+                        ta[1] = __fmaf_rn(fm, sX[j], ta[1]);
+                        ta[2] = __fmaf_rn(fm, sY[j], ta[2]);
+                        ta[3] = __fmaf_rn(fx, sM2[j], ta[3]);
+                        ta[4] = __fmaf_rn(fx, sX[j], ta[4]);
+                        ta[5] = __fmaf_rn(fx, sY[j], ta[5]);
+                        ta[6] = __fmaf_rn(fy, sM2[j], ta[6]);
+                        ta[7] = __fmaf_rn(fy, sX[j], ta[7]);
+                        ta[8] = __fmaf_rn(fy, sY[j], ta[8]);
+                        const float pm = fm * bM[j], px = fx * bX[j], py = fy * bY[j];
+                        const uint32_t sym = lds<uint32_t>(laneC + (uint32_t) ((kk * S + j * L) * 4));
+                        const int x = xl + j, y = d - x;
+                        const uint32_t mb = sym >> 19;                                  // model*25 + xb*5 + yb
+                        const uint32_t rb = ((sym & 0x1ffffu) - kRepBase) >> 2;         // repeat-table entry
+                        if (sym != 0xffffffffu && mb < 50u) {
+                            if (x > 0 && y > 0 && pm > 0.0f) {
+                                atomicAdd(hs + kHistMatch + mb, pm);
+                                if (c.rle && rb < (uint32_t) (c.nTables * kRepTable))
+                                    atomicAdd(hs + kHistSmall + rb, pm);
+                            }
+                            if (x > 0 && px > 0.0f) atomicAdd(hs + kHistGapX + (mb / 25) * 5 + (mb % 25) / 5, px);
+                            if (y > 0 && py > 0.0f) atomicAdd(hs + kHistGapY + (mb / 25) * 5 + mb % 5, py);
+                        }
+                        if (d == 0 || d == c.N) {  // the first / last cell: the start / end vectors
+                            const int sb = (d == 0 ? kHistStart : kHistEnd) + (int) c.model * 3;
+                            if (pm > 0.0f) atomicAdd(hs + sb, pm);
+                            if (px > 0.0f) atomicAdd(hs + sb + 1, px);
+                            if (py > 0.0f) atomicAdd(hs + sb + 2, py);
+                        }
+                    }
+                }
             }
             // u-values of d (emissions are zero outside the band); kept when the diagonal is off
 #pragma unroll
@@ -876,6 +955,16 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
                 Eb += kx;
             }
         }
+        if constexpr (ADJ) {
+#pragma unroll
+            for (int i = 0; i < 9; i++) accD[i] += (double) ta[i];
+            // the small histograms go to FP64 in global memory after every block
+            float *hs = reinterpret_cast<float *>(mpSmem + gm.hist);
+            for (int i = gl; i < kHistSmall; i += 32) {
+                const float v = atomicExch(hs + i, 0.0f);
+                if (v != 0.0f) atomicAdd(expect + expectSlot(i), (double) v);
+            }
+        }
         __syncwarp();
     }
     if (llSet) logLik += llTm > 0.0f ? log((double) llTm) + (double) llET * 0.69314718055994530942 : -INFINITY;
@@ -914,7 +1003,7 @@ __device__ __forceinline__ int nextTracePoint(const Ctx &c, int from, int maxWid
 // One warp-load of G tasks: forward sweep with checkpoints, then the walks.
 // ---------------------------------------------------------------------------
 
-template <int C, int L, int K>
+template <int C, int L, int K, bool ADJ>
 __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMem<C, L, K> &gm, const Scratch &sc) {
     constexpr int S = L * C;
     constexpr int R = RingSize<S>::R;
@@ -941,6 +1030,7 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
     c.repOff = kRepBase + (a.sharedRepeat ? 0u : (uint32_t) model * (uint32_t) (kRepTable * sizeof(float)));
     c.rle = dm.runLength;
     c.strandFwd = dm.strand;
+    c.nTables = a.sharedRepeat ? 1 : 2;
     const int status0 = has ? to->status : 0;
     const bool tooLong = has && c.N / K + 1 > sc.blocks;
     const bool live = has && c.N > 0 && (status0 & kTaskBand) == 0 && !tooLong;
@@ -1080,25 +1170,49 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
     // Traceback segments in the reference's order: an intermediate point D is the first
     // anti-diagonal after the previous point with D >= tracedBackTo + minDiagsBetweenTraceBack
     // and a narrow band; its posteriors cover (tracedBackTo, D - traceBackDiagonals - 1].
-    // The last segment ends at N and covers (tracedBackTo, N].
+    // The last segment ends at N and covers (tracedBackTo, N]. The likelihood-only mode
+    // (computeForwardProbability) walks just the top diagonal; the adjoint walks the whole
+    // lattice at once (no segments: the gradient of the full forward total).
+    const bool fwdOnly = (flags & kFlagForwardOnly) != 0;
+    const bool single = ADJ || fwdOnly;
     const int maxWidth = 2 * a.diagonalExpansion + 1;
     int prevD = 0, tb = 0;
     bool more = live;
+    double accD[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) accD[i] = 0.0;
     while (__any_sync(FULL_MASK, more)) {
         const int from = max(prevD + 1, tb + a.minDiagsBetweenTraceBack);
-        const int D = nextTracePoint<L>(c, from, maxWidth, more);
+        const int D = single ? c.N : nextTracePoint<L>(c, from, maxWidth, more && !single);
         const bool atEnd = D >= c.N;
         wk.D = c.N < D ? c.N : D;
-        wk.tbTo = tb;
+        wk.tbTo = ADJ ? -1 : (fwdOnly ? c.N - 1 : tb);
         wk.tbFrom = atEnd ? wk.D : wk.D - (a.traceBackDiagonals + 1);
         wk.atEnd = atEnd ? 1 : 0;
         wk.active = more ? 1 : 0;
+        wk.emit = single ? 0 : 1;
         wk.endP = (atEnd && (flags & 2)) ? dm.raggedEnd : dm.end;
-        walkSegment<C, L, K>(c, gm, sc, wk, a.threshold, o, logLik, bad);
+        walkSegment<C, L, K, ADJ>(c, gm, sc, wk, a.threshold, o, logLik, bad, accD, a.expect);
         if (more) {
             tb = wk.tbFrom;
             prevD = wk.D;
             more = !atEnd;
+        }
+    }
+    if constexpr (ADJ) {
+        // transition sums of the task (FP64 warp reduction), then the repeat histograms
+#pragma unroll
+        for (int i = 0; i < 9; i++) {
+            double v = accD[i];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(FULL_MASK, v, off);
+            if (lane == 0 && live && !bad && v != 0.0)
+                atomicAdd(a.expect + (size_t) model * kExpPerModel + kExpTrans + i, v);
+        }
+        float *hr = reinterpret_cast<float *>(mpSmem + gm.hist) + kHistSmall;
+        for (int i = lane; i < c.nTables * kRepTable; i += 32) {
+            const float v = atomicExch(hr + i, 0.0f);
+            if (v != 0.0f) atomicAdd(a.expectRep + i, (double) v);
         }
     }
     if (live && c.gl == 0) {
@@ -1115,9 +1229,9 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
     }
 }
 
-template <int C, int L, int K, int MAXW>
+template <int C, int L, int K, int MAXW, bool ADJ>
 __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
-    using GS = GroupSmem<C, L, K>;
+    using GS = GroupSmem<C, L, K, ADJ>;
     constexpr int G = 32 / L;
     constexpr int R = RingSize<L * C>::R;
     const int nTables = a.sharedRepeat ? 1 : 2;
@@ -1131,13 +1245,18 @@ __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
         gx[i] = a.models[i / 5].gapX[i % 5];
         gy[i] = a.models[i / 5].gapY[i % 5];
     }
+    const uint32_t histOff = (uint32_t) tableBytes(nTables);
+    if (ADJ) {
+        float *h = reinterpret_cast<float *>(mpSmem + histOff);
+        for (int i = threadIdx.x; i < kHistSmall + nTables * kRepTable; i += blockDim.x) h[i] = 0.0f;
+    }
     __syncthreads();
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int g = lane / L;
     const int gwarp = blockIdx.x * (blockDim.x >> 5) + warp;
-    const uint32_t mine = (uint32_t) tableBytes(nTables) + (uint32_t) ((warp * G + g) * GS::bytes);
+    const uint32_t mine = histOff + (ADJ ? (uint32_t) histBytes(nTables) : 0u) + (uint32_t) ((warp * G + g) * GS::bytes);
     GroupMem<C, L, K> gm;
     gm.rx = Ring<R>{mine, 0, 0};
     gm.ry = Ring<R>{mine + (uint32_t) (R * sizeof(uint2)), 0, 0};
@@ -1145,7 +1264,9 @@ __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
     gm.walkBand = gm.bandRing + (uint32_t) GS::bandRingBytes;
     gm.cacheA = gm.walkBand + (uint32_t) GS::walkBandBytes;
     gm.cacheB = gm.cacheA + (uint32_t) GS::cacheABytes;
-    gm.info = gm.cacheB + (uint32_t) GS::cacheBBytes;
+    gm.cacheC = gm.cacheB + (uint32_t) GS::cacheBBytes;
+    gm.info = gm.cacheC + (uint32_t) GS::cacheCBytes;
+    gm.hist = histOff;
     Scratch sc;
     sc.blocks = a.scratchBlocks;
     const size_t slot = (size_t) gwarp * G + g;  // one checkpoint area per task slot
@@ -1159,7 +1280,7 @@ __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
         q = __shfl_sync(FULL_MASK, q, 0);
         if (q >= nLoads) break;
         const int t = q * G + g;
-        runGroup<C, L, K>(a, t < a.nTasks ? a.order[t] : -1, gm, sc);
+        runGroup<C, L, K, ADJ>(a, t < a.nTasks ? a.order[t] : -1, gm, sc);
         __syncwarp();
     }
 }
@@ -1169,19 +1290,20 @@ __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
 // ---------------------------------------------------------------------------
 
 
-template <int C, int L, int K>
+template <int C, int L, int K, bool ADJ = false>
 static size_t smemFor(int warps, int nTables) {
-    return tableBytes(nTables) + (size_t) warps * (32 / L) * GroupSmem<C, L, K>::bytes;
+    return tableBytes(nTables) + (ADJ ? histBytes(nTables) : 0) +
+           (size_t) warps * (32 / L) * GroupSmem<C, L, K, ADJ>::bytes;
 }
 
-template <int C, int L, int K, int MAXW>
+template <int C, int L, int K, int MAXW, bool ADJ = false>
 static cudaError_t launchT(const DpArgs &a, int blocks, int warps, cudaStream_t s) {
     if (warps > MAXW || warps < 1) return cudaErrorInvalidValue;
-    const size_t smem = smemFor<C, L, K>(warps, a.sharedRepeat ? 1 : 2);
-    cudaError_t e = cudaFuncSetAttribute(posteriorKernel<C, L, K, MAXW>,
+    const size_t smem = smemFor<C, L, K, ADJ>(warps, a.sharedRepeat ? 1 : 2);
+    cudaError_t e = cudaFuncSetAttribute(posteriorKernel<C, L, K, MAXW, ADJ>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     if (e != cudaSuccess) return e;
-    posteriorKernel<C, L, K, MAXW><<<blocks, warps * 32, smem, s>>>(a);
+    posteriorKernel<C, L, K, MAXW, ADJ><<<blocks, warps * 32, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -1196,6 +1318,12 @@ static cudaError_t launchT(const DpArgs &a, int blocks, int warps, cudaStream_t 
     X(4, 4, 32, 4, 8)  \
     X(5, 6, 32, 4, 8)  \
     X(6, 8, 32, 4, 5)
+
+// Adjoint variants (one task per warp; the block also holds the expected-count histograms).
+#define MP_ADJ_VARIANTS(X) \
+    X(0, 2, 32, 8, 8)      \
+    X(1, 3, 32, 8, 4)      \
+    X(2, 4, 32, 4, 6)
 
 int variantCount() {
     return 7;
@@ -1232,6 +1360,45 @@ cudaError_t launchVariant(int v, const DpArgs &a, int blocks, int warps, cudaStr
 #define MP_LAUNCH(i, c_, l_, k_, w_) \
     case i: return launchT<c_, l_, k_, w_>(a, blocks, warps, s);
         MP_VARIANTS(MP_LAUNCH)
+#undef MP_LAUNCH
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+int adjointVariantCount() {
+    return 3;
+}
+
+bool adjointVariantShape(int v, int *C, int *L, int *K) {
+    switch (v) {
+#define MP_SHAPE(i, c_, l_, k_, w_) \
+    case i: *C = c_; *L = l_; *K = k_; return true;
+        MP_ADJ_VARIANTS(MP_SHAPE)
+#undef MP_SHAPE
+        default: return false;
+    }
+}
+
+int adjointVariantMaxWarps(int v, int nTables) {
+    const size_t limit = 227 * 1024;
+    switch (v) {
+#define MP_MAXW(i, c_, l_, k_, w_)                                                \
+    case i: {                                                                     \
+        int w = w_;                                                               \
+        while (w > 1 && smemFor<c_, l_, k_, true>(w, nTables) > limit) w--;       \
+        return smemFor<c_, l_, k_, true>(w, nTables) > limit ? 0 : w;             \
+    }
+        MP_ADJ_VARIANTS(MP_MAXW)
+#undef MP_MAXW
+        default: return 0;
+    }
+}
+
+cudaError_t launchAdjointVariant(int v, const DpArgs &a, int blocks, int warps, cudaStream_t s) {
+    switch (v) {
+#define MP_LAUNCH(i, c_, l_, k_, w_) \
+    case i: return launchT<c_, l_, k_, w_, true>(a, blocks, warps, s);
+        MP_ADJ_VARIANTS(MP_LAUNCH)
 #undef MP_LAUNCH
         default: return cudaErrorInvalidValue;
     }

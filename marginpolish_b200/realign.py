@@ -9,7 +9,13 @@ operator API for this path:
   poa_realign (impl/polisher.c:605-654), including the reference crop and the
   gap-x -> deletes / gap-y -> inserts naming;
 * ``realign_batch`` -- all reads of all chunks in one call (the batched form
-  poa_realignAll's per-read loop maps onto).
+  poa_realignAll's per-read loop maps onto);
+* ``compute_forward_probability`` / ``forward_batch`` -- computeForwardProbability
+  (impl/pairwiseAligner.c:813-865), the forward log-likelihood the bubble graph
+  scores alleles with (impl/bubbleGraph.c:924);
+* ``expectations_batch`` -- expected counts of transitions and emissions, i.e. the
+  gradient of the summed log-likelihood with respect to the log parameters
+  (the Baum-Welch counts of getExpectationsUsingAnchors, :1151-1156).
 
 Every call goes through the CUDA library (libmpgpu.so); errors of the C ABI
 are raised as MpError.
@@ -404,3 +410,52 @@ def get_aligned_pairs_using_anchors(engine: Engine, model: Model, sx, sy, anchor
                                     strand: int = 1, ragged_left: bool = False, ragged_right: bool = False):
     return get_aligned_pairs_with_indels_using_anchors(engine, model, sx, sy, anchors, params, strand,
                                                        ragged_left, ragged_right)[0]
+
+
+def forward_batch(engine: Engine, model: Model, params: AlignmentParams, jobs: Jobs) -> np.ndarray:
+    """ln P of every job over the band of band_construct (fixed expansion
+    params.diagonal_expansion; the anchors' own expansions are ignored), no splits."""
+    out = np.zeros(max(jobs.n_jobs, 1), dtype=np.float64)
+    ps, bs = params.struct(), jobs.struct()
+    _lib.check(engine._lib.mp_forward_batch(engine.handle, model.handle, ctypes.byref(ps), ctypes.byref(bs),
+                                            _lib.ptr(out, ctypes.c_double)))
+    return out[:jobs.n_jobs]
+
+
+def compute_forward_probability(engine: Engine, model: Model, sx, sy, anchors, params: AlignmentParams,
+                                strand: int = 1, ragged_left: bool = False, ragged_right: bool = False) -> float:
+    """computeForwardProbability for one pair of sequences (anchors may be empty)."""
+    return float(forward_batch(engine, model, params, Jobs.single(sx, sy, anchors, strand, ragged_left,
+                                                                  ragged_right))[0])
+
+
+@dataclass
+class Expectations:
+    """Expected counts of a batch (see mp_expectations_batch): per model m (0 forward
+    strand, 1 reverse) transitions[m] (3x3, from x to), match[m] (5x5, x base x y base),
+    gap_x[m], gap_y[m] (5), start[m], end[m] (state posteriors at the first / last cell),
+    repeat[t] (4 x 51 x 51 by run-length table), the summed ln P and each job's ln P."""
+    transitions: np.ndarray
+    match: np.ndarray
+    gap_x: np.ndarray
+    gap_y: np.ndarray
+    start: np.ndarray
+    end: np.ndarray
+    repeat: np.ndarray
+    log_likelihood: float
+    job_log_likelihood: np.ndarray
+
+
+def expectations_batch(engine: Engine, model: Model, params: AlignmentParams, jobs: Jobs) -> Expectations:
+    """Gradient of the summed log-likelihood with respect to the log transition and
+    emission parameters (expected counts), from the adjoint kernel."""
+    e = _lib.Expectations()
+    ll = np.zeros(max(jobs.n_jobs, 1), dtype=np.float64)
+    ps, bs = params.struct(), jobs.struct()
+    _lib.check(engine._lib.mp_expectations_batch(engine.handle, model.handle, ctypes.byref(ps), ctypes.byref(bs),
+                                                 ctypes.byref(e), _lib.ptr(ll, ctypes.c_double)))
+    arr = lambda v, shape: np.ctypeslib.as_array(v).reshape(shape).copy()  # noqa: E731
+    return Expectations(arr(e.transitions, (2, 3, 3)), arr(e.match, (2, 5, 5)), arr(e.gap_x, (2, 5)),
+                        arr(e.gap_y, (2, 5)), arr(e.start, (2, 3)), arr(e.end, (2, 3)),
+                        arr(e.repeat, (2, 4, 51, 51)), float(e.log_likelihood),
+                        ll[:jobs.n_jobs].copy())

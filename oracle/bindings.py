@@ -219,6 +219,29 @@ class RefOracle:
     def logadd_address(self) -> int:
         return ctypes.cast(self.lib.refo_logadd, c_void_p).value
 
+    def forward_probability(self, h, sx, sy, anchors, params, ragged_left=False, ragged_right=False) -> float:
+        """The reference's computeForwardProbability (impl/pairwiseAligner.c:813-865)."""
+        sx = np.ascontiguousarray(sx, dtype=np.uint16)
+        sy = np.ascontiguousarray(sy, dtype=np.uint16)
+        a = np.ascontiguousarray(np.asarray(anchors, dtype=np.int64).reshape(-1, 3))
+        op = OracleParams.from_alignment(params)
+        return self.lib.refo_forward_probability(h, _p(sx, c_uint16), sx.size, _p(sy, c_uint16), sy.size,
+                                                 _p(a, c_int64), a.shape[0], ctypes.byref(op), int(ragged_left),
+                                                 int(ragged_right))
+
+    def expectations(self, h, hmm_type, sx, sy, anchors, params, ragged_left=False, ragged_right=False):
+        """The reference's getExpectationsUsingAnchors: (9 transition counts, its likelihood sum)."""
+        sx = np.ascontiguousarray(sx, dtype=np.uint16)
+        sy = np.ascontiguousarray(sy, dtype=np.uint16)
+        a = np.ascontiguousarray(np.asarray(anchors, dtype=np.int64).reshape(-1, 3))
+        op = OracleParams.from_alignment(params)
+        t = np.zeros(9)
+        lk = c_double(0.0)
+        self.lib.refo_expectations(h, hmm_type, _p(sx, c_uint16), sx.size, _p(sy, c_uint16), sy.size,
+                                   _p(a, c_int64), a.shape[0], ctypes.byref(op), int(ragged_left), int(ragged_right),
+                                   _p(t, c_double), ctypes.byref(lk))
+        return t, lk.value
+
 
 def _gather_x(jobs):
     """Per-job contiguous X symbols and monotone offsets (the oracle harness layout)."""
@@ -252,6 +275,12 @@ class ExactOracle:
         lib.mpo_gap_x_emission.argtypes = [P(MpoModel), c_uint16]
         lib.mpo_gap_y_emission.restype = c_double
         lib.mpo_gap_y_emission.argtypes = [P(MpoModel), c_uint16]
+        lib.mpo_forward_probability.restype = c_double
+        lib.mpo_forward_probability.argtypes = [P(MpoModel), P(c_uint16), c_int64, P(c_uint16), c_int64, P(c_int64),
+                                                c_int64, c_int64, c_int, c_int, c_int, c_void_p]
+        lib.mpo_expectations.restype = c_double
+        lib.mpo_expectations.argtypes = [P(MpoModel), P(c_uint16), c_int64, P(c_uint16), c_int64, P(c_int64),
+                                         c_int64, c_int64, c_int, c_int, c_int, P(c_double)]
         lib.mpo_align_batch.restype = c_int64
         lib.mpo_align_batch.argtypes = [P(MpoModel), P(MpoModel), c_int64, P(c_int64), P(c_uint16), P(c_int64),
                                         P(c_uint16), P(c_int64), P(c_int64), P(c_uint8), P(OracleParams), c_int,
@@ -306,3 +335,27 @@ class ExactOracle:
         self.lib.mpo_split_points(_p(a, c_int64), a.shape[0], lx, ly, max_size, int(ragged_left),
                                   int(ragged_right), _p(out, c_int64), n)
         return out[:n]
+
+    def forward_probability(self, model: MpoModel, sx, sy, anchors, expansion, dynamic=False, ragged_left=False,
+                            ragged_right=False, logadd=None) -> float:
+        """ln P over the band (band_construct when not dynamic), FP64, exact log-sum unless logadd."""
+        sx = np.ascontiguousarray(sx, dtype=np.uint16)
+        sy = np.ascontiguousarray(sy, dtype=np.uint16)
+        a = np.ascontiguousarray(np.asarray(anchors, dtype=np.int64).reshape(-1, 3))
+        return self.lib.mpo_forward_probability(ctypes.byref(model), _p(sx, c_uint16), sx.size, _p(sy, c_uint16),
+                                                sy.size, _p(a, c_int64), a.shape[0], int(expansion), int(dynamic),
+                                                int(ragged_left), int(ragged_right), logadd)
+
+    def expectations(self, model: MpoModel, sx, sy, anchors, expansion, dynamic=True, ragged_left=False,
+                     ragged_right=False):
+        """Exact FP64 expected counts over the whole band: (ln P, dict of count arrays)."""
+        sx = np.ascontiguousarray(sx, dtype=np.uint16)
+        sy = np.ascontiguousarray(sy, dtype=np.uint16)
+        a = np.ascontiguousarray(np.asarray(anchors, dtype=np.int64).reshape(-1, 3))
+        out = np.zeros(50 + 4 * 51 * 51)
+        lp = self.lib.mpo_expectations(ctypes.byref(model), _p(sx, c_uint16), sx.size, _p(sy, c_uint16), sy.size,
+                                       _p(a, c_int64), a.shape[0], int(expansion), int(dynamic), int(ragged_left),
+                                       int(ragged_right), _p(out, c_double))
+        return lp, {"transitions": out[0:9].copy(), "match": out[9:34].copy(), "gap_x": out[34:39].copy(),
+                    "gap_y": out[39:44].copy(), "start": out[44:47].copy(), "end": out[47:50].copy(),
+                    "repeat": out[50:].copy()}

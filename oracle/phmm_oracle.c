@@ -508,6 +508,167 @@ static int runSubProblem(const MpoModel *m, const MpoParams *p, MpoLogAddFn add,
 }
 
 /* ------------------------------------------------------------------ */
+/* Forward likelihood and expected counts over a whole band            */
+/* ------------------------------------------------------------------ */
+
+/* Band + full forward matrix of one sub-problem; returns 0, -1 on an invalid band. */
+static int fullForward(Sub *s, const MpoModel *m, MpoLogAddFn add, const uint16_t *sx, int64_t lx, const uint16_t *sy,
+                       int64_t ly, const int64_t *anchors, int64_t nAnchors, int64_t expansion, int dynamic,
+                       int raggedLeft) {
+    memset(s, 0, sizeof(*s));
+    s->m = m;
+    s->add = add;
+    s->sx = sx;
+    s->sy = sy;
+    s->lx = lx;
+    s->ly = ly;
+    s->N = lx + ly;
+    int64_t *band = malloc(sizeof(int64_t) * 3 * (s->N + 1));
+    if (mpo_band(anchors, nAnchors, lx, ly, expansion, dynamic, band) != 0) {
+        free(band);
+        return -1;
+    }
+    s->lo = malloc(sizeof(int64_t) * (s->N + 1));
+    s->hi = malloc(sizeof(int64_t) * (s->N + 1));
+    s->off = malloc(sizeof(int64_t) * (s->N + 2));
+    int64_t total = 0;
+    for (int64_t d = 0; d <= s->N; d++) {
+        s->lo[d] = band[3 * d + 1];
+        s->hi[d] = band[3 * d + 2];
+        s->off[d] = total;
+        total += (s->hi[d] - s->lo[d]) / 2 + 1;
+    }
+    s->off[s->N + 1] = total;
+    free(band);
+    s->F = malloc(sizeof(double) * 3 * total);
+    s->B = malloc(sizeof(double) * 3 * total);
+    s->bLive = calloc(s->N + 2, 1);
+    for (int64_t i = 0; i < 3 * total; i++) {
+        s->F[i] = NEG_INF;
+        s->B[i] = NEG_INF;
+    }
+    setDiagonal(s, s->F, 0, raggedLeft ? m->raggedStart : m->start);
+    for (int64_t d = 1; d <= s->N; d++) {
+        forwardDiagonal(s, d);
+    }
+    return 0;
+}
+
+static void freeSub(Sub *s) {
+    free(s->lo);
+    free(s->hi);
+    free(s->off);
+    free(s->F);
+    free(s->B);
+    free(s->bLive);
+}
+
+double mpo_forward_probability(const MpoModel *model, const uint16_t *sx, int64_t lx, const uint16_t *sy,
+                               int64_t ly, const int64_t *anchors, int64_t nAnchors, int64_t expansion, int dynamic,
+                               int raggedLeft, int raggedRight, MpoLogAddFn logAdd) {
+    if (logAdd == NULL) {
+        logAdd = mpo_logadd_exact;
+    }
+    if (lx + ly == 0) {
+        return 0.0;
+    }
+    Sub s;
+    if (fullForward(&s, model, logAdd, sx, lx, sy, ly, anchors, nAnchors, expansion, dynamic, raggedLeft) != 0) {
+        freeSub(&s);
+        return NAN;
+    }
+    /* diagonalCalculationTotalProbability at the last diagonal: no diagonal follows it */
+    setDiagonal(&s, s.B, s.N, raggedRight ? model->raggedEnd : model->end);
+    s.bLive[s.N] = 1;
+    double total = totalProbability(&s, s.N);
+    freeSub(&s);
+    return total;
+}
+
+/* Run-length table entry of a match emission (the index mpo_match_emission reads), -1 if none. */
+static int64_t repeatEntry(const MpoModel *m, uint16_t cx, uint16_t cy) {
+    if (!m->runLength || m->repeat10 == NULL) {
+        return -1;
+    }
+    int64_t M = m->maxRepeat;
+    int xb = symbolBase(m, cx);
+    int b = xb == 4 ? 0 : xb;
+    int row = m->strand ? b : 3 - b;
+    return (row * M + (cx >> 8)) * M + (cy >> 8);
+}
+
+double mpo_expectations(const MpoModel *model, const uint16_t *sx, int64_t lx, const uint16_t *sy, int64_t ly,
+                        const int64_t *anchors, int64_t nAnchors, int64_t expansion, int dynamic, int raggedLeft,
+                        int raggedRight, double *out) {
+    if (lx + ly == 0) {
+        return 0.0;
+    }
+    Sub s;
+    if (fullForward(&s, model, mpo_logadd_exact, sx, lx, sy, ly, anchors, nAnchors, expansion, dynamic,
+                    raggedLeft) != 0) {
+        freeSub(&s);
+        return NAN;
+    }
+    for (int64_t d = 0; d <= s.N; d++) {
+        s.bLive[d] = 1;
+    }
+    setDiagonal(&s, s.B, s.N, raggedRight ? model->raggedEnd : model->end);
+    for (int64_t d = s.N; d >= 1; d--) {
+        backwardDiagonal(&s, d);
+    }
+    const double P = totalProbability(&s, s.N);
+    const double *t = model->trans;
+    {  /* state posteriors at the first and the last cell */
+        const double *f0 = cellOf(&s, s.F, 0, 0), *b0 = cellOf(&s, s.B, 0, 0);
+        const double *fN = cellOf(&s, s.F, s.N, lx - ly), *bN = cellOf(&s, s.B, s.N, lx - ly);
+        for (int k = 0; k < 3; k++) {
+            if (f0 != NULL && b0 != NULL) out[44 + k] += exp(f0[k] + b0[k] - P);
+            if (fN != NULL && bN != NULL) out[47 + k] += exp(fN[k] + bN[k] - P);
+        }
+    }
+    for (int64_t d = 1; d <= s.N; d++) {
+        for (int64_t xmy = s.lo[d]; xmy <= s.hi[d]; xmy += 2) {
+            const int64_t x = (d + xmy) / 2, y = (d - xmy) / 2;
+            const double *b = cellOf(&s, s.B, d, xmy), *f = cellOf(&s, s.F, d, xmy);
+            const double *lower = cellOf(&s, s.F, d - 1, xmy - 1);
+            const double *middle = d >= 2 ? cellOf(&s, s.F, d - 2, xmy) : NULL;
+            const double *upper = cellOf(&s, s.F, d - 1, xmy + 1);
+            const uint16_t cx = xSymbolAt(&s, d, xmy), cy = ySymbolAt(&s, d, xmy);
+            /* transitions into this cell (cell_calculateExpectation, impl/pairwiseAligner.c:347-369) */
+            for (int i = 0; i < 3; i++) {
+                if (lower != NULL) {
+                    out[i * 3 + 1] += exp(lower[i] + t[i * 3 + 1] + mpo_gap_x_emission(model, cx) + b[1] - P);
+                }
+                if (middle != NULL) {
+                    out[i * 3 + 0] += exp(middle[i] + t[i * 3 + 0] + mpo_match_emission(model, cx, cy) + b[0] - P);
+                }
+                if (upper != NULL) {
+                    out[i * 3 + 2] += exp(upper[i] + t[i * 3 + 2] + mpo_gap_y_emission(model, cy) + b[2] - P);
+                }
+            }
+            /* state posteriors by emitted symbols */
+            const int xb = symbolBase(model, cx), yb = symbolBase(model, cy);
+            if (x > 0 && y > 0) {
+                const double pm = exp(f[0] + b[0] - P);
+                out[9 + xb * 5 + yb] += pm;
+                const int64_t r = repeatEntry(model, cx, cy);
+                if (r >= 0) {
+                    out[50 + r] += pm;
+                }
+            }
+            if (x > 0) {
+                out[34 + xb] += exp(f[1] + b[1] - P);
+            }
+            if (y > 0) {
+                out[39 + yb] += exp(f[2] + b[2] - P);
+            }
+        }
+    }
+    freeSub(&s);
+    return P;
+}
+
+/* ------------------------------------------------------------------ */
 /* Public job entry: splits + coordinate correction                    */
 /* (getPosteriorProbsWithBandingSplittingAlignmentsByLargeGaps :942-991,*/
 /*  pairCoordinateCorrectionFn :1077-1086)                              */

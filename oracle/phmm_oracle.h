@@ -82,6 +82,26 @@ double mpo_match_emission(const MpoModel *m, uint16_t cx, uint16_t cy);
 double mpo_gap_x_emission(const MpoModel *m, uint16_t cx);
 double mpo_gap_y_emission(const MpoModel *m, uint16_t cy);
 
+/* Forward log-probability (computeForwardProbability, impl/pairwiseAligner.c:813-865): the
+ * forward recursion over the band (band_construct with the fixed expansion when dynamic is 0,
+ * as the reference; band_constructDynamic with the anchors' expansions when 1), total at the
+ * last anti-diagonal with the (ragged) end probabilities. No splits, no traceback segments.
+ * Returns 0 (LOG_ONE) for lx + ly = 0 and NaN on an invalid band. logAdd NULL = exact. */
+double mpo_forward_probability(const MpoModel *model, const uint16_t *sx, int64_t lx, const uint16_t *sy,
+                               int64_t ly, const int64_t *anchors, int64_t nAnchors, int64_t expansion, int dynamic,
+                               int raggedLeft, int raggedRight, MpoLogAddFn logAdd);
+
+/* Expected counts of one sub-problem by exact FP64 forward-backward over the whole band
+ * (no traceback segments, no splits): out[0..8] transitions (from*3+to), out[9..33] match
+ * posteriors by (x base, y base), out[34..38] gap-x by x base, out[39..43] gap-y by y base,
+ * out[44..46] / out[47..49] state posteriors at the first / last cell,
+ * out[50 .. 50 + 4*M*M) match posteriors by run-length table entry [row][rcx][rcy]
+ * (M = model->maxRepeat; only when the model is run-length). Counts are added to out.
+ * Returns ln P, NaN on an invalid band. */
+double mpo_expectations(const MpoModel *model, const uint16_t *sx, int64_t lx, const uint16_t *sy, int64_t ly,
+                        const int64_t *anchors, int64_t nAnchors, int64_t expansion, int dynamic, int raggedLeft,
+                        int raggedRight, double *out);
+
 /* Exact log-sum used by default. */
 double mpo_logadd_exact(double a, double b);
 

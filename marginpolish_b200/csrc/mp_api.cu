@@ -26,6 +26,7 @@
 namespace mp {
 int variantCount();
 bool variantShape(int v, int *C, int *L, int *K);
+bool variantIsF64(int v);
 int variantMaxWarps(int v, int nTables);
 cudaError_t launchVariant(int v, const DpArgs &a, int blocks, int warps, cudaStream_t s);
 int adjointVariantCount();
@@ -391,6 +392,20 @@ static int pickVariant(int lanes, int64_t slots) {
     return -1;
 }
 
+// FP64 variants (one task per warp), narrowest window that holds the hull; -1 if none.
+static int pickVariantF64(int64_t slots) {
+    for (int v = 0; v < variantCount(); v++) {
+        if (!variantIsF64(v)) continue;
+        if (slots <= variantCapacity(v)) return v;
+    }
+    return -1;
+}
+
+// Bytes of one checkpoint slot of a variant (float4 or double4).
+static size_t chkElemBytes(int v) {
+    return variantIsF64(v) ? 32 : 16;
+}
+
 // Adjoint variants (one task per warp), narrowest window that holds the hull; -1 if none.
 static int pickAdjointVariant(int64_t slots) {
     for (int v = 0; v < adjointVariantCount(); v++) {
@@ -470,6 +485,7 @@ struct mp_device_batch {
     int64_t nJobs = 0;
     std::vector<Task> tasks;
     std::vector<int32_t> hull;          // per task: window slots needed (raised by window retries)
+    std::vector<uint8_t> f64;           // per task: computed in FP64 (likelihood-only mode, or range retry)
     std::vector<int> var;               // per task: kernel variant of the current run
     std::vector<int64_t> jobFirstTask;  // n_jobs+1
     int64_t totalDiags = 0;
@@ -673,6 +689,8 @@ static mp_status planBatch(mp_device_batch *db, const mp_batch *b) {
         }
     }
     db->totalDiags = bandOff;
+    // the likelihood-only mode has no second total to check its range against: FP64 throughout
+    db->f64.assign(db->tasks.size(), db->mode == kModeForward ? 1 : 0);
     for (int k = 0; k < 3; k++) db->outCap[k] = outOff[k];
     return MP_OK;
 }
@@ -716,7 +734,8 @@ static mp_status buildQueues(mp_device_batch *db, const std::vector<int32_t> &su
     std::vector<std::vector<int32_t>> per(nV);
     for (int32_t t : subset) {
         const int v = db->mode == kModeAdjoint ? pickAdjointVariant(db->hull[t])
-                                               : pickVariant(db->e->tuning.lanes_per_task, db->hull[t]);
+                      : db->f64[t]           ? pickVariantF64(db->hull[t])
+                                             : pickVariant(db->e->tuning.lanes_per_task, db->hull[t]);
         if (v < 0)
             return failf(MP_ERR_OVERFLOW, "job %d: band wider than the widest kernel window", db->tasks[t].job);
         db->var[t] = v;
@@ -823,7 +842,8 @@ static mp_status launchQueues(mp_device_batch *db) {
         const int blocks = std::max(1, std::min(e->smCount * blocksPerSm, maxBlocks));
         const int scratchBlocks = (int) (db->varMaxN[v] / K + 2);
         const size_t slots = (size_t) blocks * warps * G;
-        needScratch = std::max(needScratch, (size_t) scratchBlocks * (size_t) (C * L) * sizeof(float4) * slots);
+        const size_t elem = adj ? sizeof(float4) : chkElemBytes(v);
+        needScratch = std::max(needScratch, (size_t) scratchBlocks * (size_t) (C * L) * elem * slots);
         needScal = std::max(needScal, sizeof(int2) * (size_t) scratchBlocks * slots);
         blocksOf[v] = blocks;
         warpsOf[v] = warps;
@@ -912,6 +932,18 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
             if (o.status & kTaskSymbol) {
                 return failf(MP_ERR_ARGUMENT, "job %d: a symbol's repeat count is >= %d", db->tasks[t].job,
                              kMaxRepeat);
+            }
+            if (o.status & kTaskRange) {
+                // FP32 lost the range (wide band of weakly related sequences): again in FP64
+                if (db->mode == kModeAdjoint || db->f64[t])
+                    return failf(MP_ERR_OVERFLOW,
+                                 "job %d: the band's probabilities exceed the range of the %s scaled "
+                                 "arithmetic", db->tasks[t].job, db->f64[t] ? "FP64" : "FP32");
+                db->f64[t] = 1;
+                o.status &= ~kTaskRange;
+                retry.push_back(t);
+                changed = true;
+                continue;
             }
             if (o.status & (kTaskCapacity | kTaskWindow | kTaskScratch)) {
                 if (o.status & kTaskWindow) {
@@ -1011,7 +1043,7 @@ extern "C" mp_status mp_device_batch_run_plain(mp_engine *e, mp_device_batch *db
     for (int v = 0; v < variantCount(); v++) {
         int C = 0, L = 0, K = 0;
         variantShape(v, &C, &L, &K);
-        needScratch = std::max(needScratch, (size_t) (maxN / K + 2) * (size_t) (C * L) * sizeof(float4) * (32 / L));
+        needScratch = std::max(needScratch, (size_t) (maxN / K + 2) * (size_t) (C * L) * chkElemBytes(v) * (32 / L));
         needScal = std::max(needScal, sizeof(int2) * (size_t) (maxN / K + 2) * (32 / L));
     }
     CUDA_TRY(cudaStreamSynchronize(st));

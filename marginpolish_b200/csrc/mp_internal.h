@@ -63,7 +63,8 @@ enum TaskStatus : int32_t {
     kTaskWindow = 2,       // band hull wider than the slot window of the class
     kTaskBand = 4,         // invalid diagonal (reference: exception)
     kTaskScratch = 8,      // checkpoint scratch too small
-    kTaskSymbol = 16       // a symbol's repeat count is >= kMaxRepeat
+    kTaskSymbol = 16,      // a symbol's repeat count is >= kMaxRepeat
+    kTaskRange = 32        // the walk's totals disagree: the scaled values lost their range
 };
 
 struct TaskOut {
@@ -85,7 +86,7 @@ struct DpArgs {
     const int2 *band;           // (xmyL, xmyR) per diagonal
     const DevModel *models;     // [0] forward strand, [1] reverse strand
     const float *repeatProb;    // [2][4][51][51] exp(scale*log10 table), per model
-    float4 *scratch;            // per task slot: checkpoints [block][window slot]
+    void *scratch;              // per task slot: checkpoints [block][window slot] (float4 or double4)
     int2 *scratchScalars;       // per task slot: (exponent, window) per checkpoint
     int4 *outT[3];              // per list: staged tuples (weight, x, y, 0) in per-task regions
     TaskOut *out;

@@ -201,6 +201,9 @@ extern "C" mp_status mp_realign_single_noalloc(mp_engine *e, const mp_model *m, 
     if (res.status & kTaskSymbol) return mp_fail(MP_ERR_ARGUMENT, "a symbol's repeat count is >= %d", kMaxRepeat);
     if (res.status & (kTaskWindow | kTaskScratch))
         return mp_fail(MP_ERR_OVERFLOW, "no-allocation pass exceeded its band window or checkpoint area");
+    if (res.status & kTaskRange)
+        return mp_fail(MP_ERR_OVERFLOW,
+                       "the band's probabilities exceed the range of FP32 scaled arithmetic; use mp_realign_batch");
     out->log_likelihood = res.logLik;
     out->cells = res.cells;
     bool tooSmall = false;

@@ -88,16 +88,58 @@ __device__ __forceinline__ int exponentOf(float m) {  // floor(log2 m) for norma
     return ((__float_as_int(m) >> 23) & 0xff) - 127;
 }
 
+// Arithmetic of the scaled probabilities: FP32 for the production kernels, FP64 for the
+// sub-problems whose dynamic range FP32 cannot hold (wide bands of weakly related
+// sequences, detected by the total-probability check) and for the likelihood-only mode.
+template <class V>
+struct Num;
+
+template <>
+struct Num<float> {
+    using V4 = float4;
+    using V2 = float2;
+    static constexpr int kMinExp = -126, kMaxExp = 127;
+    __device__ static __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+    __device__ static __forceinline__ float mx(float a, float b) { return fmaxf(a, b); }
+    __device__ static __forceinline__ float pow2(int k) { return pow2f(k); }
+    __device__ static __forceinline__ int expOf(float m) { return exponentOf(m); }
+    __device__ static __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
+    __device__ static __forceinline__ float4 v4(float a, float b, float c, float d) { return make_float4(a, b, c, d); }
+    __device__ static __forceinline__ float2 v2(float a, float b) { return make_float2(a, b); }
+    __device__ static __forceinline__ int32_t weight(float p) {  // floor(min(p, 1) * 10^7)
+        return (int32_t) floorf(fminf(p, 1.0f) * (float) kProbOne);
+    }
+};
+
+template <>
+struct Num<double> {
+    using V4 = double4;
+    using V2 = double2;
+    static constexpr int kMinExp = -1022, kMaxExp = 1023;
+    __device__ static __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+    __device__ static __forceinline__ double mx(double a, double b) { return fmax(a, b); }
+    __device__ static __forceinline__ double pow2(int k) { return __longlong_as_double((long long) (1023 + k) << 52); }
+    __device__ static __forceinline__ int expOf(double m) {
+        return (int) ((__double_as_longlong(m) >> 52) & 0x7ff) - 1023;
+    }
+    __device__ static __forceinline__ double div(double a, double b) { return a / b; }
+    __device__ static __forceinline__ double4 v4(double a, double b, double c, double d) {
+        return make_double4(a, b, c, d);
+    }
+    __device__ static __forceinline__ double2 v2(double a, double b) { return make_double2(a, b); }
+    __device__ static __forceinline__ int32_t weight(double p) { return (int32_t) floor(fmin(p, 1.0) * (double) kProbOne); }
+};
+
 // Reductions within an aligned group of L lanes.
-template <int L>
-__device__ __forceinline__ float groupMax(float v) {
+template <int L, class V>
+__device__ __forceinline__ V groupMax(V v) {
 #pragma unroll
-    for (int o = L / 2; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(FULL_MASK, v, o));
+    for (int o = L / 2; o > 0; o >>= 1) v = Num<V>::mx(v, __shfl_xor_sync(FULL_MASK, v, o));
     return v;
 }
 
-template <int L>
-__device__ __forceinline__ float groupSum(float v) {
+template <int L, class V>
+__device__ __forceinline__ V groupSum(V v) {
 #pragma unroll
     for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(FULL_MASK, v, o);
     return v;
@@ -110,17 +152,17 @@ __device__ __forceinline__ int warpMaxInt(int v) {
 }
 
 // Value held by lane gl+1 of the group (0 past the group's last lane).
-template <int L>
-__device__ __forceinline__ float fromNext(float v, int gl) {
-    const float r = __shfl_down_sync(FULL_MASK, v, 1, L);
-    return gl == L - 1 ? 0.0f : r;
+template <int L, class V>
+__device__ __forceinline__ V fromNext(V v, int gl) {
+    const V r = __shfl_down_sync(FULL_MASK, v, 1, L);
+    return gl == L - 1 ? V(0) : r;
 }
 
 // Value held by lane gl-1 of the group (0 before the group's first lane).
-template <int L>
-__device__ __forceinline__ float fromPrev(float v, int gl) {
-    const float r = __shfl_up_sync(FULL_MASK, v, 1, L);
-    return gl == 0 ? 0.0f : r;
+template <int L, class V>
+__device__ __forceinline__ V fromPrev(V v, int gl) {
+    const V r = __shfl_up_sync(FULL_MASK, v, 1, L);
+    return gl == 0 ? V(0) : r;
 }
 
 // This group's bits of a warp ballot, shifted down to bit 0.
@@ -147,6 +189,7 @@ __device__ __forceinline__ void cpAsyncWaitAllButOne() {
 // Task context (identical over the lanes of a group)
 // ---------------------------------------------------------------------------
 
+template <class V>
 struct Ctx {
     int gl;                 // lane within the group
     int g;                  // group within the warp
@@ -154,7 +197,7 @@ struct Ctx {
     const uint16_t *xs;
     const uint16_t *ys;
     const int4 *band;       // (band lo, band hi, hull lo, hull hi) of d = 0..N, in window slots
-    float t[9];
+    V t[9];                 // transitions from*3+to, in the arithmetic type
     uint32_t repOff;        // byte offset of the task's repeat table in shared memory
     uint32_t model;         // 0 forward strand, 1 reverse strand
     int rle;
@@ -168,7 +211,8 @@ struct Ctx {
 // columns. The sum of an x and a y symbol therefore holds both cell offsets (the low part stays
 // below 2^17, so it never carries). Positions outside the sequence decode to 'N' with repeat
 // count 0, so every ring entry is a valid table offset.
-__device__ __forceinline__ uint2 decodeX(const Ctx &c, int pos, int &bad) {
+template <class CT>
+__device__ __forceinline__ uint2 decodeX(const CT &c, int pos, int &bad) {
     int b = 4, rc = 0;
     if (pos >= 0 && pos < c.lx) {
         uint32_t s = c.xs[pos];
@@ -187,7 +231,8 @@ __device__ __forceinline__ uint2 decodeX(const Ctx &c, int pos, int &bad) {
     return make_uint2(pk, __float_as_uint(ldsF(kGapXOff + c.model * 20u + (uint32_t) b * 4u)));
 }
 
-__device__ __forceinline__ uint2 decodeY(const Ctx &c, int pos, int &bad) {
+template <class CT>
+__device__ __forceinline__ uint2 decodeY(const CT &c, int pos, int &bad) {
     int b = 4, rc = 0;
     if (pos >= 0 && pos < c.ly) {
         uint32_t s = c.ys[pos];
@@ -220,8 +265,8 @@ struct Ring {
 
 // Decodes positions [newLo, newLo+R) into the group's ring where `doFill`; returns 1 if a
 // symbol of this group's fill was out of range. Called by every lane of the warp.
-template <int R, int L, bool IS_X>
-__device__ __noinline__ int ringFillRaw(Ctx c, uint32_t base, int newLo, int doFill) {
+template <int R, int L, bool IS_X, class CT>
+__device__ __noinline__ int ringFillRaw(CT c, uint32_t base, int newLo, int doFill) {
     int bad = 0;
     if (doFill) {
 #pragma unroll 4
@@ -236,13 +281,13 @@ __device__ __noinline__ int ringFillRaw(Ctx c, uint32_t base, int newLo, int doF
 }
 
 // Makes positions [needLo, needHi] resident for the groups where `active`.
-template <int R, int L, bool IS_X>
-__device__ __forceinline__ void ringEnsure(const Ctx &c, Ring<R> &r, int needLo, int needHi, bool up, bool active) {
+template <int R, int L, bool IS_X, class CT>
+__device__ __forceinline__ void ringEnsure(const CT &c, Ring<R> &r, int needLo, int needHi, bool up, bool active) {
     const bool need = active && (needLo < r.lo || needHi >= r.lo + R);
     if (__any_sync(FULL_MASK, need)) {
         const int slack = R - (needHi - needLo + 1);
         const int newLo = up ? needLo - slack / 8 : needLo - (slack - slack / 8);
-        r.bad |= ringFillRaw<R, L, IS_X>(c, r.base, newLo, need ? 1 : 0);
+        r.bad |= ringFillRaw<R, L, IS_X, CT>(c, r.base, newLo, need ? 1 : 0);
         if (need) r.lo = newLo;
     }
 }
@@ -252,12 +297,12 @@ __device__ __forceinline__ void ringEnsure(const Ctx &c, Ring<R> &r, int needLo,
 // range [x0-1, x0+S-2] with x0 = Q + (d+1)/2 and the y range [y0-S, y0-1] with
 // y0 = d/2 - Q only grow, so the rings stay valid until x0+S-2 or y0-1 passes the ring's
 // top; a window shift forces a new check. Called by every lane of the warp.
-template <int R, int L, int S>
-__device__ __forceinline__ int ensureRings(const Ctx &c, Ring<R> &rx, Ring<R> &ry, int d, int Q, bool up,
+template <int R, int L, int S, class CT>
+__device__ __forceinline__ int ensureRings(const CT &c, Ring<R> &rx, Ring<R> &ry, int d, int Q, bool up,
                                            bool active) {
     const int x0 = Q + ((d + 1) >> 1), y0 = d - x0;
-    ringEnsure<R, L, true>(c, rx, x0 - 1, x0 + S - 2, up, active);
-    ringEnsure<R, L, false>(c, ry, y0 - S, y0 - 1, up, active);
+    ringEnsure<R, L, true, CT>(c, rx, x0 - 1, x0 + S - 2, up, active);
+    ringEnsure<R, L, false, CT>(c, ry, y0 - S, y0 - 1, up, active);
     // x valid while (d'+1)/2 <= rx.lo + R + 1 - S - Q, y valid while d'/2 <= ry.lo + R + Q
     const int a = min(rx.lo + R + 1 - S - Q, 1 << 28), b = min(ry.lo + R + Q, 1 << 28);
     return min(2 * a, 2 * b + 1) + 1;
@@ -331,29 +376,29 @@ __device__ __forceinline__ void stepSlots(int gl, const Ring<R> &rx, const Ring<
 
 // Forward state between diagonals: outgoing gap-x / gap-y sums of d-1 and
 // outgoing match sums of d-1 and d-2 (even diagonals own mA, odd own mB).
-template <int C>
+template <int C, class V>
 struct Fwd {
-    float ox[C], oy[C], mA[C], mB[C];
+    V ox[C], oy[C], mA[C], mB[C];
 };
 
 // New lane gl takes old lane gl+dl of the group (values leaving the group become zero).
-template <int C, int L>
-__device__ __forceinline__ void laneShift(float (&v)[C], int dl, int gl) {
+template <int C, int L, class V>
+__device__ __forceinline__ void laneShift(V (&v)[C], int dl, int gl) {
     const int src = gl + dl;
     const bool ok = src >= 0 && src < L;
 #pragma unroll
     for (int j = 0; j < C; j++) {
-        const float w = __shfl_sync(FULL_MASK, v[j], src & (L - 1), L);
-        v[j] = ok ? w : 0.0f;
+        const V w = __shfl_sync(FULL_MASK, v[j], src & (L - 1), L);
+        v[j] = ok ? w : V(0);
     }
 }
 
-template <int C, int L>
-__device__ __forceinline__ void shiftFwd(Fwd<C> &f, int dl, int gl) {
-    laneShift<C, L>(f.ox, dl, gl);
-    laneShift<C, L>(f.oy, dl, gl);
-    laneShift<C, L>(f.mA, dl, gl);
-    laneShift<C, L>(f.mB, dl, gl);
+template <int C, int L, class V>
+__device__ __forceinline__ void shiftFwd(Fwd<C, V> &f, int dl, int gl) {
+    laneShift<C, L, V>(f.ox, dl, gl);
+    laneShift<C, L, V>(f.oy, dl, gl);
+    laneShift<C, L, V>(f.mA, dl, gl);
+    laneShift<C, L, V>(f.mB, dl, gl);
 }
 
 // The window must contain the hull (in slots) of the bands of d-2..d+2; returns the
@@ -383,19 +428,21 @@ __device__ __forceinline__ int initialWindow(int needLo, int needHi) {
 // [sLo, sHi], which zeroes the cell. With CACHE, the cell values and the masked
 // emissions are written to the block cache: rowA / rowB are the byte offsets of this
 // lane's slot 0 in the diagonal's rows, slot j follows at j*L entries.
-template <int C, int L, int PAR, bool CACHE, bool SYM = false>
-__device__ __forceinline__ void forwardDiagonal(const Ctx &c, Fwd<C> &st, const Slots<C> &sy, int sLo, int sHi,
+template <int C, int L, int PAR, bool CACHE, bool SYM, class V>
+__device__ __forceinline__ void forwardDiagonal(const Ctx<V> &c, Fwd<C, V> &st, const Slots<C> &sy, int sLo, int sHi,
                                                 uint32_t rowA, uint32_t rowB, uint32_t rowC = 0) {
-    float inX[C], inY[C];
+    using N = Num<V>;
+    constexpr uint32_t kA = sizeof(typename N::V4), kB = sizeof(typename N::V2);
+    V inX[C], inY[C];
     if (PAR) {  // odd d: gap-x source slot i, gap-y source slot i+1
-        const float nb = fromNext<L>(st.oy[0], c.gl);
+        const V nb = fromNext<L>(st.oy[0], c.gl);
 #pragma unroll
         for (int j = 0; j < C; j++) {
             inX[j] = st.ox[j];
             inY[j] = (j < C - 1) ? st.oy[j + 1] : nb;
         }
     } else {  // even d: gap-x source slot i-1, gap-y source slot i
-        const float nb = fromPrev<L>(st.ox[C - 1], c.gl);
+        const V nb = fromPrev<L>(st.ox[C - 1], c.gl);
 #pragma unroll
         for (int j = 0; j < C; j++) {
             inX[j] = (j > 0) ? st.ox[j - 1] : nb;
@@ -407,21 +454,21 @@ __device__ __forceinline__ void forwardDiagonal(const Ctx &c, Fwd<C> &st, const 
 #pragma unroll
     for (int j = 0; j < C; j++) {
         const bool in = (unsigned) (base + j) <= span;
-        const float eM = in ? matchEmission(sy.xpk[j], sy.ypk[j]) : 0.0f;
-        const float eX = in ? sy.ex[j] : 0.0f;
-        const float eY = in ? sy.ey[j] : 0.0f;
-        const float fM = eM * (PAR ? st.mB[j] : st.mA[j]);
-        const float fX = eX * inX[j];
-        const float fY = eY * inY[j];
-        const float nm = __fmaf_rn(c.t[2 * 3 + 0], fY, __fmaf_rn(c.t[1 * 3 + 0], fX, c.t[0 * 3 + 0] * fM));
-        const float nx = __fmaf_rn(c.t[2 * 3 + 1], fY, __fmaf_rn(c.t[1 * 3 + 1], fX, c.t[0 * 3 + 1] * fM));
-        const float ny = __fmaf_rn(c.t[1 * 3 + 2], fX, __fmaf_rn(c.t[2 * 3 + 2], fY, c.t[0 * 3 + 2] * fM));
+        const V eM = in ? (V) matchEmission(sy.xpk[j], sy.ypk[j]) : V(0);
+        const V eX = in ? (V) sy.ex[j] : V(0);
+        const V eY = in ? (V) sy.ey[j] : V(0);
+        const V fM = eM * (PAR ? st.mB[j] : st.mA[j]);
+        const V fX = eX * inX[j];
+        const V fY = eY * inY[j];
+        const V nm = N::fma(c.t[2 * 3 + 0], fY, N::fma(c.t[1 * 3 + 0], fX, c.t[0 * 3 + 0] * fM));
+        const V nx = N::fma(c.t[2 * 3 + 1], fY, N::fma(c.t[1 * 3 + 1], fX, c.t[0 * 3 + 1] * fM));
+        const V ny = N::fma(c.t[1 * 3 + 2], fX, N::fma(c.t[2 * 3 + 2], fY, c.t[0 * 3 + 2] * fM));
         if (PAR) st.mB[j] = nm; else st.mA[j] = nm;
         st.ox[j] = nx;
         st.oy[j] = ny;
         if (CACHE) {
-            sts<float4>(rowA + j * L * 16, make_float4(fM, fX, fY, eM));
-            sts<float2>(rowB + j * L * 8, make_float2(eX, eY));
+            sts<typename N::V4>(rowA + j * L * kA, N::v4(fM, fX, fY, eM));
+            sts<typename N::V2>(rowB + j * L * kB, N::v2(eX, eY));
         }
         // the cell's table offsets (repeat | match << 17), for the adjoint's histograms
         if (SYM) sts<uint32_t>(rowC + j * L * 4, in ? sy.xpk[j] + sy.ypk[j] : 0xffffffffu);
@@ -429,36 +476,39 @@ __device__ __forceinline__ void forwardDiagonal(const Ctx &c, Fwd<C> &st, const 
 }
 
 // Diagonal 0: the start cell (x-y = 0) holds the start (or ragged-start) probabilities.
-template <int C, int L, bool CACHE>
-__device__ __forceinline__ void forwardOrigin(const Ctx &c, const float *startP, int Q, Fwd<C> &st, uint32_t rowA,
-                                              uint32_t rowB) {
+template <int C, int L, bool CACHE, class V>
+__device__ __forceinline__ void forwardOrigin(const Ctx<V> &c, const float *startP, int Q, Fwd<C, V> &st,
+                                              uint32_t rowA, uint32_t rowB) {
+    using N = Num<V>;
+    constexpr uint32_t kA = sizeof(typename N::V4), kB = sizeof(typename N::V2);
 #pragma unroll
     for (int j = 0; j < C; j++) {
         const bool here = c.gl * C + j == -Q;
-        const float fM = here ? startP[0] : 0.0f;
-        const float fX = here ? startP[1] : 0.0f;
-        const float fY = here ? startP[2] : 0.0f;
-        st.mA[j] = __fmaf_rn(c.t[2 * 3 + 0], fY, __fmaf_rn(c.t[1 * 3 + 0], fX, c.t[0 * 3 + 0] * fM));
-        st.ox[j] = __fmaf_rn(c.t[2 * 3 + 1], fY, __fmaf_rn(c.t[1 * 3 + 1], fX, c.t[0 * 3 + 1] * fM));
-        st.oy[j] = __fmaf_rn(c.t[1 * 3 + 2], fX, __fmaf_rn(c.t[2 * 3 + 2], fY, c.t[0 * 3 + 2] * fM));
-        st.mB[j] = 0.0f;
+        const V fM = here ? (V) startP[0] : V(0);
+        const V fX = here ? (V) startP[1] : V(0);
+        const V fY = here ? (V) startP[2] : V(0);
+        st.mA[j] = N::fma(c.t[2 * 3 + 0], fY, N::fma(c.t[1 * 3 + 0], fX, c.t[0 * 3 + 0] * fM));
+        st.ox[j] = N::fma(c.t[2 * 3 + 1], fY, N::fma(c.t[1 * 3 + 1], fX, c.t[0 * 3 + 1] * fM));
+        st.oy[j] = N::fma(c.t[1 * 3 + 2], fX, N::fma(c.t[2 * 3 + 2], fY, c.t[0 * 3 + 2] * fM));
+        st.mB[j] = V(0);
         if (CACHE) {
-            sts<float4>(rowA + j * L * 16, make_float4(fM, fX, fY, 0.0f));
-            sts<float2>(rowB + j * L * 8, make_float2(0.0f, 0.0f));
+            sts<typename N::V4>(rowA + j * L * kA, N::v4(fM, fX, fY, V(0)));
+            sts<typename N::V2>(rowB + j * L * kB, N::v2(V(0), V(0)));
         }
     }
 }
 
 // Rescales the carried forward state by a power of two; returns the exponent removed.
-template <int C, int L>
-__device__ __forceinline__ int rescaleFwd(Fwd<C> &st) {
-    float m = 0.0f;
+template <int C, int L, class V>
+__device__ __forceinline__ int rescaleFwd(Fwd<C, V> &st) {
+    using N = Num<V>;
+    V m = V(0);
 #pragma unroll
-    for (int j = 0; j < C; j++) m = fmaxf(m, fmaxf(fmaxf(st.ox[j], st.oy[j]), fmaxf(st.mA[j], st.mB[j])));
+    for (int j = 0; j < C; j++) m = N::mx(m, N::mx(N::mx(st.ox[j], st.oy[j]), N::mx(st.mA[j], st.mB[j])));
     m = groupMax<L>(m);
-    if (!(m > 0.0f)) return 0;
-    const int k = exponentOf(m);
-    const float sc = pow2f(-k);
+    if (!(m > V(0))) return 0;
+    const int k = N::expOf(m);
+    const V sc = N::pow2(-k);
 #pragma unroll
     for (int j = 0; j < C; j++) {
         st.ox[j] *= sc;
@@ -483,8 +533,8 @@ struct Out {
 // Called by every lane of the warp; groups with `active` false emit nothing. The
 // (list, slot) pairs are unrolled at compile time, so each tuple is written through a
 // fixed list pointer.
-template <int C, int L>
-__device__ __forceinline__ void emitDiagonal(int gl, Out &o, const float (&p)[3][C], float thr, int x0, int d,
+template <int C, int L, class V>
+__device__ __forceinline__ void emitDiagonal(int gl, Out &o, const V (&p)[3][C], V thr, int x0, int d,
                                              bool active) {
     // Ranks come from one ballot per (list, slot): a tuple's rank within its group's
     // diagonal is the number of passing slots of lower index (lower lanes, then lower
@@ -515,8 +565,7 @@ __device__ __forceinline__ void emitDiagonal(int gl, Out &o, const float (&p)[3]
             if ((b[j] >> lane) & 1u) {
                 if (pos >= 0) {
                     const int x = xl + j;
-                    o.t[k][pos] = make_int4((int32_t) floorf(fminf(p[k][j], 1.0f) * (float) kProbOne),
-                                            x - 1 + o.xShift, d - x - 1 + o.yShift, 0);
+                    o.t[k][pos] = make_int4(Num<V>::weight(p[k][j]), x - 1 + o.xShift, d - x - 1 + o.yShift, 0);
                 }
                 pos--;
             }
@@ -529,15 +578,15 @@ __device__ __forceinline__ void emitDiagonal(int gl, Out &o, const float (&p)[3]
 // Shared workspace of one group
 // ---------------------------------------------------------------------------
 
-template <int C, int L, int K, bool ADJ = false>
+template <int C, int L, int K, bool ADJ = false, class V = float>
 struct GroupSmem {
     static constexpr int S = L * C;
     static constexpr int R = RingSize<S>::R;
     static constexpr size_t ringBytes = 2 * R * sizeof(uint2);
     static constexpr size_t bandRingBytes = 64 * sizeof(int4);
     static constexpr size_t walkBandBytes = K * sizeof(int4);
-    static constexpr size_t cacheABytes = (size_t) K * S * sizeof(float4);
-    static constexpr size_t cacheBBytes = (size_t) K * S * sizeof(float2);
+    static constexpr size_t cacheABytes = (size_t) K * S * sizeof(typename Num<V>::V4);
+    static constexpr size_t cacheBBytes = (size_t) K * S * sizeof(typename Num<V>::V2);
     static constexpr size_t cacheCBytes = ADJ ? (size_t) K * S * sizeof(uint32_t) : 0;
     static constexpr size_t infoBytes = K * sizeof(int2);
     static constexpr size_t bytes =
@@ -549,8 +598,8 @@ struct GroupMem {
     Ring<RingSize<L * C>::R> rx, ry;
     uint32_t bandRing;  // byte offsets in shared memory: 64 band records (int4)
     uint32_t walkBand;  // K band records of the block being walked
-    uint32_t cacheA;    // [K][S] float4: fM, fX, fY, eM
-    uint32_t cacheB;    // [K][S] float2: eX, eY
+    uint32_t cacheA;    // [K][S] (fM, fX, fY, eM) in the arithmetic type
+    uint32_t cacheB;    // [K][S] (eX, eY)
     uint32_t cacheC;    // adjoint only: [K][S] uint32 table offsets of the cell
     uint32_t info;      // [K] int2: window, shift
     uint32_t hist;      // adjoint only: the block's histograms (small tables, then repeat tables)
@@ -574,20 +623,21 @@ __device__ __forceinline__ int expectSlot(int i) {
     return ((i - kHistEnd) / 3) * kExpPerModel + kExpEnd + (i - kHistEnd) % 3;
 }
 
+template <class V>
 struct Scratch {
-    float4 *chk;      // checkpoints of the group's task: [block][C][L]
+    typename Num<V>::V4 *chk;  // checkpoints of the group's task: [block][C][L]
     int2 *scal;       // (exponent, window) per checkpoint
     int blocks;
 };
 
-template <int C, int L>
-__device__ __forceinline__ void storeFwd(float4 *p, int gl, const Fwd<C> &st) {
+template <int C, int L, class V>
+__device__ __forceinline__ void storeFwd(typename Num<V>::V4 *p, int gl, const Fwd<C, V> &st) {
 #pragma unroll
-    for (int j = 0; j < C; j++) p[j * L + gl] = make_float4(st.ox[j], st.oy[j], st.mA[j], st.mB[j]);
+    for (int j = 0; j < C; j++) p[j * L + gl] = Num<V>::v4(st.ox[j], st.oy[j], st.mA[j], st.mB[j]);
 }
 
-template <int C>
-__device__ __forceinline__ void loadFwd(const float4 (&v)[C], Fwd<C> &st) {
+template <int C, class V>
+__device__ __forceinline__ void loadFwd(const typename Num<V>::V4 (&v)[C], Fwd<C, V> &st) {
 #pragma unroll
     for (int j = 0; j < C; j++) {
         st.ox[j] = v[j].x;
@@ -611,32 +661,37 @@ struct Walk {
     const float *endP;
 };
 
-template <int C, int L, int K, bool ADJ>
-__device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm, const Scratch &sc, const Walk &wk,
-                                            float thr, Out &o, double &logLik, bool &bad, double (&accD)[9],
-                                            double *expect) {
+template <int C, int L, int K, bool ADJ, class V>
+__device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &gm, const Scratch<V> &sc,
+                                            const Walk &wk, V thr, Out &o, double &logLik, bool &bad,
+                                            bool &rangeBad, double (&accD)[9], double *expect) {
     static_assert(!ADJ || L == 32, "the adjoint runs one task per warp");
+    static_assert(!ADJ || std::is_same<V, float>::value, "the adjoint accumulates in FP32");
+    using N = Num<V>;
+    using V4 = typename N::V4;
+    using V2 = typename N::V2;
+    constexpr uint32_t kA = sizeof(V4), kB = sizeof(V2);
     static_assert(K <= L && (K % 2) == 0, "band records of a block are held one per lane");
     constexpr int S = L * C;
     constexpr int R = RingSize<S>::R;
     const int gl = c.gl;
-    float gX[C], gY[C], gA[C], gB[C];  // backward u-values: gap-x / gap-y of d+1, match (even d in A, odd in B)
+    V gX[C], gY[C], gA[C], gB[C];  // backward u-values: gap-x / gap-y of d+1, match (even d in A, odd in B)
 #pragma unroll
-    for (int j = 0; j < C; j++) gX[j] = gY[j] = gA[j] = gB[j] = 0.0f;
+    for (int j = 0; j < C; j++) gX[j] = gY[j] = gA[j] = gB[j] = V(0);
     int Eb = 0, posts = 0, ET = 0, untilRefresh = 0;
-    float Tm = 0.0f;
-    float llTm = 0.0f;  // total of the first posterior diagonal of the final segment: the likelihood
+    V Tm = V(0);
+    V llTm = V(0);  // total of the first posterior diagonal of the final segment: the likelihood
     int llET = 0;
     bool llSet = false;
-    const float endM = wk.endP[0], endX = wk.endP[1], endY = wk.endP[2];
+    const V endM = (V) wk.endP[0], endX = (V) wk.endP[1], endY = (V) wk.endP[2];
     const int bTop = wk.active ? wk.D / K : -1;
     const int bBot = wk.active ? (wk.tbTo + 1) / K : 0;
     const int nIter = warpMaxInt(wk.active ? bTop - bBot + 1 : 0);
 
     // register prefetch of a block's checkpoint and band records
-    float4 pchk[C];
+    V4 pchk[C];
 #pragma unroll
-    for (int j = 0; j < C; j++) pchk[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (int j = 0; j < C; j++) pchk[j] = N::v4(V(0), V(0), V(0), V(0));
     int2 pscal = make_int2(0, 0);
     int4 pband = make_int4(0, 0, 0, 0);
     auto prefetch = [&](int b, bool ok) {
@@ -649,7 +704,7 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
         if (ok && gl < K && dd <= c.N) pband = c.band[dd];
     };
     prefetch(bTop, bTop >= bBot);
-    const uint32_t laneA = gm.cacheA + (uint32_t) gl * 16, laneB = gm.cacheB + (uint32_t) gl * 8;
+    const uint32_t laneA = gm.cacheA + (uint32_t) gl * kA, laneB = gm.cacheB + (uint32_t) gl * kB;
     const uint32_t laneC = gm.cacheC + (uint32_t) gl * 4;
 
     for (int w = 0; w < nIter; w++) {
@@ -657,8 +712,8 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
         const bool blockOn = b >= bBot;
         const int dStart = b * K;
         const int dEnd = min(dStart + K - 1, wk.D);
-        Fwd<C> rs;
-        float4 cchk[C];
+        Fwd<C, V> rs;
+        V4 cchk[C];
 #pragma unroll
         for (int j = 0; j < C; j++) cchk[j] = pchk[j];
         const int2 cscal = pscal;
@@ -672,8 +727,8 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
         // ---------------- recompute the block ----------------
         int Q;
         int Ef;
-        float chkSM[C];
-        loadFwd<C>(cchk, rs);
+        V chkSM[C];
+        loadFwd<C, V>(cchk, rs);
         Ef = cscal.x;
         Q = cscal.y;
 #pragma unroll
@@ -683,7 +738,7 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
             Q = initialWindow<S>(b0.z, b0.w);
             Ef = 0;
 #pragma unroll
-            for (int j = 0; j < C; j++) chkSM[j] = 0.0f;
+            for (int j = 0; j < C; j++) chkSM[j] = V(0);
         }
         Slots<C> sy;
         // A whole block past diagonal 0 whose window does not move and whose symbols stay in
@@ -704,13 +759,13 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
                 const int d = dStart + kk;
                 const int2 b0 = lds<int2>(gm.walkBand + kk * 16);
                 const int2 b1 = lds<int2>(gm.walkBand + (kk + 1) * 16);
-                const uint32_t rowA = laneA + (uint32_t) (kk * S * 16), rowB = laneB + (uint32_t) (kk * S * 8);
+                const uint32_t rowA = laneA + (uint32_t) (kk * S * kA), rowB = laneB + (uint32_t) (kk * S * kB);
                 const uint32_t rowC = laneC + (uint32_t) (kk * S * 4);
                 stepSlots<C, L, R, 0>(gl, gm.rx, gm.ry, d, Q, sy);
-                forwardDiagonal<C, L, 0, true, ADJ>(c, rs, sy, b0.x - Q, b0.y - Q, rowA, rowB, rowC);
+                forwardDiagonal<C, L, 0, true, ADJ, V>(c, rs, sy, b0.x - Q, b0.y - Q, rowA, rowB, rowC);
                 stepSlots<C, L, R, 1>(gl, gm.rx, gm.ry, d + 1, Q, sy);
-                forwardDiagonal<C, L, 1, true, ADJ>(c, rs, sy, b1.x - Q, b1.y - Q, rowA + S * 16, rowB + S * 8,
-                                                    rowC + S * 4);
+                forwardDiagonal<C, L, 1, true, ADJ, V>(c, rs, sy, b1.x - Q, b1.y - Q, rowA + S * kA, rowB + S * kB,
+                                                       rowC + S * 4);
             }
             if (gl < K) sts<int2>(gm.info + gl * 8, make_int2(Q, 0));
         } else {
@@ -730,7 +785,7 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
                     if (rare) {
                         dl = move ? windowShift<C, S>(Q, bd.z, bd.w, bad) : 0;
                         if (__any_sync(FULL_MASK, dl != 0)) {
-                            shiftFwd<C, L>(rs, dl, gl);
+                            shiftFwd<C, L, V>(rs, dl, gl);
                             if (dl != 0) {
                                 Q += C * dl;
                                 reload = true;
@@ -739,17 +794,17 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
                         checkAt = ensureRings<R, L, S>(c, gm.rx, gm.ry, d, Q, false, on);
                     }
                     const int sLo = bd.x - Q, sHi = bd.y - Q;
-                    const uint32_t rowA = laneA + (uint32_t) (kk * S * 16), rowB = laneB + (uint32_t) (kk * S * 8);
+                    const uint32_t rowA = laneA + (uint32_t) (kk * S * kA), rowB = laneB + (uint32_t) (kk * S * kB);
                     const uint32_t rowC = laneC + (uint32_t) (kk * S * 4);
                     if (par) {
                         stepSlots<C, L, R, 1>(gl, gm.rx, gm.ry, d, Q, sy);
                         if (rare && reload) loadSlots<C, R>(gl, gm.rx, gm.ry, d, Q, sy);
-                        forwardDiagonal<C, L, 1, true, ADJ>(c, rs, sy, sLo, sHi, rowA, rowB, rowC);
+                        forwardDiagonal<C, L, 1, true, ADJ, V>(c, rs, sy, sLo, sHi, rowA, rowB, rowC);
                     } else {
                         stepSlots<C, L, R, 0>(gl, gm.rx, gm.ry, d, Q, sy);
                         if (rare && reload) loadSlots<C, R>(gl, gm.rx, gm.ry, d, Q, sy);
-                        forwardDiagonal<C, L, 0, true, ADJ>(c, rs, sy, sLo, sHi, rowA, rowB, rowC);
-                        if (d == 0) forwardOrigin<C, L, true>(c, wk.startP, Q, rs, rowA, rowB);
+                        forwardDiagonal<C, L, 0, true, ADJ, V>(c, rs, sy, sLo, sHi, rowA, rowB, rowC);
+                        if (d == 0) forwardOrigin<C, L, true, V>(c, wk.startP, Q, rs, rowA, rowB);
                     }
                     if (gl == 0) sts<int2>(gm.info + kk * 8, make_int2(Q, dl));
                 }
@@ -767,25 +822,25 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
             const int d = dStart + kk;
             const bool on = FLAT || (blockOn && d <= dEnd && d > wk.tbTo);
             const int2 inf = FLAT ? make_int2(Q, 0) : lds<int2>(gm.info + kk * 8);
-            float4 f[C];
-            float2 e[C];
+            V4 f[C];
+            V2 e[C];
 #pragma unroll
             for (int j = 0; j < C; j++) {
-                f[j] = lds<float4>(laneA + (uint32_t) ((kk * S + j * L) * 16));
-                e[j] = lds<float2>(laneB + (uint32_t) ((kk * S + j * L) * 8));
+                f[j] = lds<V4>(laneA + (uint32_t) ((kk * S + j * L) * kA));
+                e[j] = lds<V2>(laneB + (uint32_t) ((kk * S + j * L) * kB));
             }
-            float bM[C], bX[C], bY[C];
-            float sX[C], sY[C], sM2[C];  // u-values of the gap-x, gap-y and match successors
+            V bM[C], bX[C], bY[C];
+            V sX[C], sY[C], sM2[C];  // u-values of the gap-x, gap-y and match successors
             {
                 if (PAR) {  // odd d: gap-x successor slot i+1, gap-y successor slot i
-                    const float nb = fromNext<L>(gX[0], gl);
+                    const V nb = fromNext<L>(gX[0], gl);
 #pragma unroll
                     for (int j = 0; j < C; j++) {
                         sX[j] = (j < C - 1) ? gX[j + 1] : nb;
                         sY[j] = gY[j];
                     }
                 } else {  // even d: gap-x successor slot i, gap-y successor slot i-1
-                    const float nb = fromPrev<L>(gY[C - 1], gl);
+                    const V nb = fromPrev<L>(gY[C - 1], gl);
 #pragma unroll
                     for (int j = 0; j < C; j++) {
                         sX[j] = gX[j];
@@ -796,11 +851,11 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
                 const bool top = !FLAT && d == wk.D;
 #pragma unroll
                 for (int j = 0; j < C; j++) {
-                    const float s2 = PAR ? gB[j] : gA[j];
+                    const V s2 = PAR ? gB[j] : gA[j];
                     sM2[j] = s2;
-                    const float m_ = __fmaf_rn(c.t[0 * 3 + 0], s2, __fmaf_rn(c.t[0 * 3 + 2], sY[j], c.t[0 * 3 + 1] * sX[j]));
-                    const float x_ = __fmaf_rn(c.t[1 * 3 + 0], s2, __fmaf_rn(c.t[1 * 3 + 2], sY[j], c.t[1 * 3 + 1] * sX[j]));
-                    const float y_ = __fmaf_rn(c.t[2 * 3 + 0], s2, __fmaf_rn(c.t[2 * 3 + 2], sY[j], c.t[2 * 3 + 1] * sX[j]));
+                    const V m_ = N::fma(c.t[0 * 3 + 0], s2, N::fma(c.t[0 * 3 + 2], sY[j], c.t[0 * 3 + 1] * sX[j]));
+                    const V x_ = N::fma(c.t[1 * 3 + 0], s2, N::fma(c.t[1 * 3 + 2], sY[j], c.t[1 * 3 + 1] * sX[j]));
+                    const V y_ = N::fma(c.t[2 * 3 + 0], s2, N::fma(c.t[2 * 3 + 2], sY[j], c.t[2 * 3 + 1] * sX[j]));
                     bM[j] = top ? endM : m_;
                     bX[j] = top ? endX : x_;
                     bY[j] = top ? endY : y_;
@@ -811,31 +866,44 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
             const bool refresh = post && untilRefresh == 0;
             if (__any_sync(FULL_MASK, refresh)) {
                 // cells of d plus the match transitions crossing d (impl/pairwiseAligner.c:567-584)
-                float sM1[C];
+                V sM1[C];
                 if (kk > 0) {
 #pragma unroll
                     for (int j = 0; j < C; j++) {
-                        const float4 q = lds<float4>(laneA + (uint32_t) (((kk - 1) * S + j * L) * 16));
-                        sM1[j] = __fmaf_rn(c.t[2 * 3 + 0], q.z, __fmaf_rn(c.t[1 * 3 + 0], q.y, c.t[0 * 3 + 0] * q.x));
+                        const V4 q = lds<V4>(laneA + (uint32_t) (((kk - 1) * S + j * L) * kA));
+                        sM1[j] = N::fma(c.t[2 * 3 + 0], q.z, N::fma(c.t[1 * 3 + 0], q.y, c.t[0 * 3 + 0] * q.x));
                     }
                 } else {
 #pragma unroll
                     for (int j = 0; j < C; j++) sM1[j] = chkSM[j];
                 }
-                if (!FLAT) laneShift<C, L>(sM1, on ? inf.y : 0, gl);
-                float part = 0.0f;
+                if (!FLAT) laneShift<C, L, V>(sM1, on ? inf.y : 0, gl);
+                V part = V(0);
 #pragma unroll
                 for (int j = 0; j < C; j++) {
-                    const float uMn = PAR ? gA[j] : gB[j];  // match u of d+1
-                    part = __fmaf_rn(f[j].x, bM[j], part);
-                    part = __fmaf_rn(f[j].y, bX[j], part);
-                    part = __fmaf_rn(f[j].z, bY[j], part);
-                    part = __fmaf_rn(uMn, sM1[j], part);
+                    const V uMn = PAR ? gA[j] : gB[j];  // match u of d+1
+                    part = N::fma(f[j].x, bM[j], part);
+                    part = N::fma(f[j].y, bX[j], part);
+                    part = N::fma(f[j].z, bY[j], part);
+                    part = N::fma(uMn, sM1[j], part);
                 }
-                const float T = groupSum<L>(part);
-                const int ex = exponentOf(T);
-                const float tm = T > 0.0f ? T * pow2f(-ex) : 0.0f;
-                const int et = T > 0.0f ? Ef + Eb + ex : 0;
+                const V T = groupSum<L>(part);
+                const int ex = N::expOf(T);
+                const V tm = T > V(0) ? T * N::pow2(-ex) : V(0);
+                const int et = T > V(0) ? Ef + Eb + ex : 0;
+                // The total through every diagonal of a walk is one quantity; a refresh that finds
+                // no total, or one that disagrees with the walk's previous total, means the scaled
+                // values lost their range (the host runs such sub-problems again in FP64).
+                if (refresh) {
+                    bool ok = tm > V(0);
+                    if (ok && posts > 0 && Tm > V(0) && abs(et - ET) <= 1) {
+                        const V r = N::div(tm * N::pow2(et - ET), Tm) - V(1);
+                        ok = r <= V(1e-3) && r >= V(-1e-3);
+                    } else if (posts > 0) {
+                        ok = false;
+                    }
+                    rangeBad = rangeBad || !ok;
+                }
                 const bool first = refresh && wk.atEnd && posts == 0;
                 llTm = first ? tm : llTm;
                 llET = first ? et : llET;
@@ -845,26 +913,26 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
             }
             untilRefresh = refresh ? 9 : untilRefresh - (post ? 1 : 0);
             posts += post ? 1 : 0;
-            const bool emit = post && Tm > 0.0f && wk.emit;
+            const bool emit = post && Tm > V(0) && wk.emit;
             if (FLAT || __any_sync(FULL_MASK, emit)) {
-                const int ex = max(-126, min(127, Ef + Eb - ET));
-                const float scale = emit ? __fdividef(pow2f(ex), Tm) : 0.0f;
-                float p[3][C];
+                const int ex = max(N::kMinExp, min(N::kMaxExp, Ef + Eb - ET));
+                const V scale = emit ? N::div(N::pow2(ex), Tm) : V(0);
+                V p[3][C];
 #pragma unroll
                 for (int j = 0; j < C; j++) {
                     p[0][j] = (f[j].x * bM[j]) * scale;
                     p[1][j] = (f[j].y * bX[j]) * scale;
                     p[2][j] = (f[j].z * bY[j]) * scale;
                 }
-                emitDiagonal<C, L>(gl, o, p, thr, slotX0(d, inf.x), d, emit);
+                emitDiagonal<C, L, V>(gl, o, p, thr, slotX0(d, inf.x), d, emit);
             }
             if constexpr (ADJ) {
                 // expected counts: transitions out of the cells of d (f_from * u_to, scaled by 1/P)
                 // and the emission posteriors of each state, binned by the cell's table entries
-                const bool acc = post && Tm > 0.0f;
+                const bool acc = post && Tm > V(0);
                 if (FLAT || __any_sync(FULL_MASK, acc)) {
-                    const int ex = max(-126, min(127, Ef + Eb - ET));
-                    const float scale = acc ? __fdividef(pow2f(ex), Tm) : 0.0f;
+                    const int ex = max(N::kMinExp, min(N::kMaxExp, Ef + Eb - ET));
+                    const float scale = acc ? N::div(N::pow2(ex), Tm) : 0.0f;
                     const int xl = slotX0(d, inf.x) + gl * C;
                     float *hs = reinterpret_cast<float *>(mpSmem + gm.hist);
 #pragma unroll
@@ -905,7 +973,7 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
             // u-values of d (emissions are zero outside the band); kept when the diagonal is off
 #pragma unroll
             for (int j = 0; j < C; j++) {
-                const float ux = e[j].x * bX[j], uy = e[j].y * bY[j], um = f[j].w * bM[j];
+                const V ux = e[j].x * bX[j], uy = e[j].y * bY[j], um = f[j].w * bM[j];
                 gX[j] = on ? ux : gX[j];
                 gY[j] = on ? uy : gY[j];
                 if (PAR) gB[j] = on ? um : gB[j]; else gA[j] = on ? um : gA[j];
@@ -914,10 +982,10 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
                 // moving below d crosses the window shift met when entering d
                 const int backShift = on ? -inf.y : 0;
                 if (__any_sync(FULL_MASK, backShift != 0)) {
-                    laneShift<C, L>(gX, backShift, gl);
-                    laneShift<C, L>(gY, backShift, gl);
-                    laneShift<C, L>(gA, backShift, gl);
-                    laneShift<C, L>(gB, backShift, gl);
+                    laneShift<C, L, V>(gX, backShift, gl);
+                    laneShift<C, L, V>(gY, backShift, gl);
+                    laneShift<C, L, V>(gA, backShift, gl);
+                    laneShift<C, L, V>(gB, backShift, gl);
                 }
             }
         };
@@ -938,13 +1006,13 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
         }
         // rescale the carried backward state at the block boundary
         {
-            float m = 0.0f;
+            V m = V(0);
 #pragma unroll
-            for (int j = 0; j < C; j++) m = fmaxf(m, fmaxf(fmaxf(gX[j], gY[j]), fmaxf(gA[j], gB[j])));
+            for (int j = 0; j < C; j++) m = N::mx(m, N::mx(N::mx(gX[j], gY[j]), N::mx(gA[j], gB[j])));
             m = groupMax<L>(m);
-            if (blockOn && m > 0.0f) {
-                const int kx = exponentOf(m);
-                const float s = pow2f(-kx);
+            if (blockOn && m > V(0)) {
+                const int kx = N::expOf(m);
+                const V s = N::pow2(-kx);
 #pragma unroll
                 for (int j = 0; j < C; j++) {
                     gX[j] *= s;
@@ -967,14 +1035,14 @@ __device__ __forceinline__ void walkSegment(const Ctx &c, GroupMem<C, L, K> &gm,
         }
         __syncwarp();
     }
-    if (llSet) logLik += llTm > 0.0f ? log((double) llTm) + (double) llET * 0.69314718055994530942 : -INFINITY;
+    if (llSet) logLik += llTm > V(0) ? log((double) llTm) + (double) llET * 0.69314718055994530942 : -INFINITY;
 }
 
 // Next traceback point of a group's task: the first anti-diagonal d in [from, N) whose band
 // is at most 2*diagonalExpansion+1 cells wide (impl/pairwiseAligner.c:722-724), else N.
 // Called by every lane of the warp; groups with `searching` false return N.
-template <int L>
-__device__ __forceinline__ int nextTracePoint(const Ctx &c, int from, int maxWidth, bool searching) {
+template <int L, class CT>
+__device__ __forceinline__ int nextTracePoint(const CT &c, int from, int maxWidth, bool searching) {
     int D = c.N;
     int pos = from;
     bool look = searching && pos < c.N;
@@ -1003,8 +1071,8 @@ __device__ __forceinline__ int nextTracePoint(const Ctx &c, int from, int maxWid
 // One warp-load of G tasks: forward sweep with checkpoints, then the walks.
 // ---------------------------------------------------------------------------
 
-template <int C, int L, int K, bool ADJ>
-__device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMem<C, L, K> &gm, const Scratch &sc) {
+template <int C, int L, int K, bool ADJ, class V>
+__device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMem<C, L, K> &gm, const Scratch<V> &sc) {
     constexpr int S = L * C;
     constexpr int R = RingSize<S>::R;
     constexpr bool kSolo = L == 32;  // one task per warp: every lane is always on
@@ -1012,7 +1080,7 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
     const bool has = taskIndex >= 0;
     const Task *tk = a.tasks + (has ? taskIndex : 0);
     TaskOut *to = a.out + (has ? taskIndex : 0);
-    Ctx c;
+    Ctx<V> c;
     c.gl = lane & (L - 1);
     c.g = lane / L;
     c.lx = has ? tk->lx : 0;
@@ -1025,7 +1093,7 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
     const int model = (flags & 4) ? 0 : 1;
     const DevModel &dm = a.models[model];
 #pragma unroll
-    for (int k = 0; k < 9; k++) c.t[k] = dm.t[k];
+    for (int k = 0; k < 9; k++) c.t[k] = (V) dm.t[k];
     c.model = (uint32_t) model;
     c.repOff = kRepBase + (a.sharedRepeat ? 0u : (uint32_t) model * (uint32_t) (kRepTable * sizeof(float)));
     c.rle = dm.runLength;
@@ -1056,6 +1124,7 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
     wk.startP = (flags & 1) ? dm.raggedStart : dm.start;
     double logLik = 0.0;
     bool bad = false;
+    bool rangeBad = false;
     gm.rx.bad = 0;
     gm.ry.bad = 0;
     gm.rx.lo = 1 << 30;  // nothing resident
@@ -1075,7 +1144,7 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
     cpAsyncWaitAllButOne();
     __syncwarp();
 
-    Fwd<C> st;
+    Fwd<C, V> st;
     Slots<C> sy;
     int Q = 0;
     if (live) {
@@ -1088,7 +1157,7 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
         const int x0 = slotX0(0, Q);
         ringEnsure<R, L, true>(c, gm.rx, x0 - 1 - 8, x0 + S - 2, true, true);
         ringEnsure<R, L, false>(c, gm.ry, -x0 - S - 8, -x0 - 1, true, true);
-        forwardOrigin<C, L, false>(c, wk.startP, Q, st, 0, 0);
+        forwardOrigin<C, L, false, V>(c, wk.startP, Q, st, 0, 0);
         loadSlots<C, R>(c.gl, gm.rx, gm.ry, 0, Q, sy);
     }
     int checkAt = 1;
@@ -1105,7 +1174,7 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
         if (rare) {
             const int dl = move ? windowShift<C, S>(Q, bd.z, bd.w, bad) : 0;
             if (__any_sync(FULL_MASK, dl != 0)) {
-                shiftFwd<C, L>(st, dl, c.gl);
+                shiftFwd<C, L, V>(st, dl, c.gl);
                 if (dl != 0) {
                     Q += C * dl;
                     reload = true;
@@ -1115,7 +1184,7 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
         }
         stepSlots<C, L, R, PAR>(c.gl, gm.rx, gm.ry, d, Q, sy);
         if (rare && reload) loadSlots<C, R>(c.gl, gm.rx, gm.ry, d, Q, sy);
-        forwardDiagonal<C, L, PAR, false>(c, st, sy, bd.x - Q, bd.y - Q, 0, 0);
+        forwardDiagonal<C, L, PAR, false, false, V>(c, st, sy, bd.x - Q, bd.y - Q, 0, 0);
     };
     const auto odd = std::integral_constant<int, 1>{};
     const auto even = std::integral_constant<int, 0>{};
@@ -1132,9 +1201,9 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
             cpAsyncWaitAllButOne();
             __syncwarp();
         }
-        Ef += rescaleFwd<C, L>(st);
+        Ef += rescaleFwd<C, L, V>(st);
         if (kSolo || d0 <= myN) {
-            storeFwd<C, L>(sc.chk + (size_t) (d0 / K) * S, c.gl, st);
+            storeFwd<C, L, V>(sc.chk + (size_t) (d0 / K) * S, c.gl, st);
             if (c.gl == 0) sc.scal[d0 / K] = make_int2(Ef, Q);
         }
         const int dLast = d0 + K - 1;
@@ -1150,9 +1219,9 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
                 const int2 b0 = lds<int2>(gm.bandRing + ((d & 63) << 4));
                 const int2 b1 = lds<int2>(gm.bandRing + (((d + 1) & 63) << 4));
                 stepSlots<C, L, R, 0>(c.gl, gm.rx, gm.ry, d, Q, sy);
-                forwardDiagonal<C, L, 0, false>(c, st, sy, b0.x - Q, b0.y - Q, 0, 0);
+                forwardDiagonal<C, L, 0, false, false, V>(c, st, sy, b0.x - Q, b0.y - Q, 0, 0);
                 stepSlots<C, L, R, 1>(c.gl, gm.rx, gm.ry, d + 1, Q, sy);
-                forwardDiagonal<C, L, 1, false>(c, st, sy, b1.x - Q, b1.y - Q, 0, 0);
+                forwardDiagonal<C, L, 1, false, false, V>(c, st, sy, b1.x - Q, b1.y - Q, 0, 0);
             }
         } else {
             for (int kk = 0; kk < K; kk += 2) {
@@ -1192,7 +1261,7 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
         wk.active = more ? 1 : 0;
         wk.emit = single ? 0 : 1;
         wk.endP = (atEnd && (flags & 2)) ? dm.raggedEnd : dm.end;
-        walkSegment<C, L, K, ADJ>(c, gm, sc, wk, a.threshold, o, logLik, bad, accD, a.expect);
+        walkSegment<C, L, K, ADJ, V>(c, gm, sc, wk, (V) a.threshold, o, logLik, bad, rangeBad, accD, a.expect);
         if (more) {
             tb = wk.tbFrom;
             prevD = wk.D;
@@ -1218,6 +1287,7 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
     if (live && c.gl == 0) {
         int s = status0;
         if (bad) s |= kTaskWindow;
+        if (rangeBad) s |= kTaskRange;
         if (gm.rx.bad | gm.ry.bad) s |= kTaskSymbol;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
@@ -1229,9 +1299,9 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
     }
 }
 
-template <int C, int L, int K, int MAXW, bool ADJ>
+template <int C, int L, int K, int MAXW, bool ADJ, class V>
 __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
-    using GS = GroupSmem<C, L, K, ADJ>;
+    using GS = GroupSmem<C, L, K, ADJ, V>;
     constexpr int G = 32 / L;
     constexpr int R = RingSize<L * C>::R;
     const int nTables = a.sharedRepeat ? 1 : 2;
@@ -1267,10 +1337,10 @@ __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
     gm.cacheC = gm.cacheB + (uint32_t) GS::cacheBBytes;
     gm.info = gm.cacheC + (uint32_t) GS::cacheCBytes;
     gm.hist = histOff;
-    Scratch sc;
+    Scratch<V> sc;
     sc.blocks = a.scratchBlocks;
     const size_t slot = (size_t) gwarp * G + g;  // one checkpoint area per task slot
-    sc.chk = a.scratch + slot * a.scratchBlocks * (size_t) (C * L);
+    sc.chk = reinterpret_cast<typename Num<V>::V4 *>(a.scratch) + slot * a.scratchBlocks * (size_t) (C * L);
     sc.scal = a.scratchScalars + slot * a.scratchBlocks;
 
     const int nLoads = (a.nTasks + G - 1) / G;
@@ -1280,7 +1350,7 @@ __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
         q = __shfl_sync(FULL_MASK, q, 0);
         if (q >= nLoads) break;
         const int t = q * G + g;
-        runGroup<C, L, K, ADJ>(a, t < a.nTasks ? a.order[t] : -1, gm, sc);
+        runGroup<C, L, K, ADJ, V>(a, t < a.nTasks ? a.order[t] : -1, gm, sc);
         __syncwarp();
     }
 }
@@ -1290,34 +1360,41 @@ __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
 // ---------------------------------------------------------------------------
 
 
-template <int C, int L, int K, bool ADJ = false>
+template <int C, int L, int K, bool ADJ = false, class V = float>
 static size_t smemFor(int warps, int nTables) {
     return tableBytes(nTables) + (ADJ ? histBytes(nTables) : 0) +
-           (size_t) warps * (32 / L) * GroupSmem<C, L, K, ADJ>::bytes;
+           (size_t) warps * (32 / L) * GroupSmem<C, L, K, ADJ, V>::bytes;
 }
 
-template <int C, int L, int K, int MAXW, bool ADJ = false>
+template <int C, int L, int K, int MAXW, bool ADJ = false, class V = float>
 static cudaError_t launchT(const DpArgs &a, int blocks, int warps, cudaStream_t s) {
     if (warps > MAXW || warps < 1) return cudaErrorInvalidValue;
-    const size_t smem = smemFor<C, L, K, ADJ>(warps, a.sharedRepeat ? 1 : 2);
-    cudaError_t e = cudaFuncSetAttribute(posteriorKernel<C, L, K, MAXW, ADJ>,
+    const size_t smem = smemFor<C, L, K, ADJ, V>(warps, a.sharedRepeat ? 1 : 2);
+    cudaError_t e = cudaFuncSetAttribute(posteriorKernel<C, L, K, MAXW, ADJ, V>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     if (e != cudaSuccess) return e;
-    posteriorKernel<C, L, K, MAXW, ADJ><<<blocks, warps * 32, smem, s>>>(a);
+    posteriorKernel<C, L, K, MAXW, ADJ, V><<<blocks, warps * 32, smem, s>>>(a);
     return cudaGetLastError();
 }
 
-// Kernel variants: (C slots per lane, L lanes per task, K checkpoint stride,
-// maximum warps per block = launch bound). The window is S = L*C slots, a warp
-// carries 32/L tasks and a task fits when its band hull spans at most S - 2C slots.
-#define MP_VARIANTS(X) \
-    X(0, 2, 32, 8, 12) \
-    X(1, 4, 16, 4, 8)  \
-    X(2, 8, 8, 4, 5)   \
-    X(3, 3, 32, 8, 8)  \
-    X(4, 4, 32, 4, 8)  \
-    X(5, 6, 32, 4, 8)  \
-    X(6, 8, 32, 4, 5)
+// Kernel variants: (index, C slots per lane, L lanes per task, K checkpoint stride,
+// maximum warps per block = launch bound, arithmetic type). The window is S = L*C slots,
+// a warp carries 32/L tasks and a task fits when its band hull spans at most S - 2C slots.
+// Variants 0-6 compute in FP32, 7-11 in FP64 (same schedule; for the sub-problems whose
+// range FP32 cannot hold, and for the likelihood-only mode).
+#define MP_VARIANTS(X)            \
+    X(0, 2, 32, 8, 12, float)     \
+    X(1, 4, 16, 4, 8, float)      \
+    X(2, 8, 8, 4, 5, float)       \
+    X(3, 3, 32, 8, 8, float)      \
+    X(4, 4, 32, 4, 8, float)      \
+    X(5, 6, 32, 4, 8, float)      \
+    X(6, 8, 32, 4, 5, float)      \
+    X(7, 2, 32, 8, 6, double)     \
+    X(8, 3, 32, 8, 4, double)     \
+    X(9, 4, 32, 4, 6, double)     \
+    X(10, 6, 32, 4, 4, double)    \
+    X(11, 8, 32, 4, 3, double)
 
 // Adjoint variants (one task per warp; the block also holds the expected-count histograms).
 #define MP_ADJ_VARIANTS(X) \
@@ -1326,12 +1403,22 @@ static cudaError_t launchT(const DpArgs &a, int blocks, int warps, cudaStream_t 
     X(2, 4, 32, 4, 6)
 
 int variantCount() {
-    return 7;
+    return 12;
+}
+
+bool variantIsF64(int v) {
+    switch (v) {
+#define MP_F64(i, c_, l_, k_, w_, t_) \
+    case i: return sizeof(t_) == 8;
+        MP_VARIANTS(MP_F64)
+#undef MP_F64
+        default: return false;
+    }
 }
 
 bool variantShape(int v, int *C, int *L, int *K) {
     switch (v) {
-#define MP_SHAPE(i, c_, l_, k_, w_) \
+#define MP_SHAPE(i, c_, l_, k_, w_, t_) \
     case i: *C = c_; *L = l_; *K = k_; return true;
         MP_VARIANTS(MP_SHAPE)
 #undef MP_SHAPE
@@ -1339,15 +1426,15 @@ bool variantShape(int v, int *C, int *L, int *K) {
     }
 }
 
-// As many warps as the kernel's bound and 227 KB of shared memory per block allow.
+// As many warps as the kernel's bound and 227 KB of shared memory per block allow (0: none).
 int variantMaxWarps(int v, int nTables) {
     const size_t limit = 227 * 1024;
     switch (v) {
-#define MP_MAXW(i, c_, l_, k_, w_)                                            \
-    case i: {                                                                 \
-        int w = w_;                                                           \
-        while (w > 1 && smemFor<c_, l_, k_>(w, nTables) > limit) w--;         \
-        return w;                                                             \
+#define MP_MAXW(i, c_, l_, k_, w_, t_)                                             \
+    case i: {                                                                      \
+        int w = w_;                                                                \
+        while (w > 1 && smemFor<c_, l_, k_, false, t_>(w, nTables) > limit) w--;   \
+        return smemFor<c_, l_, k_, false, t_>(w, nTables) > limit ? 0 : w;         \
     }
         MP_VARIANTS(MP_MAXW)
 #undef MP_MAXW
@@ -1357,8 +1444,8 @@ int variantMaxWarps(int v, int nTables) {
 
 cudaError_t launchVariant(int v, const DpArgs &a, int blocks, int warps, cudaStream_t s) {
     switch (v) {
-#define MP_LAUNCH(i, c_, l_, k_, w_) \
-    case i: return launchT<c_, l_, k_, w_>(a, blocks, warps, s);
+#define MP_LAUNCH(i, c_, l_, k_, w_, t_) \
+    case i: return launchT<c_, l_, k_, w_, false, t_>(a, blocks, warps, s);
         MP_VARIANTS(MP_LAUNCH)
 #undef MP_LAUNCH
         default: return cudaErrorInvalidValue;
@@ -1397,7 +1484,7 @@ int adjointVariantMaxWarps(int v, int nTables) {
 cudaError_t launchAdjointVariant(int v, const DpArgs &a, int blocks, int warps, cudaStream_t s) {
     switch (v) {
 #define MP_LAUNCH(i, c_, l_, k_, w_) \
-    case i: return launchT<c_, l_, k_, w_, true>(a, blocks, warps, s);
+    case i: return launchT<c_, l_, k_, w_, true, float>(a, blocks, warps, s);
         MP_ADJ_VARIANTS(MP_LAUNCH)
 #undef MP_LAUNCH
         default: return cudaErrorInvalidValue;

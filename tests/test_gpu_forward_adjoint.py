@@ -63,7 +63,8 @@ def test_forward_anchor_free_pairs(engine, gmodel, polish_model, exact_oracle):
     ap = polish_model.alignment
     rng = np.random.default_rng(12)
     parts, wants = [], []
-    for lx, ly in ((0, 0), (0, 9), (9, 0), (1, 1), (5, 40), (40, 5), (30, 33), (64, 64), (70, 66)):
+    for lx, ly in ((0, 0), (0, 9), (9, 0), (1, 1), (5, 40), (40, 5), (30, 33), (64, 64), (80, 77), (118, 120),
+                   (170, 160), (230, 228)):
         sx, sy = _rle(rng, lx), _rle(rng, ly)
         strand = int(rng.integers(0, 2))
         rl, rr = bool(rng.integers(0, 2)), bool(rng.integers(0, 2))

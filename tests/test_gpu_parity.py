@@ -154,6 +154,44 @@ def test_polish_workload_every_variant(engine, polish_model, lanes):
     assert worst <= 1e-4
 
 
+def _rle_symbols(rng, n):
+    return ((rng.integers(1, 6, size=n) << 8) | rng.integers(0, 4, size=n)).astype(np.uint16)
+
+
+def _mutate(rng, s, rate=0.1):
+    """A related sequence: substitutions, insertions and deletions at `rate` each."""
+    out = []
+    for v in s:
+        r = rng.random()
+        if r < rate:
+            continue
+        if r < 2 * rate:
+            out.append(int((v & 0xff00) | rng.integers(0, 4)))
+        else:
+            out.append(int(v))
+        if rng.random() < rate:
+            out.append(int(_rle_symbols(rng, 1)[0]))
+    return np.array(out, dtype=np.uint16)
+
+
+def test_wide_bands_every_window(engine, polish_model):
+    """Anchor-free bands as wide as the matrix, from the narrowest window to the widest (240
+    slots): unrelated sequences, whose forward and backward maxima sit far apart and need
+    the FP64 kernels, and related ones. Every job is checked against the FP64 oracle."""
+    rng = np.random.default_rng(31)
+    gm = Model.from_polish(engine, polish_model)
+    mpo = (MpoModel.from_state_model(polish_model.forward), MpoModel.from_state_model(polish_model.reverse))
+    p = AlignmentParams(threshold=0.01, diagonal_expansion=480, dynamic_anchor_expansion=False)
+    parts = []
+    for n in (20, 50, 70, 80, 100, 118, 140, 170, 200, 230):
+        sx = _rle_symbols(rng, n)
+        sy = _rle_symbols(rng, n - 3) if n % 20 else _mutate(rng, sx)[: n]
+        parts.append(Jobs.single(sx, sy, np.zeros((0, 3), np.int32), int(rng.random() < 0.5),
+                                 bool(rng.random() < 0.5), bool(rng.random() < 0.5)))
+    _, worst = _run_and_check(engine, gm, mpo, Jobs.concat(parts), p)
+    assert worst <= 1e-4
+
+
 def test_empty_and_tiny_sequences(engine, default_model):
     gm = Model(engine, default_model, default_model)
     mpo = (MpoModel.from_state_model(default_model), MpoModel.from_state_model(default_model))

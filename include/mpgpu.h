@@ -263,6 +263,98 @@ typedef struct {
 mp_status mp_expectations_batch(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
                                 mp_expectations *out, double *log_lik);
 
+/* ---- the POA loop: poa_realign / poa_realignIterative / poa_realignAll ----
+ * A set of chunks, each a draft (run-length string) with its reads, runs the reference's
+ * polishing loop in consensus mode (impl/polisher.c): every read is realigned to its chunk's
+ * reference and folded into the chunk's partial-order graph (poa_realign, :656-703, with
+ * poa_augment, :316-534), the consensus walk proposes a new reference (poa_getConsensus,
+ * :1025-1275), high-posterior observations become the next anchors
+ * (poa_getAnchorAlignments, :536-592), the run lengths are re-estimated
+ * (poa_estimateRepeatCountsUsingBayesianModel, :1556-1565) and the loop stops on an
+ * unchanged consensus or a score that does not improve (poa_realignIterative, :2034-2106).
+ * All chunks advance together: each iteration's realignments of every chunk are one batched
+ * posterior pass on the GPU; graph work runs on host threads, one chunk per thread. */
+typedef struct {
+    double reference_base_penalty;   /* referenceBasePenalty (0.5 shipped) */
+    int32_t compare_repeat_counts;   /* poaConstructCompareRepeatCounts */
+    int32_t use_run_length;          /* useRunLengthEncoding (then repeat_log10 is required) */
+    const double *anchor_probs;      /* minPosteriorProbForAlignmentAnchors: (probability, expansion) pairs */
+    int64_t n_anchor_probs;
+    int64_t min_iterations;          /* minPoaConsensusIterations */
+    int64_t max_iterations;          /* maxPoaConsensusIterations */
+} mp_polish_params;
+
+/* Chunks and reads in HOST memory. Chunk c's draft is runs [ref_offsets[c], ref_offsets[c+1])
+ * of ref_chars / ref_counts; its reads are [chunk_reads[c], chunk_reads[c+1]) (chunk_reads[0]
+ * = 0), read r is runs [read_offsets[r], read_offsets[r+1]) of read_chars / read_counts.
+ * anchors: per read (anchor_offsets[r] .. [r+1]) triples (x, y, expansion) in draft and read
+ * run coordinates, strictly increasing; anchor_offsets NULL aligns every read to the whole
+ * draft without anchors (the no-anchor path of poa_realign). */
+typedef struct {
+    int64_t n_chunks;
+    const int64_t *ref_offsets;
+    const char *ref_chars;
+    const uint32_t *ref_counts;
+    const int64_t *chunk_reads;
+    const int64_t *read_offsets;
+    const char *read_chars;
+    const uint32_t *read_counts;
+    const uint8_t *strand;            /* per read, 1 forward */
+    const int64_t *anchor_offsets;
+    const int32_t *anchors;
+} mp_polish_batch;
+
+typedef struct mp_poa_set mp_poa_set;
+typedef struct {
+    int64_t nodes;            /* graph nodes (reference runs + the leading 'N' node) */
+    int64_t max_repeat;       /* repeat-count weights per node */
+    int64_t reference_runs;   /* runs of the graph's reference string */
+    int64_t observations, inserts, deletes, insert_runs;
+    double score;             /* match weight - error weight (the stop rule's score) */
+    int64_t iterations;       /* iterations the last mp_poa_set_iterate ran for this chunk */
+} mp_poa_chunk_info;
+
+/* repeat_log10: the [4][51][51] log10 run-length table (the model's); needed when
+ * use_run_length. Nothing runs until mp_poa_set_realign. e and m may be NULL for a set that
+ * only takes caller pairs (mp_poa_set_realign_pairs) and uses the host-side steps. */
+mp_status mp_poa_set_create(mp_engine *e, const mp_model *m, const mp_params *p, const mp_polish_params *pp,
+                            const mp_polish_batch *b, const double *repeat_log10, mp_poa_set **out);
+void mp_poa_set_destroy(mp_poa_set *s);
+/* poa_realign of every chunk against its draft with the batch's anchors. */
+mp_status mp_poa_set_realign(mp_poa_set *s);
+/* poa_augment of every chunk's draft with aligned pairs the caller supplies instead of the
+ * GPU pass: for list k (0 match, 1 gap-x = deletes, 2 gap-y = inserts), read r's tuples
+ * (weight, x, y), in draft and read coordinates, are rows pair_offsets[k][r] ..
+ * pair_offsets[k][r+1] of pairs[k]. */
+mp_status mp_poa_set_realign_pairs(mp_poa_set *s, const int64_t *const pair_offsets[3], const int64_t *const pairs[3]);
+/* poa_realignIterative in consensus mode for every chunk (after mp_poa_set_realign). */
+mp_status mp_poa_set_iterate(mp_poa_set *s);
+/* poa_realignAll in consensus mode: realign, then iterate. */
+mp_status mp_poa_set_realign_all(mp_poa_set *s);
+/* poa_estimateRepeatCountsUsingBayesianModel on every chunk's graph (sets the run lengths of
+ * its reference string, as the caller of poa_realignAll does, marginPolish.c:558). */
+mp_status mp_poa_set_estimate_repeat_counts(mp_poa_set *s);
+/* Inspection of a chunk's current graph (sizes from mp_poa_info). */
+mp_status mp_poa_info(const mp_poa_set *s, int64_t chunk, mp_poa_chunk_info *info);
+mp_status mp_poa_nodes(const mp_poa_set *s, int64_t chunk, char *bases, uint64_t *repeat_counts,
+                       double *base_weights, double *repeat_count_weights, int64_t *n_obs, int64_t *n_ins,
+                       int64_t *n_del);
+mp_status mp_poa_observations(const mp_poa_set *s, int64_t chunk, int64_t *read, int64_t *offset, double *weight);
+mp_status mp_poa_inserts(const mp_poa_set *s, int64_t chunk, double *weight_fwd, double *weight_rev,
+                         int64_t *lengths, char *chars, uint64_t *counts, int64_t *n_obs);
+mp_status mp_poa_deletes(const mp_poa_set *s, int64_t chunk, int64_t *lengths, double *weight_fwd,
+                         double *weight_rev, int64_t *n_obs);
+/* The graph's reference string (reference_runs runs). */
+mp_status mp_poa_reference(const mp_poa_set *s, int64_t chunk, char *chars, uint64_t *counts);
+/* poa_getConsensus: the consensus (at most cap runs; *n_runs gets its length) and the
+ * node-to-consensus map (nodes - 1 entries, -1 for nodes not in the consensus). */
+mp_status mp_poa_consensus(const mp_poa_set *s, int64_t chunk, char *chars, uint64_t *counts, int64_t cap,
+                           int64_t *n_runs, int64_t *map);
+/* poa_getAnchorAlignments with the given map (NULL: the identity): offsets[reads+1] and
+ * triples (consensus position, read offset, expansion), at most cap. */
+mp_status mp_poa_anchor_alignments(const mp_poa_set *s, int64_t chunk, const int64_t *map, int64_t *offsets,
+                                   int64_t *triples, int64_t cap, int64_t *n_anchors);
+
 /* ---- single read without any memory allocation ----
  * No counterpart in the reference. For callers that cannot allocate device memory
  * (their framework's pool owns the GPU, or allocation is not allowed where they

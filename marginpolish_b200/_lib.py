@@ -136,6 +136,42 @@ class Expectations(Structure):
     ]
 
 
+class PolishParamsC(Structure):
+    _fields_ = [
+        ("reference_base_penalty", c_double),
+        ("compare_repeat_counts", c_int32),
+        ("use_run_length", c_int32),
+        ("anchor_probs", POINTER(c_double)),
+        ("n_anchor_probs", c_int64),
+        ("min_iterations", c_int64),
+        ("max_iterations", c_int64),
+    ]
+
+
+class PolishBatch(Structure):
+    _fields_ = [
+        ("n_chunks", c_int64),
+        ("ref_offsets", POINTER(c_int64)),
+        ("ref_chars", POINTER(c_char)),
+        ("ref_counts", POINTER(c_uint32)),
+        ("chunk_reads", POINTER(c_int64)),
+        ("read_offsets", POINTER(c_int64)),
+        ("read_chars", POINTER(c_char)),
+        ("read_counts", POINTER(c_uint32)),
+        ("strand", POINTER(c_uint8)),
+        ("anchor_offsets", POINTER(c_int64)),
+        ("anchors", POINTER(c_int32)),
+    ]
+
+
+class PoaChunkInfo(Structure):
+    _fields_ = [
+        ("nodes", c_int64), ("max_repeat", c_int64), ("reference_runs", c_int64), ("observations", c_int64),
+        ("inserts", c_int64), ("deletes", c_int64), ("insert_runs", c_int64), ("score", c_double),
+        ("iterations", c_int64),
+    ]
+
+
 class Tuning(Structure):
     _fields_ = [
         ("checkpoint_stride", c_int32),
@@ -154,6 +190,10 @@ EXPORTED = [
     "mp_rle_encode", "mp_rle_symbols", "mp_rle_anchors", "mp_device_batch_timing", "mp_measure_fp32_peak",
     "mp_realign_single_noalloc", "mp_device_batch_reset", "mp_device_batch_counts", "mp_device_batch_fetch_into",
     "mp_host_alloc", "mp_host_free", "mp_device_batch_run_plain", "mp_forward_batch", "mp_expectations_batch",
+    "mp_poa_set_create", "mp_poa_set_destroy", "mp_poa_set_realign", "mp_poa_set_realign_pairs", "mp_poa_set_iterate",
+    "mp_poa_set_realign_all", "mp_poa_set_estimate_repeat_counts", "mp_poa_info", "mp_poa_nodes",
+    "mp_poa_observations", "mp_poa_inserts", "mp_poa_deletes", "mp_poa_reference", "mp_poa_consensus",
+    "mp_poa_anchor_alignments",
 ]
 
 _lib = None
@@ -198,6 +238,26 @@ def load() -> ctypes.CDLL:
                                               c_int64, P(c_int32), c_int64, c_int, c_int, c_int, P(NoallocOutput)]),
         "mp_forward_batch": (c_int, [c_void_p, c_void_p, P(Params), P(Batch), P(c_double)]),
         "mp_expectations_batch": (c_int, [c_void_p, c_void_p, P(Params), P(Batch), P(Expectations), P(c_double)]),
+        "mp_poa_set_create": (c_int, [c_void_p, c_void_p, P(Params), P(PolishParamsC), P(PolishBatch), P(c_double),
+                                      P(c_void_p)]),
+        "mp_poa_set_destroy": (None, [c_void_p]),
+        "mp_poa_set_realign": (c_int, [c_void_p]),
+        "mp_poa_set_realign_pairs": (c_int, [c_void_p, P(P(c_int64)), P(P(c_int64))]),
+        "mp_poa_set_iterate": (c_int, [c_void_p]),
+        "mp_poa_set_realign_all": (c_int, [c_void_p]),
+        "mp_poa_set_estimate_repeat_counts": (c_int, [c_void_p]),
+        "mp_poa_info": (c_int, [c_void_p, c_int64, P(PoaChunkInfo)]),
+        "mp_poa_nodes": (c_int, [c_void_p, c_int64, P(c_char), P(ctypes.c_uint64), P(c_double), P(c_double),
+                                 P(c_int64), P(c_int64), P(c_int64)]),
+        "mp_poa_observations": (c_int, [c_void_p, c_int64, P(c_int64), P(c_int64), P(c_double)]),
+        "mp_poa_inserts": (c_int, [c_void_p, c_int64, P(c_double), P(c_double), P(c_int64), P(c_char),
+                                   P(ctypes.c_uint64), P(c_int64)]),
+        "mp_poa_deletes": (c_int, [c_void_p, c_int64, P(c_int64), P(c_double), P(c_double), P(c_int64)]),
+        "mp_poa_reference": (c_int, [c_void_p, c_int64, P(c_char), P(ctypes.c_uint64)]),
+        "mp_poa_consensus": (c_int, [c_void_p, c_int64, P(c_char), P(ctypes.c_uint64), c_int64, P(c_int64),
+                                     P(c_int64)]),
+        "mp_poa_anchor_alignments": (c_int, [c_void_p, c_int64, P(c_int64), P(c_int64), P(c_int64), c_int64,
+                                             P(c_int64)]),
         "mp_band": (c_int, [P(c_int32), c_int64, c_int64, c_int64, c_int64, c_int, P(c_int64)]),
         "mp_split_points": (c_int, [P(c_int32), c_int64, c_int64, c_int64, c_int64, c_int, c_int, P(c_int64),
                                     c_int64, P(c_int64)]),

@@ -1,0 +1,1060 @@
+// POA side of the realignment loop: the partial-order graph each chunk's reads are folded
+// into, the consensus walk, the anchor alignments for the next iteration, the run-length
+// estimate and the iterative driver (MarginPolish impl/polisher.c):
+//
+//   poa_getReferenceGraph  impl/polisher.c:118-132     Poa::fromReference
+//   poa_augment            impl/polisher.c:316-534     augment
+//   poa_getAnchorAlignments impl/polisher.c:536-592    anchorAlignments
+//   crop + naming          impl/polisher.c:605-654     realignChunks (jobs of one GPU batch)
+//   poa_realign            impl/polisher.c:656-703     realignChunks
+//   score                  impl/polisher.c:709-758     score
+//   poa_getConsensus       impl/polisher.c:1025-1275   consensus
+//   repeat-count ML        impl/polisher.c:1556-1565, :1756-1865   estimateRepeatCounts
+//   poa_realignIterative   impl/polisher.c:2034-2106   iterate (consensus mode)
+//   poa_realignAll         impl/polisher.c:2109-2129   mp_poa_set_realign_all
+//
+// All chunks advance in lockstep: every realignment of an iteration, over the reads of
+// every chunk still iterating, is one batched posterior pass on the GPU; the per-chunk
+// graph work runs on host threads, one chunk per thread. Weights are sums of integer
+// posteriors held in doubles, so they are exact; observation lists keep the reference's
+// order (the posterior tuples arrive in the reference's order).
+#include "../../include/mpgpu.h"
+#include "mp_host.h"
+#include "mp_internal.h"
+
+#include <algorithm>
+#include <atomic>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#define MP_TRY(expr)                   \
+    do {                               \
+        mp_status _s = (expr);         \
+        if (_s != MP_OK) return _s;    \
+    } while (0)
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// run-length strings
+// ---------------------------------------------------------------------------
+
+struct Rle {
+    std::string c;                // one character per run
+    std::vector<uint64_t> n;      // run lengths
+    uint64_t nonRle = 0;          // expanded length
+    int64_t length() const { return (int64_t) c.size(); }
+    void push(char ch, uint64_t k) {
+        c.push_back(ch);
+        n.push_back(k);
+        nonRle += k;
+    }
+    Rle sub(int64_t start, int64_t len) const {
+        Rle r;
+        for (int64_t i = start; i < start + len; i++) r.push(c[i], n[i]);
+        return r;
+    }
+    bool operator==(const Rle &o) const { return nonRle == o.nonRle && c == o.c && n == o.n; }
+};
+
+// rleString_construct (impl/polisher.c:1357-1389): runs of equal characters.
+Rle rleOf(const std::string &s) {
+    Rle r;
+    for (size_t i = 0; i < s.size();) {
+        size_t j = i + 1;
+        while (j < s.size() && s[j] == s[i]) j++;
+        r.push(s[i], (uint64_t) (j - i));
+        i = j;
+    }
+    return r;
+}
+
+// rleString_construct_no_rle: every character its own run of one.
+Rle rleNoRle(const std::string &s) {
+    Rle r;
+    for (char ch : s) r.push(ch, 1);
+    return r;
+}
+
+// The nucleotide alphabet (impl/stateMachine.c:25-59): A C G T, anything else N.
+int symbolOf(char ch) {
+    switch (ch) {
+        case 'A': case 'a': return 0;
+        case 'C': case 'c': return 1;
+        case 'G': case 'g': return 2;
+        case 'T': case 't': return 3;
+        default: return 4;
+    }
+}
+
+char charOf(int s) {
+    return "ACGTN"[s < 0 || s > 4 ? 4 : s];
+}
+
+// The reference's approximate log-sum (impl/pairwiseAligner.c:279-299): a four-piece cubic
+// of the difference (coefficients as the reference writes them, in single precision), the
+// smaller term dropped from a difference of 7.5. The consensus walk makes its choices on
+// sums of this function, so identical consensus needs the same function.
+double lookupCubic(double x) {
+    if (x <= 1.00f) return ((-0.009350833524763f * x + 0.130659527668286f) * x + 0.498799810682272f) * x + 0.693203116424741f;
+    if (x <= 2.50f) return ((-0.014532321752540f * x + 0.139942324101744f) * x + 0.495635523139337f) * x + 0.692140569840976f;
+    if (x <= 4.50f) return ((-0.004605031767994f * x + 0.063427417320019f) * x + 0.695956496475118f) * x + 0.514272634594009f;
+    return ((-0.000458661602210f * x + 0.009695946122598f) * x + 0.930734667215156f) * x + 0.168037164329057f;
+}
+
+double logAddApprox(double x, double y) {
+    const double kZero = -INFINITY, kUnder = 7.5;
+    if (x < y) return (x == kZero || y - x >= kUnder) ? y : lookupCubic(y - x) + x;
+    return (y == kZero || x - y >= kUnder) ? x : lookupCubic(x - y) + y;
+}
+
+// ---------------------------------------------------------------------------
+// the graph
+// ---------------------------------------------------------------------------
+
+struct Obs {
+    int64_t read, offset;
+    double weight;
+};
+
+struct Insert {
+    Rle s;
+    double wF = 0.0, wR = 0.0;
+    std::vector<Obs> obs;
+    double weight() const { return wF + wR; }
+};
+
+struct Delete {
+    int64_t len = 0;
+    double wF = 0.0, wR = 0.0;
+    std::vector<Obs> obs;
+    double weight() const { return wF + wR; }
+};
+
+struct Node {
+    char base = 'N';
+    uint64_t rc = 1;
+    double bw[5] = {0, 0, 0, 0, 0};
+    std::vector<double> rcw;
+    std::vector<Obs> obs;
+    std::vector<Insert> ins;
+    std::vector<Delete> del;
+};
+
+struct Poa {
+    uint64_t maxRC = 2;  // repeat counts are < maxRC
+    std::vector<Node> nodes;
+    Rle ref;
+
+    // poa_getReferenceGraph: node 0 is an 'N' prefix, then one node per reference run.
+    static Poa fromReference(const Rle &reference, uint64_t maxRC) {
+        Poa p;
+        p.maxRC = maxRC;
+        p.ref = reference;
+        p.nodes.resize(reference.length() + 1);
+        for (int64_t i = 0; i <= reference.length(); i++) {
+            Node &n = p.nodes[i];
+            char b = i == 0 ? 'N' : (char) toupper((unsigned char) reference.c[i - 1]);
+            n.base = charOf(symbolOf(b)) == 'N' ? 'N' : b;  // anything but ACGT becomes N
+            n.rc = i == 0 ? 1 : reference.n[i - 1];
+            n.rcw.assign(maxRC, 0.0);
+        }
+        return p;
+    }
+};
+
+struct Pair {  // (weight, x, y) of the aligner's lists
+    int64_t w, x, y;
+};
+
+// ---------------------------------------------------------------------------
+// poa_augment (impl/polisher.c:316-534) and its indel helpers (:160-314)
+// ---------------------------------------------------------------------------
+
+bool hasInternalRepeat(const Rle &s, int64_t k, bool cmpRC) {
+    if (s.length() % k != 0) return false;
+    for (int64_t i = k; i < s.length(); i += k)
+        for (int64_t j = 0; j < k; j++)
+            if (s.c[j] != s.c[j + i] || (cmpRC && s.n[j] != s.n[j + i])) return false;
+    return true;
+}
+
+bool matchesRef(const Rle &ref, int64_t start, const Rle &s, int64_t len, bool cmpRC) {
+    for (int64_t l = 0; l < len; l++)
+        if (ref.c[start + l] != s.c[l] || (cmpRC && ref.n[start + l] != s.n[l])) return false;
+    return true;
+}
+
+// Leftmost position an indel with sequence s at refStart can move to (getShift, :269-297).
+int64_t getShift(const Rle &ref, int64_t refStart, const Rle &s, bool cmpRC) {
+    int64_t minRepeat = 0;
+    while (minRepeat++ < s.length())
+        if (hasInternalRepeat(s, minRepeat, cmpRC)) break;
+    for (int64_t k = refStart - minRepeat; k >= 0; k -= minRepeat) {
+        if (!matchesRef(ref, k, s, minRepeat, cmpRC)) break;
+        refStart = k;
+    }
+    if (s.length() == 1 && cmpRC && refStart > 0 && ref.c[refStart - 1] == s.c[0]) refStart--;
+    return refStart;
+}
+
+int64_t maxCommonSuffix(const Rle &a, int64_t lenA, const Rle &b, bool cmpRC) {
+    int64_t i = 0;
+    while (lenA - i - 1 >= 0 && b.length() - i - 1 >= 0) {
+        if (a.c[lenA - 1 - i] != b.c[b.length() - 1 - i] ||
+            (cmpRC && a.n[lenA - 1 - i] != b.n[b.length() - 1 - i]))
+            break;
+        i++;
+    }
+    return i;
+}
+
+void rotate(Rle &s, int64_t k) {
+    const int64_t L = s.length();
+    std::string c(L, ' ');
+    std::vector<uint64_t> n(L);
+    for (int64_t i = 0; i < L; i++) {
+        c[(i + k) % L] = s.c[i];
+        n[(i + k) % L] = s.n[i];
+    }
+    s.c = c;
+    s.n = n;
+}
+
+struct MatchSet {  // the match coordinates of one read, sorted by (x, y)
+    std::vector<std::pair<int64_t, int64_t>> v;
+    bool has(int64_t x, int64_t y) const { return std::binary_search(v.begin(), v.end(), std::make_pair(x, y)); }
+};
+
+void augment(Poa &poa, const Rle &read, bool strand, int64_t readNo, const std::vector<Pair> &matches,
+             std::vector<Pair> inserts, std::vector<Pair> deletes, bool cmpRC) {
+    // match weights and observations
+    for (const Pair &m : matches) {
+        Node &node = poa.nodes[m.x + 1];
+        node.bw[symbolOf(read.c[m.y])] += (double) m.w;
+        uint64_t rc = read.n[m.y];
+        if (rc >= poa.maxRC) rc = poa.maxRC - 1;
+        node.rcw[rc] += (double) m.w;
+        node.obs.push_back(Obs{readNo, m.y, (double) m.w});
+    }
+    MatchSet ms;
+    ms.v.reserve(matches.size());
+    for (const Pair &m : matches) ms.v.emplace_back(m.x, m.y);
+    std::sort(ms.v.begin(), ms.v.end());
+
+    // complete inserts: same x, consecutive y, flanked by matches (or the read's ends)
+    std::sort(inserts.begin(), inserts.end(), [](const Pair &a, const Pair &b) {
+        return a.x != b.x ? a.x < b.x : a.y < b.y;
+    });
+    const int64_t nI = (int64_t) inserts.size();
+    for (int64_t i = 0; i < nI;) {
+        const Pair &st = inserts[i];
+        int64_t j = i + 1;
+        for (; j < nI; j++) {
+            if (st.x != inserts[j].x || st.y + j - i != inserts[j].y) break;
+        }
+        for (int64_t k = i; k < j; k++) {
+            if (!ms.has(st.x, st.y + k - i - 1) && st.y + k - i - 1 > -1) continue;
+            for (int64_t l = k; l < j; l++) {
+                if (!ms.has(st.x + 1, st.y + l - i + 1) && st.y + l - i + 1 < read.length()) continue;
+                Rle ins = read.sub(inserts[k].y, l + 1 - k);
+                double w = (double) UINT_MAX;
+                for (int64_t m = k; m <= l; m++) w = w < (double) inserts[m].w ? w : (double) inserts[m].w;
+                int64_t pos = st.x + 1;
+                pos = getShift(poa.ref, pos, ins, cmpRC);
+                const int64_t suf = maxCommonSuffix(poa.ref, pos, ins, cmpRC);
+                if (suf > 0) {
+                    rotate(ins, suf);
+                    pos -= suf;
+                }
+                Node &node = poa.nodes[pos];
+                Insert *target = nullptr;
+                for (Insert &e : node.ins)
+                    if (e.s == ins) {
+                        target = &e;
+                        break;
+                    }
+                if (!target) {
+                    node.ins.push_back(Insert{ins, 0.0, 0.0, {}});
+                    target = &node.ins.back();
+                }
+                if (strand) target->wF += w; else target->wR += w;
+                target->obs.push_back(Obs{readNo, inserts[k].y, w});
+            }
+        }
+        i = j;
+    }
+
+    // complete deletes: same y, consecutive x, flanked by matches (or the reference's ends)
+    std::sort(deletes.begin(), deletes.end(), [](const Pair &a, const Pair &b) {
+        return a.y != b.y ? a.y < b.y : a.x < b.x;
+    });
+    const int64_t nD = (int64_t) deletes.size();
+    for (int64_t i = 0; i < nD;) {
+        const Pair &st = deletes[i];
+        int64_t j = i + 1;
+        for (; j < nD; j++) {
+            if (st.y != deletes[j].y || st.x + j - i != deletes[j].x) break;
+        }
+        for (int64_t k = i; k < j; k++) {
+            if (!ms.has(st.x + k - i - 1, st.y) && st.x + k - i - 1 > -1) continue;
+            for (int64_t l = k; l < j; l++) {
+                if (!ms.has(st.x + l - i + 1, st.y + 1) && st.x + l - i + 1 < poa.ref.length()) continue;
+                const int64_t len = l - k + 1;
+                double w = (double) UINT_MAX;
+                for (int64_t m = k; m <= l; m++) w = w < (double) deletes[m].w ? w : (double) deletes[m].w;
+                int64_t pos = st.x + k - i;
+                const Rle del = poa.ref.sub(pos, len);
+                pos = getShift(poa.ref, pos, del, cmpRC);
+                pos -= maxCommonSuffix(poa.ref, pos, del, cmpRC);
+                Node &node = poa.nodes[pos];
+                Delete *target = nullptr;
+                for (Delete &e : node.del)
+                    if (e.len == len) {
+                        target = &e;
+                        break;
+                    }
+                if (!target) {
+                    node.del.push_back(Delete{len, 0.0, 0.0, {}});
+                    target = &node.del.back();
+                }
+                if (strand) target->wF += w; else target->wR += w;
+                target->obs.push_back(Obs{readNo, st.y, w});
+            }
+        }
+        i = j;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// weights and the stop rule (impl/polisher.c:709-758)
+// ---------------------------------------------------------------------------
+
+double score(const Poa &poa) {
+    double match = 0.0, dis = 0.0, ins = 0.0, del = 0.0;
+    for (const Node &n : poa.nodes) match += n.bw[symbolOf(n.base)];
+    for (const Node &n : poa.nodes) {
+        const int r = symbolOf(n.base);
+        for (int j = 0; j < 5; j++)
+            if (j != r) dis += n.bw[j];
+    }
+    for (const Node &n : poa.nodes)
+        for (const Insert &e : n.ins) ins += e.weight() * (double) e.s.length();
+    for (const Node &n : poa.nodes)
+        for (const Delete &e : n.del) del += e.weight() * (double) e.len;
+    return match - (del + ins + dis);
+}
+
+// ---------------------------------------------------------------------------
+// poa_getConsensus (impl/polisher.c:1025-1275)
+// ---------------------------------------------------------------------------
+
+int64_t maxWeight(const double *w, int64_t n, int64_t refIndex, double penalty) {
+    double best = 0.0;
+    int64_t at = -1;
+    for (int64_t j = 0; j < n; j++) {
+        if (j != refIndex && w[j] >= best) {
+            best = w[j];
+            at = j;
+        }
+    }
+    return w[refIndex] * penalty > best ? refIndex : at;
+}
+
+Rle consensus(const Poa &poa, std::vector<int64_t> &map, double penalty, bool useRle) {
+    const int64_t nN = (int64_t) poa.nodes.size();
+    const double kZero = -INFINITY;
+    std::vector<double> outW(nN, 0.0), fwd(nN + 1, kZero), matchFwd(nN, 0.0);
+    fwd[0] = 0.0;
+    std::vector<std::vector<const Delete *>> incoming(nN + 1);
+    for (int64_t i = 0; i < nN; i++)
+        for (const Delete &d : poa.nodes[i].del) incoming[i + d.len + 1].push_back(&d);
+    for (int64_t i = 0; i < nN; i++) {
+        const Node &node = poa.nodes[i];
+        double indel = 0.0;
+        for (const Insert &e : node.ins) indel += e.weight();
+        for (const Delete &e : node.del) indel += e.weight();
+        double mw = 0.0;
+        if (i == 0) {
+            if (nN == 1) {
+                mw = 1.0;
+            } else {
+                for (int64_t j = 1; j < nN; j++)
+                    for (int k = 0; k < 5; k++) mw += poa.nodes[j].bw[k];
+                mw /= (double) (nN - 1);
+                mw -= indel;
+            }
+        } else {
+            for (int k = 0; k < 5; k++) mw += node.bw[k];
+            mw -= indel;
+        }
+        mw = mw <= 0.0 ? 0.0001 : mw;
+        outW[i] = mw + indel;
+        for (const Insert &e : node.ins) fwd[i + 1] = logAddApprox(fwd[i + 1], fwd[i] + std::log(e.weight() / outW[i]));
+        for (const Delete &e : node.del)
+            fwd[i + e.len + 1] = logAddApprox(fwd[i + e.len + 1], fwd[i] + std::log(e.weight() / outW[i]));
+        matchFwd[i] = fwd[i] + std::log(mw / outW[i]);
+        fwd[i + 1] = logAddApprox(fwd[i + 1], matchFwd[i]);
+    }
+
+    map.assign(nN - 1, -1);
+    std::vector<std::string> pieces;
+    int64_t running = 0;
+    char prevBase = '-';
+    for (int64_t i = nN; i > 0;) {
+        if (i < nN) {
+            const Node &node = poa.nodes[i];
+            const char base = charOf((int) maxWeight(node.bw, 5, symbolOf(node.base), penalty));
+            if (useRle) {
+                int64_t rc = maxWeight(node.rcw.data(), (int64_t) poa.maxRC, (int64_t) node.rc, penalty);
+                rc = rc == 0 ? 1 : rc;
+                pieces.push_back(std::string((size_t) rc, base));
+                if (prevBase != base) map[i - 1] = running++;
+                prevBase = base;
+            } else {
+                pieces.push_back(std::string(1, base));
+                map[i - 1] = running++;
+            }
+        }
+        double maxIns = kZero, totIns = kZero;
+        const Insert *bestIns = nullptr;
+        const Node &pNode = poa.nodes[i - 1];
+        for (const Insert &e : pNode.ins) {
+            const double p = std::log(e.weight() / outW[i - 1]) + fwd[i - 1];
+            if (p > maxIns) {
+                maxIns = p;
+                bestIns = &e;
+            }
+            totIns = logAddApprox(totIns, p);
+        }
+        double maxDel = kZero, totDel = kZero;
+        const Delete *bestDel = nullptr;
+        for (const Delete *e : incoming[i]) {
+            const double p = std::log(e->weight() / outW[i - e->len - 1]) + fwd[i - e->len - 1];
+            if (p > maxDel) {
+                maxDel = p;
+                bestDel = e;
+            }
+            totDel = logAddApprox(totDel, p);
+        }
+        if (matchFwd[i - 1] >= totDel && matchFwd[i - 1] >= totIns) {
+            i--;
+        } else if (totIns >= totDel) {
+            std::string ex;
+            for (int64_t r = 0; r < bestIns->s.length(); r++) ex.append((size_t) bestIns->s.n[r], bestIns->s.c[r]);
+            pieces.push_back(ex);
+            if (useRle) {
+                const char last = bestIns->s.c[bestIns->s.length() - 1];
+                running += bestIns->s.length() + (last != prevBase ? 0 : -1);
+                prevBase = bestIns->s.c[0];
+            } else {
+                running += (int64_t) bestIns->s.nonRle;
+            }
+            i--;
+        } else {
+            i -= bestDel->len + 1;
+        }
+    }
+    std::string expanded;
+    for (auto it = pieces.rbegin(); it != pieces.rend(); ++it) expanded += *it;
+    Rle out = useRle ? rleOf(expanded) : rleNoRle(expanded);
+    for (int64_t i = 0; i < nN - 1; i++)
+        if (map[i] != -1) map[i] = out.length() - 1 - map[i];
+    return out;
+}
+
+// ---------------------------------------------------------------------------
+// poa_getAnchorAlignments (impl/polisher.c:536-592)
+// ---------------------------------------------------------------------------
+
+struct Anchor {
+    int64_t x, y, e;
+};
+
+std::vector<std::vector<Anchor>> anchorAlignments(const Poa &poa, const std::vector<int64_t> *map, int64_t nReads,
+                                                  const std::vector<double> &probs) {
+    std::vector<std::vector<Anchor>> out(nReads);
+    for (int64_t i = 1; i < (int64_t) poa.nodes.size(); i++) {
+        const int64_t ci = map ? (*map)[i - 1] : i - 1;
+        if (ci == -1) continue;
+        for (const Obs &o : poa.nodes[i].obs) {
+            const double w = o.weight / (double) mp::kProbOne;
+            if (!(w > probs[0])) continue;
+            int64_t e = (int64_t) probs[1];
+            for (size_t k = 2; k < probs.size(); k += 2) {
+                if (w >= probs[k]) e = (int64_t) probs[k + 1];
+                else break;
+            }
+            auto &l = out[o.read];
+            if (l.empty() || (l.back().x < ci && l.back().y < o.offset)) l.push_back(Anchor{ci, o.offset, e});
+        }
+    }
+    return out;
+}
+
+// ---------------------------------------------------------------------------
+// run-length estimate (impl/polisher.c:1556-1565, :1756-1865)
+// ---------------------------------------------------------------------------
+
+struct RepeatModel {
+    int64_t M = 0;                 // maximumRepeatLength
+    std::vector<double> log10;     // [base row][underlying][observed]
+    double logProb(int base, bool strand, int64_t observed, int64_t underlying) const {
+        if (base == 4) base = 0;   // 'N' reads the A table
+        const int64_t idx = (strand ? base : 3 - base) * M * M + underlying * M + observed;
+        return log10[idx];
+    }
+};
+
+uint64_t mlRepeatCount(const Poa &poa, const Node &node, const std::vector<Rle> &reads, const std::vector<uint8_t> &strand,
+                       int64_t readBase, const RepeatModel &rm) {
+    const int base = symbolOf(node.base);
+    int64_t lo = rm.M, hi = 0;
+    for (const Obs &o : node.obs) {
+        const int64_t c = (int64_t) reads[readBase + o.read].n[o.offset];
+        lo = c < lo ? c : lo;
+        hi = c > hi ? c : hi;
+    }
+    if (hi >= rm.M) hi = rm.M - 1;
+    if (lo == rm.M) return 0;
+    double best = 0.0;
+    int64_t bestAt = 0;
+    for (int64_t u = lo; u <= hi; u++) {
+        double lp = 0.0;
+        for (const Obs &o : node.obs) {
+            int64_t c = (int64_t) reads[readBase + o.read].n[o.offset];
+            c = c >= rm.M ? rm.M - 1 : c;
+            lp += rm.logProb(base, strand[readBase + o.read] != 0, c, u) * o.weight;
+        }
+        lp /= (double) mp::kProbOne;
+        if (u == lo || lp > best) {
+            best = lp;
+            bestAt = u - lo;
+        }
+    }
+    (void) poa;
+    return (uint64_t) (bestAt + lo);
+}
+
+void estimateRepeatCounts(Poa &poa, const std::vector<Rle> &reads, const std::vector<uint8_t> &strand, int64_t readBase,
+                          const RepeatModel &rm) {
+    poa.ref.nonRle = 0;
+    for (size_t i = 1; i < poa.nodes.size(); i++) {
+        uint64_t rc = mlRepeatCount(poa, poa.nodes[i], reads, strand, readBase, rm);
+        if (rc == 0) rc = 1;
+        poa.ref.n[i - 1] = rc;
+        poa.ref.nonRle += rc;
+    }
+}
+
+// Runs f(c) for every chunk index in `chunks` on up to `threads` host threads.
+template <class F>
+void forChunks(const std::vector<int64_t> &chunks, F f) {
+    const unsigned nT = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(),
+                                                        (unsigned) std::max<size_t>(chunks.size(), 1)));
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        for (size_t k = next++; k < chunks.size(); k = next++) f(chunks[k]);
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nT; t++) th.emplace_back(work);
+    work();
+    for (auto &t : th) t.join();
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// the chunk set behind the C ABI
+// ---------------------------------------------------------------------------
+
+struct mp_poa_set {
+    mp_engine *e = nullptr;
+    const mp_model *m = nullptr;
+    mp_params p{};
+    double penalty = 0.5;
+    bool cmpRC = true, useRle = true;
+    std::vector<double> anchorProbs;
+    int64_t minIter = 0, maxIter = 0;
+    RepeatModel rm;
+    int64_t nChunks = 0;
+    std::vector<Rle> drafts;                 // per chunk: the draft the set was created with
+    std::vector<int64_t> chunkReads;         // n_chunks+1
+    std::vector<Rle> reads;
+    std::vector<uint8_t> strand;
+    std::vector<std::vector<Anchor>> initialAnchors;  // per read (empty list when none given)
+    bool haveAnchors = false;
+    std::vector<Poa> poas;                   // per chunk (after a realignment)
+    std::vector<int64_t> iterations;         // per chunk: iterations run by the last iterate
+    mp_device_batch *db = nullptr;
+    ~mp_poa_set() { mp_device_batch_destroy(db); }
+};
+
+namespace {
+
+// poa_realign (impl/polisher.c:656-703) for the given chunks, each against `refs[c]` with
+// per-read anchors (NULL: align without anchors): one GPU batch for every read, then each
+// chunk's reads are folded into a fresh graph in read order.
+mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const std::vector<Rle> &refs,
+                        const std::vector<std::vector<Anchor>> *anchors, std::vector<Poa> &out) {
+    if (!s->e || !s->m) return mp_fail(MP_ERR_STATE, "mp_poa: realignment needs an engine and a model");
+    // symbol repeat counts are clamped below the repeat table's dimension on the cropping path
+    // (impl/polisher.c:634-635) and one lower on the path without anchors (:676-679)
+    const uint64_t maxRC = s->useRle ? (uint64_t) s->rm.M : 2;
+    const uint32_t maxExcl = (uint32_t) (anchors ? maxRC : maxRC - 1);
+    auto symbols = [&](const Rle &r, int64_t start, int64_t len, std::vector<uint16_t> &dst) {
+        for (int64_t i = start; i < start + len; i++) {
+            const uint16_t b = (uint16_t) symbolOf(r.c[i]);
+            uint64_t cnt = r.n[i];
+            if (s->m->host[0].runLength) {
+                cnt = cnt > maxExcl - 1 ? maxExcl - 1 : cnt;
+                dst.push_back((uint16_t) ((cnt << 8) | b));
+            } else {
+                dst.push_back(b);
+            }
+        }
+    };
+    // jobs: one per read of the listed chunks, with the reference crop (impl/polisher.c:613-628)
+    std::vector<uint16_t> xs, ys;
+    std::vector<int64_t> xb, xe, yo{0}, ao{0}, shift;
+    std::vector<int32_t> an;
+    std::vector<uint8_t> st;
+    std::vector<int64_t> refStart(s->nChunks, 0);
+    for (int64_t c : chunks) {
+        refStart[c] = (int64_t) xs.size();
+        symbols(refs[c], 0, refs[c].length(), xs);
+    }
+    std::vector<std::pair<int64_t, int64_t>> jobRead;  // (chunk, read index)
+    for (int64_t c : chunks) {
+        const int64_t L = refs[c].length();
+        for (int64_t r = s->chunkReads[c]; r < s->chunkReads[c + 1]; r++) {
+            const Rle &read = s->reads[r];
+            int64_t first = 0, end = L;
+            const std::vector<Anchor> *ra = anchors ? &(*anchors)[r] : nullptr;
+            if (ra && !ra->empty()) {
+                first = ra->front().x - ra->front().y;
+                first = first < 0 ? 0 : first;
+                end = 1 + ra->back().x + (read.length() - ra->back().y);
+                end = end > L ? L : end;
+            }
+            xb.push_back(refStart[c] + first);
+            xe.push_back(refStart[c] + end);
+            shift.push_back(first);
+            symbols(read, 0, read.length(), ys);
+            yo.push_back((int64_t) ys.size());
+            if (ra)
+                for (const Anchor &a : *ra) {
+                    an.push_back((int32_t) (a.x - first));
+                    an.push_back((int32_t) a.y);
+                    an.push_back((int32_t) a.e);
+                }
+            ao.push_back((int64_t) an.size() / 3);
+            st.push_back(s->strand[r]);
+            jobRead.emplace_back(c, r);
+        }
+    }
+    const int64_t nJobs = (int64_t) jobRead.size();
+    std::vector<int64_t> offs[3];
+    std::vector<int32_t> w[3], x[3], y[3];
+    if (nJobs > 0) {
+        mp_batch b;
+        memset(&b, 0, sizeof(b));
+        b.n_jobs = nJobs;
+        b.x_begin = xb.data();
+        b.x_end = xe.data();
+        b.x_symbols_length = (int64_t) xs.size();
+        uint16_t dummy = 0;
+        int32_t dummyA[3] = {0, 0, 0};
+        b.x_symbols = xs.empty() ? &dummy : xs.data();
+        b.y_offsets = yo.data();
+        b.y_symbols = ys.empty() ? &dummy : ys.data();
+        b.anchor_offsets = ao.data();
+        b.anchors = an.empty() ? dummyA : an.data();
+        b.strand = st.data();
+        b.x_shift = shift.data();
+        mp_status rc = s->db ? mp_device_batch_reset(s->e, s->db, &s->p, &b)
+                             : mp_device_batch_create(s->e, s->m, &s->p, &b, &s->db);
+        if (rc != MP_OK) return rc;
+        rc = mp_device_batch_run(s->e, s->db, nullptr);
+        if (rc != MP_OK) return rc;
+        int64_t totals[3];
+        rc = mp_device_batch_counts(s->db, totals);
+        if (rc != MP_OK) return rc;
+        mp_output o;
+        memset(&o, 0, sizeof(o));
+        for (int k = 0; k < 3; k++) {
+            offs[k].assign(nJobs + 1, 0);
+            w[k].resize(std::max<int64_t>(totals[k], 1));
+            x[k].resize(std::max<int64_t>(totals[k], 1));
+            y[k].resize(std::max<int64_t>(totals[k], 1));
+            o.offsets[k] = offs[k].data();
+            o.weight[k] = w[k].data();
+            o.x[k] = x[k].data();
+            o.y[k] = y[k].data();
+        }
+        rc = mp_device_batch_fetch_into(s->e, s->db, &o);
+        if (rc != MP_OK) return rc;
+    }
+    // fold each chunk's reads into its graph (chunks in parallel, reads in order)
+    std::vector<int64_t> firstJob(s->nChunks, 0);
+    {
+        int64_t j = 0;
+        for (int64_t c : chunks) {
+            firstJob[c] = j;
+            j += s->chunkReads[c + 1] - s->chunkReads[c];
+        }
+    }
+    forChunks(chunks, [&](int64_t c) {
+        Poa poa = Poa::fromReference(refs[c], maxRC);
+        for (int64_t r = s->chunkReads[c]; r < s->chunkReads[c + 1]; r++) {
+            const int64_t j = firstJob[c] + (r - s->chunkReads[c]);
+            std::vector<Pair> lists[3];
+            for (int k = 0; k < 3; k++) {
+                for (int64_t t = offs[k][j]; t < offs[k][j + 1]; t++) lists[k].push_back(Pair{w[k][t], x[k][t], y[k][t]});
+            }
+            // gap-x (consumes the reference) are deletes, gap-y inserts (impl/polisher.c:638-640)
+            augment(poa, s->reads[r], s->strand[r] != 0, r - s->chunkReads[c], lists[0], lists[2], lists[1], s->cmpRC);
+        }
+        out[c] = std::move(poa);
+    });
+    return MP_OK;
+}
+
+// poa_realignIterative in consensus mode (impl/polisher.c:2034-2106) for every chunk at once.
+mp_status iterate(mp_poa_set *s) {
+    const int64_t nC = s->nChunks;
+    std::vector<double> sc(nC);
+    std::vector<int64_t> active;
+    for (int64_t c = 0; c < nC; c++) {
+        sc[c] = score(s->poas[c]);
+        s->iterations[c] = 0;
+        if (s->maxIter > 0) active.push_back(c);
+    }
+    std::vector<Rle> cons(nC);
+    std::vector<std::vector<int64_t>> maps(nC);
+    std::vector<Poa> next(nC);
+    while (!active.empty()) {
+        std::vector<uint8_t> realign(nC, 0);
+        std::vector<std::vector<Anchor>> anchors(s->reads.size());
+        forChunks(active, [&](int64_t c) {
+            s->iterations[c]++;
+            cons[c] = consensus(s->poas[c], maps[c], s->penalty, s->useRle);
+            if (cons[c] == s->poas[c].ref) return;  // greedy convergence
+            auto a = anchorAlignments(s->poas[c], &maps[c], s->chunkReads[c + 1] - s->chunkReads[c], s->anchorProbs);
+            for (int64_t r = 0; r < (int64_t) a.size(); r++) anchors[s->chunkReads[c] + r] = std::move(a[r]);
+            realign[c] = 1;
+        });
+        std::vector<int64_t> go;
+        for (int64_t c : active)
+            if (realign[c]) go.push_back(c);
+        if (go.empty()) break;
+        MP_TRY(realignChunks(s, go, cons, &anchors, next));
+        std::vector<int64_t> still;
+        std::vector<uint8_t> keep(nC, 0);
+        forChunks(go, [&](int64_t c) {
+            if (s->useRle) estimateRepeatCounts(next[c], s->reads, s->strand, s->chunkReads[c], s->rm);
+            const double sc2 = score(next[c]);
+            if (sc2 <= sc[c] && s->iterations[c] > s->minIter) return;  // greedy stop: keep the old graph
+            s->poas[c] = std::move(next[c]);
+            sc[c] = sc2;
+            keep[c] = 1;
+        });
+        for (int64_t c : go)
+            if (keep[c] && s->iterations[c] < s->maxIter) still.push_back(c);
+        active.swap(still);
+    }
+    return MP_OK;
+}
+
+mp_status chunkCheck(const mp_poa_set *s, int64_t chunk) {
+    if (!s) return mp_fail(MP_ERR_ARGUMENT, "mp_poa: NULL set");
+    if (chunk < 0 || chunk >= s->nChunks) return mp_fail(MP_ERR_ARGUMENT, "mp_poa: chunk %lld out of range",
+                                                         (long long) chunk);
+    if (s->poas.empty()) return mp_fail(MP_ERR_STATE, "mp_poa: no graph yet (realign first)");
+    return MP_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" mp_status mp_poa_set_create(mp_engine *e, const mp_model *m, const mp_params *p, const mp_polish_params *pp,
+                                       const mp_polish_batch *b, const double *repeat_log10, mp_poa_set **out) {
+    if (!p || !pp || !b || !out) return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_create: NULL argument");
+    *out = nullptr;
+    if (b->n_chunks < 0 || !b->ref_offsets || !b->chunk_reads || !b->read_offsets || !b->strand)
+        return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_create: batch arrays missing");
+    if (pp->n_anchor_probs < 2 || (pp->n_anchor_probs & 1) || !pp->anchor_probs)
+        return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_create: anchor probabilities must be (probability, expansion) pairs");
+    if (pp->min_iterations < 0 || pp->max_iterations < pp->min_iterations)
+        return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_create: need 0 <= min_iterations <= max_iterations");
+    if (pp->use_run_length && !repeat_log10)
+        return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_create: run-length polishing needs the repeat-count table");
+    mp_poa_set *s = new mp_poa_set();
+    s->e = e;
+    s->m = m;
+    s->p = *p;
+    s->penalty = pp->reference_base_penalty;
+    s->cmpRC = pp->compare_repeat_counts != 0;
+    s->useRle = pp->use_run_length != 0;
+    s->anchorProbs.assign(pp->anchor_probs, pp->anchor_probs + pp->n_anchor_probs);
+    s->minIter = pp->min_iterations;
+    s->maxIter = pp->max_iterations;
+    s->rm.M = mp::kMaxRepeat;
+    if (repeat_log10) s->rm.log10.assign(repeat_log10, repeat_log10 + 4 * mp::kMaxRepeat * mp::kMaxRepeat);
+    s->nChunks = b->n_chunks;
+    const int64_t nReads = b->chunk_reads[b->n_chunks] - b->chunk_reads[0];
+    if (b->chunk_reads[0] != 0 || nReads < 0) {
+        delete s;
+        return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_create: chunk_reads must start at 0 and not decrease");
+    }
+    for (int64_t c = 0; c < b->n_chunks; c++) {
+        if (b->ref_offsets[c + 1] < b->ref_offsets[c] || b->chunk_reads[c + 1] < b->chunk_reads[c]) {
+            delete s;
+            return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_create: offsets of chunk %lld decrease", (long long) c);
+        }
+        Rle r;
+        for (int64_t i = b->ref_offsets[c]; i < b->ref_offsets[c + 1]; i++) r.push(b->ref_chars[i], b->ref_counts[i]);
+        s->drafts.push_back(r);
+    }
+    s->chunkReads.assign(b->chunk_reads, b->chunk_reads + b->n_chunks + 1);
+    s->haveAnchors = b->anchor_offsets != nullptr;
+    for (int64_t r = 0; r < nReads; r++) {
+        Rle rr;
+        for (int64_t i = b->read_offsets[r]; i < b->read_offsets[r + 1]; i++) {
+            if (b->read_counts[i] == 0) {
+                delete s;
+                return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_create: read %lld has a zero run length", (long long) r);
+            }
+            rr.push(b->read_chars[i], b->read_counts[i]);
+        }
+        s->reads.push_back(rr);
+        s->strand.push_back(b->strand[r]);
+        std::vector<Anchor> a;
+        if (s->haveAnchors)
+            for (int64_t k = b->anchor_offsets[r]; k < b->anchor_offsets[r + 1]; k++)
+                a.push_back(Anchor{b->anchors[3 * k], b->anchors[3 * k + 1], b->anchors[3 * k + 2]});
+        s->initialAnchors.push_back(a);
+    }
+    s->iterations.assign(s->nChunks, 0);
+    *out = s;
+    return MP_OK;
+}
+
+extern "C" void mp_poa_set_destroy(mp_poa_set *s) {
+    delete s;
+}
+
+extern "C" mp_status mp_poa_set_realign(mp_poa_set *s) {
+    if (!s) return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_realign: NULL set");
+    std::vector<int64_t> all(s->nChunks);
+    for (int64_t c = 0; c < s->nChunks; c++) all[c] = c;
+    std::vector<Poa> out(s->nChunks);
+    MP_TRY(realignChunks(s, all, s->drafts, s->haveAnchors ? &s->initialAnchors : nullptr, out));
+    s->poas = std::move(out);
+    return MP_OK;
+}
+
+extern "C" mp_status mp_poa_set_realign_pairs(mp_poa_set *s, const int64_t *const pair_offsets[3],
+                                              const int64_t *const pairs[3]) {
+    if (!s || !pair_offsets || !pairs) return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_realign_pairs: NULL argument");
+    for (int k = 0; k < 3; k++)
+        if (!pair_offsets[k] || (!pairs[k] && pair_offsets[k][s->reads.size()] > 0))
+            return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_realign_pairs: list %d missing", k);
+    // every pair must name a cell of its chunk's draft and read
+    for (int64_t c = 0; c < s->nChunks; c++)
+        for (int64_t r = s->chunkReads[c]; r < s->chunkReads[c + 1]; r++)
+            for (int k = 0; k < 3; k++)
+                for (int64_t t = pair_offsets[k][r]; t < pair_offsets[k][r + 1]; t++) {
+                    const int64_t x = pairs[k][3 * t + 1], y = pairs[k][3 * t + 2];
+                    const bool okX = k == 2 ? (x >= -1 && x < s->drafts[c].length()) : (x >= 0 && x < s->drafts[c].length());
+                    const bool okY = k == 1 ? (y >= -1 && y < s->reads[r].length()) : (y >= 0 && y < s->reads[r].length());
+                    if (!okX || !okY || pairs[k][3 * t] < 0)
+                        return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_realign_pairs: read %lld list %d pair %lld outside the "
+                                       "draft / read", (long long) r, k, (long long) (t - pair_offsets[k][r]));
+                }
+    std::vector<int64_t> all(s->nChunks);
+    for (int64_t c = 0; c < s->nChunks; c++) all[c] = c;
+    std::vector<Poa> out(s->nChunks);
+    const uint64_t maxRC = s->useRle ? (uint64_t) s->rm.M : 2;
+    forChunks(all, [&](int64_t c) {
+        Poa poa = Poa::fromReference(s->drafts[c], maxRC);
+        for (int64_t r = s->chunkReads[c]; r < s->chunkReads[c + 1]; r++) {
+            std::vector<Pair> lists[3];
+            for (int k = 0; k < 3; k++)
+                for (int64_t t = pair_offsets[k][r]; t < pair_offsets[k][r + 1]; t++)
+                    lists[k].push_back(Pair{pairs[k][3 * t], pairs[k][3 * t + 1], pairs[k][3 * t + 2]});
+            augment(poa, s->reads[r], s->strand[r] != 0, r - s->chunkReads[c], lists[0], lists[2], lists[1], s->cmpRC);
+        }
+        out[c] = std::move(poa);
+    });
+    s->poas = std::move(out);
+    return MP_OK;
+}
+
+extern "C" mp_status mp_poa_set_iterate(mp_poa_set *s) {
+    if (!s) return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_iterate: NULL set");
+    if (s->poas.empty()) return mp_fail(MP_ERR_STATE, "mp_poa_set_iterate: realign first");
+    return iterate(s);
+}
+
+extern "C" mp_status mp_poa_set_realign_all(mp_poa_set *s) {
+    MP_TRY(mp_poa_set_realign(s));
+    return mp_poa_set_iterate(s);
+}
+
+extern "C" mp_status mp_poa_set_estimate_repeat_counts(mp_poa_set *s) {
+    if (!s) return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_estimate_repeat_counts: NULL set");
+    if (s->poas.empty()) return mp_fail(MP_ERR_STATE, "mp_poa_set_estimate_repeat_counts: realign first");
+    if (!s->useRle) return MP_OK;
+    std::vector<int64_t> all(s->nChunks);
+    for (int64_t c = 0; c < s->nChunks; c++) all[c] = c;
+    forChunks(all, [&](int64_t c) { estimateRepeatCounts(s->poas[c], s->reads, s->strand, s->chunkReads[c], s->rm); });
+    return MP_OK;
+}
+
+extern "C" mp_status mp_poa_info(const mp_poa_set *s, int64_t chunk, mp_poa_chunk_info *info) {
+    MP_TRY(chunkCheck(s, chunk));
+    if (!info) return mp_fail(MP_ERR_ARGUMENT, "mp_poa_info: NULL info");
+    const Poa &poa = s->poas[chunk];
+    memset(info, 0, sizeof(*info));
+    info->nodes = (int64_t) poa.nodes.size();
+    info->max_repeat = (int64_t) poa.maxRC;
+    info->reference_runs = poa.ref.length();
+    for (const Node &n : poa.nodes) {
+        info->observations += (int64_t) n.obs.size();
+        info->inserts += (int64_t) n.ins.size();
+        info->deletes += (int64_t) n.del.size();
+        for (const Insert &e : n.ins) info->insert_runs += e.s.length();
+    }
+    info->score = score(poa);
+    info->iterations = s->iterations[chunk];
+    return MP_OK;
+}
+
+extern "C" mp_status mp_poa_nodes(const mp_poa_set *s, int64_t chunk, char *bases, uint64_t *repeat_counts,
+                                  double *base_weights, double *repeat_count_weights, int64_t *n_obs, int64_t *n_ins,
+                                  int64_t *n_del) {
+    MP_TRY(chunkCheck(s, chunk));
+    const Poa &poa = s->poas[chunk];
+    const int64_t M = (int64_t) poa.maxRC;
+    for (size_t i = 0; i < poa.nodes.size(); i++) {
+        const Node &n = poa.nodes[i];
+        if (bases) bases[i] = n.base;
+        if (repeat_counts) repeat_counts[i] = n.rc;
+        if (base_weights)
+            for (int k = 0; k < 5; k++) base_weights[5 * i + k] = n.bw[k];
+        if (repeat_count_weights)
+            for (int64_t k = 0; k < M; k++) repeat_count_weights[M * i + k] = n.rcw[k];
+        if (n_obs) n_obs[i] = (int64_t) n.obs.size();
+        if (n_ins) n_ins[i] = (int64_t) n.ins.size();
+        if (n_del) n_del[i] = (int64_t) n.del.size();
+    }
+    return MP_OK;
+}
+
+extern "C" mp_status mp_poa_observations(const mp_poa_set *s, int64_t chunk, int64_t *read, int64_t *offset,
+                                         double *weight) {
+    MP_TRY(chunkCheck(s, chunk));
+    int64_t k = 0;
+    for (const Node &n : s->poas[chunk].nodes)
+        for (const Obs &o : n.obs) {
+            read[k] = o.read;
+            offset[k] = o.offset;
+            weight[k++] = o.weight;
+        }
+    return MP_OK;
+}
+
+extern "C" mp_status mp_poa_inserts(const mp_poa_set *s, int64_t chunk, double *weight_fwd, double *weight_rev,
+                                    int64_t *lengths, char *chars, uint64_t *counts, int64_t *n_obs) {
+    MP_TRY(chunkCheck(s, chunk));
+    int64_t k = 0, runs = 0;
+    for (const Node &n : s->poas[chunk].nodes)
+        for (const Insert &e : n.ins) {
+            weight_fwd[k] = e.wF;
+            weight_rev[k] = e.wR;
+            lengths[k] = e.s.length();
+            n_obs[k] = (int64_t) e.obs.size();
+            for (int64_t r = 0; r < e.s.length(); r++) {
+                chars[runs + r] = e.s.c[r];
+                counts[runs + r] = e.s.n[r];
+            }
+            runs += e.s.length();
+            k++;
+        }
+    return MP_OK;
+}
+
+extern "C" mp_status mp_poa_deletes(const mp_poa_set *s, int64_t chunk, int64_t *lengths, double *weight_fwd,
+                                    double *weight_rev, int64_t *n_obs) {
+    MP_TRY(chunkCheck(s, chunk));
+    int64_t k = 0;
+    for (const Node &n : s->poas[chunk].nodes)
+        for (const Delete &e : n.del) {
+            lengths[k] = e.len;
+            weight_fwd[k] = e.wF;
+            weight_rev[k] = e.wR;
+            n_obs[k++] = (int64_t) e.obs.size();
+        }
+    return MP_OK;
+}
+
+extern "C" mp_status mp_poa_reference(const mp_poa_set *s, int64_t chunk, char *chars, uint64_t *counts) {
+    MP_TRY(chunkCheck(s, chunk));
+    const Rle &r = s->poas[chunk].ref;
+    for (int64_t i = 0; i < r.length(); i++) {
+        chars[i] = r.c[i];
+        counts[i] = r.n[i];
+    }
+    return MP_OK;
+}
+
+extern "C" mp_status mp_poa_consensus(const mp_poa_set *s, int64_t chunk, char *chars, uint64_t *counts, int64_t cap,
+                                      int64_t *n_runs, int64_t *map) {
+    MP_TRY(chunkCheck(s, chunk));
+    std::vector<int64_t> mp;
+    const Rle c = consensus(s->poas[chunk], mp, s->penalty, s->useRle);
+    if (n_runs) *n_runs = c.length();
+    if (c.length() > cap) return mp_fail(MP_ERR_OVERFLOW, "mp_poa_consensus: %lld runs exceed the capacity %lld",
+                                         (long long) c.length(), (long long) cap);
+    for (int64_t i = 0; i < c.length(); i++) {
+        if (chars) chars[i] = c.c[i];
+        if (counts) counts[i] = c.n[i];
+    }
+    if (map)
+        for (size_t i = 0; i < mp.size(); i++) map[i] = mp[i];
+    return MP_OK;
+}
+
+extern "C" mp_status mp_poa_anchor_alignments(const mp_poa_set *s, int64_t chunk, const int64_t *map,
+                                              int64_t *offsets, int64_t *triples, int64_t cap, int64_t *n_anchors) {
+    MP_TRY(chunkCheck(s, chunk));
+    const int64_t nR = s->chunkReads[chunk + 1] - s->chunkReads[chunk];
+    std::vector<int64_t> mv;
+    if (map) mv.assign(map, map + (s->poas[chunk].nodes.size() - 1));
+    auto a = anchorAlignments(s->poas[chunk], map ? &mv : nullptr, nR, s->anchorProbs);
+    int64_t k = 0;
+    offsets[0] = 0;
+    for (int64_t r = 0; r < nR; r++) {
+        for (const Anchor &t : a[r]) {
+            if (k < cap) {
+                triples[3 * k] = t.x;
+                triples[3 * k + 1] = t.y;
+                triples[3 * k + 2] = t.e;
+            }
+            k++;
+        }
+        offsets[r + 1] = k;
+    }
+    if (n_anchors) *n_anchors = k;
+    if (k > cap) return mp_fail(MP_ERR_OVERFLOW, "mp_poa_anchor_alignments: %lld anchors exceed the capacity",
+                                (long long) k);
+    return MP_OK;
+}

@@ -1,0 +1,260 @@
+"""Host-side interface of the POA loop (impl/polisher.c), mirroring the reference's
+operator API over the library's C ABI (mp_poa_set_*):
+
+* ``PoaSet.realign``        -- poa_realign (:656-703) of every chunk (one GPU batch);
+* ``PoaSet.realign_pairs``  -- poa_augment (:316-534) with aligned pairs from the caller;
+* ``PoaSet.consensus``      -- poa_getConsensus (:1025-1275);
+* ``PoaSet.anchor_alignments`` -- poa_getAnchorAlignments (:536-592);
+* ``PoaSet.estimate_repeat_counts`` -- poa_estimateRepeatCountsUsingBayesianModel (:1556-1565);
+* ``PoaSet.iterate`` / ``realign_all`` -- poa_realignIterative / poa_realignAll in
+  consensus mode (:2034-2129);
+* ``polish`` -- the whole loop for many chunks, returning each chunk's polished draft.
+
+Weights, observations and indels can be read back for every chunk, with the layouts of
+the reference's Poa structures (inc/margin.h:592-627).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import c_char, c_double, c_int32, c_int64, c_uint8, c_uint32, c_void_p
+from .params import AlignmentParams, PolishModel
+from .realign import Engine, Model
+from .rle import RleString
+
+c_uint64 = ctypes.c_uint64
+
+
+@dataclass
+class PolishParams:
+    """The POA fields of PolishParams (inc/margin.h:534-580); defaults are the shipped
+    params/allParams.np.json values except max_iterations (0 there: consensus mode off)."""
+    reference_base_penalty: float = 0.5
+    compare_repeat_counts: bool = True
+    use_run_length: bool = True
+    anchor_probs: Sequence[float] = (0.9, 10, 0.95, 4, 0.99, 0)
+    min_iterations: int = 0
+    max_iterations: int = 5
+
+    def struct(self):
+        probs = np.ascontiguousarray(self.anchor_probs, dtype=np.float64)
+        p = _lib.PolishParamsC(float(self.reference_base_penalty), 1 if self.compare_repeat_counts else 0,
+                               1 if self.use_run_length else 0, _lib.ptr(probs, c_double), probs.size,
+                               int(self.min_iterations), int(self.max_iterations))
+        return p, probs
+
+
+def _flat_rle(strings: Sequence[RleString]):
+    offs = np.zeros(len(strings) + 1, dtype=np.int64)
+    offs[1:] = np.cumsum([len(s) for s in strings])
+    chars = b"".join(s.chars for s in strings)
+    counts = (np.concatenate([np.asarray(s.counts, dtype=np.uint32) for s in strings])
+              if strings else np.zeros(0, np.uint32))
+    return offs, chars, np.ascontiguousarray(counts, dtype=np.uint32)
+
+
+class PoaSet:
+    """Chunks (a draft and its reads each) polished together; see mp_poa_set_create. engine
+    and model may be None for a set fed with realign_pairs (host-side steps only)."""
+
+    def __init__(self, engine: Engine, model: Model, params: AlignmentParams, polish: PolishParams,
+                 drafts: Sequence[RleString], reads: Sequence[Sequence[RleString]], strands: Sequence[Sequence[int]],
+                 anchors: Optional[Sequence[Sequence[np.ndarray]]] = None, repeat_log10: Optional[np.ndarray] = None):
+        self.engine, self.model = engine, model
+        self._lib = engine._lib if engine is not None else _lib.load()
+        self.n_chunks = len(drafts)
+        flat_reads = [r for lst in reads for r in lst]
+        self.reads_per_chunk = [len(lst) for lst in reads]
+        ref_off, ref_chars, ref_counts = _flat_rle(list(drafts))
+        rd_off, rd_chars, rd_counts = _flat_rle(flat_reads)
+        chunk_reads = np.zeros(self.n_chunks + 1, dtype=np.int64)
+        chunk_reads[1:] = np.cumsum(self.reads_per_chunk)
+        strand = np.ascontiguousarray([int(s) for lst in strands for s in lst], dtype=np.uint8)
+        if strand.size != len(flat_reads):
+            raise ValueError("one strand per read")
+        keep = [ref_off, ref_counts, rd_off, rd_counts, chunk_reads, strand]
+        b = _lib.PolishBatch()
+        b.n_chunks = self.n_chunks
+        b.ref_offsets = _lib.ptr(ref_off, c_int64)
+        self._ref_chars = ctypes.create_string_buffer(ref_chars or b"\0", max(len(ref_chars), 1))
+        b.ref_chars = ctypes.cast(self._ref_chars, ctypes.POINTER(c_char))
+        b.ref_counts = _lib.ptr(ref_counts if ref_counts.size else np.zeros(1, np.uint32), c_uint32)
+        b.chunk_reads = _lib.ptr(chunk_reads, c_int64)
+        b.read_offsets = _lib.ptr(rd_off, c_int64)
+        self._rd_chars = ctypes.create_string_buffer(rd_chars or b"\0", max(len(rd_chars), 1))
+        b.read_chars = ctypes.cast(self._rd_chars, ctypes.POINTER(c_char))
+        b.read_counts = _lib.ptr(rd_counts if rd_counts.size else np.zeros(1, np.uint32), c_uint32)
+        b.strand = _lib.ptr(strand if strand.size else np.zeros(1, np.uint8), c_uint8)
+        if anchors is not None:
+            flat_a = [np.asarray(a, dtype=np.int32).reshape(-1, 3) for lst in anchors for a in lst]
+            a_off = np.zeros(len(flat_a) + 1, dtype=np.int64)
+            a_off[1:] = np.cumsum([a.shape[0] for a in flat_a])
+            a_all = np.ascontiguousarray(np.concatenate(flat_a) if flat_a else np.zeros((1, 3), np.int32))
+            keep += [a_off, a_all]
+            b.anchor_offsets = _lib.ptr(a_off, c_int64)
+            b.anchors = _lib.ptr(a_all, c_int32)
+        pp, probs = polish.struct()
+        keep.append(probs)
+        ps = params.struct()
+        rep = None
+        if repeat_log10 is not None:
+            rep = np.ascontiguousarray(repeat_log10, dtype=np.float64).reshape(-1)
+            keep.append(rep)
+        self._keep = keep
+        h = c_void_p()
+        _lib.check(self._lib.mp_poa_set_create(engine.handle if engine is not None else None,
+                                               model.handle if model is not None else None, ctypes.byref(ps),
+                                               ctypes.byref(pp), ctypes.byref(b), _lib.ptr(rep, c_double),
+                                               ctypes.byref(h)))
+        self.handle = h
+
+    @classmethod
+    def from_polish_model(cls, engine, model, pm: PolishModel, polish: PolishParams, drafts, reads, strands,
+                          anchors=None) -> "PoaSet":
+        return cls(engine, model, pm.alignment, polish, drafts, reads, strands, anchors,
+                   pm.repeat_log10 if polish.use_run_length else None)
+
+    # ---- the loop's steps ----
+    def realign(self) -> None:
+        _lib.check(self._lib.mp_poa_set_realign(self.handle))
+
+    def realign_pairs(self, pairs: Sequence[Sequence[np.ndarray]]) -> None:
+        """poa_augment with caller pairs: pairs[r] = (matches, gap_x, gap_y) of read r (all
+        chunks' reads in order), each (n, 3) int arrays of (weight, x, y)."""
+        offs, arrs, keep = [], [], []
+        for k in range(3):
+            lists = [np.asarray(p[k], dtype=np.int64).reshape(-1, 3) for p in pairs]
+            o = np.zeros(len(lists) + 1, dtype=np.int64)
+            o[1:] = np.cumsum([a.shape[0] for a in lists])
+            a = np.ascontiguousarray(np.concatenate(lists) if lists else np.zeros((1, 3), np.int64))
+            if a.size == 0:
+                a = np.zeros((1, 3), np.int64)
+            keep += [o, a]
+            offs.append(_lib.ptr(o, c_int64))
+            arrs.append(_lib.ptr(a, c_int64))
+        po = (ctypes.POINTER(c_int64) * 3)(*offs)
+        pa = (ctypes.POINTER(c_int64) * 3)(*arrs)
+        _lib.check(self._lib.mp_poa_set_realign_pairs(self.handle, po, pa))
+
+    def iterate(self) -> None:
+        _lib.check(self._lib.mp_poa_set_iterate(self.handle))
+
+    def realign_all(self) -> None:
+        _lib.check(self._lib.mp_poa_set_realign_all(self.handle))
+
+    def estimate_repeat_counts(self) -> None:
+        _lib.check(self._lib.mp_poa_set_estimate_repeat_counts(self.handle))
+
+    # ---- inspection ----
+    def info(self, chunk: int) -> dict:
+        i = _lib.PoaChunkInfo()
+        _lib.check(self._lib.mp_poa_info(self.handle, chunk, ctypes.byref(i)))
+        return {f: getattr(i, f) for f, _ in _lib.PoaChunkInfo._fields_}
+
+    def nodes(self, chunk: int) -> dict:
+        inf = self.info(chunk)
+        n, m = inf["nodes"], inf["max_repeat"]
+        bases = (c_char * max(n, 1))()
+        rc = np.zeros(n, np.uint64)
+        bw = np.zeros((n, 5))
+        rcw = np.zeros((n, m))
+        no, ni, nd = (np.zeros(n, np.int64) for _ in range(3))
+        _lib.check(self._lib.mp_poa_nodes(self.handle, chunk, bases, _lib.ptr(rc, c_uint64), _lib.ptr(bw, c_double),
+                                          _lib.ptr(rcw, c_double), _lib.ptr(no, c_int64), _lib.ptr(ni, c_int64),
+                                          _lib.ptr(nd, c_int64)))
+        return {"bases": bytes(bases[:n]), "repeat_counts": rc, "base_weights": bw, "repeat_count_weights": rcw,
+                "n_obs": no, "n_ins": ni, "n_del": nd}
+
+    def observations(self, chunk: int) -> np.ndarray:
+        k = self.info(chunk)["observations"]
+        r, o, w = np.zeros(k, np.int64), np.zeros(k, np.int64), np.zeros(k)
+        _lib.check(self._lib.mp_poa_observations(self.handle, chunk, _lib.ptr(r, c_int64), _lib.ptr(o, c_int64),
+                                                 _lib.ptr(w, c_double)))
+        return np.stack([r, o, w], axis=1) if k else np.zeros((0, 3))
+
+    def inserts(self, chunk: int) -> list:
+        inf = self.info(chunk)
+        k, runs = inf["inserts"], inf["insert_runs"]
+        wf, wr = np.zeros(k), np.zeros(k)
+        ln, no = np.zeros(k, np.int64), np.zeros(k, np.int64)
+        chars = (c_char * max(runs, 1))()
+        counts = np.zeros(max(runs, 1), np.uint64)
+        _lib.check(self._lib.mp_poa_inserts(self.handle, chunk, _lib.ptr(wf, c_double), _lib.ptr(wr, c_double),
+                                            _lib.ptr(ln, c_int64), chars, _lib.ptr(counts, c_uint64),
+                                            _lib.ptr(no, c_int64)))
+        out, at = [], 0
+        raw = bytes(chars[:runs])
+        for i in range(k):
+            out.append((raw[at:at + ln[i]], tuple(int(v) for v in counts[at:at + ln[i]]), float(wf[i]), float(wr[i]),
+                        int(no[i])))
+            at += int(ln[i])
+        return out
+
+    def deletes(self, chunk: int) -> list:
+        k = self.info(chunk)["deletes"]
+        ln, no = np.zeros(k, np.int64), np.zeros(k, np.int64)
+        wf, wr = np.zeros(k), np.zeros(k)
+        _lib.check(self._lib.mp_poa_deletes(self.handle, chunk, _lib.ptr(ln, c_int64), _lib.ptr(wf, c_double),
+                                            _lib.ptr(wr, c_double), _lib.ptr(no, c_int64)))
+        return [(int(ln[i]), float(wf[i]), float(wr[i]), int(no[i])) for i in range(k)]
+
+    def reference(self, chunk: int) -> RleString:
+        n = self.info(chunk)["reference_runs"]
+        chars = (c_char * max(n, 1))()
+        counts = np.zeros(max(n, 1), np.uint64)
+        _lib.check(self._lib.mp_poa_reference(self.handle, chunk, chars, _lib.ptr(counts, c_uint64)))
+        return RleString(bytes(chars[:n]), counts[:n].astype(np.uint32))
+
+    def consensus(self, chunk: int):
+        """(consensus RleString, node-to-consensus map)."""
+        inf = self.info(chunk)
+        cap = 4 * inf["nodes"] + 16 * (inf["insert_runs"] + 1)
+        chars = (c_char * cap)()
+        counts = np.zeros(cap, np.uint64)
+        n = c_int64(0)
+        m = np.zeros(max(inf["nodes"] - 1, 1), np.int64)
+        _lib.check(self._lib.mp_poa_consensus(self.handle, chunk, chars, _lib.ptr(counts, c_uint64), cap, n,
+                                              _lib.ptr(m, c_int64)))
+        return RleString(bytes(chars[:n.value]), counts[:n.value].astype(np.uint32)), m[:inf["nodes"] - 1].copy()
+
+    def anchor_alignments(self, chunk: int, node_map: Optional[np.ndarray] = None) -> List[np.ndarray]:
+        nr = self.reads_per_chunk[chunk]
+        inf = self.info(chunk)
+        cap = inf["observations"] + 1
+        offs = np.zeros(nr + 1, np.int64)
+        tri = np.zeros((cap, 3), np.int64)
+        n = c_int64(0)
+        mp = None if node_map is None else np.ascontiguousarray(node_map, dtype=np.int64)
+        _lib.check(self._lib.mp_poa_anchor_alignments(self.handle, chunk, _lib.ptr(mp, c_int64),
+                                                      _lib.ptr(offs, c_int64), _lib.ptr(tri, c_int64), cap, n))
+        return [tri[offs[r]:offs[r + 1]].copy() for r in range(nr)]
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self._lib.mp_poa_set_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def polish(engine: Engine, model: Model, pm: PolishModel, polish_params: PolishParams, drafts, reads, strands,
+           anchors=None) -> List[RleString]:
+    """poa_realignAll in consensus mode for every chunk, then the run-length estimate the
+    caller applies to the result (marginPolish.c:558): each chunk's polished draft."""
+    s = PoaSet.from_polish_model(engine, model, pm, polish_params, drafts, reads, strands, anchors)
+    try:
+        s.realign_all()
+        if polish_params.use_run_length:
+            s.estimate_repeat_counts()
+        return [s.reference(c) for c in range(s.n_chunks)]
+    finally:
+        s.close()

@@ -209,5 +209,98 @@ def config_adjoint(seed: int = 4, n_reads: int = 512, n_templates: int = 64, tem
                           {"reads": n_reads, "templates": n_templates, "half_width": half_width})
 
 
+def draft_with_errors(rng: np.random.Generator, truth: np.ndarray, rate: float = 0.01, hp_bias: float = 0.7):
+    """A draft assembly: the truth with indels at `rate` per base, a fraction hp_bias of them
+    lengthening or shortening a homopolymer run by one base, the rest single-base indels
+    at random positions. Returns (draft bytes, base pairs (truth index, draft index))."""
+    n = truth.size
+    brk = np.nonzero(truth[1:] != truth[:-1])[0] + 1
+    starts = np.concatenate([[0], brk])
+    counts = np.diff(np.concatenate([starts, [n]]))
+    n_err = int(rng.binomial(n, rate))
+    ops = {}  # truth index -> 'd' (drop) or inserted base (insert after)
+    long_runs = starts[counts >= 2]
+    for _ in range(n_err):
+        if rng.random() < hp_bias and long_runs.size:
+            st = int(rng.choice(long_runs))
+            ops[st] = "d" if rng.random() < 0.5 else truth[st]
+        else:
+            i = int(rng.integers(0, n))
+            ops[i] = "d" if rng.random() < 0.5 else BASES[int(rng.integers(0, 4))]
+    out, pairs = [], []
+    for i in range(n):
+        op = ops.get(i)
+        if op == "d":
+            continue
+        pairs.append((i, len(out)))
+        out.append(truth[i])
+        if op is not None:
+            out.append(op)
+    return np.array(out, dtype=np.uint8), np.array(pairs, dtype=np.int64).reshape(-1, 2)
+
+
+@dataclass
+class PolishWorkload:
+    """Chunks for the POA loop: per chunk the truth, the draft (RLE) and the reads (RLE, strand,
+    anchors against the draft in RLE coordinates)."""
+    truths: List[RleString]
+    drafts: List[RleString]
+    reads: List[List[RleString]]
+    strands: List[List[int]]
+    anchors: List[List[np.ndarray]]
+    meta: dict = field(default_factory=dict)
+
+
+def config_polish(seed: int = 3, n_chunks: int = 1, chunk_len: int = 2000, coverage: float = 20.0,
+                  read_len=(1500, 2000), half_width: int = 25, draft_error: float = 0.01,
+                  hp_runs: bool = False) -> PolishWorkload:
+    """Polishing chunks: truth templates, drafts = truth with 1% homopolymer-biased indels,
+    reads sampled from the truth with the nanopore-like error model, anchors from the reads'
+    truth alignment carried through the truth-to-draft map (every aligned base, expansion
+    2 * half_width, then run-length encoded as CIGAR anchors are)."""
+    rng = np.random.default_rng(seed)
+    em = ErrorModel()
+    truths, drafts, reads, strands, anchors = [], [], [], [], []
+    for _ in range(n_chunks):
+        t = random_template(rng, chunk_len, gc=0.41 if hp_runs else 0.5, run_p=0.55 if hp_runs else None)
+        d, t2d = draft_with_errors(rng, t, draft_error)
+        tmap = np.full(t.size, -1, dtype=np.int64)
+        tmap[t2d[:, 0]] = t2d[:, 1]
+        drle = RleString.from_string(d.tobytes())
+        n_reads = max(1, int(round(coverage * chunk_len / float(np.mean(read_len)))))
+        # reads overhang the chunk ends and are clipped to it (as the chunker clips alignments),
+        # so the coverage is even up to the chunk's ends
+        lst = []
+        for _ in range(n_reads):
+            ln = int(rng.integers(read_len[0], read_len[1] + 1))
+            start = int(rng.integers(-ln // 2, t.size - ln // 2))
+            a, b = max(0, start), min(t.size, start + ln)
+            if b - a < 64:
+                continue
+            read, pairs = mutate_read(rng, t[a:b], em)
+            pairs[:, 0] += a
+            lst.append((read, pairs, int(rng.integers(0, 2))))
+        cr, cs, ca = [], [], []
+        for read, pairs, s in lst:
+            r = RleString.from_string(read.tobytes())
+            dp = tmap[pairs[:, 0]]
+            ok = dp >= 0
+            p = np.stack([dp[ok], pairs[ok, 1], np.full(int(ok.sum()), 2 * half_width)], axis=1)
+            a = rle_anchors(p, drle, r)
+            if a.shape[0] == 0 or len(r) == 0:
+                continue
+            cr.append(r)
+            cs.append(s)
+            ca.append(a)
+        truths.append(RleString.from_string(t.tobytes()))
+        drafts.append(drle)
+        reads.append(cr)
+        strands.append(cs)
+        anchors.append(ca)
+    return PolishWorkload(truths, drafts, reads, strands, anchors,
+                          {"chunks": n_chunks, "chunk_bp": chunk_len, "coverage": coverage, "half_width": half_width,
+                           "draft_error": draft_error})
+
+
 def config_by_name(name: str, **kw) -> Workload:
     return {"small": config_small, "batched": config_batched, "adjoint": config_adjoint}[name](**kw)

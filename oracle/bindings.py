@@ -359,3 +359,214 @@ class ExactOracle:
         return lp, {"transitions": out[0:9].copy(), "match": out[9:34].copy(), "gap_x": out[34:39].copy(),
                     "gap_y": out[39:44].copy(), "start": out[44:47].copy(), "end": out[47:50].copy(),
                     "repeat": out[50:].copy()}
+
+
+REF_POA_LIB = os.path.join(HERE, "_ref", "libref_poa.so")
+
+
+def available_reference_poa() -> bool:
+    return os.path.exists(REF_POA_LIB)
+
+
+class RefPoaOracle:
+    """The reference's own POA steps (impl/polisher.c compiled unmodified, oracle/_ref/libref_poa.so):
+    poa_realign, poa_getConsensus, poa_getAnchorAlignments, the run-length estimate and
+    poa_realignAll in consensus mode."""
+
+    def __init__(self):
+        if not os.path.exists(REF_POA_LIB):
+            raise FileNotFoundError(f"{REF_POA_LIB} missing: build with `make -C oracle reference`")
+        lib = ctypes.CDLL(REF_POA_LIB)
+        P = POINTER
+        from ctypes import c_char, c_char_p, c_uint32, c_uint64
+        self._c_char, self._c_uint64 = c_char, c_uint64
+        lib.refo_model_create.restype = c_void_p
+        lib.refo_model_create.argtypes = [c_int, P(c_double), P(c_double), c_int, P(c_double), c_int]
+        lib.refo_model_destroy.argtypes = [c_void_p]
+        lib.refo_align_with_indels.restype = P(_Pairs)
+        lib.refo_align_with_indels.argtypes = [c_void_p, P(c_uint16), c_int64, P(c_uint16), c_int64, P(c_int64),
+                                               c_int64, P(OracleParams), c_int, c_int]
+        lib.refo_pairs_free.argtypes = [P(_Pairs)]
+        lib.refpoa_params_create.restype = c_void_p
+        lib.refpoa_params_create.argtypes = [c_void_p, c_void_p, P(OracleParams), c_int, c_double, c_int, P(c_double),
+                                             c_int64, c_int64, c_int64]
+        lib.refpoa_params_destroy.argtypes = [c_void_p]
+        lib.refpoa_reads_create.restype = c_void_p
+        lib.refpoa_reads_create.argtypes = [c_int64, c_char_p, P(c_uint32), P(c_int64), P(c_uint8)]
+        lib.refpoa_reads_destroy.argtypes = [c_void_p]
+        lib.refpoa_anchors_create.restype = c_void_p
+        lib.refpoa_anchors_create.argtypes = [c_int64, P(c_int64), P(c_int64)]
+        lib.refpoa_anchors_destroy.argtypes = [c_void_p]
+        for f in ("refpoa_realign", "refpoa_realign_all"):
+            getattr(lib, f).restype = c_void_p
+            getattr(lib, f).argtypes = [c_void_p, c_void_p, c_char_p, P(c_uint32), c_int64, c_void_p]
+        lib.refpoa_destroy.argtypes = [c_void_p]
+        lib.refpoa_estimate_repeat_counts.argtypes = [c_void_p, c_void_p, c_void_p]
+        lib.refpoa_score.restype = c_double
+        lib.refpoa_score.argtypes = [c_void_p]
+        lib.refpoa_reference.restype = c_int64
+        lib.refpoa_reference.argtypes = [c_void_p, P(c_char), P(c_uint64), c_int64]
+        lib.refpoa_node_count.restype = c_int64
+        lib.refpoa_node_count.argtypes = [c_void_p]
+        lib.refpoa_max_repeat.restype = c_int64
+        lib.refpoa_max_repeat.argtypes = [c_void_p]
+        lib.refpoa_nodes.argtypes = [c_void_p, P(c_char), P(c_uint64), P(c_double), P(c_double), P(c_int64),
+                                     P(c_int64), P(c_int64)]
+        lib.refpoa_observations.argtypes = [c_void_p, P(c_int64), P(c_int64), P(c_double)]
+        lib.refpoa_inserts.restype = c_int64
+        lib.refpoa_inserts.argtypes = [c_void_p, P(c_double), P(c_double), P(c_int64), P(c_char), P(c_uint64),
+                                       P(c_int64)]
+        lib.refpoa_deletes.argtypes = [c_void_p, P(c_int64), P(c_double), P(c_double), P(c_int64)]
+        lib.refpoa_consensus.restype = c_int64
+        lib.refpoa_consensus.argtypes = [c_void_p, c_void_p, P(c_char), P(c_uint64), c_int64, P(c_int64)]
+        lib.refpoa_anchor_alignments.restype = c_int64
+        lib.refpoa_anchor_alignments.argtypes = [c_void_p, P(c_int64), c_int64, c_void_p, P(c_int64), P(c_int64),
+                                                 c_int64]
+        self.lib = lib
+
+    # ---- construction ----
+    def model(self, hmm_type, transitions, emissions, reverse_complement, repeat_log10=None, strand=1):
+        t = np.ascontiguousarray(transitions, dtype=np.float64)
+        e = np.ascontiguousarray(emissions, dtype=np.float64)
+        r = None if repeat_log10 is None else np.ascontiguousarray(repeat_log10, dtype=np.float64).reshape(-1)
+        return self.lib.refo_model_create(hmm_type, _p(t, c_double), _p(e, c_double), 1 if reverse_complement else 0,
+                                          _p(r, c_double), 1 if strand else 0)
+
+    def free_model(self, h):
+        self.lib.refo_model_destroy(h)
+
+    def params(self, hf, hr, alignment, use_rle=True, penalty=0.5, compare_repeat_counts=True,
+               anchor_probs=(0.9, 10, 0.95, 4, 0.99, 0), min_iterations=0, max_iterations=5):
+        op = OracleParams.from_alignment(alignment)
+        pr = np.ascontiguousarray(anchor_probs, dtype=np.float64)
+        return self.lib.refpoa_params_create(hf, hr, ctypes.byref(op), int(use_rle), float(penalty),
+                                             int(compare_repeat_counts), _p(pr, c_double), pr.size, int(min_iterations),
+                                             int(max_iterations))
+
+    def free_params(self, h):
+        self.lib.refpoa_params_destroy(h)
+
+    def reads(self, rle_reads, strands):
+        from ctypes import c_uint32
+        off = np.zeros(len(rle_reads) + 1, np.int64)
+        off[1:] = np.cumsum([len(r) for r in rle_reads])
+        chars = b"".join(r.chars for r in rle_reads) or b"\0"
+        counts = np.ascontiguousarray(np.concatenate([np.asarray(r.counts, np.uint32) for r in rle_reads])
+                                      if rle_reads else np.zeros(1, np.uint32), dtype=np.uint32)
+        st = np.ascontiguousarray(strands, dtype=np.uint8)
+        return self.lib.refpoa_reads_create(len(rle_reads), chars, _p(counts, c_uint32), _p(off, c_int64),
+                                            _p(st, c_uint8))
+
+    def free_reads(self, h):
+        self.lib.refpoa_reads_destroy(h)
+
+    def anchors(self, per_read):
+        lists = [np.asarray(a, dtype=np.int64).reshape(-1, 3) for a in per_read]
+        off = np.zeros(len(lists) + 1, np.int64)
+        off[1:] = np.cumsum([a.shape[0] for a in lists])
+        flat = np.ascontiguousarray(np.concatenate(lists) if lists and off[-1] else np.zeros((1, 3), np.int64))
+        return self.lib.refpoa_anchors_create(len(lists), _p(off, c_int64), _p(flat, c_int64))
+
+    def free_anchors(self, h):
+        self.lib.refpoa_anchors_destroy(h)
+
+    def align_with_indels(self, h, sx, sy, anchors, params):
+        """The reference aligner of this library (the one poa_realign calls)."""
+        sx = np.ascontiguousarray(sx, dtype=np.uint16)
+        sy = np.ascontiguousarray(sy, dtype=np.uint16)
+        a = np.ascontiguousarray(np.asarray(anchors, dtype=np.int64).reshape(-1, 3))
+        op = OracleParams.from_alignment(params)
+        r = self.lib.refo_align_with_indels(h, _p(sx, c_uint16), sx.size, _p(sy, c_uint16), sy.size, _p(a, c_int64),
+                                            a.shape[0], ctypes.byref(op), 0, 0)
+        out = tuple(_tuples(r.contents.t[k], r.contents.n[k]) for k in range(3))
+        self.lib.refo_pairs_free(r)
+        return out
+
+    # ---- the loop ----
+    def realign(self, reads_h, anchors_h, ref, params_h):
+        from ctypes import c_uint32
+        c = np.ascontiguousarray(ref.counts, dtype=np.uint32) if len(ref) else np.zeros(1, np.uint32)
+        return self.lib.refpoa_realign(reads_h, anchors_h, ref.chars or b"\0", _p(c, c_uint32), len(ref), params_h)
+
+    def realign_all(self, reads_h, anchors_h, ref, params_h):
+        from ctypes import c_uint32
+        c = np.ascontiguousarray(ref.counts, dtype=np.uint32) if len(ref) else np.zeros(1, np.uint32)
+        return self.lib.refpoa_realign_all(reads_h, anchors_h, ref.chars or b"\0", _p(c, c_uint32), len(ref),
+                                           params_h)
+
+    def free_poa(self, h):
+        self.lib.refpoa_destroy(h)
+
+    def estimate_repeat_counts(self, poa, reads_h, params_h):
+        self.lib.refpoa_estimate_repeat_counts(poa, reads_h, params_h)
+
+    def score(self, poa):
+        return self.lib.refpoa_score(poa)
+
+    def reference(self, poa):
+        n = self.lib.refpoa_reference(poa, None, None, 0)
+        chars = (self._c_char * max(n, 1))()
+        counts = np.zeros(max(n, 1), np.uint64)
+        self.lib.refpoa_reference(poa, chars, _p(counts, self._c_uint64), n)
+        return bytes(chars[:n]), counts[:n].copy()
+
+    def nodes(self, poa):
+        n = self.lib.refpoa_node_count(poa)
+        m = self.lib.refpoa_max_repeat(poa)
+        bases = (self._c_char * max(n, 1))()
+        rc = np.zeros(n, np.uint64)
+        bw = np.zeros((n, 5))
+        rcw = np.zeros((n, m))
+        no, ni, nd = (np.zeros(n, np.int64) for _ in range(3))
+        self.lib.refpoa_nodes(poa, bases, _p(rc, self._c_uint64), _p(bw, c_double), _p(rcw, c_double),
+                              _p(no, c_int64), _p(ni, c_int64), _p(nd, c_int64))
+        return {"bases": bytes(bases[:n]), "repeat_counts": rc, "base_weights": bw, "repeat_count_weights": rcw,
+                "n_obs": no, "n_ins": ni, "n_del": nd}
+
+    def observations(self, poa):
+        k = int(self.nodes(poa)["n_obs"].sum())
+        r, o, w = np.zeros(k, np.int64), np.zeros(k, np.int64), np.zeros(k)
+        self.lib.refpoa_observations(poa, _p(r, c_int64), _p(o, c_int64), _p(w, c_double))
+        return np.stack([r, o, w], axis=1) if k else np.zeros((0, 3))
+
+    def inserts(self, poa):
+        k = int(self.nodes(poa)["n_ins"].sum())
+        runs = self.lib.refpoa_inserts(poa, None, None, None, None, None, None)
+        wf, wr = np.zeros(max(k, 1)), np.zeros(max(k, 1))
+        ln, no = np.zeros(max(k, 1), np.int64), np.zeros(max(k, 1), np.int64)
+        chars = (self._c_char * max(runs, 1))()
+        counts = np.zeros(max(runs, 1), np.uint64)
+        self.lib.refpoa_inserts(poa, _p(wf, c_double), _p(wr, c_double), _p(ln, c_int64), chars,
+                                _p(counts, self._c_uint64), _p(no, c_int64))
+        out, at = [], 0
+        raw = bytes(chars[:runs])
+        for i in range(k):
+            out.append((raw[at:at + ln[i]], tuple(int(v) for v in counts[at:at + ln[i]]), float(wf[i]), float(wr[i]),
+                        int(no[i])))
+            at += int(ln[i])
+        return out
+
+    def deletes(self, poa):
+        k = int(self.nodes(poa)["n_del"].sum())
+        ln, no = np.zeros(max(k, 1), np.int64), np.zeros(max(k, 1), np.int64)
+        wf, wr = np.zeros(max(k, 1)), np.zeros(max(k, 1))
+        self.lib.refpoa_deletes(poa, _p(ln, c_int64), _p(wf, c_double), _p(wr, c_double), _p(no, c_int64))
+        return [(int(ln[i]), float(wf[i]), float(wr[i]), int(no[i])) for i in range(k)]
+
+    def consensus(self, poa, params_h):
+        n = self.lib.refpoa_node_count(poa)
+        cap = 64 * n + 64
+        chars = (self._c_char * cap)()
+        counts = np.zeros(cap, np.uint64)
+        m = np.zeros(max(n - 1, 1), np.int64)
+        k = self.lib.refpoa_consensus(poa, params_h, chars, _p(counts, self._c_uint64), cap, _p(m, c_int64))
+        return bytes(chars[:k]), counts[:k].copy(), m[:n - 1].copy()
+
+    def anchor_alignments(self, poa, node_map, n_reads, params_h):
+        mp = None if node_map is None else np.ascontiguousarray(node_map, dtype=np.int64)
+        cap = int(self.nodes(poa)["n_obs"].sum()) + 1
+        off = np.zeros(n_reads + 1, np.int64)
+        tri = np.zeros((cap, 3), np.int64)
+        self.lib.refpoa_anchor_alignments(poa, _p(mp, c_int64), n_reads, params_h, _p(off, c_int64), _p(tri, c_int64),
+                                          cap)
+        return [tri[off[r]:off[r + 1]].copy() for r in range(n_reads)]

@@ -22,6 +22,7 @@
  * but has no prototype in the public header. */
 Band *band_constructDynamic(stList *anchorPairs, int64_t lX, int64_t lY);
 
+#ifndef MP_REF_WITH_POLISHER  /* the POA oracle build links impl/polisher.c, which defines it */
 /* ------------------------------------------------------------------------ */
 /* Repeat-count table access.                                                */
 /* impl/polisher.c (not compiled into the oracle) defines                    */
@@ -45,6 +46,7 @@ double repeatSubMatrix_getLogProb(RepeatSubMatrix *repeatSubMatrix, Symbol base,
     }
     return repeatSubMatrix->logProbabilities[idx];
 }
+#endif
 
 /* ------------------------------------------------------------------------ */
 /* Model construction                                                        */
@@ -187,6 +189,19 @@ static PairwiseAlignmentParameters *toReferenceParams(const RefoParams *q) {
     p->gapGamma = (float) q->gapGamma;
     p->alignAmbiguityCharacters = 0;
     return p;
+}
+
+/* Accessors for the POA oracle (oracle/ref_poa_harness.c). */
+PairwiseAlignmentParameters *refo_params_to_reference(const RefoParams *q) {
+    return toReferenceParams(q);
+}
+
+StateMachine *refo_model_state_machine(void *handle) {
+    return ((RefoModel *) handle)->sM;
+}
+
+RepeatSubMatrix *refo_model_repeat_matrix(void *handle) {
+    return ((RefoModel *) handle)->repeatSubMatrix;
 }
 
 static SymbolString toSymbolString(Alphabet *a, const uint16_t *s, int64_t n) {

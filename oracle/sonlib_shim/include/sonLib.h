@@ -1,6 +1,7 @@
 /*
  * Minimal stand-in for the sonLib API surface used by MarginPolish's pair-HMM
- * sources (impl/pairwiseAligner.c, impl/stateMachine.c).
+ * sources (impl/pairwiseAligner.c, impl/stateMachine.c) and by the POA loop of
+ * impl/polisher.c.
  *
  * TEST INFRASTRUCTURE ONLY. sonLib (a git submodule of the reference) is not
  * present, so this header declares, from the way the reference calls them, the
@@ -24,6 +25,7 @@
 #include <string.h>
 #include <math.h>
 #include <inttypes.h>
+#include <limits.h>
 
 #ifndef TRUE
 #define TRUE 1
@@ -68,6 +70,8 @@ void st_logDebug(const char *msg, ...);
 void st_logInfo(const char *msg, ...);
 void st_logCritical(const char *msg, ...);
 int st_getLogLevel(void);
+/* log levels compared against st_getLogLevel() (impl/polisher.c:1974) */
+enum stLogLevel { off = 0, critical = 1, info = 2, debug = 3 };
 
 /* ---- strings ---- */
 char *stString_print(const char *fmt, ...);
@@ -92,6 +96,27 @@ void *stList_peek(stList *list);
 void *stList_pop(stList *list);
 void stList_reverse(stList *list);
 void stList_setDestructor(stList *list, void (*destructElement)(void *));
+
+void stList_sort(stList *list, int (*cmpFn)(const void *a, const void *b));
+
+/* ---- stSortedSet (a sorted array; the POA oracle's match sets) ---- */
+stSortedSet *stSortedSet_construct3(int (*cmpFn)(const void *, const void *), void (*destructElementFn)(void *));
+void stSortedSet_destruct(stSortedSet *set);
+void stSortedSet_insert(stSortedSet *set, void *object);
+void *stSortedSet_search(stSortedSet *set, void *object);
+
+/* ---- stHash keyed by pointer value ---- */
+stHash *stHash_construct(void);
+void stHash_destruct(stHash *hash);
+void stHash_insert(stHash *hash, void *key, void *value);
+void *stHash_remove(stHash *hash, void *key);
+
+/* ---- stSet: named by phasing code the oracle never runs ---- */
+void *stSet_search(stSet *set, void *object);
+
+/* ---- more strings ---- */
+char *stString_getSubString(const char *cA, int64_t start, int64_t length);
+char *stString_join2(const char *pad, stList *strings);
 
 /* ---- stIntTuple ---- */
 stIntTuple *stIntTuple_construct1(int64_t v1);

@@ -343,3 +343,204 @@ int64_t stJson_parseFloatArray(double *array, int64_t length, char *js, jsmntok_
     st_errAbort("sonlib_shim: JSON parsing is not provided");
     return 0;
 }
+
+/* ---------------- stList_sort ---------------- */
+
+/* qsort hands the comparator pointers to the array slots; sonLib's comparators take the
+ * list items themselves. */
+static __thread int (*gListCmp)(const void *, const void *);
+
+static int listSlotCmp(const void *a, const void *b) {
+    return gListCmp(*(void *const *) a, *(void *const *) b);
+}
+
+void stList_sort(stList *list, int (*cmpFn)(const void *a, const void *b)) {
+    int (*saved)(const void *, const void *) = gListCmp;
+    gListCmp = cmpFn;
+    qsort(list->items, (size_t) list->length, sizeof(void *), listSlotCmp);
+    gListCmp = saved;
+}
+
+/* ---------------- stSortedSet ---------------- */
+
+struct _stSortedSet {
+    void **items;
+    int64_t length, capacity;
+    int (*cmp)(const void *, const void *);
+    void (*destructElement)(void *);
+};
+
+stSortedSet *stSortedSet_construct3(int (*cmpFn)(const void *, const void *), void (*destructElementFn)(void *)) {
+    stSortedSet *s = st_calloc(1, sizeof(stSortedSet));
+    s->capacity = 16;
+    s->items = st_calloc(s->capacity, sizeof(void *));
+    s->cmp = cmpFn;
+    s->destructElement = destructElementFn;
+    return s;
+}
+
+void stSortedSet_destruct(stSortedSet *set) {
+    if (set == NULL) {
+        return;
+    }
+    if (set->destructElement != NULL) {
+        for (int64_t i = 0; i < set->length; i++) {
+            set->destructElement(set->items[i]);
+        }
+    }
+    free(set->items);
+    free(set);
+}
+
+/* first index whose item is not less than object */
+static int64_t sortedLowerBound(stSortedSet *set, void *object) {
+    int64_t lo = 0, hi = set->length;
+    while (lo < hi) {
+        int64_t mid = lo + (hi - lo) / 2;
+        if (set->cmp(set->items[mid], object) < 0) {
+            lo = mid + 1;
+        } else {
+            hi = mid;
+        }
+    }
+    return lo;
+}
+
+void stSortedSet_insert(stSortedSet *set, void *object) {
+    int64_t i = sortedLowerBound(set, object);
+    if (i < set->length && set->cmp(set->items[i], object) == 0) { /* a set: replace the equal item */
+        set->items[i] = object;
+        return;
+    }
+    if (set->length == set->capacity) {
+        set->capacity *= 2;
+        set->items = realloc(set->items, sizeof(void *) * set->capacity);
+    }
+    memmove(set->items + i + 1, set->items + i, sizeof(void *) * (set->length - i));
+    set->items[i] = object;
+    set->length++;
+}
+
+void *stSortedSet_search(stSortedSet *set, void *object) {
+    int64_t i = sortedLowerBound(set, object);
+    return (i < set->length && set->cmp(set->items[i], object) == 0) ? set->items[i] : NULL;
+}
+
+/* ---------------- stHash (pointer keys, linear probing) ---------------- */
+
+struct _stHash {
+    void **keys;
+    void **values;
+    char *used;
+    int64_t size, count;
+};
+
+stHash *stHash_construct(void) {
+    stHash *h = st_calloc(1, sizeof(stHash));
+    h->size = 64;
+    h->keys = st_calloc(h->size, sizeof(void *));
+    h->values = st_calloc(h->size, sizeof(void *));
+    h->used = st_calloc(h->size, 1);
+    return h;
+}
+
+void stHash_destruct(stHash *hash) {
+    if (hash == NULL) {
+        return;
+    }
+    free(hash->keys);
+    free(hash->values);
+    free(hash->used);
+    free(hash);
+}
+
+static int64_t hashSlot(stHash *h, void *key) {
+    uint64_t x = (uint64_t) (uintptr_t) key * 0x9E3779B97F4A7C15ull;
+    int64_t i = (int64_t) (x >> 17) & (h->size - 1);
+    while (h->used[i] && h->keys[i] != key) {
+        i = (i + 1) & (h->size - 1);
+    }
+    return i;
+}
+
+void stHash_insert(stHash *hash, void *key, void *value) {
+    if (2 * (hash->count + 1) > hash->size) {
+        stHash old = *hash;
+        hash->size *= 2;
+        hash->count = 0;
+        hash->keys = st_calloc(hash->size, sizeof(void *));
+        hash->values = st_calloc(hash->size, sizeof(void *));
+        hash->used = st_calloc(hash->size, 1);
+        for (int64_t i = 0; i < old.size; i++) {
+            if (old.used[i]) {
+                stHash_insert(hash, old.keys[i], old.values[i]);
+            }
+        }
+        free(old.keys);
+        free(old.values);
+        free(old.used);
+    }
+    int64_t i = hashSlot(hash, key);
+    if (!hash->used[i]) {
+        hash->used[i] = 1;
+        hash->keys[i] = key;
+        hash->count++;
+    }
+    hash->values[i] = value;
+}
+
+void *stHash_remove(stHash *hash, void *key) {
+    int64_t i = hashSlot(hash, key);
+    if (!hash->used[i]) {
+        return NULL;
+    }
+    void *v = hash->values[i];
+    /* re-insert the rest of the probe run */
+    hash->used[i] = 0;
+    hash->count--;
+    int64_t j = (i + 1) & (hash->size - 1);
+    while (hash->used[j]) {
+        void *k = hash->keys[j], *val = hash->values[j];
+        hash->used[j] = 0;
+        hash->count--;
+        stHash_insert(hash, k, val);
+        j = (j + 1) & (hash->size - 1);
+    }
+    return v;
+}
+
+void *stSet_search(stSet *set, void *object) {
+    (void) set;
+    (void) object;
+    st_errAbort("stSet_search: not part of the oracle's path");
+    return NULL;
+}
+
+/* ---------------- strings ---------------- */
+
+char *stString_getSubString(const char *cA, int64_t start, int64_t length) {
+    char *c = st_malloc(length + 1);
+    memcpy(c, cA + start, (size_t) length);
+    c[length] = '\0';
+    return c;
+}
+
+char *stString_join2(const char *pad, stList *strings) {
+    size_t padLen = strlen(pad), total = 1;
+    for (int64_t i = 0; i < strings->length; i++) {
+        total += strlen(strings->items[i]) + (i > 0 ? padLen : 0);
+    }
+    char *out = st_malloc((int64_t) total);
+    size_t k = 0;
+    for (int64_t i = 0; i < strings->length; i++) {
+        if (i > 0) {
+            memcpy(out + k, pad, padLen);
+            k += padLen;
+        }
+        size_t n = strlen(strings->items[i]);
+        memcpy(out + k, strings->items[i], n);
+        k += n;
+    }
+    out[k] = '\0';
+    return out;
+}

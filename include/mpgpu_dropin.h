@@ -8,6 +8,7 @@
  *   getAlignedPairsUsingAnchors             inc/pairwiseAligner.h:73    (impl/pairwiseAligner.c:1088-1103)
  *   getAlignedPairsWithIndels               inc/pairwiseAligner.h:67-69 (impl/pairwiseAligner.c:1141-1149)
  *   getAlignedPairs                         inc/pairwiseAligner.h:60-61 (impl/pairwiseAligner.c:1132-1139)
+ *   computeForwardProbability               inc/pairwiseAligner.h:103-106 (impl/pairwiseAligner.c:813-865)
  *
  * The type declarations below restate the reference's public layouts
  * (inc/stateMachine.h:13-22, :40-48, :65-75, :101-124; inc/pairwiseAligner.h:28-39)
@@ -112,6 +113,10 @@ void getAlignedPairsWithIndels(StateMachine *sM, SymbolString sX, SymbolString s
                                bool alignmentHasRaggedLeftEnd, bool alignmentHasRaggedRightEnd);
 stList *getAlignedPairs(StateMachine *sM, SymbolString sX, SymbolString sY, PairwiseAlignmentParameters *p,
                         bool alignmentHasRaggedLeftEnd, bool alignmentHasRaggedRightEnd);
+/* computeForwardProbability (impl/pairwiseAligner.c:813-865, inc/pairwiseAligner.h:103-106): ln P over
+ * the band of band_construct, through mp_forward_batch. */
+double computeForwardProbability(SymbolString sX, SymbolString sY, stList *anchorPairs, PairwiseAlignmentParameters *p,
+                                 StateMachine *sM, bool alignmentHasRaggedLeftEnd, bool alignmentHasRaggedRightEnd);
 
 /* Lowering of a caller's StateMachine to the flat description mp_model_create takes
  * (no device needed). repeat_out must hold 4*51*51 doubles; desc->repeat_log10 is set

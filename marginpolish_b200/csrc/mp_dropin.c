@@ -166,6 +166,59 @@ static stList *toList(const mp_result_view *v, int k) {
     return l;
 }
 
+static void toParams(const PairwiseAlignmentParameters *p, mp_params *q) {
+    memset(q, 0, sizeof(*q));
+    q->threshold = p->threshold;
+    q->min_diags_between_traceback = p->minDiagsBetweenTraceBack;
+    q->traceback_diagonals = p->traceBackDiagonals;
+    q->diagonal_expansion = p->diagonalExpansion;
+    q->constraint_diagonal_trim = p->constraintDiagonalTrim;
+    q->split_matrix_bigger_than_this = p->splitMatrixBiggerThanThis;
+    q->dynamic_anchor_expansion = p->dynamicAnchorExpansion ? 1 : 0;
+    q->gap_gamma = p->gapGamma;
+}
+
+/* computeForwardProbability (impl/pairwiseAligner.c:813-865). */
+double computeForwardProbability(SymbolString sX, SymbolString sY, stList *anchorPairs, PairwiseAlignmentParameters *p,
+                                 StateMachine *sM, bool alignmentHasRaggedLeftEnd, bool alignmentHasRaggedRightEnd) {
+    pthread_mutex_lock(&gLock);
+    ensureEngine();
+    mp_model *m = modelFor(sM);
+    int64_t nA = anchorPairs ? stList_length(anchorPairs) : 0;
+    int32_t *an = malloc(sizeof(int32_t) * 3 * (nA > 0 ? nA : 1));
+    if (an == NULL) die("out of memory");
+    for (int64_t i = 0; i < nA; i++) {
+        stIntTuple *t = stList_get(anchorPairs, i);
+        an[3 * i] = (int32_t) stIntTuple_get(t, 0);
+        an[3 * i + 1] = (int32_t) stIntTuple_get(t, 1);
+        an[3 * i + 2] = 0;  /* band_construct ignores the anchors' own expansions */
+    }
+    uint16_t zero = 0;
+    int64_t xb = 0, xe = sX.length, yoff[2] = {0, sY.length}, aoff[2] = {0, nA};
+    uint8_t strand = 1, rl = alignmentHasRaggedLeftEnd ? 1 : 0, rr = alignmentHasRaggedRightEnd ? 1 : 0;
+    mp_batch b;
+    memset(&b, 0, sizeof(b));
+    b.n_jobs = 1;
+    b.x_begin = &xb;
+    b.x_end = &xe;
+    b.x_symbols_length = sX.length;
+    b.x_symbols = sX.length > 0 ? sX.sequence : &zero;
+    b.y_offsets = yoff;
+    b.y_symbols = sY.length > 0 ? sY.sequence : &zero;
+    b.anchor_offsets = aoff;
+    b.anchors = an;
+    b.strand = &strand;
+    b.ragged_left = &rl;
+    b.ragged_right = &rr;
+    mp_params q;
+    toParams(p, &q);
+    double lp = 0.0;
+    if (mp_forward_batch(gEngine, m, &q, &b, &lp) != MP_OK) die("computeForwardProbability");
+    free(an);
+    pthread_mutex_unlock(&gLock);
+    return lp;
+}
+
 static void run(StateMachine *sM, SymbolString sX, SymbolString sY, stList *anchorPairs,
                 PairwiseAlignmentParameters *p, stList **alignedPairs, stList **gapXPairs, stList **gapYPairs,
                 bool raggedLeft, bool raggedRight) {
@@ -199,15 +252,7 @@ static void run(StateMachine *sM, SymbolString sX, SymbolString sY, stList *anch
     b.ragged_left = &rl;
     b.ragged_right = &rr;
     mp_params q;
-    memset(&q, 0, sizeof(q));
-    q.threshold = p->threshold;
-    q.min_diags_between_traceback = p->minDiagsBetweenTraceBack;
-    q.traceback_diagonals = p->traceBackDiagonals;
-    q.diagonal_expansion = p->diagonalExpansion;
-    q.constraint_diagonal_trim = p->constraintDiagonalTrim;
-    q.split_matrix_bigger_than_this = p->splitMatrixBiggerThanThis;
-    q.dynamic_anchor_expansion = p->dynamicAnchorExpansion ? 1 : 0;
-    q.gap_gamma = p->gapGamma;
+    toParams(p, &q);
     mp_result *r = NULL;
     if (mp_realign_batch(gEngine, m, &q, &b, &r) != MP_OK) die("getAlignedPairsWithIndelsUsingAnchors");
     mp_result_view v;

@@ -219,6 +219,12 @@ class RefOracle:
     def logadd_address(self) -> int:
         return ctypes.cast(self.lib.refo_logadd, c_void_p).value
 
+    def state_machine(self, h) -> int:
+        """Address of the reference StateMachine of a model handle (for the drop-in tests)."""
+        self.lib.refo_model_state_machine.restype = c_void_p
+        self.lib.refo_model_state_machine.argtypes = [c_void_p]
+        return self.lib.refo_model_state_machine(h)
+
     def forward_probability(self, h, sx, sy, anchors, params, ragged_left=False, ragged_right=False) -> float:
         """The reference's computeForwardProbability (impl/pairwiseAligner.c:813-865)."""
         sx = np.ascontiguousarray(sx, dtype=np.uint16)

@@ -31,8 +31,8 @@ def test_every_declared_symbol_is_exported():
 def test_drop_in_exports_reference_signatures():
     dropin = os.path.join(os.path.dirname(_lib.LIB_PATH), "libmpgpu_dropin.so")
     out = os.popen(f"nm -D --defined-only {dropin}").read()
-    names = _declared("mpgpu_dropin.h", ("get", "mpd_"))
-    assert len(names) == 5
+    names = _declared("mpgpu_dropin.h", ("get", "mpd_", "compute"))
+    assert len(names) == 6 and "computeForwardProbability" in names
     for n in names:
         assert re.search(rf"\bT {n}\b", out), n
     undefined = os.popen(f"nm -D --undefined-only {dropin}").read()

@@ -37,6 +37,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 FLOP_PER_CELL = 48  # 30 FP32 FMA-pipe instructions per cell (forward 12, backward 12, posterior 6)
+# DRAM bytes (read + write) per band cell of the posterior kernel, from one ncu capture of the
+# same kernel on a 24-chunk slice of the workload (profiles/posteriorKernel_batched24_full.md);
+# traffic grows with cells, so a full launch moves this times its cells.
+DRAM_BYTES_PER_CELL = 6.07
 METRIC = "GCUPS fwd+bwd+posterior (batched FP32 vs plain GPU, ≤1e-4 vs FP64); CPU ref"
 
 
@@ -57,6 +61,8 @@ def parse():
     ap.add_argument("--lanes", type=int, default=0, choices=[0, 8, 16, 32],
                     help="lanes per banded sub-problem (0 = the engine's automatic choice)")
     ap.add_argument("--warps", type=int, default=0, help="warps per block of the posterior kernel (0 = automatic)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the adjoint and POA-loop measurements reported beside the headline")
     return ap.parse_args()
 
 
@@ -223,6 +229,54 @@ def band_cells(jobs, pm):
     return out
 
 
+def measure_adjoint(engine, model, pm):
+    """The adjoint (expected counts) over the gradient workload: 512 reads of 2-5 kb on 64
+    random 5 kb templates; one call of mp_expectations_batch (host arrays in, counts out)."""
+    import numpy as np
+    from marginpolish_b200 import expectations_batch, synth
+    wl = synth.config_adjoint(seed=4)
+    jobs = wl.jobs()
+    cells = int(band_cells(jobs, pm).sum())
+    expectations_batch(engine, model, pm.alignment, jobs)  # warm
+    ts = []
+    for _ in range(3):
+        t = time.perf_counter()
+        ex = expectations_batch(engine, model, pm.alignment, jobs)
+        ts.append(time.perf_counter() - t)
+    t = float(np.median(ts))
+    return {"workload": "512 reads of 2-5 kb on 64 random 5 kb templates, band half-width 25", "reads": jobs.n_jobs,
+            "cells": cells, "seconds": t, "gcups": cells / t / 1e9, "log_likelihood": ex.log_likelihood,
+            "form": "mp_expectations_batch, host arrays in / counts out (FP32 cells, FP64 accumulation)"}
+
+
+def measure_polish(engine, model, pm):
+    """The POA loop (poa_realignAll in consensus mode, up to 5 iterations) over 16 chunks of a
+    homopolymer-enriched 10 kb template at 30x, reads of 3-9 kb, drafts with 1% indels."""
+    from marginpolish_b200 import PoaSet, PolishParams, synth
+    wl = synth.config_polish(seed=41, n_chunks=16, chunk_len=10_000, coverage=30, read_len=(3000, 9000),
+                             hp_runs=True)
+    pp = PolishParams(max_iterations=5)
+    best = None
+    for _ in range(2):
+        s = PoaSet.from_polish_model(engine, model, pm, pp, wl.drafts, wl.reads, wl.strands, wl.anchors)
+        t0 = time.perf_counter()
+        s.realign()
+        t1 = time.perf_counter()
+        s.iterate()
+        s.estimate_repeat_counts()
+        t2 = time.perf_counter()
+        its = [s.info(c)["iterations"] for c in range(s.n_chunks)]
+        s.close()
+        if best is None or t2 - t0 < best["seconds"]:
+            best = {"seconds": t2 - t0, "realign_seconds": t1 - t0, "iterate_seconds": t2 - t1,
+                    "iterations": its}
+    best.update({"workload": "16 chunks x 10 kb (homopolymer-enriched), 30x, reads 3-9 kb, drafts with 1% "
+                             "homopolymer-biased indels, up to 5 consensus iterations",
+                 "reads": int(sum(len(r) for r in wl.reads)), "bases": int(sum(r.non_rle_length for lst in wl.reads
+                                                                            for r in lst))})
+    return best
+
+
 def pinned_jobs(jobs):
     """Copy of a batch whose arrays live in page-locked host memory (the library's allocator)."""
     from marginpolish_b200 import Jobs
@@ -337,6 +391,10 @@ def run_ours(args, rank, world, local):
         plain = {"value": p_cells / (p_ms * 1e-3) / 1e9, "unit": "GCUPS", "reads": min(args.plain_reads, n_tasks),
                  "cells": p_cells, "ms": p_ms, "form": "one launch of one warp per read, same kernel and accuracy",
                  "batched_over_plain": (value / world) / (p_cells / (p_ms * 1e-3) / 1e9)}
+    extras = {}
+    if not args.no_extras and rank == 0:
+        extras["adjoint"] = measure_adjoint(engine, model, pm)
+        extras["polish_loop"] = measure_polish(engine, model, pm)
     peak = engine.fp32_peak_tflops()
     post = float(np.median(post_ms))
     achieved = cells * FLOP_PER_CELL / (post * 1e-3) / 1e12
@@ -364,12 +422,14 @@ def run_ours(args, rank, world, local):
             "e2e": e2e,
             "gpu_launches": launches * args.steps,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": DRAM_BYTES_PER_CELL * cells,
+                         "traffic_note": "DRAM bytes per posterior launch: ncu bytes per cell x cells",
                          "note": f"{FLOP_PER_CELL} flop per cell x cells / posterior-kernel event time; "
                                  "peak = FP32 FMA throughput measured live on this GPU (mp_measure_fp32_peak)"},
             "cpu_baseline": cpu,
             "plain_gpu": plain,
             "clocks": clocks,
+            **extras,
         }
         print(json.dumps(line), flush=True)
     db.close()

@@ -130,12 +130,75 @@ struct Num<double> {
     __device__ static __forceinline__ int32_t weight(double p) { return (int32_t) floor(fmin(p, 1.0) * (double) kProbOne); }
 };
 
+// Arithmetic over the C slots of a lane: r = a*b, r = a*s, r = fma(a, s, c) slot by slot
+// (a scalar s is broadcast). In FP32 with an even C, slots 2p and 2p+1 go through one
+// packed two-lane instruction (sm_100 FMUL2 / FFMA2: the same IEEE round-to-nearest
+// products and fused multiply-adds as the scalar forms, half the issue slots).
+template <int C, class V>
+struct SlotMath {
+    static constexpr bool kPacked = std::is_same<V, float>::value && (C % 2) == 0;
+    __device__ static __forceinline__ void mul(V (&r)[C], const V (&a)[C], const V (&b)[C]) {
+        if constexpr (kPacked) {
+#pragma unroll
+            for (int j = 0; j < C; j += 2) {
+                const float2 v = __fmul2_rn(make_float2(a[j], a[j + 1]), make_float2(b[j], b[j + 1]));
+                r[j] = v.x;
+                r[j + 1] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < C; j++) r[j] = a[j] * b[j];
+        }
+    }
+    __device__ static __forceinline__ void muls(V (&r)[C], const V (&a)[C], V s) {
+        if constexpr (kPacked) {
+#pragma unroll
+            for (int j = 0; j < C; j += 2) {
+                const float2 v = __fmul2_rn(make_float2(a[j], a[j + 1]), make_float2(s, s));
+                r[j] = v.x;
+                r[j + 1] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < C; j++) r[j] = a[j] * s;
+        }
+    }
+    __device__ static __forceinline__ void fmas(V (&r)[C], const V (&a)[C], V s, const V (&c)[C]) {
+        if constexpr (kPacked) {
+#pragma unroll
+            for (int j = 0; j < C; j += 2) {
+                const float2 v =
+                    __ffma2_rn(make_float2(a[j], a[j + 1]), make_float2(s, s), make_float2(c[j], c[j + 1]));
+                r[j] = v.x;
+                r[j + 1] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < C; j++) r[j] = Num<V>::fma(a[j], s, c[j]);
+        }
+    }
+};
+
 // Reductions within an aligned group of L lanes.
 template <int L, class V>
 __device__ __forceinline__ V groupMax(V v) {
 #pragma unroll
     for (int o = L / 2; o > 0; o >>= 1) v = Num<V>::mx(v, __shfl_xor_sync(FULL_MASK, v, o));
     return v;
+}
+
+// Maximum of non-negative values over the group. For non-negative FP32 values (never -0:
+// every state value is a product or sum of positive factors, or +0) the order of the bit
+// patterns is the order of the values, so a whole warp reduces in one redux.sync.
+template <int L>
+__device__ __forceinline__ float groupMaxNonNeg(float v) {
+    if constexpr (L == 32) return __uint_as_float(__reduce_max_sync(FULL_MASK, __float_as_uint(v)));
+    else return groupMax<L>(v);
+}
+
+template <int L>
+__device__ __forceinline__ double groupMaxNonNeg(double v) {
+    return groupMax<L>(v);
 }
 
 template <int L, class V>
@@ -146,9 +209,7 @@ __device__ __forceinline__ V groupSum(V v) {
 }
 
 __device__ __forceinline__ int warpMaxInt(int v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(FULL_MASK, v, o));
-    return v;
+    return __reduce_max_sync(FULL_MASK, v);
 }
 
 // Value held by lane gl+1 of the group (0 past the group's last lane).
@@ -424,22 +485,102 @@ __device__ __forceinline__ int initialWindow(int needLo, int needHi) {
     return needLo - (S - (needHi - needLo + 1)) / 2;
 }
 
+// One diagonal's row of the block cache: per slot the masked forward values (fM, fX, fY)
+// and the masked emissions (eM, eX, eY). FP32 with an even C keeps slot pairs adjacent,
+// so that the packed arithmetic reads them without repacking: per pair p three float4,
+// (fM, fM' fX, fX'), (fY, fY', eM, eM'), (eX, eX', eY, eY'), at [3p+q][lane]. Otherwise
+// one (fM, fX, fY, eM) per slot in the A rows and one (eX, eY) in the B rows, [slot][lane].
+// rowA / rowB are byte offsets of this lane's first entry in the diagonal's rows.
+template <int C, int L, class V>
+struct CacheRow {
+    using N = Num<V>;
+    using V4 = typename N::V4;
+    using V2 = typename N::V2;
+    static constexpr bool kPair = SlotMath<C, V>::kPacked;
+    static constexpr uint32_t kRowA = kPair ? (uint32_t) (C * L * 24) : (uint32_t) (C * L * sizeof(V4));
+    static constexpr uint32_t kRowB = kPair ? 0u : (uint32_t) (C * L * sizeof(V2));
+    static constexpr uint32_t kStrideA = sizeof(V4);  // per lane
+    static constexpr uint32_t kStrideB = sizeof(V2);
+
+    __device__ static __forceinline__ void store(uint32_t rowA, uint32_t rowB, const V (&fM)[C], const V (&fX)[C],
+                                                 const V (&fY)[C], const V (&eM)[C], const V (&eX)[C],
+                                                 const V (&eY)[C]) {
+        if constexpr (kPair) {
+#pragma unroll
+            for (int j = 0; j < C; j += 2) {
+                const uint32_t o = rowA + (uint32_t) ((j / 2) * 3 * L * 16);
+                sts<float4>(o, make_float4(fM[j], fM[j + 1], fX[j], fX[j + 1]));
+                sts<float4>(o + L * 16, make_float4(fY[j], fY[j + 1], eM[j], eM[j + 1]));
+                sts<float4>(o + 2 * L * 16, make_float4(eX[j], eX[j + 1], eY[j], eY[j + 1]));
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < C; j++) {
+                sts<V4>(rowA + j * L * (uint32_t) sizeof(V4), N::v4(fM[j], fX[j], fY[j], eM[j]));
+                sts<V2>(rowB + j * L * (uint32_t) sizeof(V2), N::v2(eX[j], eY[j]));
+            }
+        }
+    }
+
+    __device__ static __forceinline__ void load(uint32_t rowA, uint32_t rowB, V (&fM)[C], V (&fX)[C], V (&fY)[C],
+                                                V (&eM)[C], V (&eX)[C], V (&eY)[C]) {
+        if constexpr (kPair) {
+#pragma unroll
+            for (int j = 0; j < C; j += 2) {
+                const uint32_t o = rowA + (uint32_t) ((j / 2) * 3 * L * 16);
+                const float4 a = lds<float4>(o), b = lds<float4>(o + L * 16), e = lds<float4>(o + 2 * L * 16);
+                fM[j] = a.x, fM[j + 1] = a.y, fX[j] = a.z, fX[j + 1] = a.w;
+                fY[j] = b.x, fY[j + 1] = b.y, eM[j] = b.z, eM[j + 1] = b.w;
+                eX[j] = e.x, eX[j + 1] = e.y, eY[j] = e.z, eY[j + 1] = e.w;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < C; j++) {
+                const V4 a = lds<V4>(rowA + j * L * (uint32_t) sizeof(V4));
+                const V2 e = lds<V2>(rowB + j * L * (uint32_t) sizeof(V2));
+                fM[j] = a.x, fX[j] = a.y, fY[j] = a.z, eM[j] = a.w;
+                eX[j] = e.x, eY[j] = e.y;
+            }
+        }
+    }
+
+    // forward values only (fM, fX, fY)
+    __device__ static __forceinline__ void loadF(uint32_t rowA, V (&fM)[C], V (&fX)[C], V (&fY)[C]) {
+        if constexpr (kPair) {
+#pragma unroll
+            for (int j = 0; j < C; j += 2) {
+                const uint32_t o = rowA + (uint32_t) ((j / 2) * 3 * L * 16);
+                const float4 a = lds<float4>(o);
+                const float2 b = lds<float2>(o + L * 16);
+                fM[j] = a.x, fM[j + 1] = a.y, fX[j] = a.z, fX[j + 1] = a.w;
+                fY[j] = b.x, fY[j + 1] = b.y;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < C; j++) {
+                const V4 a = lds<V4>(rowA + j * L * (uint32_t) sizeof(V4));
+                fM[j] = a.x, fX[j] = a.y, fY[j] = a.z;
+            }
+        }
+    }
+};
+
 // One forward anti-diagonal (PAR = d & 1). Emissions are zeroed outside the band
 // [sLo, sHi], which zeroes the cell. With CACHE, the cell values and the masked
-// emissions are written to the block cache: rowA / rowB are the byte offsets of this
-// lane's slot 0 in the diagonal's rows, slot j follows at j*L entries.
+// emissions are written to the block cache row (rowA, rowB). With SYM, the cells'
+// table offsets go to rowC (slot j at j*L entries).
 template <int C, int L, int PAR, bool CACHE, bool SYM, class V>
 __device__ __forceinline__ void forwardDiagonal(const Ctx<V> &c, Fwd<C, V> &st, const Slots<C> &sy, int sLo, int sHi,
                                                 uint32_t rowA, uint32_t rowB, uint32_t rowC = 0) {
-    using N = Num<V>;
-    constexpr uint32_t kA = sizeof(typename N::V4), kB = sizeof(typename N::V2);
-    V inX[C], inY[C];
+    using M = SlotMath<C, V>;
+    V inX[C], inY[C], mIn[C];
     if (PAR) {  // odd d: gap-x source slot i, gap-y source slot i+1
         const V nb = fromNext<L>(st.oy[0], c.gl);
 #pragma unroll
         for (int j = 0; j < C; j++) {
             inX[j] = st.ox[j];
             inY[j] = (j < C - 1) ? st.oy[j + 1] : nb;
+            mIn[j] = st.mB[j];
         }
     } else {  // even d: gap-x source slot i-1, gap-y source slot i
         const V nb = fromPrev<L>(st.ox[C - 1], c.gl);
@@ -447,32 +588,36 @@ __device__ __forceinline__ void forwardDiagonal(const Ctx<V> &c, Fwd<C, V> &st, 
         for (int j = 0; j < C; j++) {
             inX[j] = (j > 0) ? st.ox[j - 1] : nb;
             inY[j] = st.oy[j];
+            mIn[j] = st.mA[j];
         }
     }
     const int base = c.gl * C - sLo;
     const unsigned span = (unsigned) (sHi - sLo);
+    V eM[C], eX[C], eY[C];
 #pragma unroll
     for (int j = 0; j < C; j++) {
         const bool in = (unsigned) (base + j) <= span;
-        const V eM = in ? (V) matchEmission(sy.xpk[j], sy.ypk[j]) : V(0);
-        const V eX = in ? (V) sy.ex[j] : V(0);
-        const V eY = in ? (V) sy.ey[j] : V(0);
-        const V fM = eM * (PAR ? st.mB[j] : st.mA[j]);
-        const V fX = eX * inX[j];
-        const V fY = eY * inY[j];
-        const V nm = N::fma(c.t[2 * 3 + 0], fY, N::fma(c.t[1 * 3 + 0], fX, c.t[0 * 3 + 0] * fM));
-        const V nx = N::fma(c.t[2 * 3 + 1], fY, N::fma(c.t[1 * 3 + 1], fX, c.t[0 * 3 + 1] * fM));
-        const V ny = N::fma(c.t[1 * 3 + 2], fX, N::fma(c.t[2 * 3 + 2], fY, c.t[0 * 3 + 2] * fM));
-        if (PAR) st.mB[j] = nm; else st.mA[j] = nm;
-        st.ox[j] = nx;
-        st.oy[j] = ny;
-        if (CACHE) {
-            sts<typename N::V4>(rowA + j * L * kA, N::v4(fM, fX, fY, eM));
-            sts<typename N::V2>(rowB + j * L * kB, N::v2(eX, eY));
-        }
+        eM[j] = in ? (V) matchEmission(sy.xpk[j], sy.ypk[j]) : V(0);
+        eX[j] = in ? (V) sy.ex[j] : V(0);
+        eY[j] = in ? (V) sy.ey[j] : V(0);
         // the cell's table offsets (repeat | match << 17), for the adjoint's histograms
         if (SYM) sts<uint32_t>(rowC + j * L * 4, in ? sy.xpk[j] + sy.ypk[j] : 0xffffffffu);
     }
+    V fM[C], fX[C], fY[C], a[C];
+    M::mul(fM, eM, mIn);
+    M::mul(fX, eX, inX);
+    M::mul(fY, eY, inY);
+    // match: t00*fM + t10*fX + t20*fY; gap-x: t01, t11, t21; gap-y: t02, t22, t12 (in that order)
+    M::muls(a, fM, c.t[0 * 3 + 0]);
+    M::fmas(a, fX, c.t[1 * 3 + 0], a);
+    if (PAR) M::fmas(st.mB, fY, c.t[2 * 3 + 0], a); else M::fmas(st.mA, fY, c.t[2 * 3 + 0], a);
+    M::muls(a, fM, c.t[0 * 3 + 1]);
+    M::fmas(a, fX, c.t[1 * 3 + 1], a);
+    M::fmas(st.ox, fY, c.t[2 * 3 + 1], a);
+    M::muls(a, fM, c.t[0 * 3 + 2]);
+    M::fmas(a, fY, c.t[2 * 3 + 2], a);
+    M::fmas(st.oy, fX, c.t[1 * 3 + 2], a);
+    if (CACHE) CacheRow<C, L, V>::store(rowA, rowB, fM, fX, fY, eM, eX, eY);
 }
 
 // Diagonal 0: the start cell (x-y = 0) holds the start (or ragged-start) probabilities.
@@ -480,22 +625,20 @@ template <int C, int L, bool CACHE, class V>
 __device__ __forceinline__ void forwardOrigin(const Ctx<V> &c, const float *startP, int Q, Fwd<C, V> &st,
                                               uint32_t rowA, uint32_t rowB) {
     using N = Num<V>;
-    constexpr uint32_t kA = sizeof(typename N::V4), kB = sizeof(typename N::V2);
+    V fM[C], fX[C], fY[C], z[C];
 #pragma unroll
     for (int j = 0; j < C; j++) {
         const bool here = c.gl * C + j == -Q;
-        const V fM = here ? (V) startP[0] : V(0);
-        const V fX = here ? (V) startP[1] : V(0);
-        const V fY = here ? (V) startP[2] : V(0);
-        st.mA[j] = N::fma(c.t[2 * 3 + 0], fY, N::fma(c.t[1 * 3 + 0], fX, c.t[0 * 3 + 0] * fM));
-        st.ox[j] = N::fma(c.t[2 * 3 + 1], fY, N::fma(c.t[1 * 3 + 1], fX, c.t[0 * 3 + 1] * fM));
-        st.oy[j] = N::fma(c.t[1 * 3 + 2], fX, N::fma(c.t[2 * 3 + 2], fY, c.t[0 * 3 + 2] * fM));
+        fM[j] = here ? (V) startP[0] : V(0);
+        fX[j] = here ? (V) startP[1] : V(0);
+        fY[j] = here ? (V) startP[2] : V(0);
+        z[j] = V(0);
+        st.mA[j] = N::fma(c.t[2 * 3 + 0], fY[j], N::fma(c.t[1 * 3 + 0], fX[j], c.t[0 * 3 + 0] * fM[j]));
+        st.ox[j] = N::fma(c.t[2 * 3 + 1], fY[j], N::fma(c.t[1 * 3 + 1], fX[j], c.t[0 * 3 + 1] * fM[j]));
+        st.oy[j] = N::fma(c.t[1 * 3 + 2], fX[j], N::fma(c.t[2 * 3 + 2], fY[j], c.t[0 * 3 + 2] * fM[j]));
         st.mB[j] = V(0);
-        if (CACHE) {
-            sts<typename N::V4>(rowA + j * L * kA, N::v4(fM, fX, fY, V(0)));
-            sts<typename N::V2>(rowB + j * L * kB, N::v2(V(0), V(0)));
-        }
     }
+    if (CACHE) CacheRow<C, L, V>::store(rowA, rowB, fM, fX, fY, z, z, z);
 }
 
 // Rescales the carried forward state by a power of two; returns the exponent removed.
@@ -505,7 +648,7 @@ __device__ __forceinline__ int rescaleFwd(Fwd<C, V> &st) {
     V m = V(0);
 #pragma unroll
     for (int j = 0; j < C; j++) m = N::mx(m, N::mx(N::mx(st.ox[j], st.oy[j]), N::mx(st.mA[j], st.mB[j])));
-    m = groupMax<L>(m);
+    m = groupMaxNonNeg<L>(m);
     if (!(m > V(0))) return 0;
     const int k = N::expOf(m);
     const V sc = N::pow2(-k);
@@ -585,8 +728,8 @@ struct GroupSmem {
     static constexpr size_t ringBytes = 2 * R * sizeof(uint2);
     static constexpr size_t bandRingBytes = 64 * sizeof(int4);
     static constexpr size_t walkBandBytes = K * sizeof(int4);
-    static constexpr size_t cacheABytes = (size_t) K * S * sizeof(typename Num<V>::V4);
-    static constexpr size_t cacheBBytes = (size_t) K * S * sizeof(typename Num<V>::V2);
+    static constexpr size_t cacheABytes = (size_t) K * CacheRow<C, L, V>::kRowA;
+    static constexpr size_t cacheBBytes = (size_t) K * CacheRow<C, L, V>::kRowB;
     static constexpr size_t cacheCBytes = ADJ ? (size_t) K * S * sizeof(uint32_t) : 0;
     static constexpr size_t infoBytes = K * sizeof(int2);
     static constexpr size_t bytes =
@@ -598,8 +741,8 @@ struct GroupMem {
     Ring<RingSize<L * C>::R> rx, ry;
     uint32_t bandRing;  // byte offsets in shared memory: 64 band records (int4)
     uint32_t walkBand;  // K band records of the block being walked
-    uint32_t cacheA;    // [K][S] (fM, fX, fY, eM) in the arithmetic type
-    uint32_t cacheB;    // [K][S] (eX, eY)
+    uint32_t cacheA;    // [K] rows of the block cache (CacheRow)
+    uint32_t cacheB;    // [K] B rows of the block cache (empty in the paired layout)
     uint32_t cacheC;    // adjoint only: [K][S] uint32 table offsets of the cell
     uint32_t info;      // [K] int2: window, shift
     uint32_t hist;      // adjoint only: the block's histograms (small tables, then repeat tables)
@@ -670,7 +813,8 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
     using N = Num<V>;
     using V4 = typename N::V4;
     using V2 = typename N::V2;
-    constexpr uint32_t kA = sizeof(V4), kB = sizeof(V2);
+    using CR = CacheRow<C, L, V>;
+    using M = SlotMath<C, V>;
     static_assert(K <= L && (K % 2) == 0, "band records of a block are held one per lane");
     constexpr int S = L * C;
     constexpr int R = RingSize<S>::R;
@@ -704,7 +848,7 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
         if (ok && gl < K && dd <= c.N) pband = c.band[dd];
     };
     prefetch(bTop, bTop >= bBot);
-    const uint32_t laneA = gm.cacheA + (uint32_t) gl * kA, laneB = gm.cacheB + (uint32_t) gl * kB;
+    const uint32_t laneA = gm.cacheA + (uint32_t) gl * CR::kStrideA, laneB = gm.cacheB + (uint32_t) gl * CR::kStrideB;
     const uint32_t laneC = gm.cacheC + (uint32_t) gl * 4;
 
     for (int w = 0; w < nIter; w++) {
@@ -759,12 +903,12 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
                 const int d = dStart + kk;
                 const int2 b0 = lds<int2>(gm.walkBand + kk * 16);
                 const int2 b1 = lds<int2>(gm.walkBand + (kk + 1) * 16);
-                const uint32_t rowA = laneA + (uint32_t) (kk * S * kA), rowB = laneB + (uint32_t) (kk * S * kB);
+                const uint32_t rowA = laneA + (uint32_t) kk * CR::kRowA, rowB = laneB + (uint32_t) kk * CR::kRowB;
                 const uint32_t rowC = laneC + (uint32_t) (kk * S * 4);
                 stepSlots<C, L, R, 0>(gl, gm.rx, gm.ry, d, Q, sy);
                 forwardDiagonal<C, L, 0, true, ADJ, V>(c, rs, sy, b0.x - Q, b0.y - Q, rowA, rowB, rowC);
                 stepSlots<C, L, R, 1>(gl, gm.rx, gm.ry, d + 1, Q, sy);
-                forwardDiagonal<C, L, 1, true, ADJ, V>(c, rs, sy, b1.x - Q, b1.y - Q, rowA + S * kA, rowB + S * kB,
+                forwardDiagonal<C, L, 1, true, ADJ, V>(c, rs, sy, b1.x - Q, b1.y - Q, rowA + CR::kRowA, rowB + CR::kRowB,
                                                        rowC + S * 4);
             }
             if (gl < K) sts<int2>(gm.info + gl * 8, make_int2(Q, 0));
@@ -794,7 +938,7 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
                         checkAt = ensureRings<R, L, S>(c, gm.rx, gm.ry, d, Q, false, on);
                     }
                     const int sLo = bd.x - Q, sHi = bd.y - Q;
-                    const uint32_t rowA = laneA + (uint32_t) (kk * S * kA), rowB = laneB + (uint32_t) (kk * S * kB);
+                    const uint32_t rowA = laneA + (uint32_t) kk * CR::kRowA, rowB = laneB + (uint32_t) kk * CR::kRowB;
                     const uint32_t rowC = laneC + (uint32_t) (kk * S * 4);
                     if (par) {
                         stepSlots<C, L, R, 1>(gl, gm.rx, gm.ry, d, Q, sy);
@@ -813,6 +957,12 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
         __syncwarp();
 
         // ---------------- backward over the block ----------------
+        // Posterior of a cell = f * b * 2^(Ef + Eb - ET) / Tm: the factor changes only at a
+        // total refresh and between blocks.
+        auto scaleOf = [&]() {
+            return Tm > V(0) ? N::div(N::pow2(max(N::kMinExp, min(N::kMaxExp, Ef + Eb - ET))), Tm) : V(0);
+        };
+        V postScale = scaleOf();
         // One diagonal (PAR = d & 1). FLAT: every diagonal of the block is on and no window
         // shift occurs, so the step has no votes or branches (the total is refreshed by
         // selection and tuples are written with predicated stores).
@@ -822,13 +972,8 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
             const int d = dStart + kk;
             const bool on = FLAT || (blockOn && d <= dEnd && d > wk.tbTo);
             const int2 inf = FLAT ? make_int2(Q, 0) : lds<int2>(gm.info + kk * 8);
-            V4 f[C];
-            V2 e[C];
-#pragma unroll
-            for (int j = 0; j < C; j++) {
-                f[j] = lds<V4>(laneA + (uint32_t) ((kk * S + j * L) * kA));
-                e[j] = lds<V2>(laneB + (uint32_t) ((kk * S + j * L) * kB));
-            }
+            V fM[C], fX[C], fY[C], eM[C], eX[C], eY[C];
+            CR::load(laneA + (uint32_t) kk * CR::kRowA, laneB + (uint32_t) kk * CR::kRowB, fM, fX, fY, eM, eX, eY);
             V bM[C], bX[C], bY[C];
             V sX[C], sY[C], sM2[C];  // u-values of the gap-x, gap-y and match successors
             {
@@ -847,18 +992,26 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
                         sY[j] = (j > 0) ? gY[j - 1] : nb;
                     }
                 }
-                // the walk's first diagonal holds the end probabilities (never inside a flat block)
-                const bool top = !FLAT && d == wk.D;
 #pragma unroll
-                for (int j = 0; j < C; j++) {
-                    const V s2 = PAR ? gB[j] : gA[j];
-                    sM2[j] = s2;
-                    const V m_ = N::fma(c.t[0 * 3 + 0], s2, N::fma(c.t[0 * 3 + 2], sY[j], c.t[0 * 3 + 1] * sX[j]));
-                    const V x_ = N::fma(c.t[1 * 3 + 0], s2, N::fma(c.t[1 * 3 + 2], sY[j], c.t[1 * 3 + 1] * sX[j]));
-                    const V y_ = N::fma(c.t[2 * 3 + 0], s2, N::fma(c.t[2 * 3 + 2], sY[j], c.t[2 * 3 + 1] * sX[j]));
-                    bM[j] = top ? endM : m_;
-                    bX[j] = top ? endX : x_;
-                    bY[j] = top ? endY : y_;
+                for (int j = 0; j < C; j++) sM2[j] = PAR ? gB[j] : gA[j];
+                // b_s = t_sX * uX + t_sY * uY + t_sM * uM, accumulated in that order
+                V a[C];
+                M::muls(a, sX, c.t[0 * 3 + 1]);
+                M::fmas(a, sY, c.t[0 * 3 + 2], a);
+                M::fmas(bM, sM2, c.t[0 * 3 + 0], a);
+                M::muls(a, sX, c.t[1 * 3 + 1]);
+                M::fmas(a, sY, c.t[1 * 3 + 2], a);
+                M::fmas(bX, sM2, c.t[1 * 3 + 0], a);
+                M::muls(a, sX, c.t[2 * 3 + 1]);
+                M::fmas(a, sY, c.t[2 * 3 + 2], a);
+                M::fmas(bY, sM2, c.t[2 * 3 + 0], a);
+                if (!FLAT && d == wk.D) {  // the walk's first diagonal holds the end probabilities
+#pragma unroll
+                    for (int j = 0; j < C; j++) {
+                        bM[j] = endM;
+                        bX[j] = endX;
+                        bY[j] = endY;
+                    }
                 }
             }
             const bool post = on && d <= wk.tbFrom;
@@ -868,11 +1021,11 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
                 // cells of d plus the match transitions crossing d (impl/pairwiseAligner.c:567-584)
                 V sM1[C];
                 if (kk > 0) {
+                    V qM[C], qX[C], qY[C];
+                    CR::loadF(laneA + (uint32_t) (kk - 1) * CR::kRowA, qM, qX, qY);
 #pragma unroll
-                    for (int j = 0; j < C; j++) {
-                        const V4 q = lds<V4>(laneA + (uint32_t) (((kk - 1) * S + j * L) * kA));
-                        sM1[j] = N::fma(c.t[2 * 3 + 0], q.z, N::fma(c.t[1 * 3 + 0], q.y, c.t[0 * 3 + 0] * q.x));
-                    }
+                    for (int j = 0; j < C; j++)
+                        sM1[j] = N::fma(c.t[2 * 3 + 0], qY[j], N::fma(c.t[1 * 3 + 0], qX[j], c.t[0 * 3 + 0] * qM[j]));
                 } else {
 #pragma unroll
                     for (int j = 0; j < C; j++) sM1[j] = chkSM[j];
@@ -882,9 +1035,9 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
 #pragma unroll
                 for (int j = 0; j < C; j++) {
                     const V uMn = PAR ? gA[j] : gB[j];  // match u of d+1
-                    part = N::fma(f[j].x, bM[j], part);
-                    part = N::fma(f[j].y, bX[j], part);
-                    part = N::fma(f[j].z, bY[j], part);
+                    part = N::fma(fM[j], bM[j], part);
+                    part = N::fma(fX[j], bX[j], part);
+                    part = N::fma(fY[j], bY[j], part);
                     part = N::fma(uMn, sM1[j], part);
                 }
                 const V T = groupSum<L>(part);
@@ -910,20 +1063,19 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
                 llSet = llSet || first;
                 Tm = refresh ? tm : Tm;
                 ET = refresh ? et : ET;
+                postScale = scaleOf();
             }
             untilRefresh = refresh ? 9 : untilRefresh - (post ? 1 : 0);
             posts += post ? 1 : 0;
             const bool emit = post && Tm > V(0) && wk.emit;
             if (FLAT || __any_sync(FULL_MASK, emit)) {
-                const int ex = max(N::kMinExp, min(N::kMaxExp, Ef + Eb - ET));
-                const V scale = emit ? N::div(N::pow2(ex), Tm) : V(0);
                 V p[3][C];
-#pragma unroll
-                for (int j = 0; j < C; j++) {
-                    p[0][j] = (f[j].x * bM[j]) * scale;
-                    p[1][j] = (f[j].y * bX[j]) * scale;
-                    p[2][j] = (f[j].z * bY[j]) * scale;
-                }
+                M::mul(p[0], fM, bM);
+                M::mul(p[1], fX, bX);
+                M::mul(p[2], fY, bY);
+                M::muls(p[0], p[0], postScale);
+                M::muls(p[1], p[1], postScale);
+                M::muls(p[2], p[2], postScale);
                 emitDiagonal<C, L, V>(gl, o, p, thr, slotX0(d, inf.x), d, emit);
             }
             if constexpr (ADJ) {
@@ -937,7 +1089,7 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
                     float *hs = reinterpret_cast<float *>(mpSmem + gm.hist);
 #pragma unroll
                     for (int j = 0; j < C; j++) {
-                        const float fm = f[j].x * scale, fx = f[j].y * scale, fy = f[j].z * scale;
+                        const float fm = fM[j] * scale, fx = fX[j] * scale, fy = fY[j] * scale;
                         ta[0] = __fmaf_rn(fm, sM2[j], ta[0]);
                         ta[1] = __fmaf_rn(fm, sX[j], ta[1]);
                         ta[2] = __fmaf_rn(fm, sY[j], ta[2]);
@@ -971,12 +1123,21 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
                 }
             }
             // u-values of d (emissions are zero outside the band); kept when the diagonal is off
+            if (FLAT) {
+                M::mul(gX, eX, bX);
+                M::mul(gY, eY, bY);
+                if (PAR) M::mul(gB, eM, bM); else M::mul(gA, eM, bM);
+            } else {
+                V ux[C], uy[C], um[C];
+                M::mul(ux, eX, bX);
+                M::mul(uy, eY, bY);
+                M::mul(um, eM, bM);
 #pragma unroll
-            for (int j = 0; j < C; j++) {
-                const V ux = e[j].x * bX[j], uy = e[j].y * bY[j], um = f[j].w * bM[j];
-                gX[j] = on ? ux : gX[j];
-                gY[j] = on ? uy : gY[j];
-                if (PAR) gB[j] = on ? um : gB[j]; else gA[j] = on ? um : gA[j];
+                for (int j = 0; j < C; j++) {
+                    gX[j] = on ? ux[j] : gX[j];
+                    gY[j] = on ? uy[j] : gY[j];
+                    if (PAR) gB[j] = on ? um[j] : gB[j]; else gA[j] = on ? um[j] : gA[j];
+                }
             }
             if (!FLAT) {
                 // moving below d crosses the window shift met when entering d
@@ -1009,7 +1170,7 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
             V m = V(0);
 #pragma unroll
             for (int j = 0; j < C; j++) m = N::mx(m, N::mx(N::mx(gX[j], gY[j]), N::mx(gA[j], gB[j])));
-            m = groupMax<L>(m);
+            m = groupMaxNonNeg<L>(m);
             if (blockOn && m > V(0)) {
                 const int kx = N::expOf(m);
                 const V s = N::pow2(-kx);

@@ -147,6 +147,35 @@ typedef struct {
 } mp_tuning;
 mp_status mp_engine_set_tuning(mp_engine *e, const mp_tuning *t);
 
+/* Autotuner. The posterior kernel comes in variants that differ in band tile shape (lanes
+ * per sub-problem x cells per lane: the window of S = lanes x cells slots), checkpoint
+ * stride and resident warps. mp_engine_autotune plans `sample` (a batch like the ones to
+ * come), groups its sub-problems by band hull into classes bounded by the FP32 variants'
+ * window capacities, and times on each class with enough sub-problems every variant that
+ * holds it, at several warps per block. Each candidate runs on a persistent grid cut to the
+ * blocks that get at least six task loads per warp (no tail of idle warps) and its per-block
+ * rate is scaled to the whole device. The fastest pair per class becomes the engine's
+ * choice for later calls while lanes_per_task is 0 (automatic); classes without a
+ * measurement keep the built-in choice. FP64 re-runs and the adjoint are not tuned.
+ * `report` may be NULL. mp_engine_autotune_reset restores the built-in choice. */
+#define MP_AUTOTUNE_MAX_CLASSES 8
+typedef struct {
+    int32_t n_classes;
+    int32_t max_hull[MP_AUTOTUNE_MAX_CLASSES];          /* class bound, in window slots */
+    int32_t tasks[MP_AUTOTUNE_MAX_CLASSES];             /* sub-problems of the sample in the class */
+    int32_t candidates[MP_AUTOTUNE_MAX_CLASSES];        /* (variant, warps) pairs timed; 0 = not tuned */
+    int32_t variant[MP_AUTOTUNE_MAX_CLASSES];           /* chosen kernel variant (-1: built-in choice) */
+    int32_t lanes_per_task[MP_AUTOTUNE_MAX_CLASSES];    /* tile shape of the choice */
+    int32_t cells_per_lane[MP_AUTOTUNE_MAX_CLASSES];
+    int32_t checkpoint_stride[MP_AUTOTUNE_MAX_CLASSES];
+    int32_t warps_per_block[MP_AUTOTUNE_MAX_CLASSES];
+    double gcups[MP_AUTOTUNE_MAX_CLASSES];              /* the choice, posterior kernel time only */
+    double default_gcups[MP_AUTOTUNE_MAX_CLASSES];      /* the built-in choice on the same tasks */
+} mp_autotune_report;
+mp_status mp_engine_autotune(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *sample,
+                             mp_autotune_report *report);
+mp_status mp_engine_autotune_reset(mp_engine *e);
+
 /* Full posterior pass over a batch of jobs held in host memory: host->device copies,
  * band construction, the persistent length-sorted posterior kernel, compaction and
  * device->host copies of the tuples. The engine keeps the device buffers of its last

@@ -181,6 +181,17 @@ class Tuning(Structure):
     ]
 
 
+AUTOTUNE_MAX_CLASSES = 8
+
+
+class AutotuneReport(Structure):
+    _fields_ = [("n_classes", c_int32)] + [
+        (name, c_int32 * AUTOTUNE_MAX_CLASSES)
+        for name in ("max_hull", "tasks", "candidates", "variant", "lanes_per_task", "cells_per_lane",
+                     "checkpoint_stride", "warps_per_block")
+    ] + [("gcups", c_double * AUTOTUNE_MAX_CLASSES), ("default_gcups", c_double * AUTOTUNE_MAX_CLASSES)]
+
+
 # Every symbol include/mpgpu.h declares (checked by the CPU tests).
 EXPORTED = [
     "mp_last_error", "mp_version", "mp_engine_create", "mp_engine_destroy", "mp_engine_info",
@@ -193,7 +204,7 @@ EXPORTED = [
     "mp_poa_set_create", "mp_poa_set_destroy", "mp_poa_set_realign", "mp_poa_set_realign_pairs", "mp_poa_set_iterate",
     "mp_poa_set_realign_all", "mp_poa_set_estimate_repeat_counts", "mp_poa_info", "mp_poa_nodes",
     "mp_poa_observations", "mp_poa_inserts", "mp_poa_deletes", "mp_poa_reference", "mp_poa_consensus",
-    "mp_poa_anchor_alignments",
+    "mp_poa_anchor_alignments", "mp_engine_autotune", "mp_engine_autotune_reset",
 ]
 
 _lib = None
@@ -216,6 +227,8 @@ def load() -> ctypes.CDLL:
         "mp_engine_destroy": (None, [c_void_p]),
         "mp_engine_info": (c_int, [c_void_p, P(c_int), P(c_int), P(c_int)]),
         "mp_engine_set_tuning": (c_int, [c_void_p, P(Tuning)]),
+        "mp_engine_autotune": (c_int, [c_void_p, c_void_p, P(Params), P(Batch), P(AutotuneReport)]),
+        "mp_engine_autotune_reset": (c_int, [c_void_p]),
         "mp_model_create": (c_int, [c_void_p, P(ModelDesc), P(ModelDesc), P(c_void_p)]),
         "mp_model_destroy": (None, [c_void_p]),
         "mp_realign_batch": (c_int, [c_void_p, c_void_p, P(Params), P(Batch), P(c_void_p)]),

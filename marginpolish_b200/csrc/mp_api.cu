@@ -392,6 +392,21 @@ static int pickVariant(int lanes, int64_t slots) {
     return -1;
 }
 
+// The engine's choice for a posterior task: the autotuned variant of the task's hull class
+// when the engine is tuned and lanes_per_task is automatic, else the built-in preference.
+static int pickTunedVariant(const mp_engine *e, int64_t slots) {
+    if (e->tuning.lanes_per_task == 0) {
+        for (size_t c = 0; c < e->tunedBound.size(); c++) {
+            if (slots <= e->tunedBound[c]) {
+                const int v = e->tunedVariant[c];
+                if (v >= 0 && slots <= variantCapacity(v)) return v;
+                break;
+            }
+        }
+    }
+    return pickVariant(e->tuning.lanes_per_task, slots);
+}
+
 // FP64 variants (one task per warp), narrowest window that holds the hull; -1 if none.
 static int pickVariantF64(int64_t slots) {
     for (int v = 0; v < variantCount(); v++) {
@@ -500,6 +515,9 @@ struct mp_device_batch {
     std::vector<int64_t> varMaxN;
     std::vector<TaskOut> hostOut;
     int launchesPerRun = 0;
+    int forceVariant = -1;  // autotuner: every posterior task in this variant ...
+    int forceWarps = 0;     // ... at this many warps per block
+    int forceBlocks = 0;    // ... in at most this many persistent blocks
     bool ran = false;
     float bandMs = 0.0f, posteriorMs = 0.0f;
     cudaEvent_t evBand = nullptr;
@@ -735,7 +753,8 @@ static mp_status buildQueues(mp_device_batch *db, const std::vector<int32_t> &su
     for (int32_t t : subset) {
         const int v = db->mode == kModeAdjoint ? pickAdjointVariant(db->hull[t])
                       : db->f64[t]           ? pickVariantF64(db->hull[t])
-                                             : pickVariant(db->e->tuning.lanes_per_task, db->hull[t]);
+                      : db->forceVariant >= 0 ? db->forceVariant
+                                              : pickTunedVariant(db->e, db->hull[t]);
         if (v < 0)
             return failf(MP_ERR_OVERFLOW, "job %d: band wider than the widest kernel window", db->tasks[t].job);
         db->var[t] = v;
@@ -835,11 +854,15 @@ static mp_status launchQueues(mp_device_batch *db) {
         const int nTables = db->m->sharedRepeat ? 1 : 2;
         const int maxW = adj ? adjointVariantMaxWarps(v, nTables) : variantMaxWarps(v, nTables);
         if (maxW < 1) return failf(MP_ERR_OVERFLOW, "kernel variant %d does not fit in shared memory", v);
-        const int warps = e->tuning.warps_per_block > 0 ? std::min(e->tuning.warps_per_block, maxW) : maxW;
+        int warps = e->tuning.warps_per_block > 0 ? std::min(e->tuning.warps_per_block, maxW) : maxW;
+        if (!adj && db->forceWarps > 0) warps = std::min(db->forceWarps, maxW);
+        else if (!adj && e->tuning.warps_per_block == 0 && v < (int) e->tunedWarps.size() && e->tunedWarps[v] > 0)
+            warps = std::min(e->tunedWarps[v], maxW);
         const int blocksPerSm = e->tuning.blocks_per_sm > 0 ? e->tuning.blocks_per_sm : 1;
         const int loads = (db->varCount[v] + G - 1) / G;  // warp-loads of G tasks
         const int maxBlocks = (loads + warps - 1) / warps;  // no more warps than loads
-        const int blocks = std::max(1, std::min(e->smCount * blocksPerSm, maxBlocks));
+        int blocks = std::max(1, std::min(e->smCount * blocksPerSm, maxBlocks));
+        if (!adj && db->forceBlocks > 0) blocks = std::min(blocks, db->forceBlocks);
         const int scratchBlocks = (int) (db->varMaxN[v] / K + 2);
         const size_t slots = (size_t) blocks * warps * G;
         const size_t elem = adj ? sizeof(float4) : chkElemBytes(v);
@@ -1282,6 +1305,151 @@ extern "C" void mp_device_batch_destroy(mp_device_batch *db) {
     if (!db) return;
     if (db->device >= 0) cudaSetDevice(db->device);  // the engine may already be gone
     delete db;
+}
+
+// ---------------------------------------------------------------------------
+// autotuner
+// ---------------------------------------------------------------------------
+
+// Steady-state throughput (GCUPS of a whole device) of variant v at `warps` warps per block
+// on the tasks `subset` (`cells` band cells) of a planned batch: the persistent grid is cut
+// to the blocks that get at least six task loads per warp, so that the length-sorted queue
+// drains without a tail of idle warps, and the per-block rate is scaled to every SM. Best
+// of `reps` launches after one warm-up launch.
+static mp_status timeCandidate(mp_device_batch *db, const std::vector<int32_t> &subset, int64_t cells, int v,
+                               int warps, int reps, double *gcups) {
+    mp_engine *e = db->e;
+    cudaStream_t st = e->stream;
+    int C = 0, L = 0, K = 0;
+    variantShape(v, &C, &L, &K);
+    const int loads = ((int) subset.size() + 32 / L - 1) / (32 / L);
+    const int blocks = std::max(1, std::min(e->smCount, loads / (6 * warps)));
+    db->forceVariant = v;
+    db->forceWarps = warps;
+    db->forceBlocks = blocks;
+    std::vector<int32_t> orderHost;
+    mp_status s = buildQueues(db, subset, orderHost);
+    if (s == MP_OK)
+        s = upload(db->orders, orderHost.data(), sizeof(int32_t) * std::max<size_t>(orderHost.size(), 1), st);
+    float best = 0.0f;
+    for (int r = 0; s == MP_OK && r <= reps; r++) {
+        if (cudaEventRecord(e->ev0, st) != cudaSuccess) s = failf(MP_ERR_CUDA, "event record failed");
+        if (s == MP_OK) s = launchQueues(db);
+        if (s == MP_OK && cudaEventRecord(e->ev1, st) != cudaSuccess) s = failf(MP_ERR_CUDA, "event record failed");
+        if (s == MP_OK && cudaStreamSynchronize(st) != cudaSuccess)
+            s = failf(MP_ERR_CUDA, "autotune launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+        float ms = 0.0f;
+        if (s == MP_OK && cudaEventElapsedTime(&ms, e->ev0, e->ev1) != cudaSuccess)
+            s = failf(MP_ERR_CUDA, "event timing failed");
+        if (s == MP_OK && r > 0 && (best == 0.0f || ms < best)) best = ms;
+    }
+    db->forceVariant = -1;
+    db->forceWarps = 0;
+    db->forceBlocks = 0;
+    *gcups = best > 0.0f ? (double) cells / (best * 1e6) * e->smCount / blocks : 0.0;
+    return s;
+}
+
+extern "C" mp_status mp_engine_autotune_reset(mp_engine *e) {
+    if (!e) return failf(MP_ERR_ARGUMENT, "engine is NULL");
+    e->tunedBound.clear();
+    e->tunedVariant.clear();
+    e->tunedWarps.clear();
+    return MP_OK;
+}
+
+extern "C" mp_status mp_engine_autotune(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *sample,
+                                        mp_autotune_report *report) {
+    if (!e || !m || !p || !sample) return failf(MP_ERR_ARGUMENT, "mp_engine_autotune: NULL argument");
+    CUDA_TRY(cudaSetDevice(e->device));
+    // classes: the distinct window capacities of the FP32 variants, ascending
+    std::vector<int> bounds;
+    for (int v = 0; v < variantCount(); v++)
+        if (!variantIsF64(v)) bounds.push_back(variantCapacity(v));
+    std::sort(bounds.begin(), bounds.end());
+    bounds.erase(std::unique(bounds.begin(), bounds.end()), bounds.end());
+    if ((int) bounds.size() > MP_AUTOTUNE_MAX_CLASSES) bounds.resize(MP_AUTOTUNE_MAX_CLASSES);
+    if (report) {
+        memset(report, 0, sizeof(*report));
+        report->n_classes = (int32_t) bounds.size();
+    }
+    // plan and run the sample once with the built-in choice (bands, capacities, hull retries)
+    const std::vector<int> keepBound = e->tunedBound, keepVariant = e->tunedVariant, keepWarps = e->tunedWarps;
+    MP_TRY(mp_engine_autotune_reset(e));
+    mp_device_batch *db = nullptr;
+    mp_status s = mp_device_batch_create(e, m, p, sample, &db);
+    float ms0 = 0.0f;
+    if (s == MP_OK) s = mp_device_batch_run(e, db, &ms0);
+    std::vector<int> chosenVariant(bounds.size(), -1);
+    std::vector<int> warpsOf(variantCount(), 0);
+    const int nTables = m->sharedRepeat ? 1 : 2;
+    const int kMinTasks = 2 * e->smCount;  // enough sub-problems for a steady-state measurement
+    for (size_t c = 0; s == MP_OK && c < bounds.size(); c++) {
+        const int lo = c == 0 ? 0 : bounds[c - 1], hi = bounds[c];
+        std::vector<int32_t> subset;
+        int64_t cells = 0;
+        for (size_t t = 0; t < db->tasks.size(); t++) {
+            if (db->f64[t] || db->hull[t] <= lo || db->hull[t] > hi) continue;
+            subset.push_back((int32_t) t);
+            cells += db->hostOut[t].cells;
+        }
+        if (report) {
+            report->max_hull[c] = hi;
+            report->tasks[c] = (int32_t) subset.size();
+            report->variant[c] = -1;
+        }
+        if ((int) subset.size() < kMinTasks || cells <= 0) continue;
+        // the built-in choice, for the report
+        const int def = pickVariant(0, hi);
+        double defRate = 0.0;
+        s = timeCandidate(db, subset, cells, def, variantMaxWarps(def, nTables), 2, &defRate);
+        double bestRate = 0.0;
+        int bestV = -1, bestW = 0, timed = 0;
+        for (int v = 0; s == MP_OK && v < variantCount(); v++) {
+            if (variantIsF64(v) || variantCapacity(v) < hi) continue;
+            const int maxW = variantMaxWarps(v, nTables);
+            if (maxW < 1) continue;
+            int opts[3] = {maxW, std::max(1, (maxW * 3) / 4), std::max(1, maxW / 2)};
+            for (int k = 0; s == MP_OK && k < 3; k++) {
+                if (k > 0 && opts[k] == opts[k - 1]) continue;
+                double rate = 0.0;
+                s = timeCandidate(db, subset, cells, v, opts[k], 2, &rate);
+                timed++;
+                if (s == MP_OK && rate > bestRate) {
+                    bestRate = rate;
+                    bestV = v;
+                    bestW = opts[k];
+                }
+            }
+        }
+        if (s != MP_OK || bestV < 0) break;
+        chosenVariant[c] = bestV;
+        // one warps setting per variant: the first class that chose it decides
+        if (warpsOf[bestV] == 0) warpsOf[bestV] = bestW;
+        if (report) {
+            int C = 0, L = 0, K = 0;
+            variantShape(bestV, &C, &L, &K);
+            report->candidates[c] = timed;
+            report->variant[c] = bestV;
+            report->lanes_per_task[c] = L;
+            report->cells_per_lane[c] = C;
+            report->checkpoint_stride[c] = K;
+            report->warps_per_block[c] = warpsOf[bestV];
+            report->gcups[c] = bestRate;
+            report->default_gcups[c] = defRate;
+        }
+    }
+    mp_device_batch_destroy(db);
+    if (s != MP_OK) {
+        e->tunedBound = keepBound;
+        e->tunedVariant = keepVariant;
+        e->tunedWarps = keepWarps;
+        return s;
+    }
+    e->tunedBound = bounds;
+    e->tunedVariant = chosenVariant;
+    e->tunedWarps = warpsOf;
+    return MP_OK;
 }
 
 extern "C" mp_status mp_result_view_get(const mp_result *r, mp_result_view *v) {

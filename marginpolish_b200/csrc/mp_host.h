@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <mutex>
+#include <vector>
 #include <string>
 
 // Records the thread-local error message of the C ABI and returns s.
@@ -68,6 +69,10 @@ struct mp_engine {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     mp_tuning tuning{};
+    // autotuned choice (mp_engine_autotune): ascending hull-class bounds with the FP32 kernel
+    // variant of each class, and warps per block per variant (0: as many as fit); empty when
+    // not tuned
+    std::vector<int> tunedBound, tunedVariant, tunedWarps;
     struct mp_device_batch *oneShot = nullptr;  // reused by the one-shot calls (mp_realign_batch*)
     struct mp_device_batch *forwardShot = nullptr;  // reused by mp_forward_batch
     struct mp_device_batch *adjointShot = nullptr;  // reused by mp_expectations_batch

@@ -398,12 +398,14 @@ __device__ __forceinline__ void loadSlots(int gl, const Ring<R> &rx, const Ring<
 }
 
 // Slot symbols from diagonal d-1 to d (window unchanged): entering odd d the x of
-// every slot grows by one, entering even d the y of every slot grows by one.
+// every slot grows by one, entering even d the y of every slot grows by one. `fresh` is
+// the sequence position that enters the window: x of the last slot (odd d) or y of the
+// first slot (even d).
 template <int C, int L, int R, int PAR>
-__device__ __forceinline__ void stepSlots(int gl, const Ring<R> &rx, const Ring<R> &ry, int d, int Q, Slots<C> &s) {
-    constexpr int S = L * C;
+__device__ __forceinline__ void stepSlotsAt(int gl, const Ring<R> &rx, const Ring<R> &ry, int freshPos,
+                                            Slots<C> &s) {
     if (PAR) {
-        const uint2 fresh = rx.get(slotX0(d, Q) + S - 2);
+        const uint2 fresh = rx.get(freshPos);
         uint32_t npk = __shfl_down_sync(FULL_MASK, s.xpk[0], 1, L);
         float ne = __shfl_down_sync(FULL_MASK, s.ex[0], 1, L);
         if (gl == L - 1) {
@@ -418,7 +420,7 @@ __device__ __forceinline__ void stepSlots(int gl, const Ring<R> &rx, const Ring<
         s.xpk[C - 1] = npk;
         s.ex[C - 1] = ne;
     } else {
-        const uint2 fresh = ry.get(d - slotX0(d, Q) - 1);
+        const uint2 fresh = ry.get(freshPos);
         uint32_t npk = __shfl_up_sync(FULL_MASK, s.ypk[C - 1], 1, L);
         float ne = __shfl_up_sync(FULL_MASK, s.ey[C - 1], 1, L);
         if (gl == 0) {
@@ -433,6 +435,12 @@ __device__ __forceinline__ void stepSlots(int gl, const Ring<R> &rx, const Ring<
         s.ypk[0] = npk;
         s.ey[0] = ne;
     }
+}
+
+template <int C, int L, int R, int PAR>
+__device__ __forceinline__ void stepSlots(int gl, const Ring<R> &rx, const Ring<R> &ry, int d, int Q, Slots<C> &s) {
+    constexpr int S = L * C;
+    stepSlotsAt<C, L, R, PAR>(gl, rx, ry, PAR ? slotX0(d, Q) + S - 2 : d - slotX0(d, Q) - 1, s);
 }
 
 // Forward state between diagonals: outgoing gap-x / gap-y sums of d-1 and
@@ -594,14 +602,34 @@ __device__ __forceinline__ void forwardDiagonal(const Ctx<V> &c, Fwd<C, V> &st, 
     const int base = c.gl * C - sLo;
     const unsigned span = (unsigned) (sHi - sLo);
     V eM[C], eX[C], eY[C];
+    if constexpr (M::kPacked) {
+        // band mask as a 0/1 factor (emissions are finite, so the products are exact)
+        V rp[C], mt[C], mk[C], gx[C], gy[C];
 #pragma unroll
-    for (int j = 0; j < C; j++) {
-        const bool in = (unsigned) (base + j) <= span;
-        eM[j] = in ? (V) matchEmission(sy.xpk[j], sy.ypk[j]) : V(0);
-        eX[j] = in ? (V) sy.ex[j] : V(0);
-        eY[j] = in ? (V) sy.ey[j] : V(0);
-        // the cell's table offsets (repeat | match << 17), for the adjoint's histograms
-        if (SYM) sts<uint32_t>(rowC + j * L * 4, in ? sy.xpk[j] + sy.ypk[j] : 0xffffffffu);
+        for (int j = 0; j < C; j++) {
+            const bool in = (unsigned) (base + j) <= span;
+            const uint32_t s2 = sy.xpk[j] + sy.ypk[j];
+            rp[j] = ldsF(s2 & 0x1ffffu);
+            mt[j] = ldsF(s2 >> 17);
+            mk[j] = in ? V(1) : V(0);
+            gx[j] = sy.ex[j];
+            gy[j] = sy.ey[j];
+            if (SYM) sts<uint32_t>(rowC + j * L * 4, in ? s2 : 0xffffffffu);
+        }
+        M::mul(eM, rp, mt);
+        M::mul(eM, eM, mk);
+        M::mul(eX, gx, mk);
+        M::mul(eY, gy, mk);
+    } else {
+#pragma unroll
+        for (int j = 0; j < C; j++) {
+            const bool in = (unsigned) (base + j) <= span;
+            eM[j] = in ? (V) matchEmission(sy.xpk[j], sy.ypk[j]) : V(0);
+            eX[j] = in ? (V) sy.ex[j] : V(0);
+            eY[j] = in ? (V) sy.ey[j] : V(0);
+            // the cell's table offsets (repeat | match << 17), for the adjoint's histograms
+            if (SYM) sts<uint32_t>(rowC + j * L * 4, in ? sy.xpk[j] + sy.ypk[j] : 0xffffffffu);
+        }
     }
     V fM[C], fX[C], fY[C], a[C];
     M::mul(fM, eM, mIn);
@@ -652,13 +680,11 @@ __device__ __forceinline__ int rescaleFwd(Fwd<C, V> &st) {
     if (!(m > V(0))) return 0;
     const int k = N::expOf(m);
     const V sc = N::pow2(-k);
-#pragma unroll
-    for (int j = 0; j < C; j++) {
-        st.ox[j] *= sc;
-        st.oy[j] *= sc;
-        st.mA[j] *= sc;
-        st.mB[j] *= sc;
-    }
+    using M = SlotMath<C, V>;
+    M::muls(st.ox, st.ox, sc);
+    M::muls(st.oy, st.oy, sc);
+    M::muls(st.mA, st.mA, sc);
+    M::muls(st.mB, st.mB, sc);
     return k;
 }
 
@@ -686,13 +712,16 @@ __device__ __forceinline__ void emitDiagonal(int gl, Out &o, const V (&p)[3][C],
     const unsigned below = ((1u << gl) - 1u) << (lane - gl);           // lower lanes of the group
     const unsigned group = (L == 32 ? FULL_MASK : ((1u << L) - 1u)) << (lane - gl);
     const int xl = x0 + gl * C;
+    const int xo = xl - 1 + o.xShift, yo = d - xl - 1 + o.yShift;  // output coordinates of slot 0
 #pragma unroll
     for (int k = 0; k < 3; k++) {
+        bool h[C];
         unsigned b[C];
         unsigned any = 0;
 #pragma unroll
         for (int j = 0; j < C; j++) {
-            b[j] = __ballot_sync(FULL_MASK, active && p[k][j] >= thr);
+            h[j] = active && p[k][j] >= thr;
+            b[j] = __ballot_sync(FULL_MASK, h[j]);
             any |= b[j];
         }
         if (any == 0) continue;
@@ -705,11 +734,8 @@ __device__ __forceinline__ void emitDiagonal(int gl, Out &o, const V (&p)[3][C],
         int pos = o.top[k] - 1 - o.written[k] - before;
 #pragma unroll
         for (int j = 0; j < C; j++) {
-            if ((b[j] >> lane) & 1u) {
-                if (pos >= 0) {
-                    const int x = xl + j;
-                    o.t[k][pos] = make_int4(Num<V>::weight(p[k][j]), x - 1 + o.xShift, d - x - 1 + o.yShift, 0);
-                }
+            if (h[j]) {
+                if (pos >= 0) o.t[k][pos] = make_int4(Num<V>::weight(p[k][j]), xo + j, yo - j, 0);
                 pos--;
             }
         }
@@ -1174,13 +1200,10 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
             if (blockOn && m > V(0)) {
                 const int kx = N::expOf(m);
                 const V s = N::pow2(-kx);
-#pragma unroll
-                for (int j = 0; j < C; j++) {
-                    gX[j] *= s;
-                    gY[j] *= s;
-                    gA[j] *= s;
-                    gB[j] *= s;
-                }
+                M::muls(gX, gX, s);
+                M::muls(gY, gY, s);
+                M::muls(gA, gA, s);
+                M::muls(gB, gB, s);
                 Eb += kx;
             }
         }

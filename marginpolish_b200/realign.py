@@ -52,6 +52,25 @@ class Engine:
         t = _lib.Tuning(0, warps_per_block, blocks_per_sm, lanes_per_task)
         _lib.check(self._lib.mp_engine_set_tuning(self.handle, ctypes.byref(t)))
 
+    def autotune(self, model: "Model", params, sample: "Jobs") -> list:
+        """Times the FP32 kernel variants (band tile shape, checkpoint stride) and warps per
+        block on the sub-problems of `sample` per band-hull class and makes the fastest the
+        engine's choice (mp_engine_autotune). Returns one dict per class."""
+        rep = _lib.AutotuneReport()
+        p = params.struct() if hasattr(params, "struct") else params
+        _lib.check(self._lib.mp_engine_autotune(self.handle, model.handle, ctypes.byref(p),
+                                                ctypes.byref(sample.struct()), ctypes.byref(rep)))
+        out = []
+        for c in range(rep.n_classes):
+            out.append({k: (float(getattr(rep, k)[c]) if k.endswith("gcups") else int(getattr(rep, k)[c]))
+                        for k in ("max_hull", "tasks", "candidates", "variant", "lanes_per_task", "cells_per_lane",
+                                  "checkpoint_stride", "warps_per_block", "gcups", "default_gcups")})
+        return out
+
+    def autotune_reset(self) -> None:
+        """Restores the built-in kernel choice."""
+        _lib.check(self._lib.mp_engine_autotune_reset(self.handle))
+
     def fp32_peak_tflops(self) -> float:
         """Measured FP32 FMA throughput of this device (TFLOP/s)."""
         v = ctypes.c_double()

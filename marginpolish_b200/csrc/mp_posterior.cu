@@ -552,6 +552,32 @@ struct CacheRow {
         }
     }
 
+    // Once the backward has passed diagonal kk, its row holds the cells' posteriors, slot-major
+    // per list: element (kk&1)*8 + k*kPStride + slot + (slot/32)*4 of the row (in V units). The
+    // padding after every 32 slots and the shift of odd rows make both the owner lanes' stores
+    // (consecutive slots) and the emitters' range reads (16 consecutive slots of two diagonals
+    // per 8-lane phase) free of bank conflicts. `row` is the group's row of kk.
+    static constexpr int kPStride = L * C + ((L * C) >> 5) * 4;
+    static_assert((3 * kPStride + 8) * sizeof(V) <= kRowA, "the posteriors fit in the row they replace");
+    __device__ static __forceinline__ uint32_t pAddr(uint32_t row, int kk, int slot, int k) {
+        return row + (uint32_t) (((kk & 1) * 8 + k * kPStride + slot + (slot >> 5) * 4) * (int) sizeof(V));
+    }
+    __device__ static __forceinline__ void storeP(uint32_t row, int kk, int gl, const V (&pM)[C], const V (&pX)[C],
+                                                  const V (&pY)[C]) {
+        if constexpr (C == 2 && std::is_same<V, float>::value) {
+            sts<float2>(pAddr(row, kk, 2 * gl, 0), make_float2(pM[0], pM[1]));
+            sts<float2>(pAddr(row, kk, 2 * gl, 1), make_float2(pX[0], pX[1]));
+            sts<float2>(pAddr(row, kk, 2 * gl, 2), make_float2(pY[0], pY[1]));
+        } else {
+#pragma unroll
+            for (int j = 0; j < C; j++) {
+                sts<V>(pAddr(row, kk, gl * C + j, 0), pM[j]);
+                sts<V>(pAddr(row, kk, gl * C + j, 1), pX[j]);
+                sts<V>(pAddr(row, kk, gl * C + j, 2), pY[j]);
+            }
+        }
+    }
+
     // forward values only (fM, fX, fY)
     __device__ static __forceinline__ void loadF(uint32_t rowA, V (&fM)[C], V (&fX)[C], V (&fY)[C]) {
         if constexpr (kPair) {
@@ -699,50 +725,6 @@ struct Out {
     int xShift, yShift;
 };
 
-// Called by every lane of the warp; groups with `active` false emit nothing. The
-// (list, slot) pairs are unrolled at compile time, so each tuple is written through a
-// fixed list pointer.
-template <int C, int L, class V>
-__device__ __forceinline__ void emitDiagonal(int gl, Out &o, const V (&p)[3][C], V thr, int x0, int d,
-                                             bool active) {
-    // Ranks come from one ballot per (list, slot): a tuple's rank within its group's
-    // diagonal is the number of passing slots of lower index (lower lanes, then lower
-    // slots of the same lane). A list no lane holds is skipped by the whole warp.
-    const int lane = threadIdx.x & 31;
-    const unsigned below = ((1u << gl) - 1u) << (lane - gl);           // lower lanes of the group
-    const unsigned group = (L == 32 ? FULL_MASK : ((1u << L) - 1u)) << (lane - gl);
-    const int xl = x0 + gl * C;
-    const int xo = xl - 1 + o.xShift, yo = d - xl - 1 + o.yShift;  // output coordinates of slot 0
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        bool h[C];
-        unsigned b[C];
-        unsigned any = 0;
-#pragma unroll
-        for (int j = 0; j < C; j++) {
-            h[j] = active && p[k][j] >= thr;
-            b[j] = __ballot_sync(FULL_MASK, h[j]);
-            any |= b[j];
-        }
-        if (any == 0) continue;
-        int before = 0, total = 0;
-#pragma unroll
-        for (int j = 0; j < C; j++) {
-            before += __popc(b[j] & below);
-            total += L == 32 ? __popc(b[j]) : __popc(b[j] & group);
-        }
-        int pos = o.top[k] - 1 - o.written[k] - before;
-#pragma unroll
-        for (int j = 0; j < C; j++) {
-            if (h[j]) {
-                if (pos >= 0) o.t[k][pos] = make_int4(Num<V>::weight(p[k][j]), xo + j, yo - j, 0);
-                pos--;
-            }
-        }
-        o.written[k] += total;
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Shared workspace of one group
 // ---------------------------------------------------------------------------
@@ -823,6 +805,69 @@ __device__ __forceinline__ void loadFwd(const typename Num<V>::V4 (&v)[C], Fwd<C
 // Block starts are multiples of K (even), so the parity of a block position is
 // the same in every group.
 // ---------------------------------------------------------------------------
+
+// Posterior tuples of one walked block, written after the backward has stored the block's
+// posteriors in the cache rows. The output order is the order of the walk: diagonals top
+// down, slots (ascending x-y) within a diagonal, each list written from the top of its
+// region downwards, so that the region reads in the reference's order. Lane gl of a group
+// takes E = K*C consecutive entries of that order: slots [s0, s0+E) of diagonal kk (L/K lanes
+// per diagonal). Its hits are ranked by one group-wide prefix sum per list. `emitMask` bit kk:
+// diagonal dStart+kk emits (identical over the group's lanes). Called by every lane.
+template <int C, int L, int K, class V>
+__device__ __forceinline__ void emitBlock(int gl, const GroupMem<C, L, K> &gm, unsigned emitMask, int dStart,
+                                          Out &o, V thr) {
+    using CR = CacheRow<C, L, V>;
+    constexpr int E = K * C, LPD = L / K;
+    static_assert(L % K == 0 && E <= 32, "a lane's entries lie within one diagonal and one mask word");
+    const int kk = K - 1 - gl / LPD;
+    const int s0 = (gl % LPD) * E;
+    const int d = dStart + kk;
+    const bool on = (emitMask >> kk) & 1u;
+    const int Q = lds<int2>(gm.info + kk * 8).x;
+    const int x0 = slotX0(d, Q) + s0;  // x of the lane's first slot
+    const int xo = x0 - 1 + o.xShift, yo = d - x0 - 1 + o.yShift;
+    const uint32_t row = gm.cacheA + (uint32_t) kk * CR::kRowA;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        unsigned m = 0;
+        if constexpr (C == 2 && K == 8 && std::is_same<V, float>::value) {
+            // 16 consecutive slots, 16-byte aligned and within one 32-slot stretch
+            const uint32_t base = CR::pAddr(row, kk, s0, k);
+#pragma unroll
+            for (int i = 0; i < E / 4; i++) {
+                const float4 v = lds<float4>(base + (uint32_t) (i * 16));
+                if (v.x >= thr) m |= 1u << (4 * i);
+                if (v.y >= thr) m |= 2u << (4 * i);
+                if (v.z >= thr) m |= 4u << (4 * i);
+                if (v.w >= thr) m |= 8u << (4 * i);
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < E; e++)
+                if (lds<V>(CR::pAddr(row, kk, s0 + e, k)) >= thr) m |= 1u << e;
+        }
+        if (!on) m = 0;
+        const int cnt = __popc(m);
+        int incl = cnt;
+#pragma unroll
+        for (int off = 1; off < L; off <<= 1) {
+            const int t = __shfl_up_sync(FULL_MASK, incl, off, L);
+            if (gl >= off) incl += t;
+        }
+        const int total = __shfl_sync(FULL_MASK, incl, L - 1, L);
+        int pos = o.top[k] - 1 - o.written[k] - (incl - cnt);
+        while (m) {
+            const int e = __ffs(m) - 1;
+            m &= m - 1;
+            if (pos >= 0) {
+                const V p = lds<V>(CR::pAddr(row, kk, s0 + e, k));
+                o.t[k][pos] = make_int4(Num<V>::weight(p), xo + e, yo - e, 0);
+            }
+            pos--;
+        }
+        o.written[k] += total;
+    }
+}
 
 struct Walk {
     int D, tbTo, tbFrom, atEnd, active, emit;
@@ -989,6 +1034,7 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
             return Tm > V(0) ? N::div(N::pow2(max(N::kMinExp, min(N::kMaxExp, Ef + Eb - ET))), Tm) : V(0);
         };
         V postScale = scaleOf();
+        unsigned emitMask = 0;  // diagonals of the block that emit tuples
         // One diagonal (PAR = d & 1). FLAT: every diagonal of the block is on and no window
         // shift occurs, so the step has no votes or branches (the total is refreshed by
         // selection and tuples are written with predicated stores).
@@ -1094,15 +1140,22 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
             untilRefresh = refresh ? 9 : untilRefresh - (post ? 1 : 0);
             posts += post ? 1 : 0;
             const bool emit = post && Tm > V(0) && wk.emit;
-            if (FLAT || __any_sync(FULL_MASK, emit)) {
-                V p[3][C];
-                M::mul(p[0], fM, bM);
-                M::mul(p[1], fX, bX);
-                M::mul(p[2], fY, bY);
-                M::muls(p[0], p[0], postScale);
-                M::muls(p[1], p[1], postScale);
-                M::muls(p[2], p[2], postScale);
-                emitDiagonal<C, L, V>(gl, o, p, thr, slotX0(d, inf.x), d, emit);
+            if constexpr (!ADJ) {
+                // the row of d is not read again: it takes the posteriors (tuples after the block)
+                if (FLAT || __any_sync(FULL_MASK, emit)) {
+                    V p[3][C];
+                    M::mul(p[0], fM, bM);
+                    M::mul(p[1], fX, bX);
+                    M::mul(p[2], fY, bY);
+                    M::muls(p[0], p[0], postScale);
+                    M::muls(p[1], p[1], postScale);
+                    M::muls(p[2], p[2], postScale);
+                    __syncwarp();  // every lane has read its part of the row
+                    CR::storeP(gm.cacheA + (uint32_t) kk * CR::kRowA, kk, gl, p[0], p[1], p[2]);
+                }
+                emitMask |= emit ? 1u << kk : 0u;
+            } else {
+                (void) emit;
             }
             if constexpr (ADJ) {
                 // expected counts: transitions out of the cells of d (f_from * u_to, scaled by 1/P)
@@ -1190,6 +1243,10 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
                 back(odd, std::false_type{}, k + 1);
                 back(even, std::false_type{}, k);
             }
+        }
+        if constexpr (!ADJ) {
+            __syncwarp();
+            if (__any_sync(FULL_MASK, emitMask != 0)) emitBlock<C, L, K, V>(gl, gm, emitMask, dStart, o, thr);
         }
         // rescale the carried backward state at the block boundary
         {

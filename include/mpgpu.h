@@ -147,6 +147,13 @@ typedef struct {
 } mp_tuning;
 mp_status mp_engine_set_tuning(mp_engine *e, const mp_tuning *t);
 
+/* CUDA graph capture of the device-resident pass (mp_device_batch_run): the band kernels,
+ * the queue reset and the persistent posterior launches of a run are captured into one graph
+ * per batch, replayed while the launches are identical (repeated runs of the batch) and
+ * updated in place when they change. Re-runs after capacity, window or range retries stay
+ * direct launches. Off by default. */
+mp_status mp_engine_set_graph_capture(mp_engine *e, int enable);
+
 /* Autotuner. The posterior kernel comes in variants that differ in band tile shape (lanes
  * per sub-problem x cells per lane: the window of S = lanes x cells slots), checkpoint
  * stride and resident warps. mp_engine_autotune plans `sample` (a batch like the ones to

@@ -148,6 +148,12 @@ extern "C" mp_status mp_engine_set_tuning(mp_engine *e, const mp_tuning *t) {
     return MP_OK;
 }
 
+extern "C" mp_status mp_engine_set_graph_capture(mp_engine *e, int enable) {
+    if (!e) return failf(MP_ERR_ARGUMENT, "engine is NULL");
+    e->graphs = enable != 0;
+    return MP_OK;
+}
+
 static float probOf(double logp) {
     return (float) std::exp(logp);
 }
@@ -521,7 +527,11 @@ struct mp_device_batch {
     bool ran = false;
     float bandMs = 0.0f, posteriorMs = 0.0f;
     cudaEvent_t evBand = nullptr;
+    cudaGraphExec_t graphExec = nullptr;  // the pass's launches (engine graph capture on)
+    std::vector<unsigned char> graphKey;  // their arguments when captured
+    int graphCaptures = 0;
     ~mp_device_batch() {
+        if (graphExec) cudaGraphExecDestroy(graphExec);
         if (evBand) cudaEventDestroy(evBand);
     }
 };
@@ -836,12 +846,20 @@ extern "C" mp_status mp_device_batch_reset(mp_engine *e, mp_device_batch *db, co
     return batchReset(e, db, db->m, p, b);
 }
 
-// Launches the posterior kernels for the current queues (one persistent launch per
-// variant with tasks). Scratch for all variants is reserved before the first launch:
-// every task slot (warp x tasks per warp) owns checkpoints for the longest task.
-static mp_status launchQueues(mp_device_batch *db) {
+// The posterior launches of the current queues: one persistent launch per variant with
+// tasks, with its grid, block and kernel arguments.
+struct QueueLaunch {
+    int v, blocks, warps;
+    DpArgs a;
+};
+
+// Plans the posterior launches for the current queues. Scratch for all variants is reserved
+// here, before any launch: every task slot (warp x tasks per warp) owns checkpoints for the
+// longest task.
+static mp_status planQueues(mp_device_batch *db, std::vector<QueueLaunch> &plan) {
     mp_engine *e = db->e;
     cudaStream_t st = e->stream;
+    plan.clear();
     const int nV = modeVariantCount(db);
     const bool adj = db->mode == kModeAdjoint;
     std::vector<int> blocksOf(nV, 0), warpsOf(nV, 0), scratchBlocksOf(nV, 0);
@@ -877,7 +895,6 @@ static mp_status launchQueues(mp_device_batch *db) {
         MP_TRY(db->scratch.reserve(needScratch));
         MP_TRY(db->scratchScal.reserve(needScal));
     }
-    CUDA_TRY(cudaMemsetAsync(db->queue.p, 0, sizeof(int32_t) * nV, st));
     for (int v = 0; v < nV; v++) {
         if (db->varCount[v] == 0) continue;
         DpArgs a;
@@ -903,11 +920,35 @@ static mp_status launchQueues(mp_device_batch *db) {
         a.sharedRepeat = db->m->sharedRepeat;
         a.expect = db->expect.as<double>();
         a.expectRep = db->expectRep.as<double>();
-        if (adj) CUDA_TRY(launchAdjointVariant(v, a, blocksOf[v], warpsOf[v], st));
-        else CUDA_TRY(launchVariant(v, a, blocksOf[v], warpsOf[v], st));
+        plan.push_back(QueueLaunch{v, blocksOf[v], warpsOf[v], a});
+    }
+    return MP_OK;
+}
+
+// Issues planned posterior launches (stream-ordered only: capturable into a CUDA graph).
+static mp_status issueQueues(mp_device_batch *db, const std::vector<QueueLaunch> &plan) {
+    cudaStream_t st = db->e->stream;
+    const bool adj = db->mode == kModeAdjoint;
+    CUDA_TRY(cudaMemsetAsync(db->queue.p, 0, sizeof(int32_t) * modeVariantCount(db), st));
+    for (const QueueLaunch &q : plan) {
+        if (adj) CUDA_TRY(launchAdjointVariant(q.v, q.a, q.blocks, q.warps, st));
+        else CUDA_TRY(launchVariant(q.v, q.a, q.blocks, q.warps, st));
         db->launchesPerRun++;
     }
     return MP_OK;
+}
+
+static mp_status launchQueues(mp_device_batch *db) {
+    std::vector<QueueLaunch> plan;
+    MP_TRY(planQueues(db, plan));
+    return issueQueues(db, plan);
+}
+
+// Appends the bytes of a trivially copyable value to a launch signature.
+template <class T>
+static void keyAppend(std::vector<unsigned char> &key, const T &v) {
+    const unsigned char *b = reinterpret_cast<const unsigned char *>(&v);
+    key.insert(key.end(), b, b + sizeof(T));
 }
 
 extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, float *kernelMs) {
@@ -921,19 +962,80 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
     MP_TRY(buildQueues(db, all, orderHost));
     MP_TRY(upload(db->orders, orderHost.data(), sizeof(int32_t) * std::max<size_t>(orderHost.size(), 1), st));
     if (!db->evBand) CUDA_TRY(cudaEventCreate(&db->evBand));
-    CUDA_TRY(cudaEventRecord(e->ev0, st));
     BandArgs ba;
+    memset(&ba, 0, sizeof(ba));
     ba.tasks = db->dTasks.as<Task>();
     ba.nTasks = nTasks;
     ba.anchors = db->anchors.as<int32_t>();
     ba.band = db->band.as<int2>();
     ba.out = db->dOut.as<TaskOut>();
-    CUDA_TRY(launchBand(ba, st));
-    db->launchesPerRun += nTasks > 0 ? 2 : 0;
-    CUDA_TRY(cudaEventRecord(db->evBand, st));
-    if (db->mode == kModeAdjoint) MP_TRY(zeroExpectations(db));
-    MP_TRY(launchQueues(db));
-    CUDA_TRY(cudaEventRecord(e->ev1, st));
+    if (db->mode == kModeAdjoint) {
+        MP_TRY(db->expect.reserve(sizeof(double) * 2 * kExpPerModel));
+        MP_TRY(db->expectRep.reserve(sizeof(double) * 2 * kRepTable));
+    }
+    std::vector<QueueLaunch> plan;
+    MP_TRY(planQueues(db, plan));
+    // the pass's launches: band kernels, then (adjoint: zeroed accumulators) the queues
+    auto issuePass = [&](bool capturing) -> mp_status {
+        CUDA_TRY(launchBand(ba, st));
+        db->launchesPerRun += nTasks > 0 ? 2 : 0;
+        // inside a capture, an event record becomes a graph node only when marked external
+        if (capturing) CUDA_TRY(cudaEventRecordWithFlags(db->evBand, st, cudaEventRecordExternal));
+        else CUDA_TRY(cudaEventRecord(db->evBand, st));
+        if (db->mode == kModeAdjoint) MP_TRY(zeroExpectations(db));
+        return issueQueues(db, plan);
+    };
+    if (e->graphs) {
+        // One CUDA graph per batch: replayed while the launches are identical (repeated runs),
+        // re-captured and updated in place when they change.
+        std::vector<unsigned char> key;
+        keyAppend(key, db->mode);
+        keyAppend(key, ba);
+        for (const QueueLaunch &q : plan) {
+            keyAppend(key, q.v);
+            keyAppend(key, q.blocks);
+            keyAppend(key, q.warps);
+            keyAppend(key, q.a);
+        }
+        if (!db->graphExec || key != db->graphKey) {
+            cudaGraph_t g = nullptr;
+            CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+            const mp_status cs = issuePass(true);
+            const cudaError_t ce = cudaStreamEndCapture(st, &g);
+            if (cs != MP_OK) {
+                if (g) cudaGraphDestroy(g);
+                return cs;
+            }
+            CUDA_TRY(ce);
+            bool updated = false;
+            if (db->graphExec) {
+                cudaGraphExecUpdateResultInfo info;
+                updated = cudaGraphExecUpdate(db->graphExec, g, &info) == cudaSuccess;
+                if (!updated) {
+                    cudaGetLastError();
+                    cudaGraphExecDestroy(db->graphExec);
+                    db->graphExec = nullptr;
+                }
+            }
+            if (!updated) {
+                const cudaError_t ie = cudaGraphInstantiate(&db->graphExec, g, 0);
+                cudaGraphDestroy(g);
+                CUDA_TRY(ie);
+            } else {
+                cudaGraphDestroy(g);
+            }
+            db->graphKey = key;
+            db->graphCaptures++;
+        }
+        db->launchesPerRun = (nTasks > 0 ? 2 : 0) + (int) plan.size();
+        CUDA_TRY(cudaEventRecord(e->ev0, st));
+        CUDA_TRY(cudaGraphLaunch(db->graphExec, st));
+        CUDA_TRY(cudaEventRecord(e->ev1, st));
+    } else {
+        CUDA_TRY(cudaEventRecord(e->ev0, st));
+        MP_TRY(issuePass(false));
+        CUDA_TRY(cudaEventRecord(e->ev1, st));
+    }
     // statuses
     db->hostOut.resize(nTasks);
     if (nTasks) CUDA_TRY(cudaMemcpyAsync(db->hostOut.data(), db->dOut.p, sizeof(TaskOut) * nTasks, cudaMemcpyDeviceToHost, st));

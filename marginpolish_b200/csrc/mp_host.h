@@ -69,6 +69,7 @@ struct mp_engine {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     mp_tuning tuning{};
+    bool graphs = false;  // device-batch passes run as captured CUDA graphs
     // autotuned choice (mp_engine_autotune): ascending hull-class bounds with the FP32 kernel
     // variant of each class, and warps per block per variant (0: as many as fit); empty when
     // not tuned

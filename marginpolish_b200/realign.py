@@ -67,6 +67,10 @@ class Engine:
                                   "checkpoint_stride", "warps_per_block", "gcups", "default_gcups")})
         return out
 
+    def set_graph_capture(self, enable: bool = True) -> None:
+        """Runs device-batch passes as captured CUDA graphs (replayed while identical)."""
+        _lib.check(self._lib.mp_engine_set_graph_capture(self.handle, 1 if enable else 0))
+
     def autotune_reset(self) -> None:
         """Restores the built-in kernel choice."""
         _lib.check(self._lib.mp_engine_autotune_reset(self.handle))

@@ -40,7 +40,7 @@ FLOP_PER_CELL = 48  # 30 FP32 FMA-pipe instructions per cell (forward 12, backwa
 # DRAM bytes (read + write) per band cell of the posterior kernel, from one ncu capture of the
 # same kernel on a 24-chunk slice of the workload (profiles/posteriorKernel_batched24_full.md);
 # traffic grows with cells, so a full launch moves this times its cells.
-DRAM_BYTES_PER_CELL = 6.07
+DRAM_BYTES_PER_CELL = 6.09
 METRIC = "GCUPS fwd+bwd+posterior (batched FP32 vs plain GPU, ≤1e-4 vs FP64); CPU ref"
 
 
@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--lanes", type=int, default=0, choices=[0, 8, 16, 32],
                     help="lanes per banded sub-problem (0 = the engine's automatic choice)")
     ap.add_argument("--warps", type=int, default=0, help="warps per block of the posterior kernel (0 = automatic)")
+    ap.add_argument("--no-graphs", action="store_true", help="direct launches instead of CUDA graph replay")
+    ap.add_argument("--autotune-chunks", type=int, default=24,
+                    help="chunks of the separate seeded sample the autotuner times the kernel variants on (0 = off)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the adjoint and POA-loop measurements reported beside the headline")
     return ap.parse_args()
@@ -316,6 +319,21 @@ def run_ours(args, rank, world, local):
     engine = Engine(local)
     engine.set_tuning(warps_per_block=args.warps, lanes_per_task=args.lanes)
     model = Model.from_polish(engine, pm)
+    # autotuner: kernel variant (band tile, checkpoint stride) and warps per hull class, timed on
+    # a separate sample of the same kind of batch (outside the timed region)
+    tuned = None
+    if args.autotune_chunks > 0 and args.lanes == 0 and args.warps == 0 and args.config == "batched":
+        from marginpolish_b200 import synth
+        t1 = time.perf_counter()
+        sample = synth.config_batched(seed=args.seed + 1000 + rank, n_chunks=args.autotune_chunks).jobs()
+        rep = engine.autotune(model, pm.alignment, sample)
+        tuned = {"sample_chunks": args.autotune_chunks, "seconds": round(time.perf_counter() - t1, 1),
+                 "classes": [{k: (round(r[k], 1) if k.endswith("gcups") else r[k])
+                              for k in ("max_hull", "tasks", "candidates", "variant", "lanes_per_task",
+                                        "cells_per_lane", "checkpoint_stride", "warps_per_block", "gcups",
+                                        "default_gcups")} for r in rep if r["candidates"] > 0]}
+    if not args.no_graphs:
+        engine.set_graph_capture(True)
     db = DeviceBatch(engine, model, pm.alignment, jobs)
 
     def barrier():
@@ -418,7 +436,9 @@ def run_ours(args, rank, world, local):
                        "tasks": n_tasks, "l2": "inputs and band/scratch/output buffers exceed the 126 MB L2",
                        "generation_s": round(gen_s, 1), "band_ms": float(np.median(band_ms)),
                        "posterior_ms": post, "wall_s_timed": wall,
-                       "tuning": {"lanes_per_task": args.lanes or "auto", "warps_per_block": args.warps or "auto"}},
+                       "tuning": {"lanes_per_task": args.lanes or "auto", "warps_per_block": args.warps or "auto",
+                                  "autotune": tuned},
+                       "launch": "direct" if args.no_graphs else "CUDA graph replay of the pass's launches"},
             "e2e": e2e,
             "gpu_launches": launches * args.steps,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

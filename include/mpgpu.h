@@ -191,6 +191,7 @@ mp_status mp_engine_autotune_reset(mp_engine *e);
 mp_status mp_realign_batch(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
                            mp_result **out);
 mp_status mp_result_view_get(const mp_result *r, mp_result_view *v);
+
 void mp_result_destroy(mp_result *r);
 
 /* ---- device-resident path (inputs already in HBM; used for kernel timing) ---- */
@@ -221,6 +222,18 @@ typedef struct {
 mp_status mp_device_batch_counts(const mp_device_batch *db, int64_t totals[3]);
 /* Copies the last run's results into caller-owned host arrays (no allocation on the host). */
 mp_status mp_device_batch_fetch_into(mp_engine *e, mp_device_batch *db, const mp_output *out);
+/* The end-to-end pass of mp_realign_batch, pipelined for throughput, into caller-owned arrays. The jobs are
+ * cut into `parts` contiguous slices of similar work (0: automatic, 4 for large batches).
+ * Two device batches on two streams take the slices in turn, so one slice's input copies and
+ * kernels overlap the previous slice's compaction and tuple copies. Page-locked output arrays
+ * (mp_host_alloc) are needed for the copies to overlap. `out` receives offsets,
+ * log-likelihoods and cells for every job and the tuples of list k at weight/x/y[k], which
+ * hold cap[k] tuples. A list that needs more gets no tuples; the call then returns
+ * MP_ERR_OVERFLOW. need[k] (need may be NULL) receives the totals, so the caller can grow its
+ * arrays and call again. The results equal mp_realign_batch's. The batch's host arrays must
+ * stay valid until the call returns. */
+mp_status mp_realign_batch_into(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
+                                int32_t parts, const mp_output *out, const int64_t cap[3], int64_t need[3]);
 /* Page-locked host memory for inputs and outputs (cudaHostAlloc / cudaFreeHost). */
 mp_status mp_host_alloc(size_t bytes, void **out);
 void mp_host_free(void *p);

@@ -5,14 +5,15 @@ from . import _lib
 from .params import AlignmentParams, PolishModel, StateModel, build_state_model, load_polish_model
 from .realign import (DeviceBatch, Engine, Expectations, Jobs, Model, Pairs, compute_forward_probability,
                       expectations_batch, forward_batch, get_aligned_pairs_using_anchors,
-                      get_aligned_pairs_with_indels_using_anchors, realign_batch)
+                      get_aligned_pairs_with_indels_using_anchors, realign_batch,
+                      realign_batch_pipelined)
 from .rle import RleString, crop_range, rle_anchors
 from .poa import PoaSet, PolishParams, polish
 
 __all__ = [
     "AlignmentParams", "PolishModel", "StateModel", "build_state_model", "load_polish_model", "DeviceBatch",
     "Engine", "Jobs", "Model", "Pairs", "get_aligned_pairs_using_anchors",
-    "get_aligned_pairs_with_indels_using_anchors", "realign_batch", "RleString", "crop_range", "rle_anchors",
+    "get_aligned_pairs_with_indels_using_anchors", "realign_batch", "realign_batch_pipelined", "RleString", "crop_range", "rle_anchors",
     "compute_forward_probability", "forward_batch", "expectations_batch", "Expectations", "PoaSet", "PolishParams",
     "polish",
 ]

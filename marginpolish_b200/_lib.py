@@ -205,7 +205,7 @@ EXPORTED = [
     "mp_poa_set_realign_all", "mp_poa_set_estimate_repeat_counts", "mp_poa_info", "mp_poa_nodes",
     "mp_poa_observations", "mp_poa_inserts", "mp_poa_deletes", "mp_poa_reference", "mp_poa_consensus",
     "mp_poa_anchor_alignments", "mp_engine_autotune", "mp_engine_autotune_reset",
-    "mp_engine_set_graph_capture",
+    "mp_engine_set_graph_capture", "mp_realign_batch_into",
 ]
 
 _lib = None
@@ -244,6 +244,8 @@ def load() -> ctypes.CDLL:
         "mp_device_batch_reset": (c_int, [c_void_p, c_void_p, P(Params), P(Batch)]),
         "mp_device_batch_counts": (c_int, [c_void_p, P(c_int64)]),
         "mp_device_batch_fetch_into": (c_int, [c_void_p, c_void_p, P(Output)]),
+        "mp_realign_batch_into": (c_int, [c_void_p, c_void_p, P(Params), P(Batch), ctypes.c_int32, P(Output),
+                                          P(c_int64), P(c_int64)]),
         "mp_host_alloc": (c_int, [ctypes.c_size_t, P(c_void_p)]),
         "mp_host_free": (None, [c_void_p]),
         "mp_device_batch_run_plain": (c_int, [c_void_p, c_void_p, c_int64, P(c_float), P(c_int64)]),

@@ -126,6 +126,10 @@ extern "C" void mp_engine_destroy(mp_engine *e) {
     mp_device_batch_destroy(e->forwardShot);
     mp_device_batch_destroy(e->adjointShot);
     e->oneShot = e->forwardShot = e->adjointShot = nullptr;
+    for (int k = 0; k < 2; k++) {
+        mp_device_batch_destroy(e->pipe[k]);  // destroys its own stream
+        e->pipe[k] = nullptr;
+    }
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }
@@ -527,12 +531,21 @@ struct mp_device_batch {
     bool ran = false;
     float bandMs = 0.0f, posteriorMs = 0.0f;
     cudaEvent_t evBand = nullptr;
+    cudaStream_t stream = nullptr;          // the batch's stream (the engine's unless a pipelined call set one)
+    bool ownStream = false;                 // `stream` was created for this batch
+    TaskOut *pinOut = nullptr;              // page-locked copy of the task statuses
+    size_t pinOutCap = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaGraphExec_t graphExec = nullptr;  // the pass's launches (engine graph capture on)
     std::vector<unsigned char> graphKey;  // their arguments when captured
     int graphCaptures = 0;
     ~mp_device_batch() {
         if (graphExec) cudaGraphExecDestroy(graphExec);
         if (evBand) cudaEventDestroy(evBand);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (pinOut) cudaFreeHost(pinOut);
+        if (ownStream && stream) cudaStreamDestroy(stream);
     }
 };
 
@@ -738,8 +751,8 @@ static int modeMaxHullSlots(const mp_device_batch *db) {
 static mp_status zeroExpectations(mp_device_batch *db) {
     MP_TRY(db->expect.reserve(sizeof(double) * 2 * kExpPerModel));
     MP_TRY(db->expectRep.reserve(sizeof(double) * 2 * kRepTable));
-    CUDA_TRY(cudaMemsetAsync(db->expect.p, 0, sizeof(double) * 2 * kExpPerModel, db->e->stream));
-    CUDA_TRY(cudaMemsetAsync(db->expectRep.p, 0, sizeof(double) * 2 * kRepTable, db->e->stream));
+    CUDA_TRY(cudaMemsetAsync(db->expect.p, 0, sizeof(double) * 2 * kExpPerModel, db->stream));
+    CUDA_TRY(cudaMemsetAsync(db->expectRep.p, 0, sizeof(double) * 2 * kRepTable, db->stream));
     return MP_OK;
 }
 
@@ -795,7 +808,7 @@ static mp_status upload(DevBuf &buf, const void *src, size_t bytes, cudaStream_t
 // Plans a batch into `db` and uploads it, reusing the device buffers db already holds
 // (they only grow).
 static mp_status batchReset(mp_engine *e, mp_device_batch *db, const mp_model *m, const mp_params *p,
-                            const mp_batch *b) {
+                            const mp_batch *b, bool syncInputs = true) {
     MP_TRY(validateParams(p));
     if (b->n_jobs < 0) return failf(MP_ERR_ARGUMENT, "negative job count");
     if (b->n_jobs > 0 && (!b->x_begin || !b->x_end || !b->y_offsets || !b->anchor_offsets || !b->strand))
@@ -803,13 +816,16 @@ static mp_status batchReset(mp_engine *e, mp_device_batch *db, const mp_model *m
     CUDA_TRY(cudaSetDevice(e->device));
     db->e = e;
     db->device = e->device;
+    if (!db->stream) db->stream = e->stream;
+    if (!db->ev0) CUDA_TRY(cudaEventCreate(&db->ev0));
+    if (!db->ev1) CUDA_TRY(cudaEventCreate(&db->ev1));
     db->m = m;
     db->p = *p;
     db->nJobs = b->n_jobs;
     db->ran = false;
     db->hostOut.clear();
     MP_TRY(planBatch(db, b));
-    cudaStream_t st = e->stream;
+    cudaStream_t st = db->stream;
     int64_t ny = b->n_jobs > 0 ? b->y_offsets[b->n_jobs] : 0;
     int64_t na = b->n_jobs > 0 ? b->anchor_offsets[b->n_jobs] : 0;
     MP_TRY(upload(db->xs, b->x_symbols, sizeof(uint16_t) * b->x_symbols_length, st));
@@ -822,8 +838,9 @@ static mp_status batchReset(mp_engine *e, mp_device_batch *db, const mp_model *m
         MP_TRY(db->outT[k].reserve(sizeof(int4) * std::max<int64_t>(db->outCap[k], 1)));
     }
     MP_TRY(db->queue.reserve(sizeof(int32_t) * variantCount()));
-    // the caller's host arrays may be reused as soon as this returns
-    CUDA_TRY(cudaStreamSynchronize(st));
+    // the caller's host arrays may be reused as soon as this returns (unless the caller keeps
+    // them valid until its own synchronisation)
+    if (syncInputs) CUDA_TRY(cudaStreamSynchronize(st));
     return MP_OK;
 }
 
@@ -858,7 +875,7 @@ struct QueueLaunch {
 // longest task.
 static mp_status planQueues(mp_device_batch *db, std::vector<QueueLaunch> &plan) {
     mp_engine *e = db->e;
-    cudaStream_t st = e->stream;
+    cudaStream_t st = db->stream;
     plan.clear();
     const int nV = modeVariantCount(db);
     const bool adj = db->mode == kModeAdjoint;
@@ -927,7 +944,7 @@ static mp_status planQueues(mp_device_batch *db, std::vector<QueueLaunch> &plan)
 
 // Issues planned posterior launches (stream-ordered only: capturable into a CUDA graph).
 static mp_status issueQueues(mp_device_batch *db, const std::vector<QueueLaunch> &plan) {
-    cudaStream_t st = db->e->stream;
+    cudaStream_t st = db->stream;
     const bool adj = db->mode == kModeAdjoint;
     CUDA_TRY(cudaMemsetAsync(db->queue.p, 0, sizeof(int32_t) * modeVariantCount(db), st));
     for (const QueueLaunch &q : plan) {
@@ -951,10 +968,11 @@ static void keyAppend(std::vector<unsigned char> &key, const T &v) {
     key.insert(key.end(), b, b + sizeof(T));
 }
 
-extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, float *kernelMs) {
-    if (!e || !db) return failf(MP_ERR_ARGUMENT, "mp_device_batch_run: NULL argument");
+// Issues a run's launches and the copy of its task statuses on the batch's stream, without
+// waiting for them.
+static mp_status runIssue(mp_engine *e, mp_device_batch *db) {
     CUDA_TRY(cudaSetDevice(e->device));
-    cudaStream_t st = e->stream;
+    cudaStream_t st = db->stream;
     const int nTasks = (int) db->tasks.size();
     db->launchesPerRun = 0;
     std::vector<int32_t> all(nTasks), orderHost;
@@ -985,8 +1003,9 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
         if (db->mode == kModeAdjoint) MP_TRY(zeroExpectations(db));
         return issueQueues(db, plan);
     };
-    if (e->graphs) {
-        // One CUDA graph per batch: replayed while the launches are identical (repeated runs),
+    if (e->graphs && !db->ownStream) {
+        // One CUDA graph per batch (the pipelined slices of mp_realign_batch_into change every
+        // call and run direct): replayed while the launches are identical (repeated runs),
         // re-captured and updated in place when they change.
         std::vector<unsigned char> key;
         keyAppend(key, db->mode);
@@ -1028,22 +1047,38 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
             db->graphCaptures++;
         }
         db->launchesPerRun = (nTasks > 0 ? 2 : 0) + (int) plan.size();
-        CUDA_TRY(cudaEventRecord(e->ev0, st));
+        CUDA_TRY(cudaEventRecord(db->ev0, st));
         CUDA_TRY(cudaGraphLaunch(db->graphExec, st));
-        CUDA_TRY(cudaEventRecord(e->ev1, st));
+        CUDA_TRY(cudaEventRecord(db->ev1, st));
     } else {
-        CUDA_TRY(cudaEventRecord(e->ev0, st));
+        CUDA_TRY(cudaEventRecord(db->ev0, st));
         MP_TRY(issuePass(false));
-        CUDA_TRY(cudaEventRecord(e->ev1, st));
+        CUDA_TRY(cudaEventRecord(db->ev1, st));
     }
-    // statuses
-    db->hostOut.resize(nTasks);
-    if (nTasks) CUDA_TRY(cudaMemcpyAsync(db->hostOut.data(), db->dOut.p, sizeof(TaskOut) * nTasks, cudaMemcpyDeviceToHost, st));
+    // statuses, into page-locked memory so that the copy does not wait on the host
+    if ((size_t) nTasks > db->pinOutCap) {
+        if (db->pinOut) cudaFreeHost(db->pinOut);
+        db->pinOut = nullptr;
+        db->pinOutCap = 0;
+        CUDA_TRY(cudaMallocHost(&db->pinOut, sizeof(TaskOut) * (size_t) nTasks));
+        db->pinOutCap = (size_t) nTasks;
+    }
+    if (nTasks) CUDA_TRY(cudaMemcpyAsync(db->pinOut, db->dOut.p, sizeof(TaskOut) * nTasks, cudaMemcpyDeviceToHost, st));
+    return MP_OK;
+}
+
+// Waits for an issued run, re-runs the tasks that need it (capacity, window, range, scratch)
+// and marks the batch ran.
+static mp_status runFinish(mp_engine *e, mp_device_batch *db, float *kernelMs) {
+    cudaStream_t st = db->stream;
+    const int nTasks = (int) db->tasks.size();
+    std::vector<int32_t> orderHost;
     CUDA_TRY(cudaStreamSynchronize(st));
+    db->hostOut.assign(db->pinOut, db->pinOut + nTasks);
     float ms = 0.0f;
-    CUDA_TRY(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
-    CUDA_TRY(cudaEventElapsedTime(&db->bandMs, e->ev0, db->evBand));
-    CUDA_TRY(cudaEventElapsedTime(&db->posteriorMs, db->evBand, e->ev1));
+    CUDA_TRY(cudaEventElapsedTime(&ms, db->ev0, db->ev1));
+    CUDA_TRY(cudaEventElapsedTime(&db->bandMs, db->ev0, db->evBand));
+    CUDA_TRY(cudaEventElapsedTime(&db->posteriorMs, db->evBand, db->ev1));
     // retries: capacity overflows (exact counts known), window overflows (next wider variant), scratch
     for (int round = 0; round < 4; round++) {
         std::vector<int32_t> retry;
@@ -1118,13 +1153,13 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
         CUDA_TRY(cudaMemcpyAsync(db->dOut.p, db->hostOut.data(), sizeof(TaskOut) * nTasks, cudaMemcpyHostToDevice, st));
         MP_TRY(buildQueues(db, retry, orderHost));
         MP_TRY(upload(db->orders, orderHost.data(), sizeof(int32_t) * std::max<size_t>(orderHost.size(), 1), st));
-        CUDA_TRY(cudaEventRecord(e->ev0, st));
+        CUDA_TRY(cudaEventRecord(db->ev0, st));
         MP_TRY(launchQueues(db));
-        CUDA_TRY(cudaEventRecord(e->ev1, st));
+        CUDA_TRY(cudaEventRecord(db->ev1, st));
         CUDA_TRY(cudaMemcpyAsync(db->hostOut.data(), db->dOut.p, sizeof(TaskOut) * nTasks, cudaMemcpyDeviceToHost, st));
         CUDA_TRY(cudaStreamSynchronize(st));
         float ms2 = 0.0f;
-        CUDA_TRY(cudaEventElapsedTime(&ms2, e->ev0, e->ev1));
+        CUDA_TRY(cudaEventElapsedTime(&ms2, db->ev0, db->ev1));
         ms += ms2;
         db->posteriorMs += ms2;
     }
@@ -1137,6 +1172,12 @@ extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, floa
     return MP_OK;
 }
 
+extern "C" mp_status mp_device_batch_run(mp_engine *e, mp_device_batch *db, float *kernelMs) {
+    if (!e || !db) return failf(MP_ERR_ARGUMENT, "mp_device_batch_run: NULL argument");
+    MP_TRY(runIssue(e, db));
+    return runFinish(e, db, kernelMs);
+}
+
 // The plain form of the same computation, for comparison: band kernels for the batch,
 // then one posterior launch per task (one block of one warp, no persistent queue), in
 // batch order, for the first max_tasks tasks. Returns the CUDA-event time of the
@@ -1145,7 +1186,7 @@ extern "C" mp_status mp_device_batch_run_plain(mp_engine *e, mp_device_batch *db
                                                int64_t *cells) {
     if (!e || !db) return failf(MP_ERR_ARGUMENT, "mp_device_batch_run_plain: NULL argument");
     CUDA_TRY(cudaSetDevice(e->device));
-    cudaStream_t st = e->stream;
+    cudaStream_t st = db->stream;
     const int nTasks = (int) db->tasks.size();
     const int n = (int) std::max<int64_t>(0, std::min<int64_t>(max_tasks, nTasks));
     std::vector<int32_t> all(nTasks), orderHost;
@@ -1176,7 +1217,7 @@ extern "C" mp_status mp_device_batch_run_plain(mp_engine *e, mp_device_batch *db
     MP_TRY(db->scratchScal.reserve(needScal));
     MP_TRY(db->queue.reserve(sizeof(int32_t) * std::max(n, 1)));
     CUDA_TRY(cudaMemsetAsync(db->queue.p, 0, sizeof(int32_t) * std::max(n, 1), st));
-    CUDA_TRY(cudaEventRecord(e->ev0, st));
+    CUDA_TRY(cudaEventRecord(db->ev0, st));
     for (int t = 0; t < n; t++) {
         int C = 0, L = 0, K = 0;
         const int v = db->var[t];
@@ -1204,12 +1245,12 @@ extern "C" mp_status mp_device_batch_run_plain(mp_engine *e, mp_device_batch *db
         a.sharedRepeat = db->m->sharedRepeat;
         CUDA_TRY(launchVariant(v, a, 1, 1, st));
     }
-    CUDA_TRY(cudaEventRecord(e->ev1, st));
+    CUDA_TRY(cudaEventRecord(db->ev1, st));
     std::vector<TaskOut> host(std::max(nTasks, 1));
     if (nTasks) CUDA_TRY(cudaMemcpyAsync(host.data(), db->dOut.p, sizeof(TaskOut) * nTasks, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     float ms = 0.0f;
-    CUDA_TRY(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+    CUDA_TRY(cudaEventElapsedTime(&ms, db->ev0, db->ev1));
     int64_t c = 0;
     for (int t = 0; t < n; t++) {
         if (host[t].status != 0)
@@ -1312,18 +1353,31 @@ static void fetchLayout(const mp_device_batch *db, int64_t total[3], std::vector
     }
 }
 
-// Compacts every task's tuples into the batch's staging lists and copies them into the
-// caller's host arrays (page-locked ones are copied by DMA at full link speed).
-static mp_status fetchInto(mp_engine *e, mp_device_batch *db, const mp_output *out) {
+// Compacts every task's tuples into the batch's staging lists and queues their copies into
+// the caller's host arrays (page-locked ones are copied by DMA at full link speed), without
+// waiting for them. The batch's jobs are jobs j0.. of the caller's arrays and its tuples of
+// list k start at tuple base[k]; a list whose tuples would pass cap[k] (cap may be NULL: no
+// limit) is not copied. total[k] receives the batch's tuple counts.
+static mp_status fetchIssue(mp_engine *e, mp_device_batch *db, const mp_output *out, int64_t j0,
+                            const int64_t base[3], const int64_t *cap, int64_t total[3]) {
     if (!db->ran) return failf(MP_ERR_STATE, "fetch before a successful run");
     CUDA_TRY(cudaSetDevice(e->device));
-    cudaStream_t st = e->stream;
+    cudaStream_t st = db->stream;
     const int nTasks = (int) db->tasks.size();
-    int64_t total[3];
-    std::vector<int64_t> dst[3];
-    fetchLayout(db, total, dst, out->offsets, out->log_likelihood, out->cells);
+    std::vector<int64_t> dst[3], off[3];
+    int64_t *offp[3];
     for (int k = 0; k < 3; k++) {
-        if (total[k] > 0 && (!out->weight[k] || !out->x[k] || !out->y[k]))
+        off[k].assign(db->nJobs + 1, 0);
+        offp[k] = off[k].data();
+    }
+    fetchLayout(db, total, dst, offp, out->log_likelihood ? out->log_likelihood + j0 : nullptr,
+                out->cells ? out->cells + j0 : nullptr);
+    bool copy[3];
+    for (int k = 0; k < 3; k++) {
+        if (out->offsets[k])
+            for (int64_t j = 0; j <= db->nJobs; j++) out->offsets[k][j0 + j] = base[k] + off[k][j];
+        copy[k] = total[k] > 0 && (!cap || base[k] + total[k] <= cap[k]);
+        if (copy[k] && (!out->weight[k] || !out->x[k] || !out->y[k]))
             return failf(MP_ERR_ARGUMENT, "output arrays of list %d missing", k);
         MP_TRY(upload(db->fetchDst[k], dst[k].data(), sizeof(int64_t) * dst[k].size(), st));
         const size_t n = sizeof(int32_t) * std::max<int64_t>(total[k], 1);
@@ -1346,13 +1400,20 @@ static mp_status fetchInto(mp_engine *e, mp_device_batch *db, const mp_output *o
         CUDA_TRY(launchCompact(ca, st));
     }
     for (int k = 0; k < 3; k++) {
-        if (!total[k]) continue;
+        if (!copy[k]) continue;
         const size_t n = sizeof(int32_t) * total[k];
-        CUDA_TRY(cudaMemcpyAsync(out->weight[k], db->fetchW[k].p, n, cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(cudaMemcpyAsync(out->x[k], db->fetchX[k].p, n, cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(cudaMemcpyAsync(out->y[k], db->fetchY[k].p, n, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(out->weight[k] + base[k], db->fetchW[k].p, n, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(out->x[k] + base[k], db->fetchX[k].p, n, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(out->y[k] + base[k], db->fetchY[k].p, n, cudaMemcpyDeviceToHost, st));
     }
-    CUDA_TRY(cudaStreamSynchronize(st));
+    return MP_OK;
+}
+
+static mp_status fetchInto(mp_engine *e, mp_device_batch *db, const mp_output *out) {
+    const int64_t base[3] = {0, 0, 0};
+    int64_t total[3];
+    MP_TRY(fetchIssue(e, db, out, 0, base, nullptr, total));
+    CUDA_TRY(cudaStreamSynchronize(db->stream));
     return MP_OK;
 }
 
@@ -1421,7 +1482,7 @@ extern "C" void mp_device_batch_destroy(mp_device_batch *db) {
 static mp_status timeCandidate(mp_device_batch *db, const std::vector<int32_t> &subset, int64_t cells, int v,
                                int warps, int reps, double *gcups) {
     mp_engine *e = db->e;
-    cudaStream_t st = e->stream;
+    cudaStream_t st = db->stream;
     int C = 0, L = 0, K = 0;
     variantShape(v, &C, &L, &K);
     const int loads = ((int) subset.size() + 32 / L - 1) / (32 / L);
@@ -1435,13 +1496,13 @@ static mp_status timeCandidate(mp_device_batch *db, const std::vector<int32_t> &
         s = upload(db->orders, orderHost.data(), sizeof(int32_t) * std::max<size_t>(orderHost.size(), 1), st);
     float best = 0.0f;
     for (int r = 0; s == MP_OK && r <= reps; r++) {
-        if (cudaEventRecord(e->ev0, st) != cudaSuccess) s = failf(MP_ERR_CUDA, "event record failed");
+        if (cudaEventRecord(db->ev0, st) != cudaSuccess) s = failf(MP_ERR_CUDA, "event record failed");
         if (s == MP_OK) s = launchQueues(db);
-        if (s == MP_OK && cudaEventRecord(e->ev1, st) != cudaSuccess) s = failf(MP_ERR_CUDA, "event record failed");
+        if (s == MP_OK && cudaEventRecord(db->ev1, st) != cudaSuccess) s = failf(MP_ERR_CUDA, "event record failed");
         if (s == MP_OK && cudaStreamSynchronize(st) != cudaSuccess)
             s = failf(MP_ERR_CUDA, "autotune launch failed: %s", cudaGetErrorString(cudaGetLastError()));
         float ms = 0.0f;
-        if (s == MP_OK && cudaEventElapsedTime(&ms, e->ev0, e->ev1) != cudaSuccess)
+        if (s == MP_OK && cudaEventElapsedTime(&ms, db->ev0, db->ev1) != cudaSuccess)
             s = failf(MP_ERR_CUDA, "event timing failed");
         if (s == MP_OK && r > 0 && (best == 0.0f || ms < best)) best = ms;
     }
@@ -1589,6 +1650,106 @@ extern "C" mp_status mp_realign_batch(mp_engine *e, const mp_model *m, const mp_
     MP_TRY(mp_device_batch_run(e, db, &ms));
     MP_TRY(mp_device_batch_fetch(e, db, out));
     (*out)->deviceMs = ms;
+    return MP_OK;
+}
+
+// Slices [cut[i], cut[i+1]) of a batch's jobs with similar work (template + read symbols).
+static std::vector<int64_t> sliceJobs(const mp_batch *b, int parts) {
+    const int64_t n = b->n_jobs;
+    std::vector<int64_t> cut(1, 0);
+    int64_t work = 0;
+    for (int64_t j = 0; j < n; j++) work += (b->x_end[j] - b->x_begin[j]) + (b->y_offsets[j + 1] - b->y_offsets[j]);
+    int64_t acc = 0;
+    for (int64_t j = 0; j < n && (int) cut.size() < parts; j++) {
+        acc += (b->x_end[j] - b->x_begin[j]) + (b->y_offsets[j + 1] - b->y_offsets[j]);
+        if (acc * parts >= work * (int64_t) cut.size() && j + 1 < n) cut.push_back(j + 1);
+    }
+    cut.push_back(n);
+    return cut;
+}
+
+extern "C" mp_status mp_realign_batch_into(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
+                                           int32_t parts, const mp_output *out, const int64_t cap[3], int64_t need[3]) {
+    if (!e || !m || !p || !b || !out || !cap) return failf(MP_ERR_ARGUMENT, "mp_realign_batch_into: NULL argument");
+    if (b->n_jobs < 0) return failf(MP_ERR_ARGUMENT, "negative job count");
+    if (b->n_jobs > 0 && (!b->x_begin || !b->x_end || !b->y_offsets || !b->anchor_offsets || !b->strand))
+        return failf(MP_ERR_ARGUMENT, "batch arrays missing");
+    std::lock_guard<std::mutex> guard(e->oneShotLock);
+    CUDA_TRY(cudaSetDevice(e->device));
+    const int64_t n = b->n_jobs;
+    if (parts <= 0) parts = n >= 2048 ? 4 : 1;
+    parts = (int32_t) std::max<int64_t>(1, std::min<int64_t>(parts, std::max<int64_t>(n, 1)));
+    for (int k = 0; k < 2; k++) {
+        if (e->pipe[k]) continue;
+        mp_device_batch *db = new mp_device_batch();
+        if (cudaStreamCreateWithFlags(&db->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            db->stream = nullptr;
+            delete db;
+            return failf(MP_ERR_CUDA, "stream creation failed");
+        }
+        db->ownStream = true;
+        e->pipe[k] = db;
+    }
+    const std::vector<int64_t> cut = sliceJobs(b, parts);
+    const int nSlices = (int) cut.size() - 1;
+    int64_t base[3] = {0, 0, 0};
+    bool over[3] = {false, false, false};
+    for (int k = 0; k < 3; k++)
+        if (out->offsets[k]) out->offsets[k][0] = 0;
+    // finishes slice i (waits for its run, re-runs what needs it) and queues its tuple copies
+    auto finish = [&](int i) -> mp_status {
+        mp_device_batch *db = e->pipe[i % 2];
+        MP_TRY(runFinish(e, db, nullptr));
+        int64_t total[3];
+        MP_TRY(fetchIssue(e, db, out, cut[i], base, cap, total));
+        for (int k = 0; k < 3; k++) {
+            if (base[k] + total[k] > cap[k]) over[k] = true;
+            base[k] += total[k];
+        }
+        return MP_OK;
+    };
+    mp_status st = MP_OK;
+    int pending = -1;
+    for (int i = 0; st == MP_OK && i < nSlices; i++) {
+        const int64_t j0 = cut[i], j1 = cut[i + 1];
+        std::vector<int64_t> yOff(j1 - j0 + 1), aOff(j1 - j0 + 1);
+        for (int64_t j = j0; j <= j1; j++) {
+            yOff[j - j0] = b->y_offsets[j] - b->y_offsets[j0];
+            aOff[j - j0] = b->anchor_offsets[j] - b->anchor_offsets[j0];
+        }
+        mp_batch sb = *b;
+        sb.n_jobs = j1 - j0;
+        sb.x_begin = b->x_begin + j0;
+        sb.x_end = b->x_end + j0;
+        sb.y_offsets = yOff.data();
+        sb.y_symbols = b->y_symbols ? b->y_symbols + b->y_offsets[j0] : nullptr;
+        sb.anchor_offsets = aOff.data();
+        sb.anchors = b->anchors ? b->anchors + 3 * b->anchor_offsets[j0] : nullptr;
+        sb.strand = b->strand + j0;
+        sb.ragged_left = b->ragged_left ? b->ragged_left + j0 : nullptr;
+        sb.ragged_right = b->ragged_right ? b->ragged_right + j0 : nullptr;
+        sb.x_shift = b->x_shift ? b->x_shift + j0 : nullptr;
+        mp_device_batch *db = e->pipe[i % 2];
+        db->mode = kModePosterior;
+        // the slot's previous slice has queued its copies on the same stream: the new inputs
+        // follow them in stream order; the batch's host arrays stay valid until the return
+        st = batchReset(e, db, m, p, &sb, false);
+        if (st == MP_OK) st = runIssue(e, db);
+        if (st == MP_OK && pending >= 0) st = finish(pending);
+        pending = i;
+    }
+    if (st == MP_OK && pending >= 0) st = finish(pending);
+    for (int k = 0; k < 2; k++) {
+        const cudaError_t ce = cudaStreamSynchronize(e->pipe[k]->stream);
+        if (st == MP_OK && ce != cudaSuccess)
+            st = failf(MP_ERR_CUDA, "pipelined pass failed: %s", cudaGetErrorString(ce));
+    }
+    if (st != MP_OK) return st;
+    if (need)
+        for (int k = 0; k < 3; k++) need[k] = base[k];
+    if (over[0] || over[1] || over[2])
+        return failf(MP_ERR_OVERFLOW, "output capacity too small: need %lld / %lld / %lld tuples",
+                     (long long) base[0], (long long) base[1], (long long) base[2]);
     return MP_OK;
 }
 

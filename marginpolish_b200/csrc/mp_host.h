@@ -77,6 +77,7 @@ struct mp_engine {
     struct mp_device_batch *oneShot = nullptr;  // reused by the one-shot calls (mp_realign_batch*)
     struct mp_device_batch *forwardShot = nullptr;  // reused by mp_forward_batch
     struct mp_device_batch *adjointShot = nullptr;  // reused by mp_expectations_batch
+    struct mp_device_batch *pipe[2] = {nullptr, nullptr};  // the two slots of mp_realign_batch_into (own streams)
     std::mutex oneShotLock;
 };
 

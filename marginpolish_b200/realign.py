@@ -339,6 +339,31 @@ def realign_batch(engine: Engine, model: Model, params: AlignmentParams, jobs: J
     return db.fetch_into(out if out is not None else OutputBuffer(pinned=False), ms)
 
 
+def realign_batch_pipelined(engine: Engine, model: Model, params: AlignmentParams, jobs: Jobs,
+                            out: Optional[OutputBuffer] = None, parts: int = 0) -> Pairs:
+    """The same pass as realign_batch, pipelined (mp_realign_batch_into): slices of the jobs
+    alternate between two streams so that one slice's copies overlap another's kernels. Results
+    go into `out` (page-locked by default; grown and the call repeated when a list does not
+    fit) and are returned as views of it."""
+    out = out if out is not None else OutputBuffer(pinned=True)
+    n = jobs.n_jobs
+    lib = engine._lib
+    ps, bs = params.struct(), jobs.struct()
+    out.ensure(n, [t.shape[1] if t is not None else 0 for t in out._tuples])
+    need = (c_int64 * 3)()
+    for attempt in range(2):
+        o = out.struct()
+        cap = (c_int64 * 3)(*[out._tuples[k].shape[1] for k in range(3)])
+        st = lib.mp_realign_batch_into(engine.handle, model.handle, ctypes.byref(ps), ctypes.byref(bs), int(parts),
+                                       ctypes.byref(o), cap, need)
+        if st == _lib.MP_ERR_OVERFLOW and attempt == 0:
+            out.ensure(n, [int(need[k]) for k in range(3)])
+            continue
+        _lib.check(st)
+        break
+    return out.pairs(n, [int(need[k]) for k in range(3)], 0.0)
+
+
 class DeviceBatch:
     """A batch resident in HBM; ``run`` times only the device work (band + posterior kernels)."""
 

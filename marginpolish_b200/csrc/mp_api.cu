@@ -319,6 +319,12 @@ static bool splitGap(int64_t &x1, int64_t &y1, int64_t x2, int64_t y2, int64_t x
 
 static void splitPoints(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, int64_t maxSize, bool raggedL,
                         bool raggedR, std::vector<SplitRect> &out) {
+    // every gap between anchors is a sub-rectangle of the matrix: none can exceed maxSize when
+    // the whole matrix does not, and then the matrix is one rectangle
+    if (lx * ly <= maxSize) {
+        out.push_back({0, 0, lx, ly});
+        return;
+    }
     int64_t x1 = 0, y1 = 0, x2 = 0, y2 = 0;
     for (int64_t i = 0; i < nA; i++) {
         int64_t x3 = an[3 * i], y3 = an[3 * i + 1];
@@ -480,6 +486,36 @@ static int64_t hullSlotBound(const int32_t *an, int64_t nA, int64_t x1, int64_t 
     return best;
 }
 
+// One pass over a job's anchors for the common case of a single rectangle: validation
+// (strictly increasing, in range, even non-negative expansions when dynamic) and the hull bound
+// of hullSlotBound(an, nA, 0, 0, lx, ly, ...), without branches in the loop. Returns -1 when an
+// anchor is invalid (the caller then reports it through validateJob).
+static int64_t scanSingleRect(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, bool dynamic, int64_t fixedExp) {
+    int64_t lo1 = 0, hi1 = 0, lo2 = 0, hi2 = 0, best = 1;
+    int64_t px = 0, py = 0;  // previous anchor + 1 (0 before the first)
+    int64_t prevX = -1, prevY = -1;
+    unsigned bad = 0;
+    for (int64_t k = 0; k < nA; k++) {
+        const int64_t x = an[3 * k], y = an[3 * k + 1], ex = an[3 * k + 2];
+        bad |= (unsigned) (x <= prevX) | (unsigned) (y <= prevY) | (unsigned) (x >= lx) | (unsigned) (y >= ly);
+        if (dynamic) bad |= (unsigned) (ex < 0) | (unsigned) (ex & 1);
+        const int64_t e = dynamic ? ex : fixedExp;
+        const int64_t nx = x + 1, ny = y + 1;
+        const int64_t lo = std::max(px - ny - e, -ly), hi = std::min(nx - py + e, lx);
+        const int64_t L = std::min(lo, std::min(lo1, lo2)), H = std::max(hi, std::max(hi1, hi2));
+        best = std::max(best, ((H >> 1) - (L >> 1)) + 1);
+        lo2 = lo1, hi2 = hi1, lo1 = lo, hi1 = hi;
+        px = nx, py = ny, prevX = x, prevY = y;
+    }
+    {  // the box from the last anchor to the end
+        const int64_t e = dynamic ? (nA > 0 ? (int64_t) an[3 * (nA - 1) + 2] : 0) : fixedExp;
+        const int64_t lo = std::max(px - ly - e, -ly), hi = std::min(lx - py + e, lx);
+        const int64_t L = std::min(lo, std::min(lo1, lo2)), H = std::max(hi, std::max(hi1, hi2));
+        best = std::max(best, ((H >> 1) - (L >> 1)) + 1);
+    }
+    return bad ? -1 : best;
+}
+
 namespace mp {
 int64_t splitCount(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, int64_t maxSize, bool raggedL, bool raggedR) {
     std::vector<SplitRect> r;
@@ -533,6 +569,11 @@ struct mp_device_batch {
     cudaEvent_t evBand = nullptr;
     cudaStream_t stream = nullptr;          // the batch's stream (the engine's unless a pipelined call set one)
     bool ownStream = false;                 // `stream` was created for this batch
+    // pipelined slots: tuple copies run on their own stream, so that the slot's next inputs and
+    // kernels do not queue behind them; evCopied guards the staging lists until they are copied
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t evCompacted = nullptr, evCopied = nullptr;
+    bool copyPending = false;
     TaskOut *pinOut = nullptr;              // page-locked copy of the task statuses
     size_t pinOutCap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -546,6 +587,9 @@ struct mp_device_batch {
         if (ev1) cudaEventDestroy(ev1);
         if (pinOut) cudaFreeHost(pinOut);
         if (ownStream && stream) cudaStreamDestroy(stream);
+        if (copyStream) cudaStreamDestroy(copyStream);
+        if (evCompacted) cudaEventDestroy(evCompacted);
+        if (evCopied) cudaEventDestroy(evCopied);
     }
 };
 
@@ -630,30 +674,44 @@ static mp_status planBatch(mp_device_batch *db, const mp_batch *b) {
         int64_t j0 = t * chunk, j1 = std::min(nJobs, j0 + chunk);
         std::vector<SplitRect> rects;
         for (int64_t j = j0; j < j1; j++) {
-            mp_status s = validateJob(b, j, p, dynamic);
-            if (s != MP_OK) {
-                statuses[t] = s;
-                errors[t] = g_lastError;
-                return;
-            }
             int64_t lx = b->x_end[j] - b->x_begin[j];
             int64_t ly = b->y_offsets[j + 1] - b->y_offsets[j];
             const int32_t *an = b->anchors + 3 * b->anchor_offsets[j];
             int64_t nA = b->anchor_offsets[j + 1] - b->anchor_offsets[j];
             bool rL = b->ragged_left ? b->ragged_left[j] != 0 : false;
             bool rR = b->ragged_right ? b->ragged_right[j] != 0 : false;
+            // one rectangle (no split possible): validation and hull bound in one pass; the
+            // general path validates first and bounds each rectangle's hull separately
+            const bool whole = forward || lx * ly <= p->split_matrix_bigger_than_this;
+            const bool shapeOk = b->x_begin[j] >= 0 && b->x_end[j] <= b->x_symbols_length && lx >= 0 && ly >= 0 &&
+                                 lx + ly <= ((int64_t) 1 << 30) && b->anchor_offsets[j + 1] >= b->anchor_offsets[j];
+            int64_t wholeHull = -1;
+            if (whole && shapeOk)
+                wholeHull = scanSingleRect(an, nA, lx, ly, dynamic, p->diagonal_expansion);
+            if (wholeHull < 0) {
+                mp_status s = validateJob(b, j, p, dynamic);
+                if (s != MP_OK) {
+                    statuses[t] = s;
+                    errors[t] = g_lastError;
+                    return;
+                }
+            }
             rects.clear();
-            if (forward) rects.push_back(SplitRect{0, 0, lx, ly});
+            if (whole) rects.push_back(SplitRect{0, 0, lx, ly});
             else splitPoints(an, nA, lx, ly, p->split_matrix_bigger_than_this, rL, rR, rects);
             int64_t ai = 0;
             int64_t count = 0;
             for (size_t i = 0; i < rects.size(); i++) {
                 const SplitRect &r = rects[i];
                 int64_t first = ai;
-                while (ai < nA) {
-                    int64_t x = an[3 * ai], y = an[3 * ai + 1];
-                    if (x + y >= r.x2 + r.y2) break;
-                    ai++;
+                if (rects.size() == 1) {
+                    ai = nA;  // every anchor lies in the only rectangle
+                } else {
+                    while (ai < nA) {
+                        int64_t x = an[3 * ai], y = an[3 * ai + 1];
+                        if (x + y >= r.x2 + r.y2) break;
+                        ai++;
+                    }
                 }
                 PlannedTask pt;
                 memset(&pt, 0, sizeof(pt));
@@ -673,8 +731,9 @@ static mp_status planBatch(mp_device_batch *db, const mp_batch *b) {
                            (forward ? kFlagForwardOnly : 0);
                 tk.job = (int32_t) j;
                 tk.expansion = (int32_t) p->diagonal_expansion;
-                int64_t slots = hullSlotBound(an + 3 * first, tk.nAnchors, r.x1, r.y1, tk.lx, tk.ly, dynamic,
-                                              p->diagonal_expansion);
+                int64_t slots = wholeHull >= 0 ? wholeHull
+                                               : hullSlotBound(an + 3 * first, tk.nAnchors, r.x1, r.y1, tk.lx, tk.ly,
+                                                               dynamic, p->diagonal_expansion);
                 pt.hull = (int32_t) std::min<int64_t>(slots, 1 << 30);
                 const int64_t maxHull = db->mode == kModeAdjoint ? adjointMaxHull() : kMaxHullSlots;
                 if (slots > maxHull) {
@@ -718,9 +777,11 @@ static mp_status planBatch(mp_device_batch *db, const mp_batch *b) {
         int64_t N = (int64_t) tk.lx + tk.ly;
         tk.bandOff = bandOff;
         bandOff += N + 1;
-        // capacity: measured densities are ~0.75 match and ~0.45 gap tuples per anti-diagonal at
-        // threshold 0.01; overflowing tasks are re-run with their exact counts
-        int32_t capM = (int32_t) (N + N / 8 + 64), capX = (int32_t) (N * 3 / 4 + 64), capY = (int32_t) (N * 3 / 4 + 64);
+        // capacity: measured densities are ~0.7 match and ~0.4-0.55 gap tuples per anti-diagonal
+        // at threshold 0.01, higher in repetitive sequence; overflowing tasks are re-run with their
+        // exact counts (a synchronous round trip, so the margins are generous: staging is 16 B per
+        // entry, ~4 GB for a 77 M-diagonal batch)
+        int32_t capM = (int32_t) (N + N / 2 + 64), capX = (int32_t) (N + 64), capY = (int32_t) (N + 64);
         int32_t caps[3] = {capM, capX, capY};
         if (db->mode != kModePosterior) caps[0] = caps[1] = caps[2] = 0;  // no tuples
         for (int k = 0; k < 3; k++) {
@@ -1379,6 +1440,8 @@ static mp_status fetchIssue(mp_engine *e, mp_device_batch *db, const mp_output *
         copy[k] = total[k] > 0 && (!cap || base[k] + total[k] <= cap[k]);
         if (copy[k] && (!out->weight[k] || !out->x[k] || !out->y[k]))
             return failf(MP_ERR_ARGUMENT, "output arrays of list %d missing", k);
+        // the previous fetch's copies out of the staging lists must be done before they are reused
+        if (k == 0 && db->copyPending) CUDA_TRY(cudaStreamWaitEvent(st, db->evCopied, 0));
         MP_TRY(upload(db->fetchDst[k], dst[k].data(), sizeof(int64_t) * dst[k].size(), st));
         const size_t n = sizeof(int32_t) * std::max<int64_t>(total[k], 1);
         MP_TRY(db->fetchW[k].reserve(n));
@@ -1399,12 +1462,22 @@ static mp_status fetchIssue(mp_engine *e, mp_device_batch *db, const mp_output *
         }
         CUDA_TRY(launchCompact(ca, st));
     }
+    cudaStream_t cs = st;
+    if (db->copyStream) {
+        CUDA_TRY(cudaEventRecord(db->evCompacted, st));
+        CUDA_TRY(cudaStreamWaitEvent(db->copyStream, db->evCompacted, 0));
+        cs = db->copyStream;
+    }
     for (int k = 0; k < 3; k++) {
         if (!copy[k]) continue;
         const size_t n = sizeof(int32_t) * total[k];
-        CUDA_TRY(cudaMemcpyAsync(out->weight[k] + base[k], db->fetchW[k].p, n, cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(cudaMemcpyAsync(out->x[k] + base[k], db->fetchX[k].p, n, cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(cudaMemcpyAsync(out->y[k] + base[k], db->fetchY[k].p, n, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(out->weight[k] + base[k], db->fetchW[k].p, n, cudaMemcpyDeviceToHost, cs));
+        CUDA_TRY(cudaMemcpyAsync(out->x[k] + base[k], db->fetchX[k].p, n, cudaMemcpyDeviceToHost, cs));
+        CUDA_TRY(cudaMemcpyAsync(out->y[k] + base[k], db->fetchY[k].p, n, cudaMemcpyDeviceToHost, cs));
+    }
+    if (db->copyStream) {
+        CUDA_TRY(cudaEventRecord(db->evCopied, cs));
+        db->copyPending = true;
     }
     return MP_OK;
 }
@@ -1653,16 +1726,30 @@ extern "C" mp_status mp_realign_batch(mp_engine *e, const mp_model *m, const mp_
     return MP_OK;
 }
 
-// Slices [cut[i], cut[i+1]) of a batch's jobs with similar work (template + read symbols).
+// Slices [cut[i], cut[i+1]) of a batch's jobs by work (template + read symbols). With three or
+// more slices the first and the last get half the work of the others: the first one's inputs
+// are copied before any kernel runs and the last one's tuples after the last kernel, so small
+// end slices shorten the pipeline's fill and drain.
 static std::vector<int64_t> sliceJobs(const mp_batch *b, int parts) {
     const int64_t n = b->n_jobs;
+    std::vector<double> target;  // cumulative work fraction at each inner cut
+    const double units = parts >= 3 ? (double) parts - 1.0 : (double) parts;
+    double acc = 0.0;
+    for (int i = 0; i + 1 < parts; i++) {
+        acc += (parts >= 3 && i == 0) ? 0.5 : 1.0;
+        target.push_back(acc / units);
+    }
     std::vector<int64_t> cut(1, 0);
     int64_t work = 0;
     for (int64_t j = 0; j < n; j++) work += (b->x_end[j] - b->x_begin[j]) + (b->y_offsets[j + 1] - b->y_offsets[j]);
-    int64_t acc = 0;
-    for (int64_t j = 0; j < n && (int) cut.size() < parts; j++) {
-        acc += (b->x_end[j] - b->x_begin[j]) + (b->y_offsets[j + 1] - b->y_offsets[j]);
-        if (acc * parts >= work * (int64_t) cut.size() && j + 1 < n) cut.push_back(j + 1);
+    int64_t sum = 0;
+    size_t next = 0;
+    for (int64_t j = 0; j + 1 < n && next < target.size(); j++) {
+        sum += (b->x_end[j] - b->x_begin[j]) + (b->y_offsets[j + 1] - b->y_offsets[j]);
+        if ((double) sum >= target[next] * (double) work) {
+            cut.push_back(j + 1);
+            next++;
+        }
     }
     cut.push_back(n);
     return cut;
@@ -1688,6 +1775,12 @@ extern "C" mp_status mp_realign_batch_into(mp_engine *e, const mp_model *m, cons
             return failf(MP_ERR_CUDA, "stream creation failed");
         }
         db->ownStream = true;
+        if (cudaStreamCreateWithFlags(&db->copyStream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&db->evCompacted, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&db->evCopied, cudaEventDisableTiming) != cudaSuccess) {
+            delete db;
+            return failf(MP_ERR_CUDA, "stream / event creation failed");
+        }
         e->pipe[k] = db;
     }
     const std::vector<int64_t> cut = sliceJobs(b, parts);
@@ -1740,7 +1833,9 @@ extern "C" mp_status mp_realign_batch_into(mp_engine *e, const mp_model *m, cons
     }
     if (st == MP_OK && pending >= 0) st = finish(pending);
     for (int k = 0; k < 2; k++) {
-        const cudaError_t ce = cudaStreamSynchronize(e->pipe[k]->stream);
+        cudaError_t ce = cudaStreamSynchronize(e->pipe[k]->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->pipe[k]->copyStream);
+        e->pipe[k]->copyPending = false;
         if (st == MP_OK && ce != cudaSuccess)
             st = failf(MP_ERR_CUDA, "pipelined pass failed: %s", cudaGetErrorString(ce));
     }

@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--no-graphs", action="store_true", help="direct launches instead of CUDA graph replay")
     ap.add_argument("--autotune-chunks", type=int, default=24,
                     help="chunks of the separate seeded sample the autotuner times the kernel variants on (0 = off)")
+    ap.add_argument("--polish-large", action="store_true",
+                    help="also time the POA loop on 10 chunks of 110 kb (1 Mb in 100 kb chunks with 10 kb overlap), "
+                         "50x, log-normal reads (median 20 kb, max 100 kb), band half-width 64")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the adjoint and POA-loop measurements reported beside the headline")
     return ap.parse_args()
@@ -280,6 +283,32 @@ def measure_polish(engine, model, pm):
     return best
 
 
+def measure_polish_large(engine, model, pm):
+    """The POA loop at genome scale: 1 Mb as 10 chunks of 110 kb (100 kb plus 10 kb overlap;
+    independent synthetic templates, since chunk stitching is outside this library), 50x,
+    log-normal reads (median 20 kb, sigma 0.6, at most 100 kb, clipped to the chunk), band
+    half-width 64, drafts with 1% homopolymer-biased indels, up to 5 iterations."""
+    from marginpolish_b200 import PoaSet, PolishParams, synth
+    t0 = time.perf_counter()
+    wl = synth.config_polish(seed=47, n_chunks=10, chunk_len=110_000, coverage=50, half_width=64,
+                             hp_runs=True, read_lognormal=(20_000, 0.6, 100_000))
+    gen = time.perf_counter() - t0
+    pp = PolishParams(max_iterations=5)
+    s = PoaSet.from_polish_model(engine, model, pm, pp, wl.drafts, wl.reads, wl.strands, wl.anchors)
+    t0 = time.perf_counter()
+    s.realign()
+    t1 = time.perf_counter()
+    s.iterate()
+    s.estimate_repeat_counts()
+    t2 = time.perf_counter()
+    its = [s.info(c)["iterations"] for c in range(s.n_chunks)]
+    s.close()
+    return {"seconds": t2 - t0, "realign_seconds": t1 - t0, "iterate_seconds": t2 - t1, "iterations": its,
+            "generation_s": round(gen, 1), "workload": measure_polish_large.__doc__.split("\n")[0],
+            "chunks": 10, "reads": int(sum(len(r) for r in wl.reads)),
+            "bases": int(sum(r.non_rle_length for lst in wl.reads for r in lst))}
+
+
 def pinned_jobs(jobs):
     """Copy of a batch whose arrays live in page-locked host memory (the library's allocator)."""
     from marginpolish_b200 import Jobs
@@ -416,6 +445,8 @@ def run_ours(args, rank, world, local):
     if not args.no_extras and rank == 0:
         extras["adjoint"] = measure_adjoint(engine, model, pm)
         extras["polish_loop"] = measure_polish(engine, model, pm)
+    if args.polish_large and rank == 0:
+        extras["polish_loop_1mb"] = measure_polish_large(engine, model, pm)
     peak = engine.fp32_peak_tflops()
     post = float(np.median(post_ms))
     achieved = cells * FLOP_PER_CELL / (post * 1e-3) / 1e12

@@ -231,7 +231,7 @@ struct MatchSet {  // the match coordinates of one read, sorted by (x, y)
 };
 
 void augment(Poa &poa, const Rle &read, bool strand, int64_t readNo, const std::vector<Pair> &matches,
-             std::vector<Pair> inserts, std::vector<Pair> deletes, bool cmpRC) {
+             std::vector<Pair> &inserts, std::vector<Pair> &deletes, bool cmpRC) {
     // match weights and observations
     for (const Pair &m : matches) {
         Node &node = poa.nodes[m.x + 1];
@@ -591,7 +591,13 @@ struct mp_poa_set {
     std::vector<Poa> poas;                   // per chunk (after a realignment)
     std::vector<int64_t> iterations;         // per chunk: iterations run by the last iterate
     mp_device_batch *db = nullptr;
-    ~mp_poa_set() { mp_device_batch_destroy(db); }
+    // page-locked tuple arrays of the last realignment (grow only): the copies run by DMA
+    void *pinned[3] = {nullptr, nullptr, nullptr};
+    size_t pinnedCap[3] = {0, 0, 0};  // tuples
+    ~mp_poa_set() {
+        mp_device_batch_destroy(db);
+        for (void *q : pinned) mp_host_free(q);
+    }
 };
 
 namespace {
@@ -624,6 +630,26 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
     std::vector<int32_t> an;
     std::vector<uint8_t> st;
     std::vector<int64_t> refStart(s->nChunks, 0);
+    {
+        size_t nx = 0, ny = 0, nr = 0, na = 0;
+        for (int64_t c : chunks) {
+            nx += (size_t) refs[c].length();
+            for (int64_t r = s->chunkReads[c]; r < s->chunkReads[c + 1]; r++) {
+                ny += (size_t) s->reads[r].length();
+                nr++;
+                if (anchors) na += (*anchors)[r].size();
+            }
+        }
+        xs.reserve(nx);
+        ys.reserve(ny);
+        an.reserve(3 * na);
+        xb.reserve(nr);
+        xe.reserve(nr);
+        shift.reserve(nr);
+        st.reserve(nr);
+        yo.reserve(nr + 1);
+        ao.reserve(nr + 1);
+    }
     for (int64_t c : chunks) {
         refStart[c] = (int64_t) xs.size();
         symbols(refs[c], 0, refs[c].length(), xs);
@@ -659,7 +685,8 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
     }
     const int64_t nJobs = (int64_t) jobRead.size();
     std::vector<int64_t> offs[3];
-    std::vector<int32_t> w[3], x[3], y[3];
+    const int32_t *w[3] = {nullptr, nullptr, nullptr}, *x[3] = {nullptr, nullptr, nullptr},
+                  *y[3] = {nullptr, nullptr, nullptr};
     if (nJobs > 0) {
         mp_batch b;
         memset(&b, 0, sizeof(b));
@@ -688,13 +715,24 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
         memset(&o, 0, sizeof(o));
         for (int k = 0; k < 3; k++) {
             offs[k].assign(nJobs + 1, 0);
-            w[k].resize(std::max<int64_t>(totals[k], 1));
-            x[k].resize(std::max<int64_t>(totals[k], 1));
-            y[k].resize(std::max<int64_t>(totals[k], 1));
+            const size_t need = (size_t) std::max<int64_t>(totals[k], 1);
+            if (need > s->pinnedCap[k]) {
+                mp_host_free(s->pinned[k]);
+                s->pinned[k] = nullptr;
+                s->pinnedCap[k] = 0;
+                const size_t cap = need + need / 4;
+                rc = mp_host_alloc(3 * sizeof(int32_t) * cap, &s->pinned[k]);
+                if (rc != MP_OK) return rc;
+                s->pinnedCap[k] = cap;
+            }
+            int32_t *base = static_cast<int32_t *>(s->pinned[k]);
+            w[k] = base;
+            x[k] = base + s->pinnedCap[k];
+            y[k] = base + 2 * s->pinnedCap[k];
             o.offsets[k] = offs[k].data();
-            o.weight[k] = w[k].data();
-            o.x[k] = x[k].data();
-            o.y[k] = y[k].data();
+            o.weight[k] = base;
+            o.x[k] = base + s->pinnedCap[k];
+            o.y[k] = base + 2 * s->pinnedCap[k];
         }
         rc = mp_device_batch_fetch_into(s->e, s->db, &o);
         if (rc != MP_OK) return rc;
@@ -714,6 +752,7 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
             const int64_t j = firstJob[c] + (r - s->chunkReads[c]);
             std::vector<Pair> lists[3];
             for (int k = 0; k < 3; k++) {
+                lists[k].reserve((size_t) (offs[k][j + 1] - offs[k][j]));
                 for (int64_t t = offs[k][j]; t < offs[k][j + 1]; t++) lists[k].push_back(Pair{w[k][t], x[k][t], y[k][t]});
             }
             // gap-x (consumes the reference) are deletes, gap-y inserts (impl/polisher.c:638-640)

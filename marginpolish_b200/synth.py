@@ -253,11 +253,12 @@ class PolishWorkload:
 
 def config_polish(seed: int = 3, n_chunks: int = 1, chunk_len: int = 2000, coverage: float = 20.0,
                   read_len=(1500, 2000), half_width: int = 25, draft_error: float = 0.01,
-                  hp_runs: bool = False) -> PolishWorkload:
+                  hp_runs: bool = False, read_lognormal=None) -> PolishWorkload:
     """Polishing chunks: truth templates, drafts = truth with 1% homopolymer-biased indels,
     reads sampled from the truth with the nanopore-like error model, anchors from the reads'
     truth alignment carried through the truth-to-draft map (every aligned base, expansion
-    2 * half_width, then run-length encoded as CIGAR anchors are)."""
+    2 * half_width, then run-length encoded as CIGAR anchors are). Read lengths are uniform in
+    read_len, or log-normal when read_lognormal = (median, sigma, maximum) is given."""
     rng = np.random.default_rng(seed)
     em = ErrorModel()
     truths, drafts, reads, strands, anchors = [], [], [], [], []
@@ -267,12 +268,19 @@ def config_polish(seed: int = 3, n_chunks: int = 1, chunk_len: int = 2000, cover
         tmap = np.full(t.size, -1, dtype=np.int64)
         tmap[t2d[:, 0]] = t2d[:, 1]
         drle = RleString.from_string(d.tobytes())
-        n_reads = max(1, int(round(coverage * chunk_len / float(np.mean(read_len)))))
+        if read_lognormal is not None:
+            med, sig, mx = read_lognormal
+            mean_len = min(float(mx), float(med) * float(np.exp(sig ** 2 / 2)))
+            draw = lambda: int(min(mx, rng.lognormal(np.log(med), sig)))  # noqa: E731
+        else:
+            mean_len = float(np.mean(read_len))
+            draw = lambda: int(rng.integers(read_len[0], read_len[1] + 1))  # noqa: E731
+        n_reads = max(1, int(round(coverage * chunk_len / mean_len)))
         # reads overhang the chunk ends and are clipped to it (as the chunker clips alignments),
         # so the coverage is even up to the chunk's ends
         lst = []
         for _ in range(n_reads):
-            ln = int(rng.integers(read_len[0], read_len[1] + 1))
+            ln = max(64, draw())
             start = int(rng.integers(-ln // 2, t.size - ln // 2))
             a, b = max(0, start), min(t.size, start + ln)
             if b - a < 64:

@@ -1621,8 +1621,9 @@ static cudaError_t launchT(const DpArgs &a, int blocks, int warps, cudaStream_t 
 // Kernel variants: (index, C slots per lane, L lanes per task, K checkpoint stride,
 // maximum warps per block = launch bound, arithmetic type). The window is S = L*C slots,
 // a warp carries 32/L tasks and a task fits when its band hull spans at most S - 2C slots.
-// Variants 0-6 compute in FP32, 7-11 in FP64 (same schedule; for the sub-problems whose
-// range FP32 cannot hold, and for the likelihood-only mode).
+// Variants 0-6 and 12 compute in FP32, 7-11 in FP64 (same schedule; for the sub-problems whose
+// range FP32 cannot hold, and for the likelihood-only mode). Variant 12 trades a shorter
+// checkpoint stride for more resident warps (an autotuner candidate).
 #define MP_VARIANTS(X)            \
     X(0, 2, 32, 8, 12, float)     \
     X(1, 4, 16, 4, 8, float)      \
@@ -1635,7 +1636,8 @@ static cudaError_t launchT(const DpArgs &a, int blocks, int warps, cudaStream_t 
     X(8, 3, 32, 8, 4, double)     \
     X(9, 4, 32, 4, 6, double)     \
     X(10, 6, 32, 4, 4, double)    \
-    X(11, 8, 32, 4, 3, double)
+    X(11, 8, 32, 4, 3, double)    \
+    X(12, 2, 32, 4, 16, float)
 
 // Adjoint variants (one task per warp; the block also holds the expected-count histograms).
 #define MP_ADJ_VARIANTS(X) \
@@ -1644,7 +1646,7 @@ static cudaError_t launchT(const DpArgs &a, int blocks, int warps, cudaStream_t 
     X(2, 4, 32, 4, 6)
 
 int variantCount() {
-    return 12;
+    return 13;
 }
 
 bool variantIsF64(int v) {

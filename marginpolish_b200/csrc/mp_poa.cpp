@@ -55,8 +55,15 @@ struct Rle {
     }
     Rle sub(int64_t start, int64_t len) const {
         Rle r;
-        for (int64_t i = start; i < start + len; i++) r.push(c[i], n[i]);
+        subInto(r, start, len);
         return r;
+    }
+    // sub() into an existing string, reusing its storage
+    void subInto(Rle &r, int64_t start, int64_t len) const {
+        r.c.assign(c.begin() + start, c.begin() + start + len);
+        r.n.assign(n.begin() + start, n.begin() + start + len);
+        r.nonRle = 0;
+        for (int64_t i = start; i < start + len; i++) r.nonRle += n[i];
     }
     bool operator==(const Rle &o) const { return nonRle == o.nonRle && c == o.c && n == o.n; }
 };
@@ -213,16 +220,13 @@ int64_t maxCommonSuffix(const Rle &a, int64_t lenA, const Rle &b, bool cmpRC) {
     return i;
 }
 
+// Rotates right by k: run i moves to (i + k) mod L (in place).
 void rotate(Rle &s, int64_t k) {
     const int64_t L = s.length();
-    std::string c(L, ' ');
-    std::vector<uint64_t> n(L);
-    for (int64_t i = 0; i < L; i++) {
-        c[(i + k) % L] = s.c[i];
-        n[(i + k) % L] = s.n[i];
-    }
-    s.c = c;
-    s.n = n;
+    if (L == 0) return;
+    const int64_t m = (L - k % L) % L;
+    std::rotate(s.c.begin(), s.c.begin() + m, s.c.end());
+    std::rotate(s.n.begin(), s.n.begin() + m, s.n.end());
 }
 
 struct MatchSet {  // the match coordinates of one read, sorted by (x, y)
@@ -232,6 +236,8 @@ struct MatchSet {  // the match coordinates of one read, sorted by (x, y)
 
 void augment(Poa &poa, const Rle &read, bool strand, int64_t readNo, const std::vector<Pair> &matches,
              std::vector<Pair> &inserts, std::vector<Pair> &deletes, bool cmpRC) {
+    // candidate indel sequences, reused across candidates and calls of this thread
+    thread_local Rle scratchIns, scratchDel;
     // match weights and observations
     for (const Pair &m : matches) {
         Node &node = poa.nodes[m.x + 1];
@@ -261,7 +267,8 @@ void augment(Poa &poa, const Rle &read, bool strand, int64_t readNo, const std::
             if (!ms.has(st.x, st.y + k - i - 1) && st.y + k - i - 1 > -1) continue;
             for (int64_t l = k; l < j; l++) {
                 if (!ms.has(st.x + 1, st.y + l - i + 1) && st.y + l - i + 1 < read.length()) continue;
-                Rle ins = read.sub(inserts[k].y, l + 1 - k);
+                Rle &ins = scratchIns;
+                read.subInto(ins, inserts[k].y, l + 1 - k);
                 double w = (double) UINT_MAX;
                 for (int64_t m = k; m <= l; m++) w = w < (double) inserts[m].w ? w : (double) inserts[m].w;
                 int64_t pos = st.x + 1;
@@ -308,7 +315,8 @@ void augment(Poa &poa, const Rle &read, bool strand, int64_t readNo, const std::
                 double w = (double) UINT_MAX;
                 for (int64_t m = k; m <= l; m++) w = w < (double) deletes[m].w ? w : (double) deletes[m].w;
                 int64_t pos = st.x + k - i;
-                const Rle del = poa.ref.sub(pos, len);
+                Rle &del = scratchDel;
+                poa.ref.subInto(del, pos, len);
                 pos = getShift(poa.ref, pos, del, cmpRC);
                 pos -= maxCommonSuffix(poa.ref, pos, del, cmpRC);
                 Node &node = poa.nodes[pos];

@@ -146,8 +146,6 @@ struct Node {
     char base = 'N';
     uint64_t rc = 1;
     double bw[5] = {0, 0, 0, 0, 0};
-    std::vector<double> rcw;
-    std::vector<Obs> obs;
     std::vector<Insert> ins;
     std::vector<Delete> del;
 };
@@ -156,6 +154,33 @@ struct Poa {
     uint64_t maxRC = 2;  // repeat counts are < maxRC
     std::vector<Node> nodes;
     Rle ref;
+    // Run-length weights of every node, [node][maxRC], in one array.
+    std::vector<double> rcw;
+    // Match observations. Folding a read appends them (obsNode: the node of each); groupObs
+    // then orders them by node, keeping append order within a node (the reference's
+    // observation order), and node i's are obs[obsStart[i] .. obsStart[i+1]).
+    std::vector<Obs> obs;
+    std::vector<int32_t> obsNode;
+    std::vector<int64_t> obsStart;
+
+    double *rcwOf(int64_t i) { return rcw.data() + i * (int64_t) maxRC; }
+    const double *rcwOf(int64_t i) const { return rcw.data() + i * (int64_t) maxRC; }
+    const Obs *obsBegin(int64_t i) const { return obs.data() + obsStart[i]; }
+    const Obs *obsEnd(int64_t i) const { return obs.data() + obsStart[i + 1]; }
+    int64_t obsCount(int64_t i) const { return obsStart[i + 1] - obsStart[i]; }
+
+    void groupObs() {
+        const int64_t nN = (int64_t) nodes.size();
+        obsStart.assign(nN + 1, 0);
+        for (int32_t v : obsNode) obsStart[v + 1]++;
+        for (int64_t i = 0; i < nN; i++) obsStart[i + 1] += obsStart[i];
+        std::vector<Obs> sorted(obs.size());
+        std::vector<int64_t> at(obsStart.begin(), obsStart.end() - 1);
+        for (size_t k = 0; k < obs.size(); k++) sorted[(size_t) at[obsNode[k]]++] = obs[k];
+        obs.swap(sorted);
+        obsNode.clear();
+        obsNode.shrink_to_fit();
+    }
 
     // poa_getReferenceGraph: node 0 is an 'N' prefix, then one node per reference run.
     static Poa fromReference(const Rle &reference, uint64_t maxRC) {
@@ -168,8 +193,9 @@ struct Poa {
             char b = i == 0 ? 'N' : (char) toupper((unsigned char) reference.c[i - 1]);
             n.base = charOf(symbolOf(b)) == 'N' ? 'N' : b;  // anything but ACGT becomes N
             n.rc = i == 0 ? 1 : reference.n[i - 1];
-            n.rcw.assign(maxRC, 0.0);
         }
+        p.rcw.assign((size_t) (reference.length() + 1) * maxRC, 0.0);
+        p.obsStart.assign((size_t) reference.length() + 2, 0);
         return p;
     }
 };
@@ -244,8 +270,9 @@ void augment(Poa &poa, const Rle &read, bool strand, int64_t readNo, const std::
         node.bw[symbolOf(read.c[m.y])] += (double) m.w;
         uint64_t rc = read.n[m.y];
         if (rc >= poa.maxRC) rc = poa.maxRC - 1;
-        node.rcw[rc] += (double) m.w;
-        node.obs.push_back(Obs{readNo, m.y, (double) m.w});
+        poa.rcwOf(m.x + 1)[rc] += (double) m.w;
+        poa.obs.push_back(Obs{readNo, m.y, (double) m.w});
+        poa.obsNode.push_back((int32_t) (m.x + 1));
     }
     MatchSet ms;
     ms.v.reserve(matches.size());
@@ -418,7 +445,7 @@ Rle consensus(const Poa &poa, std::vector<int64_t> &map, double penalty, bool us
             const Node &node = poa.nodes[i];
             const char base = charOf((int) maxWeight(node.bw, 5, symbolOf(node.base), penalty));
             if (useRle) {
-                int64_t rc = maxWeight(node.rcw.data(), (int64_t) poa.maxRC, (int64_t) node.rc, penalty);
+                int64_t rc = maxWeight(poa.rcwOf(i), (int64_t) poa.maxRC, (int64_t) node.rc, penalty);
                 rc = rc == 0 ? 1 : rc;
                 pieces.push_back(std::string((size_t) rc, base));
                 if (prevBase != base) map[i - 1] = running++;
@@ -489,7 +516,8 @@ std::vector<std::vector<Anchor>> anchorAlignments(const Poa &poa, const std::vec
     for (int64_t i = 1; i < (int64_t) poa.nodes.size(); i++) {
         const int64_t ci = map ? (*map)[i - 1] : i - 1;
         if (ci == -1) continue;
-        for (const Obs &o : poa.nodes[i].obs) {
+        for (const Obs *op = poa.obsBegin(i); op != poa.obsEnd(i); ++op) {
+            const Obs &o = *op;
             const double w = o.weight / (double) mp::kProbOne;
             if (!(w > probs[0])) continue;
             int64_t e = (int64_t) probs[1];
@@ -518,11 +546,14 @@ struct RepeatModel {
     }
 };
 
-uint64_t mlRepeatCount(const Poa &poa, const Node &node, const std::vector<Rle> &reads, const std::vector<uint8_t> &strand,
+uint64_t mlRepeatCount(const Poa &poa, int64_t i, const std::vector<Rle> &reads, const std::vector<uint8_t> &strand,
                        int64_t readBase, const RepeatModel &rm) {
+    const Node &node = poa.nodes[i];
+    const Obs *ob = poa.obsBegin(i), *oe = poa.obsEnd(i);
     const int base = symbolOf(node.base);
     int64_t lo = rm.M, hi = 0;
-    for (const Obs &o : node.obs) {
+    for (const Obs *op = ob; op != oe; ++op) {
+        const Obs &o = *op;
         const int64_t c = (int64_t) reads[readBase + o.read].n[o.offset];
         lo = c < lo ? c : lo;
         hi = c > hi ? c : hi;
@@ -533,7 +564,8 @@ uint64_t mlRepeatCount(const Poa &poa, const Node &node, const std::vector<Rle> 
     int64_t bestAt = 0;
     for (int64_t u = lo; u <= hi; u++) {
         double lp = 0.0;
-        for (const Obs &o : node.obs) {
+        for (const Obs *op = ob; op != oe; ++op) {
+            const Obs &o = *op;
             int64_t c = (int64_t) reads[readBase + o.read].n[o.offset];
             c = c >= rm.M ? rm.M - 1 : c;
             lp += rm.logProb(base, strand[readBase + o.read] != 0, c, u) * o.weight;
@@ -544,7 +576,6 @@ uint64_t mlRepeatCount(const Poa &poa, const Node &node, const std::vector<Rle> 
             bestAt = u - lo;
         }
     }
-    (void) poa;
     return (uint64_t) (bestAt + lo);
 }
 
@@ -552,7 +583,7 @@ void estimateRepeatCounts(Poa &poa, const std::vector<Rle> &reads, const std::ve
                           const RepeatModel &rm) {
     poa.ref.nonRle = 0;
     for (size_t i = 1; i < poa.nodes.size(); i++) {
-        uint64_t rc = mlRepeatCount(poa, poa.nodes[i], reads, strand, readBase, rm);
+        uint64_t rc = mlRepeatCount(poa, (int64_t) i, reads, strand, readBase, rm);
         if (rc == 0) rc = 1;
         poa.ref.n[i - 1] = rc;
         poa.ref.nonRle += rc;
@@ -766,6 +797,7 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
             // gap-x (consumes the reference) are deletes, gap-y inserts (impl/polisher.c:638-640)
             augment(poa, s->reads[r], s->strand[r] != 0, r - s->chunkReads[c], lists[0], lists[2], lists[1], s->cmpRC);
         }
+        poa.groupObs();
         out[c] = std::move(poa);
     });
     return MP_OK;
@@ -939,6 +971,7 @@ extern "C" mp_status mp_poa_set_realign_pairs(mp_poa_set *s, const int64_t *cons
                     lists[k].push_back(Pair{pairs[k][3 * t], pairs[k][3 * t + 1], pairs[k][3 * t + 2]});
             augment(poa, s->reads[r], s->strand[r] != 0, r - s->chunkReads[c], lists[0], lists[2], lists[1], s->cmpRC);
         }
+        poa.groupObs();
         out[c] = std::move(poa);
     });
     s->poas = std::move(out);
@@ -974,8 +1007,8 @@ extern "C" mp_status mp_poa_info(const mp_poa_set *s, int64_t chunk, mp_poa_chun
     info->nodes = (int64_t) poa.nodes.size();
     info->max_repeat = (int64_t) poa.maxRC;
     info->reference_runs = poa.ref.length();
+    info->observations = (int64_t) poa.obs.size();
     for (const Node &n : poa.nodes) {
-        info->observations += (int64_t) n.obs.size();
         info->inserts += (int64_t) n.ins.size();
         info->deletes += (int64_t) n.del.size();
         for (const Insert &e : n.ins) info->insert_runs += e.s.length();
@@ -998,8 +1031,8 @@ extern "C" mp_status mp_poa_nodes(const mp_poa_set *s, int64_t chunk, char *base
         if (base_weights)
             for (int k = 0; k < 5; k++) base_weights[5 * i + k] = n.bw[k];
         if (repeat_count_weights)
-            for (int64_t k = 0; k < M; k++) repeat_count_weights[M * i + k] = n.rcw[k];
-        if (n_obs) n_obs[i] = (int64_t) n.obs.size();
+            for (int64_t k = 0; k < M; k++) repeat_count_weights[M * i + k] = poa.rcwOf((int64_t) i)[k];
+        if (n_obs) n_obs[i] = poa.obsCount((int64_t) i);
         if (n_ins) n_ins[i] = (int64_t) n.ins.size();
         if (n_del) n_del[i] = (int64_t) n.del.size();
     }
@@ -1010,12 +1043,11 @@ extern "C" mp_status mp_poa_observations(const mp_poa_set *s, int64_t chunk, int
                                          double *weight) {
     MP_TRY(chunkCheck(s, chunk));
     int64_t k = 0;
-    for (const Node &n : s->poas[chunk].nodes)
-        for (const Obs &o : n.obs) {
-            read[k] = o.read;
-            offset[k] = o.offset;
-            weight[k++] = o.weight;
-        }
+    for (const Obs &o : s->poas[chunk].obs) {  // grouped by node, in the reference's order
+        read[k] = o.read;
+        offset[k] = o.offset;
+        weight[k++] = o.weight;
+    }
     return MP_OK;
 }
 

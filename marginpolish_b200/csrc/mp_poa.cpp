@@ -255,9 +255,27 @@ void rotate(Rle &s, int64_t k) {
     std::rotate(s.n.begin(), s.n.begin() + m, s.n.end());
 }
 
-struct MatchSet {  // the match coordinates of one read, sorted by (x, y)
-    std::vector<std::pair<int64_t, int64_t>> v;
-    bool has(int64_t x, int64_t y) const { return std::binary_search(v.begin(), v.end(), std::make_pair(x, y)); }
+// The match coordinates of one read, indexed by read position: the x values matched to read
+// position y are xs[at[y] .. at[y+1]) (a few per position at the posterior threshold).
+struct MatchSet {
+    std::vector<int32_t> at;
+    std::vector<int64_t> xs;
+    void build(const std::vector<Pair> &matches, int64_t readLen) {
+        at.assign((size_t) readLen + 2, 0);
+        for (const Pair &m : matches)
+            if (m.y >= 0 && m.y < readLen) at[(size_t) m.y + 1]++;
+        for (int64_t y = 0; y <= readLen; y++) at[(size_t) y + 1] += at[(size_t) y];
+        xs.resize(matches.size());
+        std::vector<int32_t> fill(at.begin(), at.end() - 1);
+        for (const Pair &m : matches)
+            if (m.y >= 0 && m.y < readLen) xs[(size_t) fill[(size_t) m.y]++] = m.x;
+    }
+    bool has(int64_t x, int64_t y) const {
+        if (y < 0 || y + 1 >= (int64_t) at.size()) return false;
+        for (int32_t k = at[(size_t) y]; k < at[(size_t) y + 1]; k++)
+            if (xs[(size_t) k] == x) return true;
+        return false;
+    }
 };
 
 void augment(Poa &poa, const Rle &read, bool strand, int64_t readNo, const std::vector<Pair> &matches,
@@ -274,10 +292,8 @@ void augment(Poa &poa, const Rle &read, bool strand, int64_t readNo, const std::
         poa.obs.push_back(Obs{readNo, m.y, (double) m.w});
         poa.obsNode.push_back((int32_t) (m.x + 1));
     }
-    MatchSet ms;
-    ms.v.reserve(matches.size());
-    for (const Pair &m : matches) ms.v.emplace_back(m.x, m.y);
-    std::sort(ms.v.begin(), ms.v.end());
+    thread_local MatchSet ms;
+    ms.build(matches, read.length());
 
     // complete inserts: same x, consecutive y, flanked by matches (or the read's ends)
     std::sort(inserts.begin(), inserts.end(), [](const Pair &a, const Pair &b) {
@@ -837,7 +853,10 @@ mp_status iterate(mp_poa_set *s) {
         forChunks(go, [&](int64_t c) {
             if (s->useRle) estimateRepeatCounts(next[c], s->reads, s->strand, s->chunkReads[c], s->rm);
             const double sc2 = score(next[c]);
-            if (sc2 <= sc[c] && s->iterations[c] > s->minIter) return;  // greedy stop: keep the old graph
+            if (sc2 <= sc[c] && s->iterations[c] > s->minIter) {  // greedy stop: keep the old graph
+                Poa drop = std::move(next[c]);                   // (freed here, in parallel)
+                return;
+            }
             s->poas[c] = std::move(next[c]);
             sc[c] = sc2;
             keep[c] = 1;

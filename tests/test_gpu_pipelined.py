@@ -38,3 +38,22 @@ def test_pipelined_equals_one_shot(polish_model, parts):
         gm.close()
     finally:
         eng.close()
+
+
+def test_pipelined_ragged_ends_and_strands(polish_model):
+    """Ragged starts / ends and both strands, sliced into several parts."""
+    import dataclasses
+    params = polish_model.alignment
+    jobs = synth.config_small(seed=9, n_reads=20).jobs()
+    rng = np.random.default_rng(0)
+    jobs = dataclasses.replace(jobs, ragged_left=rng.integers(0, 2, jobs.n_jobs).astype(np.uint8),
+                               ragged_right=rng.integers(0, 2, jobs.n_jobs).astype(np.uint8))
+    eng = Engine(0)
+    try:
+        gm = Model.from_polish(eng, polish_model)
+        want = realign_batch(eng, gm, params, jobs)
+        for parts in (2, 5):
+            _check_same(realign_batch_pipelined(eng, gm, params, jobs, parts=parts), want, jobs.n_jobs)
+        gm.close()
+    finally:
+        eng.close()

@@ -827,6 +827,7 @@ __device__ __forceinline__ void emitBlock(int gl, const GroupMem<C, L, K> &gm, u
     const int x0 = slotX0(d, Q) + s0;  // x of the lane's first slot
     const int xo = x0 - 1 + o.xShift, yo = d - x0 - 1 + o.yShift;
     const uint32_t row = gm.cacheA + (uint32_t) kk * CR::kRowA;
+    unsigned mask[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         unsigned m = 0;
@@ -846,16 +847,45 @@ __device__ __forceinline__ void emitBlock(int gl, const GroupMem<C, L, K> &gm, u
             for (int e = 0; e < E; e++)
                 if (lds<V>(CR::pAddr(row, kk, s0 + e, k)) >= thr) m |= 1u << e;
         }
-        if (!on) m = 0;
-        const int cnt = __popc(m);
-        int incl = cnt;
+        mask[k] = on ? m : 0u;
+    }
+    // ranks: exclusive prefix sums of the lanes' hit counts over the group, the three lists
+    // packed in 10-bit fields of one word when a group's total (at most K*S) fits
+    int excl[3], total[3];
+    if constexpr (K * L * C < 1024) {
+        const unsigned cnt = (unsigned) __popc(mask[0]) | ((unsigned) __popc(mask[1]) << 10) |
+                             ((unsigned) __popc(mask[2]) << 20);
+        unsigned incl = cnt;
 #pragma unroll
         for (int off = 1; off < L; off <<= 1) {
-            const int t = __shfl_up_sync(FULL_MASK, incl, off, L);
+            const unsigned t = __shfl_up_sync(FULL_MASK, incl, off, L);
             if (gl >= off) incl += t;
         }
-        const int total = __shfl_sync(FULL_MASK, incl, L - 1, L);
-        int pos = o.top[k] - 1 - o.written[k] - (incl - cnt);
+        const unsigned tot = __shfl_sync(FULL_MASK, incl, L - 1, L);
+        const unsigned ex = incl - cnt;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            excl[k] = (int) ((ex >> (10 * k)) & 1023u);
+            total[k] = (int) ((tot >> (10 * k)) & 1023u);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const int cnt = __popc(mask[k]);
+            int incl = cnt;
+#pragma unroll
+            for (int off = 1; off < L; off <<= 1) {
+                const int t = __shfl_up_sync(FULL_MASK, incl, off, L);
+                if (gl >= off) incl += t;
+            }
+            total[k] = __shfl_sync(FULL_MASK, incl, L - 1, L);
+            excl[k] = incl - cnt;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        unsigned m = mask[k];
+        int pos = o.top[k] - 1 - o.written[k] - excl[k];
         while (m) {
             const int e = __ffs(m) - 1;
             m &= m - 1;
@@ -865,7 +895,7 @@ __device__ __forceinline__ void emitBlock(int gl, const GroupMem<C, L, K> &gm, u
             }
             pos--;
         }
-        o.written[k] += total;
+        o.written[k] += total[k];
     }
 }
 

@@ -917,6 +917,8 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
     using CR = CacheRow<C, L, V>;
     using M = SlotMath<C, V>;
     static_assert(K <= L && (K % 2) == 0, "band records of a block are held one per lane");
+    static_assert(K <= 10, "a block holds at most one total refresh");
+    constexpr bool kSolo = L == 32;  // one task per warp: per-task decisions are warp-uniform
     constexpr int S = L * C;
     constexpr int R = RingSize<S>::R;
     const int gl = c.gl;
@@ -1065,6 +1067,10 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
         };
         V postScale = scaleOf();
         unsigned emitMask = 0;  // diagonals of the block that emit tuples
+        // Flat blocks: the posterior diagonals are kk <= pLim, the first processed is firstPost,
+        // and the total is refreshed at kk = refreshKK (-1: none; at most one, as K <= 10);
+        // the walk's counters are advanced once after the block.
+        int pLim = 0, firstPost = -1, refreshKK = -1, posts0 = 0;
         // One diagonal (PAR = d & 1). FLAT: every diagonal of the block is on and no window
         // shift occurs, so the step has no votes or branches (the total is refreshed by
         // selection and tuples are written with predicated stores).
@@ -1118,8 +1124,9 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
             }
             const bool post = on && d <= wk.tbFrom;
             // total probability refresh: 1st, 11th, 21st ... posterior diagonal of the walk
-            const bool refresh = post && untilRefresh == 0;
-            if (__any_sync(FULL_MASK, refresh)) {
+            const bool refresh = FLAT ? kk == refreshKK : post && untilRefresh == 0;
+            const int postsNow = FLAT ? posts0 + (firstPost - kk) : posts;  // posterior diagonals before d
+            if ((FLAT && kSolo) ? refresh : __any_sync(FULL_MASK, refresh)) {
                 // cells of d plus the match transitions crossing d (impl/pairwiseAligner.c:567-584)
                 V sM1[C];
                 if (kk > 0) {
@@ -1151,15 +1158,15 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
                 // values lost their range (the host runs such sub-problems again in FP64).
                 if (refresh) {
                     bool ok = tm > V(0);
-                    if (ok && posts > 0 && Tm > V(0) && abs(et - ET) <= 1) {
+                    if (ok && postsNow > 0 && Tm > V(0) && abs(et - ET) <= 1) {
                         const V r = N::div(tm * N::pow2(et - ET), Tm) - V(1);
                         ok = r <= V(1e-3) && r >= V(-1e-3);
-                    } else if (posts > 0) {
+                    } else if (postsNow > 0) {
                         ok = false;
                     }
                     rangeBad = rangeBad || !ok;
                 }
-                const bool first = refresh && wk.atEnd && posts == 0;
+                const bool first = refresh && wk.atEnd && postsNow == 0;
                 llTm = first ? tm : llTm;
                 llET = first ? et : llET;
                 llSet = llSet || first;
@@ -1167,8 +1174,10 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
                 ET = refresh ? et : ET;
                 postScale = scaleOf();
             }
-            untilRefresh = refresh ? 9 : untilRefresh - (post ? 1 : 0);
-            posts += post ? 1 : 0;
+            if constexpr (!FLAT) {
+                untilRefresh = refresh ? 9 : untilRefresh - (post ? 1 : 0);
+                posts += post ? 1 : 0;
+            }
             const bool emit = post && Tm > V(0) && wk.emit;
             if constexpr (!ADJ) {
                 // the row of d is not read again: it takes the posteriors (tuples after the block)
@@ -1262,11 +1271,19 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
         const auto odd = std::integral_constant<int, 1>{};
         const auto even = std::integral_constant<int, 0>{};
         if (flat && __all_sync(FULL_MASK, dStart > wk.tbTo && dEnd < wk.D)) {
+            pLim = wk.tbFrom - dStart;
+            firstPost = min(K - 1, pLim);
+            const int nPost = firstPost >= 0 ? firstPost + 1 : 0;
+            refreshKK = nPost > untilRefresh ? firstPost - untilRefresh : -1;
+            posts0 = posts;
 #pragma unroll 1
             for (int k = K - 2; k >= 0; k -= 2) {
                 back(odd, std::true_type{}, k + 1);
                 back(even, std::true_type{}, k);
             }
+            // post diagonals after the refresh are kk = refreshKK-1 .. 0
+            untilRefresh = refreshKK >= 0 ? 9 - refreshKK : untilRefresh - nPost;
+            posts += nPost;
         } else {
 #pragma unroll 1
             for (int k = K - 2; k >= 0; k -= 2) {

@@ -40,7 +40,7 @@ FLOP_PER_CELL = 48  # 30 FP32 FMA-pipe instructions per cell (forward 12, backwa
 # DRAM bytes (read + write) per band cell of the posterior kernel, from one ncu capture of the
 # same kernel on a 24-chunk slice of the workload (profiles/posteriorKernel_batched24_full.md);
 # traffic grows with cells, so a full launch moves this times its cells.
-DRAM_BYTES_PER_CELL = 6.09
+DRAM_BYTES_PER_CELL = 6.08
 METRIC = "GCUPS fwd+bwd+posterior (batched FP32 vs plain GPU, ≤1e-4 vs FP64); CPU ref"
 
 

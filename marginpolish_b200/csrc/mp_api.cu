@@ -556,6 +556,7 @@ struct mp_device_batch {
     DevBuf orders, queue, scratch, scratchScal;
     DevBuf expect, expectRep;  // adjoint accumulators (FP64)
     DevBuf fetchDst[3], fetchW[3], fetchX[3], fetchY[3];  // compaction staging (reused)
+    PinBuf stageTasks, stageOrders, stageDst[3];           // page-locked staging of the small uploads
     std::vector<int> varOrderOff;  // per variant offset into orders
     std::vector<int> varCount;
     std::vector<int64_t> varMaxN;
@@ -866,6 +867,19 @@ static mp_status upload(DevBuf &buf, const void *src, size_t bytes, cudaStream_t
     return MP_OK;
 }
 
+// upload() of a host vector through a page-locked staging buffer: the copy is DMA in stream
+// order and the host returns at once. The staging buffer is rewritten by the next staged
+// upload of the same purpose, which the batch's call sequence issues only after a
+// synchronisation of this stream.
+static mp_status uploadStaged(DevBuf &buf, PinBuf &stage, const void *src, size_t bytes, cudaStream_t s) {
+    MP_TRY(buf.reserve(bytes));
+    if (!bytes) return MP_OK;
+    MP_TRY(stage.reserve(bytes));
+    memcpy(stage.p, src, bytes);
+    CUDA_TRY(cudaMemcpyAsync(buf.p, stage.p, bytes, cudaMemcpyHostToDevice, s));
+    return MP_OK;
+}
+
 // Plans a batch into `db` and uploads it, reusing the device buffers db already holds
 // (they only grow).
 static mp_status batchReset(mp_engine *e, mp_device_batch *db, const mp_model *m, const mp_params *p,
@@ -892,7 +906,7 @@ static mp_status batchReset(mp_engine *e, mp_device_batch *db, const mp_model *m
     MP_TRY(upload(db->xs, b->x_symbols, sizeof(uint16_t) * b->x_symbols_length, st));
     MP_TRY(upload(db->ys, b->y_symbols, sizeof(uint16_t) * ny, st));
     MP_TRY(upload(db->anchors, b->anchors, sizeof(int32_t) * 3 * na, st));
-    MP_TRY(upload(db->dTasks, db->tasks.data(), sizeof(Task) * db->tasks.size(), st));
+    MP_TRY(uploadStaged(db->dTasks, db->stageTasks, db->tasks.data(), sizeof(Task) * db->tasks.size(), st));
     MP_TRY(db->band.reserve(sizeof(int4) * std::max<int64_t>(db->totalDiags, 1)));
     MP_TRY(db->dOut.reserve(sizeof(TaskOut) * std::max<size_t>(db->tasks.size(), 1)));
     for (int k = 0; k < 3; k++) {
@@ -1039,7 +1053,7 @@ static mp_status runIssue(mp_engine *e, mp_device_batch *db) {
     std::vector<int32_t> all(nTasks), orderHost;
     for (int i = 0; i < nTasks; i++) all[i] = i;
     MP_TRY(buildQueues(db, all, orderHost));
-    MP_TRY(upload(db->orders, orderHost.data(), sizeof(int32_t) * std::max<size_t>(orderHost.size(), 1), st));
+    MP_TRY(uploadStaged(db->orders, db->stageOrders, orderHost.data(), sizeof(int32_t) * std::max<size_t>(orderHost.size(), 1), st));
     if (!db->evBand) CUDA_TRY(cudaEventCreate(&db->evBand));
     BandArgs ba;
     memset(&ba, 0, sizeof(ba));
@@ -1442,7 +1456,7 @@ static mp_status fetchIssue(mp_engine *e, mp_device_batch *db, const mp_output *
             return failf(MP_ERR_ARGUMENT, "output arrays of list %d missing", k);
         // the previous fetch's copies out of the staging lists must be done before they are reused
         if (k == 0 && db->copyPending) CUDA_TRY(cudaStreamWaitEvent(st, db->evCopied, 0));
-        MP_TRY(upload(db->fetchDst[k], dst[k].data(), sizeof(int64_t) * dst[k].size(), st));
+        MP_TRY(uploadStaged(db->fetchDst[k], db->stageDst[k], dst[k].data(), sizeof(int64_t) * dst[k].size(), st));
         const size_t n = sizeof(int32_t) * std::max<int64_t>(total[k], 1);
         MP_TRY(db->fetchW[k].reserve(n));
         MP_TRY(db->fetchX[k].reserve(n));

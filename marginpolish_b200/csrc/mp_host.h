@@ -58,6 +58,32 @@ struct DevBuf {
     T *as() const { return static_cast<T *>(p); }
 };
 
+// Grow-only page-locked host buffer (staging for the planner's small uploads, so that their
+// copies are asynchronous DMA like the caller's page-locked inputs).
+struct PinBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    PinBuf() = default;
+    PinBuf(const PinBuf &) = delete;
+    PinBuf &operator=(const PinBuf &) = delete;
+    ~PinBuf() {
+        if (p) cudaFreeHost(p);
+    }
+    mp_status reserve(size_t n) {
+        if (n <= bytes && p) return MP_OK;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        const size_t want = n + n / 4 + 256;
+        if (cudaMallocHost(&p, want) != cudaSuccess) {
+            p = nullptr;
+            return mp_fail(MP_ERR_MEMORY, "cudaMallocHost(%zu) failed", want);
+        }
+        bytes = want;
+        return MP_OK;
+    }
+};
+
 // ---------------------------------------------------------------------------
 // engine and model
 // ---------------------------------------------------------------------------

@@ -184,6 +184,33 @@ def time_reference(jobs, cells, pm, seconds, steps=1, warmup=0):
             "gcups_1core": one_cells / max(t1, 1e-9) / 1e9, "reads_1core": one.n_jobs}
 
 
+def accuracy_sample(jobs, res, pm, n_reads=6):
+    """The timed batch's results on its first reads against the exact FP64 oracle (the checker,
+    run in the CPU-baseline leg): max |posterior - FP64| over every emitted tuple, and the
+    relative log-likelihood error."""
+    from oracle.bindings import ExactOracle, MpoModel
+    from oracle.compare import check_job
+    eo = ExactOracle()
+    models = (MpoModel.from_state_model(pm.forward), MpoModel.from_state_model(pm.reverse))
+    worst, worst_ll, tuples = 0.0, 0.0, 0
+    n = min(n_reads, jobs.n_jobs)
+    for j in range(n):
+        sx = jobs.x_symbols[jobs.x_begin[j]:jobs.x_end[j]]
+        sy = jobs.y_symbols[jobs.y_offsets[j]:jobs.y_offsets[j + 1]]
+        a = jobs.anchors[jobs.anchor_offsets[j]:jobs.anchor_offsets[j + 1]]
+        o = eo.align_with_indels(models[0] if jobs.strand[j] else models[1], sx, sy, a, pm.alignment, dense=True)
+        g = [res.job(j, k).copy() for k in range(3)]
+        shift = int(jobs.x_shift[j]) if jobs.x_shift is not None else 0
+        for k in range(3):
+            g[k][:, 1] -= shift
+            tuples += g[k].shape[0]
+        worst = max(worst, check_job(g, o, pm.alignment.threshold)["max_abs_posterior_error"])
+        ll = o["log_likelihood"]
+        worst_ll = max(worst_ll, abs(float(res.log_likelihood[j]) - ll) / max(1.0, abs(ll)))
+    return {"reads": n, "tuples": tuples, "max_abs_posterior_error_vs_fp64": worst,
+            "max_rel_loglik_error_vs_fp64": worst_ll, "bar": "posteriors 1e-4 absolute, log-likelihood 1e-5 relative"}
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -400,6 +427,9 @@ def run_ours(args, rank, world, local):
     else:
         max_ms, all_cells = total_ms, float(cells)
     value = all_cells * args.steps / (max_ms * 1e-3) / 1e9
+    # the timed run's results, for the FP64 check in the CPU-baseline leg (fetched before the
+    # plain form reuses the batch)
+    timed_res = db.fetch() if (rank == 0 and world == 1 and not args.no_cpu) else None
 
     # end-to-end through the public API with pinned host buffers
     e2e = None
@@ -461,7 +491,8 @@ def run_ours(args, rank, world, local):
                 cpu = {"value": r["gcups"], "unit": "GCUPS", "cores": r["cores"], "kind": "reference",
                        "sample": f"first {r['reads']} reads of the workload ({r['cells']} cells), "
                                  f"OpenMP over reads on {r['cores']} threads",
-                       "value_1core": r["gcups_1core"], "sample_1core": f"first {r['reads_1core']} reads, 1 thread"}
+                       "value_1core": r["gcups_1core"], "sample_1core": f"first {r['reads_1core']} reads, 1 thread",
+                       "accuracy_of_timed_results": accuracy_sample(jobs, timed_res, pm)}
         line = {
             "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",

@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--polish-large", action="store_true",
                     help="also time the POA loop on 10 chunks of 110 kb (1 Mb in 100 kb chunks with 10 kb overlap), "
                          "50x, log-normal reads (median 20 kb, max 100 kb), band half-width 64")
+    ap.add_argument("--polish-5mb", action="store_true",
+                    help="also time one realign+consensus pass on 5 Mb as 50 chunks of 100 kb, 60x, log-normal "
+                         "reads (median 25 kb, max 150 kb), band half-width 96")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the adjoint and POA-loop measurements reported beside the headline")
     return ap.parse_args()
@@ -310,6 +313,30 @@ def measure_polish(engine, model, pm):
     return best
 
 
+def measure_polish_5mb(engine, model, pm):
+    """One realign+consensus pass at scale: 5 Mb as 50 independent chunks of 100 kb
+    (homopolymer-enriched: geometric run lengths, p = 0.55), 60x, log-normal reads (median 25
+    kb, sigma 0.6, at most 150 kb, clipped to the chunk), band half-width 96, drafts with 1%
+    indels."""
+    from marginpolish_b200 import PoaSet, PolishParams, synth
+    t0 = time.perf_counter()
+    wl = synth.config_polish(seed=53, n_chunks=50, chunk_len=100_000, coverage=60, half_width=96,
+                             hp_runs=True, read_lognormal=(25_000, 0.6, 150_000))
+    gen = time.perf_counter() - t0
+    s = PoaSet.from_polish_model(engine, model, pm, PolishParams(max_iterations=1), wl.drafts, wl.reads,
+                                 wl.strands, wl.anchors)
+    t0 = time.perf_counter()
+    s.realign()
+    t1 = time.perf_counter()
+    s.iterate()
+    t2 = time.perf_counter()
+    s.close()
+    return {"seconds": t2 - t0, "realign_seconds": t1 - t0, "consensus_and_realign_seconds": t2 - t1,
+            "generation_s": round(gen, 1), "workload": measure_polish_5mb.__doc__.split("\n")[0],
+            "chunks": 50, "reads": int(sum(len(r) for r in wl.reads)),
+            "bases": int(sum(r.non_rle_length for lst in wl.reads for r in lst))}
+
+
 def measure_polish_large(engine, model, pm):
     """The POA loop at genome scale: 1 Mb as 10 chunks of 110 kb (100 kb plus 10 kb overlap;
     independent synthetic templates, since chunk stitching is outside this library), 50x,
@@ -477,6 +504,8 @@ def run_ours(args, rank, world, local):
         extras["polish_loop"] = measure_polish(engine, model, pm)
     if args.polish_large and rank == 0:
         extras["polish_loop_1mb"] = measure_polish_large(engine, model, pm)
+    if args.polish_5mb and rank == 0:
+        extras["polish_pass_5mb"] = measure_polish_5mb(engine, model, pm)
     peak = engine.fp32_peak_tflops()
     post = float(np.median(post_ms))
     achieved = cells * FLOP_PER_CELL / (post * 1e-3) / 1e12

@@ -667,52 +667,39 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
     // (impl/polisher.c:634-635) and one lower on the path without anchors (:676-679)
     const uint64_t maxRC = s->useRle ? (uint64_t) s->rm.M : 2;
     const uint32_t maxExcl = (uint32_t) (anchors ? maxRC : maxRC - 1);
-    auto symbols = [&](const Rle &r, int64_t start, int64_t len, std::vector<uint16_t> &dst) {
-        for (int64_t i = start; i < start + len; i++) {
+    const bool rle = s->m->host[0].runLength != 0;
+    auto symbols = [&](const Rle &r, uint16_t *dst) {
+        for (int64_t i = 0; i < r.length(); i++) {
             const uint16_t b = (uint16_t) symbolOf(r.c[i]);
             uint64_t cnt = r.n[i];
-            if (s->m->host[0].runLength) {
-                cnt = cnt > maxExcl - 1 ? maxExcl - 1 : cnt;
-                dst.push_back((uint16_t) ((cnt << 8) | b));
-            } else {
-                dst.push_back(b);
-            }
+            cnt = cnt > maxExcl - 1 ? maxExcl - 1 : cnt;
+            dst[i] = rle ? (uint16_t) ((cnt << 8) | b) : b;
         }
     };
-    // jobs: one per read of the listed chunks, with the reference crop (impl/polisher.c:613-628)
-    std::vector<uint16_t> xs, ys;
-    std::vector<int64_t> xb, xe, yo{0}, ao{0}, shift;
-    std::vector<int32_t> an;
-    std::vector<uint8_t> st;
-    std::vector<int64_t> refStart(s->nChunks, 0);
-    {
-        size_t nx = 0, ny = 0, nr = 0, na = 0;
-        for (int64_t c : chunks) {
-            nx += (size_t) refs[c].length();
-            for (int64_t r = s->chunkReads[c]; r < s->chunkReads[c + 1]; r++) {
-                ny += (size_t) s->reads[r].length();
-                nr++;
-                if (anchors) na += (*anchors)[r].size();
-            }
-        }
-        xs.reserve(nx);
-        ys.reserve(ny);
-        an.reserve(3 * na);
-        xb.reserve(nr);
-        xe.reserve(nr);
-        shift.reserve(nr);
-        st.reserve(nr);
-        yo.reserve(nr + 1);
-        ao.reserve(nr + 1);
-    }
+    // jobs: one per read of the listed chunks, with the reference crop (impl/polisher.c:613-628).
+    // Offsets first (chunk order, reads in order), then every chunk's arrays filled in parallel.
+    std::vector<int64_t> refStart(s->nChunks, 0), firstJobOf(s->nChunks, 0);
+    std::vector<int64_t> yo{0}, ao{0};
+    int64_t nx = 0;
     for (int64_t c : chunks) {
-        refStart[c] = (int64_t) xs.size();
-        symbols(refs[c], 0, refs[c].length(), xs);
-    }
-    std::vector<std::pair<int64_t, int64_t>> jobRead;  // (chunk, read index)
-    for (int64_t c : chunks) {
-        const int64_t L = refs[c].length();
+        refStart[c] = nx;
+        nx += refs[c].length();
+        firstJobOf[c] = (int64_t) yo.size() - 1;
         for (int64_t r = s->chunkReads[c]; r < s->chunkReads[c + 1]; r++) {
+            yo.push_back(yo.back() + s->reads[r].length());
+            ao.push_back(ao.back() + (anchors ? (int64_t) (*anchors)[r].size() : 0));
+        }
+    }
+    const int64_t nJobs = (int64_t) yo.size() - 1;
+    std::vector<uint16_t> xs((size_t) nx), ys((size_t) yo.back());
+    std::vector<int64_t> xb((size_t) nJobs), xe((size_t) nJobs), shift((size_t) nJobs);
+    std::vector<int32_t> an((size_t) (3 * ao.back()));
+    std::vector<uint8_t> st((size_t) nJobs);
+    forChunks(chunks, [&](int64_t c) {
+        const int64_t L = refs[c].length();
+        symbols(refs[c], xs.data() + refStart[c]);
+        int64_t j = firstJobOf[c];
+        for (int64_t r = s->chunkReads[c]; r < s->chunkReads[c + 1]; r++, j++) {
             const Rle &read = s->reads[r];
             int64_t first = 0, end = L;
             const std::vector<Anchor> *ra = anchors ? &(*anchors)[r] : nullptr;
@@ -722,23 +709,21 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
                 end = 1 + ra->back().x + (read.length() - ra->back().y);
                 end = end > L ? L : end;
             }
-            xb.push_back(refStart[c] + first);
-            xe.push_back(refStart[c] + end);
-            shift.push_back(first);
-            symbols(read, 0, read.length(), ys);
-            yo.push_back((int64_t) ys.size());
-            if (ra)
+            xb[(size_t) j] = refStart[c] + first;
+            xe[(size_t) j] = refStart[c] + end;
+            shift[(size_t) j] = first;
+            symbols(read, ys.data() + yo[(size_t) j]);
+            if (ra) {
+                int32_t *dst = an.data() + 3 * ao[(size_t) j];
                 for (const Anchor &a : *ra) {
-                    an.push_back((int32_t) (a.x - first));
-                    an.push_back((int32_t) a.y);
-                    an.push_back((int32_t) a.e);
+                    *dst++ = (int32_t) (a.x - first);
+                    *dst++ = (int32_t) a.y;
+                    *dst++ = (int32_t) a.e;
                 }
-            ao.push_back((int64_t) an.size() / 3);
-            st.push_back(s->strand[r]);
-            jobRead.emplace_back(c, r);
+            }
+            st[(size_t) j] = s->strand[r];
         }
-    }
-    const int64_t nJobs = (int64_t) jobRead.size();
+    });
     std::vector<int64_t> offs[3];
     const int32_t *w[3] = {nullptr, nullptr, nullptr}, *x[3] = {nullptr, nullptr, nullptr},
                   *y[3] = {nullptr, nullptr, nullptr};

@@ -1222,14 +1222,20 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
                         const int x = xl + j, y = d - x;
                         const uint32_t mb = sym >> 19;                                  // model*25 + xb*5 + yb
                         const uint32_t rb = ((sym & 0x1ffffu) - kRepBase) >> 2;         // repeat-table entry
+                        // State posteriors below kTinyPosterior are left out of the emission
+                        // histograms: even 1e8 such cells in one bin move it by < 1e-4, while
+                        // the band's cells far from the alignment path stop costing a
+                        // contended shared-memory atomic each.
+                        constexpr float kTinyPosterior = 1e-12f;
                         if (sym != 0xffffffffu && mb < 50u) {
-                            if (x > 0 && y > 0 && pm > 0.0f) {
+                            if (x > 0 && y > 0 && pm > kTinyPosterior) {
                                 atomicAdd(hs + kHistMatch + mb, pm);
                                 if (c.rle && rb < (uint32_t) (c.nTables * kRepTable))
                                     atomicAdd(hs + kHistSmall + rb, pm);
                             }
-                            if (x > 0 && px > 0.0f) atomicAdd(hs + kHistGapX + (mb / 25) * 5 + (mb % 25) / 5, px);
-                            if (y > 0 && py > 0.0f) atomicAdd(hs + kHistGapY + (mb / 25) * 5 + mb % 5, py);
+                            if (x > 0 && px > kTinyPosterior)
+                                atomicAdd(hs + kHistGapX + (mb / 25) * 5 + (mb % 25) / 5, px);
+                            if (y > 0 && py > kTinyPosterior) atomicAdd(hs + kHistGapY + (mb / 25) * 5 + mb % 5, py);
                         }
                         if (d == 0 || d == c.N) {  // the first / last cell: the start / end vectors
                             const int sb = (d == 0 ? kHistStart : kHistEnd) + (int) c.model * 3;

@@ -142,9 +142,10 @@ def fit(engine: Engine, jobs: Jobs, params, init: FitParams, steps: int = 20, lr
         loss = -ll / max(jobs.n_jobs, 1)
         loss.backward()
         opt.step()
-        history.append(float(ll))
+        value = float(ll.detach())
+        history.append(value)
         if callback:
-            callback(step, float(ll))
+            callback(step, value)
     return history
 
 

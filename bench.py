@@ -285,6 +285,62 @@ def measure_adjoint(engine, model, pm):
             "form": "mp_expectations_batch, host arrays in / counts out (FP32 cells, FP64 accumulation)"}
 
 
+def measure_bubble_scoring(engine, model, pm, bubbles=2000, seed=61):
+    """The scoring step of bubble-graph polishing: every read substring of a bubble against
+    each of its candidate alleles, computeForwardProbability without anchors (the band of
+    band_construct over the whole pair), as one mp_forward_batch call. Synthetic bubbles:
+    2-4 alleles of 10-100 RLE symbols, 40 read substrings per bubble (the allele with
+    about 5% substitutions, run lengths 1-3)."""
+    import numpy as np
+    from marginpolish_b200 import Jobs, forward_batch
+    rng = np.random.default_rng(seed)
+    xs, ys, xb, xe, yo, st = [], [], [], [], [0], []
+    x_at, y_at = 0, 0
+    for _ in range(bubbles):
+        n_al = int(rng.integers(2, 5))
+        length = int(rng.integers(10, 101))
+        base = rng.integers(0, 4, size=length)
+        alleles = []
+        for _ in range(n_al):
+            a = base.copy()
+            flip = rng.random(length) < 0.03
+            a[flip] = rng.integers(0, 4, size=int(flip.sum()))
+            sym = ((rng.integers(1, 4, size=length) << 8) | a).astype(np.uint16)
+            alleles.append(sym)
+        for _ in range(40):
+            r = base.copy()
+            flip = rng.random(length) < 0.05
+            r[flip] = rng.integers(0, 4, size=int(flip.sum()))
+            rsym = ((rng.integers(1, 4, size=length) << 8) | r).astype(np.uint16)
+            strand = int(rng.integers(0, 2))
+            for a in alleles:
+                xs.append(a)
+                xb.append(x_at)
+                x_at += a.size
+                xe.append(x_at)
+                ys.append(rsym)
+                y_at += rsym.size
+                yo.append(y_at)
+                st.append(strand)
+    n = len(xb)
+    jobs = Jobs(np.concatenate(xs), np.array(xb, np.int64), np.array(xe, np.int64), np.concatenate(ys),
+                np.array(yo, np.int64), np.zeros((0, 3), np.int32), np.zeros(n + 1, np.int64),
+                np.array(st, np.uint8), None, None, None)
+    forward_batch(engine, model, pm.alignment, jobs)  # warm
+    ts = []
+    for _ in range(3):
+        t = time.perf_counter()
+        lp = forward_batch(engine, model, pm.alignment, jobs)
+        ts.append(time.perf_counter() - t)
+    t = float(np.median(ts))
+    lx = np.array(xe) - np.array(xb)
+    ly = np.diff(np.array(yo))
+    return {"workload": f"{bubbles} bubbles x 2-4 alleles of 10-100 RLE symbols x 40 read substrings",
+            "pairs": n, "matrix_cells": int(np.sum((lx + 1) * (ly + 1))), "seconds": t, "pairs_per_s": n / t,
+            "all_finite": bool(np.all(np.isfinite(lp))),
+            "form": "mp_forward_batch: host arrays in, ln P per pair out (FP64 forward-only variants)"}
+
+
 def measure_polish(engine, model, pm):
     """The POA loop (poa_realignAll in consensus mode, up to 5 iterations) over 16 chunks of a
     homopolymer-enriched 10 kb template at 30x, reads of 3-9 kb, drafts with 1% indels."""
@@ -502,6 +558,7 @@ def run_ours(args, rank, world, local):
     if not args.no_extras and rank == 0:
         extras["adjoint"] = measure_adjoint(engine, model, pm)
         extras["polish_loop"] = measure_polish(engine, model, pm)
+        extras["bubble_scoring"] = measure_bubble_scoring(engine, model, pm)
     if args.polish_large and rank == 0:
         extras["polish_loop_1mb"] = measure_polish_large(engine, model, pm)
     if args.polish_5mb and rank == 0:

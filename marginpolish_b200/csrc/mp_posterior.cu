@@ -1501,6 +1501,16 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
             if (c.gl == 0) sc.scal[d0 / K] = make_int2(Ef, Q);
         }
         const int dLast = d0 + K - 1;
+        // A ring that would run out inside the block is refilled for the whole block now
+        // (positions needed at d0 .. dLast in the current window: x0-1 .. x0'+S-2 and
+        // y0-S .. y0'-1, at most S + K/2 + 1 entries), so that the block can run flat.
+        if (__any_sync(FULL_MASK, dLast >= checkAt && dLast <= myN)) {
+            const bool on = kSolo || dLast <= myN;
+            const int xa = slotX0(d0, Q), xb = slotX0(dLast, Q);
+            ringEnsure<R, L, true>(c, gm.rx, xa - 1, xb + S - 2, true, on);
+            ringEnsure<R, L, false>(c, gm.ry, d0 - xa - S, dLast - xb - 1, true, on);
+            checkAt = ensureRings<R, L, S>(c, gm.rx, gm.ry, d0, Q, true, on);
+        }
         bool clear = dLast <= myN && dLast < checkAt;
         if (c.gl < K) {
             const int4 bd = lds<int4>(gm.bandRing + (((d0 + c.gl) & 63) << 4));

@@ -729,6 +729,11 @@ struct Out {
 // Shared workspace of one group
 // ---------------------------------------------------------------------------
 
+// Adjoint histogram bins (floats): match posteriors by (model, x base, y base), gap-x by
+// (model, x base), gap-y by (model, y base), state posteriors at the first and the last cell by
+// (model, state); then the repeat tables (block-wide).
+constexpr int kHistMatch = 0, kHistGapX = 50, kHistGapY = 60, kHistStart = 70, kHistEnd = 76, kHistSmall = 82;
+
 template <int C, int L, int K, bool ADJ = false, class V = float>
 struct GroupSmem {
     static constexpr int S = L * C;
@@ -740,8 +745,10 @@ struct GroupSmem {
     static constexpr size_t cacheBBytes = (size_t) K * CacheRow<C, L, V>::kRowB;
     static constexpr size_t cacheCBytes = ADJ ? (size_t) K * S * sizeof(uint32_t) : 0;
     static constexpr size_t infoBytes = K * sizeof(int2);
-    static constexpr size_t bytes =
-        ringBytes + bandRingBytes + walkBandBytes + cacheABytes + cacheBBytes + cacheCBytes + infoBytes;
+    // adjoint only: the warp's own small histograms (no contention with the block's other warps)
+    static constexpr size_t smallHistBytes = ADJ ? (((size_t) kHistSmall * sizeof(float) + 15) & ~(size_t) 15) : 0;
+    static constexpr size_t bytes = ringBytes + bandRingBytes + walkBandBytes + cacheABytes + cacheBBytes +
+                                    cacheCBytes + infoBytes + smallHistBytes;
 };
 
 template <int C, int L, int K>
@@ -753,14 +760,11 @@ struct GroupMem {
     uint32_t cacheB;    // [K] B rows of the block cache (empty in the paired layout)
     uint32_t cacheC;    // adjoint only: [K][S] uint32 table offsets of the cell
     uint32_t info;      // [K] int2: window, shift
-    uint32_t hist;      // adjoint only: the block's histograms (small tables, then repeat tables)
+    uint32_t hist;      // adjoint only: the block's histograms (its repeat tables at kHistSmall)
+    uint32_t whist;     // adjoint only: the warp's small histograms (kHistSmall floats)
 };
 
-// Adjoint histograms in shared memory (floats): match posteriors by (model, x base, y base),
-// gap-x by (model, x base), gap-y by (model, y base), state posteriors at the first and the
-// last cell by (model, state), then the repeat tables.
-constexpr int kHistMatch = 0, kHistGapX = 50, kHistGapY = 60, kHistStart = 70, kHistEnd = 76, kHistSmall = 82;
-
+// Bytes of the block-wide adjoint histograms (the repeat tables start at bin kHistSmall).
 __host__ __device__ constexpr size_t histBytes(int nTables) {
     return ((size_t) (kHistSmall + nTables * kRepTable) * sizeof(float) + 15) & ~(size_t) 15;
 }
@@ -1205,6 +1209,7 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
                     const float scale = acc ? N::div(N::pow2(ex), Tm) : 0.0f;
                     const int xl = slotX0(d, inf.x) + gl * C;
                     float *hs = reinterpret_cast<float *>(mpSmem + gm.hist);
+                    float *ws = reinterpret_cast<float *>(mpSmem + gm.whist);
 #pragma unroll
                     for (int j = 0; j < C; j++) {
                         const float fm = fM[j] * scale, fx = fX[j] * scale, fy = fY[j] * scale;
@@ -1229,19 +1234,19 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
                         constexpr float kTinyPosterior = 1e-12f;
                         if (sym != 0xffffffffu && mb < 50u) {
                             if (x > 0 && y > 0 && pm > kTinyPosterior) {
-                                atomicAdd(hs + kHistMatch + mb, pm);
+                                atomicAdd(ws + kHistMatch + mb, pm);
                                 if (c.rle && rb < (uint32_t) (c.nTables * kRepTable))
                                     atomicAdd(hs + kHistSmall + rb, pm);
                             }
                             if (x > 0 && px > kTinyPosterior)
-                                atomicAdd(hs + kHistGapX + (mb / 25) * 5 + (mb % 25) / 5, px);
-                            if (y > 0 && py > kTinyPosterior) atomicAdd(hs + kHistGapY + (mb / 25) * 5 + mb % 5, py);
+                                atomicAdd(ws + kHistGapX + (mb / 25) * 5 + (mb % 25) / 5, px);
+                            if (y > 0 && py > kTinyPosterior) atomicAdd(ws + kHistGapY + (mb / 25) * 5 + mb % 5, py);
                         }
                         if (d == 0 || d == c.N) {  // the first / last cell: the start / end vectors
                             const int sb = (d == 0 ? kHistStart : kHistEnd) + (int) c.model * 3;
-                            if (pm > 0.0f) atomicAdd(hs + sb, pm);
-                            if (px > 0.0f) atomicAdd(hs + sb + 1, px);
-                            if (py > 0.0f) atomicAdd(hs + sb + 2, py);
+                            if (pm > 0.0f) atomicAdd(ws + sb, pm);
+                            if (px > 0.0f) atomicAdd(ws + sb + 1, px);
+                            if (py > 0.0f) atomicAdd(ws + sb + 2, py);
                         }
                     }
                 }
@@ -1320,10 +1325,12 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
         if constexpr (ADJ) {
 #pragma unroll
             for (int i = 0; i < 9; i++) accD[i] += (double) ta[i];
-            // the small histograms go to FP64 in global memory after every block
-            float *hs = reinterpret_cast<float *>(mpSmem + gm.hist);
+            // the warp's small histograms go to FP64 in global memory after every block
+            __syncwarp();
+            float *ws = reinterpret_cast<float *>(mpSmem + gm.whist);
             for (int i = gl; i < kHistSmall; i += 32) {
-                const float v = atomicExch(hs + i, 0.0f);
+                const float v = ws[i];
+                ws[i] = 0.0f;
                 if (v != 0.0f) atomicAdd(expect + expectSlot(i), (double) v);
             }
         }
@@ -1641,6 +1648,12 @@ __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
     gm.cacheC = gm.cacheB + (uint32_t) GS::cacheBBytes;
     gm.info = gm.cacheC + (uint32_t) GS::cacheCBytes;
     gm.hist = histOff;
+    gm.whist = gm.info + (uint32_t) GS::infoBytes;
+    if (ADJ) {
+        float *w = reinterpret_cast<float *>(mpSmem + gm.whist);
+        for (int i = lane; i < kHistSmall; i += 32) w[i] = 0.0f;
+        __syncwarp();
+    }
     Scratch<V> sc;
     sc.blocks = a.scratchBlocks;
     const size_t slot = (size_t) gwarp * G + g;  // one checkpoint area per task slot

@@ -87,3 +87,34 @@ def test_fetch_before_run_is_a_state_error(engine, polish_model):
     assert err.value.status == _lib.MP_ERR_STATE
     db.close()
     model.close()
+
+
+def test_argument_errors_are_reported(engine, polish_model):
+    """Malformed jobs come back as MP_ERR_ARGUMENT with a message: anchors not strictly
+    increasing, an anchor outside the matrix, an odd expansion under dynamic anchor expansion
+    (all found by the planner), and a repeat count at the run-length table's limit (found by
+    the kernel, which clamps the lookup and flags the task)."""
+    from marginpolish_b200 import Jobs
+    model = Model.from_polish(engine, polish_model)
+    params = polish_model.alignment
+    sx = np.array([(1 << 8) | b for b in (0, 1, 2, 3, 0, 1, 2, 3)], np.uint16)
+    sy = sx.copy()
+    cases = {
+        "not strictly increasing": np.array([[2, 2, 4], [2, 3, 4]], np.int32),
+        "outside the matrix": np.array([[2, 2, 4], [8, 7, 4]], np.int32),
+        "odd expansion": np.array([[2, 2, 3]], np.int32),
+    }
+    for what, anchors in cases.items():
+        jobs = Jobs.single(sx, sy, anchors)
+        with pytest.raises(_lib.MpError) as err:
+            realign_batch(engine, model, params, jobs)
+        assert err.value.status == _lib.MP_ERR_ARGUMENT, what
+    big = sx.copy()
+    big[3] = (51 << 8) | 3  # observed repeat count 51: beyond the 51 x 51 table
+    with pytest.raises(_lib.MpError) as err:
+        realign_batch(engine, model, params, Jobs.single(big, sy, np.zeros((0, 3), np.int32)))
+    assert err.value.status == _lib.MP_ERR_ARGUMENT
+    # the engine still works after the errors
+    ok = realign_batch(engine, model, params, Jobs.single(sx, sy, np.array([[2, 2, 4]], np.int32)))
+    assert ok.total_cells > 0
+    model.close()

@@ -199,3 +199,21 @@ def test_empty_and_tiny_sequences(engine, default_model):
     for sx, sy in [([], []), ([0, 1, 2], []), ([], [3, 3]), ([1], [1]), ([0, 4, 2], [0, 2])]:
         jobs = Jobs.single(np.array(sx, np.uint16), np.array(sy, np.uint16), np.zeros((0, 3), np.int32))
         _run_and_check(engine, gm, mpo, jobs, p)
+
+
+def test_low_threshold_forces_capacity_retries(engine, polish_model):
+    """At threshold 0.001 the gap lists hold several times the tuples the planner reserves per
+    task (1.5 N match, N per gap list), so tasks overflow and are re-run with their exact
+    counts; the results keep the parity bar at that threshold."""
+    import dataclasses
+    params = dataclasses.replace(polish_model.alignment, threshold=0.001)
+    jobs = synth.config_small(seed=8, n_reads=6).jobs()
+    gm = Model.from_polish(engine, polish_model)
+    mpo = (MpoModel.from_state_model(polish_model.forward), MpoModel.from_state_model(polish_model.reverse))
+    res, worst = _run_and_check(engine, gm, mpo, jobs, params)
+    assert worst <= 1e-4
+    n = jobs.x_end - jobs.x_begin + np.diff(jobs.y_offsets)
+    # more tuples than the first launch had room for in at least one list of one job
+    over = [int(res.offsets[k][j + 1] - res.offsets[k][j]) > (1.5 * n[j] if k == 0 else n[j])
+            for j in range(jobs.n_jobs) for k in range(3)]
+    assert any(over)

@@ -217,3 +217,20 @@ def test_low_threshold_forces_capacity_retries(engine, polish_model):
     over = [int(res.offsets[k][j + 1] - res.offsets[k][j]) > (1.5 * n[j] if k == 0 else n[j])
             for j in range(jobs.n_jobs) for k in range(3)]
     assert any(over)
+
+
+def test_separate_repeat_tables_per_strand(engine, polish_model):
+    """Forward- and reverse-strand reads with different run-length tables: both tables are
+    held in shared memory (the two-table layout) and each task reads its strand's."""
+    import dataclasses
+    rng = np.random.default_rng(3)
+    rev = dataclasses.replace(polish_model.reverse,
+                              repeat_log10=polish_model.reverse.repeat_log10 + 0.05 * rng.standard_normal(
+                                  polish_model.reverse.repeat_log10.shape))
+    gm = Model(engine, polish_model.forward, rev)
+    mpo = (MpoModel.from_state_model(polish_model.forward), MpoModel.from_state_model(rev))
+    jobs = synth.config_small(seed=12, n_reads=8).jobs()
+    assert 0 < int(np.sum(jobs.strand)) < jobs.n_jobs  # both strands present
+    _, worst = _run_and_check(engine, gm, mpo, jobs, polish_model.alignment)
+    assert worst <= 1e-4
+    gm.close()

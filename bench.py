@@ -15,8 +15,11 @@ buffers in pinned memory (host->device copies, planning, kernels, compaction
 and device->host copies of every tuple inside the timed region).
 
 --impl reference: the reference's own C implementation (pairwiseAligner.c /
-stateMachine.c compiled unmodified, OpenMP over reads on all host cores) on a
-bounded sample of the same workload.
+stateMachine.c compiled unmodified) on all host cores, OpenMP over chunks with
+schedule(dynamic,1) and the reads of a chunk in order (marginPolish.c:436-439),
+timed on a prefix of whole chunks of the same workload; its cells come from the
+reference's own band construction. That arm loads no library of this package:
+the workload generator is numpy only.
 
 Multi-GPU: one process per GPU (torchrun); reads are independent, so every rank
 runs its own full workload (weak scaling, no data-path collective); value is
@@ -38,8 +41,8 @@ sys.path.insert(0, ROOT)
 
 FLOP_PER_CELL = 48  # 30 FP32 FMA-pipe instructions per cell (forward 12, backward 12, posterior 6)
 # DRAM bytes (read + write) per band cell of the posterior kernel, from one ncu capture of the
-# same kernel on a 24-chunk slice of the workload (profiles/posteriorKernel_batched24_full.md);
-# traffic grows with cells, so a full launch moves this times its cells.
+# same kernel on a 24-chunk slice of the workload; traffic grows with cells, so a full launch
+# moves this times its cells.
 DRAM_BYTES_PER_CELL = 6.08
 METRIC = "GCUPS fwd+bwd+posterior (batched FP32 vs plain GPU, ≤1e-4 vs FP64); CPU ref"
 
@@ -53,7 +56,7 @@ def parse():
     ap.add_argument("--config", choices=["batched", "small"], default="batched")
     ap.add_argument("--chunks", type=int, default=256)
     ap.add_argument("--seed", type=int, default=2)
-    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work per baseline sample")
+    ap.add_argument("--cpu-seconds", type=float, default=8.0, help="CPU work per baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -135,17 +138,22 @@ def make_workload(args, rank):
     return synth.config_batched(seed=args.seed + rank, n_chunks=args.chunks)
 
 
-def cpu_sample(jobs, cells, target_cells):
-    """First jobs whose cells add up to about target_cells (a bounded sample of the workload)."""
+def chunk_offsets(wl):
+    """Job offsets of the workload's chunks (the jobs of a chunk are consecutive)."""
     import numpy as np
+    t = np.asarray(wl.read_template, dtype=np.int64)
+    assert t.size == 0 or np.all(np.diff(t) >= 0)
+    off = np.zeros(len(wl.templates) + 1, dtype=np.int64)
+    off[1:] = np.cumsum(np.bincount(t, minlength=len(wl.templates)))
+    return off
+
+
+def job_prefix(jobs, n):
+    """The first n jobs of a batch."""
     from marginpolish_b200 import Jobs
-    c = np.cumsum(cells)
-    n = int(np.searchsorted(c, target_cells)) + 1
-    n = max(1, min(n, jobs.n_jobs))
     a0, a1 = int(jobs.anchor_offsets[0]), int(jobs.anchor_offsets[n])
-    sub = Jobs(jobs.x_symbols, jobs.x_begin[:n], jobs.x_end[:n], jobs.y_symbols[:int(jobs.y_offsets[n])],
-               jobs.y_offsets[:n + 1], jobs.anchors[a0:a1], jobs.anchor_offsets[:n + 1], jobs.strand[:n])
-    return sub, int(c[n - 1])
+    return Jobs(jobs.x_symbols, jobs.x_begin[:n], jobs.x_end[:n], jobs.y_symbols[:int(jobs.y_offsets[n])],
+                jobs.y_offsets[:n + 1], jobs.anchors[a0:a1], jobs.anchor_offsets[:n + 1], jobs.strand[:n])
 
 
 def reference_models(ref, pm):
@@ -156,35 +164,72 @@ def reference_models(ref, pm):
     return hf, hr
 
 
-def time_reference(jobs, cells, pm, seconds, steps=1, warmup=0):
-    """Oracle A (the reference's own code) with OpenMP over reads on all host cores."""
-    from oracle.bindings import RefOracle
-    ref = RefOracle()
-    hf, hr = reference_models(ref, pm)
-    cores = os.cpu_count() or 1
-    # calibrate the sample size on a short run
-    probe, probe_cells = cpu_sample(jobs, cells, 4e6 * cores * 0.25)
-    t = time.perf_counter()
-    ref.align_batch(hf, hr, probe, pm.alignment, cores)
-    rate = probe_cells / max(time.perf_counter() - t, 1e-3)
-    sample, sample_cells = cpu_sample(jobs, cells, rate * seconds)
-    for _ in range(warmup):
-        ref.align_batch(hf, hr, sample, pm.alignment, cores)
-    times = []
-    for _ in range(steps):
+def reference_cells(ref, jobs, pm):
+    """Cells per job from the reference's own band construction (band_constructDynamic,
+    impl/pairwiseAligner.c:120-173, run through Oracle A)."""
+    import numpy as np
+    ap = pm.alignment
+    out = np.zeros(jobs.n_jobs, dtype=np.int64)
+    for j in range(jobs.n_jobs):
+        lx = int(jobs.x_end[j] - jobs.x_begin[j])
+        ly = int(jobs.y_offsets[j + 1] - jobs.y_offsets[j])
+        a = jobs.anchors[jobs.anchor_offsets[j]:jobs.anchor_offsets[j + 1]]
+        out[j] = ref.band_cells(a, lx, ly, ap.diagonal_expansion, ap.dynamic_anchor_expansion)
+    return out
+
+
+class ReferenceCpu:
+    """Oracle A (the reference's own code) on whole chunks: OpenMP over chunks with
+    schedule(dynamic,1) on all host cores, each chunk's reads in order on one thread."""
+
+    def __init__(self, pm, jobs, offsets):
+        from oracle.bindings import RefOracle
+        self.ref = RefOracle()
+        self.pm = pm
+        self.jobs = jobs
+        self.offsets = offsets
+        self.hf, self.hr = reference_models(self.ref, pm)
+        self.cores = os.cpu_count() or 1
+
+    def sample(self, n_chunks):
+        n_chunks = max(1, min(n_chunks, self.offsets.size - 1))
+        sub = job_prefix(self.jobs, int(self.offsets[n_chunks]))
+        return sub, self.offsets[:n_chunks + 1], int(reference_cells(self.ref, sub, self.pm).sum())
+
+    def run(self, sample, threads):
+        sub, off, _ = sample
         t = time.perf_counter()
-        ref.align_batch(hf, hr, sample, pm.alignment, cores)
-        times.append(time.perf_counter() - t)
-    # one core, on a sample of about a fifth of the time
-    one, one_cells = cpu_sample(jobs, cells, rate / cores * seconds * 0.2)
-    t = time.perf_counter()
-    ref.align_batch(hf, hr, one, pm.alignment, 1)
-    t1 = time.perf_counter() - t
-    ref.free_model(hf)
-    ref.free_model(hr)
-    return {"gcups": sample_cells / statistics.median(times) / 1e9, "cores": cores, "reads": sample.n_jobs,
-            "cells": sample_cells, "seconds": statistics.median(times),
-            "gcups_1core": one_cells / max(t1, 1e-9) / 1e9, "reads_1core": one.n_jobs}
+        self.ref.align_chunks(self.hf, self.hr, sub, off, self.pm.alignment, threads)
+        return time.perf_counter() - t
+
+    def calibrated_sample(self, seconds):
+        """A prefix of whole chunks, a multiple of the core count, of about `seconds` of work."""
+        probe = self.sample(self.cores)
+        t = self.run(probe, self.cores)
+        rounds = max(1, int(round(seconds / max(t, 1e-3))))
+        return probe if rounds == 1 else self.sample(self.cores * rounds)
+
+    def close(self):
+        self.ref.free_model(self.hf)
+        self.ref.free_model(self.hr)
+
+
+def time_reference(pm, wl, jobs, seconds, steps=1, warmup=0):
+    """The reference's CPU rate (GCUPS) on a prefix of whole chunks, all cores, plus one core on
+    the first chunk."""
+    import numpy as np
+    rc = ReferenceCpu(pm, jobs, chunk_offsets(wl))
+    sample = rc.calibrated_sample(seconds)
+    for _ in range(warmup):
+        rc.run(sample, rc.cores)
+    times = [rc.run(sample, rc.cores) for _ in range(steps)]
+    one = rc.sample(1)
+    t1 = rc.run(one, 1)
+    rc.close()
+    n_chunks = sample[1].size - 1
+    return {"gcups": sample[2] / float(np.median(times)) / 1e9, "cores": rc.cores, "chunks": n_chunks,
+            "reads": int(sample[1][-1]), "cells": sample[2], "seconds": float(np.median(times)),
+            "gcups_1core": one[2] / max(t1, 1e-9) / 1e9, "reads_1core": int(one[1][-1])}
 
 
 def accuracy_sample(jobs, res, pm, n_reads=6):
@@ -221,26 +266,24 @@ def run_reference_arm(args, rank, world):
     if not available_reference():
         print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libref_oracle.so missing"}))
         return
-    import numpy as np
-    from marginpolish_b200 import Engine, Model, realign_batch  # noqa: F401
     pm = load_model()
     wl = make_workload(args, 0)
     jobs = wl.jobs()
-    # cells per job from the band (the oracle counts them identically)
-    from oracle.bindings import ExactOracle
-    cells = band_cells(jobs, pm)
-    r = time_reference(jobs, cells, pm, args.cpu_seconds, steps=args.steps, warmup=args.warmup)
+    r = time_reference(pm, wl, jobs, args.cpu_seconds, steps=args.steps, warmup=args.warmup)
+    sample = (f"rate on a prefix of {r['chunks']} whole chunks ({r['reads']} reads, {r['cells']} cells) of the "
+              f"{len(wl.templates)}-chunk workload per step, OpenMP over chunks (schedule(dynamic,1)) on "
+              f"{r['cores']} threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": r["gcups"], "unit": "GCUPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["seconds"] * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": f"{args.config}: {wl.meta}", "reads_in_sample": r["reads"],
-                   "cells_per_step": r["cells"]},
+        "config": {"workload": f"{args.config}: {wl.meta}", "sample": sample, "chunks_in_sample": r["chunks"],
+                   "reads_in_sample": r["reads"], "cells_per_step": r["cells"]},
         "cpu_baseline": {"value": r["gcups"], "unit": "GCUPS", "cores": r["cores"], "kind": "reference",
-                         "sample": f"first {r['reads']} reads of the workload ({r['cells']} cells) per step"},
+                         "sample": sample, "value_1core": r["gcups_1core"],
+                         "sample_1core": f"first chunk ({r['reads_1core']} reads), 1 thread"},
         "e2e": {"value": r["gcups"], "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    del np, ExactOracle
     print(json.dumps(line), flush=True)
 
 
@@ -526,7 +569,7 @@ def run_ours(args, rank, world, local):
         h2d = int(pj.x_symbols.nbytes + pj.y_symbols.nbytes + pj.anchors.nbytes + pj.x_begin.nbytes * 2 +
                   pj.y_offsets.nbytes + pj.anchor_offsets.nbytes + pj.strand.nbytes + pj.x_shift.nbytes)
         d2h = 0
-        steps_e2e = max(1, min(args.steps, 3))
+        steps_e2e = args.steps
         for _ in range(steps_e2e):
             barrier()
             t = time.perf_counter()
@@ -571,13 +614,14 @@ def run_ours(args, rank, world, local):
         cpu = None
         if not args.no_cpu and world == 1:
             from oracle.bindings import available_reference
-            if available_reference():
-                cpc = band_cells(jobs, pm)
-                r = time_reference(jobs, cpc, pm, args.cpu_seconds)
+            if available_reference() and args.config == "batched":
+                r = time_reference(pm, wl, jobs, args.cpu_seconds)
                 cpu = {"value": r["gcups"], "unit": "GCUPS", "cores": r["cores"], "kind": "reference",
-                       "sample": f"first {r['reads']} reads of the workload ({r['cells']} cells), "
-                                 f"OpenMP over reads on {r['cores']} threads",
-                       "value_1core": r["gcups_1core"], "sample_1core": f"first {r['reads_1core']} reads, 1 thread",
+                       "sample": f"rate on a prefix of {r['chunks']} whole chunks ({r['reads']} reads, "
+                                 f"{r['cells']} cells), OpenMP over chunks (schedule(dynamic,1)) on "
+                                 f"{r['cores']} threads",
+                       "value_1core": r["gcups_1core"],
+                       "sample_1core": f"first chunk ({r['reads_1core']} reads), 1 thread",
                        "accuracy_of_timed_results": accuracy_sample(jobs, timed_res, pm)}
         line = {
             "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,

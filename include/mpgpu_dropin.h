@@ -8,10 +8,12 @@
  *   getAlignedPairsUsingAnchors             inc/pairwiseAligner.h:73    (impl/pairwiseAligner.c:1088-1103)
  *   getAlignedPairsWithIndels               inc/pairwiseAligner.h:67-69 (impl/pairwiseAligner.c:1141-1149)
  *   getAlignedPairs                         inc/pairwiseAligner.h:60-61 (impl/pairwiseAligner.c:1132-1139)
- *   computeForwardProbability               inc/pairwiseAligner.h:103-106 (impl/pairwiseAligner.c:813-865)
+ *   computeForwardProbability               inc/pairwiseAligner.h:54-55 (impl/pairwiseAligner.c:813-865)
+ *   getExpectationsUsingAnchors             inc/pairwiseAligner.h:103-104 (impl/pairwiseAligner.c:1151-1156)
+ *   getExpectations                         inc/pairwiseAligner.h:106 (impl/pairwiseAligner.c:1158-1164)
  *
  * The type declarations below restate the reference's public layouts
- * (inc/stateMachine.h:13-22, :40-48, :65-75, :101-124; inc/pairwiseAligner.h:28-39)
+ * (inc/stateMachine.h:13-22, :40-48, :60-75, :96-124, :138-148; inc/pairwiseAligner.h:28-39)
  * so that objects built by the caller are read correctly. stList / stIntTuple
  * are the caller's sonLib; the library resolves stList_* / stIntTuple_* from the
  * host application at load time. The StateMachine is lowered to flat tables
@@ -22,8 +24,15 @@
  * returned lists are newly allocated, own their stIntTuple elements and are
  * destroyed by the caller. Failures (no sm_100 device, malformed anchors,
  * unsupported machines) print the library's message and call exit(1), which
- * matches the reference's st_errAbort behaviour. Calls are serialised by an
- * internal mutex (the reference calls them from OpenMP threads).
+ * matches the reference's st_errAbort behaviour.
+ *
+ * Threading: the reference calls these from OpenMP threads, one chunk per thread
+ * (marginPolish.c:436-439). Each calling thread gets its own engine -- its own CUDA
+ * stream and device buffers, created on the thread's first call and released when
+ * the thread exits -- and its own cache of lowered machines, so concurrent callers'
+ * passes run side by side on the GPU. MPGPU_DEVICE selects the device (default 0).
+ * A machine is recognised by its address and a fingerprint of its values; its tables
+ * must not change in place once it has been passed in.
  */
 #ifndef MPGPU_DROPIN_H_
 #define MPGPU_DROPIN_H_
@@ -67,6 +76,20 @@ struct _emissions {
 };
 
 typedef enum { threeState = 2, threeStateAsymmetric = 3 } StateMachineType;
+typedef enum { nucleotideEmissions = 0, nucleotideEmissionsSymmetric = 1 } EmissionType;
+
+/* Expectation accumulator (inc/stateMachine.h:138-148); transitions[from * stateNumber + to]. */
+typedef struct _hmm {
+    StateMachineType type;
+    EmissionType emissionsType;
+    int64_t *emissionNoPerState;
+    int64_t *emissionOffsetPerState;
+    int64_t totalEmissions;
+    double *transitions;
+    double *emissions;
+    double likelihood;
+    int64_t stateNumber;
+} Hmm;
 
 typedef struct _stateMachine StateMachine;
 
@@ -113,10 +136,25 @@ void getAlignedPairsWithIndels(StateMachine *sM, SymbolString sX, SymbolString s
                                bool alignmentHasRaggedLeftEnd, bool alignmentHasRaggedRightEnd);
 stList *getAlignedPairs(StateMachine *sM, SymbolString sX, SymbolString sY, PairwiseAlignmentParameters *p,
                         bool alignmentHasRaggedLeftEnd, bool alignmentHasRaggedRightEnd);
-/* computeForwardProbability (impl/pairwiseAligner.c:813-865, inc/pairwiseAligner.h:103-106): ln P over
+/* computeForwardProbability (impl/pairwiseAligner.c:813-865, inc/pairwiseAligner.h:54-55): ln P over
  * the band of band_construct, through mp_forward_batch. */
 double computeForwardProbability(SymbolString sX, SymbolString sY, stList *anchorPairs, PairwiseAlignmentParameters *p,
                                  StateMachine *sM, bool alignmentHasRaggedLeftEnd, bool alignmentHasRaggedRightEnd);
+/* getExpectationsUsingAnchors (impl/pairwiseAligner.c:1151-1156, inc/pairwiseAligner.h:103-104): adds the
+ * expected transition counts E[n_ij] (impl/pairwiseAligner.c:347-357) of the read to
+ * hmmExpectations->transitions, through the adjoint pass mp_expectations_batch over the read's
+ * band and split rectangles, and adds (lX + lY) * ln P to hmmExpectations->likelihood (the
+ * reference adds its total once per posterior diagonal, impl/pairwiseAligner.c:674). Emission
+ * expectations are left alone, as in the reference (:359-362). The counts are those of the whole
+ * lattice; for a read whose band passes the reference's traceback points
+ * (minDiagsBetweenTraceBack) the reference seeds each segment's backward at that point instead,
+ * which moves its counts by the difference of those approximate posteriors. */
+void getExpectationsUsingAnchors(StateMachine *sM, Hmm *hmmExpectations, SymbolString sX, SymbolString sY,
+                                 stList *anchorPairs, PairwiseAlignmentParameters *p, bool alignmentHasRaggedLeftEnd,
+                                 bool alignmentHasRaggedRightEnd);
+/* getExpectations (impl/pairwiseAligner.c:1158-1164, inc/pairwiseAligner.h:106): the same without anchors. */
+void getExpectations(StateMachine *sM, Hmm *hmmExpectations, SymbolString sX, SymbolString sY,
+                     PairwiseAlignmentParameters *p, bool alignmentHasRaggedLeftEnd, bool alignmentHasRaggedRightEnd);
 
 /* Lowering of a caller's StateMachine to the flat description mp_model_create takes
  * (no device needed). repeat_out must hold 4*51*51 doubles; desc->repeat_log10 is set

@@ -523,8 +523,21 @@ int64_t splitCount(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, int64_
     return (int64_t) r.size();
 }
 
+void splitRects(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, int64_t maxSize, bool raggedL, bool raggedR,
+                std::vector<SplitRectH> &out) {
+    std::vector<SplitRect> r;
+    splitPoints(an, nA, lx, ly, maxSize, raggedL, raggedR, r);
+    out.clear();
+    for (const SplitRect &q : r) out.push_back(SplitRectH{q.x1, q.y1, q.x2, q.y2});
+}
+
 int64_t hullSlots(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, bool dynamic, int64_t fixedExp) {
     return hullSlotBound(an, nA, 0, 0, lx, ly, dynamic, fixedExp);
+}
+
+int64_t hullSlotsRect(const int32_t *an, int64_t nA, int64_t x1, int64_t y1, int64_t lx, int64_t ly, bool dynamic,
+                      int64_t fixedExp) {
+    return hullSlotBound(an, nA, x1, y1, lx, ly, dynamic, fixedExp);
 }
 }  // namespace mp
 

@@ -19,8 +19,16 @@ struct SplitRectH {
 };
 // Number of split rectangles of one job (getSplitPoints, impl/pairwiseAligner.c:899-926).
 int64_t splitCount(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, int64_t maxSize, bool raggedL, bool raggedR);
+// The split rectangles themselves (same rule; a single rectangle may be trimmed when a ragged
+// end skips the first or last large gap).
+void splitRects(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, int64_t maxSize, bool raggedL, bool raggedR,
+                std::vector<SplitRectH> &out);
 // Upper bound of the 5-diagonal band hull in window slots.
 int64_t hullSlots(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, bool dynamic, int64_t fixedExp);
+// The same bound for the sub-rectangle with origin (x1, y1) and lengths (lx, ly), whose anchors
+// are given in the job's coordinates.
+int64_t hullSlotsRect(const int32_t *an, int64_t nA, int64_t x1, int64_t y1, int64_t lx, int64_t ly, bool dynamic,
+                      int64_t fixedExp);
 // Checks anchor order / range / expansion parity of one job.
 mp_status validateAnchors(const int32_t *an, int64_t nA, int64_t lx, int64_t ly, bool dynamic, int64_t job);
 mp_status validateParamsStruct(const mp_params *p);

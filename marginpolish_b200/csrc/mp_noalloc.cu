@@ -11,15 +11,17 @@
 // library holds until the process exits.
 //
 // Limits (checked before any device work, MP_ERR_ARGUMENT beyond them): one
-// read, lx + ly <= MP_NOALLOC_MAX_DIAGONALS - 1, a single split rectangle,
-// and a band hull of at most 60 window slots (the narrowest slot class).
+// read, lx + ly <= MP_NOALLOC_MAX_DIAGONALS - 1, a single split rectangle
+// (possibly trimmed by a ragged end, as in the batched pass), and a band hull
+// of at most 60 window slots (the narrowest slot class).
 //
 // The first call on a device takes the array's device address with
 // cudaGetSymbolAddress while that device is current, so that first call
 // should happen before any stream capture. Calls share the array: the pass
 // writes every word it later reads (and zeroes its work counter and status
 // record itself), and calls serialise on an internal mutex and wait for their
-// own completion; two calls that ran on the GPU at the same time would race.
+// own completion, on the error paths too; two calls that ran on the GPU at the
+// same time would race.
 #include "../../include/mpgpu.h"
 #include "mp_host.h"
 #include "mp_internal.h"
@@ -83,7 +85,8 @@ static_assert(kUsed <= MP_NOALLOC_SCRATCH_BYTES, "no-allocation scratch layout e
 
 namespace {
 std::mutex gNoallocMutex;
-unsigned char *gNoallocAddr[128] = {nullptr};
+constexpr int kMaxDevices = 128;
+unsigned char *gNoallocAddr[kMaxDevices] = {nullptr};
 }  // namespace
 
 extern "C" mp_status mp_realign_single_noalloc(mp_engine *e, const mp_model *m, const mp_params *p,
@@ -107,21 +110,29 @@ extern "C" mp_status mp_realign_single_noalloc(mp_engine *e, const mp_model *m, 
     const bool dynamic = p->dynamic_anchor_expansion != 0;
     st = validateAnchors(anchors, nAnchors, lx, ly, dynamic, 0);
     if (st != MP_OK) return st;
-    if (splitCount(anchors, nAnchors, lx, ly, p->split_matrix_bigger_than_this, raggedLeft != 0, raggedRight != 0) !=
-        1)
+    // The single split rectangle of the read. With a ragged end the rule may skip the first or
+    // last large gap, so the rectangle can be a trimmed part of the matrix: the task then covers
+    // exactly that rectangle (origin x1, y1), as the batched planner does.
+    std::vector<SplitRectH> rects;
+    splitRects(anchors, nAnchors, lx, ly, p->split_matrix_bigger_than_this, raggedLeft != 0, raggedRight != 0, rects);
+    if (rects.size() != 1)
         return mp_fail(MP_ERR_ARGUMENT,
                        "mp_realign_single_noalloc: the read needs split rectangles; use mp_realign_batch");
-    const int64_t slots = hullSlots(anchors, nAnchors, lx, ly, dynamic, p->diagonal_expansion);
+    const SplitRectH r = rects[0];
+    const int64_t rlx = r.x2 - r.x1, rly = r.y2 - r.y1;
+    const int64_t slots = hullSlotsRect(anchors, nAnchors, r.x1, r.y1, rlx, rly, dynamic, p->diagonal_expansion);
     if (slots > 32 * kC - 2 * kC)
         return mp_fail(MP_ERR_ARGUMENT,
                        "mp_realign_single_noalloc: band hull of %lld slots exceeds the limit of %d; use "
                        "mp_realign_batch",
                        (long long) slots, 32 * kC - 2 * kC);
+    if (e->device < 0 || e->device >= kMaxDevices)
+        return mp_fail(MP_ERR_ARGUMENT, "mp_realign_single_noalloc: device index %d outside [0, %d)", e->device,
+                       kMaxDevices);
 
     std::lock_guard<std::mutex> lock(gNoallocMutex);
     cudaError_t ce = cudaSetDevice(e->device);
     if (ce != cudaSuccess) return mp_fail(MP_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(ce));
-    if (e->device < 0 || e->device >= 128) return mp_fail(MP_ERR_ARGUMENT, "device index out of range");
     if (gNoallocAddr[e->device] == nullptr) {
         // set-up, once per device, with that device current
         unsigned char *ptr = nullptr;
@@ -132,12 +143,24 @@ extern "C" mp_status mp_realign_single_noalloc(mp_engine *e, const mp_model *m, 
     }
     unsigned char *base = gNoallocAddr[e->device];
     cudaStream_t s = e->stream;
+    // Every return after the first queued copy waits for the stream first (declared after the
+    // lock, so it runs before the unlock): a failed call never leaves work that writes the shared
+    // array running while the next call starts.
+    struct StreamDrain {
+        cudaStream_t s;
+        bool armed = false;
+        ~StreamDrain() {
+            if (armed) (void) cudaStreamSynchronize(s);
+        }
+    } drain{s};
 
-    const int32_t N = (int32_t) (lx + ly);
+    const int32_t N = (int32_t) (rlx + rly);
     Task tk;
     memset(&tk, 0, sizeof(tk));
-    tk.lx = (int32_t) lx;
-    tk.ly = (int32_t) ly;
+    tk.lx = (int32_t) rlx;
+    tk.ly = (int32_t) rly;
+    tk.x1 = (int32_t) r.x1;
+    tk.y1 = (int32_t) r.y1;
     tk.nAnchors = (int32_t) nAnchors;
     tk.flags = (raggedLeft ? 1 : 0) | (raggedRight ? 2 : 0) | (strand ? 4 : 0) | (dynamic ? 8 : 0);
     tk.expansion = (int32_t) p->diagonal_expansion;
@@ -153,11 +176,14 @@ extern "C" mp_status mp_realign_single_noalloc(mp_engine *e, const mp_model *m, 
         if (_e != cudaSuccess) return mp_fail(MP_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(_e)); \
     } while (0)
 
+    drain.armed = true;
     NA_TRY(cudaMemcpyAsync(base + kOffTask, &tk, sizeof(tk), cudaMemcpyHostToDevice, s));
     NA_TRY(cudaMemcpyAsync(base + kOffTaskOut, &zero, sizeof(zero), cudaMemcpyHostToDevice, s));
     NA_TRY(cudaMemcpyAsync(base + kOffQueue, queueAndOrder, sizeof(queueAndOrder), cudaMemcpyHostToDevice, s));
-    if (lx > 0) NA_TRY(cudaMemcpyAsync(base + kOffXs, x, sizeof(uint16_t) * lx, cudaMemcpyHostToDevice, s));
-    if (ly > 0) NA_TRY(cudaMemcpyAsync(base + kOffYs, y, sizeof(uint16_t) * ly, cudaMemcpyHostToDevice, s));
+    if (rlx > 0)
+        NA_TRY(cudaMemcpyAsync(base + kOffXs, x + r.x1, sizeof(uint16_t) * rlx, cudaMemcpyHostToDevice, s));
+    if (rly > 0)
+        NA_TRY(cudaMemcpyAsync(base + kOffYs, y + r.y1, sizeof(uint16_t) * rly, cudaMemcpyHostToDevice, s));
     if (nAnchors > 0)
         NA_TRY(cudaMemcpyAsync(base + kOffAnchors, anchors, sizeof(int32_t) * 3 * nAnchors, cudaMemcpyHostToDevice, s));
 
@@ -197,6 +223,7 @@ extern "C" mp_status mp_realign_single_noalloc(mp_engine *e, const mp_model *m, 
     TaskOut res;
     NA_TRY(cudaMemcpyAsync(&res, dOut, sizeof(res), cudaMemcpyDeviceToHost, s));
     NA_TRY(cudaStreamSynchronize(s));
+    drain.armed = false;  // nothing of this call is in flight until the compaction below
     if (res.status & kTaskBand) return mp_fail(MP_ERR_ARGUMENT, "invalid band diagonal (anchors inconsistent)");
     if (res.status & kTaskSymbol) return mp_fail(MP_ERR_ARGUMENT, "a symbol's repeat count is >= %d", kMaxRepeat);
     if (res.status & (kTaskWindow | kTaskScratch))
@@ -227,6 +254,7 @@ extern "C" mp_status mp_realign_single_noalloc(mp_engine *e, const mp_model *m, 
         ca.x[k] = reinterpret_cast<int32_t *>(base + kOffOutList(k, 1));
         ca.y[k] = reinterpret_cast<int32_t *>(base + kOffOutList(k, 2));
     }
+    drain.armed = true;
     NA_TRY(launchCompact(ca, s));
     for (int k = 0; k < 3; k++) {
         const int64_t n = res.count[k];
@@ -236,6 +264,7 @@ extern "C" mp_status mp_realign_single_noalloc(mp_engine *e, const mp_model *m, 
         NA_TRY(cudaMemcpyAsync(out->y[k], ca.y[k], sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
     }
     NA_TRY(cudaStreamSynchronize(s));
+    drain.armed = false;
 #undef NA_TRY
     return MP_OK;
 }

@@ -1,9 +1,11 @@
-"""Sharding of independent reads across GPUs (one process per GPU).
+"""Sharding of chunks across GPUs (one process per GPU).
 
-Reads of different chunks -- and reads within a chunk, up to the POA update --
-are independent (the reference runs chunks in parallel, marginPolish.c:436-439),
-so a batch splits across ranks with no data-path collective: each rank runs the
-posterior pass on its own subset and only per-rank scalars are combined.
+Chunks are independent (the reference runs them in parallel, marginPolish.c:436-439),
+and a chunk's reads must stay together, since its POA update folds all of them
+into one graph. A batch therefore splits across ranks by whole chunks, assigned
+greedily longest-processing-time first by their estimated cells, with the model
+tables replicated and no data-path collective: each rank runs the posterior pass
+(and the polishing loop) on its own chunks, and only per-rank scalars are combined.
 """
 from __future__ import annotations
 
@@ -56,7 +58,28 @@ def estimated_cells(jobs: Jobs, half_width: int) -> np.ndarray:
     return (lx + ly + 1) * (2 * half_width + 2)
 
 
-def shard(jobs: Jobs, rank: int, world: int, half_width: int = 25) -> tuple[Jobs, np.ndarray]:
-    """This rank's share of a batch and the indices of its jobs in the batch."""
-    parts = assign_lpt(estimated_cells(jobs, half_width), world)
-    return subset(jobs, parts[rank]), parts[rank]
+def chunk_costs(jobs: Jobs, chunk_offsets: np.ndarray, half_width: int) -> np.ndarray:
+    """Estimated cells of each chunk (its jobs are chunk_offsets[c] .. chunk_offsets[c+1]-1)."""
+    per_job = estimated_cells(jobs, half_width)
+    csum = np.concatenate([[0], np.cumsum(per_job)])
+    off = np.asarray(chunk_offsets, dtype=np.int64)
+    return csum[off[1:]] - csum[off[:-1]]
+
+
+def shard_chunks(chunk_offsets: np.ndarray, costs: np.ndarray, rank: int, world: int) -> tuple[np.ndarray, np.ndarray]:
+    """This rank's chunks (LPT over the chunk costs) and the indices of their jobs, in chunk order."""
+    off = np.asarray(chunk_offsets, dtype=np.int64)
+    chunks = assign_lpt(costs, world)[rank]
+    idx = (np.concatenate([np.arange(off[c], off[c + 1]) for c in chunks]) if chunks.size
+           else np.zeros(0, np.int64))
+    return chunks, idx
+
+
+def shard(jobs: Jobs, rank: int, world: int, chunk_offsets: np.ndarray = None,
+          half_width: int = 25) -> tuple[Jobs, np.ndarray]:
+    """This rank's share of a batch (whole chunks) and the indices of its jobs in the batch.
+    chunk_offsets (n_chunks + 1 job offsets) defaults to one chunk per job."""
+    if chunk_offsets is None:
+        chunk_offsets = np.arange(jobs.n_jobs + 1, dtype=np.int64)
+    _, idx = shard_chunks(chunk_offsets, chunk_costs(jobs, chunk_offsets, half_width), rank, world)
+    return subset(jobs, idx), idx

@@ -11,6 +11,12 @@ getAlignedPairsWithIndelsCroppingReference (impl/polisher.c:613-628).
 Error model: homopolymer run length perturbed by +-1 (p=0.15) or +-2
 (p=0.03), then per base: deletion 5%, substitution 3%, insertion after the
 base 4%. Generator: numpy PCG64 with the given seed.
+
+The generator's integer steps (run-length encoding, symbols, run-length anchors,
+reference crop) are numpy restatements of the same reference rules, so that
+building a workload maps no native library: the reference arm of the benchmark
+generates its inputs without loading the CUDA library. tests/test_rle.py checks
+them bit-exact against the library's routines.
 """
 from __future__ import annotations
 
@@ -20,9 +26,77 @@ from typing import List, Optional
 import numpy as np
 
 from .realign import Jobs
-from .rle import RleString, crop_range, rle_anchors
+from .rle import RleString
 
 BASES = np.frombuffer(b"ACGT", dtype=np.uint8)
+
+# nucleotide alphabet of impl/stateMachine.c:25-42 ('N' and every other character -> 4)
+_SYMBOL_OF = np.full(256, 4, dtype=np.uint16)
+for _c, _v in zip(b"ACGTacgt", (0, 1, 2, 3, 0, 1, 2, 3)):
+    _SYMBOL_OF[_c] = _v
+
+
+def rle_encode(seq) -> RleString:
+    """rleString_construct (impl/polisher.c:1357-1389): one run per maximal stretch of equal
+    characters (case-sensitive)."""
+    a = np.frombuffer(bytes(seq), dtype=np.uint8) if not isinstance(seq, np.ndarray) else seq.astype(np.uint8)
+    if a.size == 0:
+        return RleString(b"", np.zeros(0, dtype=np.uint32))
+    ends = np.concatenate([np.nonzero(a[1:] != a[:-1])[0], [a.size - 1]])
+    starts = np.concatenate([[0], ends[:-1] + 1])
+    return RleString(a[ends].tobytes(), (ends - starts + 1).astype(np.uint32))
+
+
+def rle_symbols(r: RleString, include_counts: bool = True, max_repeat_exclusive: int = 51) -> np.ndarray:
+    """rleString_constructSymbolString (impl/stateMachine.c:133-146): base symbol, and the run
+    length clamped to max_repeat_exclusive - 1 in the high byte (symbol_addRepeatCount, :124-131)."""
+    b = _SYMBOL_OF[np.frombuffer(r.chars, dtype=np.uint8)]
+    if include_counts:
+        rc = np.minimum(r.counts.astype(np.int64), max_repeat_exclusive - 1).astype(np.uint16)
+        b = (rc << np.uint16(8)) | b
+    return b.astype(np.uint16)
+
+
+def rle_anchors_monotone(pairs: np.ndarray, x: RleString, y: RleString) -> np.ndarray:
+    """runLengthEncodeAlignment (impl/polisher.c:1732-1750) for base pairs strictly increasing in
+    both coordinates: each pair goes through the non-RLE -> RLE coordinate maps (:1718-1730) and is
+    kept when both RLE coordinates exceed the last kept pair's. The mapped coordinates are then
+    non-decreasing, so the pair kept after pair i is the first j with x2[j] > x2[i] and
+    y2[j] > y2[i], i.e. the larger of the two searchsorted positions; the kept pairs are the orbit
+    of pair 0 under that successor map, found by doubling."""
+    pairs = np.asarray(pairs, dtype=np.int64).reshape(-1, 3)
+    m = pairs.shape[0]
+    if m == 0:
+        return np.zeros((0, 3), dtype=np.int32)
+    if np.any(np.diff(pairs[:, 0]) <= 0) or np.any(np.diff(pairs[:, 1]) <= 0):
+        raise ValueError("base pairs must be strictly increasing in both coordinates")
+    xmap = np.repeat(np.arange(len(x), dtype=np.int64), x.counts.astype(np.int64))
+    ymap = np.repeat(np.arange(len(y), dtype=np.int64), y.counts.astype(np.int64))
+    x2 = xmap[pairs[:, 0]]
+    y2 = ymap[pairs[:, 1]]
+    succ = np.empty(m + 1, dtype=np.int64)
+    succ[:m] = np.maximum(np.searchsorted(x2, x2, side="right"), np.searchsorted(y2, y2, side="right"))
+    succ[m] = m  # sink
+    orbit = np.zeros(1, dtype=np.int64)
+    step = succ
+    while orbit[-1] < m:
+        orbit = np.concatenate([orbit, step[orbit]])  # the next len(orbit) members
+        step = step[step]
+    keep = np.unique(orbit[orbit < m])
+    return np.stack([x2[keep], y2[keep], pairs[keep, 2]], axis=1).astype(np.int32)
+
+
+def crop_range(anchors: np.ndarray, template_length: int, read_length: int) -> tuple:
+    """Template crop of getAlignedPairsWithIndelsCroppingReference (impl/polisher.c:613-628):
+    [max(0, x0 - y0), min(lX, 1 + xN + (lY - yN)))."""
+    a = np.asarray(anchors, dtype=np.int64).reshape(-1, 3)
+    if a.shape[0] == 0:
+        return 0, int(template_length)
+    s = max(0, int(a[0, 0] - a[0, 1]))
+    e = min(int(template_length), int(1 + a[-1, 0] + (read_length - a[-1, 1])))
+    if s >= template_length or e < 0:
+        raise ValueError("crop range outside the template")
+    return s, e
 
 
 @dataclass
@@ -49,7 +123,7 @@ class Workload:
 
     def jobs(self, max_repeat_exclusive: int = 51, include_counts: bool = True) -> Jobs:
         """Cropped jobs exactly as poa_realign hands them to the aligner."""
-        tsyms = [t.symbols(include_counts, max_repeat_exclusive) for t in self.templates]
+        tsyms = [rle_symbols(t, include_counts, max_repeat_exclusive) for t in self.templates]
         toff = np.zeros(len(tsyms) + 1, dtype=np.int64)
         toff[1:] = np.cumsum([s.size for s in tsyms])
         xs = np.concatenate(tsyms) if tsyms else np.zeros(0, np.uint16)
@@ -68,7 +142,7 @@ class Workload:
             aa = a.copy()
             aa[:, 0] -= s
             an_list.append(aa)
-            ys_list.append(r.symbols(include_counts, max_repeat_exclusive))
+            ys_list.append(rle_symbols(r, include_counts, max_repeat_exclusive))
             yoff[i + 1] = yoff[i] + ys_list[-1].size
             aoff[i + 1] = aoff[i] + aa.shape[0]
         ys = np.concatenate(ys_list) if ys_list else np.zeros(0, np.uint16)
@@ -151,13 +225,13 @@ def sample_reads(rng, template: np.ndarray, n_reads: int, length_sampler, em: Er
 
 def build_workload(name: str, rng, templates_ascii: List[np.ndarray], reads_per_template: List[list],
                    expansion: int, meta: dict) -> Workload:
-    templates = [RleString.from_string(t.tobytes()) for t in templates_ascii]
+    templates = [rle_encode(t) for t in templates_ascii]
     reads, anchors, rt, strand = [], [], [], []
     for ti, lst in enumerate(reads_per_template):
         for read, pairs, s in lst:
-            r = RleString.from_string(read.tobytes())
+            r = rle_encode(read)
             p = np.concatenate([pairs, np.full((pairs.shape[0], 1), expansion, dtype=np.int64)], axis=1)
-            a = rle_anchors(p, templates[ti], r)
+            a = rle_anchors_monotone(p, templates[ti], r)
             if a.shape[0] == 0 or len(r) == 0:
                 continue
             reads.append(r)
@@ -207,6 +281,25 @@ def config_adjoint(seed: int = 4, n_reads: int = 512, n_templates: int = 64, tem
         per[ti] += sample_reads(rng, templates[ti], 1, lambda: rng.integers(2000, 5001), em)
     return build_workload("adjoint", rng, templates, per, 2 * half_width,
                           {"reads": n_reads, "templates": n_templates, "half_width": half_width})
+
+
+def config_long_reads(seed: int, lengths, half_width: int, template_len: int = 160_000) -> Workload:
+    """Reads of the given base lengths sampled from one homopolymer-enriched template (GC 0.5,
+    geometric run lengths p = 0.55, capped at 20) with the nanopore-like error model, anchors of
+    band half-width `half_width` (the long reads of the polishing configurations at scale)."""
+    rng = np.random.default_rng(seed)
+    em = ErrorModel()
+    t = random_template(rng, template_len, gc=0.5, run_p=0.55, run_cap=20)
+    lst = []
+    for ln in lengths:
+        ln = int(min(ln, t.size))
+        off = int(rng.integers(0, t.size - ln + 1))
+        read, pairs = mutate_read(rng, t[off:off + ln], em)
+        pairs[:, 0] += off
+        lst.append((read, pairs, int(rng.integers(0, 2))))
+    return build_workload("long_reads", rng, [t], [lst], 2 * half_width,
+                          {"template_bp": template_len, "read_bp": [int(v) for v in lengths],
+                           "half_width": half_width})
 
 
 def draft_with_errors(rng: np.random.Generator, truth: np.ndarray, rate: float = 0.01, hp_bias: float = 0.7):
@@ -267,7 +360,7 @@ def config_polish(seed: int = 3, n_chunks: int = 1, chunk_len: int = 2000, cover
         d, t2d = draft_with_errors(rng, t, draft_error)
         tmap = np.full(t.size, -1, dtype=np.int64)
         tmap[t2d[:, 0]] = t2d[:, 1]
-        drle = RleString.from_string(d.tobytes())
+        drle = rle_encode(d)
         if read_lognormal is not None:
             med, sig, mx = read_lognormal
             mean_len = min(float(mx), float(med) * float(np.exp(sig ** 2 / 2)))
@@ -290,17 +383,17 @@ def config_polish(seed: int = 3, n_chunks: int = 1, chunk_len: int = 2000, cover
             lst.append((read, pairs, int(rng.integers(0, 2))))
         cr, cs, ca = [], [], []
         for read, pairs, s in lst:
-            r = RleString.from_string(read.tobytes())
+            r = rle_encode(read)
             dp = tmap[pairs[:, 0]]
             ok = dp >= 0
             p = np.stack([dp[ok], pairs[ok, 1], np.full(int(ok.sum()), 2 * half_width)], axis=1)
-            a = rle_anchors(p, drle, r)
+            a = rle_anchors_monotone(p, drle, r)
             if a.shape[0] == 0 or len(r) == 0:
                 continue
             cr.append(r)
             cs.append(s)
             ca.append(a)
-        truths.append(RleString.from_string(t.tobytes()))
+        truths.append(rle_encode(t))
         drafts.append(drle)
         reads.append(cr)
         strands.append(cs)

@@ -129,6 +129,10 @@ class RefOracle:
         lib.refo_align_batch.argtypes = [c_void_p, c_void_p, c_int64, P(c_int64), P(c_uint16), P(c_int64),
                                          P(c_uint16), P(c_int64), P(c_int64), P(c_uint8), P(OracleParams), c_int,
                                          P(c_int64), c_void_p]
+        lib.refo_align_chunks.restype = c_int64
+        lib.refo_align_chunks.argtypes = [c_void_p, c_void_p, c_int64, P(c_int64), P(c_int64), P(c_uint16),
+                                          P(c_int64), P(c_uint16), P(c_int64), P(c_int64), P(c_uint8),
+                                          P(OracleParams), c_int, P(c_int64)]
         lib.refo_band.argtypes = [P(c_int64), c_int64, c_int64, c_int64, c_int64, c_int, P(c_int64)]
         lib.refo_split_points.restype = c_int64
         lib.refo_split_points.argtypes = [P(c_int64), c_int64, c_int64, c_int64, c_int64, c_int, c_int, P(c_int64),
@@ -201,11 +205,36 @@ class RefOracle:
         del xoff_b
         return counts
 
+    def align_chunks(self, hf, hr, jobs, chunk_offsets, params, n_threads=0):
+        """OpenMP over chunks (schedule(dynamic,1)), the reads of a chunk in order on one thread,
+        as marginPolish.c:436-439 runs poa_realign; chunk c is jobs chunk_offsets[c] ..
+        chunk_offsets[c+1]-1. Returns per-job tuple counts (n, 3)."""
+        n = jobs.n_jobs
+        xs, xo = _gather_x(jobs)
+        op = OracleParams.from_alignment(params)
+        counts = np.zeros((n, 3), dtype=np.int64)
+        an = np.ascontiguousarray(jobs.anchors, dtype=np.int64)
+        co = np.ascontiguousarray(chunk_offsets, dtype=np.int64)
+        assert co[0] == 0 and co[-1] == n
+        self.lib.refo_align_chunks(hf, hr, co.size - 1, _p(co, c_int64), _p(xo, c_int64), _p(xs, c_uint16),
+                                   _p(jobs.y_offsets, c_int64), _p(jobs.y_symbols, c_uint16),
+                                   _p(jobs.anchor_offsets, c_int64), _p(an, c_int64), _p(jobs.strand, c_uint8),
+                                   ctypes.byref(op), n_threads, _p(counts, c_int64))
+        return counts
+
     def band(self, anchors, lx, ly, expansion, dynamic):
         a = np.ascontiguousarray(np.asarray(anchors, dtype=np.int64).reshape(-1, 3))
         out = np.zeros((lx + ly + 1, 3), dtype=np.int64)
         self.lib.refo_band(_p(a, c_int64), a.shape[0], lx, ly, expansion, int(dynamic), _p(out, c_int64))
         return out
+
+    def band_cells(self, anchors, lx, ly, expansion, dynamic) -> int:
+        """Cells of one job's band from the reference's own band construction: the sum over
+        anti-diagonals of (xmyR - xmyL) / 2 + 1."""
+        if lx + ly == 0:
+            return 0
+        b = self.band(anchors, lx, ly, expansion, dynamic)
+        return int(((b[:, 2] - b[:, 1]) // 2 + 1).sum())
 
     def split_points(self, anchors, lx, ly, max_size, ragged_left, ragged_right):
         a = np.ascontiguousarray(np.asarray(anchors, dtype=np.int64).reshape(-1, 3))
@@ -301,7 +330,7 @@ class ExactOracle:
         op = OracleParams.from_alignment(params)
         r = self.lib.mpo_align_with_indels(ctypes.byref(model), _p(sx, c_uint16), sx.size, _p(sy, c_uint16), sy.size,
                                            _p(a, c_int64), a.shape[0], ctypes.byref(op), int(ragged_left),
-                                           int(ragged_right), logadd, 1 if dense else 0)
+                                           int(ragged_right), logadd, 2 if dense == "near" else (1 if dense else 0))
         rc = r.contents
         out = {
             "pairs": tuple(_tuples(rc.t[k], rc.n[k]) for k in range(3)),

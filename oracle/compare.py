@@ -76,7 +76,9 @@ def set_diff_against_reference(gpu_lists, ref_lists, oracle_out, threshold, band
         g = {(int(x), int(y)) for _, x, y in np.asarray(gpu_lists[k]).reshape(-1, 3)}
         r = {(int(x), int(y)) for _, x, y in np.asarray(ref_lists[k]).reshape(-1, 3)}
         for key in g ^ r:
-            p = table[key][k]
+            rec = table.get(key)
+            assert rec is not None, f"list {k}: {key} differs from the reference, far below the threshold in FP64"
+            p = rec[k]
             assert abs(p - threshold) <= band, f"list {k}: {key} differs from the reference with FP64 p={p}"
             ndiff += 1
     return ndiff

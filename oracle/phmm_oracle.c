@@ -209,6 +209,7 @@ static void tupleAppend(TupleBuf *b, int64_t w, int64_t x, int64_t y) {
 typedef struct {
     int64_t n, cap;
     double *v;
+    double floor; /* records are kept when one of the cell's posteriors is at least this */
 } DenseBuf;
 
 static void denseAppend(DenseBuf *b, double x, double y, double pm, double px, double py) {
@@ -401,7 +402,7 @@ static void posteriorDiagonal(Sub *s, int64_t d, double total, TupleBuf *out, De
             py = exp((f[2] + b[2]) - total);
             addPosterior(s->p, &out[2], x, y, py);
         }
-        if (dense != NULL) {
+        if (dense != NULL && (pm >= dense->floor || px >= dense->floor || py >= dense->floor)) {
             denseAppend(dense, (double) (x - 1), (double) (y - 1), pm, px, py);
         }
     }
@@ -690,6 +691,10 @@ MpoResult *mpo_align_with_indels(const MpoModel *model, const uint16_t *sx, int6
     memset(final, 0, sizeof(final));
     DenseBuf dense;
     memset(&dense, 0, sizeof(dense));
+    /* wantDense 1: every band cell of every posterior diagonal; 2: only cells with a posterior
+     * within 1e-3 of the threshold or above it (enough to check emitted tuples and completeness
+     * on long reads) */
+    dense.floor = wantDense == 2 ? params->threshold - 1e-3 : -HUGE_VAL;
     int64_t *subAnchors = malloc(sizeof(int64_t) * 3 * (nAnchors > 0 ? nAnchors : 1));
     int64_t j = 0;
     int failed = 0;

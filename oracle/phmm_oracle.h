@@ -62,7 +62,9 @@ typedef struct {
     double *dense;          /* nDense*5: x, y, pM, pX, pY in emission order; -1 = not defined */
 } MpoResult;
 
-/* Full posterior pass of one job (getAlignedPairsWithIndelsUsingAnchors semantics). */
+/* Full posterior pass of one job (getAlignedPairsWithIndelsUsingAnchors semantics). wantDense:
+ * 0 none, 1 a record for every band cell of every posterior diagonal, 2 only the records of cells
+ * with a posterior of at least threshold - 1e-3. */
 MpoResult *mpo_align_with_indels(const MpoModel *model, const uint16_t *sx, int64_t lx, const uint16_t *sy,
                                  int64_t ly, const int64_t *anchors, int64_t nAnchors, const MpoParams *params,
                                  int raggedLeft, int raggedRight, MpoLogAddFn logAdd, int wantDense);

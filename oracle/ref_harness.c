@@ -339,6 +339,37 @@ int64_t refo_align_batch(void *modelFwd, void *modelRev, int64_t nJobs,
     return nJobs;
 }
 
+/* The same over chunks: OpenMP over chunks with schedule(dynamic,1), the reads of a chunk  */
+/* aligned one after another by the thread that holds the chunk -- the parallel loop of     */
+/* marginPolish.c:436-439 around poa_realign's per-read loop (impl/polisher.c:656-703).     */
+/* Chunk c holds jobs chunkOffsets[c] .. chunkOffsets[c+1]-1. Fills counts (nJobs*3).       */
+int64_t refo_align_chunks(void *modelFwd, void *modelRev, int64_t nChunks, const int64_t *chunkOffsets,
+                          const int64_t *xOffsets, const uint16_t *xSymbols,
+                          const int64_t *yOffsets, const uint16_t *ySymbols,
+                          const int64_t *anchorOffsets, const int64_t *anchors,
+                          const uint8_t *strand, const RefoParams *params, int nThreads, int64_t *counts) {
+#ifdef _OPENMP
+    if (nThreads > 0) {
+        omp_set_num_threads(nThreads);
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+    for (int64_t c = 0; c < nChunks; c++) {
+        for (int64_t j = chunkOffsets[c]; j < chunkOffsets[c + 1]; j++) {
+            RefoPairs *r = refo_align_with_indels(strand[j] ? modelFwd : modelRev,
+                                                  xSymbols + xOffsets[j], xOffsets[j + 1] - xOffsets[j],
+                                                  ySymbols + yOffsets[j], yOffsets[j + 1] - yOffsets[j],
+                                                  anchors + 3 * anchorOffsets[j],
+                                                  anchorOffsets[j + 1] - anchorOffsets[j], params, 0, 0);
+            for (int k = 0; k < 3; k++) {
+                counts[3 * j + k] = r->n[k];
+            }
+            refo_pairs_free(r);
+        }
+    }
+    return nChunks;
+}
+
 void refo_free(void *p) {
     free(p);
 }

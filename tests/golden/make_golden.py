@@ -75,4 +75,7 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    tree = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MP_REFERENCE_TREE")
+    if not tree:
+        sys.exit("usage: make_golden.py <reference tree> (or set MP_REFERENCE_TREE)")
+    main(tree)

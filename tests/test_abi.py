@@ -32,7 +32,7 @@ def test_drop_in_exports_reference_signatures():
     dropin = os.path.join(os.path.dirname(_lib.LIB_PATH), "libmpgpu_dropin.so")
     out = os.popen(f"nm -D --defined-only {dropin}").read()
     names = _declared("mpgpu_dropin.h", ("get", "mpd_", "compute"))
-    assert len(names) == 6 and "computeForwardProbability" in names
+    assert len(names) == 8 and "computeForwardProbability" in names and "getExpectationsUsingAnchors" in names
     for n in names:
         assert re.search(rf"\bT {n}\b", out), n
     undefined = os.popen(f"nm -D --undefined-only {dropin}").read()

@@ -61,3 +61,28 @@ def test_crop_range_follows_reference():
     assert crop_range(anchors, 100, 40) == (7, 46)
     assert crop_range(np.zeros((0, 3), np.int32), 100, 40) == (0, 100)
     assert crop_range(np.array([[2, 5, 0]], np.int32), 30, 400) == (0, 30)
+
+
+def test_generator_restatements_match_the_library():
+    """The workload generator's numpy routines (so that generating inputs maps no native library)
+    give bit-identical results to the library's run-length encoding, symbols, anchors and crop."""
+    from marginpolish_b200 import synth
+    rng = np.random.default_rng(3)
+    for _ in range(100):
+        s = "".join(rng.choice(list("ACGTacgtN"), size=int(rng.integers(0, 200))))
+        a, b = synth.rle_encode(s.encode()), RleString.from_string(s)
+        assert a.chars == b.chars and np.array_equal(a.counts, b.counts)
+        for inc, mx in ((True, 51), (True, 50), (False, 51)):
+            assert np.array_equal(synth.rle_symbols(a, inc, mx), b.symbols(inc, mx))
+    for _ in range(100):
+        x = RleString.from_string("".join(rng.choice(list("ACGT"), size=300, p=[0.4, 0.1, 0.1, 0.4])))
+        y = RleString.from_string("".join(rng.choice(list("ACGT"), size=280, p=[0.4, 0.1, 0.1, 0.4])))
+        n = int(rng.integers(0, 250))
+        px = np.sort(rng.choice(300, size=n, replace=False))
+        py = np.sort(rng.choice(280, size=n, replace=False))
+        pairs = np.stack([px, py, 2 * rng.integers(0, 30, size=n)], axis=1)
+        assert np.array_equal(synth.rle_anchors_monotone(pairs, x, y), rle_anchors(pairs, x, y))
+        if n:
+            an = rle_anchors(pairs, x, y)
+            if an.shape[0]:
+                assert synth.crop_range(an, len(x), len(y)) == crop_range(an, len(x), len(y))

@@ -67,12 +67,10 @@ def parse():
     ap.add_argument("--no-graphs", action="store_true", help="direct launches instead of CUDA graph replay")
     ap.add_argument("--autotune-chunks", type=int, default=24,
                     help="chunks of the separate seeded sample the autotuner times the kernel variants on (0 = off)")
-    ap.add_argument("--polish-large", action="store_true",
-                    help="also time the POA loop on 10 chunks of 110 kb (1 Mb in 100 kb chunks with 10 kb overlap), "
-                         "50x, log-normal reads (median 20 kb, max 100 kb), band half-width 64")
-    ap.add_argument("--polish-5mb", action="store_true",
-                    help="also time one realign+consensus pass on 5 Mb as 50 chunks of 100 kb, 60x, log-normal "
-                         "reads (median 25 kb, max 150 kb), band half-width 96")
+    ap.add_argument("--chunks-5mb", type=int, default=20,
+                    help="chunks of the 5 Mb configuration (of 50) whose realignment pass is measured")
+    ap.add_argument("--no-scale", action="store_true",
+                    help="skip the 1 Mb polishing-loop and 5 Mb realignment-pass measurements")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the adjoint and POA-loop measurements reported beside the headline")
     return ap.parse_args()
@@ -412,42 +410,87 @@ def measure_polish(engine, model, pm):
     return best
 
 
-def measure_polish_5mb(engine, model, pm):
-    """One realign+consensus pass at scale: 5 Mb as 50 independent chunks of 100 kb
-    (homopolymer-enriched: geometric run lengths, p = 0.55), 60x, log-normal reads (median 25
-    kb, sigma 0.6, at most 150 kb, clipped to the chunk), band half-width 96, drafts with 1%
-    indels."""
-    from marginpolish_b200 import PoaSet, PolishParams, synth
-    t0 = time.perf_counter()
-    wl = synth.config_polish(seed=53, n_chunks=50, chunk_len=100_000, coverage=60, half_width=96,
-                             hp_runs=True, read_lognormal=(25_000, 0.6, 150_000))
-    gen = time.perf_counter() - t0
-    s = PoaSet.from_polish_model(engine, model, pm, PolishParams(max_iterations=1), wl.drafts, wl.reads,
-                                 wl.strands, wl.anchors)
-    t0 = time.perf_counter()
-    s.realign()
-    t1 = time.perf_counter()
-    s.iterate()
-    t2 = time.perf_counter()
-    s.close()
-    return {"seconds": t2 - t0, "realign_seconds": t1 - t0, "consensus_and_realign_seconds": t2 - t1,
-            "generation_s": round(gen, 1), "workload": measure_polish_5mb.__doc__.split("\n")[0],
-            "chunks": 50, "reads": int(sum(len(r) for r in wl.reads)),
-            "bases": int(sum(r.non_rle_length for lst in wl.reads for r in lst))}
+def config_1mb():
+    """The polishing loop at genome scale: 1 Mb as 10 chunks of 110 kb (100 kb plus 10 kb
+    overlap; independent synthetic templates, since chunk stitching is outside this library),
+    50x, log-normal reads (median 20 kb, sigma 0.6, at most 100 kb, clipped to the chunk), band
+    half-width 64, drafts with 1% homopolymer-biased indels."""
+    from marginpolish_b200 import synth
+    return synth.config_polish(seed=47, n_chunks=10, chunk_len=110_000, coverage=50, half_width=64, hp_runs=True,
+                               read_lognormal=(20_000, 0.6, 100_000))
 
 
-def measure_polish_large(engine, model, pm):
-    """The POA loop at genome scale: 1 Mb as 10 chunks of 110 kb (100 kb plus 10 kb overlap;
-    independent synthetic templates, since chunk stitching is outside this library), 50x,
-    log-normal reads (median 20 kb, sigma 0.6, at most 100 kb, clipped to the chunk), band
-    half-width 64, drafts with 1% homopolymer-biased indels, up to 5 iterations."""
-    from marginpolish_b200 import PoaSet, PolishParams, synth
+def config_5mb(n_chunks=50):
+    """The large-scale pass: 5 Mb as 50 independent chunks of 100 kb (homopolymer-enriched:
+    geometric run lengths, p = 0.55), 60x, log-normal reads (median 25 kb, sigma 0.6, at most
+    150 kb, clipped to the chunk), band half-width 96, drafts with 1% indels."""
+    from marginpolish_b200 import synth
+    return synth.config_polish(seed=53, n_chunks=n_chunks, chunk_len=100_000, coverage=60, half_width=96,
+                               hp_runs=True, read_lognormal=(25_000, 0.6, 150_000))
+
+
+def measure_realign_pass(engine, model, pm, wl, peak, cpu_seconds, plain_reads=16):
+    """The first realignment pass of a polishing workload (every read against its chunk's draft)
+    in the device-resident form of the headline: GCUPS (band + posterior kernels, CUDA events,
+    inputs resident in HBM), the posterior kernel's FP32-roofline fraction, the plain
+    one-read-per-launch form on its first reads, and the reference's own code (Oracle A) on all
+    host cores on a bounded prefix of the same jobs (OpenMP over reads)."""
+    import numpy as np
+    from marginpolish_b200 import DeviceBatch
     t0 = time.perf_counter()
-    wl = synth.config_polish(seed=47, n_chunks=10, chunk_len=110_000, coverage=50, half_width=64,
-                             hp_runs=True, read_lognormal=(20_000, 0.6, 100_000))
-    gen = time.perf_counter() - t0
-    pp = PolishParams(max_iterations=5)
-    s = PoaSet.from_polish_model(engine, model, pm, pp, wl.drafts, wl.reads, wl.strands, wl.anchors)
+    jobs = wl.realign_workload().jobs()
+    db = DeviceBatch(engine, model, pm.alignment, jobs)
+    plan_s = time.perf_counter() - t0
+    for _ in range(2):
+        db.run()
+    cells, n_tasks, _ = db.stats()
+    ms, post = [], []
+    for _ in range(5):
+        ms.append(db.run())
+        post.append(db.timing()[1])
+    m, p = float(np.median(ms)), float(np.median(post))
+    achieved = cells * FLOP_PER_CELL / (p * 1e-3) / 1e12
+    p_ms, p_cells = db.run_plain(plain_reads)
+    db.close()
+    out = {"reads": jobs.n_jobs, "cells": cells, "tasks": n_tasks, "ms": m, "gcups": cells / (m * 1e-3) / 1e9,
+           "posterior_ms": p,
+           "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                        "frac": achieved / peak},
+           "plain_gpu": {"gcups": p_cells / (p_ms * 1e-3) / 1e9, "reads": min(plain_reads, n_tasks), "cells": p_cells},
+           "plan_and_upload_s": round(plan_s, 2)}
+    from oracle.bindings import RefOracle, available_reference
+    if available_reference():
+        ref = RefOracle()
+        hf, hr = reference_models(ref, pm)
+        cores = os.cpu_count() or 1
+        pc = reference_cells(ref, job_prefix(jobs, min(jobs.n_jobs, 4 * cores)), pm)
+
+        def run(n):
+            t = time.perf_counter()
+            ref.align_batch(hf, hr, job_prefix(jobs, n), pm.alignment, cores)
+            return time.perf_counter() - t
+
+        n = min(jobs.n_jobs, cores)
+        t = run(n)
+        rounds = max(1, min(4, int(round(cpu_seconds / max(t, 1e-3)))))
+        n = min(jobs.n_jobs, cores * rounds)
+        t = run(n)
+        c = int(pc[:n].sum()) if n <= pc.size else int(reference_cells(ref, job_prefix(jobs, n), pm).sum())
+        ref.free_model(hf)
+        ref.free_model(hr)
+        out["cpu_reference"] = {"gcups": c / t / 1e9, "cores": cores, "kind": "reference",
+                                "sample": f"first {n} reads ({c} cells), OpenMP over reads on {cores} threads"}
+        out["batched_over_reference"] = out["gcups"] / out["cpu_reference"]["gcups"]
+    out["batched_over_plain"] = out["gcups"] / out["plain_gpu"]["gcups"]
+    return out
+
+
+def measure_polish_loop(engine, model, pm, wl, max_iterations):
+    """poa_realignAll in consensus mode over a polishing workload: the first realignment, then
+    the consensus iterations, wall seconds with the per-phase split."""
+    from marginpolish_b200 import PoaSet, PolishParams
+    s = PoaSet.from_polish_model(engine, model, pm, PolishParams(max_iterations=max_iterations), wl.drafts,
+                                 wl.reads, wl.strands, wl.anchors)
     t0 = time.perf_counter()
     s.realign()
     t1 = time.perf_counter()
@@ -457,9 +500,30 @@ def measure_polish_large(engine, model, pm):
     its = [s.info(c)["iterations"] for c in range(s.n_chunks)]
     s.close()
     return {"seconds": t2 - t0, "realign_seconds": t1 - t0, "iterate_seconds": t2 - t1, "iterations": its,
-            "generation_s": round(gen, 1), "workload": measure_polish_large.__doc__.split("\n")[0],
-            "chunks": 10, "reads": int(sum(len(r) for r in wl.reads)),
+            "chunks": len(wl.drafts), "reads": int(sum(len(r) for r in wl.reads)),
             "bases": int(sum(r.non_rle_length for lst in wl.reads for r in lst))}
+
+
+def measure_scale_configs(engine, model, pm, peak, cpu_seconds, chunks_5mb):
+    """The two larger configurations, reported beside the headline."""
+    out = {}
+    t = time.perf_counter()
+    wl = config_1mb()
+    gen = time.perf_counter() - t
+    r = measure_realign_pass(engine, model, pm, wl, peak, cpu_seconds)
+    r["workload"] = config_1mb.__doc__.split(".")[0].replace("\n", " ").replace("    ", " ")
+    r["generation_s"] = round(gen, 1)
+    r["polish_loop"] = measure_polish_loop(engine, model, pm, wl, 5)
+    out["config_1mb_polish"] = r
+    t = time.perf_counter()
+    wl = config_5mb(chunks_5mb)
+    gen = time.perf_counter() - t
+    r = measure_realign_pass(engine, model, pm, wl, peak, cpu_seconds)
+    r["workload"] = (config_5mb.__doc__.split(".")[0].replace("\n", " ").replace("    ", " ") +
+                     (f" (the first {chunks_5mb} of its 50 chunks)" if chunks_5mb < 50 else ""))
+    r["generation_s"] = round(gen, 1)
+    out["config_5mb_pass"] = r
+    return out
 
 
 def pinned_jobs(jobs):
@@ -602,11 +666,14 @@ def run_ours(args, rank, world, local):
         extras["adjoint"] = measure_adjoint(engine, model, pm)
         extras["polish_loop"] = measure_polish(engine, model, pm)
         extras["bubble_scoring"] = measure_bubble_scoring(engine, model, pm)
-    if args.polish_large and rank == 0:
-        extras["polish_loop_1mb"] = measure_polish_large(engine, model, pm)
-    if args.polish_5mb and rank == 0:
-        extras["polish_pass_5mb"] = measure_polish_5mb(engine, model, pm)
     peak = engine.fp32_peak_tflops()
+    if not args.no_scale and rank == 0 and world == 1 and args.config == "batched":
+        # the larger configurations need the device memory the headline's buffers hold
+        engine.release_buffers()
+        try:
+            extras.update(measure_scale_configs(engine, model, pm, peak, args.cpu_seconds / 2, args.chunks_5mb))
+        except Exception as exc:  # reported in the line; the headline stands on its own
+            extras["scale_configs_error"] = f"{type(exc).__name__}: {exc}"
     post = float(np.median(post_ms))
     achieved = cells * FLOP_PER_CELL / (post * 1e-3) / 1e12
     line = None

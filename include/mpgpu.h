@@ -128,6 +128,12 @@ mp_status mp_engine_create(int device, mp_engine **out);
 void mp_engine_destroy(mp_engine *e);
 /* Query: SM count, and whether the device is sm_100. */
 mp_status mp_engine_info(const mp_engine *e, int *sm_count, int *cc_major, int *cc_minor);
+/* Releases the device buffers the engine keeps between calls (the batches of the one-shot
+ * calls and the slots of mp_realign_batch_into); later calls allocate them again. Each batch
+ * holds forward checkpoints for its longest task in every task slot of its persistent grid, up
+ * to half the device's memory (the grid shrinks beyond that; the pipelined call shares that
+ * budget among its slots). */
+mp_status mp_engine_release_buffers(mp_engine *e);
 
 /* Lowered models for forward-strand (fwd) and reverse-strand (rev) reads. */
 mp_status mp_model_create(mp_engine *e, const mp_model_desc *fwd, const mp_model_desc *rev, mp_model **out);

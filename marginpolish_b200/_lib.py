@@ -205,7 +205,7 @@ EXPORTED = [
     "mp_poa_set_realign_all", "mp_poa_set_estimate_repeat_counts", "mp_poa_info", "mp_poa_nodes",
     "mp_poa_observations", "mp_poa_inserts", "mp_poa_deletes", "mp_poa_reference", "mp_poa_consensus",
     "mp_poa_anchor_alignments", "mp_engine_autotune", "mp_engine_autotune_reset",
-    "mp_engine_set_graph_capture", "mp_realign_batch_into",
+    "mp_engine_set_graph_capture", "mp_realign_batch_into", "mp_engine_release_buffers",
 ]
 
 _lib = None
@@ -227,6 +227,7 @@ def load() -> ctypes.CDLL:
         "mp_engine_create": (c_int, [c_int, P(c_void_p)]),
         "mp_engine_destroy": (None, [c_void_p]),
         "mp_engine_info": (c_int, [c_void_p, P(c_int), P(c_int), P(c_int)]),
+        "mp_engine_release_buffers": (c_int, [c_void_p]),
         "mp_engine_set_tuning": (c_int, [c_void_p, P(Tuning)]),
         "mp_engine_autotune": (c_int, [c_void_p, c_void_p, P(Params), P(Batch), P(AutotuneReport)]),
         "mp_engine_autotune_reset": (c_int, [c_void_p]),

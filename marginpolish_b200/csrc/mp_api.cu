@@ -103,6 +103,7 @@ extern "C" mp_status mp_engine_create(int device, mp_engine **out) {
     }
     mp_engine *eng = new mp_engine();
     eng->device = device;
+    eng->scratchBudget = (size_t) ((double) prop.totalGlobalMem * 0.5);
     eng->smCount = prop.multiProcessorCount;
     eng->ccMajor = prop.major;
     eng->ccMinor = prop.minor;
@@ -126,12 +127,27 @@ extern "C" void mp_engine_destroy(mp_engine *e) {
     mp_device_batch_destroy(e->forwardShot);
     mp_device_batch_destroy(e->adjointShot);
     e->oneShot = e->forwardShot = e->adjointShot = nullptr;
-    for (int k = 0; k < 2; k++) {
+    for (int k = 0; k < mp_engine::kPipeSlots; k++) {
         mp_device_batch_destroy(e->pipe[k]);  // destroys its own stream
         e->pipe[k] = nullptr;
     }
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
+}
+
+extern "C" mp_status mp_engine_release_buffers(mp_engine *e) {
+    if (!e) return failf(MP_ERR_ARGUMENT, "engine is NULL");
+    std::lock_guard<std::mutex> guard(e->oneShotLock);
+    CUDA_TRY(cudaSetDevice(e->device));
+    mp_device_batch_destroy(e->oneShot);
+    mp_device_batch_destroy(e->forwardShot);
+    mp_device_batch_destroy(e->adjointShot);
+    e->oneShot = e->forwardShot = e->adjointShot = nullptr;
+    for (int k = 0; k < mp_engine::kPipeSlots; k++) {
+        mp_device_batch_destroy(e->pipe[k]);
+        e->pipe[k] = nullptr;
+    }
+    return MP_OK;
 }
 
 extern "C" mp_status mp_engine_info(const mp_engine *e, int *sm, int *ma, int *mi) {
@@ -217,6 +233,8 @@ extern "C" mp_status mp_model_create(mp_engine *e, const mp_model_desc *fwd, con
     }
     if (s == MP_OK) {
         m->sharedRepeat = memcmp(rp.data(), rp.data() + kRepTable, sizeof(float) * kRepTable) == 0 ? 1 : 0;
+        m->noSwitch = (m->host[0].t[1 * 3 + 2] == 0.0f && m->host[0].t[2 * 3 + 1] == 0.0f &&
+                       m->host[1].t[1 * 3 + 2] == 0.0f && m->host[1].t[2 * 3 + 1] == 0.0f) ? 1 : 0;
         cudaSetDevice(e->device);
         s = m->models.reserve(sizeof(DevModel) * 2);
         if (s == MP_OK) s = m->repeat.reserve(sizeof(float) * 2 * kRepTable);
@@ -578,6 +596,7 @@ struct mp_device_batch {
     int forceVariant = -1;  // autotuner: every posterior task in this variant ...
     int forceWarps = 0;     // ... at this many warps per block
     int forceBlocks = 0;    // ... in at most this many persistent blocks
+    size_t scratchBudget = 0;  // checkpoint bytes this batch may hold (0: the engine's budget)
     bool ran = false;
     float bandMs = 0.0f, posteriorMs = 0.0f;
     cudaEvent_t evBand = nullptr;
@@ -987,8 +1006,16 @@ static mp_status planQueues(mp_device_batch *db, std::vector<QueueLaunch> &plan)
         int blocks = std::max(1, std::min(e->smCount * blocksPerSm, maxBlocks));
         if (!adj && db->forceBlocks > 0) blocks = std::min(blocks, db->forceBlocks);
         const int scratchBlocks = (int) (db->varMaxN[v] / K + 2);
-        const size_t slots = (size_t) blocks * warps * G;
         const size_t elem = adj ? sizeof(float4) : chkElemBytes(v);
+        // every task slot holds checkpoints for the variant's longest task: within the budget,
+        // fewer persistent blocks (long reads in wide windows need ~1 KB per anti-diagonal)
+        {
+            const size_t perSlot = (size_t) scratchBlocks * (size_t) (C * L) * elem + sizeof(int2) * scratchBlocks;
+            const size_t budget = db->scratchBudget ? db->scratchBudget : e->scratchBudget;
+            const size_t perBlock = perSlot * (size_t) warps * (size_t) G;
+            if (budget > 0 && perBlock > 0) blocks = std::max(1, std::min(blocks, (int) std::min<size_t>(budget / perBlock, 1 << 20)));
+        }
+        const size_t slots = (size_t) blocks * warps * G;
         needScratch = std::max(needScratch, (size_t) scratchBlocks * (size_t) (C * L) * elem * slots);
         needScal = std::max(needScal, sizeof(int2) * (size_t) scratchBlocks * slots);
         blocksOf[v] = blocks;
@@ -1023,6 +1050,7 @@ static mp_status planQueues(mp_device_batch *db, std::vector<QueueLaunch> &plan)
         a.traceBackDiagonals = (int32_t) db->p.traceback_diagonals;
         a.diagonalExpansion = (int32_t) std::min<int64_t>(db->p.diagonal_expansion, 1 << 29);
         a.sharedRepeat = db->m->sharedRepeat;
+        a.noSwitch = db->m->noSwitch;
         a.expect = db->expect.as<double>();
         a.expectRep = db->expectRep.as<double>();
         plan.push_back(QueueLaunch{v, blocksOf[v], warpsOf[v], a});
@@ -1331,6 +1359,7 @@ extern "C" mp_status mp_device_batch_run_plain(mp_engine *e, mp_device_batch *db
         a.traceBackDiagonals = (int32_t) db->p.traceback_diagonals;
         a.diagonalExpansion = (int32_t) std::min<int64_t>(db->p.diagonal_expansion, 1 << 29);
         a.sharedRepeat = db->m->sharedRepeat;
+        a.noSwitch = db->m->noSwitch;
         CUDA_TRY(launchVariant(v, a, 1, 1, st));
     }
     CUDA_TRY(cudaEventRecord(db->ev1, st));
@@ -1791,9 +1820,10 @@ extern "C" mp_status mp_realign_batch_into(mp_engine *e, const mp_model *m, cons
     std::lock_guard<std::mutex> guard(e->oneShotLock);
     CUDA_TRY(cudaSetDevice(e->device));
     const int64_t n = b->n_jobs;
-    if (parts <= 0) parts = n >= 2048 ? 4 : 1;
+    if (parts <= 0) parts = n >= 2048 ? mp_engine::kPipeSlots : 1;
     parts = (int32_t) std::max<int64_t>(1, std::min<int64_t>(parts, std::max<int64_t>(n, 1)));
-    for (int k = 0; k < 2; k++) {
+    const int nSlots = std::min<int>(parts, mp_engine::kPipeSlots);
+    for (int k = 0; k < nSlots; k++) {
         if (e->pipe[k]) continue;
         mp_device_batch *db = new mp_device_batch();
         if (cudaStreamCreateWithFlags(&db->stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -1816,21 +1846,29 @@ extern "C" mp_status mp_realign_batch_into(mp_engine *e, const mp_model *m, cons
     bool over[3] = {false, false, false};
     for (int k = 0; k < 3; k++)
         if (out->offsets[k]) out->offsets[k][0] = 0;
-    // finishes slice i (waits for its run, re-runs what needs it) and queues its tuple copies
-    auto finish = [&](int i) -> mp_status {
-        mp_device_batch *db = e->pipe[i % 2];
+    // finishes slice i (waits for its run, re-runs what needs it) and queues its tuple copies;
+    // slices finish in order, since a slice's output offsets follow the tuples of those before it
+    int finished = 0;
+    auto finishNext = [&]() -> mp_status {
+        mp_device_batch *db = e->pipe[finished % nSlots];
         MP_TRY(runFinish(e, db, nullptr));
         int64_t total[3];
-        MP_TRY(fetchIssue(e, db, out, cut[i], base, cap, total));
+        MP_TRY(fetchIssue(e, db, out, cut[finished], base, cap, total));
         for (int k = 0; k < 3; k++) {
             if (base[k] + total[k] > cap[k]) over[k] = true;
             base[k] += total[k];
         }
+        finished++;
         return MP_OK;
     };
+    // Every slice is planned, copied in and launched on its own slot as early as the slots allow
+    // (all at once when there are no more slices than slots): later slices' kernels fill the SMs
+    // that an earlier slice's last tasks leave idle, and each slice's tuples stream out as soon
+    // as its kernels end.
     mp_status st = MP_OK;
-    int pending = -1;
     for (int i = 0; st == MP_OK && i < nSlices; i++) {
+        if (i >= nSlots) st = finishNext();  // frees slot i % nSlots
+        if (st != MP_OK) break;
         const int64_t j0 = cut[i], j1 = cut[i + 1];
         std::vector<int64_t> yOff(j1 - j0 + 1), aOff(j1 - j0 + 1);
         for (int64_t j = j0; j <= j1; j++) {
@@ -1849,17 +1887,16 @@ extern "C" mp_status mp_realign_batch_into(mp_engine *e, const mp_model *m, cons
         sb.ragged_left = b->ragged_left ? b->ragged_left + j0 : nullptr;
         sb.ragged_right = b->ragged_right ? b->ragged_right + j0 : nullptr;
         sb.x_shift = b->x_shift ? b->x_shift + j0 : nullptr;
-        mp_device_batch *db = e->pipe[i % 2];
+        mp_device_batch *db = e->pipe[i % nSlots];
         db->mode = kModePosterior;
-        // the slot's previous slice has queued its copies on the same stream: the new inputs
-        // follow them in stream order; the batch's host arrays stay valid until the return
+        db->scratchBudget = e->scratchBudget / (size_t) nSlots;
+        // a reused slot's previous slice has queued its copies on the slot's streams: the new
+        // inputs follow them in stream order; the batch's host arrays stay valid until the return
         st = batchReset(e, db, m, p, &sb, false);
         if (st == MP_OK) st = runIssue(e, db);
-        if (st == MP_OK && pending >= 0) st = finish(pending);
-        pending = i;
     }
-    if (st == MP_OK && pending >= 0) st = finish(pending);
-    for (int k = 0; k < 2; k++) {
+    while (st == MP_OK && finished < nSlices) st = finishNext();
+    for (int k = 0; k < nSlots; k++) {
         cudaError_t ce = cudaStreamSynchronize(e->pipe[k]->stream);
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->pipe[k]->copyStream);
         e->pipe[k]->copyPending = false;

@@ -4,6 +4,7 @@
 #include "../../include/mpgpu.h"
 #include "mp_internal.h"
 
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
 #include <vector>
@@ -50,10 +51,13 @@ struct DevBuf {
         p = nullptr;
         bytes = 0;
     }
+    // Grows to at least n bytes, with headroom of half the need up to 64 MiB: buffers sized by
+    // per-call counts (tuples, tasks) then stop growing after a few calls. Growth frees the old
+    // buffer, and cudaFree waits for the whole device, which would stall other threads' passes.
     mp_status reserve(size_t n) {
         if (n <= bytes && p) return MP_OK;
         release();
-        size_t want = n > 0 ? n : 16;
+        size_t want = n > 0 ? n + std::min(n / 2, (size_t) 64 << 20) : 16;
         cudaError_t e = cudaMalloc(&p, want);
         if (e != cudaSuccess) {
             p = nullptr;
@@ -102,6 +106,10 @@ struct mp_engine {
     int ccMajor = 0, ccMinor = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // Device bytes one batch may hold for forward checkpoints (half the device's memory). A
+    // batch whose persistent grid would need more runs on fewer blocks; the pipelined call splits
+    // the budget over its slots.
+    size_t scratchBudget = 0;
     mp_tuning tuning{};
     bool graphs = false;  // device-batch passes run as captured CUDA graphs
     // autotuned choice (mp_engine_autotune): ascending hull-class bounds with the FP32 kernel
@@ -111,13 +119,15 @@ struct mp_engine {
     struct mp_device_batch *oneShot = nullptr;  // reused by the one-shot calls (mp_realign_batch*)
     struct mp_device_batch *forwardShot = nullptr;  // reused by mp_forward_batch
     struct mp_device_batch *adjointShot = nullptr;  // reused by mp_expectations_batch
-    struct mp_device_batch *pipe[2] = {nullptr, nullptr};  // the two slots of mp_realign_batch_into (own streams)
+    static constexpr int kPipeSlots = 8;
+    struct mp_device_batch *pipe[kPipeSlots] = {};  // the slots of mp_realign_batch_into (own streams)
     std::mutex oneShotLock;
 };
 
 struct mp_model {
     mp_engine *engine = nullptr;
     int sharedRepeat = 0;  // the two strands' repeat tables are identical
+    int noSwitch = 0;      // both strands' switch transitions (gap-x <-> gap-y) are zero
     mp::DevModel host[2];
     double logT[2][9];   // log transitions as given (the adjoint scales its sums by exp(logT))
     DevBuf models;   // DevModel[2]

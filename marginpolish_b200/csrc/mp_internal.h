@@ -95,6 +95,7 @@ struct DpArgs {
     int32_t traceBackDiagonals;
     int32_t diagonalExpansion;
     int32_t sharedRepeat;       // both models use repeat table 0
+    int32_t noSwitch;           // both models' switch transitions (gap-x <-> gap-y) are zero
     double *expect;             // adjoint only: [2][kExpPerModel]
     double *expectRep;          // adjoint only: [tables][kRepTable]
 };

@@ -39,6 +39,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <mutex>
 #include <type_traits>
 
 namespace mp {
@@ -602,8 +603,10 @@ struct CacheRow {
 // One forward anti-diagonal (PAR = d & 1). Emissions are zeroed outside the band
 // [sLo, sHi], which zeroes the cell. With CACHE, the cell values and the masked
 // emissions are written to the block cache row (rowA, rowB). With SYM, the cells'
-// table offsets go to rowC (slot j at j*L entries).
-template <int C, int L, int PAR, bool CACHE, bool SYM, class V>
+// table offsets go to rowC (slot j at j*L entries). SW false: the model's switch
+// transitions (gap-x -> gap-y, gap-y -> gap-x) are zero, and their products, which add
+// exact zeros, are left out.
+template <int C, int L, int PAR, bool CACHE, bool SYM, class V, bool SW = true>
 __device__ __forceinline__ void forwardDiagonal(const Ctx<V> &c, Fwd<C, V> &st, const Slots<C> &sy, int sLo, int sHi,
                                                 uint32_t rowA, uint32_t rowB, uint32_t rowC = 0) {
     using M = SlotMath<C, V>;
@@ -666,11 +669,19 @@ __device__ __forceinline__ void forwardDiagonal(const Ctx<V> &c, Fwd<C, V> &st, 
     M::fmas(a, fX, c.t[1 * 3 + 0], a);
     if (PAR) M::fmas(st.mB, fY, c.t[2 * 3 + 0], a); else M::fmas(st.mA, fY, c.t[2 * 3 + 0], a);
     M::muls(a, fM, c.t[0 * 3 + 1]);
-    M::fmas(a, fX, c.t[1 * 3 + 1], a);
-    M::fmas(st.ox, fY, c.t[2 * 3 + 1], a);
+    if constexpr (SW) {
+        M::fmas(a, fX, c.t[1 * 3 + 1], a);
+        M::fmas(st.ox, fY, c.t[2 * 3 + 1], a);
+    } else {
+        M::fmas(st.ox, fX, c.t[1 * 3 + 1], a);
+    }
     M::muls(a, fM, c.t[0 * 3 + 2]);
-    M::fmas(a, fY, c.t[2 * 3 + 2], a);
-    M::fmas(st.oy, fX, c.t[1 * 3 + 2], a);
+    if constexpr (SW) {
+        M::fmas(a, fY, c.t[2 * 3 + 2], a);
+        M::fmas(st.oy, fX, c.t[1 * 3 + 2], a);
+    } else {
+        M::fmas(st.oy, fY, c.t[2 * 3 + 2], a);
+    }
     if (CACHE) CacheRow<C, L, V>::store(rowA, rowB, fM, fX, fY, eM, eX, eY);
 }
 
@@ -909,7 +920,7 @@ struct Walk {
     const float *endP;
 };
 
-template <int C, int L, int K, bool ADJ, class V>
+template <int C, int L, int K, bool ADJ, class V, bool SW>
 __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &gm, const Scratch<V> &sc,
                                             const Walk &wk, V thr, Out &o, double &logLik, bool &bad,
                                             bool &rangeBad, double (&accD)[9], double *expect) {
@@ -1013,9 +1024,9 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
                 const uint32_t rowA = laneA + (uint32_t) kk * CR::kRowA, rowB = laneB + (uint32_t) kk * CR::kRowB;
                 const uint32_t rowC = laneC + (uint32_t) (kk * S * 4);
                 stepSlots<C, L, R, 0>(gl, gm.rx, gm.ry, d, Q, sy);
-                forwardDiagonal<C, L, 0, true, ADJ, V>(c, rs, sy, b0.x - Q, b0.y - Q, rowA, rowB, rowC);
+                forwardDiagonal<C, L, 0, true, ADJ, V, SW>(c, rs, sy, b0.x - Q, b0.y - Q, rowA, rowB, rowC);
                 stepSlots<C, L, R, 1>(gl, gm.rx, gm.ry, d + 1, Q, sy);
-                forwardDiagonal<C, L, 1, true, ADJ, V>(c, rs, sy, b1.x - Q, b1.y - Q, rowA + CR::kRowA, rowB + CR::kRowB,
+                forwardDiagonal<C, L, 1, true, ADJ, V, SW>(c, rs, sy, b1.x - Q, b1.y - Q, rowA + CR::kRowA, rowB + CR::kRowB,
                                                        rowC + S * 4);
             }
             if (gl < K) sts<int2>(gm.info + gl * 8, make_int2(Q, 0));
@@ -1050,11 +1061,11 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
                     if (par) {
                         stepSlots<C, L, R, 1>(gl, gm.rx, gm.ry, d, Q, sy);
                         if (rare && reload) loadSlots<C, R>(gl, gm.rx, gm.ry, d, Q, sy);
-                        forwardDiagonal<C, L, 1, true, ADJ, V>(c, rs, sy, sLo, sHi, rowA, rowB, rowC);
+                        forwardDiagonal<C, L, 1, true, ADJ, V, SW>(c, rs, sy, sLo, sHi, rowA, rowB, rowC);
                     } else {
                         stepSlots<C, L, R, 0>(gl, gm.rx, gm.ry, d, Q, sy);
                         if (rare && reload) loadSlots<C, R>(gl, gm.rx, gm.ry, d, Q, sy);
-                        forwardDiagonal<C, L, 0, true, ADJ, V>(c, rs, sy, sLo, sHi, rowA, rowB, rowC);
+                        forwardDiagonal<C, L, 0, true, ADJ, V, SW>(c, rs, sy, sLo, sHi, rowA, rowB, rowC);
                         if (d == 0) forwardOrigin<C, L, true, V>(c, wk.startP, Q, rs, rowA, rowB);
                     }
                     if (gl == 0) sts<int2>(gm.info + kk * 8, make_int2(Q, dl));
@@ -1112,10 +1123,14 @@ __device__ __forceinline__ void walkSegment(const Ctx<V> &c, GroupMem<C, L, K> &
                 M::fmas(a, sY, c.t[0 * 3 + 2], a);
                 M::fmas(bM, sM2, c.t[0 * 3 + 0], a);
                 M::muls(a, sX, c.t[1 * 3 + 1]);
-                M::fmas(a, sY, c.t[1 * 3 + 2], a);
+                if constexpr (SW) M::fmas(a, sY, c.t[1 * 3 + 2], a);
                 M::fmas(bX, sM2, c.t[1 * 3 + 0], a);
-                M::muls(a, sX, c.t[2 * 3 + 1]);
-                M::fmas(a, sY, c.t[2 * 3 + 2], a);
+                if constexpr (SW) {
+                    M::muls(a, sX, c.t[2 * 3 + 1]);
+                    M::fmas(a, sY, c.t[2 * 3 + 2], a);
+                } else {
+                    M::muls(a, sY, c.t[2 * 3 + 2]);
+                }
                 M::fmas(bY, sM2, c.t[2 * 3 + 0], a);
                 if (!FLAT && d == wk.D) {  // the walk's first diagonal holds the end probabilities
 #pragma unroll
@@ -1372,7 +1387,7 @@ __device__ __forceinline__ int nextTracePoint(const CT &c, int from, int maxWidt
 // One warp-load of G tasks: forward sweep with checkpoints, then the walks.
 // ---------------------------------------------------------------------------
 
-template <int C, int L, int K, bool ADJ, class V>
+template <int C, int L, int K, bool ADJ, class V, bool SW>
 __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMem<C, L, K> &gm, const Scratch<V> &sc) {
     constexpr int S = L * C;
     constexpr int R = RingSize<S>::R;
@@ -1485,7 +1500,7 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
         }
         stepSlots<C, L, R, PAR>(c.gl, gm.rx, gm.ry, d, Q, sy);
         if (rare && reload) loadSlots<C, R>(c.gl, gm.rx, gm.ry, d, Q, sy);
-        forwardDiagonal<C, L, PAR, false, false, V>(c, st, sy, bd.x - Q, bd.y - Q, 0, 0);
+        forwardDiagonal<C, L, PAR, false, false, V, SW>(c, st, sy, bd.x - Q, bd.y - Q, 0, 0);
     };
     const auto odd = std::integral_constant<int, 1>{};
     const auto even = std::integral_constant<int, 0>{};
@@ -1530,9 +1545,9 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
                 const int2 b0 = lds<int2>(gm.bandRing + ((d & 63) << 4));
                 const int2 b1 = lds<int2>(gm.bandRing + (((d + 1) & 63) << 4));
                 stepSlots<C, L, R, 0>(c.gl, gm.rx, gm.ry, d, Q, sy);
-                forwardDiagonal<C, L, 0, false, false, V>(c, st, sy, b0.x - Q, b0.y - Q, 0, 0);
+                forwardDiagonal<C, L, 0, false, false, V, SW>(c, st, sy, b0.x - Q, b0.y - Q, 0, 0);
                 stepSlots<C, L, R, 1>(c.gl, gm.rx, gm.ry, d + 1, Q, sy);
-                forwardDiagonal<C, L, 1, false, false, V>(c, st, sy, b1.x - Q, b1.y - Q, 0, 0);
+                forwardDiagonal<C, L, 1, false, false, V, SW>(c, st, sy, b1.x - Q, b1.y - Q, 0, 0);
             }
         } else {
             for (int kk = 0; kk < K; kk += 2) {
@@ -1572,7 +1587,7 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
         wk.active = more ? 1 : 0;
         wk.emit = single ? 0 : 1;
         wk.endP = (atEnd && (flags & 2)) ? dm.raggedEnd : dm.end;
-        walkSegment<C, L, K, ADJ, V>(c, gm, sc, wk, (V) a.threshold, o, logLik, bad, rangeBad, accD, a.expect);
+        walkSegment<C, L, K, ADJ, V, SW>(c, gm, sc, wk, (V) a.threshold, o, logLik, bad, rangeBad, accD, a.expect);
         if (more) {
             tb = wk.tbFrom;
             prevD = wk.D;
@@ -1610,7 +1625,7 @@ __device__ __forceinline__ void runGroup(const DpArgs &a, int taskIndex, GroupMe
     }
 }
 
-template <int C, int L, int K, int MAXW, bool ADJ, class V>
+template <int C, int L, int K, int MAXW, bool ADJ, class V, bool SW>
 __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
     using GS = GroupSmem<C, L, K, ADJ, V>;
     constexpr int G = 32 / L;
@@ -1667,7 +1682,7 @@ __global__ void __launch_bounds__(MAXW * 32, 1) posteriorKernel(DpArgs a) {
         q = __shfl_sync(FULL_MASK, q, 0);
         if (q >= nLoads) break;
         const int t = q * G + g;
-        runGroup<C, L, K, ADJ, V>(a, t < a.nTasks ? a.order[t] : -1, gm, sc);
+        runGroup<C, L, K, ADJ, V, SW>(a, t < a.nTasks ? a.order[t] : -1, gm, sc);
         __syncwarp();
     }
 }
@@ -1683,15 +1698,40 @@ static size_t smemFor(int warps, int nTables) {
            (size_t) warps * (32 / L) * GroupSmem<C, L, K, ADJ, V>::bytes;
 }
 
+template <int C, int L, int K, int MAXW, bool ADJ, class V, bool SW>
+static cudaError_t launchSW(const DpArgs &a, int blocks, int warps, cudaStream_t s) {
+    const size_t smem = smemFor<C, L, K, ADJ, V>(warps, a.sharedRepeat ? 1 : 2);
+    // the shared-memory limit of the kernel only grows, once per device (calls from many threads
+    // then skip the attribute call)
+    static std::mutex lock;
+    static size_t granted[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    {
+        std::lock_guard<std::mutex> g(lock);
+        const int slot = dev & 63;
+        if (smem > granted[slot]) {
+            e = cudaFuncSetAttribute(posteriorKernel<C, L, K, MAXW, ADJ, V, SW>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+            if (e == cudaSuccess) granted[slot] = smem;
+        }
+    }
+    if (e != cudaSuccess) return e;
+    posteriorKernel<C, L, K, MAXW, ADJ, V, SW><<<blocks, warps * 32, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+// The FP32 posterior variants come in two builds: with the switch transitions, and without them
+// for models whose switch transitions are zero (the shipped model's); the FP64 variants and the
+// adjoint always carry them.
 template <int C, int L, int K, int MAXW, bool ADJ = false, class V = float>
 static cudaError_t launchT(const DpArgs &a, int blocks, int warps, cudaStream_t s) {
     if (warps > MAXW || warps < 1) return cudaErrorInvalidValue;
-    const size_t smem = smemFor<C, L, K, ADJ, V>(warps, a.sharedRepeat ? 1 : 2);
-    cudaError_t e = cudaFuncSetAttribute(posteriorKernel<C, L, K, MAXW, ADJ, V>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-    if (e != cudaSuccess) return e;
-    posteriorKernel<C, L, K, MAXW, ADJ, V><<<blocks, warps * 32, smem, s>>>(a);
-    return cudaGetLastError();
+    if constexpr (!ADJ && std::is_same<V, float>::value) {
+        if (a.noSwitch) return launchSW<C, L, K, MAXW, ADJ, V, false>(a, blocks, warps, s);
+    }
+    return launchSW<C, L, K, MAXW, ADJ, V, true>(a, blocks, warps, s);
 }
 
 // Kernel variants: (index, C slots per lane, L lanes per task, K checkpoint stride,

@@ -75,6 +75,14 @@ class Engine:
         """Restores the built-in kernel choice."""
         _lib.check(self._lib.mp_engine_autotune_reset(self.handle))
 
+    def release_buffers(self) -> None:
+        """Frees the device buffers kept between calls (mp_engine_release_buffers)."""
+        db = getattr(self, "_one_shot", None)
+        if db is not None:
+            db.close()
+            self._one_shot = None
+        _lib.check(self._lib.mp_engine_release_buffers(self.handle))
+
     def fp32_peak_tflops(self) -> float:
         """Measured FP32 FMA throughput of this device (TFLOP/s)."""
         v = ctypes.c_double()

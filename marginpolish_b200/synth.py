@@ -57,32 +57,44 @@ def rle_symbols(r: RleString, include_counts: bool = True, max_repeat_exclusive:
     return b.astype(np.uint16)
 
 
-def rle_anchors_monotone(pairs: np.ndarray, x: RleString, y: RleString) -> np.ndarray:
+def _run_ends(v: np.ndarray) -> np.ndarray:
+    """For a non-decreasing array: per element, the index of the first element greater than it."""
+    step = v[1:] != v[:-1]
+    ends = np.append(np.flatnonzero(step) + 1, v.size)
+    run = np.concatenate([[0], np.cumsum(step)])
+    return ends[run]
+
+
+def rle_anchors_monotone(pairs: np.ndarray, x: RleString, y: RleString, xmap: Optional[np.ndarray] = None,
+                         ymap: Optional[np.ndarray] = None) -> np.ndarray:
     """runLengthEncodeAlignment (impl/polisher.c:1732-1750) for base pairs strictly increasing in
-    both coordinates: each pair goes through the non-RLE -> RLE coordinate maps (:1718-1730) and is
-    kept when both RLE coordinates exceed the last kept pair's. The mapped coordinates are then
-    non-decreasing, so the pair kept after pair i is the first j with x2[j] > x2[i] and
-    y2[j] > y2[i], i.e. the larger of the two searchsorted positions; the kept pairs are the orbit
-    of pair 0 under that successor map, found by doubling."""
+    both coordinates: each pair goes through the non-RLE -> RLE coordinate maps (:1718-1730; xmap /
+    ymap may be passed in precomputed) and is kept when both RLE coordinates exceed the last kept
+    pair's. The mapped coordinates are then non-decreasing, so the pair kept after pair i is the
+    first j with x2[j] > x2[i] and y2[j] > y2[i], i.e. the later of the ends of the runs of equal
+    x2 and of equal y2 that hold i; the kept pairs are the orbit of pair 0 under that successor
+    map, found by doubling (the orbit is increasing, so it comes out in order)."""
     pairs = np.asarray(pairs, dtype=np.int64).reshape(-1, 3)
     m = pairs.shape[0]
     if m == 0:
         return np.zeros((0, 3), dtype=np.int32)
     if np.any(np.diff(pairs[:, 0]) <= 0) or np.any(np.diff(pairs[:, 1]) <= 0):
         raise ValueError("base pairs must be strictly increasing in both coordinates")
-    xmap = np.repeat(np.arange(len(x), dtype=np.int64), x.counts.astype(np.int64))
-    ymap = np.repeat(np.arange(len(y), dtype=np.int64), y.counts.astype(np.int64))
+    if xmap is None:
+        xmap = np.repeat(np.arange(len(x), dtype=np.int64), x.counts.astype(np.int64))
+    if ymap is None:
+        ymap = np.repeat(np.arange(len(y), dtype=np.int64), y.counts.astype(np.int64))
     x2 = xmap[pairs[:, 0]]
     y2 = ymap[pairs[:, 1]]
     succ = np.empty(m + 1, dtype=np.int64)
-    succ[:m] = np.maximum(np.searchsorted(x2, x2, side="right"), np.searchsorted(y2, y2, side="right"))
+    succ[:m] = np.maximum(_run_ends(x2), _run_ends(y2))
     succ[m] = m  # sink
     orbit = np.zeros(1, dtype=np.int64)
     step = succ
     while orbit[-1] < m:
         orbit = np.concatenate([orbit, step[orbit]])  # the next len(orbit) members
         step = step[step]
-    keep = np.unique(orbit[orbit < m])
+    keep = orbit[orbit < m]
     return np.stack([x2[keep], y2[keep], pairs[keep, 2]], axis=1).astype(np.int32)
 
 
@@ -343,6 +355,20 @@ class PolishWorkload:
     anchors: List[List[np.ndarray]]
     meta: dict = field(default_factory=dict)
 
+    def realign_workload(self) -> Workload:
+        """The first realignment of the polishing loop as a plain workload: every read of every
+        chunk against its chunk's draft with its anchors (poa_realign, impl/polisher.c:656-703)."""
+        reads, anchors, rt, strand = [], [], [], []
+        for c in range(len(self.drafts)):
+            for r, s, a in zip(self.reads[c], self.strands[c], self.anchors[c]):
+                reads.append(r)
+                anchors.append(a)
+                rt.append(c)
+                strand.append(s)
+        exp = int(anchors[0][0, 2]) if anchors and anchors[0].shape[0] else 0
+        return Workload("realign", list(self.drafts), reads, np.array(rt, dtype=np.int64),
+                        np.array(strand, dtype=np.uint8), anchors, exp, dict(self.meta))
+
 
 def config_polish(seed: int = 3, n_chunks: int = 1, chunk_len: int = 2000, coverage: float = 20.0,
                   read_len=(1500, 2000), half_width: int = 25, draft_error: float = 0.01,
@@ -361,6 +387,7 @@ def config_polish(seed: int = 3, n_chunks: int = 1, chunk_len: int = 2000, cover
         tmap = np.full(t.size, -1, dtype=np.int64)
         tmap[t2d[:, 0]] = t2d[:, 1]
         drle = rle_encode(d)
+        dmap = np.repeat(np.arange(len(drle), dtype=np.int64), drle.counts.astype(np.int64))
         if read_lognormal is not None:
             med, sig, mx = read_lognormal
             mean_len = min(float(mx), float(med) * float(np.exp(sig ** 2 / 2)))
@@ -387,7 +414,7 @@ def config_polish(seed: int = 3, n_chunks: int = 1, chunk_len: int = 2000, cover
             dp = tmap[pairs[:, 0]]
             ok = dp >= 0
             p = np.stack([dp[ok], pairs[ok, 1], np.full(int(ok.sum()), 2 * half_width)], axis=1)
-            a = rle_anchors_monotone(p, drle, r)
+            a = rle_anchors_monotone(p, drle, r, xmap=dmap)
             if a.shape[0] == 0 or len(r) == 0:
                 continue
             cr.append(r)

@@ -606,6 +606,8 @@ struct mp_device_batch {
     // kernels do not queue behind them; evCopied guards the staging lists until they are copied
     cudaStream_t copyStream = nullptr;
     cudaEvent_t evCompacted = nullptr, evCopied = nullptr;
+    cudaEvent_t evUploaded = nullptr;       // pipelined slots: this slice's input copies are done
+    cudaEvent_t evSync = nullptr;           // blocking-sync event the host waits on (sleeps, no spin)
     bool copyPending = false;
     TaskOut *pinOut = nullptr;              // page-locked copy of the task statuses
     size_t pinOutCap = 0;
@@ -623,8 +625,24 @@ struct mp_device_batch {
         if (copyStream) cudaStreamDestroy(copyStream);
         if (evCompacted) cudaEventDestroy(evCompacted);
         if (evCopied) cudaEventDestroy(evCopied);
+        if (evUploaded) cudaEventDestroy(evUploaded);
+        if (evSync) cudaEventDestroy(evSync);
     }
 };
+
+// Waits until everything queued on `st` has run. The host thread sleeps on a blocking-sync
+// event instead of spinning: callers that drive the engine from many threads at once (the
+// drop-in's OpenMP callers, each with its own engine) leave the cores to the threads that
+// are planning and filling their next calls.
+static cudaError_t waitStream(mp_device_batch *db, cudaStream_t st) {
+    if (!db->evSync) {
+        const cudaError_t e = cudaEventCreateWithFlags(&db->evSync, cudaEventBlockingSync | cudaEventDisableTiming);
+        if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = cudaEventRecord(db->evSync, st);
+    if (e == cudaSuccess) e = cudaEventSynchronize(db->evSync);
+    return e;
+}
 
 static mp_status validateJob(const mp_batch *b, int64_t j, const mp_params *p, bool dynamic) {
     int64_t lx = b->x_end[j] - b->x_begin[j];
@@ -947,7 +965,7 @@ static mp_status batchReset(mp_engine *e, mp_device_batch *db, const mp_model *m
     MP_TRY(db->queue.reserve(sizeof(int32_t) * variantCount()));
     // the caller's host arrays may be reused as soon as this returns (unless the caller keeps
     // them valid until its own synchronisation)
-    if (syncInputs) CUDA_TRY(cudaStreamSynchronize(st));
+    if (syncInputs) CUDA_TRY(waitStream(db, st));
     return MP_OK;
 }
 
@@ -1189,7 +1207,7 @@ static mp_status runFinish(mp_engine *e, mp_device_batch *db, float *kernelMs) {
     cudaStream_t st = db->stream;
     const int nTasks = (int) db->tasks.size();
     std::vector<int32_t> orderHost;
-    CUDA_TRY(cudaStreamSynchronize(st));
+    CUDA_TRY(waitStream(db, st));
     db->hostOut.assign(db->pinOut, db->pinOut + nTasks);
     float ms = 0.0f;
     CUDA_TRY(cudaEventElapsedTime(&ms, db->ev0, db->ev1));
@@ -1542,7 +1560,7 @@ static mp_status fetchInto(mp_engine *e, mp_device_batch *db, const mp_output *o
     const int64_t base[3] = {0, 0, 0};
     int64_t total[3];
     MP_TRY(fetchIssue(e, db, out, 0, base, nullptr, total));
-    CUDA_TRY(cudaStreamSynchronize(db->stream));
+    CUDA_TRY(waitStream(db, db->copyStream ? db->copyStream : db->stream));
     return MP_OK;
 }
 
@@ -1834,7 +1852,8 @@ extern "C" mp_status mp_realign_batch_into(mp_engine *e, const mp_model *m, cons
         db->ownStream = true;
         if (cudaStreamCreateWithFlags(&db->copyStream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&db->evCompacted, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&db->evCopied, cudaEventDisableTiming) != cudaSuccess) {
+            cudaEventCreateWithFlags(&db->evCopied, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&db->evUploaded, cudaEventDisableTiming) != cudaSuccess) {
             delete db;
             return failf(MP_ERR_CUDA, "stream / event creation failed");
         }
@@ -1865,7 +1884,11 @@ extern "C" mp_status mp_realign_batch_into(mp_engine *e, const mp_model *m, cons
     // (all at once when there are no more slices than slots): later slices' kernels fill the SMs
     // that an earlier slice's last tasks leave idle, and each slice's tuples stream out as soon
     // as its kernels end.
+    // The slices' input copies run one after another in slice order (each slot's stream waits
+    // for the previous slice's copies), so the first slices' inputs arrive at the link's full
+    // speed instead of sharing it with every later slice's.
     mp_status st = MP_OK;
+    cudaEvent_t prevUploaded = nullptr;
     for (int i = 0; st == MP_OK && i < nSlices; i++) {
         if (i >= nSlots) st = finishNext();  // frees slot i % nSlots
         if (st != MP_OK) break;
@@ -1892,7 +1915,14 @@ extern "C" mp_status mp_realign_batch_into(mp_engine *e, const mp_model *m, cons
         db->scratchBudget = e->scratchBudget / (size_t) nSlots;
         // a reused slot's previous slice has queued its copies on the slot's streams: the new
         // inputs follow them in stream order; the batch's host arrays stay valid until the return
+        if (prevUploaded && cudaStreamWaitEvent(db->stream, prevUploaded, 0) != cudaSuccess) {
+            st = failf(MP_ERR_CUDA, "stream wait failed");
+            break;
+        }
         st = batchReset(e, db, m, p, &sb, false);
+        if (st == MP_OK && cudaEventRecord(db->evUploaded, db->stream) != cudaSuccess)
+            st = failf(MP_ERR_CUDA, "event record failed");
+        prevUploaded = db->evUploaded;
         if (st == MP_OK) st = runIssue(e, db);
     }
     while (st == MP_OK && finished < nSlices) st = finishNext();

@@ -278,21 +278,33 @@ struct MatchSet {
     }
 };
 
-void augment(Poa &poa, const Rle &read, bool strand, int64_t readNo, const std::vector<Pair> &matches,
-             std::vector<Pair> &inserts, std::vector<Pair> &deletes, bool cmpRC) {
+// The complete indels of one read against a graph's reference, in the order poa_augment adds
+// them to the graph (every insert, then every delete, each in enumeration order). They depend
+// only on the reference string, so the candidates of all reads can be found in parallel; adding
+// them to the graph (mergeRead) then runs read by read, which keeps the reference's order of
+// the graph's insert / delete lists and of their observations.
+struct IndelCands {
+    std::vector<int64_t> pos;     // node the indel is attached to
+    std::vector<int64_t> len;     // runs inserted / deleted
+    std::vector<int64_t> at;      // inserts: first run in chars / counts
+    std::vector<uint64_t> nonRle; // inserts: expanded length
+    std::vector<double> w;
+    std::vector<int64_t> offset;  // observation: read position
+    std::string chars;
+    std::vector<uint64_t> counts;
+    int64_t nIns = 0;
+    void clear() {
+        pos.clear(), len.clear(), at.clear(), nonRle.clear(), w.clear(), offset.clear(), chars.clear(), counts.clear();
+        nIns = 0;
+    }
+};
+
+void indelCandidates(const Rle &ref, const Rle &read, const std::vector<Pair> &matches, std::vector<Pair> &inserts,
+                     std::vector<Pair> &deletes, bool cmpRC, IndelCands &out) {
     // candidate indel sequences, reused across candidates and calls of this thread
     thread_local Rle scratchIns, scratchDel;
-    // match weights and observations
-    for (const Pair &m : matches) {
-        Node &node = poa.nodes[m.x + 1];
-        node.bw[symbolOf(read.c[m.y])] += (double) m.w;
-        uint64_t rc = read.n[m.y];
-        if (rc >= poa.maxRC) rc = poa.maxRC - 1;
-        poa.rcwOf(m.x + 1)[rc] += (double) m.w;
-        poa.obs.push_back(Obs{readNo, m.y, (double) m.w});
-        poa.obsNode.push_back((int32_t) (m.x + 1));
-    }
     thread_local MatchSet ms;
+    out.clear();
     ms.build(matches, read.length());
 
     // complete inserts: same x, consecutive y, flanked by matches (or the read's ends)
@@ -315,29 +327,25 @@ void augment(Poa &poa, const Rle &read, bool strand, int64_t readNo, const std::
                 double w = (double) UINT_MAX;
                 for (int64_t m = k; m <= l; m++) w = w < (double) inserts[m].w ? w : (double) inserts[m].w;
                 int64_t pos = st.x + 1;
-                pos = getShift(poa.ref, pos, ins, cmpRC);
-                const int64_t suf = maxCommonSuffix(poa.ref, pos, ins, cmpRC);
+                pos = getShift(ref, pos, ins, cmpRC);
+                const int64_t suf = maxCommonSuffix(ref, pos, ins, cmpRC);
                 if (suf > 0) {
                     rotate(ins, suf);
                     pos -= suf;
                 }
-                Node &node = poa.nodes[pos];
-                Insert *target = nullptr;
-                for (Insert &e : node.ins)
-                    if (e.s == ins) {
-                        target = &e;
-                        break;
-                    }
-                if (!target) {
-                    node.ins.push_back(Insert{ins, 0.0, 0.0, {}});
-                    target = &node.ins.back();
-                }
-                if (strand) target->wF += w; else target->wR += w;
-                target->obs.push_back(Obs{readNo, inserts[k].y, w});
+                out.pos.push_back(pos);
+                out.len.push_back(ins.length());
+                out.at.push_back((int64_t) out.counts.size());
+                out.nonRle.push_back(ins.nonRle);
+                out.w.push_back(w);
+                out.offset.push_back(inserts[k].y);
+                out.chars.append(ins.c);
+                out.counts.insert(out.counts.end(), ins.n.begin(), ins.n.end());
             }
         }
         i = j;
     }
+    out.nIns = (int64_t) out.pos.size();
 
     // complete deletes: same y, consecutive x, flanked by matches (or the reference's ends)
     std::sort(deletes.begin(), deletes.end(), [](const Pair &a, const Pair &b) {
@@ -353,32 +361,96 @@ void augment(Poa &poa, const Rle &read, bool strand, int64_t readNo, const std::
         for (int64_t k = i; k < j; k++) {
             if (!ms.has(st.x + k - i - 1, st.y) && st.x + k - i - 1 > -1) continue;
             for (int64_t l = k; l < j; l++) {
-                if (!ms.has(st.x + l - i + 1, st.y + 1) && st.x + l - i + 1 < poa.ref.length()) continue;
+                if (!ms.has(st.x + l - i + 1, st.y + 1) && st.x + l - i + 1 < ref.length()) continue;
                 const int64_t len = l - k + 1;
                 double w = (double) UINT_MAX;
                 for (int64_t m = k; m <= l; m++) w = w < (double) deletes[m].w ? w : (double) deletes[m].w;
                 int64_t pos = st.x + k - i;
                 Rle &del = scratchDel;
-                poa.ref.subInto(del, pos, len);
-                pos = getShift(poa.ref, pos, del, cmpRC);
-                pos -= maxCommonSuffix(poa.ref, pos, del, cmpRC);
-                Node &node = poa.nodes[pos];
-                Delete *target = nullptr;
-                for (Delete &e : node.del)
-                    if (e.len == len) {
-                        target = &e;
-                        break;
-                    }
-                if (!target) {
-                    node.del.push_back(Delete{len, 0.0, 0.0, {}});
-                    target = &node.del.back();
-                }
-                if (strand) target->wF += w; else target->wR += w;
-                target->obs.push_back(Obs{readNo, st.y, w});
+                ref.subInto(del, pos, len);
+                pos = getShift(ref, pos, del, cmpRC);
+                pos -= maxCommonSuffix(ref, pos, del, cmpRC);
+                out.pos.push_back(pos);
+                out.len.push_back(len);
+                out.at.push_back(-1);
+                out.nonRle.push_back(0);
+                out.w.push_back(w);
+                out.offset.push_back(st.y);
             }
         }
         i = j;
     }
+}
+
+// Adds one read to the graph: match weights and observations (tuple order), then its complete
+// indels, each merged into an equal insert / delete of its node or appended as a new one.
+void mergeRead(Poa &poa, const Rle &read, bool strand, int64_t readNo, int64_t nMatches, const int32_t *mw,
+               const int32_t *mx, const int32_t *my, const IndelCands &ic) {
+    for (int64_t t = 0; t < nMatches; t++) {
+        Node &node = poa.nodes[mx[t] + 1];
+        const double w = (double) mw[t];
+        node.bw[symbolOf(read.c[my[t]])] += w;
+        uint64_t rc = read.n[my[t]];
+        if (rc >= poa.maxRC) rc = poa.maxRC - 1;
+        poa.rcwOf(mx[t] + 1)[rc] += w;
+        poa.obs.push_back(Obs{readNo, my[t], w});
+        poa.obsNode.push_back((int32_t) (mx[t] + 1));
+    }
+    const int64_t n = (int64_t) ic.pos.size();
+    for (int64_t q = 0; q < n; q++) {
+        Node &node = poa.nodes[ic.pos[q]];
+        const double w = ic.w[q];
+        if (q < ic.nIns) {
+            const int64_t L = ic.len[q], at = ic.at[q];
+            Insert *target = nullptr;
+            for (Insert &e : node.ins) {
+                if (e.s.nonRle == ic.nonRle[q] && e.s.length() == L &&
+                    std::equal(e.s.c.begin(), e.s.c.end(), ic.chars.begin() + at) &&
+                    std::equal(e.s.n.begin(), e.s.n.end(), ic.counts.begin() + at)) {
+                    target = &e;
+                    break;
+                }
+            }
+            if (!target) {
+                Insert e;
+                e.s.c.assign(ic.chars.begin() + at, ic.chars.begin() + at + L);
+                e.s.n.assign(ic.counts.begin() + at, ic.counts.begin() + at + L);
+                e.s.nonRle = ic.nonRle[q];
+                node.ins.push_back(std::move(e));
+                target = &node.ins.back();
+            }
+            if (strand) target->wF += w; else target->wR += w;
+            target->obs.push_back(Obs{readNo, ic.offset[q], w});
+        } else {
+            const int64_t len = ic.len[q];
+            Delete *target = nullptr;
+            for (Delete &e : node.del)
+                if (e.len == len) {
+                    target = &e;
+                    break;
+                }
+            if (!target) {
+                node.del.push_back(Delete{len, 0.0, 0.0, {}});
+                target = &node.del.back();
+            }
+            if (strand) target->wF += w; else target->wR += w;
+            target->obs.push_back(Obs{readNo, ic.offset[q], w});
+        }
+    }
+}
+
+// poa_augment (impl/polisher.c:316-534) of one read: its candidates, then the merge.
+void augment(Poa &poa, const Rle &read, bool strand, int64_t readNo, const std::vector<Pair> &matches,
+             std::vector<Pair> &inserts, std::vector<Pair> &deletes, bool cmpRC) {
+    thread_local IndelCands ic;
+    indelCandidates(poa.ref, read, matches, inserts, deletes, cmpRC, ic);
+    std::vector<int32_t> w(matches.size()), x(matches.size()), y(matches.size());
+    for (size_t t = 0; t < matches.size(); t++) {
+        w[t] = (int32_t) matches[t].w;
+        x[t] = (int32_t) matches[t].x;
+        y[t] = (int32_t) matches[t].y;
+    }
+    mergeRead(poa, read, strand, readNo, (int64_t) matches.size(), w.data(), x.data(), y.data(), ic);
 }
 
 // ---------------------------------------------------------------------------
@@ -786,17 +858,36 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
             j += s->chunkReads[c + 1] - s->chunkReads[c];
         }
     }
+    // Candidates first: every read of every listed chunk in parallel (they depend only on the
+    // chunk's reference). Gap-x tuples (consuming the reference) are deletes, gap-y inserts
+    // (impl/polisher.c:638-640).
+    std::vector<int64_t> jobIdx((size_t) nJobs), jobChunk((size_t) nJobs), jobRead((size_t) nJobs);
+    for (int64_t c : chunks)
+        for (int64_t r = s->chunkReads[c]; r < s->chunkReads[c + 1]; r++) {
+            const int64_t j = firstJob[c] + (r - s->chunkReads[c]);
+            jobIdx[(size_t) j] = j;
+            jobChunk[(size_t) j] = c;
+            jobRead[(size_t) j] = r;
+        }
+    std::vector<IndelCands> cands(jobIdx.size());
+    forChunks(jobIdx, [&](int64_t j) {
+        thread_local std::vector<Pair> lists[3];
+        for (int k = 0; k < 3; k++) {
+            lists[k].clear();
+            for (int64_t t = offs[k][j]; t < offs[k][j + 1]; t++) lists[k].push_back(Pair{w[k][t], x[k][t], y[k][t]});
+        }
+        indelCandidates(refs[jobChunk[(size_t) j]], s->reads[jobRead[(size_t) j]], lists[0], lists[2], lists[1],
+                        s->cmpRC, cands[(size_t) j]);
+    });
+    // then each chunk's graph, reads in order (chunks in parallel)
     forChunks(chunks, [&](int64_t c) {
         Poa poa = Poa::fromReference(refs[c], maxRC);
         for (int64_t r = s->chunkReads[c]; r < s->chunkReads[c + 1]; r++) {
             const int64_t j = firstJob[c] + (r - s->chunkReads[c]);
-            std::vector<Pair> lists[3];
-            for (int k = 0; k < 3; k++) {
-                lists[k].reserve((size_t) (offs[k][j + 1] - offs[k][j]));
-                for (int64_t t = offs[k][j]; t < offs[k][j + 1]; t++) lists[k].push_back(Pair{w[k][t], x[k][t], y[k][t]});
-            }
-            // gap-x (consumes the reference) are deletes, gap-y inserts (impl/polisher.c:638-640)
-            augment(poa, s->reads[r], s->strand[r] != 0, r - s->chunkReads[c], lists[0], lists[2], lists[1], s->cmpRC);
+            const int64_t t0 = offs[0][j];
+            mergeRead(poa, s->reads[r], s->strand[r] != 0, r - s->chunkReads[c], offs[0][j + 1] - t0, w[0] + t0,
+                      x[0] + t0, y[0] + t0, cands[(size_t) j]);
+            cands[(size_t) j] = IndelCands();  // release as we go
         }
         poa.groupObs();
         out[c] = std::move(poa);

@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--no-graphs", action="store_true", help="direct launches instead of CUDA graph replay")
     ap.add_argument("--autotune-chunks", type=int, default=24,
                     help="chunks of the separate seeded sample the autotuner times the kernel variants on (0 = off)")
-    ap.add_argument("--chunks-5mb", type=int, default=20,
+    ap.add_argument("--chunks-5mb", type=int, default=50,
                     help="chunks of the 5 Mb configuration (of 50) whose realignment pass is measured")
     ap.add_argument("--no-scale", action="store_true",
                     help="skip the 1 Mb polishing-loop and 5 Mb realignment-pass measurements")

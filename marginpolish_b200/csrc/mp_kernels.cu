@@ -1,5 +1,5 @@
 // Auxiliary device kernels of the realignment engine (sm_100a): anchor band
-// construction (impl/pairwiseAligner.c:96-173) and its 5-diagonal hull, the
+// construction (impl/pairwiseAligner.c:96-173) with its 5-diagonal hull in one pass, the
 // per-job compaction of posterior tuples, and an FP32 FMA throughput probe.
 // The posterior kernel itself is in mp_posterior.cu.
 #include "mp_internal.h"
@@ -41,7 +41,14 @@ __device__ __forceinline__ int clampCoord(int z, int lz) {
     return z < 0 ? 0 : (z > lz ? lz : z);
 }
 
-__global__ void bandKernel(BandArgs a) {
+// Band and hull in one pass. One warp per task; lane l takes anti-diagonal d = base + l of
+// each step of 32. The anchor boxes follow each other along x+y: box k covers the diagonals
+// (e_{k-1}, e_k] with e_k = (x_k + 1) + (y_k + 1) in sub-problem coordinates (e_nA = N), so the
+// 32 boxes from the one holding `base` (each covers at least 2 diagonals) hold every diagonal
+// of the step: a lane finds its box by a binary search over the boxes' ends held across the
+// warp. The raw band of d (impl/pairwiseAligner.c:96-173) and the hull of d-2..d+2 are then
+// written as one 16-byte record, in window-slot units: x-y = 2*slot + (d&1), slot = (x-y) >> 1.
+__global__ void bandHullKernel(BandArgs a) {
     const int lane = threadIdx.x & 31;
     const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (t >= a.nTasks) return;
@@ -49,17 +56,18 @@ __global__ void bandKernel(BandArgs a) {
     const int lx = tk.lx, ly = tk.ly, N = lx + ly;
     const int nA = tk.nAnchors;
     const int32_t *an = a.anchors + 3 * tk.anchorOff;
-    int2 *band = a.band + 2 * tk.bandOff;  // int4 records viewed as pairs: [2d] = (lo, hi)
+    int4 *rec = reinterpret_cast<int4 *>(a.band) + tk.bandOff;
     const bool dynamic = tk.flags & 8;
+    const int2 none = make_int2(INT_MAX, INT_MIN);
     long long cells = 0;
     bool ok = true;
-    if (lane == 0) {
-        band[0] = make_int2(0, 0);
-        cells += N > 0 ? 1 : 0;  // an empty sub-problem computes nothing (impl/pairwiseAligner.c:698-701)
-    }
-    for (int k0 = 0; k0 <= nA; k0 += 32) {
-        int k = k0 + lane;
-        if (k <= nA && N > 0) {
+    int kb = 0;                        // box holding the step's first diagonal (diagonal 0: box 0)
+    int2 below1 = none, below2 = none; // raw bands of base-1 and base-2
+    for (int base = 0; base <= N; base += 32) {
+        // lane i: box kb + i
+        const int k = kb + lane;
+        int end = INT_MAX, xL = 0, yL = 0, xU = 0, yU = 0;
+        if (k <= nA) {
             int px = 0, py = 0, nx, ny, e;
             if (k > 0) {
                 px = an[3 * (k - 1)] - tk.x1 + 1;
@@ -74,54 +82,40 @@ __global__ void bandKernel(BandArgs a) {
                 ny = ly;
                 e = dynamic ? (nA > 0 ? an[3 * (nA - 1) + 2] : 0) : tk.expansion;
             }
-            int pxay = px + py, pxmy = px - py, nxay = nx + ny, nxmy = nx - ny;
-            int xL = clampCoord((pxay + (pxmy - e)) / 2, lx);
-            int yL = clampCoord((nxay - (nxmy - e)) / 2, ly);
-            int xU = clampCoord((nxay + (nxmy + e)) / 2, lx);
-            int yU = clampCoord((pxay - (pxmy + e)) / 2, ly);
-            int dEnd = min(nxay, N);
-            for (int dd = pxay + 1; dd <= dEnd; dd++) {
-                int lo, hi;
-                if (!boxDiagonal(dd, xL, yL, xU, yU, lo, hi)) {
-                    ok = false;
-                    lo = 0;
-                    hi = 0;
-                }
-                band[2 * dd] = make_int2(lo, hi);
-                cells += ((hi - lo) >> 1) + 1;
-            }
+            const int pxay = px + py, pxmy = px - py, nxay = nx + ny, nxmy = nx - ny;
+            xL = clampCoord((pxay + (pxmy - e)) / 2, lx);
+            yL = clampCoord((nxay - (nxmy - e)) / 2, ly);
+            xU = clampCoord((nxay + (nxmy + e)) / 2, lx);
+            yU = clampCoord((pxay - (pxmy + e)) / 2, ly);
+            end = k < nA ? nxay : N;
         }
-    }
-    // reduce cells and validity
+        // raw band of diagonal dd (0 <= dd <= N); `box` receives its box offset from kb
+        auto rawBand = [&](int dd, int &box) -> int2 {
+            int pos = 0;  // first loaded box whose end >= dd
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) cells += __shfl_xor_sync(FULL_MASK, cells, o);
-    bool allOk = __all_sync(FULL_MASK, ok);
-    if (lane == 0) {
-        a.out[t].cells = cells;
-        a.out[t].status = allOk ? 0 : kTaskBand;
-    }
-}
-
-// Hull of the bands of d-2..d+2 (clamped to the task), then every record is
-// converted to window-slot units: x-y = 2*slot + (d&1), so slot = (x-y) >> 1 (floor)
-// for both the band and the hull of the diagonal. One warp per task, lanes stride
-// over diagonals; the raw bands of the two diagonals below each 32-diagonal chunk
-// are carried in registers because the chunk before has already been converted.
-__global__ void hullKernel(BandArgs a) {
-    const int lane = threadIdx.x & 31;
-    const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (t >= a.nTasks) return;
-    const Task &tk = a.tasks[t];
-    const int N = tk.lx + tk.ly;
-    int2 *band = a.band + 2 * tk.bandOff;
-    const int2 none = make_int2(INT_MAX, INT_MIN);
-    int2 below1 = none, below2 = none;  // raw bands of base-1 and base-2
-    for (int base = 0; base <= N; base += 32) {
+            for (int step = 16; step > 0; step >>= 1) {
+                const int v = __shfl_sync(FULL_MASK, end, pos + step - 1);
+                if (v < dd) pos += step;
+            }
+            box = pos;
+            const int bxL = __shfl_sync(FULL_MASK, xL, pos), byL = __shfl_sync(FULL_MASK, yL, pos);
+            const int bxU = __shfl_sync(FULL_MASK, xU, pos), byU = __shfl_sync(FULL_MASK, yU, pos);
+            if (dd == 0) return make_int2(0, 0);
+            int lo, hi;
+            if (!boxDiagonal(dd, bxL, byL, bxU, byU, lo, hi)) {
+                ok = false;
+                return make_int2(0, 0);
+            }
+            return make_int2(lo, hi);
+        };
         const int d = base + lane;
-        const int2 v = d <= N ? band[2 * d] : none;
-        // the two diagonals above the chunk are not converted yet
-        const int2 above = (lane < 2 && base + 32 + lane <= N) ? band[2 * (base + 32 + lane)] : none;
-        int2 n[4];  // bands of d-2, d-1, d+1, d+2
+        int box0 = 0, boxUp = 0;
+        const int2 v = d <= N ? rawBand(d, box0) : (rawBand(N, box0), none);
+        // diagonals base+32 and base+33 (the hull of the step's last two lanes needs them)
+        const int du = base + 32 + (lane & 1);
+        const int2 up = du <= N ? rawBand(du, boxUp) : (rawBand(N, boxUp), none);
+        if (d <= N && N > 0) cells += ((v.y - v.x) >> 1) + 1;  // an empty sub-problem computes nothing
+        int2 n[4];  // raw bands of d-2, d-1, d+1, d+2
         const int offs[4] = {-2, -1, 1, 2};
 #pragma unroll
         for (int q = 0; q < 4; q++) {
@@ -129,8 +123,7 @@ __global__ void hullKernel(BandArgs a) {
             int2 w;
             w.x = __shfl_sync(FULL_MASK, v.x, src & 31);
             w.y = __shfl_sync(FULL_MASK, v.y, src & 31);
-            const int2 ab = make_int2(__shfl_sync(FULL_MASK, above.x, src & 1),
-                                      __shfl_sync(FULL_MASK, above.y, src & 1));
+            const int2 ab = make_int2(__shfl_sync(FULL_MASK, up.x, src & 1), __shfl_sync(FULL_MASK, up.y, src & 1));
             if (src < 0) w = src == -1 ? below1 : below2;
             if (src > 31) w = ab;
             const int e = d + offs[q];
@@ -142,13 +135,18 @@ __global__ void hullKernel(BandArgs a) {
             lo = min(lo, n[q].x);
             hi = max(hi, n[q].y);
         }
+        if (d <= N) rec[d] = make_int4(v.x >> 1, v.y >> 1, lo >> 1, hi >> 1);
         below1 = make_int2(__shfl_sync(FULL_MASK, v.x, 31), __shfl_sync(FULL_MASK, v.y, 31));
         below2 = make_int2(__shfl_sync(FULL_MASK, v.x, 30), __shfl_sync(FULL_MASK, v.y, 30));
-        __syncwarp();
-        if (d <= N) {
-            band[2 * d] = make_int2(v.x >> 1, v.y >> 1);
-            band[2 * d + 1] = make_int2(lo >> 1, hi >> 1);
-        }
+        // the next step starts at the box of diagonal base + 32
+        kb += __shfl_sync(FULL_MASK, boxUp, 0);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cells += __shfl_xor_sync(FULL_MASK, cells, o);
+    const bool allOk = __all_sync(FULL_MASK, ok);
+    if (lane == 0) {
+        a.out[t].cells = cells;
+        a.out[t].status = allOk ? 0 : kTaskBand;
     }
 }
 
@@ -207,10 +205,7 @@ cudaError_t launchBand(const BandArgs &a, cudaStream_t s) {
     if (a.nTasks == 0) return cudaSuccess;
     int threads = 256;
     int blocks = (a.nTasks * 32 + threads - 1) / threads;
-    bandKernel<<<blocks, threads, 0, s>>>(a);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    hullKernel<<<blocks, threads, 0, s>>>(a);
+    bandHullKernel<<<blocks, threads, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -35,6 +35,7 @@ int adjointVariantMaxWarps(int v, int nTables);
 cudaError_t launchAdjointVariant(int v, const DpArgs &a, int blocks, int warps, cudaStream_t s);
 cudaError_t launchBand(const BandArgs &a, cudaStream_t s);
 cudaError_t launchCompact(const CompactArgs &a, cudaStream_t s);
+cudaError_t launchStatusCopy(const TaskOut *src, TaskOut *dst, int n, cudaStream_t s);
 }  // namespace mp
 
 using namespace mp;
@@ -588,6 +589,8 @@ struct mp_device_batch {
     DevBuf expect, expectRep;  // adjoint accumulators (FP64)
     DevBuf fetchDst[3], fetchW[3], fetchX[3], fetchY[3];  // compaction staging (reused)
     PinBuf stageTasks, stageOrders, stageDst[3];           // page-locked staging of the small uploads
+    PinBuf stageIn[3];     // small inputs (templates, reads, anchors) from pageable caller memory
+    PinBuf stageFetch;     // small results on their way to pageable result arrays
     std::vector<int> varOrderOff;  // per variant offset into orders
     std::vector<int> varCount;
     std::vector<int64_t> varMaxN;
@@ -609,7 +612,8 @@ struct mp_device_batch {
     cudaEvent_t evUploaded = nullptr;       // pipelined slots: this slice's input copies are done
     cudaEvent_t evSync = nullptr;           // blocking-sync event the host waits on (sleeps, no spin)
     bool copyPending = false;
-    TaskOut *pinOut = nullptr;              // page-locked copy of the task statuses
+    TaskOut *pinOut = nullptr;              // page-locked, mapped copy of the task statuses
+    TaskOut *pinOutDev = nullptr;           // its device address (written by a small kernel)
     size_t pinOutCap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaGraphExec_t graphExec = nullptr;  // the pass's launches (engine graph capture on)
@@ -917,6 +921,11 @@ static mp_status upload(DevBuf &buf, const void *src, size_t bytes, cudaStream_t
     return MP_OK;
 }
 
+// Transfers at most this many bytes go through the batch's page-locked staging when the
+// caller's memory is pageable: the host copy is cheap, and a pageable transfer would go
+// through the driver's own staging, which many calling threads share and queue on.
+constexpr size_t kStageMax = (size_t) 8 << 20;
+
 // upload() of a host vector through a page-locked staging buffer: the copy is DMA in stream
 // order and the host returns at once. The staging buffer is rewritten by the next staged
 // upload of the same purpose, which the batch's call sequence issues only after a
@@ -928,6 +937,21 @@ static mp_status uploadStaged(DevBuf &buf, PinBuf &stage, const void *src, size_
     memcpy(stage.p, src, bytes);
     CUDA_TRY(cudaMemcpyAsync(buf.p, stage.p, bytes, cudaMemcpyHostToDevice, s));
     return MP_OK;
+}
+
+// Pageable host memory (not page-locked, not registered with CUDA).
+static bool pageable(const void *p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return at.type == cudaMemoryTypeUnregistered;
+}
+
+static mp_status uploadSmall(DevBuf &buf, PinBuf &stage, const void *src, size_t bytes, cudaStream_t s) {
+    return bytes > 0 && bytes <= kStageMax && pageable(src) ? uploadStaged(buf, stage, src, bytes, s)
+                                                            : upload(buf, src, bytes, s);
 }
 
 // Plans a batch into `db` and uploads it, reusing the device buffers db already holds
@@ -953,9 +977,9 @@ static mp_status batchReset(mp_engine *e, mp_device_batch *db, const mp_model *m
     cudaStream_t st = db->stream;
     int64_t ny = b->n_jobs > 0 ? b->y_offsets[b->n_jobs] : 0;
     int64_t na = b->n_jobs > 0 ? b->anchor_offsets[b->n_jobs] : 0;
-    MP_TRY(upload(db->xs, b->x_symbols, sizeof(uint16_t) * b->x_symbols_length, st));
-    MP_TRY(upload(db->ys, b->y_symbols, sizeof(uint16_t) * ny, st));
-    MP_TRY(upload(db->anchors, b->anchors, sizeof(int32_t) * 3 * na, st));
+    MP_TRY(uploadSmall(db->xs, db->stageIn[0], b->x_symbols, sizeof(uint16_t) * b->x_symbols_length, st));
+    MP_TRY(uploadSmall(db->ys, db->stageIn[1], b->y_symbols, sizeof(uint16_t) * ny, st));
+    MP_TRY(uploadSmall(db->anchors, db->stageIn[2], b->anchors, sizeof(int32_t) * 3 * na, st));
     MP_TRY(uploadStaged(db->dTasks, db->stageTasks, db->tasks.data(), sizeof(Task) * db->tasks.size(), st));
     MP_TRY(db->band.reserve(sizeof(int4) * std::max<int64_t>(db->totalDiags, 1)));
     MP_TRY(db->dOut.reserve(sizeof(TaskOut) * std::max<size_t>(db->tasks.size(), 1)));
@@ -1190,14 +1214,19 @@ static mp_status runIssue(mp_engine *e, mp_device_batch *db) {
         CUDA_TRY(cudaEventRecord(db->ev1, st));
     }
     // statuses, into page-locked memory so that the copy does not wait on the host
+    // The statuses go to mapped page-locked memory through a small kernel: a copy would queue on
+    // the copy engine behind earlier slices' tuple copies, and the host would learn late that
+    // this run has ended.
     if ((size_t) nTasks > db->pinOutCap) {
         if (db->pinOut) cudaFreeHost(db->pinOut);
         db->pinOut = nullptr;
+        db->pinOutDev = nullptr;
         db->pinOutCap = 0;
-        CUDA_TRY(cudaMallocHost(&db->pinOut, sizeof(TaskOut) * (size_t) nTasks));
+        CUDA_TRY(cudaHostAlloc(&db->pinOut, sizeof(TaskOut) * (size_t) nTasks, cudaHostAllocMapped | cudaHostAllocPortable));
+        CUDA_TRY(cudaHostGetDevicePointer((void **) &db->pinOutDev, db->pinOut, 0));
         db->pinOutCap = (size_t) nTasks;
     }
-    if (nTasks) CUDA_TRY(cudaMemcpyAsync(db->pinOut, db->dOut.p, sizeof(TaskOut) * nTasks, cudaMemcpyDeviceToHost, st));
+    if (nTasks) CUDA_TRY(launchStatusCopy(db->dOut.as<TaskOut>(), db->pinOutDev, nTasks, st));
     return MP_OK;
 }
 
@@ -1522,6 +1551,14 @@ static mp_status fetchIssue(mp_engine *e, mp_device_batch *db, const mp_output *
         MP_TRY(db->fetchX[k].reserve(n));
         MP_TRY(db->fetchY[k].reserve(n));
     }
+    // With a copy stream (pipelined slots), the compaction runs there too, at high priority, so
+    // that it is not queued behind later slices' posterior kernels.
+    cudaStream_t cs = st;
+    if (db->copyStream) {
+        CUDA_TRY(cudaEventRecord(db->evCompacted, st));
+        CUDA_TRY(cudaStreamWaitEvent(db->copyStream, db->evCompacted, 0));
+        cs = db->copyStream;
+    }
     if (nTasks > 0) {
         CompactArgs ca;
         ca.tasks = db->dTasks.as<Task>();
@@ -1534,13 +1571,7 @@ static mp_status fetchIssue(mp_engine *e, mp_device_batch *db, const mp_output *
             ca.x[k] = db->fetchX[k].as<int32_t>();
             ca.y[k] = db->fetchY[k].as<int32_t>();
         }
-        CUDA_TRY(launchCompact(ca, st));
-    }
-    cudaStream_t cs = st;
-    if (db->copyStream) {
-        CUDA_TRY(cudaEventRecord(db->evCompacted, st));
-        CUDA_TRY(cudaStreamWaitEvent(db->copyStream, db->evCompacted, 0));
-        cs = db->copyStream;
+        CUDA_TRY(launchCompact(ca, cs));
     }
     for (int k = 0; k < 3; k++) {
         if (!copy[k]) continue;
@@ -1601,10 +1632,38 @@ extern "C" mp_status mp_device_batch_fetch(mp_engine *e, mp_device_batch *db, mp
     r->cells.assign(db->nJobs, 0);
     o.log_likelihood = r->logLik.data();
     o.cells = r->cells.data();
+    // small results come through page-locked staging (one block, lists back to back), then a
+    // host copy into the result's arrays
+    const size_t tupleBytes = sizeof(int32_t) * 3 * (size_t) (totals[0] + totals[1] + totals[2]);
+    const bool staged = tupleBytes <= kStageMax;
+    if (staged) {
+        mp_status rs = db->stageFetch.reserve(std::max<size_t>(tupleBytes, 16));
+        if (rs != MP_OK) {
+            delete r;
+            return rs;
+        }
+        int32_t *at = static_cast<int32_t *>(db->stageFetch.p);
+        for (int k = 0; k < 3; k++) {
+            o.weight[k] = at;
+            o.x[k] = at + totals[k];
+            o.y[k] = at + 2 * totals[k];
+            at += 3 * totals[k];
+        }
+    }
     mp_status s = fetchInto(e, db, &o);
     if (s != MP_OK) {
         delete r;
         return s;
+    }
+    if (staged) {
+        const int32_t *at = static_cast<const int32_t *>(db->stageFetch.p);
+        for (int k = 0; k < 3; k++) {
+            const size_t n = sizeof(int32_t) * (size_t) totals[k];
+            memcpy(r->w[k].get(), at, n);
+            memcpy(r->x[k].get(), at + totals[k], n);
+            memcpy(r->y[k].get(), at + 2 * totals[k], n);
+            at += 3 * totals[k];
+        }
     }
     for (int64_t c : r->cells) r->totalCells += c;
     *out = r;
@@ -1850,7 +1909,9 @@ extern "C" mp_status mp_realign_batch_into(mp_engine *e, const mp_model *m, cons
             return failf(MP_ERR_CUDA, "stream creation failed");
         }
         db->ownStream = true;
-        if (cudaStreamCreateWithFlags(&db->copyStream, cudaStreamNonBlocking) != cudaSuccess ||
+        int leastPrio = 0, greatestPrio = 0;
+        cudaDeviceGetStreamPriorityRange(&leastPrio, &greatestPrio);
+        if (cudaStreamCreateWithPriority(&db->copyStream, cudaStreamNonBlocking, greatestPrio) != cudaSuccess ||
             cudaEventCreateWithFlags(&db->evCompacted, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&db->evCopied, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&db->evUploaded, cudaEventDisableTiming) != cudaSuccess) {
@@ -1915,6 +1976,12 @@ extern "C" mp_status mp_realign_batch_into(mp_engine *e, const mp_model *m, cons
         db->scratchBudget = e->scratchBudget / (size_t) nSlots;
         // a reused slot's previous slice has queued its copies on the slot's streams: the new
         // inputs follow them in stream order; the batch's host arrays stay valid until the return
+        // the slot's previous slice is compacted and copied out on the copy stream: its buffers
+        // are rewritten only after that (a wait on the device, not on the host)
+        if (db->copyPending && cudaStreamWaitEvent(db->stream, db->evCopied, 0) != cudaSuccess) {
+            st = failf(MP_ERR_CUDA, "stream wait failed");
+            break;
+        }
         if (prevUploaded && cudaStreamWaitEvent(db->stream, prevUploaded, 0) != cudaSuccess) {
             st = failf(MP_ERR_CUDA, "stream wait failed");
             break;

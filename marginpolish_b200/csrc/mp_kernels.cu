@@ -4,6 +4,7 @@
 // The posterior kernel itself is in mp_posterior.cu.
 #include "mp_internal.h"
 
+#include <algorithm>
 #include <cstdio>
 
 namespace mp {
@@ -41,13 +42,15 @@ __device__ __forceinline__ int clampCoord(int z, int lz) {
     return z < 0 ? 0 : (z > lz ? lz : z);
 }
 
-// Band and hull in one pass. One warp per task; lane l takes anti-diagonal d = base + l of
-// each step of 32. The anchor boxes follow each other along x+y: box k covers the diagonals
-// (e_{k-1}, e_k] with e_k = (x_k + 1) + (y_k + 1) in sub-problem coordinates (e_nA = N), so the
-// 32 boxes from the one holding `base` (each covers at least 2 diagonals) hold every diagonal
-// of the step: a lane finds its box by a binary search over the boxes' ends held across the
-// warp. The raw band of d (impl/pairwiseAligner.c:96-173) and the hull of d-2..d+2 are then
-// written as one 16-byte record, in window-slot units: x-y = 2*slot + (d&1), slot = (x-y) >> 1.
+// Band and hull in one pass. One warp per task; lane l computes the raw band of anti-diagonal
+// d = base + l of each step of 32 (impl/pairwiseAligner.c:96-173). The anchor boxes follow
+// each other along x+y: box k covers the diagonals (e_{k-1}, e_k] with e_k = (x_k + 1) +
+// (y_k + 1) in sub-problem coordinates (e_nA = N). The 32 boxes from the one holding `base`
+// (each covers at least 2 diagonals) hold every diagonal of the step: lane i holds box kb+i,
+// the step's box ends are gathered into one bit mask (one warp OR), and the box of d is the
+// count of ends before it. The hull of d-2..d+2 needs the next two diagonals, so each step
+// writes the records of base-2 .. base+29 (a last step writes the remainder), one 16-byte
+// store per diagonal, in window-slot units: x-y = 2*slot + (d&1), slot = (x-y) >> 1.
 __global__ void bandHullKernel(BandArgs a) {
     const int lane = threadIdx.x & 31;
     const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -61,13 +64,13 @@ __global__ void bandHullKernel(BandArgs a) {
     const int2 none = make_int2(INT_MAX, INT_MIN);
     long long cells = 0;
     bool ok = true;
-    int kb = 0;                        // box holding the step's first diagonal (diagonal 0: box 0)
-    int2 below1 = none, below2 = none; // raw bands of base-1 and base-2
-    for (int base = 0; base <= N; base += 32) {
+    int kb = 0;             // box holding the step's first diagonal (diagonal 0: box 0)
+    int2 prev = none;       // this lane's raw band in the previous step
+    for (int base = 0; base <= N + 2; base += 32) {
         // lane i: box kb + i
         const int k = kb + lane;
         int end = INT_MAX, xL = 0, yL = 0, xU = 0, yU = 0;
-        if (k <= nA) {
+        if (k <= nA && base <= N) {
             int px = 0, py = 0, nx, ny, e;
             if (k > 0) {
                 px = an[3 * (k - 1)] - tk.x1 + 1;
@@ -89,57 +92,47 @@ __global__ void bandHullKernel(BandArgs a) {
             yU = clampCoord((pxay - (pxmy + e)) / 2, ly);
             end = k < nA ? nxay : N;
         }
-        // raw band of diagonal dd (0 <= dd <= N); `box` receives its box offset from kb
-        auto rawBand = [&](int dd, int &box) -> int2 {
-            int pos = 0;  // first loaded box whose end >= dd
-#pragma unroll
-            for (int step = 16; step > 0; step >>= 1) {
-                const int v = __shfl_sync(FULL_MASK, end, pos + step - 1);
-                if (v < dd) pos += step;
-            }
-            box = pos;
-            const int bxL = __shfl_sync(FULL_MASK, xL, pos), byL = __shfl_sync(FULL_MASK, yL, pos);
-            const int bxU = __shfl_sync(FULL_MASK, xU, pos), byU = __shfl_sync(FULL_MASK, yU, pos);
-            if (dd == 0) return make_int2(0, 0);
-            int lo, hi;
-            if (!boxDiagonal(dd, bxL, byL, bxU, byU, lo, hi)) {
-                ok = false;
-                return make_int2(0, 0);
-            }
-            return make_int2(lo, hi);
-        };
+        // ends within the step (box kb ends at or after base, so none is before it)
+        const int m = end - base;
+        const unsigned ends = __reduce_or_sync(FULL_MASK, (m >= 0 && m < 32) ? 1u << m : 0u);
+        const int box = __popc(ends & ((1u << lane) - 1u));  // boxes ending before d
+        const int bxL = __shfl_sync(FULL_MASK, xL, box), byL = __shfl_sync(FULL_MASK, yL, box);
+        const int bxU = __shfl_sync(FULL_MASK, xU, box), byU = __shfl_sync(FULL_MASK, yU, box);
         const int d = base + lane;
-        int box0 = 0, boxUp = 0;
-        const int2 v = d <= N ? rawBand(d, box0) : (rawBand(N, box0), none);
-        // diagonals base+32 and base+33 (the hull of the step's last two lanes needs them)
-        const int du = base + 32 + (lane & 1);
-        const int2 up = du <= N ? rawBand(du, boxUp) : (rawBand(N, boxUp), none);
+        int2 v = none;
+        if (d == 0) {
+            v = make_int2(0, 0);
+        } else if (d <= N) {
+            int lo, hi;
+            if (!boxDiagonal(d, bxL, byL, bxU, byU, lo, hi)) {
+                ok = false;
+                lo = hi = 0;
+            }
+            v = make_int2(lo, hi);
+        }
         if (d <= N && N > 0) cells += ((v.y - v.x) >> 1) + 1;  // an empty sub-problem computes nothing
-        int2 n[4];  // raw bands of d-2, d-1, d+1, d+2
-        const int offs[4] = {-2, -1, 1, 2};
+        // record of diagonal f = base - 2 + lane: raw bands of f-2 .. f+2 = base-4+lane .. base+lane
+        const int f = d - 2;
+        int2 w[5];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int src = lane + offs[q];
-            int2 w;
-            w.x = __shfl_sync(FULL_MASK, v.x, src & 31);
-            w.y = __shfl_sync(FULL_MASK, v.y, src & 31);
-            const int2 ab = make_int2(__shfl_sync(FULL_MASK, up.x, src & 1), __shfl_sync(FULL_MASK, up.y, src & 1));
-            if (src < 0) w = src == -1 ? below1 : below2;
-            if (src > 31) w = ab;
-            const int e = d + offs[q];
-            n[q] = (e < 0 || e > N) ? none : w;
+        for (int q = 0; q < 5; q++) {
+            const int src = lane + q - 4;
+            const int2 cur = make_int2(__shfl_sync(FULL_MASK, v.x, src & 31), __shfl_sync(FULL_MASK, v.y, src & 31));
+            const int2 old = make_int2(__shfl_sync(FULL_MASK, prev.x, src & 31), __shfl_sync(FULL_MASK, prev.y, src & 31));
+            w[q] = src >= 0 ? cur : old;
         }
-        int lo = v.x, hi = v.y;
+        if (f >= 0 && f <= N) {
+            int lo = w[2].x, hi = w[2].y;
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            lo = min(lo, n[q].x);
-            hi = max(hi, n[q].y);
+            for (int q = 0; q < 5; q++) {  // diagonals outside 0..N hold `none`
+                lo = min(lo, w[q].x);
+                hi = max(hi, w[q].y);
+            }
+            rec[f] = make_int4(w[2].x >> 1, w[2].y >> 1, lo >> 1, hi >> 1);
         }
-        if (d <= N) rec[d] = make_int4(v.x >> 1, v.y >> 1, lo >> 1, hi >> 1);
-        below1 = make_int2(__shfl_sync(FULL_MASK, v.x, 31), __shfl_sync(FULL_MASK, v.y, 31));
-        below2 = make_int2(__shfl_sync(FULL_MASK, v.x, 30), __shfl_sync(FULL_MASK, v.y, 30));
+        prev = v;
         // the next step starts at the box of diagonal base + 32
-        kb += __shfl_sync(FULL_MASK, boxUp, 0);
+        kb += __popc(__ballot_sync(FULL_MASK, m < 32));
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) cells += __shfl_xor_sync(FULL_MASK, cells, o);
@@ -206,6 +199,19 @@ cudaError_t launchBand(const BandArgs &a, cudaStream_t s) {
     int threads = 256;
     int blocks = (a.nTasks * 32 + threads - 1) / threads;
     bandHullKernel<<<blocks, threads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// Task statuses into mapped page-locked host memory (16-byte words; a TaskOut is two).
+__global__ void statusCopyKernel(const int4 *src, int4 *dst, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[i];
+}
+
+cudaError_t launchStatusCopy(const TaskOut *src, TaskOut *dst, int nTasks, cudaStream_t s) {
+    static_assert(sizeof(TaskOut) == 32, "a task status is two 16-byte words");
+    const int n = 2 * nTasks;
+    const int blocks = std::min(148, (n + 255) / 256);
+    statusCopyKernel<<<blocks, 256, 0, s>>>(reinterpret_cast<const int4 *>(src), reinterpret_cast<int4 *>(dst), n);
     return cudaGetLastError();
 }
 

@@ -10,6 +10,8 @@
 #include "mp_internal.h"
 #include "mp_host.h"
 
+#include <sched.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -611,6 +613,7 @@ struct mp_device_batch {
     cudaEvent_t evCompacted = nullptr, evCopied = nullptr;
     cudaEvent_t evUploaded = nullptr;       // pipelined slots: this slice's input copies are done
     cudaEvent_t evSync = nullptr;           // blocking-sync event the host waits on (sleeps, no spin)
+    cudaEvent_t evKernels = nullptr;        // pipelined slots: the run's kernels are done
     bool copyPending = false;
     TaskOut *pinOut = nullptr;              // page-locked, mapped copy of the task statuses
     TaskOut *pinOutDev = nullptr;           // its device address (written by a small kernel)
@@ -631,20 +634,23 @@ struct mp_device_batch {
         if (evCopied) cudaEventDestroy(evCopied);
         if (evUploaded) cudaEventDestroy(evUploaded);
         if (evSync) cudaEventDestroy(evSync);
+        if (evKernels) cudaEventDestroy(evKernels);
     }
 };
 
-// Waits until everything queued on `st` has run. The host thread sleeps on a blocking-sync
-// event instead of spinning: callers that drive the engine from many threads at once (the
-// drop-in's OpenMP callers, each with its own engine) leave the cores to the threads that
-// are planning and filling their next calls.
+// Waits until everything queued on `st` has run. The host thread polls an event and yields its
+// core between polls, instead of spinning in the runtime: callers that drive the engine from
+// many threads at once (the drop-in's OpenMP callers, each with its own engine) leave the
+// cores to the threads still planning and filling their calls, while a lone caller still
+// sees the end of its work within a scheduler tick.
 static cudaError_t waitStream(mp_device_batch *db, cudaStream_t st) {
     if (!db->evSync) {
-        const cudaError_t e = cudaEventCreateWithFlags(&db->evSync, cudaEventBlockingSync | cudaEventDisableTiming);
+        const cudaError_t e = cudaEventCreateWithFlags(&db->evSync, cudaEventDisableTiming);
         if (e != cudaSuccess) return e;
     }
     cudaError_t e = cudaEventRecord(db->evSync, st);
-    if (e == cudaSuccess) e = cudaEventSynchronize(db->evSync);
+    if (e != cudaSuccess) return e;
+    while ((e = cudaEventQuery(db->evSync)) == cudaErrorNotReady) sched_yield();
     return e;
 }
 
@@ -1226,7 +1232,15 @@ static mp_status runIssue(mp_engine *e, mp_device_batch *db) {
         CUDA_TRY(cudaHostGetDevicePointer((void **) &db->pinOutDev, db->pinOut, 0));
         db->pinOutCap = (size_t) nTasks;
     }
-    if (nTasks) CUDA_TRY(launchStatusCopy(db->dOut.as<TaskOut>(), db->pinOutDev, nTasks, st));
+    // pipelined slots: on the high-priority copy stream, so that the status copy is not queued
+    // behind other slices' posterior kernels
+    cudaStream_t ss = st;
+    if (db->copyStream) {
+        CUDA_TRY(cudaEventRecord(db->evKernels, st));
+        CUDA_TRY(cudaStreamWaitEvent(db->copyStream, db->evKernels, 0));
+        ss = db->copyStream;
+    }
+    if (nTasks) CUDA_TRY(launchStatusCopy(db->dOut.as<TaskOut>(), db->pinOutDev, nTasks, ss));
     return MP_OK;
 }
 
@@ -1236,7 +1250,7 @@ static mp_status runFinish(mp_engine *e, mp_device_batch *db, float *kernelMs) {
     cudaStream_t st = db->stream;
     const int nTasks = (int) db->tasks.size();
     std::vector<int32_t> orderHost;
-    CUDA_TRY(waitStream(db, st));
+    CUDA_TRY(waitStream(db, db->copyStream ? db->copyStream : st));  // the statuses are written there
     db->hostOut.assign(db->pinOut, db->pinOut + nTasks);
     float ms = 0.0f;
     CUDA_TRY(cudaEventElapsedTime(&ms, db->ev0, db->ev1));
@@ -1914,7 +1928,8 @@ extern "C" mp_status mp_realign_batch_into(mp_engine *e, const mp_model *m, cons
         if (cudaStreamCreateWithPriority(&db->copyStream, cudaStreamNonBlocking, greatestPrio) != cudaSuccess ||
             cudaEventCreateWithFlags(&db->evCompacted, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&db->evCopied, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&db->evUploaded, cudaEventDisableTiming) != cudaSuccess) {
+            cudaEventCreateWithFlags(&db->evUploaded, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&db->evKernels, cudaEventDisableTiming) != cudaSuccess) {
             delete db;
             return failf(MP_ERR_CUDA, "stream / event creation failed");
         }

@@ -145,24 +145,30 @@ __global__ void bandHullKernel(BandArgs a) {
 
 // ---------------------------------------------------------------------------
 // Compaction: gathers each task's tuples (top of its region) into the final
-// per-job layout (tasks of a job are consecutive, in split order).
+// per-job layout (tasks of a job are consecutive, in split order). A small grid of warps
+// walks the (task, list) items: the compaction often shares the SMs with posterior blocks of
+// other batches, so it asks for few blocks and no shared memory.
 // ---------------------------------------------------------------------------
 
 __global__ void compactKernel(CompactArgs a) {
-    const int k = blockIdx.y;
-    const int t = blockIdx.x;
-    if (t >= a.nTasks) return;
-    const Task &tk = a.tasks[t];
-    const int n = a.out[t].count[k];
-    const int64_t from = tk.outOff[k] + tk.cap[k] - n;
-    const int64_t to = a.dst[k] ? a.dst[k][t] : 0;
-    const int4 *src = a.src[k] + from;
-    int32_t *w = a.w[k] + to, *x = a.x[k] + to, *y = a.y[k] + to;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const int4 v = src[i];
-        w[i] = v.x;
-        x[i] = v.y;
-        y[i] = v.z;
+    // one warp per (task, list) item, items strided over the grid's warps
+    const int lane = threadIdx.x & 31;
+    const int nItems = 3 * a.nTasks;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < nItems; item += warps) {
+        const int t = item / 3, k = item - 3 * t;
+        const Task &tk = a.tasks[t];
+        const int n = a.out[t].count[k];
+        const int64_t from = tk.outOff[k] + tk.cap[k] - n;
+        const int64_t to = a.dst[k] ? a.dst[k][t] : 0;
+        const int4 *src = a.src[k] + from;
+        int32_t *w = a.w[k] + to, *x = a.x[k] + to, *y = a.y[k] + to;
+        for (int i = lane; i < n; i += 32) {
+            const int4 v = src[i];
+            w[i] = v.x;
+            x[i] = v.y;
+            y[i] = v.z;
+        }
     }
 }
 
@@ -217,8 +223,9 @@ cudaError_t launchStatusCopy(const TaskOut *src, TaskOut *dst, int nTasks, cudaS
 
 cudaError_t launchCompact(const CompactArgs &a, cudaStream_t s) {
     if (a.nTasks == 0) return cudaSuccess;
-    dim3 grid(a.nTasks, 3);
-    compactKernel<<<grid, 128, 0, s>>>(a);
+    const int items = 3 * a.nTasks;                      // warps of work
+    const int blocks = std::min(4 * 148, (items + 7) / 8);  // 8 warps a block
+    compactKernel<<<blocks, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -134,6 +134,7 @@ extern "C" void mp_engine_destroy(mp_engine *e) {
         mp_device_batch_destroy(e->pipe[k]);  // destroys its own stream
         e->pipe[k] = nullptr;
     }
+    if (e->outStream) cudaStreamDestroy(e->outStream);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }
@@ -614,6 +615,9 @@ struct mp_device_batch {
     cudaEvent_t evUploaded = nullptr;       // pipelined slots: this slice's input copies are done
     cudaEvent_t evSync = nullptr;           // blocking-sync event the host waits on (sleeps, no spin)
     cudaEvent_t evKernels = nullptr;        // pipelined slots: the run's kernels are done
+    cudaEvent_t evStatus = nullptr;         // pipelined slots: the run's statuses are on the host
+    cudaEvent_t evReady = nullptr;          // pipelined slots: the run's tuples are compacted
+    cudaStream_t outStream = nullptr;       // pipelined slots: the engine's stream of tuple copies
     bool copyPending = false;
     TaskOut *pinOut = nullptr;              // page-locked, mapped copy of the task statuses
     TaskOut *pinOutDev = nullptr;           // its device address (written by a small kernel)
@@ -635,6 +639,8 @@ struct mp_device_batch {
         if (evUploaded) cudaEventDestroy(evUploaded);
         if (evSync) cudaEventDestroy(evSync);
         if (evKernels) cudaEventDestroy(evKernels);
+        if (evStatus) cudaEventDestroy(evStatus);
+        if (evReady) cudaEventDestroy(evReady);
     }
 };
 
@@ -1241,6 +1247,7 @@ static mp_status runIssue(mp_engine *e, mp_device_batch *db) {
         ss = db->copyStream;
     }
     if (nTasks) CUDA_TRY(launchStatusCopy(db->dOut.as<TaskOut>(), db->pinOutDev, nTasks, ss));
+    if (db->copyStream) CUDA_TRY(cudaEventRecord(db->evStatus, ss));
     return MP_OK;
 }
 
@@ -1587,6 +1594,13 @@ static mp_status fetchIssue(mp_engine *e, mp_device_batch *db, const mp_output *
         }
         CUDA_TRY(launchCompact(ca, cs));
     }
+    // the pipelined slots' tuple copies all go to the engine's one copy stream, so that the
+    // slices' tuples leave in slice order at the link's full speed
+    if (db->outStream) {
+        CUDA_TRY(cudaEventRecord(db->evReady, cs));
+        CUDA_TRY(cudaStreamWaitEvent(db->outStream, db->evReady, 0));
+        cs = db->outStream;
+    }
     for (int k = 0; k < 3; k++) {
         if (!copy[k]) continue;
         const size_t n = sizeof(int32_t) * total[k];
@@ -1914,6 +1928,7 @@ extern "C" mp_status mp_realign_batch_into(mp_engine *e, const mp_model *m, cons
     if (parts <= 0) parts = n >= 2048 ? mp_engine::kPipeSlots : 1;
     parts = (int32_t) std::max<int64_t>(1, std::min<int64_t>(parts, std::max<int64_t>(n, 1)));
     const int nSlots = std::min<int>(parts, mp_engine::kPipeSlots);
+    if (!e->outStream) CUDA_TRY(cudaStreamCreateWithFlags(&e->outStream, cudaStreamNonBlocking));
     for (int k = 0; k < nSlots; k++) {
         if (e->pipe[k]) continue;
         mp_device_batch *db = new mp_device_batch();
@@ -1929,7 +1944,9 @@ extern "C" mp_status mp_realign_batch_into(mp_engine *e, const mp_model *m, cons
             cudaEventCreateWithFlags(&db->evCompacted, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&db->evCopied, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&db->evUploaded, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&db->evKernels, cudaEventDisableTiming) != cudaSuccess) {
+            cudaEventCreateWithFlags(&db->evKernels, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&db->evStatus, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&db->evReady, cudaEventDisableTiming) != cudaSuccess) {
             delete db;
             return failf(MP_ERR_CUDA, "stream / event creation failed");
         }
@@ -1988,6 +2005,7 @@ extern "C" mp_status mp_realign_batch_into(mp_engine *e, const mp_model *m, cons
         sb.x_shift = b->x_shift ? b->x_shift + j0 : nullptr;
         mp_device_batch *db = e->pipe[i % nSlots];
         db->mode = kModePosterior;
+        db->outStream = e->outStream;
         db->scratchBudget = e->scratchBudget / (size_t) nSlots;
         // a reused slot's previous slice has queued its copies on the slot's streams: the new
         // inputs follow them in stream order; the batch's host arrays stay valid until the return
@@ -2006,11 +2024,16 @@ extern "C" mp_status mp_realign_batch_into(mp_engine *e, const mp_model *m, cons
             st = failf(MP_ERR_CUDA, "event record failed");
         prevUploaded = db->evUploaded;
         if (st == MP_OK) st = runIssue(e, db);
+        // slices whose kernels have ended are finished at once (their tuples start to leave)
+        // rather than after the last slice is planned
+        while (st == MP_OK && finished < i && cudaEventQuery(e->pipe[finished % nSlots]->evStatus) == cudaSuccess)
+            st = finishNext();
     }
     while (st == MP_OK && finished < nSlices) st = finishNext();
     for (int k = 0; k < nSlots; k++) {
         cudaError_t ce = cudaStreamSynchronize(e->pipe[k]->stream);
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->pipe[k]->copyStream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->outStream);
         e->pipe[k]->copyPending = false;
         if (st == MP_OK && ce != cudaSuccess)
             st = failf(MP_ERR_CUDA, "pipelined pass failed: %s", cudaGetErrorString(ce));

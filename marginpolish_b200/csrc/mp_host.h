@@ -121,6 +121,7 @@ struct mp_engine {
     struct mp_device_batch *adjointShot = nullptr;  // reused by mp_expectations_batch
     static constexpr int kPipeSlots = 8;
     struct mp_device_batch *pipe[kPipeSlots] = {};  // the slots of mp_realign_batch_into (own streams)
+    cudaStream_t outStream = nullptr;  // tuple copies of mp_realign_batch_into's slots, in slice order
     std::mutex oneShotLock;
 };
 

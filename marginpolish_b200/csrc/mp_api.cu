@@ -11,6 +11,7 @@
 #include "mp_host.h"
 
 #include <sched.h>
+#include <time.h>
 
 #include <algorithm>
 #include <atomic>
@@ -644,11 +645,11 @@ struct mp_device_batch {
     }
 };
 
-// Waits until everything queued on `st` has run. The host thread polls an event and yields its
-// core between polls, instead of spinning in the runtime: callers that drive the engine from
-// many threads at once (the drop-in's OpenMP callers, each with its own engine) leave the
-// cores to the threads still planning and filling their calls, while a lone caller still
-// sees the end of its work within a scheduler tick.
+// Waits until everything queued on `st` has run. The host thread polls an event, yielding its
+// core for the first polls and then sleeping 20 us between them, instead of spinning in the
+// runtime: callers that drive the engine from as many threads as the host has cores (the
+// drop-in's OpenMP callers, each with its own engine) leave the cores to the threads still
+// planning and filling their calls, while a lone caller still sees its work end promptly.
 static cudaError_t waitStream(mp_device_batch *db, cudaStream_t st) {
     if (!db->evSync) {
         const cudaError_t e = cudaEventCreateWithFlags(&db->evSync, cudaEventDisableTiming);
@@ -656,7 +657,14 @@ static cudaError_t waitStream(mp_device_batch *db, cudaStream_t st) {
     }
     cudaError_t e = cudaEventRecord(db->evSync, st);
     if (e != cudaSuccess) return e;
-    while ((e = cudaEventQuery(db->evSync)) == cudaErrorNotReady) sched_yield();
+    for (int polls = 0; (e = cudaEventQuery(db->evSync)) == cudaErrorNotReady; polls++) {
+        if (polls < 32) {
+            sched_yield();
+        } else {
+            struct timespec ts = {0, 20000};
+            nanosleep(&ts, nullptr);
+        }
+    }
     return e;
 }
 
@@ -1879,7 +1887,8 @@ extern "C" mp_status mp_realign_batch(mp_engine *e, const mp_model *m, const mp_
     std::lock_guard<std::mutex> guard(e->oneShotLock);
     if (!e->oneShot) e->oneShot = new mp_device_batch();
     mp_device_batch *db = e->oneShot;
-    MP_TRY(batchReset(e, db, m, p, b));
+    // the input copies need no wait of their own: the call returns after its last wait
+    MP_TRY(batchReset(e, db, m, p, b, false));
     float ms = 0.0f;
     MP_TRY(mp_device_batch_run(e, db, &ms));
     MP_TRY(mp_device_batch_fetch(e, db, out));

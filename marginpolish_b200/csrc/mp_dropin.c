@@ -97,6 +97,15 @@ mp_status mpd_lower_state_machine(StateMachine *sM, mp_model_desc *d, double *re
     return MP_OK;
 }
 
+/* Each calling thread drives its own CUDA stream. CUDA maps streams onto a fixed number of
+ * hardware work queues (8 by default), so with more calling threads than queues, unrelated
+ * threads' kernels wait on one another. When the library is loaded -- before the host
+ * application has created its CUDA context -- it asks for 32 queues, unless the application's
+ * environment already sets CUDA_DEVICE_MAX_CONNECTIONS. */
+__attribute__((constructor)) static void mpdRaiseHardwareQueues(void) {
+    setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0);
+}
+
 /* ---------------- per-thread engine and lowered-machine cache ---------------- */
 
 /* The reference's callers run one chunk per OpenMP thread (marginPolish.c:436-439), each thread

@@ -11,6 +11,11 @@ if ROOT not in sys.path:
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
+# The drop-in library raises CUDA's hardware work queues to 32 when a host application loads it
+# before creating its CUDA context; this test process creates its context first, so it asks
+# for the same here, before any CUDA call.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs an sm_100 (B200) GPU")

@@ -182,7 +182,7 @@ def test_sixteen_calling_threads_fill_the_gpu(host, ref_oracle, exact_oracle, po
     z, hf, hr = _ref_models(ref_oracle)
     ap = polish_model.alignment
     bp = _params(ap)
-    wl = synth.config_batched(seed=5, n_chunks=16, chunk_len=6000, coverage=6)
+    wl = synth.config_batched(seed=5, n_chunks=16, chunk_len=6000, coverage=12)
     jobs = wl.jobs()
     reads = []
     for j in range(jobs.n_jobs):

@@ -326,60 +326,144 @@ def measure_adjoint(engine, model, pm):
             "form": "mp_expectations_batch, host arrays in / counts out (FP32 cells, FP64 accumulation)"}
 
 
-def measure_bubble_scoring(engine, model, pm, bubbles=2000, seed=61):
-    """The scoring step of bubble-graph polishing: every read substring of a bubble against
-    each of its candidate alleles, computeForwardProbability without anchors (the band of
-    band_construct over the whole pair), as one mp_forward_batch call. Synthetic bubbles:
-    2-4 alleles of 10-100 RLE symbols, 40 read substrings per bubble (the allele with
-    about 5% substitutions, run lengths 1-3)."""
+# FP64 adds and products of one cell of the bubble scorer with a switch-free model: three
+# incoming terms f + (e + t) of the match state, two of each gap state (2 operations each), the
+# run-length emission sum, and four approximate log-sums (a subtraction, a three-step cubic and
+# the final addition: 8 each)
+DP_OPS_PER_PAIR_CELL = 14 + 1 + 32
+
+
+def polish_workload():
+    """8 chunks of a homopolymer-enriched 10 kb template at 50x, reads of 3-9 kb with seeded
+    nanopore-like base qualities, drafts with 1% homopolymer-biased indels."""
+    from marginpolish_b200 import synth
+    wl = synth.config_polish(seed=41, n_chunks=8, chunk_len=10_000, coverage=50, read_len=(3000, 9000), hp_runs=True)
+    return wl, wl.qualities(41)
+
+
+def measure_bubble_scoring(engine, model, pm, cpu_sample=True):
+    """The scoring step of the polish step's bubble graphs (impl/bubbleGraph.c:905-955) on real
+    graphs: the first realignment of the polish workload, every chunk's bubble graph, then one
+    mp_forward_pairs launch over every (allele, distinct read substring) pair of every bubble,
+    in the reference's arithmetic (FP64 log cells, its approximate log-sum). The reference's own
+    bubbleGraph_constructFromPoa, which computes the same scores one pair at a time, is timed
+    on a sample chunk on one core."""
+    import ctypes
+
     import numpy as np
-    from marginpolish_b200 import Jobs, forward_batch
-    rng = np.random.default_rng(seed)
-    xs, ys, xb, xe, yo, st = [], [], [], [], [0], []
-    x_at, y_at = 0, 0
-    for _ in range(bubbles):
-        n_al = int(rng.integers(2, 5))
-        length = int(rng.integers(10, 101))
-        base = rng.integers(0, 4, size=length)
-        alleles = []
-        for _ in range(n_al):
-            a = base.copy()
-            flip = rng.random(length) < 0.03
-            a[flip] = rng.integers(0, 4, size=int(flip.sum()))
-            sym = ((rng.integers(1, 4, size=length) << 8) | a).astype(np.uint16)
-            alleles.append(sym)
-        for _ in range(40):
-            r = base.copy()
-            flip = rng.random(length) < 0.05
-            r[flip] = rng.integers(0, 4, size=int(flip.sum()))
-            rsym = ((rng.integers(1, 4, size=length) << 8) | r).astype(np.uint16)
-            strand = int(rng.integers(0, 2))
-            for a in alleles:
-                xs.append(a)
-                xb.append(x_at)
-                x_at += a.size
-                xe.append(x_at)
-                ys.append(rsym)
-                y_at += rsym.size
-                yo.append(y_at)
-                st.append(strand)
-    n = len(xb)
-    jobs = Jobs(np.concatenate(xs), np.array(xb, np.int64), np.array(xe, np.int64), np.concatenate(ys),
-                np.array(yo, np.int64), np.zeros((0, 3), np.int32), np.zeros(n + 1, np.int64),
-                np.array(st, np.uint8), None, None, None)
-    forward_batch(engine, model, pm.alignment, jobs)  # warm
-    ts = []
-    for _ in range(3):
+    from marginpolish_b200 import PoaSet, PolishParams, _lib, forward_pairs_timing
+    wl, quals = polish_workload()
+    s = PoaSet.from_polish_model(engine, model, pm, PolishParams.shipped(), wl.drafts, wl.reads, wl.strands,
+                                 wl.anchors, quals)
+    s.realign()
+    t = time.perf_counter()
+    s.build_bubbles()
+    build_s = time.perf_counter() - t
+    s.score_bubbles()  # warm
+    calls, kernels = [], []
+    for _ in range(5):
         t = time.perf_counter()
-        lp = forward_batch(engine, model, pm.alignment, jobs)
-        ts.append(time.perf_counter() - t)
-    t = float(np.median(ts))
-    lx = np.array(xe) - np.array(xb)
-    ly = np.diff(np.array(yo))
-    return {"workload": f"{bubbles} bubbles x 2-4 alleles of 10-100 RLE symbols x 40 read substrings",
-            "pairs": n, "matrix_cells": int(np.sum((lx + 1) * (ly + 1))), "seconds": t, "pairs_per_s": n / t,
-            "all_finite": bool(np.all(np.isfinite(lp))),
-            "form": "mp_forward_batch: host arrays in, ln P per pair out (FP64 forward-only variants)"}
+        s.score_bubbles()
+        calls.append(time.perf_counter() - t)
+        kernels.append(forward_pairs_timing(engine)["kernel_ms"])
+    tm = forward_pairs_timing(engine)
+    n_bubbles = sum(len(s.bubbles(c)) for c in range(s.n_chunks))
+    s.close()
+    g = ctypes.c_double(0.0)
+    _lib.check(engine._lib.mp_measure_fp64_peak(engine.handle, ctypes.byref(g)))
+    k_ms = float(np.median(kernels))
+    call_s = float(np.median(calls))
+    achieved = tm["cells"] * DP_OPS_PER_PAIR_CELL / (k_ms * 1e-3) / 1e9
+    out = {"workload": "bubble graphs of 8 chunks x 10 kb (homopolymer-enriched), 50x, reads of 3-9 kb with base "
+                       "qualities, drafts with 1% homopolymer-biased indels",
+           "bubbles": n_bubbles, "pairs": tm["pairs"], "cells": tm["cells"], "kernel_ms": k_ms,
+           "call_ms": call_s * 1e3, "gcups_kernel": tm["cells"] / (k_ms * 1e-3) / 1e9,
+           "gcups_call": tm["cells"] / call_s / 1e9, "pairs_per_s": tm["pairs"] / call_s,
+           "build_ms": build_s * 1e3,
+           "roofline": {"bound": "fp64", "achieved": achieved, "peak": g.value, "unit": "G FP64 ops/s",
+                        "frac": achieved / g.value,
+                        "note": f"{DP_OPS_PER_PAIR_CELL} FP64 adds/products per cell x cells / kernel event time; "
+                                "peak = FP64 add/product issue rate measured live (mp_measure_fp64_peak)"},
+           "form": "mp_poa_set_score_bubbles -> mp_forward_pairs: one thread per pair, reference arithmetic, "
+                   "bit-identical scores"}
+    if cpu_sample:
+        out["cpu_reference"] = reference_bubble_sample(pm)
+    return out
+
+
+def reference_bubble_sample(pm):
+    """The reference's bubbleGraph_constructFromPoa (oracle/_ref/libref_poa.so, one core) on the
+    graph of one 3 kb chunk at 50x: seconds, and its rate over the pairs it scores."""
+    import os as _os
+
+    import numpy as np
+    from marginpolish_b200 import PolishParams, synth
+    from oracle.bindings import RefPoaOracle, available_reference_poa
+    if not available_reference_poa():
+        return {"unavailable": "reference POA build (oracle/_ref/libref_poa.so) not present"}
+    ref = RefPoaOracle()
+    z = np.load(_os.path.join(ROOT, "tests", "golden", "model_np.npz"))
+    hf = ref.model(int(z["hmm_type"]), z["transitions"], z["emissions"], False, z["repeat_log10"], 1)
+    hr = ref.model(int(z["hmm_type"]), z["transitions"], z["emissions"], True, z["repeat_log10"], 0)
+    wl = synth.config_polish(seed=9, n_chunks=1, chunk_len=3000, coverage=50, read_len=(1500, 2500), hp_runs=True)
+    quals = wl.qualities(9)
+    pp = PolishParams.shipped()
+    params_h = ref.params(hf, hr, pm.alignment, max_iterations=0)
+    ref.set_polish(params_h, pp)
+    reads_h = ref.reads(wl.reads[0], wl.strands[0])
+    ref.set_qualities(reads_h, quals[0])
+    anchors_h = ref.anchors(wl.anchors[0])
+    poa = ref.realign(reads_h, anchors_h, wl.drafts[0], params_h)
+    t = time.perf_counter()
+    g = ref.bubble_graph(poa, reads_h, params_h)
+    sec = time.perf_counter() - t
+    cells = pairs = 0
+    for b in g["bubbles"]:
+        seen = set()
+        for read, start, length in b["reads"].tolist():
+            r = wl.reads[0][read]
+            key = (r.chars[start:start + length], tuple(int(v) for v in r.counts[start:start + length]))
+            if key in seen:
+                continue
+            seen.add(key)
+            for chars, _ in b["alleles"]:
+                cells += (len(chars) + 1) * (length + 1)
+                pairs += 1
+    ref.free_poa(poa)
+    ref.free_anchors(anchors_h)
+    ref.free_reads(reads_h)
+    ref.free_params(params_h)
+    ref.free_model(hf)
+    ref.free_model(hr)
+    return {"seconds": sec, "bubbles": len(g["bubbles"]), "pairs": pairs, "cells": cells,
+            "gcups": cells / sec / 1e9, "cores": 1, "kind": "reference",
+            "sample": "bubbleGraph_constructFromPoa (construction and scores) on one 3 kb chunk at 50x, one core"}
+
+
+def measure_polish_shipped(engine, model, pm):
+    """The shipped loop (poa_realignAll with one polish iteration, then the run-length estimate)
+    over the polish workload: realignment, bubble graphs, scores, new consensus, anchors,
+    second realignment."""
+    from marginpolish_b200 import PoaSet, PolishParams
+    wl, quals = polish_workload()
+    best = None
+    for _ in range(2):
+        s = PoaSet.from_polish_model(engine, model, pm, PolishParams.shipped(), wl.drafts, wl.reads, wl.strands,
+                                     wl.anchors, quals)
+        t0 = time.perf_counter()
+        s.realign_all()
+        s.estimate_repeat_counts()
+        t1 = time.perf_counter()
+        changed = sum(int(s.reference(c).chars != wl.drafts[c].chars) for c in range(s.n_chunks))
+        s.close()
+        if best is None or t1 - t0 < best["seconds"]:
+            best = {"seconds": t1 - t0, "chunks_changed": changed}
+    best.update({"workload": "8 chunks x 10 kb (homopolymer-enriched), 50x, reads of 3-9 kb with base qualities, "
+                             "drafts with 1% homopolymer-biased indels; no consensus iterations, one polish "
+                             "iteration (params/allParams.np.json)",
+                 "reads": int(sum(len(r) for r in wl.reads)),
+                 "bases": int(sum(r.non_rle_length for lst in wl.reads for r in lst))})
+    return best
 
 
 def measure_polish(engine, model, pm):
@@ -665,7 +749,8 @@ def run_ours(args, rank, world, local):
     if not args.no_extras and rank == 0:
         extras["adjoint"] = measure_adjoint(engine, model, pm)
         extras["polish_loop"] = measure_polish(engine, model, pm)
-        extras["bubble_scoring"] = measure_bubble_scoring(engine, model, pm)
+        extras["bubble_scoring"] = measure_bubble_scoring(engine, model, pm, cpu_sample=not args.no_cpu)
+        extras["polish_loop_shipped"] = measure_polish_shipped(engine, model, pm)
     peak = engine.fp32_peak_tflops()
     if not args.no_scale and rank == 0 and world == 1 and args.config == "batched":
         # the larger configurations need the device memory the headline's buffers hold

@@ -261,6 +261,9 @@ mp_status mp_device_batch_run_plain(mp_engine *e, mp_device_batch *db, int64_t m
  * (TFLOP/s, FMA = 2 flops), timed with CUDA events; the roofline denominator of the
  * posterior kernel, whose bound is the FP32 pipe. */
 mp_status mp_measure_fp32_peak(mp_engine *e, double *tflops);
+/* FP64 add / multiply issue rate of the device (G operations/s, one per instruction), measured
+ * the same way; the roofline denominator of the bubble scorer, built of such operations. */
+mp_status mp_measure_fp64_peak(mp_engine *e, double *gops);
 
 /* ---- geometry helpers (host, integer-exact restatements used by the planner) ---- */
 /* Band of one sub-problem: (xay, xmyL, xmyR) for d = 0..lX+lY into out[3*(lX+lY+1)]. */
@@ -285,6 +288,35 @@ mp_status mp_crop_range(const int32_t *anchors, int64_t n_anchors, int64_t templ
  * callers (impl/bubbleGraph.c:924) pass no anchors: the band is then the whole matrix. */
 mp_status mp_forward_batch(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
                            double *log_prob);
+
+/* ---- bubble scoring: computeForwardProbability (impl/pairwiseAligner.c:813-865) as the
+ * bubble graph calls it (impl/bubbleGraph.c:924: no anchors, no ragged ends), in the
+ * reference's own arithmetic ----
+ * Pair j aligns X = x_symbols[x_offset[j] .. + x_length[j]) (an allele) against
+ * Y = y_symbols[y_offset[j] .. + y_length[j]) (a read substring) with the forward (strand[j]
+ * = 1) or reverse model; pairs may share symbols. log_prob[j] gets the forward log
+ * probability over the whole matrix computed as the reference computes it: FP64 log-space
+ * cells, its approximate log-sum (impl/pairwiseAligner.c:279-299) and its operation order, so
+ * the value equals the reference's bit for bit. x_length + y_length = 0 gives 0 (LOG_ONE).
+ * Run lengths in the symbols must be below the model's table (51), as rleString_
+ * constructSymbolString clamps them; otherwise MP_ERR_ARGUMENT. */
+typedef struct {
+    int64_t n_pairs;
+    const int64_t *x_offset;
+    const int32_t *x_length;
+    const int64_t *y_offset;
+    const int32_t *y_length;
+    const uint8_t *strand;
+    int64_t x_symbols_length;
+    const uint16_t *x_symbols;
+    int64_t y_symbols_length;
+    const uint16_t *y_symbols;
+} mp_pair_batch;
+
+mp_status mp_forward_pairs(mp_engine *e, const mp_model *m, const mp_pair_batch *b, double *log_prob);
+/* The last mp_forward_pairs call of the engine: device time of its launches (CUDA events on the
+ * engine's stream), its matrix cells (sum of (x_length + 1) (y_length + 1)) and its pairs. */
+mp_status mp_forward_pairs_timing(mp_engine *e, float *kernel_ms, int64_t *cells, int64_t *pairs);
 
 /* ---- adjoint: expected counts = gradient of the summed log-likelihood ----
  * For the FP32 scaled-probability DP over each job's band (the posterior pass's band,
@@ -337,6 +369,17 @@ typedef struct {
     int64_t n_anchor_probs;
     int64_t min_iterations;          /* minPoaConsensusIterations */
     int64_t max_iterations;          /* maxPoaConsensusIterations */
+    /* polish mode (poa_polish, impl/polisher.c:2008-2031; the bubble graph of
+     * impl/bubbleGraph.c:800-978), run by mp_poa_set_realign_all after the consensus iterations */
+    int64_t min_polish_iterations;   /* minRealignmentPolishIterations (1 shipped) */
+    int64_t max_polish_iterations;   /* maxRealignmentPolishIterations (1 shipped; 0: no polish mode) */
+    int32_t use_read_alleles;        /* useReadAlleles: alleles are the reads' substrings (1 shipped; the
+                                        other allele source is not built: 0 is refused when polishing) */
+    int32_t reserved;
+    double candidate_variant_weight; /* candidateVariantWeight (0.18 shipped) */
+    int64_t column_anchor_trim;      /* columnAnchorTrim (5 shipped) */
+    int64_t filter_reads_coverage;   /* filterReadsWhileHaveAtLeastThisCoverage (15 shipped) */
+    double min_avg_base_quality;     /* minAvgBaseQuality (10 shipped) */
 } mp_polish_params;
 
 /* Chunks and reads in HOST memory. Chunk c's draft is runs [ref_offsets[c], ref_offsets[c+1])
@@ -357,6 +400,9 @@ typedef struct {
     const uint8_t *strand;            /* per read, 1 forward */
     const int64_t *anchor_offsets;
     const int32_t *anchors;
+    const uint8_t *read_qualities;    /* per read run, laid out like read_chars (the run-length form
+                                         of rleString_rleQualities, impl/polisher.c:1692-1714); NULL:
+                                         reads without qualities */
 } mp_polish_batch;
 
 typedef struct mp_poa_set mp_poa_set;
@@ -384,8 +430,32 @@ mp_status mp_poa_set_realign(mp_poa_set *s);
 mp_status mp_poa_set_realign_pairs(mp_poa_set *s, const int64_t *const pair_offsets[3], const int64_t *const pairs[3]);
 /* poa_realignIterative in consensus mode for every chunk (after mp_poa_set_realign). */
 mp_status mp_poa_set_iterate(mp_poa_set *s);
-/* poa_realignAll in consensus mode: realign, then iterate. */
+/* poa_realignIterative in polish mode (poa_polish) for every chunk: each iteration builds every
+ * chunk's bubble graph on host threads and scores all of them in one GPU launch
+ * (mp_forward_pairs). */
+mp_status mp_poa_set_iterate_polish(mp_poa_set *s);
+/* poa_realignAll (impl/polisher.c:2109-2129): realign, the consensus iterations when
+ * max_iterations > 0, then the polish iterations when max_polish_iterations > 0. */
 mp_status mp_poa_set_realign_all(mp_poa_set *s);
+/* The steps of one polish iteration, for inspection: bubbleGraph_constructFromPoa on every
+ * chunk's current graph without the scores (it sorts each node's observations by read and
+ * descending weight, as the reference does), then the scores of all chunks in one launch. */
+mp_status mp_poa_set_build_bubbles(mp_poa_set *s);
+mp_status mp_poa_set_score_bubbles(mp_poa_set *s);
+/* sizes[4]: bubbles, alleles, allele runs and read substrings of a chunk's bubble graph. */
+mp_status mp_poa_bubble_sizes(const mp_poa_set *s, int64_t chunk, int64_t sizes[4]);
+/* The graph: per bubble six values (reference start, reference allele runs, first allele,
+ * alleles, first read substring, read substrings); per allele its run count, its runs laid end
+ * to end (chars, counts); per read substring (read index in the chunk, start run, runs) and its
+ * mean quality (-1 without qualities); the supports, per bubble alleles x reads (allele-major),
+ * bubbles in order (zeros before mp_poa_set_score_bubbles). Any output may be NULL. */
+mp_status mp_poa_bubbles(const mp_poa_set *s, int64_t chunk, int64_t *bubbles, int64_t *allele_runs, char *chars,
+                         uint64_t *counts, int64_t *reads, double *quals, float *supports);
+/* bubbleGraph_getConsensusPath and bubbleGraph_getConsensusString of a scored graph: the
+ * chosen allele per bubble, the new consensus (at most cap runs; *n_runs its length) and the
+ * map from the graph's reference runs to the consensus runs (-1: none). */
+mp_status mp_poa_bubble_consensus(const mp_poa_set *s, int64_t chunk, int64_t *path, char *chars, uint64_t *counts,
+                                  int64_t cap, int64_t *n_runs, int64_t *map);
 /* poa_estimateRepeatCountsUsingBayesianModel on every chunk's graph (sets the run lengths of
  * its reference string, as the caller of poa_realignAll does, marginPolish.c:558). */
 mp_status mp_poa_set_estimate_repeat_counts(mp_poa_set *s);

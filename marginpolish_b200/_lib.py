@@ -145,6 +145,14 @@ class PolishParamsC(Structure):
         ("n_anchor_probs", c_int64),
         ("min_iterations", c_int64),
         ("max_iterations", c_int64),
+        ("min_polish_iterations", c_int64),
+        ("max_polish_iterations", c_int64),
+        ("use_read_alleles", c_int32),
+        ("reserved", c_int32),
+        ("candidate_variant_weight", c_double),
+        ("column_anchor_trim", c_int64),
+        ("filter_reads_coverage", c_int64),
+        ("min_avg_base_quality", c_double),
     ]
 
 
@@ -161,6 +169,22 @@ class PolishBatch(Structure):
         ("strand", POINTER(c_uint8)),
         ("anchor_offsets", POINTER(c_int64)),
         ("anchors", POINTER(c_int32)),
+        ("read_qualities", POINTER(c_uint8)),
+    ]
+
+
+class PairBatch(Structure):
+    _fields_ = [
+        ("n_pairs", c_int64),
+        ("x_offset", POINTER(c_int64)),
+        ("x_length", POINTER(c_int32)),
+        ("y_offset", POINTER(c_int64)),
+        ("y_length", POINTER(c_int32)),
+        ("strand", POINTER(c_uint8)),
+        ("x_symbols_length", c_int64),
+        ("x_symbols", POINTER(c_uint16)),
+        ("y_symbols_length", c_int64),
+        ("y_symbols", POINTER(c_uint16)),
     ]
 
 
@@ -205,7 +229,9 @@ EXPORTED = [
     "mp_poa_set_realign_all", "mp_poa_set_estimate_repeat_counts", "mp_poa_info", "mp_poa_nodes",
     "mp_poa_observations", "mp_poa_inserts", "mp_poa_deletes", "mp_poa_reference", "mp_poa_consensus",
     "mp_poa_anchor_alignments", "mp_engine_autotune", "mp_engine_autotune_reset",
-    "mp_engine_set_graph_capture", "mp_realign_batch_into", "mp_engine_release_buffers",
+    "mp_engine_set_graph_capture", "mp_realign_batch_into", "mp_engine_release_buffers", "mp_forward_pairs",
+    "mp_forward_pairs_timing", "mp_measure_fp64_peak", "mp_poa_set_iterate_polish", "mp_poa_set_build_bubbles", "mp_poa_set_score_bubbles", "mp_poa_bubble_sizes",
+    "mp_poa_bubbles", "mp_poa_bubble_consensus",
 ]
 
 _lib = None
@@ -252,6 +278,7 @@ def load() -> ctypes.CDLL:
         "mp_device_batch_run_plain": (c_int, [c_void_p, c_void_p, c_int64, P(c_float), P(c_int64)]),
         "mp_device_batch_timing": (c_int, [c_void_p, P(c_float), P(c_float)]),
         "mp_measure_fp32_peak": (c_int, [c_void_p, P(c_double)]),
+        "mp_measure_fp64_peak": (c_int, [c_void_p, P(c_double)]),
         "mp_realign_single_noalloc": (c_int, [c_void_p, c_void_p, P(Params), P(c_uint16), c_int64, P(c_uint16),
                                               c_int64, P(c_int32), c_int64, c_int, c_int, c_int, P(NoallocOutput)]),
         "mp_forward_batch": (c_int, [c_void_p, c_void_p, P(Params), P(Batch), P(c_double)]),
@@ -262,6 +289,16 @@ def load() -> ctypes.CDLL:
         "mp_poa_set_realign": (c_int, [c_void_p]),
         "mp_poa_set_realign_pairs": (c_int, [c_void_p, P(P(c_int64)), P(P(c_int64))]),
         "mp_poa_set_iterate": (c_int, [c_void_p]),
+        "mp_poa_set_iterate_polish": (c_int, [c_void_p]),
+        "mp_poa_set_build_bubbles": (c_int, [c_void_p]),
+        "mp_poa_set_score_bubbles": (c_int, [c_void_p]),
+        "mp_poa_bubble_sizes": (c_int, [c_void_p, c_int64, P(c_int64)]),
+        "mp_poa_bubbles": (c_int, [c_void_p, c_int64, P(c_int64), P(c_int64), P(c_char), P(ctypes.c_uint64),
+                                   P(c_int64), P(c_double), P(c_float)]),
+        "mp_poa_bubble_consensus": (c_int, [c_void_p, c_int64, P(c_int64), P(c_char), P(ctypes.c_uint64), c_int64,
+                                            P(c_int64), P(c_int64)]),
+        "mp_forward_pairs": (c_int, [c_void_p, c_void_p, P(PairBatch), P(c_double)]),
+        "mp_forward_pairs_timing": (c_int, [c_void_p, P(c_float), P(c_int64), P(c_int64)]),
         "mp_poa_set_realign_all": (c_int, [c_void_p]),
         "mp_poa_set_estimate_repeat_counts": (c_int, [c_void_p]),
         "mp_poa_info": (c_int, [c_void_p, c_int64, P(PoaChunkInfo)]),

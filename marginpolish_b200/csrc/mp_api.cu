@@ -240,12 +240,21 @@ extern "C" mp_status mp_model_create(mp_engine *e, const mp_model_desc *fwd, con
         m->sharedRepeat = memcmp(rp.data(), rp.data() + kRepTable, sizeof(float) * kRepTable) == 0 ? 1 : 0;
         m->noSwitch = (m->host[0].t[1 * 3 + 2] == 0.0f && m->host[0].t[2 * 3 + 1] == 0.0f &&
                        m->host[1].t[1 * 3 + 2] == 0.0f && m->host[1].t[2 * 3 + 1] == 0.0f) ? 1 : 0;
+        std::vector<double> lrp(2 * kRepTable);
+        mp_model_lower_log(fwd, m->logHost[0], lrp.data());
+        mp_model_lower_log(rev, m->logHost[1], lrp.data() + kRepTable);
         cudaSetDevice(e->device);
         s = m->models.reserve(sizeof(DevModel) * 2);
         if (s == MP_OK) s = m->repeat.reserve(sizeof(float) * 2 * kRepTable);
+        if (s == MP_OK) s = m->logModels.reserve(sizeof(mp::DevLogModel) * 2);
+        if (s == MP_OK) s = m->logRepeat.reserve(sizeof(double) * 2 * kRepTable);
         if (s == MP_OK) {
             cudaError_t ce = cudaMemcpy(m->models.p, m->host, sizeof(DevModel) * 2, cudaMemcpyHostToDevice);
             if (ce == cudaSuccess) ce = cudaMemcpy(m->repeat.p, rp.data(), sizeof(float) * 2 * kRepTable, cudaMemcpyHostToDevice);
+            if (ce == cudaSuccess)
+                ce = cudaMemcpy(m->logModels.p, m->logHost, sizeof(mp::DevLogModel) * 2, cudaMemcpyHostToDevice);
+            if (ce == cudaSuccess)
+                ce = cudaMemcpy(m->logRepeat.p, lrp.data(), sizeof(double) * 2 * kRepTable, cudaMemcpyHostToDevice);
             if (ce != cudaSuccess) s = failf(MP_ERR_CUDA, "model upload failed: %s", cudaGetErrorString(ce));
         }
     }
@@ -1465,6 +1474,7 @@ extern "C" mp_status mp_device_batch_timing(const mp_device_batch *db, float *ba
 
 namespace mp {
 cudaError_t launchFmaProbe(float *out, int blocks, int threads, int iters, cudaStream_t s);
+cudaError_t launchDpProbe(double *out, int blocks, int threads, int iters, cudaStream_t s);
 }
 
 extern "C" mp_status mp_measure_fp32_peak(mp_engine *e, double *tflops) {
@@ -1489,6 +1499,30 @@ extern "C" mp_status mp_measure_fp32_peak(mp_engine *e, double *tflops) {
     // 16 independent FMA chains per thread, `iters` rounds each
     double flops = 2.0 * 16.0 * iters * (double) blocks * threads;
     *tflops = flops / (best * 1e-3) / 1e12;
+    return MP_OK;
+}
+
+extern "C" mp_status mp_measure_fp64_peak(mp_engine *e, double *gops) {
+    if (!e || !gops) return failf(MP_ERR_ARGUMENT, "mp_measure_fp64_peak: NULL argument");
+    CUDA_TRY(cudaSetDevice(e->device));
+    DevBuf out;
+    const int threads = 256, blocksPerSm = 4, iters = 1024;
+    const int blocks = e->smCount * blocksPerSm;
+    MP_TRY(out.reserve(sizeof(double) * blocks * threads));
+    cudaStream_t st = e->stream;
+    for (int w = 0; w < 3; w++) CUDA_TRY(launchDpProbe(out.as<double>(), blocks, threads, iters, st));
+    float best = 1e30f;
+    for (int r = 0; r < 5; r++) {
+        CUDA_TRY(cudaEventRecord(e->ev0, st));
+        CUDA_TRY(launchDpProbe(out.as<double>(), blocks, threads, iters, st));
+        CUDA_TRY(cudaEventRecord(e->ev1, st));
+        CUDA_TRY(cudaEventSynchronize(e->ev1));
+        float ms = 0.0f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+        best = std::min(best, ms);
+    }
+    const double ops = 16.0 * iters * (double) blocks * threads;
+    *gops = ops / (best * 1e-3) / 1e9;
     return MP_OK;
 }
 

@@ -100,6 +100,22 @@ struct PinBuf {
 // engine and model
 // ---------------------------------------------------------------------------
 
+// Device arrays of mp_forward_pairs (grow only).
+struct mp_pair_scratch {
+    DevBuf idx, xOff, yOff, xLen, yLen, strand, xs, ys, out, rowOff, rows;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    float kernelMs = 0.0f;  // device time of the last call's launches
+    int64_t cells = 0;      // matrix cells of the last call: sum of (lx + 1) (ly + 1)
+    int64_t pairs = 0;
+    mp_pair_scratch() = default;
+    mp_pair_scratch(const mp_pair_scratch &) = delete;
+    mp_pair_scratch &operator=(const mp_pair_scratch &) = delete;
+    ~mp_pair_scratch() {
+        for (cudaEvent_t x : ev)
+            if (x) cudaEventDestroy(x);
+    }
+};
+
 struct mp_engine {
     int device = 0;
     int smCount = 0;
@@ -122,6 +138,7 @@ struct mp_engine {
     static constexpr int kPipeSlots = 8;
     struct mp_device_batch *pipe[kPipeSlots] = {};  // the slots of mp_realign_batch_into (own streams)
     cudaStream_t outStream = nullptr;  // tuple copies of mp_realign_batch_into's slots, in slice order
+    mp_pair_scratch pairScratch;       // mp_forward_pairs (under oneShotLock)
     std::mutex oneShotLock;
 };
 
@@ -133,5 +150,12 @@ struct mp_model {
     double logT[2][9];   // log transitions as given (the adjoint scales its sums by exp(logT))
     DevBuf models;   // DevModel[2]
     DevBuf repeat;   // float [2][kRepTable]
+    // FP64 log-space copy for the bubble scorer (mp_forward_pairs)
+    mp::DevLogModel logHost[2];
+    DevBuf logModels;  // DevLogModel[2]
+    DevBuf logRepeat;  // double [2][kRepTable]: repeat_scale * log10 table
 };
+
+// Fills the FP64 log-space tables of one strand's model (defined in mp_bubble.cu).
+mp_status mp_model_lower_log(const mp_model_desc *d, mp::DevLogModel &m, double *rep);
 

@@ -26,6 +26,38 @@ struct DevModel {
     int32_t pad[2];
 };
 
+// Log-space state machine of one read strand in FP64, the values the reference's cells use
+// (the bubble scorer reproduces the reference's arithmetic on them).
+struct DevLogModel {
+    double t[9];           // log transitions from*3+to
+    double start[3];
+    double raggedStart[3];
+    double end[3];
+    double raggedEnd[3];
+    double match[25];      // log match emissions [xbase*5 + ybase]
+    double gapX[5];
+    double gapY[5];
+    int32_t runLength;
+    int32_t strand;
+    int32_t noSwitch;      // both switch transitions (gap-x <-> gap-y) are log 0
+    int32_t pad;
+};
+
+// Bubble-scoring launch: one thread per (allele, read substring) pair of a length class.
+struct PairArgs {
+    const int32_t *pairs;       // pair indices of this launch (a length class)
+    int32_t nPairs;
+    const int64_t *xOff, *yOff;
+    const int32_t *xLen, *yLen;
+    const uint8_t *strand;
+    const uint16_t *xs, *ys;
+    const DevLogModel *models;  // [0] forward strand, [1] reverse strand
+    const double *repeatLog;    // [2][kRepTable] repeat_scale * log10 table, per model
+    double *rows;               // generic class only: one row of 3 (lx+1) doubles per pair
+    const int64_t *rowOff;      // generic class only: each pair's row (in doubles)
+    double *out;                // ln P per pair (indexed by pair)
+};
+
 // One banded sub-problem (one split rectangle of one job).
 struct Task {
     int64_t xOff;          // first X symbol of the sub-problem (device symbol buffer index)

@@ -196,6 +196,28 @@ cudaError_t launchFmaProbe(float *out, int blocks, int threads, int iters, cudaS
     return cudaGetLastError();
 }
 
+// FP64 issue rate: 16 independent chains of separately rounded adds and products per thread
+// (the operations the bubble scorer is made of).
+__global__ void dpProbeKernel(double *out, int iters) {
+    double a[16];
+    const double m = 1.0000001, c = 1e-7;
+#pragma unroll
+    for (int k = 0; k < 16; k++) a[k] = (double) (threadIdx.x + k) * 1e-3;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 16; k++) a[k] = (k & 1) ? __dmul_rn(a[k], m) : __dadd_rn(a[k], c);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 16; k++) s += a[k];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+cudaError_t launchDpProbe(double *out, int blocks, int threads, int iters, cudaStream_t s) {
+    dpProbeKernel<<<blocks, threads, 0, s>>>(out, iters);
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // Host-side launch wrappers
 // ---------------------------------------------------------------------------

@@ -678,6 +678,331 @@ void estimateRepeatCounts(Poa &poa, const std::vector<Rle> &reads, const std::ve
     }
 }
 
+// ---------------------------------------------------------------------------
+// bubble graph of the polish step (poa_polish, impl/polisher.c:2008-2031, and
+// bubbleGraph_constructFromPoa, impl/bubbleGraph.c:415-978)
+// ---------------------------------------------------------------------------
+
+struct ReadSub {  // bamChunkRead_getSubstring (impl/bubbleGraph.c:415-438)
+    int64_t read;    // read index within the chunk
+    int64_t start, length;
+    double qual;     // mean quality of the substring's runs, -1 without qualities
+};
+
+struct Bubble {
+    int64_t refStart, refLength;    // reference allele: runs [refStart, refStart + refLength)
+    int64_t alleleFirst, nAlleles;  // into BubbleGraph::alleles
+    int64_t readFirst, nReads;      // into BubbleGraph::reads, in the bubble's order
+    int64_t supportFirst;           // nAlleles x nReads log-likelihoods, allele-major
+};
+
+struct BubbleGraph {
+    std::vector<Bubble> bubbles;
+    std::vector<Rle> alleles;
+    std::vector<ReadSub> reads;
+    std::vector<int32_t> scoreFrom;  // per read: the earlier read of the bubble with an equal
+                                     // substring whose scores it shares (itself when scored)
+    std::vector<float> supports;
+    bool scored = false;
+};
+
+double totalWeight(const Node &n) {
+    double t = 0.0;
+    for (int k = 0; k < 5; k++) t += n.bw[k];
+    return t;
+}
+
+// getCandidateWeights (impl/bubbleGraph.c:583-612): a fraction of the coverage averaged over a
+// window of 100 nodes.
+std::vector<double> candidateWeights(const Poa &poa, double fraction) {
+    const int64_t n = (int64_t) poa.nodes.size(), window = 100;
+    std::vector<double> w((size_t) n, 0.0);
+    if (window >= n) {
+        double avg = 0.0;
+        for (int64_t j = 0; j < n; j++) avg += totalWeight(poa.nodes[j]);
+        avg /= (double) n;
+        std::fill(w.begin(), w.end(), avg * fraction);
+        return w;
+    }
+    double total = 0.0;
+    for (int64_t i = 0; i < n; i++) {
+        total += totalWeight(poa.nodes[i]);
+        if (i >= window) {
+            total -= totalWeight(poa.nodes[i - window]);
+            w[i - window / 2] = total / (double) window * fraction;
+        }
+    }
+    for (int64_t i = 0; i < window / 2; i++) {
+        w[i] = w[window / 2];
+        w[n - 1 - i] = w[n - 1 - window / 2];
+    }
+    return w;
+}
+
+// getFilteredAnchorPositions (impl/bubbleGraph.c:614-695): nodes away from every candidate
+// variant (a base or run length other than the node's, an insert, or a delete start, with more
+// than the candidate weight; repeat counts need twice the weight) by columnAnchorTrim.
+std::vector<uint8_t> anchorPositions(const Poa &poa, const std::vector<double> &cw, int64_t trim) {
+    const int64_t n = (int64_t) poa.nodes.size();
+    std::vector<uint8_t> variant((size_t) n, 0);
+    for (int64_t i = 0; i < n; i++) {
+        const Node &node = poa.nodes[i];
+        const double w = cw[i];
+        bool v = false;
+        for (int k = 0; k < 5 && !v; k++) {  // hasCandidateSubstitution (:231-244)
+            const char base = charOf(k);
+            if ((node.bw[k] > w || node.base == base) && base != node.base) v = true;
+        }
+        const double *rcw = poa.rcwOf(i);
+        for (uint64_t rc = 0; rc < poa.maxRC && !v; rc++)  // hasCandidateRepeatCountChange (:246-259)
+            if ((rcw[rc] > 2.0 * w || node.rc == rc) && rc != node.rc) v = true;
+        for (size_t k = 0; k < node.ins.size() && !v; k++)  // hasCandidateInsert (:274-280)
+            if (node.ins[k].weight() > w) v = true;
+        if (v) variant[i] = 1;
+        // maxCandidateDeleteLength is declared bool (:295), so a candidate delete marks the node
+        // and the one after it, whatever its length
+        bool del = false;
+        for (const Delete &d : node.del)
+            if (d.weight() > w && d.len > 0) del = true;
+        if (del) {
+            variant[i] = 1;
+            if (i + 1 < n) variant[i + 1] = 1;
+        }
+    }
+    // expand (:647-664): [i - trim, i + trim) around every variant node
+    std::vector<uint8_t> anchor((size_t) n, 1);
+    for (int64_t i = 0; i < n; i++)
+        if (variant[i])
+            for (int64_t j = std::max<int64_t>(i - trim, 0); j < std::min<int64_t>(i + trim, n); j++) anchor[j] = 0;
+    return anchor;
+}
+
+// sortBaseObservations (:448-468): each node's observations by read, then by descending
+// weight. The reference sorts with qsort, a stable merge sort in glibc; the graph keeps the
+// new order (the anchor alignments made from it afterwards read it).
+void sortObservations(Poa &poa) {
+    for (size_t i = 0; i + 1 < poa.obsStart.size(); i++)
+        std::stable_sort(poa.obs.begin() + poa.obsStart[i], poa.obs.begin() + poa.obsStart[i + 1],
+                         [](const Obs &a, const Obs &b) {
+                             if (a.read != b.read) return a.read < b.read;
+                             return a.weight > b.weight;
+                         });
+}
+
+// getReadSubstrings (:508-581) for 0 < from < to < nodes: the runs of every read that has
+// observations at both nodes (its first, heaviest one at each), from the one at `from` up to the
+// one at `to`; then filterReadSubstrings (:491-506).
+void readSubstrings(const Poa &poa, int64_t from, int64_t to, const std::vector<std::vector<uint8_t>> *quals,
+                    int64_t readBase, int64_t keepAtLeast, double minQual, std::vector<ReadSub> &out) {
+    out.clear();
+    const Obs *f = poa.obsBegin(from), *fe = poa.obsEnd(from);
+    const Obs *t = poa.obsBegin(to), *te = poa.obsEnd(to);
+    auto skip = [](const Obs *p, const Obs *e, int64_t read) {
+        while (p != e && p->read == read) ++p;
+        return p;
+    };
+    while (f != fe && t != te) {
+        if (f->read == t->read) {
+            const int64_t len = t->offset - f->offset;
+            if (len > 0) {
+                ReadSub rs{f->read, f->offset, len, -1.0};
+                if (quals) {
+                    const std::vector<uint8_t> &q = (*quals)[readBase + f->read];
+                    int64_t sum = 0;
+                    for (int64_t k = 0; k < len; k++) sum += (int64_t) q[f->offset + k];
+                    rs.qual = (double) sum / (double) len;
+                }
+                out.push_back(rs);
+            }
+            const int64_t r = f->read;
+            f = skip(f + 1, fe, r);
+            t = skip(t + 1, te, t->read);
+        } else if (f->read < t->read) {
+            f = skip(f + 1, fe, f->read);
+        } else {
+            t = skip(t + 1, te, t->read);
+        }
+    }
+    std::stable_sort(out.begin(), out.end(), [](const ReadSub &a, const ReadSub &b) { return a.qual > b.qual; });
+    while ((int64_t) out.size() > keepAtLeast) {
+        const ReadSub &last = out.back();
+        if (last.qual >= minQual || last.qual == -1.0) break;
+        out.pop_back();
+    }
+}
+
+bool sameRuns(const Rle &r, int64_t start, int64_t len, const Rle &s, int64_t sStart) {
+    return std::equal(r.c.begin() + start, r.c.begin() + start + len, s.c.begin() + sStart) &&
+           std::equal(r.n.begin() + start, r.n.begin() + start + len, s.n.begin() + sStart);
+}
+
+// bubbleGraph_constructFromPoa (:800-978) without the scores: the bubbles between consecutive
+// anchor nodes that have read substrings and more than one allele. The alleles are the distinct
+// read substrings (groupRleStrings keys on the run characters and run lengths, :722-742), in
+// order of first appearance, with run lengths capped at 255 (getConsensusRleString, :744-765),
+// then the reference allele if no read spells it.
+BubbleGraph buildBubbles(Poa &poa, const std::vector<Rle> &reads, const std::vector<std::vector<uint8_t>> *quals,
+                         int64_t readBase, double candidateFraction, int64_t trim, int64_t keepAtLeast, double minQual) {
+    BubbleGraph g;
+    const std::vector<double> cw = candidateWeights(poa, candidateFraction);
+    sortObservations(poa);
+    const std::vector<uint8_t> anchor = anchorPositions(poa, cw, trim);
+    const int64_t n = (int64_t) poa.nodes.size();
+    std::vector<ReadSub> subs;
+    std::vector<int64_t> firstOf;  // per distinct allele: a substring that spells it
+    int64_t pAnchor = 0;
+    for (int64_t i = 1; i < n; i++) {
+        if (!anchor[i]) continue;
+        if (i - pAnchor != 1) {
+            readSubstrings(poa, pAnchor + 1, i, quals, readBase, keepAtLeast, minQual, subs);
+            if (!subs.empty()) {
+                // distinct substrings in order of first appearance
+                firstOf.clear();
+                for (size_t k = 0; k < subs.size(); k++) {
+                    const Rle &rk = reads[readBase + subs[k].read];
+                    bool seen = false;
+                    for (int64_t f : firstOf) {
+                        const ReadSub &o = subs[(size_t) f];
+                        if (o.length == subs[k].length &&
+                            sameRuns(rk, subs[k].start, subs[k].length, reads[readBase + o.read], o.start)) {
+                            seen = true;
+                            break;
+                        }
+                    }
+                    if (!seen) firstOf.push_back((int64_t) k);
+                }
+                const int64_t refLen = i - 1 - pAnchor;
+                const size_t a0 = g.alleles.size();
+                bool seenRef = false;
+                for (int64_t f : firstOf) {
+                    const ReadSub &o = subs[(size_t) f];
+                    const Rle &ro = reads[readBase + o.read];
+                    Rle a;
+                    for (int64_t k = 0; k < o.length; k++) {
+                        const uint64_t c = ro.n[o.start + k];
+                        a.push(ro.c[o.start + k], c == 0 ? 1 : (c > 255 ? 255 : c));
+                    }
+                    if (a.length() == refLen && sameRuns(poa.ref, pAnchor, refLen, a, 0)) seenRef = true;
+                    g.alleles.push_back(std::move(a));
+                }
+                if (!seenRef) g.alleles.push_back(poa.ref.sub(pAnchor, refLen));
+                const int64_t nAlleles = (int64_t) (g.alleles.size() - a0);
+                if (nAlleles > 1) {
+                    Bubble b;
+                    b.refStart = pAnchor;
+                    b.refLength = refLen;
+                    b.alleleFirst = (int64_t) a0;
+                    b.nAlleles = nAlleles;
+                    b.readFirst = (int64_t) g.reads.size();
+                    b.nReads = (int64_t) subs.size();
+                    b.supportFirst = 0;
+                    // the bubble takes the substrings from the end of the list (stList_pop)
+                    for (size_t k = subs.size(); k-- > 0;) g.reads.push_back(subs[k]);
+                    // the score cache (:905-951) keys on the substring's runs; the strand is
+                    // not part of the key
+                    for (int64_t k = 0; k < b.nReads; k++) {
+                        const ReadSub &rk = g.reads[(size_t) (b.readFirst + k)];
+                        int32_t from = (int32_t) k;
+                        for (int64_t q = 0; q < k; q++) {
+                            const ReadSub &rq = g.reads[(size_t) (b.readFirst + q)];
+                            if (g.scoreFrom[(size_t) (b.readFirst + q)] == (int32_t) q && rq.length == rk.length &&
+                                sameRuns(reads[readBase + rk.read], rk.start, rk.length, reads[readBase + rq.read],
+                                         rq.start)) {
+                                from = (int32_t) q;
+                                break;
+                            }
+                        }
+                        g.scoreFrom.push_back(from);
+                    }
+                    g.bubbles.push_back(b);
+                } else {
+                    g.alleles.resize(a0);
+                }
+            }
+        }
+        pAnchor = i;
+    }
+    int64_t at = 0;
+    for (Bubble &b : g.bubbles) {
+        b.supportFirst = at;
+        at += b.nAlleles * b.nReads;
+    }
+    g.supports.assign((size_t) at, 0.0f);
+    return g;
+}
+
+// bubbleGraph_getConsensusPath (:52-59): per bubble, the allele with the largest summed support
+// (reads in the bubble's order; the first of equal sums).
+std::vector<int64_t> consensusPath(const BubbleGraph &g) {
+    std::vector<int64_t> path(g.bubbles.size(), 0);
+    for (size_t i = 0; i < g.bubbles.size(); i++) {
+        const Bubble &b = g.bubbles[i];
+        double best = 0.0;
+        for (int64_t j = 0; j < b.nAlleles; j++) {
+            double ll = 0.0;
+            for (int64_t k = 0; k < b.nReads; k++) ll += (double) g.supports[(size_t) (b.supportFirst + j * b.nReads + k)];
+            if (j == 0 || ll > best) {
+                best = ll;
+                path[i] = j;
+            }
+        }
+    }
+    return path;
+}
+
+// bubbleGraph_getConsensusString (:61-177): the reference between bubbles and the chosen allele
+// of every bubble, joined and run-length encoded again (runs meeting at a seam merge), and the
+// map from reference runs to the new string's runs.
+Rle bubbleConsensus(const Poa &poa, const BubbleGraph &g, const std::vector<int64_t> &path, bool useRle,
+                    std::vector<int64_t> &map) {
+    const Rle &ref = poa.ref;
+    const int64_t refLen = ref.length();
+    map.assign((size_t) refLen, -1);
+    Rle out;
+    auto append = [&](const Rle &s, int64_t start, int64_t len) {
+        for (int64_t k = start; k < start + len; k++) {
+            if (useRle) {
+                if (out.length() > 0 && out.c.back() == s.c[k]) {
+                    out.n.back() += s.n[k];
+                    out.nonRle += s.n[k];
+                } else {
+                    out.push(s.c[k], s.n[k]);
+                }
+            } else {
+                for (uint64_t r = 0; r < s.n[k]; r++) out.push(s.c[k], 1);
+            }
+        }
+    };
+    char previous = '-';
+    int64_t j = 0, k = 0;
+    for (size_t i = 0; i < g.bubbles.size(); i++) {
+        const Bubble &b = g.bubbles[i];
+        if (k < b.refStart) {
+            append(ref, k, b.refStart - k);
+            const char first = ref.c[k], last = ref.c[b.refStart - 1];
+            if (useRle && first == previous) k++;
+            while (k < b.refStart) map[(size_t) k++] = j++;
+            previous = last;
+        }
+        const Rle &allele = g.alleles[(size_t) (b.alleleFirst + path[i])];
+        append(allele, 0, allele.length());
+        if (allele.length() == b.refLength && sameRuns(ref, b.refStart, b.refLength, allele, 0)) {  // rleString_eq
+            if (useRle && allele.c[0] == previous) k++;
+            while (k < b.refStart + b.refLength) map[(size_t) k++] = j++;
+        } else {
+            k += b.refLength;
+            j += allele.length() + ((useRle && allele.c[0] == previous) ? -1 : 0);
+        }
+        previous = allele.c[allele.length() - 1];
+    }
+    if (k < refLen) {
+        append(ref, k, refLen - k);
+        if (useRle && ref.c[k] == previous) k++;
+        while (k < refLen) map[(size_t) k++] = j++;
+    }
+    return out;
+}
+
 // Runs f(c) for every chunk index in `chunks` on up to `threads` host threads.
 template <class F>
 void forChunks(const std::vector<int64_t> &chunks, F f) {
@@ -717,6 +1042,13 @@ struct mp_poa_set {
     bool haveAnchors = false;
     std::vector<Poa> poas;                   // per chunk (after a realignment)
     std::vector<int64_t> iterations;         // per chunk: iterations run by the last iterate
+    // polish mode (poa_polish)
+    int64_t minPolish = 0, maxPolish = 0;
+    double candidateFraction = 0.18;
+    int64_t anchorTrim = 5, keepAtLeast = 15;
+    double minQual = 10.0;
+    std::vector<std::vector<uint8_t>> quals;  // per read, per run (empty when none given)
+    std::vector<BubbleGraph> bubbles;        // per chunk: the last graph mp_poa_set_build_bubbles made
     mp_device_batch *db = nullptr;
     // page-locked tuple arrays of the last realignment (grow only): the copies run by DMA
     void *pinned[3] = {nullptr, nullptr, nullptr};
@@ -895,25 +1227,151 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
     return MP_OK;
 }
 
-// poa_realignIterative in consensus mode (impl/polisher.c:2034-2106) for every chunk at once.
-mp_status iterate(mp_poa_set *s) {
+// Scores the bubble graphs of the listed chunks (their `graphs` entries) with one bubble-scoring
+// launch: every allele against every distinct read substring of its bubble (the symbol strings
+// of rleString_constructSymbolString, run lengths capped below the table), the result stored as
+// float like the reference's alleleReadSupports, then copied to the reads that share a substring.
+mp_status scoreBubbles(mp_poa_set *s, const std::vector<int64_t> &chunks, std::vector<BubbleGraph> &graphs) {
+    if (!s->e || !s->m) return mp_fail(MP_ERR_STATE, "mp_poa: bubble scoring needs an engine and a model");
+    const bool rle = s->m->host[0].runLength != 0;
+    const uint64_t maxRC = s->useRle ? (uint64_t) s->rm.M : 2;
+    auto symbol = [&](char ch, uint64_t cnt) {
+        const uint16_t b = (uint16_t) symbolOf(ch);
+        cnt = cnt > maxRC - 1 ? maxRC - 1 : cnt;
+        return rle ? (uint16_t) ((cnt << 8) | b) : b;
+    };
+    struct Count {
+        int64_t pairs = 0, xs = 0, ys = 0;
+    };
+    std::vector<Count> cnt(s->nChunks), base(s->nChunks);
+    forChunks(chunks, [&](int64_t c) {
+        const BubbleGraph &g = graphs[c];
+        Count k;
+        for (const Bubble &b : g.bubbles) {
+            int64_t distinct = 0;
+            for (int64_t r = 0; r < b.nReads; r++)
+                if (g.scoreFrom[(size_t) (b.readFirst + r)] == (int32_t) r) {
+                    distinct++;
+                    k.ys += g.reads[(size_t) (b.readFirst + r)].length;
+                }
+            k.pairs += distinct * b.nAlleles;
+            for (int64_t j = 0; j < b.nAlleles; j++) k.xs += g.alleles[(size_t) (b.alleleFirst + j)].length();
+        }
+        cnt[c] = k;
+    });
+    Count total;
+    for (int64_t c : chunks) {
+        base[c] = total;
+        total.pairs += cnt[c].pairs;
+        total.xs += cnt[c].xs;
+        total.ys += cnt[c].ys;
+    }
+    if (total.pairs == 0) {
+        for (int64_t c : chunks) graphs[c].scored = true;
+        return MP_OK;
+    }
+    std::vector<int64_t> xo((size_t) total.pairs), yo((size_t) total.pairs);
+    std::vector<int32_t> xl((size_t) total.pairs), yl((size_t) total.pairs);
+    std::vector<uint8_t> st((size_t) total.pairs);
+    std::vector<uint16_t> xs((size_t) std::max<int64_t>(total.xs, 1)), ys((size_t) std::max<int64_t>(total.ys, 1));
+    std::vector<double> ll((size_t) total.pairs);
+    forChunks(chunks, [&](int64_t c) {
+        const BubbleGraph &g = graphs[c];
+        int64_t p = base[c].pairs, x = base[c].xs, y = base[c].ys;
+        std::vector<int64_t> alleleAt;
+        for (const Bubble &b : g.bubbles) {
+            alleleAt.assign((size_t) b.nAlleles, 0);
+            for (int64_t j = 0; j < b.nAlleles; j++) {
+                const Rle &a = g.alleles[(size_t) (b.alleleFirst + j)];
+                alleleAt[(size_t) j] = x;
+                for (int64_t k = 0; k < a.length(); k++) xs[(size_t) x++] = symbol(a.c[k], a.n[k]);
+            }
+            for (int64_t r = 0; r < b.nReads; r++) {
+                if (g.scoreFrom[(size_t) (b.readFirst + r)] != (int32_t) r) continue;
+                const ReadSub &rs = g.reads[(size_t) (b.readFirst + r)];
+                const Rle &read = s->reads[s->chunkReads[c] + rs.read];
+                const int64_t yAt = y;
+                for (int64_t k = 0; k < rs.length; k++) ys[(size_t) y++] = symbol(read.c[rs.start + k], read.n[rs.start + k]);
+                for (int64_t j = 0; j < b.nAlleles; j++) {
+                    xo[(size_t) p] = alleleAt[(size_t) j];
+                    xl[(size_t) p] = (int32_t) g.alleles[(size_t) (b.alleleFirst + j)].length();
+                    yo[(size_t) p] = yAt;
+                    yl[(size_t) p] = (int32_t) rs.length;
+                    st[(size_t) p] = s->strand[s->chunkReads[c] + rs.read];
+                    p++;
+                }
+            }
+        }
+    });
+    mp_pair_batch pb;
+    pb.n_pairs = total.pairs;
+    pb.x_offset = xo.data();
+    pb.x_length = xl.data();
+    pb.y_offset = yo.data();
+    pb.y_length = yl.data();
+    pb.strand = st.data();
+    pb.x_symbols_length = total.xs;
+    pb.x_symbols = xs.data();
+    pb.y_symbols_length = total.ys;
+    pb.y_symbols = ys.data();
+    MP_TRY(mp_forward_pairs(s->e, s->m, &pb, ll.data()));
+    forChunks(chunks, [&](int64_t c) {
+        BubbleGraph &g = graphs[c];
+        int64_t p = base[c].pairs;
+        for (const Bubble &b : g.bubbles) {
+            float *sup = g.supports.data() + b.supportFirst;
+            for (int64_t r = 0; r < b.nReads; r++) {
+                const int32_t from = g.scoreFrom[(size_t) (b.readFirst + r)];
+                if (from == (int32_t) r) {
+                    for (int64_t j = 0; j < b.nAlleles; j++) sup[j * b.nReads + r] = (float) ll[(size_t) p++];
+                } else {
+                    for (int64_t j = 0; j < b.nAlleles; j++) sup[j * b.nReads + r] = sup[j * b.nReads + from];
+                }
+            }
+        }
+        g.scored = true;
+    });
+    return MP_OK;
+}
+
+BubbleGraph buildBubblesOf(mp_poa_set *s, int64_t c) {
+    return buildBubbles(s->poas[c], s->reads, s->quals.empty() ? nullptr : &s->quals, s->chunkReads[c],
+                        s->candidateFraction, s->anchorTrim, s->keepAtLeast, s->minQual);
+}
+
+// poa_realignIterative (impl/polisher.c:2034-2106) for every chunk at once, in consensus mode
+// (poa_getConsensus) or polish mode (poa_polish: the bubble graphs of all chunks built on host
+// threads, scored in one launch, then each chunk's allele choice and new consensus).
+mp_status iterate(mp_poa_set *s, bool polishMode) {
     const int64_t nC = s->nChunks;
+    const int64_t minIter = polishMode ? s->minPolish : s->minIter;
+    const int64_t maxIter = polishMode ? s->maxPolish : s->maxIter;
     std::vector<double> sc(nC);
     std::vector<int64_t> active;
     for (int64_t c = 0; c < nC; c++) {
         sc[c] = score(s->poas[c]);
         s->iterations[c] = 0;
-        if (s->maxIter > 0) active.push_back(c);
+        if (maxIter > 0) active.push_back(c);
     }
     std::vector<Rle> cons(nC);
     std::vector<std::vector<int64_t>> maps(nC);
     std::vector<Poa> next(nC);
+    std::vector<BubbleGraph> graphs(polishMode ? nC : 0);
     while (!active.empty()) {
         std::vector<uint8_t> realign(nC, 0);
+        if (polishMode) {
+            forChunks(active, [&](int64_t c) { graphs[c] = buildBubblesOf(s, c); });
+            MP_TRY(scoreBubbles(s, active, graphs));
+        }
         std::vector<std::vector<Anchor>> anchors(s->reads.size());
         forChunks(active, [&](int64_t c) {
             s->iterations[c]++;
-            cons[c] = consensus(s->poas[c], maps[c], s->penalty, s->useRle);
+            if (polishMode) {
+                cons[c] = bubbleConsensus(s->poas[c], graphs[c], consensusPath(graphs[c]), s->useRle, maps[c]);
+                graphs[c] = BubbleGraph();
+            } else {
+                cons[c] = consensus(s->poas[c], maps[c], s->penalty, s->useRle);
+            }
             if (cons[c] == s->poas[c].ref) return;  // greedy convergence
             auto a = anchorAlignments(s->poas[c], &maps[c], s->chunkReads[c + 1] - s->chunkReads[c], s->anchorProbs);
             for (int64_t r = 0; r < (int64_t) a.size(); r++) anchors[s->chunkReads[c] + r] = std::move(a[r]);
@@ -929,8 +1387,8 @@ mp_status iterate(mp_poa_set *s) {
         forChunks(go, [&](int64_t c) {
             if (s->useRle) estimateRepeatCounts(next[c], s->reads, s->strand, s->chunkReads[c], s->rm);
             const double sc2 = score(next[c]);
-            if (sc2 <= sc[c] && s->iterations[c] > s->minIter) {  // greedy stop: keep the old graph
-                Poa drop = std::move(next[c]);                   // (freed here, in parallel)
+            if (sc2 <= sc[c] && s->iterations[c] > minIter) {  // greedy stop: keep the old graph
+                Poa drop = std::move(next[c]);                // (freed here, in parallel)
                 return;
             }
             s->poas[c] = std::move(next[c]);
@@ -938,7 +1396,7 @@ mp_status iterate(mp_poa_set *s) {
             keep[c] = 1;
         });
         for (int64_t c : go)
-            if (keep[c] && s->iterations[c] < s->maxIter) still.push_back(c);
+            if (keep[c] && s->iterations[c] < maxIter) still.push_back(c);
         active.swap(still);
     }
     return MP_OK;
@@ -970,6 +1428,14 @@ extern "C" mp_status mp_poa_set_create(mp_engine *e, const mp_model *m, const mp
         return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_create: need 0 <= min_iterations <= max_iterations");
     if (pp->use_run_length && !repeat_log10)
         return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_create: run-length polishing needs the repeat-count table");
+    if (pp->min_polish_iterations < 0 || pp->max_polish_iterations < pp->min_polish_iterations)
+        return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_create: need 0 <= min_polish_iterations <= max_polish_iterations");
+    if (pp->max_polish_iterations > 0 && !pp->use_read_alleles)
+        return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_create: polish mode builds its alleles from the reads' substrings "
+                       "(use_read_alleles = 1); the enumeration of candidate variants is not built");
+    if (pp->column_anchor_trim < 0 || pp->filter_reads_coverage < 0 || std::isnan(pp->candidate_variant_weight) ||
+        std::isnan(pp->min_avg_base_quality))
+        return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_create: polish-mode parameters out of range");
     mp_poa_set *s = new mp_poa_set();
     s->e = e;
     s->m = m;
@@ -980,6 +1446,12 @@ extern "C" mp_status mp_poa_set_create(mp_engine *e, const mp_model *m, const mp
     s->anchorProbs.assign(pp->anchor_probs, pp->anchor_probs + pp->n_anchor_probs);
     s->minIter = pp->min_iterations;
     s->maxIter = pp->max_iterations;
+    s->minPolish = pp->min_polish_iterations;
+    s->maxPolish = pp->max_polish_iterations;
+    s->candidateFraction = pp->candidate_variant_weight;
+    s->anchorTrim = pp->column_anchor_trim;
+    s->keepAtLeast = pp->filter_reads_coverage;
+    s->minQual = pp->min_avg_base_quality;
     s->rm.M = mp::kMaxRepeat;
     if (repeat_log10) s->rm.log10.assign(repeat_log10, repeat_log10 + 4 * mp::kMaxRepeat * mp::kMaxRepeat);
     s->nChunks = b->n_chunks;
@@ -1010,6 +1482,8 @@ extern "C" mp_status mp_poa_set_create(mp_engine *e, const mp_model *m, const mp
         }
         s->reads.push_back(rr);
         s->strand.push_back(b->strand[r]);
+        if (b->read_qualities)
+            s->quals.emplace_back(b->read_qualities + b->read_offsets[r], b->read_qualities + b->read_offsets[r + 1]);
         std::vector<Anchor> a;
         if (s->haveAnchors)
             for (int64_t k = b->anchor_offsets[r]; k < b->anchor_offsets[r + 1]; k++)
@@ -1017,6 +1491,7 @@ extern "C" mp_status mp_poa_set_create(mp_engine *e, const mp_model *m, const mp
         s->initialAnchors.push_back(a);
     }
     s->iterations.assign(s->nChunks, 0);
+    s->bubbles.resize(s->nChunks);
     *out = s;
     return MP_OK;
 }
@@ -1076,12 +1551,100 @@ extern "C" mp_status mp_poa_set_realign_pairs(mp_poa_set *s, const int64_t *cons
 extern "C" mp_status mp_poa_set_iterate(mp_poa_set *s) {
     if (!s) return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_iterate: NULL set");
     if (s->poas.empty()) return mp_fail(MP_ERR_STATE, "mp_poa_set_iterate: realign first");
-    return iterate(s);
+    return iterate(s, false);
+}
+
+extern "C" mp_status mp_poa_set_iterate_polish(mp_poa_set *s) {
+    if (!s) return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_iterate_polish: NULL set");
+    if (s->poas.empty()) return mp_fail(MP_ERR_STATE, "mp_poa_set_iterate_polish: realign first");
+    return iterate(s, true);
 }
 
 extern "C" mp_status mp_poa_set_realign_all(mp_poa_set *s) {
     MP_TRY(mp_poa_set_realign(s));
-    return mp_poa_set_iterate(s);
+    if (s->maxIter > 0) MP_TRY(iterate(s, false));
+    if (s->maxPolish > 0) MP_TRY(iterate(s, true));
+    return MP_OK;
+}
+
+extern "C" mp_status mp_poa_set_build_bubbles(mp_poa_set *s) {
+    if (!s) return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_build_bubbles: NULL set");
+    if (s->poas.empty()) return mp_fail(MP_ERR_STATE, "mp_poa_set_build_bubbles: realign first");
+    std::vector<int64_t> all(s->nChunks);
+    for (int64_t c = 0; c < s->nChunks; c++) all[c] = c;
+    forChunks(all, [&](int64_t c) { s->bubbles[c] = buildBubblesOf(s, c); });
+    return MP_OK;
+}
+
+extern "C" mp_status mp_poa_set_score_bubbles(mp_poa_set *s) {
+    if (!s) return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_score_bubbles: NULL set");
+    std::vector<int64_t> all(s->nChunks);
+    for (int64_t c = 0; c < s->nChunks; c++) all[c] = c;
+    return scoreBubbles(s, all, s->bubbles);
+}
+
+extern "C" mp_status mp_poa_bubble_sizes(const mp_poa_set *s, int64_t chunk, int64_t sizes[4]) {
+    MP_TRY(chunkCheck(s, chunk));
+    if (!sizes) return mp_fail(MP_ERR_ARGUMENT, "mp_poa_bubble_sizes: NULL sizes");
+    const BubbleGraph &g = s->bubbles[chunk];
+    int64_t runs = 0;
+    for (const Rle &a : g.alleles) runs += a.length();
+    sizes[0] = (int64_t) g.bubbles.size();
+    sizes[1] = (int64_t) g.alleles.size();
+    sizes[2] = runs;
+    sizes[3] = (int64_t) g.reads.size();
+    return MP_OK;
+}
+
+extern "C" mp_status mp_poa_bubbles(const mp_poa_set *s, int64_t chunk, int64_t *bubbles, int64_t *allele_runs,
+                                    char *chars, uint64_t *counts, int64_t *reads, double *quals, float *supports) {
+    MP_TRY(chunkCheck(s, chunk));
+    const BubbleGraph &g = s->bubbles[chunk];
+    for (size_t i = 0; bubbles && i < g.bubbles.size(); i++) {
+        const Bubble &b = g.bubbles[i];
+        const int64_t v[6] = {b.refStart, b.refLength, b.alleleFirst, b.nAlleles, b.readFirst, b.nReads};
+        memcpy(bubbles + 6 * i, v, sizeof(v));
+    }
+    int64_t at = 0;
+    for (size_t j = 0; j < g.alleles.size(); j++) {
+        const Rle &a = g.alleles[j];
+        if (allele_runs) allele_runs[j] = a.length();
+        for (int64_t k = 0; k < a.length(); k++, at++) {
+            if (chars) chars[at] = a.c[k];
+            if (counts) counts[at] = a.n[k];
+        }
+    }
+    for (size_t k = 0; k < g.reads.size(); k++) {
+        if (reads) {
+            reads[3 * k] = g.reads[k].read;
+            reads[3 * k + 1] = g.reads[k].start;
+            reads[3 * k + 2] = g.reads[k].length;
+        }
+        if (quals) quals[k] = g.reads[k].qual;
+    }
+    if (supports && !g.supports.empty()) memcpy(supports, g.supports.data(), sizeof(float) * g.supports.size());
+    return MP_OK;
+}
+
+extern "C" mp_status mp_poa_bubble_consensus(const mp_poa_set *s, int64_t chunk, int64_t *path, char *chars,
+                                             uint64_t *counts, int64_t cap, int64_t *n_runs, int64_t *map) {
+    MP_TRY(chunkCheck(s, chunk));
+    const BubbleGraph &g = s->bubbles[chunk];
+    if (!g.scored) return mp_fail(MP_ERR_STATE, "mp_poa_bubble_consensus: score the bubbles first");
+    if (!n_runs) return mp_fail(MP_ERR_ARGUMENT, "mp_poa_bubble_consensus: NULL n_runs");
+    const std::vector<int64_t> p = consensusPath(g);
+    std::vector<int64_t> m;
+    const Rle c = bubbleConsensus(s->poas[chunk], g, p, s->useRle, m);
+    *n_runs = c.length();
+    if (path) std::copy(p.begin(), p.end(), path);
+    if (map) std::copy(m.begin(), m.end(), map);
+    if (c.length() > cap) return mp_fail(MP_ERR_OVERFLOW, "mp_poa_bubble_consensus: %lld runs, room for %lld",
+                                         (long long) c.length(), (long long) cap);
+    for (int64_t k = 0; k < c.length(); k++) {
+        if (chars) chars[k] = c.c[k];
+        if (counts) counts[k] = c.n[k];
+    }
+    return MP_OK;
 }
 
 extern "C" mp_status mp_poa_set_estimate_repeat_counts(mp_poa_set *s) {

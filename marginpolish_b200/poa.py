@@ -6,8 +6,11 @@ operator API over the library's C ABI (mp_poa_set_*):
 * ``PoaSet.consensus``      -- poa_getConsensus (:1025-1275);
 * ``PoaSet.anchor_alignments`` -- poa_getAnchorAlignments (:536-592);
 * ``PoaSet.estimate_repeat_counts`` -- poa_estimateRepeatCountsUsingBayesianModel (:1556-1565);
-* ``PoaSet.iterate`` / ``realign_all`` -- poa_realignIterative / poa_realignAll in
-  consensus mode (:2034-2129);
+* ``PoaSet.iterate`` / ``iterate_polish`` / ``realign_all`` -- poa_realignIterative in
+  consensus or polish mode and poa_realignAll (:2034-2129);
+* ``PoaSet.build_bubbles`` / ``score_bubbles`` / ``bubbles`` / ``bubble_consensus`` -- the
+  steps of poa_polish (:2008-2031): bubbleGraph_constructFromPoa, the allele scores (one
+  GPU launch for all chunks), the allele choice and the new consensus (impl/bubbleGraph.c);
 * ``polish`` -- the whole loop for many chunks, returning each chunk's polished draft.
 
 Weights, observations and indels can be read back for every chunk, with the layouts of
@@ -32,20 +35,40 @@ c_uint64 = ctypes.c_uint64
 
 @dataclass
 class PolishParams:
-    """The POA fields of PolishParams (inc/margin.h:534-580); defaults are the shipped
-    params/allParams.np.json values except max_iterations (0 there: consensus mode off)."""
+    """The POA fields of PolishParams (inc/margin.h:534-580). Defaults are the shipped
+    params/allParams.np.json values except the iteration counts: these defaults run the
+    consensus mode (max_iterations 5) and no polish mode; ``shipped()`` gives the shipped loop
+    (no consensus iterations, one polish iteration)."""
     reference_base_penalty: float = 0.5
     compare_repeat_counts: bool = True
     use_run_length: bool = True
     anchor_probs: Sequence[float] = (0.9, 10, 0.95, 4, 0.99, 0)
     min_iterations: int = 0
     max_iterations: int = 5
+    # polish mode (poa_polish)
+    min_polish_iterations: int = 0
+    max_polish_iterations: int = 0
+    use_read_alleles: bool = True
+    candidate_variant_weight: float = 0.18
+    column_anchor_trim: int = 5
+    filter_reads_coverage: int = 15
+    min_avg_base_quality: float = 10.0
+    max_consensus_strings: int = 100
+
+    @classmethod
+    def shipped(cls) -> "PolishParams":
+        """The loop params/allParams.np.json configures: poa_realignAll with no consensus
+        iterations and one polish iteration (impl/polisher.c:2109-2129)."""
+        return cls(min_iterations=0, max_iterations=0, min_polish_iterations=1, max_polish_iterations=1)
 
     def struct(self):
         probs = np.ascontiguousarray(self.anchor_probs, dtype=np.float64)
         p = _lib.PolishParamsC(float(self.reference_base_penalty), 1 if self.compare_repeat_counts else 0,
                                1 if self.use_run_length else 0, _lib.ptr(probs, c_double), probs.size,
-                               int(self.min_iterations), int(self.max_iterations))
+                               int(self.min_iterations), int(self.max_iterations), int(self.min_polish_iterations),
+                               int(self.max_polish_iterations), 1 if self.use_read_alleles else 0, 0,
+                               float(self.candidate_variant_weight), int(self.column_anchor_trim),
+                               int(self.filter_reads_coverage), float(self.min_avg_base_quality))
         return p, probs
 
 
@@ -64,7 +87,8 @@ class PoaSet:
 
     def __init__(self, engine: Engine, model: Model, params: AlignmentParams, polish: PolishParams,
                  drafts: Sequence[RleString], reads: Sequence[Sequence[RleString]], strands: Sequence[Sequence[int]],
-                 anchors: Optional[Sequence[Sequence[np.ndarray]]] = None, repeat_log10: Optional[np.ndarray] = None):
+                 anchors: Optional[Sequence[Sequence[np.ndarray]]] = None, repeat_log10: Optional[np.ndarray] = None,
+                 qualities: Optional[Sequence[Sequence[np.ndarray]]] = None):
         self.engine, self.model = engine, model
         self._lib = engine._lib if engine is not None else _lib.load()
         self.n_chunks = len(drafts)
@@ -98,6 +122,13 @@ class PoaSet:
             keep += [a_off, a_all]
             b.anchor_offsets = _lib.ptr(a_off, c_int64)
             b.anchors = _lib.ptr(a_all, c_int32)
+        if qualities is not None:
+            flat_q = [np.asarray(q, dtype=np.uint8) for lst in qualities for q in lst]
+            if len(flat_q) != len(flat_reads) or any(q.size != len(r) for q, r in zip(flat_q, flat_reads)):
+                raise ValueError("one quality per read run")
+            q_all = np.ascontiguousarray(np.concatenate(flat_q) if flat_q and rd_off[-1] else np.zeros(1, np.uint8))
+            keep.append(q_all)
+            b.read_qualities = _lib.ptr(q_all, c_uint8)
         pp, probs = polish.struct()
         keep.append(probs)
         ps = params.struct()
@@ -115,9 +146,9 @@ class PoaSet:
 
     @classmethod
     def from_polish_model(cls, engine, model, pm: PolishModel, polish: PolishParams, drafts, reads, strands,
-                          anchors=None) -> "PoaSet":
+                          anchors=None, qualities=None) -> "PoaSet":
         return cls(engine, model, pm.alignment, polish, drafts, reads, strands, anchors,
-                   pm.repeat_log10 if polish.use_run_length else None)
+                   pm.repeat_log10 if polish.use_run_length else None, qualities)
 
     # ---- the loop's steps ----
     def realign(self) -> None:
@@ -143,6 +174,65 @@ class PoaSet:
 
     def iterate(self) -> None:
         _lib.check(self._lib.mp_poa_set_iterate(self.handle))
+
+    def iterate_polish(self) -> None:
+        """poa_realignIterative in polish mode (poa_polish) for every chunk."""
+        _lib.check(self._lib.mp_poa_set_iterate_polish(self.handle))
+
+    # ---- the bubble graph of one polish iteration (impl/bubbleGraph.c:800-978) ----
+    def build_bubbles(self) -> None:
+        _lib.check(self._lib.mp_poa_set_build_bubbles(self.handle))
+
+    def score_bubbles(self) -> None:
+        _lib.check(self._lib.mp_poa_set_score_bubbles(self.handle))
+
+    def bubbles(self, chunk: int) -> list:
+        """The chunk's bubble graph: per bubble a dict with ref_start, ref_length, alleles (list of
+        (chars, counts)), reads ((n, 3) rows of read, start, length), quals and supports
+        (alleles x reads, float32)."""
+        sz = np.zeros(4, np.int64)
+        _lib.check(self._lib.mp_poa_bubble_sizes(self.handle, chunk, _lib.ptr(sz, c_int64)))
+        nb, na, runs, nr = (int(v) for v in sz)
+        rows = np.zeros((max(nb, 1), 6), np.int64)
+        alen = np.zeros(max(na, 1), np.int64)
+        chars = (c_char * max(runs, 1))()
+        counts = np.zeros(max(runs, 1), np.uint64)
+        rd = np.zeros((max(nr, 1), 3), np.int64)
+        q = np.zeros(max(nr, 1))
+        _lib.check(self._lib.mp_poa_bubbles(self.handle, chunk, _lib.ptr(rows, c_int64), _lib.ptr(alen, c_int64),
+                                            chars, _lib.ptr(counts, c_uint64), _lib.ptr(rd, c_int64),
+                                            _lib.ptr(q, c_double), None))
+        n_sup = int(np.sum(rows[:nb, 3] * rows[:nb, 5]))
+        sup = np.zeros(max(n_sup, 1), np.float32)
+        _lib.check(self._lib.mp_poa_bubbles(self.handle, chunk, None, None, None, None, None, None,
+                                            _lib.ptr(sup, ctypes.c_float)))
+        raw = bytes(chars[:runs])
+        starts = np.concatenate([[0], np.cumsum(alen[:na])]).astype(np.int64)
+        out, at = [], 0
+        for i in range(nb):
+            rs, rl, af, n_al, rf, n_rd = (int(v) for v in rows[i])
+            alleles = [(raw[starts[j]:starts[j + 1]], counts[starts[j]:starts[j + 1]].copy()) for j in range(af, af + n_al)]
+            out.append(dict(ref_start=rs, ref_length=rl, alleles=alleles, reads=rd[rf:rf + n_rd].copy(),
+                            quals=q[rf:rf + n_rd].copy(), supports=sup[at:at + n_al * n_rd].reshape(n_al, n_rd).copy()))
+            at += n_al * n_rd
+        return out
+
+    def bubble_consensus(self, chunk: int):
+        """(path, consensus RleString, reference-to-consensus map) of the scored bubble graph."""
+        sz = np.zeros(4, np.int64)
+        _lib.check(self._lib.mp_poa_bubble_sizes(self.handle, chunk, _lib.ptr(sz, c_int64)))
+        inf = self.info(chunk)
+        cap = 4 * inf["nodes"] + 4 * int(sz[2]) + 16
+        path = np.zeros(max(int(sz[0]), 1), np.int64)
+        chars = (c_char * cap)()
+        counts = np.zeros(cap, np.uint64)
+        n = c_int64(0)
+        m = np.zeros(max(inf["reference_runs"], 1), np.int64)
+        _lib.check(self._lib.mp_poa_bubble_consensus(self.handle, chunk, _lib.ptr(path, c_int64), chars,
+                                                     _lib.ptr(counts, c_uint64), cap, ctypes.byref(n),
+                                                     _lib.ptr(m, c_int64)))
+        return (path[:int(sz[0])].copy(), RleString(bytes(chars[:n.value]), counts[:n.value].astype(np.uint32)),
+                m[:inf["reference_runs"]].copy())
 
     def realign_all(self) -> None:
         _lib.check(self._lib.mp_poa_set_realign_all(self.handle))
@@ -247,10 +337,11 @@ class PoaSet:
 
 
 def polish(engine: Engine, model: Model, pm: PolishModel, polish_params: PolishParams, drafts, reads, strands,
-           anchors=None) -> List[RleString]:
-    """poa_realignAll in consensus mode for every chunk, then the run-length estimate the
-    caller applies to the result (marginPolish.c:558): each chunk's polished draft."""
-    s = PoaSet.from_polish_model(engine, model, pm, polish_params, drafts, reads, strands, anchors)
+           anchors=None, qualities=None) -> List[RleString]:
+    """poa_realignAll for every chunk (the consensus iterations, then the polish iterations, as
+    polish_params sets them), then the run-length estimate the caller applies to the result
+    (marginPolish.c:554-560): each chunk's polished draft."""
+    s = PoaSet.from_polish_model(engine, model, pm, polish_params, drafts, reads, strands, anchors, qualities)
     try:
         s.realign_all()
         if polish_params.use_run_length:

@@ -485,6 +485,41 @@ def compute_forward_probability(engine: Engine, model: Model, sx, sy, anchors, p
                                                                   ragged_right))[0])
 
 
+def forward_pairs(engine: Engine, model: Model, x_symbols, y_symbols, x_offset, x_length, y_offset, y_length,
+                  strand) -> np.ndarray:
+    """computeForwardProbability without anchors for many (allele, read substring) pairs, as
+    the bubble graph calls it (impl/bubbleGraph.c:924), in the reference's arithmetic (see
+    mp_forward_pairs): pair j aligns x_symbols[x_offset[j]:+x_length[j]] against
+    y_symbols[y_offset[j]:+y_length[j]] with the forward (strand 1) or reverse model."""
+    xs = np.ascontiguousarray(x_symbols, dtype=np.uint16)
+    ys = np.ascontiguousarray(y_symbols, dtype=np.uint16)
+    xo = np.ascontiguousarray(x_offset, dtype=np.int64)
+    xl = np.ascontiguousarray(x_length, dtype=np.int32)
+    yo = np.ascontiguousarray(y_offset, dtype=np.int64)
+    yl = np.ascontiguousarray(y_length, dtype=np.int32)
+    st = np.ascontiguousarray(strand, dtype=np.uint8)
+    n = xo.size
+    if not (xl.size == yo.size == yl.size == st.size == n):
+        raise ValueError("one offset, length and strand per pair")
+    b = _lib.PairBatch(n, _lib.ptr(xo, ctypes.c_int64), _lib.ptr(xl, ctypes.c_int32), _lib.ptr(yo, ctypes.c_int64),
+                       _lib.ptr(yl, ctypes.c_int32), _lib.ptr(st, ctypes.c_uint8), xs.size,
+                       _lib.ptr(xs if xs.size else np.zeros(1, np.uint16), ctypes.c_uint16), ys.size,
+                       _lib.ptr(ys if ys.size else np.zeros(1, np.uint16), ctypes.c_uint16))
+    out = np.zeros(max(n, 1), dtype=np.float64)
+    _lib.check(engine._lib.mp_forward_pairs(engine.handle, model.handle, ctypes.byref(b), _lib.ptr(out, ctypes.c_double)))
+    return out[:n]
+
+
+def forward_pairs_timing(engine: Engine) -> dict:
+    """The last forward_pairs call: kernel_ms (device time of its launches), cells, pairs."""
+    ms = ctypes.c_float(0.0)
+    cells = ctypes.c_int64(0)
+    pairs = ctypes.c_int64(0)
+    _lib.check(engine._lib.mp_forward_pairs_timing(engine.handle, ctypes.byref(ms), ctypes.byref(cells),
+                                                   ctypes.byref(pairs)))
+    return {"kernel_ms": ms.value, "cells": cells.value, "pairs": pairs.value}
+
+
 @dataclass
 class Expectations:
     """Expected counts of a batch (see mp_expectations_batch): per model m (0 forward

@@ -355,6 +355,25 @@ class PolishWorkload:
     anchors: List[List[np.ndarray]]
     meta: dict = field(default_factory=dict)
 
+    def qualities(self, seed: int = 0, mean=(12.0, 3.0), spread: float = 4.0) -> List[List[np.ndarray]]:
+        """Seeded nanopore-like base qualities in the run-length form the reference keeps
+        (rleString_rleQualities, impl/polisher.c:1692-1714: each run gets the integer mean of
+        its bases' qualities): per read a phred level drawn from N(mean), per base that level
+        plus N(0, spread), clipped to [2, 40]."""
+        rng = np.random.default_rng(seed)
+        out = []
+        for chunk in self.reads:
+            lst = []
+            for r in chunk:
+                counts = np.asarray(r.counts, dtype=np.int64)
+                level = float(np.clip(rng.normal(mean[0], mean[1]), 4.0, 30.0))
+                q = np.clip(np.rint(rng.normal(level, spread, size=int(counts.sum()))), 2, 40).astype(np.int64)
+                starts = np.concatenate([[0], np.cumsum(counts)[:-1]]) if counts.size else np.zeros(0, np.int64)
+                sums = np.add.reduceat(q, starts) if counts.size else np.zeros(0, np.int64)
+                lst.append((sums // np.maximum(counts, 1)).astype(np.uint8))
+            out.append(lst)
+        return out
+
     def realign_workload(self) -> Workload:
         """The first realignment of the polishing loop as a plain workload: every read of every
         chunk against its chunk's draft with its anchors (poa_realign, impl/polisher.c:656-703)."""

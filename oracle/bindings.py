@@ -404,9 +404,10 @@ def available_reference_poa() -> bool:
 
 
 class RefPoaOracle:
-    """The reference's own POA steps (impl/polisher.c compiled unmodified, oracle/_ref/libref_poa.so):
-    poa_realign, poa_getConsensus, poa_getAnchorAlignments, the run-length estimate and
-    poa_realignAll in consensus mode."""
+    """The reference's own POA steps (impl/polisher.c and impl/bubbleGraph.c compiled unmodified,
+    oracle/_ref/libref_poa.so): poa_realign, poa_getConsensus, poa_getAnchorAlignments, the
+    run-length estimate, the bubble graph of poa_polish and poa_realignAll in consensus and
+    polish mode."""
 
     def __init__(self):
         if not os.path.exists(REF_POA_LIB):
@@ -457,6 +458,23 @@ class RefPoaOracle:
         lib.refpoa_anchor_alignments.restype = c_int64
         lib.refpoa_anchor_alignments.argtypes = [c_void_p, P(c_int64), c_int64, c_void_p, P(c_int64), P(c_int64),
                                                  c_int64]
+        lib.refpoa_params_set_polish.argtypes = [c_void_p, c_int, c_double, c_int64, c_int64, c_double, c_int64,
+                                                 c_int64, c_int64]
+        lib.refpoa_reads_set_qualities.argtypes = [c_void_p, P(c_uint8), P(c_int64)]
+        lib.refpoa_bubble_graph.restype = c_void_p
+        lib.refpoa_bubble_graph.argtypes = [c_void_p, c_void_p, c_void_p]
+        lib.refpoa_bubble_graph_destroy.argtypes = [c_void_p]
+        lib.refpoa_bubble_count.restype = c_int64
+        lib.refpoa_bubble_count.argtypes = [c_void_p]
+        lib.refpoa_bubble_info.argtypes = [c_void_p, c_int64] + [P(c_int64)] * 4
+        lib.refpoa_bubble_allele.restype = c_int64
+        lib.refpoa_bubble_allele.argtypes = [c_void_p, c_int64, c_int64, P(c_char), P(c_uint64), c_int64]
+        lib.refpoa_bubble_reads.argtypes = [c_void_p, c_int64, c_void_p, P(c_int64), P(c_int64), P(c_int64),
+                                            P(c_double)]
+        lib.refpoa_bubble_supports.argtypes = [c_void_p, c_int64, P(ctypes.c_float)]
+        lib.refpoa_bubble_consensus.restype = c_int64
+        lib.refpoa_bubble_consensus.argtypes = [c_void_p, c_void_p, P(c_uint64), P(c_char), P(c_uint64), c_int64,
+                                                P(c_int64)]
         self.lib = lib
 
     # ---- construction ----
@@ -480,6 +498,64 @@ class RefPoaOracle:
 
     def free_params(self, h):
         self.lib.refpoa_params_destroy(h)
+
+    def set_polish(self, params_h, polish):
+        """The polish-mode fields of the parameters from a PolishParams (use_read_alleles,
+        candidate_variant_weight, column_anchor_trim, filter_reads_coverage,
+        min_avg_base_quality, max_consensus_strings, min/max_polish_iterations)."""
+        self.lib.refpoa_params_set_polish(params_h, int(polish.use_read_alleles), float(polish.candidate_variant_weight),
+                                          int(polish.column_anchor_trim), int(polish.filter_reads_coverage),
+                                          float(polish.min_avg_base_quality), int(polish.max_consensus_strings),
+                                          int(polish.min_polish_iterations), int(polish.max_polish_iterations))
+
+    def set_qualities(self, reads_h, qualities):
+        """Per-run qualities of every read (a list of uint8 arrays, one per read run)."""
+        off = np.zeros(len(qualities) + 1, np.int64)
+        off[1:] = np.cumsum([len(q) for q in qualities])
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(q, np.uint8) for q in qualities])
+                                    if off[-1] else np.zeros(1, np.uint8))
+        self.lib.refpoa_reads_set_qualities(reads_h, _p(flat, c_uint8), _p(off, c_int64))
+
+    def bubble_graph(self, poa, reads_h, params_h):
+        """bubbleGraph_constructFromPoa, exported: a list of bubbles, each a dict with ref_start,
+        ref_length, alleles (list of (chars, counts)), reads (rows read, start, length), quals
+        and supports (alleles x reads, float32); plus the consensus path, the new consensus and
+        the POA-to-consensus map of bubbleGraph_getConsensusPath / getConsensusString."""
+        from ctypes import c_float
+        bg = self.lib.refpoa_bubble_graph(poa, reads_h, params_h)
+        out = []
+        for i in range(self.lib.refpoa_bubble_count(bg)):
+            v = [c_int64() for _ in range(4)]
+            self.lib.refpoa_bubble_info(bg, i, *[ctypes.byref(x) for x in v])
+            ref_start, ref_len, n_al, n_rd = (x.value for x in v)
+            alleles = []
+            for j in range(n_al):
+                n = self.lib.refpoa_bubble_allele(bg, i, j, None, None, 0)
+                chars = (self._c_char * max(n, 1))()
+                counts = np.zeros(max(n, 1), np.uint64)
+                self.lib.refpoa_bubble_allele(bg, i, j, chars, _p(counts, self._c_uint64), n)
+                alleles.append((bytes(chars[:n]), counts[:n].copy()))
+            rd = np.zeros((3, max(n_rd, 1)), np.int64)
+            q = np.zeros(max(n_rd, 1), np.float64)
+            self.lib.refpoa_bubble_reads(bg, i, reads_h, _p(rd[0], c_int64), _p(rd[1], c_int64), _p(rd[2], c_int64),
+                                         _p(q, c_double))
+            sup = np.zeros(max(n_al * n_rd, 1), np.float32)
+            self.lib.refpoa_bubble_supports(bg, i, _p(sup, c_float))
+            out.append(dict(ref_start=ref_start, ref_length=ref_len, alleles=alleles,
+                            reads=rd[:, :n_rd].T.copy(), quals=q[:n_rd].copy(),
+                            supports=sup[:n_al * n_rd].reshape(n_al, n_rd).copy()))
+        n_nodes = self.lib.refpoa_node_count(poa)
+        path = np.zeros(max(len(out), 1), np.uint64)
+        cap = 4 * n_nodes + 64
+        chars = (self._c_char * cap)()
+        counts = np.zeros(cap, np.uint64)
+        node_map = np.zeros(max(n_nodes - 1, 1), np.int64)
+        n = self.lib.refpoa_bubble_consensus(bg, params_h, _p(path, self._c_uint64), chars,
+                                             _p(counts, self._c_uint64), cap, _p(node_map, c_int64))
+        assert n <= cap
+        self.lib.refpoa_bubble_graph_destroy(bg)
+        return dict(bubbles=out, path=path[:len(out)].astype(np.int64), chars=bytes(chars[:n]),
+                    counts=counts[:n].copy(), map=node_map[:n_nodes - 1].copy())
 
     def reads(self, rle_reads, strands):
         from ctypes import c_uint32

@@ -10,9 +10,11 @@
  * loop with the reference's node weights, indels, anchors and consensus. Only tests/
  * load it, as the checker.
  *
- * The bubble-graph polish (poa_polish) is not part of this oracle: its functions, which
- * live in impl/bubbleGraph.c, are stand-ins that abort, and the loop is run with
- * maxRealignmentPolishIterations = 0.
+ * impl/bubbleGraph.c is compiled in as well, so the polish mode of the loop (poa_polish:
+ * bubbleGraph_constructFromPoa, the allele choice and the new consensus string) runs as the
+ * reference wrote it; its bubbles, read substrings, alleles and allele supports are exported
+ * for the tests. The diploid phasing functions that file also holds call into impl/hmm.c and
+ * its neighbours, which are not compiled: their stand-ins below abort.
  */
 #include "margin.h"
 
@@ -34,25 +36,75 @@ RepeatSubMatrix *refo_model_repeat_matrix(void *handle);
 /* defined in impl/polisher.c without a prototype in inc/margin.h */
 double poa_getTotalErrorWeight(Poa *poa);
 
-/* ---- bubble-graph functions named by impl/polisher.c; never reached in consensus mode ---- */
-BubbleGraph *bubbleGraph_constructFromPoa(Poa *poa, stList *bamChunkReads, PolishParams *params) {
-    (void) poa, (void) bamChunkReads, (void) params;
-    st_errAbort("bubble graph polish is not part of the POA oracle");
+/* ---- phasing functions named by impl/bubbleGraph.c: the diploid phasing (impl/hmm.c and
+ * its neighbours) is not part of this oracle, so these stand-ins abort if ever reached ---- */
+#define PHASING_ONLY(name) st_errAbort("%s: phasing is not part of the POA oracle", name)
+
+stGenomeFragment *stGenomeFragment_construct(stRPHmm *hmm, stList *path) {
+    (void) hmm, (void) path;
+    PHASING_ONLY("stGenomeFragment_construct");
     return NULL;
 }
-void bubbleGraph_destruct(BubbleGraph *bg) {
-    (void) bg;
-}
-uint64_t *bubbleGraph_getConsensusPath(BubbleGraph *bg, PolishParams *polishParams) {
-    (void) bg, (void) polishParams;
-    st_errAbort("bubble graph polish is not part of the POA oracle");
+stGenomeFragment *stGenomeFragment_constructEmpty(stReference *ref, uint64_t refStart, uint64_t length, stSet *reads1,
+                                                  stSet *reads2) {
+    (void) ref, (void) refStart, (void) length, (void) reads1, (void) reads2;
+    PHASING_ONLY("stGenomeFragment_constructEmpty");
     return NULL;
 }
-RleString *bubbleGraph_getConsensusString(BubbleGraph *bg, uint64_t *consensusPath, int64_t **poaToConsensusMap,
-                                          PolishParams *polishParams) {
-    (void) bg, (void) consensusPath, (void) poaToConsensusMap, (void) polishParams;
-    st_errAbort("bubble graph polish is not part of the POA oracle");
+void stGenomeFragment_refineGenomeFragment(stGenomeFragment *gF, stRPHmm *hmm, stList *path, int64_t maxIterations) {
+    (void) gF, (void) hmm, (void) path, (void) maxIterations;
+    PHASING_ONLY("stGenomeFragment_refineGenomeFragment");
+}
+stProfileSeq *stProfileSeq_constructEmptyProfile(stReference *ref, char *readId, int64_t referenceStart,
+                                                 int64_t length) {
+    (void) ref, (void) readId, (void) referenceStart, (void) length;
+    PHASING_ONLY("stProfileSeq_constructEmptyProfile");
     return NULL;
+}
+void stProfileSeq_destruct(stProfileSeq *seq) {
+    (void) seq;
+    PHASING_ONLY("stProfileSeq_destruct");
+}
+void stRPHmm_forwardBackward(stRPHmm *hmm) {
+    (void) hmm;
+    PHASING_ONLY("stRPHmm_forwardBackward");
+}
+stList *stRPHmm_forwardTraceBack(stRPHmm *hmm) {
+    (void) hmm;
+    PHASING_ONLY("stRPHmm_forwardTraceBack");
+    return NULL;
+}
+stList *getRPHmms(stList *profileSeqs, stRPHmmParameters *params) {
+    (void) profileSeqs, (void) params;
+    PHASING_ONLY("getRPHmms");
+    return NULL;
+}
+stList *filterReadsByCoverageDepth(stList *profileSeqs, stRPHmmParameters *params, stList *filteredProfileSeqs,
+                                   stList *discardedProfileSeqs) {
+    (void) profileSeqs, (void) params, (void) filteredProfileSeqs, (void) discardedProfileSeqs;
+    PHASING_ONLY("filterReadsByCoverageDepth");
+    return NULL;
+}
+stRPHmm *fuseTilingPath(stList *tilingPath) {
+    (void) tilingPath;
+    PHASING_ONLY("fuseTilingPath");
+    return NULL;
+}
+stList *mergeTwoTilingPaths(stList *tilingPath1, stList *tilingPath2) {
+    (void) tilingPath1, (void) tilingPath2;
+    PHASING_ONLY("mergeTwoTilingPaths");
+    return NULL;
+}
+double getLogProbOfReadGivenHaplotype(uint64_t *haplotypeString, int64_t start, int64_t length,
+                                      stProfileSeq *profileSeq, stReference *ref) {
+    (void) haplotypeString, (void) start, (void) length, (void) profileSeq, (void) ref;
+    PHASING_ONLY("getLogProbOfReadGivenHaplotype");
+    return 0.0;
+}
+int popcount64(uint64_t x) {
+    (void) x;
+    PHASING_ONLY("popcount64");
+    return 0;
 }
 
 /* ---- construction ---- */
@@ -106,9 +158,26 @@ void refpoa_params_destroy(void *handle) {
     free(pp);
 }
 
+/* The polish-mode parameters of poa_polish (impl/bubbleGraph.c:800-978) and the number of
+ * polish iterations poa_realignAll runs after the consensus iterations (impl/polisher.c:2123-2126). */
+void refpoa_params_set_polish(void *handle, int useReadAlleles, double candidateVariantWeight, int64_t columnAnchorTrim,
+                              int64_t filterReadsWhileHaveAtLeastThisCoverage, double minAvgBaseQuality,
+                              int64_t maxConsensusStrings, int64_t minPolishIterations, int64_t maxPolishIterations) {
+    PolishParams *pp = handle;
+    pp->useReadAlleles = useReadAlleles != 0;
+    pp->candidateVariantWeight = candidateVariantWeight;
+    pp->columnAnchorTrim = (uint64_t) columnAnchorTrim;
+    pp->filterReadsWhileHaveAtLeastThisCoverage = (uint64_t) filterReadsWhileHaveAtLeastThisCoverage;
+    pp->minAvgBaseQuality = minAvgBaseQuality;
+    pp->maxConsensusStrings = (uint64_t) maxConsensusStrings;
+    pp->minRealignmentPolishIterations = (uint64_t) minPolishIterations;
+    pp->maxRealignmentPolishIterations = (uint64_t) maxPolishIterations;
+}
+
 static void readDestruct(void *p) {
     BamChunkRead *r = p;
     rleString_destruct(r->rleRead);
+    free(r->qualities);
     free(r);
 }
 
@@ -123,6 +192,18 @@ void *refpoa_reads_create(int64_t n, const char *chars, const uint32_t *counts, 
         stList_append(reads, r);
     }
     return reads;
+}
+
+/* Per-run quality values of every read (the run-length form rleString_rleQualities makes,
+ * impl/polisher.c:1692-1714), laid end to end like the reads' runs. */
+void refpoa_reads_set_qualities(void *reads, const uint8_t *qualities, const int64_t *offsets) {
+    for (int64_t i = 0; i < stList_length(reads); i++) {
+        BamChunkRead *r = stList_get(reads, i);
+        free(r->qualities);
+        int64_t n = offsets[i + 1] - offsets[i];
+        r->qualities = st_calloc(n > 0 ? n : 1, 1);
+        memcpy(r->qualities, qualities + offsets[i], (size_t) n);
+    }
 }
 
 void refpoa_reads_destroy(void *reads) {
@@ -317,4 +398,88 @@ int64_t refpoa_anchor_alignments(void *handle, const int64_t *map, int64_t nRead
     }
     stList_destruct(a);
     return k;
+}
+
+/* ---- the polish mode: bubble graph, allele choice, new consensus ---- */
+
+/* bubbleGraph_constructFromPoa (impl/bubbleGraph.c:800-978); sorts the POA's observations
+ * in place as the reference does. */
+void *refpoa_bubble_graph(void *poa, void *reads, void *params) {
+    return bubbleGraph_constructFromPoa(poa, reads, params);
+}
+
+void refpoa_bubble_graph_destroy(void *bg) {
+    bubbleGraph_destruct(bg);
+}
+
+int64_t refpoa_bubble_count(void *handle) {
+    return (int64_t) ((BubbleGraph *) handle)->bubbleNo;
+}
+
+/* Bubble i: reference start, reference allele length (runs), allele and read counts. */
+void refpoa_bubble_info(void *handle, int64_t i, int64_t *refStart, int64_t *refAlleleLength, int64_t *alleleNo,
+                        int64_t *readNo) {
+    Bubble *b = &((BubbleGraph *) handle)->bubbles[i];
+    *refStart = (int64_t) b->refStart;
+    *refAlleleLength = (int64_t) b->refAllele->length;
+    *alleleNo = (int64_t) b->alleleNo;
+    *readNo = (int64_t) b->readNo;
+}
+
+/* Allele j of bubble i as a run-length string; returns its run count (copies at most cap). */
+int64_t refpoa_bubble_allele(void *handle, int64_t i, int64_t j, char *chars, uint64_t *counts, int64_t cap) {
+    RleString *a = ((BubbleGraph *) handle)->bubbles[i].alleles[j];
+    for (int64_t k = 0; k < (int64_t) a->length && k < cap; k++) {
+        chars[k] = a->rleString[k];
+        counts[k] = a->repeatCounts[k];
+    }
+    return (int64_t) a->length;
+}
+
+/* The read substrings of bubble i in the bubble's order: read index in `reads`, start and
+ * length in the read's runs, and the mean quality (-1 without qualities). */
+void refpoa_bubble_reads(void *handle, int64_t i, void *reads, int64_t *readNo, int64_t *start, int64_t *length,
+                         double *qual) {
+    Bubble *b = &((BubbleGraph *) handle)->bubbles[i];
+    for (int64_t k = 0; k < (int64_t) b->readNo; k++) {
+        BamChunkReadSubstring *rs = b->reads[k];
+        readNo[k] = -1;
+        for (int64_t r = 0; r < stList_length(reads); r++) {
+            if (stList_get(reads, r) == rs->read) {
+                readNo[k] = r;
+                break;
+            }
+        }
+        start[k] = (int64_t) rs->start;
+        length[k] = (int64_t) rs->length;
+        qual[k] = rs->qualValue;
+    }
+}
+
+/* The allele supports of bubble i: alleleNo x readNo log-likelihoods (float, allele-major). */
+void refpoa_bubble_supports(void *handle, int64_t i, float *out) {
+    Bubble *b = &((BubbleGraph *) handle)->bubbles[i];
+    memcpy(out, b->alleleReadSupports, sizeof(float) * b->alleleNo * b->readNo);
+}
+
+/* bubbleGraph_getConsensusPath then bubbleGraph_getConsensusString: the chosen allele of every
+ * bubble (path, bubbleNo entries), the new consensus (returns its run count; copies at most
+ * cap runs) and the POA-to-consensus map (reference length entries). */
+int64_t refpoa_bubble_consensus(void *handle, void *params, uint64_t *path, char *chars, uint64_t *counts, int64_t cap,
+                                int64_t *map) {
+    BubbleGraph *bg = handle;
+    uint64_t *p = bubbleGraph_getConsensusPath(bg, params);
+    memcpy(path, p, sizeof(uint64_t) * bg->bubbleNo);
+    int64_t *m = NULL;
+    RleString *c = bubbleGraph_getConsensusString(bg, p, &m, params);
+    int64_t n = (int64_t) c->length;
+    for (int64_t k = 0; k < n && k < cap; k++) {
+        chars[k] = c->rleString[k];
+        counts[k] = c->repeatCounts[k];
+    }
+    memcpy(map, m, sizeof(int64_t) * bg->refString->length);
+    free(m);
+    free(p);
+    rleString_destruct(c);
+    return n;
 }

@@ -105,14 +105,37 @@ void stSortedSet_destruct(stSortedSet *set);
 void stSortedSet_insert(stSortedSet *set, void *object);
 void *stSortedSet_search(stSortedSet *set, void *object);
 
-/* ---- stHash keyed by pointer value ---- */
+/* ---- stHash: keyed by pointer value, or by the caller's hash and equality functions
+ * (construct3, as impl/bubbleGraph.c:728 and :905 use it). Iteration visits the keys in
+ * insertion order; sonLib's own table visits them in bucket order, which only decides
+ * the order of equal-likelihood alleles in the bubble graph. ---- */
 stHash *stHash_construct(void);
+stHash *stHash_construct2(void (*destructKeys)(void *), void (*destructValues)(void *));
+stHash *stHash_construct3(uint64_t (*hashKey)(const void *), int (*hashEqualsKey)(const void *, const void *),
+                          void (*destructKeys)(void *), void (*destructValues)(void *));
 void stHash_destruct(stHash *hash);
 void stHash_insert(stHash *hash, void *key, void *value);
+void *stHash_search(stHash *hash, void *key);
 void *stHash_remove(stHash *hash, void *key);
+stHashIterator *stHash_getIterator(stHash *hash);
+void *stHash_getNext(stHashIterator *iterator);
+void stHash_destructIterator(stHashIterator *iterator);
+stList *stHash_getValues(stHash *hash);
+uint64_t stHash_stringKey(const char *k);
 
-/* ---- stSet: named by phasing code the oracle never runs ---- */
+/* ---- stSet and stMath_logAddExact: named by the phasing code of impl/bubbleGraph.c, which
+ * the oracle never runs (they abort) ---- */
+stSet *stSet_construct(void);
+void stSet_destruct(stSet *set);
+void stSet_insert(stSet *set, void *object);
 void *stSet_search(stSet *set, void *object);
+int64_t stSet_size(stSet *set);
+stSet *stSet_getIntersection(stSet *set1, stSet *set2);
+stSetIterator *stSet_getIterator(stSet *set);
+void *stSet_getNext(stSetIterator *iterator);
+void stSet_destructIterator(stSetIterator *iterator);
+stSet *stList_getSet(stList *list);
+double stMath_logAddExact(double logX, double logY);
 
 /* ---- more strings ---- */
 char *stString_getSubString(const char *cA, int64_t start, int64_t length);

@@ -426,16 +426,30 @@ void *stSortedSet_search(stSortedSet *set, void *object) {
     return (i < set->length && set->cmp(set->items[i], object) == 0) ? set->items[i] : NULL;
 }
 
-/* ---------------- stHash (pointer keys, linear probing) ---------------- */
+/* ---------------- stHash (linear probing; insertion-ordered iteration) ----------------
+ * Keys hash by pointer value unless construct3 gives a hash and an equality function.
+ * Every key also sits in `order` (insertion order, removed keys taken out), which is
+ * the order the iterator visits. */
 
 struct _stHash {
     void **keys;
     void **values;
     char *used;
     int64_t size, count;
+    uint64_t (*hashKey)(const void *);
+    int (*equalKeys)(const void *, const void *);
+    void (*destructKeys)(void *);
+    void (*destructValues)(void *);
+    void **order;
+    int64_t orderLength, orderCap;
 };
 
-stHash *stHash_construct(void) {
+struct _stHashIterator {
+    stHash *hash;
+    int64_t next;
+};
+
+static stHash *hashAlloc(void) {
     stHash *h = st_calloc(1, sizeof(stHash));
     h->size = 64;
     h->keys = st_calloc(h->size, sizeof(void *));
@@ -444,26 +458,75 @@ stHash *stHash_construct(void) {
     return h;
 }
 
+stHash *stHash_construct(void) {
+    return hashAlloc();
+}
+
+stHash *stHash_construct2(void (*destructKeys)(void *), void (*destructValues)(void *)) {
+    stHash *h = hashAlloc();
+    h->destructKeys = destructKeys;
+    h->destructValues = destructValues;
+    return h;
+}
+
+stHash *stHash_construct3(uint64_t (*hashKey)(const void *), int (*hashEqualsKey)(const void *, const void *),
+                          void (*destructKeys)(void *), void (*destructValues)(void *)) {
+    stHash *h = stHash_construct2(destructKeys, destructValues);
+    h->hashKey = hashKey;
+    h->equalKeys = hashEqualsKey;
+    return h;
+}
+
 void stHash_destruct(stHash *hash) {
     if (hash == NULL) {
         return;
     }
+    for (int64_t i = 0; i < hash->size; i++) {
+        if (hash->used[i]) {
+            if (hash->destructKeys != NULL) {
+                hash->destructKeys(hash->keys[i]);
+            }
+            if (hash->destructValues != NULL) {
+                hash->destructValues(hash->values[i]);
+            }
+        }
+    }
     free(hash->keys);
     free(hash->values);
     free(hash->used);
+    free(hash->order);
     free(hash);
 }
 
+static int sameKey(stHash *h, void *a, void *b) {
+    return h->equalKeys != NULL ? h->equalKeys(a, b) != 0 : a == b;
+}
+
 static int64_t hashSlot(stHash *h, void *key) {
-    uint64_t x = (uint64_t) (uintptr_t) key * 0x9E3779B97F4A7C15ull;
+    uint64_t x = h->hashKey != NULL ? h->hashKey(key) : (uint64_t) (uintptr_t) key;
+    x *= 0x9E3779B97F4A7C15ull;
     int64_t i = (int64_t) (x >> 17) & (h->size - 1);
-    while (h->used[i] && h->keys[i] != key) {
+    while (h->used[i] && !sameKey(h, h->keys[i], key)) {
         i = (i + 1) & (h->size - 1);
     }
     return i;
 }
 
+/* places a key that is not in the table (no order bookkeeping) */
+static void hashPlace(stHash *hash, void *key, void *value) {
+    int64_t i = hashSlot(hash, key);
+    hash->used[i] = 1;
+    hash->keys[i] = key;
+    hash->values[i] = value;
+    hash->count++;
+}
+
 void stHash_insert(stHash *hash, void *key, void *value) {
+    int64_t i = hashSlot(hash, key);
+    if (hash->used[i]) {
+        hash->values[i] = value;
+        return;
+    }
     if (2 * (hash->count + 1) > hash->size) {
         stHash old = *hash;
         hash->size *= 2;
@@ -471,22 +534,29 @@ void stHash_insert(stHash *hash, void *key, void *value) {
         hash->keys = st_calloc(hash->size, sizeof(void *));
         hash->values = st_calloc(hash->size, sizeof(void *));
         hash->used = st_calloc(hash->size, 1);
-        for (int64_t i = 0; i < old.size; i++) {
-            if (old.used[i]) {
-                stHash_insert(hash, old.keys[i], old.values[i]);
+        for (int64_t k = 0; k < old.size; k++) {
+            if (old.used[k]) {
+                hashPlace(hash, old.keys[k], old.values[k]);
             }
         }
         free(old.keys);
         free(old.values);
         free(old.used);
     }
-    int64_t i = hashSlot(hash, key);
-    if (!hash->used[i]) {
-        hash->used[i] = 1;
-        hash->keys[i] = key;
-        hash->count++;
+    hashPlace(hash, key, value);
+    if (hash->orderLength == hash->orderCap) {
+        hash->orderCap = hash->orderCap ? 2 * hash->orderCap : 16;
+        hash->order = realloc(hash->order, sizeof(void *) * (size_t) hash->orderCap);
+        if (hash->order == NULL) {
+            st_errAbort("stHash: out of memory");
+        }
     }
-    hash->values[i] = value;
+    hash->order[hash->orderLength++] = key;
+}
+
+void *stHash_search(stHash *hash, void *key) {
+    int64_t i = hashSlot(hash, key);
+    return hash->used[i] ? hash->values[i] : NULL;
 }
 
 void *stHash_remove(stHash *hash, void *key) {
@@ -495,7 +565,15 @@ void *stHash_remove(stHash *hash, void *key) {
         return NULL;
     }
     void *v = hash->values[i];
-    /* re-insert the rest of the probe run */
+    void *stored = hash->keys[i];
+    for (int64_t k = 0; k < hash->orderLength; k++) {
+        if (hash->order[k] == stored) {
+            memmove(hash->order + k, hash->order + k + 1, sizeof(void *) * (size_t) (hash->orderLength - k - 1));
+            hash->orderLength--;
+            break;
+        }
+    }
+    /* re-place the rest of the probe run */
     hash->used[i] = 0;
     hash->count--;
     int64_t j = (i + 1) & (hash->size - 1);
@@ -503,17 +581,97 @@ void *stHash_remove(stHash *hash, void *key) {
         void *k = hash->keys[j], *val = hash->values[j];
         hash->used[j] = 0;
         hash->count--;
-        stHash_insert(hash, k, val);
+        hashPlace(hash, k, val);
         j = (j + 1) & (hash->size - 1);
     }
     return v;
 }
 
-void *stSet_search(stSet *set, void *object) {
-    (void) set;
-    (void) object;
-    st_errAbort("stSet_search: not part of the oracle's path");
+stHashIterator *stHash_getIterator(stHash *hash) {
+    stHashIterator *it = st_calloc(1, sizeof(stHashIterator));
+    it->hash = hash;
+    return it;
+}
+
+void *stHash_getNext(stHashIterator *iterator) {
+    return iterator->next < iterator->hash->orderLength ? iterator->hash->order[iterator->next++] : NULL;
+}
+
+void stHash_destructIterator(stHashIterator *iterator) {
+    free(iterator);
+}
+
+stList *stHash_getValues(stHash *hash) {
+    stList *l = stList_construct();
+    for (int64_t k = 0; k < hash->orderLength; k++) {
+        stList_append(l, stHash_search(hash, hash->order[k]));
+    }
+    return l;
+}
+
+/* FNV-1a over the string's bytes */
+uint64_t stHash_stringKey(const char *k) {
+    uint64_t h = 1469598103934665603ull;
+    for (const unsigned char *c = (const unsigned char *) k; *c; c++) {
+        h = (h ^ *c) * 1099511628211ull;
+    }
+    return h;
+}
+
+/* ---------------- stSet, stMath_logAddExact: phasing only ---------------- */
+
+#define PHASING_ONLY(name) st_errAbort("%s: phasing is not part of the oracle", name)
+
+stSet *stSet_construct(void) {
+    PHASING_ONLY("stSet_construct");
     return NULL;
+}
+void stSet_destruct(stSet *set) {
+    (void) set;
+    PHASING_ONLY("stSet_destruct");
+}
+void stSet_insert(stSet *set, void *object) {
+    (void) set, (void) object;
+    PHASING_ONLY("stSet_insert");
+}
+void *stSet_search(stSet *set, void *object) {
+    (void) set, (void) object;
+    PHASING_ONLY("stSet_search");
+    return NULL;
+}
+int64_t stSet_size(stSet *set) {
+    (void) set;
+    PHASING_ONLY("stSet_size");
+    return 0;
+}
+stSet *stSet_getIntersection(stSet *set1, stSet *set2) {
+    (void) set1, (void) set2;
+    PHASING_ONLY("stSet_getIntersection");
+    return NULL;
+}
+stSetIterator *stSet_getIterator(stSet *set) {
+    (void) set;
+    PHASING_ONLY("stSet_getIterator");
+    return NULL;
+}
+void *stSet_getNext(stSetIterator *iterator) {
+    (void) iterator;
+    PHASING_ONLY("stSet_getNext");
+    return NULL;
+}
+void stSet_destructIterator(stSetIterator *iterator) {
+    (void) iterator;
+    PHASING_ONLY("stSet_destructIterator");
+}
+stSet *stList_getSet(stList *list) {
+    (void) list;
+    PHASING_ONLY("stList_getSet");
+    return NULL;
+}
+double stMath_logAddExact(double logX, double logY) {
+    (void) logX, (void) logY;
+    PHASING_ONLY("stMath_logAddExact");
+    return 0.0;
 }
 
 /* ---------------- strings ---------------- */

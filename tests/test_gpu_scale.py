@@ -200,3 +200,59 @@ def test_consensus_of_a_110kb_chunk(engine, gmodel, polish_model, ref_oracle, re
     print(f"110 kb chunk: {len(ref_chars)} runs, identical bases; run lengths differ from the reference's at "
           f"{diff.size} runs {diff[:10].tolist()} (the reference's approximate posteriors)")
     assert diff.size <= max(1, len(ref_chars) // 10000)
+
+
+def _run_differences(a: bytes, ac, b: bytes, bc, window: int = 24):
+    """Runs where two nearly equal run-length strings differ: walk both, and at a mismatch (base
+    or run length) resynchronise on the smallest shift that makes the next `window` runs agree.
+    Returns the number of differing runs."""
+    i = j = diffs = 0
+    while i < len(a) and j < len(b):
+        if a[i] == b[j] and ac[i] == bc[j]:
+            i += 1
+            j += 1
+            continue
+        diffs += 1
+        best = None
+        for di in range(0, 8):
+            for dj in range(0, 8):
+                if (di, dj) == (0, 0):
+                    continue
+                if a[i + di:i + di + window] == b[j + dj:j + dj + window]:
+                    if best is None or di + dj < sum(best):
+                        best = (di, dj)
+        if best is None:
+            best = (1, 1)
+        i += best[0]
+        j += best[1]
+    return diffs + (len(a) - i) + (len(b) - j)
+
+
+def test_shipped_polish_of_a_110kb_chunk(engine, gmodel, polish_model):
+    """The shipped loop (poa_realignAll with one polish iteration: bubble graph, allele scores in
+    the reference's arithmetic, new consensus, realignment; then the run-length estimate) on the
+    110 kb chunk at 50x with base qualities, against the reference's own loop on the same chunk
+    (tests/golden/polish_110kb.npz). The two differ only where the GPU's posteriors and the
+    reference's approximate ones tip a near-tie of the graph's weights."""
+    path = os.path.join(GOLDEN, "polish_110kb.npz")
+    if not os.path.exists(path):
+        pytest.skip("polish fixture not generated")
+    import importlib.util
+    from marginpolish_b200 import polish
+    spec = importlib.util.spec_from_file_location("mpg", os.path.join(GOLDEN, "make_polish_golden.py"))
+    mpg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mpg)
+    z = np.load(path)
+    wl, quals, base_digest = mpg.chunk_workload()
+    assert mpg.digest(wl, quals, base_digest) == str(z["digest"]), \
+        "the seeded generator no longer makes the fixture's inputs"
+    want_chars, want_counts = z["chars"].tobytes(), z["counts"].astype(np.uint32)
+    got = polish(engine, gmodel, polish_model, PolishParams.shipped(), wl.drafts, wl.reads, wl.strands, wl.anchors,
+                 quals)[0]
+    draft = wl.drafts[0]
+    changed_by_ref = _run_differences(draft.chars, draft.counts, want_chars, want_counts)
+    diffs = _run_differences(got.chars, got.counts, want_chars, want_counts)
+    print(f"110 kb chunk, shipped loop: reference {len(want_chars)} runs ({changed_by_ref} runs changed from the "
+          f"draft), GPU {len(got)} runs, {diffs} runs differ from the reference")
+    assert changed_by_ref > 20
+    assert diffs <= max(2, changed_by_ref // 20)

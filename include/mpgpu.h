@@ -352,15 +352,18 @@ mp_status mp_expectations_batch(mp_engine *e, const mp_model *m, const mp_params
 
 /* ---- the POA loop: poa_realign / poa_realignIterative / poa_realignAll ----
  * A set of chunks, each a draft (run-length string) with its reads, runs the reference's
- * polishing loop in consensus mode (impl/polisher.c): every read is realigned to its chunk's
- * reference and folded into the chunk's partial-order graph (poa_realign, :656-703, with
- * poa_augment, :316-534), the consensus walk proposes a new reference (poa_getConsensus,
- * :1025-1275), high-posterior observations become the next anchors
+ * polishing loop (impl/polisher.c): every read is realigned to its chunk's reference and
+ * folded into the chunk's partial-order graph (poa_realign, :656-703, with poa_augment,
+ * :316-534); a new reference is proposed by the consensus walk (consensus mode,
+ * poa_getConsensus, :1025-1275) or by the bubble graph (polish mode, poa_polish, :2008-2031:
+ * candidate alleles between anchor nodes scored against every read substring,
+ * impl/bubbleGraph.c:800-978); high-posterior observations become the next anchors
  * (poa_getAnchorAlignments, :536-592), the run lengths are re-estimated
  * (poa_estimateRepeatCountsUsingBayesianModel, :1556-1565) and the loop stops on an
- * unchanged consensus or a score that does not improve (poa_realignIterative, :2034-2106).
+ * unchanged reference or a score that does not improve (poa_realignIterative, :2034-2106).
  * All chunks advance together: each iteration's realignments of every chunk are one batched
- * posterior pass on the GPU; graph work runs on host threads, one chunk per thread. */
+ * posterior pass on the GPU, and all bubble scores one mp_forward_pairs call; graph work runs
+ * on host threads, one chunk per thread. */
 typedef struct {
     double reference_base_penalty;   /* referenceBasePenalty (0.5 shipped) */
     int32_t compare_repeat_counts;   /* poaConstructCompareRepeatCounts */

@@ -31,6 +31,7 @@
 #include "mp_host.h"
 #include "mp_internal.h"
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -50,46 +51,51 @@ namespace {
 
 constexpr double kLogZero = -INFINITY;
 
-// lookup() of impl/pairwiseAligner.c:282-293 for 0 <= d < 7.5, each operation rounded alone.
-__device__ __forceinline__ double lookupCubic(double d) {
-    double c3, c2, c1, c0;
-    if (d <= (double) 1.00f) {
-        c3 = (double) -0.009350833524763f;
-        c2 = (double) 0.130659527668286f;
-        c1 = (double) 0.498799810682272f;
-        c0 = (double) 0.693203116424741f;
-    } else if (d <= (double) 2.50f) {
-        c3 = (double) -0.014532321752540f;
-        c2 = (double) 0.139942324101744f;
-        c1 = (double) 0.495635523139337f;
-        c0 = (double) 0.692140569840976f;
-    } else if (d <= (double) 4.50f) {
-        c3 = (double) -0.004605031767994f;
-        c2 = (double) 0.063427417320019f;
-        c1 = (double) 0.695956496475118f;
-        c0 = (double) 0.514272634594009f;
-    } else {
-        c3 = (double) -0.000458661602210f;
-        c2 = (double) 0.009695946122598f;
-        c1 = (double) 0.930734667215156f;
-        c0 = (double) 0.168037164329057f;
-    }
-    double v = __dmul_rn(c3, d);
-    v = __dadd_rn(v, c2);
-    v = __dmul_rn(v, d);
-    v = __dadd_rn(v, c1);
-    v = __dmul_rn(v, d);
-    return __dadd_rn(v, c0);
+// The cubic of impl/pairwiseAligner.c:282-293, piece by piece: (c3, c2), (c1, c0) for d <= 1,
+// d <= 2.5, d <= 4.5 and beyond, the coefficients as the reference writes them (single-precision
+// literals, widened to double).
+__constant__ double2 kCubic[8] = {
+    {(double) -0.009350833524763f, (double) 0.130659527668286f}, {(double) 0.498799810682272f, (double) 0.693203116424741f},
+    {(double) -0.014532321752540f, (double) 0.139942324101744f}, {(double) 0.495635523139337f, (double) 0.692140569840976f},
+    {(double) -0.004605031767994f, (double) 0.063427417320019f}, {(double) 0.695956496475118f, (double) 0.514272634594009f},
+    {(double) -0.000458661602210f, (double) 0.009695946122598f}, {(double) 0.930734667215156f, (double) 0.168037164329057f},
+};
+
+// What a block keeps in shared memory: the cubic and both strands' models.
+struct Tables {
+    double2 cubic[8];
+    DevLogModel models[2];
+};
+
+__device__ __forceinline__ void loadTables(Tables &T, const DevLogModel *models) {
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(models);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(T.models);
+    for (int i = threadIdx.x; i < (int) (2 * sizeof(DevLogModel) / 4); i += blockDim.x) dst[i] = src[i];
+    if (threadIdx.x < 8) T.cubic[threadIdx.x] = kCubic[threadIdx.x];
+    __syncthreads();
 }
 
-// logAdd of impl/pairwiseAligner.c:295-299.
-__device__ __forceinline__ double logAdd(double x, double y) {
-    if (x < y) {
-        const double d = __dsub_rn(y, x);
-        return (x == kLogZero || d >= 7.5) ? y : __dadd_rn(lookupCubic(d), x);
-    }
-    const double d = __dsub_rn(x, y);
-    return (y == kLogZero || d >= 7.5) ? x : __dadd_rn(lookupCubic(d), y);
+// lookup() for 0 <= d < 7.5: the piece picked by comparisons (the reference's if-chain), its
+// coefficients read from the table, every operation rounded alone.
+__device__ __forceinline__ double lookupCubic(const Tables &T, double d) {
+    const int piece = (d > (double) 1.00f) + (d > (double) 2.50f) + (d > (double) 4.50f);
+    const double2 hi = T.cubic[2 * piece], lo = T.cubic[2 * piece + 1];
+    double v = __dmul_rn(hi.x, d);
+    v = __dadd_rn(v, hi.y);
+    v = __dmul_rn(v, d);
+    v = __dadd_rn(v, lo.x);
+    v = __dmul_rn(v, d);
+    return __dadd_rn(v, lo.y);
+}
+
+// logAdd of impl/pairwiseAligner.c:295-299 without branches: a is the term the reference keeps
+// (y when x < y, else x), b the other; both of its branches compute lookup(a - b) + b.
+__device__ __forceinline__ double logAdd(const Tables &T, double x, double y) {
+    const bool lt = x < y;
+    const double a = lt ? y : x, b = lt ? x : y;
+    const double d = __dsub_rn(a, b);
+    const double r = __dadd_rn(lookupCubic(T, d), b);
+    return (b == kLogZero || d >= 7.5) ? a : r;
 }
 
 // f + (e + t): the term doTransitionForward adds (impl/pairwiseAligner.c:311-314).
@@ -102,8 +108,63 @@ __device__ __forceinline__ int baseOf(uint16_t s, int runLength) {
     return b >= 4 ? 4 : b;
 }
 
+// One cell of stateMachine3_cellCalculate (impl/stateMachine.c:559-581) with doTransitionForward:
+// lower (gap-x from (x-1, y)), middle (match from (x-1, y-1)), upper (gap-y from (x, y-1)); a
+// missing neighbour leaves its state at LOG_ZERO. The first term of a state needs no log-sum
+// (logAdd(LOG_ZERO, v) = v); without switch transitions (SW false) their terms are log 0 and
+// leave the sum unchanged, so they are skipped.
+template <bool SW>
+__device__ __forceinline__ void cellForward(const Tables &T, const DevLogModel &m, bool lower, bool middle, bool upper,
+                                            double eX, double eM, double eY, const double *l, const double *d,
+                                            const double *u, double *c) {
+    c[0] = c[1] = c[2] = kLogZero;
+    if (lower) {
+        double v = term(l[0], eX, m.t[1]);
+        v = logAdd(T, v, term(l[1], eX, m.t[4]));
+        if (SW) v = logAdd(T, v, term(l[2], eX, m.t[7]));
+        c[1] = v;
+    }
+    if (middle) {
+        double v = term(d[0], eM, m.t[0]);
+        v = logAdd(T, v, term(d[1], eM, m.t[3]));
+        v = logAdd(T, v, term(d[2], eM, m.t[6]));
+        c[0] = v;
+    }
+    if (upper) {
+        double v = term(u[0], eY, m.t[2]);
+        v = logAdd(T, v, term(u[2], eY, m.t[8]));
+        if (SW) v = logAdd(T, v, term(u[1], eY, m.t[5]));
+        c[2] = v;
+    }
+}
+
+// The match emission of the run-length model (impl/stateMachine.c:718-722): the base pair's
+// log probability plus 2.3025 * log10 R[row][x run][y run] (the product precomputed on the host).
+__device__ __forceinline__ double matchEmission(const DevLogModel &m, const double *rep, int xb, int repRow, int yb,
+                                                int ry) {
+    double e = m.match[xb * 5 + yb];
+    if (m.runLength) e = __dadd_rn(e, rep[repRow + ry]);
+    return e;
+}
+
+__device__ __forceinline__ int repRowOf(const DevLogModel &m, uint16_t cx, int xb) {
+    if (!m.runLength) return 0;
+    const int r = xb == 4 ? 0 : xb;
+    const int tableRow = m.strand ? r : 3 - r;
+    return (tableRow * mp::kMaxRepeat + (cx >> 8)) * mp::kMaxRepeat;
+}
+
+// The total of diagonalCalculationTotalProbability at the last diagonal
+// (impl/pairwiseAligner.c:567-584), where only the cell (lx, ly) is in the band: cellDot with the
+// end probabilities, then logAdd(LOG_ZERO, .).
+__device__ __forceinline__ double totalAtEnd(const Tables &T, const DevLogModel &m, const double *c) {
+    double v = __dadd_rn(c[0], m.end[0]);
+    v = logAdd(T, v, __dadd_rn(c[1], m.end[1]));
+    v = logAdd(T, v, __dadd_rn(c[2], m.end[2]));
+    return logAdd(T, kLogZero, v);
+}
+
 // The row of one thread: column x, state k.
-template <int LXMAX>
 struct SharedRow {
     double *base;
     __device__ __forceinline__ double &at(int x, int k) const { return base[(x * 3 + k) * blockDim.x]; }
@@ -114,160 +175,229 @@ struct GlobalRow {
     __device__ __forceinline__ double &at(int x, int k) const { return base[x * 3 + k]; }
 };
 
-// One pair: the forward recursion over the whole (lx+1) x (ly+1) matrix and the total at the
-// last cell with the end probabilities (diagonalCalculationTotalProbability at the last
-// diagonal, impl/pairwiseAligner.c:567-584, where only that cell is in the band).
+// One pair on one thread: the matrix row by row (row y = 0: the start cell, then gap-x cells;
+// then per row the gap-y cell of column 0 and the full cells).
 template <bool SW, class Row>
-__device__ double forwardPair(const PairArgs &a, int p, const Row &row) {
+__device__ double forwardPairThread(const Tables &T, const PairArgs &a, int p, const Row &row) {
     const int lx = a.xLen[p], ly = a.yLen[p];
     if (lx + ly == 0) return 0.0;  // LOG_ONE (impl/pairwiseAligner.c:822-824)
-    const DevLogModel &m = a.models[a.strand[p] ? 0 : 1];
+    const DevLogModel &m = T.models[a.strand[p] ? 0 : 1];
     const double *rep = a.repeatLog + (a.strand[p] ? 0 : mp::kRepTable);
     const uint16_t *sx = a.xs + a.xOff[p];
     const uint16_t *sy = a.ys + a.yOff[p];
     const int rl = m.runLength;
-    const double t00 = m.t[0], t01 = m.t[1], t02 = m.t[2];
-    const double t10 = m.t[3], t11 = m.t[4], t12 = m.t[5];
-    const double t20 = m.t[6], t21 = m.t[7], t22 = m.t[8];
-    // row y = 0: the start cell, then gap-x cells fed from the left
-    double l0 = m.start[0], l1 = m.start[1], l2 = m.start[2];
-    row.at(0, 0) = l0;
-    row.at(0, 1) = l1;
-    row.at(0, 2) = l2;
+    double l[3] = {m.start[0], m.start[1], m.start[2]}, c[3];
+    row.at(0, 0) = l[0];
+    row.at(0, 1) = l[1];
+    row.at(0, 2) = l[2];
     for (int x = 1; x <= lx; x++) {
-        const double e = m.gapX[baseOf(sx[x - 1], rl)];
-        double c1 = term(l0, e, t01);
-        c1 = logAdd(c1, term(l1, e, t11));
-        if (SW) c1 = logAdd(c1, term(l2, e, t21));
-        l0 = kLogZero;
-        l1 = c1;
-        l2 = kLogZero;
-        row.at(x, 0) = l0;
-        row.at(x, 1) = l1;
-        row.at(x, 2) = l2;
+        cellForward<SW>(T, m, true, false, false, m.gapX[baseOf(sx[x - 1], rl)], 0.0, 0.0, l, l, l, c);
+        l[0] = c[0], l[1] = c[1], l[2] = c[2];
+        row.at(x, 0) = c[0];
+        row.at(x, 1) = c[1];
+        row.at(x, 2) = c[2];
     }
     for (int y = 1; y <= ly; y++) {
         const uint16_t cy = sy[y - 1];
         const int yb = baseOf(cy, rl);
         const int ry = rl ? (cy >> 8) : 0;
         const double eY = m.gapY[yb];
-        // column 0: a gap-y cell fed from above
-        double d0 = row.at(0, 0), d1 = row.at(0, 1), d2 = row.at(0, 2);  // (x-1, y-1) for column 1
-        {
-            double c2 = term(d0, eY, t02);
-            c2 = logAdd(c2, term(d2, eY, t22));
-            if (SW) c2 = logAdd(c2, term(d1, eY, t12));
-            l0 = kLogZero;
-            l1 = kLogZero;
-            l2 = c2;
-            row.at(0, 0) = l0;
-            row.at(0, 1) = l1;
-            row.at(0, 2) = l2;
-        }
+        double d[3] = {row.at(0, 0), row.at(0, 1), row.at(0, 2)};  // (x-1, y-1) for column 1
+        cellForward<SW>(T, m, false, false, true, 0.0, 0.0, eY, d, d, d, l);
+        row.at(0, 0) = l[0];
+        row.at(0, 1) = l[1];
+        row.at(0, 2) = l[2];
+        // unrolled so that the match and gap-y sums of the next column, which do not wait for
+        // this column, can be issued while this column's gap-x sum completes
+#pragma unroll 2
         for (int x = 1; x <= lx; x++) {
             const uint16_t cx = sx[x - 1];
             const int xb = baseOf(cx, rl);
-            const double u0 = row.at(x, 0), u1 = row.at(x, 1), u2 = row.at(x, 2);  // (x, y-1)
-            // lower: gap-x from (x-1, y)
-            const double eX = m.gapX[xb];
-            double c1 = term(l0, eX, t01);
-            c1 = logAdd(c1, term(l1, eX, t11));
-            if (SW) c1 = logAdd(c1, term(l2, eX, t21));
-            // middle: match from (x-1, y-1)
-            double eM = m.match[xb * 5 + yb];
-            if (rl) {
-                const int rx = cx >> 8;
-                const int r = xb == 4 ? 0 : xb;
-                const int tableRow = m.strand ? r : 3 - r;
-                eM = __dadd_rn(eM, rep[(tableRow * mp::kMaxRepeat + rx) * mp::kMaxRepeat + ry]);
-            }
-            double c0 = term(d0, eM, t00);
-            c0 = logAdd(c0, term(d1, eM, t10));
-            c0 = logAdd(c0, term(d2, eM, t20));
-            // upper: gap-y from (x, y-1)
-            double c2 = term(u0, eY, t02);
-            c2 = logAdd(c2, term(u2, eY, t22));
-            if (SW) c2 = logAdd(c2, term(u1, eY, t12));
-            d0 = u0;
-            d1 = u1;
-            d2 = u2;
-            l0 = c0;
-            l1 = c1;
-            l2 = c2;
-            row.at(x, 0) = c0;
-            row.at(x, 1) = c1;
-            row.at(x, 2) = c2;
+            const double u[3] = {row.at(x, 0), row.at(x, 1), row.at(x, 2)};  // (x, y-1)
+            const double eM = matchEmission(m, rep, xb, repRowOf(m, cx, xb), yb, ry);
+            cellForward<SW>(T, m, true, true, true, m.gapX[xb], eM, eY, l, d, u, c);
+            d[0] = u[0], d[1] = u[1], d[2] = u[2];
+            l[0] = c[0], l[1] = c[1], l[2] = c[2];
+            row.at(x, 0) = c[0];
+            row.at(x, 1) = c[1];
+            row.at(x, 2) = c[2];
         }
     }
-    // the last cell (lx, ly) with the end probabilities: cellDot, then logAdd(LOG_ZERO, .)
-    double v = __dadd_rn(l0, m.end[0]);
-    v = logAdd(v, __dadd_rn(l1, m.end[1]));
-    v = logAdd(v, __dadd_rn(l2, m.end[2]));
-    return logAdd(kLogZero, v);
+    return totalAtEnd(T, m, l);
 }
 
-// LXMAX > 0: alleles of at most LXMAX runs, rows in shared memory; LXMAX = 0: any length, rows
-// in global memory.
+// Short alleles (at most LXMAX = 16 or 31 runs): one thread per pair, its row in shared memory;
+// LXMAX = 0: any length, rows in global memory.
 template <int LXMAX, bool SW>
-__global__ void __launch_bounds__(128) pairForwardKernel(PairArgs a) {
+__global__ void __launch_bounds__(128) pairThreadKernel(PairArgs a) {
     extern __shared__ double smemRows[];
+    __shared__ Tables T;
+    loadTables(T, a.models);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nPairs) return;
     const int p = a.pairs[i];
     double r;
     if (LXMAX > 0) {
-        SharedRow<LXMAX> row{smemRows + threadIdx.x};
-        r = forwardPair<SW>(a, p, row);
+        r = forwardPairThread<SW>(T, a, p, SharedRow{smemRows + threadIdx.x});
     } else {
-        GlobalRow row{a.rows + a.rowOff[i]};
-        r = forwardPair<SW>(a, p, row);
+        r = forwardPairThread<SW>(T, a, p, GlobalRow{a.rows + a.rowOff[i]});
     }
     a.out[p] = r;
 }
 
-constexpr int kThreads = 128;
-
-template <int LXMAX>
-size_t sharedBytes() {
-    return LXMAX > 0 ? sizeof(double) * 3 * (LXMAX + 1) * kThreads : 0;
-}
-
-// Callers hold the engine's one-shot lock; the attribute is set once per device and kernel.
-template <int LXMAX, bool SW>
-cudaError_t launchClass(const PairArgs &a, int device, cudaStream_t st) {
-    if (a.nPairs == 0) return cudaSuccess;
-    const size_t smem = sharedBytes<LXMAX>();
-    static std::mutex lock;
-    static bool granted[128] = {};
-    if (smem > 48 * 1024) {
-        std::lock_guard<std::mutex> g(lock);
-        if (!granted[device & 127]) {
-            cudaError_t e = cudaFuncSetAttribute(pairForwardKernel<LXMAX, SW>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-            if (e != cudaSuccess) return e;
-            granted[device & 127] = true;
+// Longer alleles (32 to 32 S - 1 runs): one warp per pair, sweeping anti-diagonals. Lane l owns
+// the columns x = l + 32 k (k < S) and keeps, per column, the cell it computed on the previous
+// anti-diagonal; the left column's cells of the two previous anti-diagonals come by shuffles.
+// Every cell is cellForward of the same neighbours as in the row sweep, so the values agree.
+template <int S, bool SW>
+__global__ void __launch_bounds__(128) pairWarpKernel(PairArgs a) {
+    __shared__ Tables T;
+    loadTables(T, a.models);
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= a.nPairs) return;  // warp-uniform
+    const int p = a.pairs[i];
+    const int lx = a.xLen[p], ly = a.yLen[p];
+    if (lx + ly == 0) {
+        if (lane == 0) a.out[p] = 0.0;
+        return;
+    }
+    const DevLogModel &m = T.models[a.strand[p] ? 0 : 1];
+    const double *rep = a.repeatLog + (a.strand[p] ? 0 : mp::kRepTable);
+    const uint16_t *sx = a.xs + a.xOff[p];
+    const uint16_t *sy = a.ys + a.yOff[p];
+    const int rl = m.runLength;
+    int xb[S], repRow[S];
+    double eX[S], own[S][3], left2[S][3];
+#pragma unroll
+    for (int k = 0; k < S; k++) {
+        const int x = lane + 32 * k;
+        xb[k] = 4;
+        repRow[k] = 0;
+        eX[k] = 0.0;
+        if (x >= 1 && x <= lx) {
+            const uint16_t cx = sx[x - 1];
+            xb[k] = baseOf(cx, rl);
+            repRow[k] = repRowOf(m, cx, xb[k]);
+            eX[k] = m.gapX[xb[k]];
+        }
+        own[k][0] = own[k][1] = own[k][2] = kLogZero;
+        left2[k][0] = left2[k][1] = left2[k][2] = kLogZero;
+    }
+    if (lane == 0) {  // anti-diagonal 0: the start cell (0, 0)
+        own[0][0] = m.start[0];
+        own[0][1] = m.start[1];
+        own[0][2] = m.start[2];
+    }
+    const int N = lx + ly;
+    for (int dg = 1; dg <= N; dg++) {
+        double left1[S][3];
+#pragma unroll
+        for (int k = 0; k < S; k++) {
+#pragma unroll
+            for (int s = 0; s < 3; s++) {
+                const double up = __shfl_up_sync(0xffffffffu, own[k][s], 1);
+                const double wrap = k > 0 ? __shfl_sync(0xffffffffu, own[k > 0 ? k - 1 : 0][s], 31) : kLogZero;
+                left1[k][s] = lane == 0 ? wrap : up;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < S; k++) {
+            const int x = lane + 32 * k, y = dg - x;
+            if (x <= lx && y >= 0 && y <= ly) {
+                double eY = 0.0, eM = 0.0;
+                if (y >= 1) {
+                    const uint16_t cy = sy[y - 1];
+                    const int yb = baseOf(cy, rl);
+                    eY = m.gapY[yb];
+                    if (x >= 1) eM = matchEmission(m, rep, xb[k], repRow[k], yb, rl ? (cy >> 8) : 0);
+                }
+                double c[3];
+                cellForward<SW>(T, m, x >= 1, x >= 1 && y >= 1, y >= 1, eX[k], eM, eY, left1[k], left2[k], own[k],
+                                c);
+                own[k][0] = c[0], own[k][1] = c[1], own[k][2] = c[2];
+                if (x == lx && y == ly) a.out[p] = totalAtEnd(T, m, c);  // the last anti-diagonal's one cell
+            }
+            left2[k][0] = left1[k][0], left2[k][1] = left1[k][1], left2[k][2] = left1[k][2];
         }
     }
-    const int blocks = (a.nPairs + kThreads - 1) / kThreads;
-    pairForwardKernel<LXMAX, SW><<<blocks, kThreads, smem, st>>>(a);
-    return cudaGetLastError();
+}
+
+constexpr int kThreads = 128;
+constexpr int kShortMax = 16;     // thread-per-pair class with shared-memory rows of 17 columns
+constexpr int kMidMax = 31;       // the same with rows of 32 columns
+constexpr int kWarpStrips = 4;    // warp-per-pair classes: alleles of up to 32 * 4 - 1 runs
+
+// Launch classes: 0 short and 1 mid (thread, shared rows), 2..4 warp with S = 2..4 strips,
+// 5 long (thread, global rows).
+constexpr int kClasses = 6;
+
+int classOf(int32_t lx) {
+    if (lx <= kShortMax) return 0;
+    if (lx <= kMidMax) return 1;
+    if (lx < 32 * kWarpStrips) return (lx + 1 + 31) / 32;  // S = strips for columns 0..lx
+    return kClasses - 1;
+}
+
+template <int LXMAX>
+constexpr size_t rowBytes() {
+    return sizeof(double) * 3 * (LXMAX + 1) * kThreads;
+}
+
+// Callers hold the engine's one-shot lock; the shared-memory attributes are set once per device.
+template <bool SW>
+cudaError_t setAttributes(int device) {
+    static std::mutex lock;
+    static bool granted[128] = {};
+    std::lock_guard<std::mutex> g(lock);
+    if (granted[device & 127]) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(pairThreadKernel<kShortMax, SW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int) rowBytes<kShortMax>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(pairThreadKernel<kMidMax, SW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int) rowBytes<kMidMax>());
+    if (e == cudaSuccess) granted[device & 127] = true;
+    return e;
 }
 
 template <bool SW>
-cudaError_t launchAll(PairArgs a, const int32_t *const cls[4], const int32_t nCls[4], int device, cudaStream_t st) {
-    cudaError_t e = cudaSuccess;
-    a.pairs = cls[0];
-    a.nPairs = nCls[0];
-    if ((e = launchClass<16, SW>(a, device, st)) != cudaSuccess) return e;
-    a.pairs = cls[1];
-    a.nPairs = nCls[1];
-    if ((e = launchClass<32, SW>(a, device, st)) != cudaSuccess) return e;
-    a.pairs = cls[2];
-    a.nPairs = nCls[2];
-    if ((e = launchClass<64, SW>(a, device, st)) != cudaSuccess) return e;
-    a.pairs = cls[3];
-    a.nPairs = nCls[3];
-    return launchClass<0, SW>(a, device, st);
+cudaError_t launchAll(PairArgs a, const int32_t *const cls[kClasses], const int32_t nCls[kClasses], int device,
+                      cudaStream_t st) {
+    cudaError_t e = setAttributes<SW>(device);
+    if (e != cudaSuccess) return e;
+    auto blocksFor = [](int32_t threads) { return (threads + kThreads - 1) / kThreads; };
+    // the warp classes first (longest first): their pairs are the longest
+    for (int c = kWarpStrips; c >= 2; c--) {
+        if (nCls[c] == 0) continue;
+        a.pairs = cls[c];
+        a.nPairs = nCls[c];
+        const int blocks = blocksFor(32 * nCls[c]);
+        switch (c) {
+            case 2: pairWarpKernel<2, SW><<<blocks, kThreads, 0, st>>>(a); break;
+            case 3: pairWarpKernel<3, SW><<<blocks, kThreads, 0, st>>>(a); break;
+            default: pairWarpKernel<4, SW><<<blocks, kThreads, 0, st>>>(a); break;
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (nCls[kClasses - 1] > 0) {
+        a.pairs = cls[kClasses - 1];
+        a.nPairs = nCls[kClasses - 1];
+        pairThreadKernel<0, SW><<<blocksFor(a.nPairs), kThreads, 0, st>>>(a);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (nCls[1] > 0) {
+        a.pairs = cls[1];
+        a.nPairs = nCls[1];
+        pairThreadKernel<kMidMax, SW><<<blocksFor(a.nPairs), kThreads, rowBytes<kMidMax>(), st>>>(a);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (nCls[0] > 0) {
+        a.pairs = cls[0];
+        a.nPairs = nCls[0];
+        pairThreadKernel<kShortMax, SW><<<blocksFor(a.nPairs), kThreads, rowBytes<kShortMax>(), st>>>(a);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace
@@ -323,20 +453,25 @@ extern "C" mp_status mp_forward_pairs(mp_engine *e, const mp_model *m, const mp_
     std::lock_guard<std::mutex> guard(e->oneShotLock);
     cudaSetDevice(e->device);
     mp_pair_scratch &s = e->pairScratch;
-    // length classes by allele length (stable: pairs of a bubble stay together)
+    // pairs ordered by allele length (a counting sort, stable: pairs of a bubble stay together),
+    // which makes the classes contiguous and gives the threads of a warp equal row lengths
+    const int kSortMax = 32 * kWarpStrips;
     std::vector<int32_t> idx((size_t) n);
-    int32_t nCls[4] = {0, 0, 0, 0};
-    auto classOf = [](int32_t lx) { return lx <= 16 ? 0 : lx <= 32 ? 1 : lx <= 64 ? 2 : 3; };
-    for (int64_t j = 0; j < n; j++) nCls[classOf(b->x_length[j])]++;
-    int32_t start[4] = {0, nCls[0], nCls[0] + nCls[1], nCls[0] + nCls[1] + nCls[2]};
-    int32_t at[4] = {start[0], start[1], start[2], start[3]};
-    std::vector<int64_t> rowOff((size_t) nCls[3] + 1, 0);
-    for (int64_t j = 0; j < n; j++) {
-        const int c = classOf(b->x_length[j]);
-        if (c == 3) rowOff[(size_t) (at[3] - start[3]) + 1] = 3 * ((int64_t) b->x_length[j] + 1);
-        idx[(size_t) at[c]++] = (int32_t) j;
+    {
+        std::vector<int64_t> at((size_t) kSortMax + 2, 0);
+        for (int64_t j = 0; j < n; j++) at[(size_t) std::min<int32_t>(b->x_length[j], kSortMax) + 1]++;
+        for (int k = 1; k <= kSortMax + 1; k++) at[k] += at[k - 1];
+        for (int64_t j = 0; j < n; j++) idx[(size_t) at[(size_t) std::min<int32_t>(b->x_length[j], kSortMax)]++] = (int32_t) j;
     }
-    for (size_t k = 1; k < rowOff.size(); k++) rowOff[k] += rowOff[k - 1];
+    int32_t nCls[kClasses] = {}, start[kClasses] = {};
+    for (int64_t j = 0; j < n; j++) nCls[classOf(b->x_length[j])]++;
+    for (int c = 1; c < kClasses; c++) start[c] = start[c - 1] + nCls[c - 1];
+    // warp classes longest first
+    for (int c = 2; c <= kWarpStrips; c++) std::reverse(idx.begin() + start[c], idx.begin() + start[c] + nCls[c]);
+    const int cl = kClasses - 1;
+    std::vector<int64_t> rowOff((size_t) nCls[cl] + 1, 0);
+    for (int32_t k = 0; k < nCls[cl]; k++)
+        rowOff[(size_t) k + 1] = rowOff[(size_t) k] + 3 * ((int64_t) b->x_length[idx[(size_t) (start[cl] + k)]] + 1);
     const size_t nx = (size_t) std::max<int64_t>(b->x_symbols_length, 1), ny = (size_t) std::max<int64_t>(b->y_symbols_length, 1);
     PAIR_TRY(s.idx.reserve(sizeof(int32_t) * (size_t) n));
     PAIR_TRY(s.xOff.reserve(sizeof(int64_t) * (size_t) n));
@@ -384,8 +519,8 @@ extern "C" mp_status mp_forward_pairs(mp_engine *e, const mp_model *m, const mp_
     a.rows = s.rows.as<double>();
     a.rowOff = s.rowOff.as<int64_t>();
     a.out = s.out.as<double>();
-    const int32_t *cls[4];
-    for (int c = 0; c < 4; c++) cls[c] = s.idx.as<int32_t>() + start[c];
+    const int32_t *cls[kClasses];
+    for (int c = 0; c < kClasses; c++) cls[c] = s.idx.as<int32_t>() + start[c];
     const bool sw = !(m->logHost[0].noSwitch && m->logHost[1].noSwitch);
     cudaError_t ce = cudaSuccess;
     for (int k = 0; k < 2 && ce == cudaSuccess; k++)

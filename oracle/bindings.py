@@ -600,6 +600,7 @@ class RefPoaOracle:
         return self.lib.refpoa_realign(reads_h, anchors_h, ref.chars or b"\0", _p(c, c_uint32), len(ref), params_h)
 
     def realign_all(self, reads_h, anchors_h, ref, params_h):
+        """poa_realignAll; anchors_h None aligns every read to the whole reference (no anchors)."""
         from ctypes import c_uint32
         c = np.ascontiguousarray(ref.counts, dtype=np.uint32) if len(ref) else np.zeros(1, np.uint32)
         return self.lib.refpoa_realign_all(reads_h, anchors_h, ref.chars or b"\0", _p(c, c_uint32), len(ref),

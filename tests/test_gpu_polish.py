@@ -200,3 +200,48 @@ def test_shipped_loop_identical_to_reference(engine, gmodel, ref_poa, ref_models
             print(f"chunk {c}: GPU loop differs from the reference ({len(gpu[c])} vs {len(want[c][0])} runs, "
                   f"similarity {ratio:.5f})")
             assert ratio > 0.999
+
+
+def _rle_list(z, name, off_name=None):
+    off = z[(off_name or name) + "_offsets"]
+    chars = z[name + "_chars"].tobytes()
+    counts = z[name + "_counts"].astype(np.uint32)
+    from marginpolish_b200.rle import RleString as R
+    return [R(chars[off[i]:off[i + 1]], counts[off[i]:off[i + 1]]) for i in range(off.size - 1)]
+
+
+def _identity(a: str, b: str) -> float:
+    """2 * matches / (len a + len b) of a global alignment (unit edit costs)."""
+    from difflib import SequenceMatcher
+    m = sum(blk.size for blk in SequenceMatcher(None, a, b, autojunk=False).get_matching_blocks())
+    return 2.0 * m / (len(a) + len(b))
+
+
+def test_real_nanopore_windows_identical_to_reference(engine, gmodel, polish_model):
+    """Real reads: the reference's own polishing examples (20 E. coli windows of Guppy-called
+    nanopore reads, tests/polisherTest.c:736-819), polished without anchors with the test's loop
+    (up to 100 consensus iterations at reference base penalty 0.6, then three polish
+    iterations) and the run-length estimate. The GPU loop gives the reference's polished windows
+    exactly (tests/golden/ecoli_windows.npz, made by make_ecoli_golden.py), and moves them
+    towards the true reference."""
+    path = os.path.join(GOLDEN, "ecoli_windows.npz")
+    z = np.load(path)
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("meg", os.path.join(GOLDEN, "make_ecoli_golden.py"))
+    meg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(meg)
+    drafts = _rle_list(z, "draft")
+    truths = _rle_list(z, "truth")
+    want = _rle_list(z, "polished")
+    flat_reads = _rle_list(z, "read")
+    cr = z["chunk_reads"]
+    reads = [flat_reads[cr[w]:cr[w + 1]] for w in range(cr.size - 1)]
+    strands = [list(z["strands"][cr[w]:cr[w + 1]]) for w in range(cr.size - 1)]
+    got = polish(engine, gmodel, polish_model, meg.loop_params(), drafts, reads, strands, None)
+    same = [g.chars == w.chars and np.array_equal(g.counts, w.counts) for g, w in zip(got, want)]
+    before = sum(_identity(d.expand(), t.expand()) for d, t in zip(drafts, truths)) / len(drafts)
+    after = sum(_identity(g.expand(), t.expand()) for g, t in zip(got, truths)) / len(got)
+    print(f"{len(got)} E. coli windows, {len(flat_reads)} reads: {sum(same)} identical to the reference's polished "
+          f"windows; identity to the truth {before:.4f} -> {after:.4f}")
+    assert all(same)
+    assert after > before

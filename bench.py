@@ -73,6 +73,8 @@ def parse():
                     help="skip the 1 Mb polishing-loop and 5 Mb realignment-pass measurements")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the adjoint and POA-loop measurements reported beside the headline")
+    ap.add_argument("--bubble-scores", action="store_true",
+                    help="only the polish step's bubble-score measurement (one JSON line; no CPU sample)")
     return ap.parse_args()
 
 
@@ -814,6 +816,12 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+    elif args.bubble_scores:
+        from marginpolish_b200 import Engine, Model, params
+        pm = params.polish_model_from_npz(os.path.join(ROOT, "tests", "golden", "model_np.npz"))
+        engine = Engine(local)
+        model = Model.from_polish(engine, pm)
+        print(json.dumps({"bubble_scoring": measure_bubble_scoring(engine, model, pm, cpu_sample=False)}), flush=True)
     else:
         run_ours(args, rank, world, local)
 

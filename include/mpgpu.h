@@ -483,6 +483,37 @@ mp_status mp_poa_consensus(const mp_poa_set *s, int64_t chunk, char *chars, uint
 mp_status mp_poa_anchor_alignments(const mp_poa_set *s, int64_t chunk, const int64_t *map, int64_t *offsets,
                                    int64_t *triples, int64_t cap, int64_t *n_anchors);
 
+/* ---- chunk stitching: mergeContigChunks (impl/chunker.c:50-112) with removeOverlap
+ * (impl/polisher.c:1937-2006) ----
+ * Joins the polished chunks of one contig (expanded strings, chunk c = chars[offsets[c] ..
+ * offsets[c+1]), in order). At every boundary the last `overlap` characters of the previous
+ * chunk (as cropped so far) and the first `overlap` characters of the next are aligned without
+ * anchors, ragged at both ends, with model m (the reference uses its code-default nucleotide
+ * machine, stateMachine3_constructNucleotide) and parameters p; both are cut at the first match
+ * pair of the largest weight (the previous chunk before its x, the next from its y). A boundary
+ * without match pairs puts `spacer_length` Ns in place of an empty chunk, or ten Ns at the seam
+ * of a non-empty one (overlap > 0). All boundaries are aligned in one GPU batch. The merged
+ * contig goes to out (at most cap characters; *out_length gets its length, MP_ERR_OVERFLOW when
+ * it does not fit); report (NULL or 3 per chunk) gets each chunk's boundary weight with the
+ * previous chunk, the characters cut from its start, and 1 for a spacer, 2 for a seam of Ns.
+ * The reference's overlap is twice chunkBoundary (marginPolish.c:658; 100 shipped). The
+ * alignments are computed in the reference's arithmetic (mp_match_pairs_reference), so the cuts
+ * are the reference's; an overlap above about 2,000 characters is refused (MP_ERR_OVERFLOW). */
+/* getAlignedPairs (impl/pairwiseAligner.c:1132-1139) for small anchor-free alignments, in the
+ * reference's own arithmetic: FP64 log cells over the whole matrix, its approximate log-sum
+ * (:279-299), its walk schedule and total refresh, so every match weight is the reference's (up
+ * to CUDA's exp within one unit in the last place). For choices that depend on near-equal
+ * weights. Jobs of b (no anchors; ragged ends and strand honoured) with a model without run
+ * lengths, at most 2^22 matrix cells each. Job j's tuples are [offsets[j], offsets[j+1]) of
+ * weight, x, y (at most cap in all; *total gets the count) in the reference's list order. */
+mp_status mp_match_pairs_reference(mp_engine *e, const mp_model *m, const mp_params *p, const mp_batch *b,
+                                   int64_t *offsets, int32_t *weight, int32_t *x, int32_t *y, int64_t cap,
+                                   int64_t *total);
+
+mp_status mp_merge_contig(mp_engine *e, const mp_model *m, const mp_params *p, int64_t n_chunks,
+                          const int64_t *offsets, const char *chars, int64_t overlap, int64_t spacer_length,
+                          char *out, int64_t cap, int64_t *out_length, int64_t *report);
+
 /* ---- single read without any memory allocation ----
  * No counterpart in the reference. For callers that cannot allocate device memory
  * (their framework's pool owns the GPU, or allocation is not allowed where they

@@ -4,16 +4,16 @@ posterior pass. The compute path is the in-tree CUDA library libmpgpu.so
 from . import _lib
 from .params import AlignmentParams, PolishModel, StateModel, build_state_model, load_polish_model
 from .realign import (DeviceBatch, Engine, Expectations, Jobs, Model, Pairs, compute_forward_probability,
-                      expectations_batch, forward_batch, forward_pairs, forward_pairs_timing, get_aligned_pairs_using_anchors,
+                      expectations_batch, forward_batch, forward_pairs, forward_pairs_timing, match_pairs_reference, get_aligned_pairs_using_anchors,
                       get_aligned_pairs_with_indels_using_anchors, realign_batch,
                       realign_batch_pipelined)
 from .rle import RleString, crop_range, rle_anchors
-from .poa import PoaSet, PolishParams, polish
+from .poa import PoaSet, PolishParams, merge_contig, polish
 
 __all__ = [
     "AlignmentParams", "PolishModel", "StateModel", "build_state_model", "load_polish_model", "DeviceBatch",
     "Engine", "Jobs", "Model", "Pairs", "get_aligned_pairs_using_anchors",
     "get_aligned_pairs_with_indels_using_anchors", "realign_batch", "realign_batch_pipelined", "RleString", "crop_range", "rle_anchors",
-    "compute_forward_probability", "forward_batch", "forward_pairs", "forward_pairs_timing", "expectations_batch", "Expectations", "PoaSet", "PolishParams",
-    "polish",
+    "compute_forward_probability", "forward_batch", "forward_pairs", "forward_pairs_timing", "match_pairs_reference", "expectations_batch", "Expectations", "PoaSet", "PolishParams",
+    "polish", "merge_contig",
 ]

@@ -231,7 +231,7 @@ EXPORTED = [
     "mp_poa_anchor_alignments", "mp_engine_autotune", "mp_engine_autotune_reset",
     "mp_engine_set_graph_capture", "mp_realign_batch_into", "mp_engine_release_buffers", "mp_forward_pairs",
     "mp_forward_pairs_timing", "mp_measure_fp64_peak", "mp_poa_set_iterate_polish", "mp_poa_set_build_bubbles", "mp_poa_set_score_bubbles", "mp_poa_bubble_sizes",
-    "mp_poa_bubbles", "mp_poa_bubble_consensus",
+    "mp_poa_bubbles", "mp_poa_bubble_consensus", "mp_merge_contig", "mp_match_pairs_reference",
 ]
 
 _lib = None
@@ -298,6 +298,10 @@ def load() -> ctypes.CDLL:
         "mp_poa_bubble_consensus": (c_int, [c_void_p, c_int64, P(c_int64), P(c_char), P(ctypes.c_uint64), c_int64,
                                             P(c_int64), P(c_int64)]),
         "mp_forward_pairs": (c_int, [c_void_p, c_void_p, P(PairBatch), P(c_double)]),
+        "mp_match_pairs_reference": (c_int, [c_void_p, c_void_p, P(Params), P(Batch), P(c_int64), P(c_int32),
+                                             P(c_int32), P(c_int32), c_int64, P(c_int64)]),
+        "mp_merge_contig": (c_int, [c_void_p, c_void_p, P(Params), c_int64, P(c_int64), c_char_p, c_int64, c_int64,
+                                    P(c_char), c_int64, P(c_int64), P(c_int64)]),
         "mp_forward_pairs_timing": (c_int, [c_void_p, P(c_float), P(c_int64), P(c_int64)]),
         "mp_poa_set_realign_all": (c_int, [c_void_p]),
         "mp_poa_set_estimate_repeat_counts": (c_int, [c_void_p]),

@@ -159,3 +159,20 @@ struct mp_model {
 // Fills the FP64 log-space tables of one strand's model (defined in mp_bubble.cu).
 mp_status mp_model_lower_log(const mp_model_desc *d, mp::DevLogModel &m, double *rep);
 
+// Anchor-free alignments whose match posteriors are computed in the reference's own arithmetic
+// (getAlignedPairs over the whole matrix, FP64 logs, its approximate log-sum; defined in
+// mp_refpost.cu), for the few small alignments whose results decide a choice among near-equal
+// weights (the cut of chunk stitching). The model must be without run lengths.
+struct RefPair {
+    int64_t xOff, yOff;   // into the x and y symbol arrays
+    int32_t lx, ly;
+    bool raggedLeft, raggedRight, forward;
+};
+struct RefTuple {
+    int32_t weight, x, y;
+};
+constexpr int64_t kRefMaxCells = (int64_t) 1 << 22;  // per alignment
+// out[k]: pair k's match tuples in the reference's list order.
+mp_status refMatchPairs(mp_engine *e, const mp_model *m, const mp_params *p, const std::vector<RefPair> &pairs,
+                        const std::vector<uint16_t> &xs, const std::vector<uint16_t> &ys,
+                        std::vector<std::vector<RefTuple>> &out);

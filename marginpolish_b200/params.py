@@ -283,3 +283,33 @@ def default_state_model(transitions, match, gap, boundary) -> StateModel:
     b = np.asarray(boundary, dtype=np.float64).reshape(4, 3)
     return StateModel(np.asarray(transitions, dtype=np.float64), b[0], b[1], b[2], b[3],
                       np.asarray(match, dtype=np.float64), gap[:, 0].copy(), gap[:, 1].copy(), run_length=False)
+
+
+# The reference's code-default 3-state nucleotide machine, which removeOverlap aligns chunk
+# overlaps with (stateMachine3_constructNucleotide, impl/polisher.c:1958-1959): the transition
+# constants of impl/stateMachine.c:598-608 and the nucleotide emission tables of
+# nucleotideEmissions_construct, as natural logs (tests/test_model.py pins them against the
+# reference build). Transitions are from*3+to over (match, gap-x, gap-y); emissions by base
+# A C G T N.
+CODE_DEFAULT_TRANSITIONS = (
+    -0.030064059121770816, -4.21256642, -4.21256642,
+    -1.272871422049609, -0.3388262689231553, -4.910694825551255,
+    -1.272871422049609, -4.910694825551255, -0.3388262689231553)
+CODE_DEFAULT_MATCH = (
+    -1.8917761142, -4.3459578861, -3.760242452, -4.3459578861, -2.772588722,
+    -4.3459578861, -1.8917761142, -4.3459578861, -3.760242452, -2.772588722,
+    -3.760242452, -4.3459578861, -1.8917761142, -4.3459578861, -2.772588722,
+    -4.3459578861, -3.760242452, -4.3459578861, -1.8917761142, -2.772588722,
+    -2.772588722, -2.772588722, -2.772588722, -2.772588722, -2.772588722)
+CODE_DEFAULT_GAP = (  # (gap-x, gap-y) per base
+    (-1.3862943611, -1.3862943611), (-1.3862943611, -1.3862943611), (-1.3862943611, -1.3862943611),
+    (-1.3862943611, -1.3862943611), (-1.386294361, -1.386294361))
+CODE_DEFAULT_BOUNDARY = (  # start, ragged start, end, ragged end
+    (0.0, -np.inf, -np.inf), (-np.inf, 0.0, 0.0),
+    (-0.030064059121770816, -1.272871422049609, -1.272871422049609),
+    (-4.21256642, -0.3388262689231553, -0.3388262689231553))
+
+
+def code_default_state_model() -> StateModel:
+    """The code-default nucleotide machine (see CODE_DEFAULT_TRANSITIONS)."""
+    return default_state_model(CODE_DEFAULT_TRANSITIONS, CODE_DEFAULT_MATCH, CODE_DEFAULT_GAP, CODE_DEFAULT_BOUNDARY)

@@ -349,3 +349,29 @@ def polish(engine: Engine, model: Model, pm: PolishModel, polish_params: PolishP
         return [s.reference(c) for c in range(s.n_chunks)]
     finally:
         s.close()
+
+
+def merge_contig(engine: Engine, model: Model, params: AlignmentParams, chunks: Sequence[str], overlap: int,
+                 spacer_length: Optional[int] = None):
+    """mergeContigChunks (impl/chunker.c:50-112): the polished chunks of one contig (expanded
+    strings, in order) joined at their overlaps, each boundary cut by removeOverlap
+    (impl/polisher.c:1937-2006) with `model` (the reference uses the code-default nucleotide
+    machine, params.code_default_state_model()). overlap is twice the chunk boundary
+    (marginPolish.c:658); the spacer for a missing chunk is 3 x the chunk boundary Ns (50 with
+    no boundary, marginPolish.c:639). Returns (merged string, report rows of (boundary weight,
+    characters cut from the chunk's start, 1 spacer / 2 seam of Ns / 0))."""
+    if spacer_length is None:
+        spacer_length = 50 if overlap == 0 else 3 * (overlap // 2)
+    raw = [c.encode() for c in chunks]
+    off = np.zeros(len(raw) + 1, np.int64)
+    off[1:] = np.cumsum([len(c) for c in raw])
+    flat = b"".join(raw) or b"\0"
+    cap = int(off[-1]) + spacer_length * len(raw) + 10 * len(raw) + 16
+    out = (c_char * cap)()
+    n = c_int64(0)
+    report = np.zeros((max(len(raw), 1), 3), np.int64)
+    ps = params.struct()
+    _lib.check(engine._lib.mp_merge_contig(engine.handle, model.handle, ctypes.byref(ps), len(raw),
+                                           _lib.ptr(off, c_int64), flat, int(overlap), int(spacer_length), out, cap,
+                                           ctypes.byref(n), _lib.ptr(report, c_int64)))
+    return bytes(out[:n.value]).decode(), report[:len(raw)].copy()

@@ -25,7 +25,7 @@ from __future__ import annotations
 import ctypes
 import weakref
 from dataclasses import dataclass, field
-from typing import Optional, Sequence
+from typing import List, Optional, Sequence
 
 import numpy as np
 
@@ -508,6 +508,24 @@ def forward_pairs(engine: Engine, model: Model, x_symbols, y_symbols, x_offset, 
     out = np.zeros(max(n, 1), dtype=np.float64)
     _lib.check(engine._lib.mp_forward_pairs(engine.handle, model.handle, ctypes.byref(b), _lib.ptr(out, ctypes.c_double)))
     return out[:n]
+
+
+def match_pairs_reference(engine: Engine, model: Model, params: AlignmentParams, jobs: "Jobs") -> List[np.ndarray]:
+    """getAlignedPairs of anchor-free jobs in the reference's own arithmetic (see
+    mp_match_pairs_reference): per job an (n, 3) array of (weight, x, y) in the reference's
+    order. The model must be without run lengths (the code-default nucleotide machine)."""
+    ps, bs = params.struct(), jobs.struct()
+    offs = np.zeros(jobs.n_jobs + 1, np.int64)
+    total = ctypes.c_int64(0)
+    cap = int(sum((jobs.x_end[j] - jobs.x_begin[j]) * (jobs.y_offsets[j + 1] - jobs.y_offsets[j])
+                  for j in range(jobs.n_jobs))) + 1
+    w, x, y = (np.zeros(cap, np.int32) for _ in range(3))
+    _lib.check(engine._lib.mp_match_pairs_reference(engine.handle, model.handle, ctypes.byref(ps), ctypes.byref(bs),
+                                                    _lib.ptr(offs, ctypes.c_int64), _lib.ptr(w, ctypes.c_int32),
+                                                    _lib.ptr(x, ctypes.c_int32), _lib.ptr(y, ctypes.c_int32), cap,
+                                                    ctypes.byref(total)))
+    return [np.stack([w[offs[j]:offs[j + 1]], x[offs[j]:offs[j + 1]], y[offs[j]:offs[j + 1]]], axis=1).astype(np.int64)
+            for j in range(jobs.n_jobs)]
 
 
 def forward_pairs_timing(engine: Engine) -> dict:

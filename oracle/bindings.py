@@ -472,6 +472,8 @@ class RefPoaOracle:
         lib.refpoa_bubble_reads.argtypes = [c_void_p, c_int64, c_void_p, P(c_int64), P(c_int64), P(c_int64),
                                             P(c_double)]
         lib.refpoa_bubble_supports.argtypes = [c_void_p, c_int64, P(ctypes.c_float)]
+        lib.refpoa_remove_overlap.restype = c_int64
+        lib.refpoa_remove_overlap.argtypes = [c_char_p, c_char_p, c_int64, c_void_p, P(c_int64), P(c_int64)]
         lib.refpoa_bubble_consensus.restype = c_int64
         lib.refpoa_bubble_consensus.argtypes = [c_void_p, c_void_p, P(c_uint64), P(c_char), P(c_uint64), c_int64,
                                                 P(c_int64)]
@@ -556,6 +558,13 @@ class RefPoaOracle:
         self.lib.refpoa_bubble_graph_destroy(bg)
         return dict(bubbles=out, path=path[:len(out)].astype(np.int64), chars=bytes(chars[:n]),
                     counts=counts[:n].copy(), map=node_map[:n_nodes - 1].copy())
+
+    def remove_overlap(self, prefix: str, suffix: str, overlap: int, params_h):
+        """removeOverlap: (overlap match weight, prefix crop end, suffix crop start)."""
+        a, b = c_int64(0), c_int64(0)
+        w = self.lib.refpoa_remove_overlap(prefix.encode(), suffix.encode(), int(overlap), params_h, ctypes.byref(a),
+                                           ctypes.byref(b))
+        return int(w), a.value, b.value
 
     def reads(self, rle_reads, strands):
         from ctypes import c_uint32

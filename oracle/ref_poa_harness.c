@@ -483,3 +483,16 @@ int64_t refpoa_bubble_consensus(void *handle, void *params, uint64_t *path, char
     rleString_destruct(c);
     return n;
 }
+
+/* ---- chunk stitching ---- */
+
+/* removeOverlap (impl/polisher.c:1937-2006) on copies of the two strings: returns the overlap
+ * match weight and the two crop points. */
+int64_t refpoa_remove_overlap(const char *prefix, const char *suffix, int64_t approxOverlap, void *params,
+                              int64_t *prefixCropEnd, int64_t *suffixCropStart) {
+    char *a = stString_copy(prefix), *b = stString_copy(suffix);
+    int64_t w = removeOverlap(a, b, approxOverlap, params, prefixCropEnd, suffixCropStart);
+    free(a);
+    free(b);
+    return w;
+}

@@ -52,6 +52,25 @@ def test_asymmetric_and_default_machines(ref_oracle):
     ref_oracle.free_model(d)
 
 
+def test_code_default_machine_is_the_reference_build(ref_oracle, exact_oracle):
+    """The library's code-default nucleotide machine (params.code_default_state_model, which
+    chunk stitching uses) against the reference build's stateMachine3_constructNucleotide,
+    table by table and on every symbol pair."""
+    sm = params.code_default_state_model()
+    d = ref_oracle.default_model()
+    assert np.array_equal(ref_oracle.transitions(d), sm.log_transitions)
+    for which, vec in enumerate((sm.log_start, sm.log_ragged_start, sm.log_end, sm.log_ragged_end)):
+        assert np.array_equal(ref_oracle.boundary(d, which), vec)
+    m = MpoModel.from_state_model(sm)
+    for cx in range(5):
+        gx, gy = ref_oracle.gap_emissions(d, cx)
+        assert gx == exact_oracle.lib.mpo_gap_x_emission(ctypes.byref(m), cx)
+        assert gy == exact_oracle.lib.mpo_gap_y_emission(ctypes.byref(m), cx)
+        for cy in range(5):
+            assert ref_oracle.match_emission(d, cx, cy) == exact_oracle.lib.mpo_match_emission(ctypes.byref(m), cx, cy)
+    ref_oracle.free_model(d)
+
+
 def test_params_json_parsing_rejects_unknown_keys():
     with pytest.raises(ValueError):
         params.parse_alignment_params({"threshold": 0.1, "bogus": 1})

@@ -499,6 +499,49 @@ mp_status mp_poa_anchor_alignments(const mp_poa_set *s, int64_t chunk, const int
  * The reference's overlap is twice chunkBoundary (marginPolish.c:658; 100 shipped). The
  * alignments are computed in the reference's arithmetic (mp_match_pairs_reference), so the cuts
  * are the reference's; an overlap above about 2,000 characters is refused (MP_ERR_OVERFLOW). */
+/* ---- ingest: a coordinate-sorted BAM to chunks, reads and anchors ----
+ * bamChunker_construct2 (impl/htsIntegration.c:149-273) and convertToReadsAndAlignments
+ * (:347-661), with the run-length forms the loop takes (rleString_rleQualities,
+ * runLengthEncodeAlignment, impl/polisher.c:1692-1750). The BAM is read here (BGZF and the
+ * record layout of the SAM/BAM specification; no index is needed: opening scans the file once
+ * and keeps each record's offset, so a conversion seeks to the first record that can overlap its
+ * chunks). Host-only code. */
+typedef struct mp_bam mp_bam;
+typedef struct {
+    int64_t chunk_size;              /* chunkSize (0: whole contigs) */
+    int64_t chunk_boundary;          /* chunkBoundary: the margin each chunk extends by */
+    int32_t include_soft_clip;       /* includeSoftClipping */
+    int32_t include_secondary;       /* includeSecondaryAlignments */
+    int32_t include_supplementary;   /* includeSupplementaryAlignments */
+    int32_t use_run_length;          /* useRunLengthEncoding */
+    int64_t min_mapq;                /* filterAlignmentsWithMapQBelowThisThreshold (conversion only) */
+    const char *region;              /* "contig:start-end" (0-based start, exclusive end) or NULL */
+} mp_bam_params;
+
+mp_status mp_bam_open(const char *path, const mp_bam_params *p, mp_bam **out);
+void mp_bam_close(mp_bam *b);
+mp_status mp_bam_chunk_count(const mp_bam *b, int64_t *n);
+/* Chunk i: its contig name (at most cap bytes with the terminator) and bounds[4] = (boundary
+ * start, start, end, boundary end), the reference's BamChunk fields. */
+mp_status mp_bam_chunk(const mp_bam *b, int64_t i, char *contig, int64_t cap, int64_t bounds[4]);
+/* Converts chunks [first, first + n): every record in the chunk's bounds that passes the filters
+ * becomes a read trimmed to the chunk and its aligned pairs (reference, read, 10). ref_offsets /
+ * ref_chars (NULL: none) give each chunk's reference over its bounds (expanded); with run
+ * lengths the anchors need it (without it the reads come without anchors, as in the reference).
+ * max_depth > 0 downsamples chunks whose depth reaches it, keeping each read with probability
+ * max_depth / depth (poorMansDownsample, impl/htsIntegration.c:663-697) from a generator
+ * seeded with seed; the reference draws from sonLib's, so its sample differs. */
+mp_status mp_bam_convert(mp_bam *b, int64_t first, int64_t n, const int64_t *ref_offsets, const char *ref_chars,
+                         int64_t max_depth, uint64_t seed);
+/* sizes[4] of the k-th chunk of the last conversion: reads, read runs, anchors, name bytes. */
+mp_status mp_bam_reads_sizes(const mp_bam *b, int64_t k, int64_t sizes[4]);
+/* Its reads: runs laid end to end (read_offsets[reads+1], chars, counts), per-run qualities
+ * (has_qualities per read), strand (1 forward), anchors (anchor_offsets[reads+1], int32 triples
+ * (reference run, read run, 10)) and names (name_offsets[reads+1], names). Any output may be NULL. */
+mp_status mp_bam_reads(const mp_bam *b, int64_t k, int64_t *read_offsets, char *chars, uint32_t *counts,
+                       uint8_t *qualities, uint8_t *has_qualities, uint8_t *strand, int64_t *anchor_offsets,
+                       int32_t *anchors, int64_t *name_offsets, char *names);
+
 /* getAlignedPairs (impl/pairwiseAligner.c:1132-1139) for small anchor-free alignments, in the
  * reference's own arithmetic: FP64 log cells over the whole matrix, its approximate log-sum
  * (:279-299), its walk schedule and total refresh, so every match weight is the reference's (up

@@ -8,12 +8,12 @@ from .realign import (DeviceBatch, Engine, Expectations, Jobs, Model, Pairs, com
                       get_aligned_pairs_with_indels_using_anchors, realign_batch,
                       realign_batch_pipelined)
 from .rle import RleString, crop_range, rle_anchors
-from .poa import PoaSet, PolishParams, merge_contig, polish
+from .poa import PoaSet, PolishParams, merge_contig, merge_contig_threaded, polish
 
 __all__ = [
     "AlignmentParams", "PolishModel", "StateModel", "build_state_model", "load_polish_model", "DeviceBatch",
     "Engine", "Jobs", "Model", "Pairs", "get_aligned_pairs_using_anchors",
     "get_aligned_pairs_with_indels_using_anchors", "realign_batch", "realign_batch_pipelined", "RleString", "crop_range", "rle_anchors",
     "compute_forward_probability", "forward_batch", "forward_pairs", "forward_pairs_timing", "match_pairs_reference", "expectations_batch", "Expectations", "PoaSet", "PolishParams",
-    "polish", "merge_contig",
+    "polish", "merge_contig", "merge_contig_threaded",
 ]

@@ -188,6 +188,14 @@ class PairBatch(Structure):
     ]
 
 
+class BamParamsC(Structure):
+    _fields_ = [
+        ("chunk_size", c_int64), ("chunk_boundary", c_int64), ("include_soft_clip", c_int32),
+        ("include_secondary", c_int32), ("include_supplementary", c_int32), ("use_run_length", c_int32),
+        ("min_mapq", c_int64), ("region", c_char_p),
+    ]
+
+
 class PoaChunkInfo(Structure):
     _fields_ = [
         ("nodes", c_int64), ("max_repeat", c_int64), ("reference_runs", c_int64), ("observations", c_int64),
@@ -232,6 +240,8 @@ EXPORTED = [
     "mp_engine_set_graph_capture", "mp_realign_batch_into", "mp_engine_release_buffers", "mp_forward_pairs",
     "mp_forward_pairs_timing", "mp_measure_fp64_peak", "mp_poa_set_iterate_polish", "mp_poa_set_build_bubbles", "mp_poa_set_score_bubbles", "mp_poa_bubble_sizes",
     "mp_poa_bubbles", "mp_poa_bubble_consensus", "mp_merge_contig", "mp_match_pairs_reference",
+    "mp_bam_open", "mp_bam_close", "mp_bam_chunk_count", "mp_bam_chunk", "mp_bam_convert", "mp_bam_reads_sizes",
+    "mp_bam_reads",
 ]
 
 _lib = None
@@ -303,6 +313,14 @@ def load() -> ctypes.CDLL:
         "mp_merge_contig": (c_int, [c_void_p, c_void_p, P(Params), c_int64, P(c_int64), c_char_p, c_int64, c_int64,
                                     P(c_char), c_int64, P(c_int64), P(c_int64)]),
         "mp_forward_pairs_timing": (c_int, [c_void_p, P(c_float), P(c_int64), P(c_int64)]),
+        "mp_bam_open": (c_int, [c_char_p, P(BamParamsC), P(c_void_p)]),
+        "mp_bam_close": (None, [c_void_p]),
+        "mp_bam_chunk_count": (c_int, [c_void_p, P(c_int64)]),
+        "mp_bam_chunk": (c_int, [c_void_p, c_int64, P(c_char), c_int64, P(c_int64)]),
+        "mp_bam_convert": (c_int, [c_void_p, c_int64, c_int64, P(c_int64), c_char_p, c_int64, ctypes.c_uint64]),
+        "mp_bam_reads_sizes": (c_int, [c_void_p, c_int64, P(c_int64)]),
+        "mp_bam_reads": (c_int, [c_void_p, c_int64, P(c_int64), P(c_char), P(c_uint32), P(c_uint8), P(c_uint8),
+                                 P(c_uint8), P(c_int64), P(c_int32), P(c_int64), P(c_char)]),
         "mp_poa_set_realign_all": (c_int, [c_void_p]),
         "mp_poa_set_estimate_repeat_counts": (c_int, [c_void_p]),
         "mp_poa_info": (c_int, [c_void_p, c_int64, P(PoaChunkInfo)]),

@@ -375,3 +375,19 @@ def merge_contig(engine: Engine, model: Model, params: AlignmentParams, chunks: 
                                            _lib.ptr(off, c_int64), flat, int(overlap), int(spacer_length), out, cap,
                                            ctypes.byref(n), _lib.ptr(report, c_int64)))
     return bytes(out[:n.value]).decode(), report[:len(raw)].copy()
+
+def merge_contig_threaded(engine: Engine, model: Model, params: AlignmentParams, chunks: Sequence[str],
+                          overlap: int, groups: int, spacer_length: Optional[int] = None) -> str:
+    """mergeContigChunksThreaded (impl/chunker.c:114-152): the chunks split into `groups` runs of
+    ceil(n / groups) (fewer groups when the last would be empty), each run merged, then the
+    merged runs merged with the same overlap. One GPU call per run (each already batches its
+    boundaries), one for the runs."""
+    n = len(chunks)
+    if groups <= 1 or n == 0:
+        return merge_contig(engine, model, params, chunks, overlap, spacer_length)[0]
+    per = -(-n // groups)
+    while per * (groups - 1) >= n:
+        groups -= 1
+    runs = [merge_contig(engine, model, params, chunks[g * per:min(n, (g + 1) * per)], overlap, spacer_length)[0]
+            for g in range(groups)]
+    return merge_contig(engine, model, params, runs, overlap, spacer_length)[0]

@@ -16,7 +16,7 @@ import os
 import numpy as np
 import pytest
 
-from marginpolish_b200 import Jobs, Model, match_pairs_reference, merge_contig, params
+from marginpolish_b200 import Jobs, Model, match_pairs_reference, merge_contig, merge_contig_threaded, params
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -148,3 +148,29 @@ def test_overlap_zero_and_single_chunk(engine, stitch_env, polish_model):
     assert got == "".join(chunks) and report[:, 2].tolist() == [0, 0, 0]
     got, _ = merge_contig(engine, gm, polish_model.alignment, chunks[:1], 100)
     assert got == chunks[0]
+
+
+KA_CHUNKS = ["AAAAAAAACC", "AACCCCCCCCGG", "CCGGGGGGGGTT", "GGTTTTTTTT"]
+KA_THREADED = ["AAAAAAAACC", "AACCCCCCCCGG", "CCGGGGGGGGTT"] + \
+    ["GGTTTTTTTTAA", "TTAAAAAAAACC", "AACCCCCCCCGG", "CCGGGGGGGGTT"] * 3 + ["GGTTTTTTTT"]
+KA_TRUTH = "AAAAAAAACCCCCCCCGGGGGGGGTTTTTTTT"
+
+
+@pytest.fixture(scope="module")
+def default_model(engine):
+    default = params.code_default_state_model()
+    gm = Model(engine, default, default)
+    yield gm
+    gm.close()
+
+
+def test_merge_known_answers(engine, default_model, polish_model):
+    """test_mergeContigChunks and test_mergeContigChunksThreaded (tests/chunkingTest.c:907-960):
+    overlap 4, spacer "NNNNNN", with 1 to 8 merge groups."""
+    gm = default_model
+    got, report = merge_contig(engine, gm, polish_model.alignment, KA_CHUNKS, 4, 6)
+    assert got == KA_TRUTH
+    assert (report[1:, 0] > 0).all()
+    assert len(KA_THREADED) == 16
+    for groups in range(1, 9):
+        assert merge_contig_threaded(engine, gm, polish_model.alignment, KA_THREADED, 4, groups, 6) == KA_TRUTH * 4

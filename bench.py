@@ -457,9 +457,10 @@ def measure_polish_shipped(engine, model, pm):
         s.estimate_repeat_counts()
         t1 = time.perf_counter()
         changed = sum(int(s.reference(c).chars != wl.drafts[c].chars) for c in range(s.n_chunks))
+        phases = {k: round(v, 4) for k, v in s.phase_seconds().items()}
         s.close()
         if best is None or t1 - t0 < best["seconds"]:
-            best = {"seconds": t1 - t0, "chunks_changed": changed}
+            best = {"seconds": t1 - t0, "chunks_changed": changed, "phase_seconds": phases}
     best.update({"workload": "8 chunks x 10 kb (homopolymer-enriched), 50x, reads of 3-9 kb with base qualities, "
                              "drafts with 1% homopolymer-biased indels; no consensus iterations, one polish "
                              "iteration (params/allParams.np.json)",
@@ -584,8 +585,10 @@ def measure_polish_loop(engine, model, pm, wl, max_iterations):
     s.estimate_repeat_counts()
     t2 = time.perf_counter()
     its = [s.info(c)["iterations"] for c in range(s.n_chunks)]
+    phases = {k: round(v, 3) for k, v in s.phase_seconds().items()}
     s.close()
-    return {"seconds": t2 - t0, "realign_seconds": t1 - t0, "iterate_seconds": t2 - t1, "iterations": its,
+    return {"seconds": t2 - t0, "realign_seconds": t1 - t0, "iterate_seconds": t2 - t1, "phase_seconds": phases,
+            "iterations": its,
             "chunks": len(wl.drafts), "reads": int(sum(len(r) for r in wl.reads)),
             "bases": int(sum(r.non_rle_length for lst in wl.reads for r in lst))}
 

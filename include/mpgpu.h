@@ -462,6 +462,13 @@ mp_status mp_poa_bubble_consensus(const mp_poa_set *s, int64_t chunk, int64_t *p
 /* poa_estimateRepeatCountsUsingBayesianModel on every chunk's graph (sets the run lengths of
  * its reference string, as the caller of poa_realignAll does, marginPolish.c:558). */
 mp_status mp_poa_set_estimate_repeat_counts(mp_poa_set *s);
+/* Wall seconds the set has spent in each step of the loop since it was created, summed over
+ * calls: [0] job arrays of a realignment (crop, symbols, anchors), [1] the posterior pass on the
+ * GPU, [2] tuples into host arrays, [3] complete-indel candidates, [4] reads folded into the
+ * graphs, [5] consensus walks and anchor alignments, [6] run-length estimates and scores, [7]
+ * bubble graphs and their scores. Entries past 8 are set to 0. Instrumentation of this
+ * library's loop; the reference has no counterpart. */
+mp_status mp_poa_set_phase_seconds(const mp_poa_set *s, double *seconds, int64_t n);
 /* Inspection of a chunk's current graph (sizes from mp_poa_info). */
 mp_status mp_poa_info(const mp_poa_set *s, int64_t chunk, mp_poa_chunk_info *info);
 mp_status mp_poa_nodes(const mp_poa_set *s, int64_t chunk, char *bases, uint64_t *repeat_counts,

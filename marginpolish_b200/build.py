@@ -12,7 +12,8 @@ ROOT = os.path.dirname(HERE)
 
 
 def build_library() -> None:
-    subprocess.run(["make", "-C", os.path.join(HERE, "csrc"), os.path.join(HERE, "libmpgpu.so"),
+    subprocess.run(["make", "-j", str(max(1, min(os.cpu_count() or 1, 12))), "-C", os.path.join(HERE, "csrc"),
+                    os.path.join(HERE, "libmpgpu.so"),
                     os.path.join(HERE, "libmpgpu_dropin.so")], check=True)
 
 

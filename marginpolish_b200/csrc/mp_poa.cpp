@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -1024,6 +1025,27 @@ void forChunks(const std::vector<int64_t> &chunks, F f) {
 // the chunk set behind the C ABI
 // ---------------------------------------------------------------------------
 
+// Steps of the loop whose wall time a set accumulates (mp_poa_set_phase_seconds).
+enum {
+    kPhaseJobs,        // job arrays of a realignment (crop, symbols, anchors)
+    kPhaseDevice,      // the posterior pass on the GPU (upload, kernels, compaction)
+    kPhaseFetch,       // tuples into page-locked host arrays
+    kPhaseCandidates,  // complete-indel candidates of every read (host threads)
+    kPhaseMerge,       // reads folded into the chunks' graphs in read order
+    kPhaseConsensus,   // consensus walk and anchor alignments of an iteration
+    kPhaseRepeat,      // run-length estimate and score of the new graphs
+    kPhaseBubbles,     // bubble graphs and their scores (polish mode)
+    kPhaseCount
+};
+
+// Adds the wall time of its scope to one phase counter.
+struct PhaseTimer {
+    double &acc;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    explicit PhaseTimer(double &a) : acc(a) {}
+    ~PhaseTimer() { acc += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+};
+
 struct mp_poa_set {
     mp_engine *e = nullptr;
     const mp_model *m = nullptr;
@@ -1053,6 +1075,8 @@ struct mp_poa_set {
     // page-locked tuple arrays of the last realignment (grow only): the copies run by DMA
     void *pinned[3] = {nullptr, nullptr, nullptr};
     size_t pinnedCap[3] = {0, 0, 0};  // tuples
+    // Wall seconds spent in each step of the loop since the set was created (kPhase*).
+    double phase[kPhaseCount] = {};
     ~mp_poa_set() {
         mp_device_batch_destroy(db);
         for (void *q : pinned) mp_host_free(q);
@@ -1082,6 +1106,7 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
     };
     // jobs: one per read of the listed chunks, with the reference crop (impl/polisher.c:613-628).
     // Offsets first (chunk order, reads in order), then every chunk's arrays filled in parallel.
+    auto tJobs = std::chrono::steady_clock::now();
     std::vector<int64_t> refStart(s->nChunks, 0), firstJobOf(s->nChunks, 0);
     std::vector<int64_t> yo{0}, ao{0};
     int64_t nx = 0;
@@ -1131,7 +1156,9 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
     std::vector<int64_t> offs[3];
     const int32_t *w[3] = {nullptr, nullptr, nullptr}, *x[3] = {nullptr, nullptr, nullptr},
                   *y[3] = {nullptr, nullptr, nullptr};
+    s->phase[kPhaseJobs] += std::chrono::duration<double>(std::chrono::steady_clock::now() - tJobs).count();
     if (nJobs > 0) {
+        PhaseTimer tDev(s->phase[kPhaseDevice]);
         mp_batch b;
         memset(&b, 0, sizeof(b));
         b.n_jobs = nJobs;
@@ -1152,6 +1179,10 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
         if (rc != MP_OK) return rc;
         rc = mp_device_batch_run(s->e, s->db, nullptr);
         if (rc != MP_OK) return rc;
+    }
+    if (nJobs > 0) {
+        PhaseTimer tFetch(s->phase[kPhaseFetch]);
+        mp_status rc;
         int64_t totals[3];
         rc = mp_device_batch_counts(s->db, totals);
         if (rc != MP_OK) return rc;
@@ -1202,16 +1233,20 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
             jobRead[(size_t) j] = r;
         }
     std::vector<IndelCands> cands(jobIdx.size());
-    forChunks(jobIdx, [&](int64_t j) {
-        thread_local std::vector<Pair> lists[3];
-        for (int k = 0; k < 3; k++) {
-            lists[k].clear();
-            for (int64_t t = offs[k][j]; t < offs[k][j + 1]; t++) lists[k].push_back(Pair{w[k][t], x[k][t], y[k][t]});
-        }
-        indelCandidates(refs[jobChunk[(size_t) j]], s->reads[jobRead[(size_t) j]], lists[0], lists[2], lists[1],
-                        s->cmpRC, cands[(size_t) j]);
-    });
+    {
+        PhaseTimer tCands(s->phase[kPhaseCandidates]);
+        forChunks(jobIdx, [&](int64_t j) {
+            thread_local std::vector<Pair> lists[3];
+            for (int k = 0; k < 3; k++) {
+                lists[k].clear();
+                for (int64_t t = offs[k][j]; t < offs[k][j + 1]; t++) lists[k].push_back(Pair{w[k][t], x[k][t], y[k][t]});
+            }
+            indelCandidates(refs[jobChunk[(size_t) j]], s->reads[jobRead[(size_t) j]], lists[0], lists[2], lists[1],
+                            s->cmpRC, cands[(size_t) j]);
+        });
+    }
     // then each chunk's graph, reads in order (chunks in parallel)
+    PhaseTimer tMerge(s->phase[kPhaseMerge]);
     forChunks(chunks, [&](int64_t c) {
         Poa poa = Poa::fromReference(refs[c], maxRC);
         for (int64_t r = s->chunkReads[c]; r < s->chunkReads[c + 1]; r++) {
@@ -1360,10 +1395,12 @@ mp_status iterate(mp_poa_set *s, bool polishMode) {
     while (!active.empty()) {
         std::vector<uint8_t> realign(nC, 0);
         if (polishMode) {
+            PhaseTimer t(s->phase[kPhaseBubbles]);
             forChunks(active, [&](int64_t c) { graphs[c] = buildBubblesOf(s, c); });
             MP_TRY(scoreBubbles(s, active, graphs));
         }
         std::vector<std::vector<Anchor>> anchors(s->reads.size());
+        auto tCons = std::chrono::steady_clock::now();
         forChunks(active, [&](int64_t c) {
             s->iterations[c]++;
             if (polishMode) {
@@ -1377,6 +1414,7 @@ mp_status iterate(mp_poa_set *s, bool polishMode) {
             for (int64_t r = 0; r < (int64_t) a.size(); r++) anchors[s->chunkReads[c] + r] = std::move(a[r]);
             realign[c] = 1;
         });
+        s->phase[kPhaseConsensus] += std::chrono::duration<double>(std::chrono::steady_clock::now() - tCons).count();
         std::vector<int64_t> go;
         for (int64_t c : active)
             if (realign[c]) go.push_back(c);
@@ -1384,6 +1422,7 @@ mp_status iterate(mp_poa_set *s, bool polishMode) {
         MP_TRY(realignChunks(s, go, cons, &anchors, next));
         std::vector<int64_t> still;
         std::vector<uint8_t> keep(nC, 0);
+        PhaseTimer tRep(s->phase[kPhaseRepeat]);
         forChunks(go, [&](int64_t c) {
             if (s->useRle) estimateRepeatCounts(next[c], s->reads, s->strand, s->chunkReads[c], s->rm);
             const double sc2 = score(next[c]);
@@ -1653,7 +1692,14 @@ extern "C" mp_status mp_poa_set_estimate_repeat_counts(mp_poa_set *s) {
     if (!s->useRle) return MP_OK;
     std::vector<int64_t> all(s->nChunks);
     for (int64_t c = 0; c < s->nChunks; c++) all[c] = c;
+    PhaseTimer t(s->phase[kPhaseRepeat]);
     forChunks(all, [&](int64_t c) { estimateRepeatCounts(s->poas[c], s->reads, s->strand, s->chunkReads[c], s->rm); });
+    return MP_OK;
+}
+
+extern "C" mp_status mp_poa_set_phase_seconds(const mp_poa_set *s, double *seconds, int64_t n) {
+    if (!s || (!seconds && n > 0) || n < 0) return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_phase_seconds: bad arguments");
+    for (int64_t k = 0; k < n; k++) seconds[k] = k < kPhaseCount ? s->phase[k] : 0.0;
     return MP_OK;
 }
 

@@ -240,6 +240,15 @@ class PoaSet:
     def estimate_repeat_counts(self) -> None:
         _lib.check(self._lib.mp_poa_set_estimate_repeat_counts(self.handle))
 
+    PHASES = ("jobs", "device_pass", "fetch", "indel_candidates", "merge", "consensus", "repeat_counts",
+              "bubbles")
+
+    def phase_seconds(self) -> dict:
+        """Wall seconds spent in each step of the loop since the set was created."""
+        v = np.zeros(len(self.PHASES))
+        _lib.check(self._lib.mp_poa_set_phase_seconds(self.handle, _lib.ptr(v, c_double), v.size))
+        return {k: float(x) for k, x in zip(self.PHASES, v)}
+
     # ---- inspection ----
     def info(self, chunk: int) -> dict:
         i = _lib.PoaChunkInfo()

@@ -318,6 +318,49 @@ mp_status mp_forward_pairs(mp_engine *e, const mp_model *m, const mp_pair_batch 
  * engine's stream), its matrix cells (sum of (x_length + 1) (y_length + 1)) and its pairs. */
 mp_status mp_forward_pairs_timing(mp_engine *e, float *kernel_ms, int64_t *cells, int64_t *pairs);
 
+/* ---- device-side node update of the POA graphs ----
+ * The match part of poa_augment (impl/polisher.c:322-340) and the run-length estimate
+ * (poa_estimateRepeatCountsUsingBayesianModel, impl/polisher.c:1556-1565, :1796-1865) for every
+ * graph of a batch of chunks at once, on the GPU, from the aligner's match tuples. A chunk's graph
+ * has node 0 (the 'N' prefix) and node i >= 1 for reference run i-1; a match (weight, x, y) of a
+ * read adds to node x+1 the weight in the bin of the read's base at run y and in the bin of its
+ * run length (clamped below max_repeat), and appends the observation (read number within the
+ * chunk, y, weight). Observations keep poa_augment's order: reads in order, each read's tuples in
+ * the given order. The run-length estimate of node i >= 1 is the reference's maximum-likelihood
+ * count over its observations (1 when it has none), bit-identical: every product and sum is
+ * rounded separately, in the reference's order. */
+typedef struct {
+    int64_t n_chunks;
+    const int64_t *node_offsets;   /* n_chunks + 1 (starts at 0): chunk c's nodes, node 0 first */
+    const char *node_bases;        /* per node: its base (the prefix node 'N') */
+    const int64_t *chunk_reads;    /* n_chunks + 1 (starts at 0): chunk c's reads */
+    const int64_t *read_offsets;   /* n_reads + 1 (starts at 0): runs of read r */
+    const char *read_chars;        /* run characters of every read */
+    const uint32_t *read_counts;   /* run lengths of every read */
+    const uint8_t *strand;         /* per read: 1 forward strand */
+    const int64_t *match_offsets;  /* n_reads + 1 (starts at 0): match tuples of read r */
+    const int32_t *weight;         /* match tuples (weight, x, y): x a run of the chunk's reference, */
+    const int32_t *x;              /* y a run of the read */
+    const int32_t *y;
+    int64_t max_repeat;            /* the graphs' maxRepeatCount (the repeat table's dimension M) */
+    const double *repeat_log10;    /* [4][M][M] log10 P(observed | underlying) per base row (the
+                                    * polish model's table); NULL: no run-length estimate */
+} mp_node_batch;
+
+/* Outputs of mp_node_update; any may be NULL. */
+typedef struct {
+    double *base_weights;    /* [nodes][5] (A C G T N) */
+    double *repeat_weights;  /* [nodes][max_repeat] */
+    int64_t *obs_offsets;    /* nodes + 1: node g's observations are [obs_offsets[g], obs_offsets[g+1]) */
+    int64_t *obs_read;       /* [tuples]: read number within the chunk */
+    int64_t *obs_offset;     /* [tuples]: run of the read */
+    double *obs_weight;      /* [tuples] */
+    uint64_t *repeat_counts; /* [nodes]: the estimate (0 for each chunk's node 0) */
+} mp_node_result;
+
+/* A tuple outside its chunk's graph or its read is MP_ERR_ARGUMENT. */
+mp_status mp_node_update(mp_engine *e, const mp_node_batch *b, const mp_node_result *r);
+
 /* ---- adjoint: expected counts = gradient of the summed log-likelihood ----
  * For the FP32 scaled-probability DP over each job's band (the posterior pass's band,
  * splits and ragged ends, but one walk over the whole lattice: no traceback segments), the

@@ -136,6 +136,8 @@ extern "C" void mp_engine_destroy(mp_engine *e) {
         e->pipe[k] = nullptr;
     }
     if (e->outStream) cudaStreamDestroy(e->outStream);
+    mp_node_scratch_free(e->nodeScratch);
+    e->nodeScratch = nullptr;
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }

@@ -139,8 +139,12 @@ struct mp_engine {
     struct mp_device_batch *pipe[kPipeSlots] = {};  // the slots of mp_realign_batch_into (own streams)
     cudaStream_t outStream = nullptr;  // tuple copies of mp_realign_batch_into's slots, in slice order
     mp_pair_scratch pairScratch;       // mp_forward_pairs (under oneShotLock)
+    struct mp_node_scratch *nodeScratch = nullptr;  // mp_node_update's device arrays
     std::mutex oneShotLock;
 };
+
+// Frees the node update's device arrays (mp_nodes.cu).
+void mp_node_scratch_free(struct mp_node_scratch *s);
 
 struct mp_model {
     mp_engine *engine = nullptr;

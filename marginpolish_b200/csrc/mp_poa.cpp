@@ -163,6 +163,9 @@ struct Poa {
     std::vector<Obs> obs;
     std::vector<int32_t> obsNode;
     std::vector<int64_t> obsStart;
+    // Run-length estimate of nodes 1.. computed on the GPU from the tuples the graph was built
+    // from (mp_node_update); empty when the graph was built on the host only.
+    std::vector<uint64_t> ml;
 
     double *rcwOf(int64_t i) { return rcw.data() + i * (int64_t) maxRC; }
     const double *rcwOf(int64_t i) const { return rcw.data() + i * (int64_t) maxRC; }
@@ -383,22 +386,29 @@ void indelCandidates(const Rle &ref, const Rle &read, const std::vector<Pair> &m
     }
 }
 
-// Adds one read to the graph: match weights and observations (tuple order), then its complete
-// indels, each merged into an equal insert / delete of its node or appended as a new one.
+// Adds one read to the nodes [lo, hi) of the graph: match weights and observations (tuple
+// order; the observations go to obs / obsNode for grouping), then its complete indels, each
+// merged into an equal insert / delete of its node or appended as a new one. Every list a node
+// holds grows in read order whichever range the node is merged in, so merging disjoint ranges
+// on different threads gives the graph of one sequential merge.
 void mergeRead(Poa &poa, const Rle &read, bool strand, int64_t readNo, int64_t nMatches, const int32_t *mw,
-               const int32_t *mx, const int32_t *my, const IndelCands &ic) {
+               const int32_t *mx, const int32_t *my, const IndelCands &ic, int64_t lo, int64_t hi,
+               std::vector<Obs> &obs, std::vector<int32_t> &obsNode) {
     for (int64_t t = 0; t < nMatches; t++) {
-        Node &node = poa.nodes[mx[t] + 1];
+        const int64_t v = mx[t] + 1;
+        if (v < lo || v >= hi) continue;
+        Node &node = poa.nodes[v];
         const double w = (double) mw[t];
         node.bw[symbolOf(read.c[my[t]])] += w;
         uint64_t rc = read.n[my[t]];
         if (rc >= poa.maxRC) rc = poa.maxRC - 1;
-        poa.rcwOf(mx[t] + 1)[rc] += w;
-        poa.obs.push_back(Obs{readNo, my[t], w});
-        poa.obsNode.push_back((int32_t) (mx[t] + 1));
+        poa.rcwOf(v)[rc] += w;
+        obs.push_back(Obs{readNo, my[t], w});
+        obsNode.push_back((int32_t) v);
     }
     const int64_t n = (int64_t) ic.pos.size();
     for (int64_t q = 0; q < n; q++) {
+        if (ic.pos[q] < lo || ic.pos[q] >= hi) continue;
         Node &node = poa.nodes[ic.pos[q]];
         const double w = ic.w[q];
         if (q < ic.nIns) {
@@ -451,7 +461,8 @@ void augment(Poa &poa, const Rle &read, bool strand, int64_t readNo, const std::
         x[t] = (int32_t) matches[t].x;
         y[t] = (int32_t) matches[t].y;
     }
-    mergeRead(poa, read, strand, readNo, (int64_t) matches.size(), w.data(), x.data(), y.data(), ic);
+    mergeRead(poa, read, strand, readNo, (int64_t) matches.size(), w.data(), x.data(), y.data(), ic, 0,
+              (int64_t) poa.nodes.size(), poa.obs, poa.obsNode);
 }
 
 // ---------------------------------------------------------------------------
@@ -671,8 +682,9 @@ uint64_t mlRepeatCount(const Poa &poa, int64_t i, const std::vector<Rle> &reads,
 void estimateRepeatCounts(Poa &poa, const std::vector<Rle> &reads, const std::vector<uint8_t> &strand, int64_t readBase,
                           const RepeatModel &rm) {
     poa.ref.nonRle = 0;
+    const bool device = poa.ml.size() + 1 == poa.nodes.size();
     for (size_t i = 1; i < poa.nodes.size(); i++) {
-        uint64_t rc = mlRepeatCount(poa, (int64_t) i, reads, strand, readBase, rm);
+        uint64_t rc = device ? poa.ml[i - 1] : mlRepeatCount(poa, (int64_t) i, reads, strand, readBase, rm);
         if (rc == 0) rc = 1;
         poa.ref.n[i - 1] = rc;
         poa.ref.nonRle += rc;
@@ -1077,6 +1089,10 @@ struct mp_poa_set {
     size_t pinnedCap[3] = {0, 0, 0};  // tuples
     // Wall seconds spent in each step of the loop since the set was created (kPhase*).
     double phase[kPhaseCount] = {};
+    // every read's runs in one array each (the device-side node update's input)
+    std::vector<int64_t> flatReadOff;
+    std::string flatReadChars;
+    std::vector<uint32_t> flatReadCounts;
     ~mp_poa_set() {
         mp_device_batch_destroy(db);
         for (void *q : pinned) mp_host_free(q);
@@ -1084,6 +1100,55 @@ struct mp_poa_set {
 };
 
 namespace {
+
+// The run-length estimate (impl/polisher.c:1556-1565) of the graphs realignChunks builds for
+// `chunks`, on the GPU from the realignment's match tuples (jobs of the listed chunks in order,
+// tuples of job j at [off[j], off[j+1])). Every chunk of the set is a graph of the batch; the
+// unlisted ones have no tuples. ml receives every node's estimate, chunk c's nodes starting at
+// nodeBase[c].
+mp_status deviceRepeatCounts(mp_poa_set *s, const std::vector<int64_t> &chunks, const std::vector<Rle> &refs,
+                             const std::vector<int64_t> &off, const int32_t *w, const int32_t *x, const int32_t *y,
+                             std::vector<uint64_t> &ml, std::vector<int64_t> &nodeBase) {
+    const int64_t nC = s->nChunks, nReads = (int64_t) s->reads.size();
+    std::vector<uint8_t> listed((size_t) nC, 0);
+    for (int64_t c : chunks) listed[(size_t) c] = 1;
+    nodeBase.assign((size_t) nC + 1, 0);
+    std::string bases;
+    for (int64_t c = 0; c < nC; c++) {
+        bases.push_back('N');
+        if (listed[(size_t) c]) bases.append(refs[c].c);
+        nodeBase[(size_t) c + 1] = (int64_t) bases.size();
+    }
+    // match offsets per read of the set: the listed chunks' jobs are their reads, in order
+    std::vector<int64_t> mOff((size_t) nReads + 1, 0);
+    int64_t j = 0, at = 0;
+    for (int64_t c = 0; c < nC; c++)
+        for (int64_t r = s->chunkReads[c]; r < s->chunkReads[c + 1]; r++) {
+            if (listed[(size_t) c]) at = off[(size_t) j++ + 1];
+            mOff[(size_t) r + 1] = at;
+        }
+    mp_node_batch b;
+    memset(&b, 0, sizeof(b));
+    b.n_chunks = nC;
+    b.node_offsets = nodeBase.data();
+    b.node_bases = bases.data();
+    b.chunk_reads = s->chunkReads.data();
+    b.read_offsets = s->flatReadOff.data();
+    b.read_chars = s->flatReadChars.data();
+    b.read_counts = s->flatReadCounts.data();
+    b.strand = s->strand.data();
+    b.match_offsets = mOff.data();
+    b.weight = w;
+    b.x = x;
+    b.y = y;
+    b.max_repeat = s->rm.M;
+    b.repeat_log10 = s->rm.log10.data();
+    ml.assign(bases.size(), 0);
+    mp_node_result r;
+    memset(&r, 0, sizeof(r));
+    r.repeat_counts = ml.data();
+    return mp_node_update(s->e, &b, &r);
+}
 
 // poa_realign (impl/polisher.c:656-703) for the given chunks, each against `refs[c]` with
 // per-read anchors (NULL: align without anchors): one GPU batch for every read, then each
@@ -1212,6 +1277,16 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
         rc = mp_device_batch_fetch_into(s->e, s->db, &o);
         if (rc != MP_OK) return rc;
     }
+    // The run-length estimate of the new graphs runs on the GPU (mp_node_update, from the same
+    // match tuples) while the host threads fold the reads into the graphs.
+    std::vector<uint64_t> ml;
+    std::vector<int64_t> nodeBase;
+    mp_status mlStatus = MP_OK;
+    std::thread mlThread;
+    if (s->useRle && nJobs > 0) {
+        mlThread = std::thread([&]() { mlStatus = deviceRepeatCounts(s, chunks, refs, offs[0], w[0], x[0], y[0], ml,
+                                                                     nodeBase); });
+    }
     // fold each chunk's reads into its graph (chunks in parallel, reads in order)
     std::vector<int64_t> firstJob(s->nChunks, 0);
     {
@@ -1245,20 +1320,52 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
                             s->cmpRC, cands[(size_t) j]);
         });
     }
-    // then each chunk's graph, reads in order (chunks in parallel)
+    // then each chunk's graph, reads in order. With fewer chunks than host threads, a chunk's
+    // nodes are split into ranges merged on separate threads (each range takes every read in
+    // order, so every node's lists keep the sequential order).
     PhaseTimer tMerge(s->phase[kPhaseMerge]);
-    forChunks(chunks, [&](int64_t c) {
-        Poa poa = Poa::fromReference(refs[c], maxRC);
+    const int64_t nT = std::max(1u, std::thread::hardware_concurrency());
+    const int64_t P = std::max<int64_t>(1, std::min<int64_t>(8, (2 * nT + (int64_t) chunks.size() - 1) /
+                                                                   std::max<int64_t>(1, (int64_t) chunks.size())));
+    forChunks(chunks, [&](int64_t c) { out[c] = Poa::fromReference(refs[c], maxRC); });
+    std::vector<int64_t> items;
+    for (int64_t c : chunks)
+        for (int64_t k = 0; k < P; k++) items.push_back(c * P + k);
+    std::vector<std::vector<Obs>> rangeObs((size_t) (s->nChunks * P));
+    std::vector<std::vector<int32_t>> rangeNode((size_t) (s->nChunks * P));
+    forChunks(items, [&](int64_t item) {
+        const int64_t c = item / P, k = item % P;
+        Poa &poa = out[c];
+        const int64_t nN = (int64_t) poa.nodes.size();
+        const int64_t lo = nN * k / P, hi = nN * (k + 1) / P;
         for (int64_t r = s->chunkReads[c]; r < s->chunkReads[c + 1]; r++) {
             const int64_t j = firstJob[c] + (r - s->chunkReads[c]);
             const int64_t t0 = offs[0][j];
             mergeRead(poa, s->reads[r], s->strand[r] != 0, r - s->chunkReads[c], offs[0][j + 1] - t0, w[0] + t0,
-                      x[0] + t0, y[0] + t0, cands[(size_t) j]);
-            cands[(size_t) j] = IndelCands();  // release as we go
+                      x[0] + t0, y[0] + t0, cands[(size_t) j], lo, hi, rangeObs[(size_t) item],
+                      rangeNode[(size_t) item]);
+        }
+    });
+    forChunks(chunks, [&](int64_t c) {
+        Poa &poa = out[c];
+        for (int64_t k = 0; k < P; k++) {
+            std::vector<Obs> &o = rangeObs[(size_t) (c * P + k)];
+            std::vector<int32_t> &v = rangeNode[(size_t) (c * P + k)];
+            poa.obs.insert(poa.obs.end(), o.begin(), o.end());
+            poa.obsNode.insert(poa.obsNode.end(), v.begin(), v.end());
+            std::vector<Obs>().swap(o);
+            std::vector<int32_t>().swap(v);
         }
         poa.groupObs();
-        out[c] = std::move(poa);
+        for (int64_t r = s->chunkReads[c]; r < s->chunkReads[c + 1]; r++)
+            cands[(size_t) (firstJob[c] + (r - s->chunkReads[c]))] = IndelCands();
     });
+    if (mlThread.joinable()) {
+        mlThread.join();
+        if (mlStatus != MP_OK) return mlStatus;
+        for (int64_t c : chunks)
+            out[c].ml.assign(ml.begin() + nodeBase[c] + 1, ml.begin() + nodeBase[c] + refs[c].length() + 1);
+    }
     return MP_OK;
 }
 
@@ -1521,6 +1628,8 @@ extern "C" mp_status mp_poa_set_create(mp_engine *e, const mp_model *m, const mp
         }
         s->reads.push_back(rr);
         s->strand.push_back(b->strand[r]);
+        s->flatReadChars.append(rr.c);
+        for (uint64_t k : rr.n) s->flatReadCounts.push_back((uint32_t) k);
         if (b->read_qualities)
             s->quals.emplace_back(b->read_qualities + b->read_offsets[r], b->read_qualities + b->read_offsets[r + 1]);
         std::vector<Anchor> a;
@@ -1530,6 +1639,8 @@ extern "C" mp_status mp_poa_set_create(mp_engine *e, const mp_model *m, const mp
         s->initialAnchors.push_back(a);
     }
     s->iterations.assign(s->nChunks, 0);
+    s->flatReadOff.assign((size_t) nReads + 1, 0);
+    for (int64_t r = 0; r < nReads; r++) s->flatReadOff[(size_t) r + 1] = s->flatReadOff[(size_t) r] + s->reads[r].length();
     s->bubbles.resize(s->nChunks);
     *out = s;
     return MP_OK;

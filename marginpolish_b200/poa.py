@@ -400,3 +400,81 @@ def merge_contig_threaded(engine: Engine, model: Model, params: AlignmentParams,
     runs = [merge_contig(engine, model, params, chunks[g * per:min(n, (g + 1) * per)], overlap, spacer_length)[0]
             for g in range(groups)]
     return merge_contig(engine, model, params, runs, overlap, spacer_length)[0]
+
+
+def node_update(engine: Engine, drafts: Sequence[RleString], reads: Sequence[Sequence[RleString]],
+                strands: Sequence[Sequence[int]], matches: Sequence[np.ndarray], max_repeat: int,
+                repeat_log10: Optional[np.ndarray] = None, observations: bool = True) -> dict:
+    """The device-side node update (mp_node_update) of one graph per draft: the match part of
+    poa_augment (impl/polisher.c:322-340) and the run-length estimate (:1556-1565, :1796-1865).
+    matches[r] is the (n, 3) (weight, x, y) match list of read r (all chunks' reads in order).
+    Returns per chunk the base weights, run-length weights, observations (read, offset, weight) in
+    poa_augment's order and, with repeat_log10, the estimated run length of every node."""
+    lib = engine._lib
+    n_chunks = len(drafts)
+    node_off = np.zeros(n_chunks + 1, dtype=np.int64)
+    node_off[1:] = np.cumsum([len(d) + 1 for d in drafts])
+    bases = b"".join(b"N" + bytes(b if chr(b) in "ACGT" else ord("N") for b in d.chars.upper()) for d in drafts)
+    flat = [r for lst in reads for r in lst]
+    chunk_reads = np.zeros(n_chunks + 1, dtype=np.int64)
+    chunk_reads[1:] = np.cumsum([len(lst) for lst in reads])
+    rd_off, rd_chars, rd_counts = _flat_rle(flat)
+    strand = np.ascontiguousarray([int(s) for lst in strands for s in lst], dtype=np.uint8)
+    if strand.size != len(flat) or len(matches) != len(flat):
+        raise ValueError("one strand and one match list per read")
+    lists = [np.asarray(m, dtype=np.int64).reshape(-1, 3) for m in matches]
+    m_off = np.zeros(len(lists) + 1, dtype=np.int64)
+    m_off[1:] = np.cumsum([a.shape[0] for a in lists])
+    allm = np.concatenate(lists) if lists else np.zeros((0, 3), np.int64)
+    w = np.ascontiguousarray(allm[:, 0], dtype=np.int32)
+    x = np.ascontiguousarray(allm[:, 1], dtype=np.int32)
+    y = np.ascontiguousarray(allm[:, 2], dtype=np.int32)
+    rep = None if repeat_log10 is None else np.ascontiguousarray(repeat_log10, dtype=np.float64).reshape(-1)
+    b = _lib.NodeBatch()
+    b.n_chunks = n_chunks
+    b.node_offsets = _lib.ptr(node_off, c_int64)
+    bases_buf = ctypes.create_string_buffer(bases, max(len(bases), 1))
+    b.node_bases = ctypes.cast(bases_buf, ctypes.POINTER(c_char))
+    b.chunk_reads = _lib.ptr(chunk_reads, c_int64)
+    b.read_offsets = _lib.ptr(rd_off, c_int64)
+    chars_buf = ctypes.create_string_buffer(rd_chars or b"\0", max(len(rd_chars), 1))
+    b.read_chars = ctypes.cast(chars_buf, ctypes.POINTER(c_char))
+    b.read_counts = _lib.ptr(rd_counts if rd_counts.size else np.zeros(1, np.uint32), c_uint32)
+    b.strand = _lib.ptr(strand if strand.size else np.zeros(1, np.uint8), c_uint8)
+    b.match_offsets = _lib.ptr(m_off, c_int64)
+    b.weight = _lib.ptr(w if w.size else np.zeros(1, np.int32), c_int32)
+    b.x = _lib.ptr(x if x.size else np.zeros(1, np.int32), c_int32)
+    b.y = _lib.ptr(y if y.size else np.zeros(1, np.int32), c_int32)
+    b.max_repeat = int(max_repeat)
+    b.repeat_log10 = _lib.ptr(rep, c_double)
+    n_nodes, n_tup = int(node_off[-1]), int(m_off[-1])
+    bw = np.zeros((max(n_nodes, 1), 5))
+    rcw = np.zeros((max(n_nodes, 1), int(max_repeat)))
+    obs_off = np.zeros(n_nodes + 1, dtype=np.int64)
+    o_read, o_off = np.zeros(max(n_tup, 1), np.int64), np.zeros(max(n_tup, 1), np.int64)
+    o_w = np.zeros(max(n_tup, 1))
+    rc = np.zeros(max(n_nodes, 1), np.uint64)
+    r = _lib.NodeResult()
+    r.base_weights = _lib.ptr(bw, c_double)
+    r.repeat_weights = _lib.ptr(rcw, c_double)
+    r.obs_offsets = _lib.ptr(obs_off, c_int64)
+    if observations:
+        r.obs_read = _lib.ptr(o_read, c_int64)
+        r.obs_offset = _lib.ptr(o_off, c_int64)
+        r.obs_weight = _lib.ptr(o_w, c_double)
+    if rep is not None:
+        r.repeat_counts = _lib.ptr(rc, c_uint64)
+    _lib.check(lib.mp_node_update(engine.handle, ctypes.byref(b), ctypes.byref(r)))
+    out = []
+    for c in range(n_chunks):
+        g0, g1 = int(node_off[c]), int(node_off[c + 1])
+        o0, o1 = int(obs_off[g0]), int(obs_off[g1])
+        d = {"base_weights": bw[g0:g1].copy(), "repeat_count_weights": rcw[g0:g1].copy(),
+             "n_obs": np.diff(obs_off[g0:g1 + 1])}
+        if observations:
+            d["observations"] = np.stack([o_read[o0:o1], o_off[o0:o1], o_w[o0:o1]], axis=1) if o1 > o0 \
+                else np.zeros((0, 3))
+        if rep is not None:
+            d["repeat_counts"] = rc[g0 + 1:g1].copy()
+        out.append(d)
+    return {"chunks": out}

@@ -75,6 +75,10 @@ def parse():
                     help="skip the adjoint and POA-loop measurements reported beside the headline")
     ap.add_argument("--bubble-scores", action="store_true",
                     help="only the polish step's bubble-score measurement (one JSON line; no CPU sample)")
+    ap.add_argument("--polish-shipped", action="store_true",
+                    help="only the shipped polishing loop's measurement, with its per-step times (one JSON line)")
+    ap.add_argument("--device-indels", action="store_true",
+                    help="polishing loops find the reads' indel candidates on the GPU (MP_POA_DEVICE_INDELS)")
     return ap.parse_args()
 
 
@@ -442,7 +446,7 @@ def reference_bubble_sample(pm):
             "sample": "bubbleGraph_constructFromPoa (construction and scores) on one 3 kb chunk at 50x, one core"}
 
 
-def measure_polish_shipped(engine, model, pm):
+def measure_polish_shipped(engine, model, pm, device_indels=False):
     """The shipped loop (poa_realignAll with one polish iteration, then the run-length estimate)
     over the polish workload: realignment, bubble graphs, scores, new consensus, anchors,
     second realignment."""
@@ -452,6 +456,7 @@ def measure_polish_shipped(engine, model, pm):
     for _ in range(2):
         s = PoaSet.from_polish_model(engine, model, pm, PolishParams.shipped(), wl.drafts, wl.reads, wl.strands,
                                      wl.anchors, quals)
+        s.set_device_steps(run_lengths=True, indels=device_indels)
         t0 = time.perf_counter()
         s.realign_all()
         s.estimate_repeat_counts()
@@ -819,6 +824,13 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+    elif args.polish_shipped:
+        from marginpolish_b200 import Engine, Model, params
+        pm = params.polish_model_from_npz(os.path.join(ROOT, "tests", "golden", "model_np.npz"))
+        engine = Engine(local)
+        model = Model.from_polish(engine, pm)
+        print(json.dumps({"polish_loop_shipped": measure_polish_shipped(engine, model, pm, args.device_indels)}),
+              flush=True)
     elif args.bubble_scores:
         from marginpolish_b200 import Engine, Model, params
         pm = params.polish_model_from_npz(os.path.join(ROOT, "tests", "golden", "model_np.npz"))

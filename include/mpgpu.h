@@ -509,9 +509,19 @@ mp_status mp_poa_set_estimate_repeat_counts(mp_poa_set *s);
  * calls: [0] job arrays of a realignment (crop, symbols, anchors), [1] the posterior pass on the
  * GPU, [2] tuples into host arrays, [3] complete-indel candidates, [4] reads folded into the
  * graphs, [5] consensus walks and anchor alignments, [6] run-length estimates and scores, [7]
- * bubble graphs and their scores. Entries past 8 are set to 0. Instrumentation of this
- * library's loop; the reference has no counterpart. */
+ * bubble graphs and their scores, [8] the graphs' observation lists put together, [9] waiting for the
+ * GPU's run-length estimate after the merge. Entries past 10 are set to 0. Instrumentation of
+ * this library's loop; the reference has no counterpart. */
 mp_status mp_poa_set_phase_seconds(const mp_poa_set *s, double *seconds, int64_t n);
+/* Steps of a realignment that run on the GPU instead of the host threads; both forms build
+ * identical graphs. MP_POA_DEVICE_RUN_LENGTHS (the default): the new graphs' run lengths
+ * (impl/polisher.c:1556-1565) by mp_node_update, while the host threads fold the reads.
+ * MP_POA_DEVICE_INDELS: every read's complete-indel candidates (poa_augment,
+ * impl/polisher.c:354-522) in one GPU pass; off by default, because moving the tuples up and the
+ * candidates down costs more than the host threads' enumeration at these sizes. */
+#define MP_POA_DEVICE_RUN_LENGTHS 1
+#define MP_POA_DEVICE_INDELS 2
+mp_status mp_poa_set_device_steps(mp_poa_set *s, int32_t steps);
 /* Inspection of a chunk's current graph (sizes from mp_poa_info). */
 mp_status mp_poa_info(const mp_poa_set *s, int64_t chunk, mp_poa_chunk_info *info);
 mp_status mp_poa_nodes(const mp_poa_set *s, int64_t chunk, char *bases, uint64_t *repeat_counts,

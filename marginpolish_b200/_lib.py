@@ -265,7 +265,7 @@ EXPORTED = [
     "mp_realign_single_noalloc", "mp_device_batch_reset", "mp_device_batch_counts", "mp_device_batch_fetch_into",
     "mp_host_alloc", "mp_host_free", "mp_device_batch_run_plain", "mp_forward_batch", "mp_expectations_batch",
     "mp_poa_set_create", "mp_poa_set_destroy", "mp_poa_set_realign", "mp_poa_set_realign_pairs", "mp_poa_set_iterate",
-    "mp_poa_set_realign_all", "mp_poa_set_estimate_repeat_counts", "mp_poa_set_phase_seconds", "mp_node_update", "mp_poa_info", "mp_poa_nodes",
+    "mp_poa_set_realign_all", "mp_poa_set_estimate_repeat_counts", "mp_poa_set_phase_seconds", "mp_poa_set_device_steps", "mp_node_update", "mp_poa_info", "mp_poa_nodes",
     "mp_poa_observations", "mp_poa_inserts", "mp_poa_deletes", "mp_poa_reference", "mp_poa_consensus",
     "mp_poa_anchor_alignments", "mp_engine_autotune", "mp_engine_autotune_reset",
     "mp_engine_set_graph_capture", "mp_realign_batch_into", "mp_engine_release_buffers", "mp_forward_pairs",
@@ -355,6 +355,7 @@ def load() -> ctypes.CDLL:
         "mp_poa_set_realign_all": (c_int, [c_void_p]),
         "mp_poa_set_estimate_repeat_counts": (c_int, [c_void_p]),
         "mp_poa_set_phase_seconds": (c_int, [c_void_p, P(c_double), c_int64]),
+        "mp_poa_set_device_steps": (c_int, [c_void_p, c_int32]),
         "mp_node_update": (c_int, [c_void_p, P(NodeBatch), P(NodeResult)]),
         "mp_poa_info": (c_int, [c_void_p, c_int64, P(PoaChunkInfo)]),
         "mp_poa_nodes": (c_int, [c_void_p, c_int64, P(c_char), P(ctypes.c_uint64), P(c_double), P(c_double),

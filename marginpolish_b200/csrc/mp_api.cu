@@ -138,6 +138,8 @@ extern "C" void mp_engine_destroy(mp_engine *e) {
     if (e->outStream) cudaStreamDestroy(e->outStream);
     mp_node_scratch_free(e->nodeScratch);
     e->nodeScratch = nullptr;
+    mp_indel_scratch_free(e->indelScratch);
+    e->indelScratch = nullptr;
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }

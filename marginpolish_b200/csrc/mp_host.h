@@ -139,12 +139,47 @@ struct mp_engine {
     struct mp_device_batch *pipe[kPipeSlots] = {};  // the slots of mp_realign_batch_into (own streams)
     cudaStream_t outStream = nullptr;  // tuple copies of mp_realign_batch_into's slots, in slice order
     mp_pair_scratch pairScratch;       // mp_forward_pairs (under oneShotLock)
-    struct mp_node_scratch *nodeScratch = nullptr;  // mp_node_update's device arrays
+    struct mp_node_scratch *nodeScratch = nullptr;    // mp_node_update's device arrays
+    struct mp_indel_scratch *indelScratch = nullptr;  // the indel candidates' device arrays
     std::mutex oneShotLock;
 };
 
 // Frees the node update's device arrays (mp_nodes.cu).
 void mp_node_scratch_free(struct mp_node_scratch *s);
+// Frees the indel candidates' device arrays (mp_indels.cu).
+void mp_indel_scratch_free(struct mp_indel_scratch *s);
+
+namespace mp {
+// Inputs of the complete-indel candidates of many reads (mp_indels.cu): per job its reference's
+// and its read's runs in the flat run arrays, and its three tuple lists (matches, gap-x, gap-y)
+// with nJobs + 1 offsets each.
+struct IndelBatch {
+    int64_t nJobs = 0;
+    const int64_t *refBase = nullptr, *refRuns = nullptr, *readBase = nullptr, *readRuns = nullptr;
+    int64_t nRefRuns = 0, nReadRuns = 0;
+    const char *refChars = nullptr;
+    const uint32_t *refCounts = nullptr;
+    const char *readChars = nullptr;
+    const uint32_t *readCounts = nullptr;
+    const int64_t *off[3] = {nullptr, nullptr, nullptr};
+    const int32_t *w[3] = {nullptr, nullptr, nullptr}, *x[3] = {nullptr, nullptr, nullptr},
+                  *y[3] = {nullptr, nullptr, nullptr};
+    bool cmpRC = true;
+};
+// Candidates of every job, inserts first, in poa_augment's order: job j's are
+// [candOff[j], candOff[j+1]) of which the first nIns[j] are inserts, whose runs are
+// [runOff[j] + at, runOff[j] + at + len) of chars / counts. The per-candidate arrays are
+// page-locked buffers of the engine, valid until its next deviceIndelCandidates call.
+struct IndelOut {
+    std::vector<int64_t> candOff, runOff, nIns;
+    const int64_t *pos = nullptr, *len = nullptr, *at = nullptr, *offset = nullptr;
+    const uint64_t *nonRle = nullptr;
+    const double *weight = nullptr;
+    const char *chars = nullptr;
+    const uint64_t *counts = nullptr;
+};
+mp_status deviceIndelCandidates(mp_engine *e, const IndelBatch &b, IndelOut &out);
+}  // namespace mp
 
 struct mp_model {
     mp_engine *engine = nullptr;

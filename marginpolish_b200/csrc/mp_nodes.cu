@@ -201,6 +201,11 @@ __global__ void finishKernel(FinishArgs a) {
 struct mp_node_scratch {
     DevBuf reads, chars, counts, w, x, y, bw, rcw, count, start, cursor, tupNode, tupRead, slot, nodeSym, nodeFirst,
         log10, rc, obsRead, obsOffset, obsWeight, cubTemp, bad;
+    // its own stream: the loop runs the node update beside other GPU work of the same engine
+    cudaStream_t stream = nullptr;
+    ~mp_node_scratch() {
+        if (stream) cudaStreamDestroy(stream);
+    }
 };
 
 namespace {
@@ -265,7 +270,8 @@ extern "C" mp_status mp_node_update(mp_engine *e, const mp_node_batch *b, const 
     NODE_CUDA(cudaSetDevice(e->device));
     if (!e->nodeScratch) e->nodeScratch = new mp_node_scratch();
     mp_node_scratch &s = *e->nodeScratch;
-    cudaStream_t st = e->stream;
+    if (!s.stream) NODE_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+    cudaStream_t st = s.stream;
     const int64_t nC = b->n_chunks;
     const int64_t nNodes = nC > 0 ? b->node_offsets[nC] : 0;
     const int64_t nReads = nC > 0 ? b->chunk_reads[nC] : 0;

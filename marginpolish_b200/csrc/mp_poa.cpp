@@ -303,6 +303,24 @@ struct IndelCands {
     }
 };
 
+// The candidates of one read as the merge reads them: arrays owned by an IndelCands (host
+// steps) or slices of the GPU pass's page-locked output (device steps).
+struct IndelView {
+    const int64_t *pos = nullptr, *len = nullptr, *at = nullptr, *offset = nullptr;
+    const uint64_t *nonRle = nullptr;
+    const double *w = nullptr;
+    const char *chars = nullptr;
+    const uint64_t *counts = nullptr;
+    int64_t n = 0, nIns = 0;
+    static IndelView of(const IndelCands &c) {
+        IndelView v;
+        v.pos = c.pos.data(), v.len = c.len.data(), v.at = c.at.data(), v.offset = c.offset.data();
+        v.nonRle = c.nonRle.data(), v.w = c.w.data(), v.chars = c.chars.data(), v.counts = c.counts.data();
+        v.n = (int64_t) c.pos.size(), v.nIns = c.nIns;
+        return v;
+    }
+};
+
 void indelCandidates(const Rle &ref, const Rle &read, const std::vector<Pair> &matches, std::vector<Pair> &inserts,
                      std::vector<Pair> &deletes, bool cmpRC, IndelCands &out) {
     // candidate indel sequences, reused across candidates and calls of this thread
@@ -392,7 +410,7 @@ void indelCandidates(const Rle &ref, const Rle &read, const std::vector<Pair> &m
 // holds grows in read order whichever range the node is merged in, so merging disjoint ranges
 // on different threads gives the graph of one sequential merge.
 void mergeRead(Poa &poa, const Rle &read, bool strand, int64_t readNo, int64_t nMatches, const int32_t *mw,
-               const int32_t *mx, const int32_t *my, const IndelCands &ic, int64_t lo, int64_t hi,
+               const int32_t *mx, const int32_t *my, const IndelView &ic, int64_t lo, int64_t hi,
                std::vector<Obs> &obs, std::vector<int32_t> &obsNode) {
     for (int64_t t = 0; t < nMatches; t++) {
         const int64_t v = mx[t] + 1;
@@ -406,7 +424,7 @@ void mergeRead(Poa &poa, const Rle &read, bool strand, int64_t readNo, int64_t n
         obs.push_back(Obs{readNo, my[t], w});
         obsNode.push_back((int32_t) v);
     }
-    const int64_t n = (int64_t) ic.pos.size();
+    const int64_t n = ic.n;
     for (int64_t q = 0; q < n; q++) {
         if (ic.pos[q] < lo || ic.pos[q] >= hi) continue;
         Node &node = poa.nodes[ic.pos[q]];
@@ -416,16 +434,16 @@ void mergeRead(Poa &poa, const Rle &read, bool strand, int64_t readNo, int64_t n
             Insert *target = nullptr;
             for (Insert &e : node.ins) {
                 if (e.s.nonRle == ic.nonRle[q] && e.s.length() == L &&
-                    std::equal(e.s.c.begin(), e.s.c.end(), ic.chars.begin() + at) &&
-                    std::equal(e.s.n.begin(), e.s.n.end(), ic.counts.begin() + at)) {
+                    std::equal(e.s.c.begin(), e.s.c.end(), ic.chars + at) &&
+                    std::equal(e.s.n.begin(), e.s.n.end(), ic.counts + at)) {
                     target = &e;
                     break;
                 }
             }
             if (!target) {
                 Insert e;
-                e.s.c.assign(ic.chars.begin() + at, ic.chars.begin() + at + L);
-                e.s.n.assign(ic.counts.begin() + at, ic.counts.begin() + at + L);
+                e.s.c.assign(ic.chars + at, ic.chars + at + L);
+                e.s.n.assign(ic.counts + at, ic.counts + at + L);
                 e.s.nonRle = ic.nonRle[q];
                 node.ins.push_back(std::move(e));
                 target = &node.ins.back();
@@ -461,7 +479,7 @@ void augment(Poa &poa, const Rle &read, bool strand, int64_t readNo, const std::
         x[t] = (int32_t) matches[t].x;
         y[t] = (int32_t) matches[t].y;
     }
-    mergeRead(poa, read, strand, readNo, (int64_t) matches.size(), w.data(), x.data(), y.data(), ic, 0,
+    mergeRead(poa, read, strand, readNo, (int64_t) matches.size(), w.data(), x.data(), y.data(), IndelView::of(ic), 0,
               (int64_t) poa.nodes.size(), poa.obs, poa.obsNode);
 }
 
@@ -1047,6 +1065,8 @@ enum {
     kPhaseConsensus,   // consensus walk and anchor alignments of an iteration
     kPhaseRepeat,      // run-length estimate and score of the new graphs
     kPhaseBubbles,     // bubble graphs and their scores (polish mode)
+    kPhaseGroup,       // observation lists grouped by node after the merge
+    kPhaseJoin,        // waiting for the GPU's run-length estimate after the merge
     kPhaseCount
 };
 
@@ -1089,7 +1109,10 @@ struct mp_poa_set {
     size_t pinnedCap[3] = {0, 0, 0};  // tuples
     // Wall seconds spent in each step of the loop since the set was created (kPhase*).
     double phase[kPhaseCount] = {};
-    // every read's runs in one array each (the device-side node update's input)
+    // Steps of a realignment that run on the GPU instead of the host threads
+    // (mp_poa_set_device_steps; both forms build the same graphs).
+    int32_t deviceSteps = MP_POA_DEVICE_RUN_LENGTHS;
+    // every read's runs in one array each (the device-side steps' input)
     std::vector<int64_t> flatReadOff;
     std::string flatReadChars;
     std::vector<uint32_t> flatReadCounts;
@@ -1283,7 +1306,7 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
     std::vector<int64_t> nodeBase;
     mp_status mlStatus = MP_OK;
     std::thread mlThread;
-    if (s->useRle && nJobs > 0) {
+    if (s->useRle && nJobs > 0 && (s->deviceSteps & MP_POA_DEVICE_RUN_LENGTHS)) {
         mlThread = std::thread([&]() { mlStatus = deviceRepeatCounts(s, chunks, refs, offs[0], w[0], x[0], y[0], ml,
                                                                      nodeBase); });
     }
@@ -1308,7 +1331,62 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
             jobRead[(size_t) j] = r;
         }
     std::vector<IndelCands> cands(jobIdx.size());
-    {
+    std::vector<IndelView> views(jobIdx.size());
+    mp::IndelOut io;
+    if ((s->deviceSteps & MP_POA_DEVICE_INDELS) && nJobs > 0) {
+        // on the GPU: every read's candidates at once (mp_indels.cu)
+        PhaseTimer tCands(s->phase[kPhaseCandidates]);
+        std::vector<int64_t> refBase(s->nChunks, 0), jRefBase((size_t) nJobs), jRefRuns((size_t) nJobs),
+            jReadBase((size_t) nJobs), jReadRuns((size_t) nJobs);
+        std::string refChars;
+        std::vector<uint32_t> refCounts;
+        for (int64_t c : chunks) {
+            refBase[c] = (int64_t) refChars.size();
+            refChars.append(refs[c].c);
+            for (uint64_t k : refs[c].n) refCounts.push_back((uint32_t) k);
+        }
+        for (int64_t j = 0; j < nJobs; j++) {
+            const int64_t c = jobChunk[(size_t) j], r = jobRead[(size_t) j];
+            jRefBase[(size_t) j] = refBase[c];
+            jRefRuns[(size_t) j] = refs[c].length();
+            jReadBase[(size_t) j] = s->flatReadOff[(size_t) r];
+            jReadRuns[(size_t) j] = s->reads[r].length();
+        }
+        mp::IndelBatch ib;
+        ib.nJobs = nJobs;
+        ib.refBase = jRefBase.data();
+        ib.refRuns = jRefRuns.data();
+        ib.readBase = jReadBase.data();
+        ib.readRuns = jReadRuns.data();
+        ib.nRefRuns = (int64_t) refChars.size();
+        ib.nReadRuns = (int64_t) s->flatReadChars.size();
+        ib.refChars = refChars.data();
+        ib.refCounts = refCounts.data();
+        ib.readChars = s->flatReadChars.data();
+        ib.readCounts = s->flatReadCounts.data();
+        for (int k = 0; k < 3; k++) {
+            ib.off[k] = offs[k].data();
+            ib.w[k] = w[k];
+            ib.x[k] = x[k];
+            ib.y[k] = y[k];
+        }
+        ib.cmpRC = s->cmpRC;
+        mp_status rc = mp::deviceIndelCandidates(s->e, ib, io);
+        if (rc != MP_OK) {
+            if (mlThread.joinable()) mlThread.join();
+            return rc;
+        }
+        // each read's candidates are a slice of the pass's page-locked output
+        for (int64_t j = 0; j < nJobs; j++) {
+            IndelView &v = views[(size_t) j];
+            const int64_t c0 = io.candOff[(size_t) j], r0 = io.runOff[(size_t) j];
+            v.pos = io.pos + c0, v.len = io.len + c0, v.at = io.at + c0, v.offset = io.offset + c0;
+            v.nonRle = io.nonRle + c0, v.w = io.weight + c0;
+            v.chars = io.chars + r0, v.counts = io.counts + r0;
+            v.n = io.candOff[(size_t) j + 1] - c0;
+            v.nIns = io.nIns[(size_t) j];
+        }
+    } else {
         PhaseTimer tCands(s->phase[kPhaseCandidates]);
         forChunks(jobIdx, [&](int64_t j) {
             thread_local std::vector<Pair> lists[3];
@@ -1318,12 +1396,13 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
             }
             indelCandidates(refs[jobChunk[(size_t) j]], s->reads[jobRead[(size_t) j]], lists[0], lists[2], lists[1],
                             s->cmpRC, cands[(size_t) j]);
+            views[(size_t) j] = IndelView::of(cands[(size_t) j]);
         });
     }
     // then each chunk's graph, reads in order. With fewer chunks than host threads, a chunk's
     // nodes are split into ranges merged on separate threads (each range takes every read in
     // order, so every node's lists keep the sequential order).
-    PhaseTimer tMerge(s->phase[kPhaseMerge]);
+    auto tMerge = std::chrono::steady_clock::now();
     const int64_t nT = std::max(1u, std::thread::hardware_concurrency());
     const int64_t P = std::max<int64_t>(1, std::min<int64_t>(8, (2 * nT + (int64_t) chunks.size() - 1) /
                                                                    std::max<int64_t>(1, (int64_t) chunks.size())));
@@ -1331,36 +1410,59 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
     std::vector<int64_t> items;
     for (int64_t c : chunks)
         for (int64_t k = 0; k < P; k++) items.push_back(c * P + k);
+    // per range: its observations, then grouped by node (counting sort over the range's nodes,
+    // stable: every node's observations stay in read order)
     std::vector<std::vector<Obs>> rangeObs((size_t) (s->nChunks * P));
-    std::vector<std::vector<int32_t>> rangeNode((size_t) (s->nChunks * P));
+    std::vector<std::vector<int64_t>> rangeCount((size_t) (s->nChunks * P));
     forChunks(items, [&](int64_t item) {
         const int64_t c = item / P, k = item % P;
         Poa &poa = out[c];
         const int64_t nN = (int64_t) poa.nodes.size();
         const int64_t lo = nN * k / P, hi = nN * (k + 1) / P;
+        std::vector<Obs> obs;
+        std::vector<int32_t> node;
         for (int64_t r = s->chunkReads[c]; r < s->chunkReads[c + 1]; r++) {
             const int64_t j = firstJob[c] + (r - s->chunkReads[c]);
             const int64_t t0 = offs[0][j];
             mergeRead(poa, s->reads[r], s->strand[r] != 0, r - s->chunkReads[c], offs[0][j + 1] - t0, w[0] + t0,
-                      x[0] + t0, y[0] + t0, cands[(size_t) j], lo, hi, rangeObs[(size_t) item],
-                      rangeNode[(size_t) item]);
+                      x[0] + t0, y[0] + t0, views[(size_t) j], lo, hi, obs, node);
         }
+        std::vector<int64_t> &cnt = rangeCount[(size_t) item];
+        cnt.assign((size_t) (hi - lo + 1), 0);
+        for (int32_t v : node) cnt[(size_t) (v - lo) + 1]++;
+        for (int64_t i = 0; i < hi - lo; i++) cnt[(size_t) i + 1] += cnt[(size_t) i];
+        std::vector<Obs> &sorted = rangeObs[(size_t) item];
+        sorted.resize(obs.size());
+        std::vector<int64_t> at(cnt.begin(), cnt.end() - 1);
+        for (size_t q = 0; q < obs.size(); q++) sorted[(size_t) at[(size_t) (node[q] - lo)]++] = obs[q];
     });
+    auto tGroup = std::chrono::steady_clock::now();
+    s->phase[kPhaseMerge] += std::chrono::duration<double>(tGroup - tMerge).count();
+    // the chunk's observation list: the ranges' grouped lists in node order
     forChunks(chunks, [&](int64_t c) {
         Poa &poa = out[c];
+        const int64_t nN = (int64_t) poa.nodes.size();
+        size_t total = 0;
+        for (int64_t k = 0; k < P; k++) total += rangeObs[(size_t) (c * P + k)].size();
+        poa.obs.clear();
+        poa.obs.reserve(total);
+        poa.obsStart.assign((size_t) nN + 1, 0);
         for (int64_t k = 0; k < P; k++) {
+            const int64_t lo = nN * k / P, hi = nN * (k + 1) / P;
+            const std::vector<int64_t> &cnt = rangeCount[(size_t) (c * P + k)];
+            const int64_t base = (int64_t) poa.obs.size();
+            for (int64_t i = lo; i < hi; i++) poa.obsStart[(size_t) i + 1] = base + cnt[(size_t) (i - lo) + 1];
             std::vector<Obs> &o = rangeObs[(size_t) (c * P + k)];
-            std::vector<int32_t> &v = rangeNode[(size_t) (c * P + k)];
             poa.obs.insert(poa.obs.end(), o.begin(), o.end());
-            poa.obsNode.insert(poa.obsNode.end(), v.begin(), v.end());
             std::vector<Obs>().swap(o);
-            std::vector<int32_t>().swap(v);
         }
-        poa.groupObs();
+        poa.obsNode.clear();
         for (int64_t r = s->chunkReads[c]; r < s->chunkReads[c + 1]; r++)
             cands[(size_t) (firstJob[c] + (r - s->chunkReads[c]))] = IndelCands();
     });
+    s->phase[kPhaseGroup] += std::chrono::duration<double>(std::chrono::steady_clock::now() - tGroup).count();
     if (mlThread.joinable()) {
+        PhaseTimer tJoin(s->phase[kPhaseJoin]);
         mlThread.join();
         if (mlStatus != MP_OK) return mlStatus;
         for (int64_t c : chunks)
@@ -1805,6 +1907,13 @@ extern "C" mp_status mp_poa_set_estimate_repeat_counts(mp_poa_set *s) {
     for (int64_t c = 0; c < s->nChunks; c++) all[c] = c;
     PhaseTimer t(s->phase[kPhaseRepeat]);
     forChunks(all, [&](int64_t c) { estimateRepeatCounts(s->poas[c], s->reads, s->strand, s->chunkReads[c], s->rm); });
+    return MP_OK;
+}
+
+extern "C" mp_status mp_poa_set_device_steps(mp_poa_set *s, int32_t steps) {
+    if (!s || (steps & ~(MP_POA_DEVICE_RUN_LENGTHS | MP_POA_DEVICE_INDELS)))
+        return mp_fail(MP_ERR_ARGUMENT, "mp_poa_set_device_steps: NULL set or unknown steps");
+    s->deviceSteps = steps;
     return MP_OK;
 }
 

@@ -78,7 +78,9 @@ def parse():
     ap.add_argument("--polish-shipped", action="store_true",
                     help="only the shipped polishing loop's measurement, with its per-step times (one JSON line)")
     ap.add_argument("--device-indels", action="store_true",
-                    help="polishing loops find the reads' indel candidates on the GPU (MP_POA_DEVICE_INDELS)")
+                    help="the shipped loop finds the reads' indel candidates on the GPU (the default)")
+    ap.add_argument("--host-indels", action="store_true",
+                    help="the shipped loop finds the reads' indel candidates on the host threads")
     return ap.parse_args()
 
 
@@ -446,7 +448,7 @@ def reference_bubble_sample(pm):
             "sample": "bubbleGraph_constructFromPoa (construction and scores) on one 3 kb chunk at 50x, one core"}
 
 
-def measure_polish_shipped(engine, model, pm, device_indels=False):
+def measure_polish_shipped(engine, model, pm, device_indels=True):
     """The shipped loop (poa_realignAll with one polish iteration, then the run-length estimate)
     over the polish workload: realignment, bubble graphs, scores, new consensus, anchors,
     second realignment."""
@@ -829,7 +831,7 @@ def main():
         pm = params.polish_model_from_npz(os.path.join(ROOT, "tests", "golden", "model_np.npz"))
         engine = Engine(local)
         model = Model.from_polish(engine, pm)
-        print(json.dumps({"polish_loop_shipped": measure_polish_shipped(engine, model, pm, args.device_indels)}),
+        print(json.dumps({"polish_loop_shipped": measure_polish_shipped(engine, model, pm, not args.host_indels)}),
               flush=True)
     elif args.bubble_scores:
         from marginpolish_b200 import Engine, Model, params

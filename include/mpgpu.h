@@ -513,12 +513,12 @@ mp_status mp_poa_set_estimate_repeat_counts(mp_poa_set *s);
  * GPU's run-length estimate after the merge. Entries past 10 are set to 0. Instrumentation of
  * this library's loop; the reference has no counterpart. */
 mp_status mp_poa_set_phase_seconds(const mp_poa_set *s, double *seconds, int64_t n);
-/* Steps of a realignment that run on the GPU instead of the host threads; both forms build
- * identical graphs. MP_POA_DEVICE_RUN_LENGTHS (the default): the new graphs' run lengths
- * (impl/polisher.c:1556-1565) by mp_node_update, while the host threads fold the reads.
+/* Steps of a realignment that run on the GPU instead of the host threads (both on by default;
+ * every combination builds identical graphs). MP_POA_DEVICE_RUN_LENGTHS: the new graphs' run
+ * lengths (impl/polisher.c:1556-1565) by mp_node_update, while the host threads fold the reads.
  * MP_POA_DEVICE_INDELS: every read's complete-indel candidates (poa_augment,
- * impl/polisher.c:354-522) in one GPU pass; off by default, because moving the tuples up and the
- * candidates down costs more than the host threads' enumeration at these sizes. */
+ * impl/polisher.c:354-522) in one GPU pass. Its buffers (device and page-locked) grow on first
+ * use and are kept by the engine, so an engine's first realignment pays their allocation. */
 #define MP_POA_DEVICE_RUN_LENGTHS 1
 #define MP_POA_DEVICE_INDELS 2
 mp_status mp_poa_set_device_steps(mp_poa_set *s, int32_t steps);

@@ -1111,7 +1111,7 @@ struct mp_poa_set {
     double phase[kPhaseCount] = {};
     // Steps of a realignment that run on the GPU instead of the host threads
     // (mp_poa_set_device_steps; both forms build the same graphs).
-    int32_t deviceSteps = MP_POA_DEVICE_RUN_LENGTHS;
+    int32_t deviceSteps = MP_POA_DEVICE_RUN_LENGTHS | MP_POA_DEVICE_INDELS;
     // every read's runs in one array each (the device-side steps' input)
     std::vector<int64_t> flatReadOff;
     std::string flatReadChars;

@@ -240,9 +240,9 @@ class PoaSet:
     def estimate_repeat_counts(self) -> None:
         _lib.check(self._lib.mp_poa_set_estimate_repeat_counts(self.handle))
 
-    def set_device_steps(self, run_lengths: bool = True, indels: bool = False) -> None:
+    def set_device_steps(self, run_lengths: bool = True, indels: bool = True) -> None:
         """Which steps of a realignment run on the GPU instead of the host threads: the run-length
-        estimate (default on) and the complete-indel candidates (default off); both forms build
+        estimate and the complete-indel candidates (both on by default); every combination builds
         identical graphs (mp_poa_set_device_steps)."""
         _lib.check(self._lib.mp_poa_set_device_steps(self.handle, (1 if run_lengths else 0) | (2 if indels else 0)))
 

@@ -367,6 +367,9 @@ mp_status deviceIndelCandidates(mp_engine *e, const IndelBatch &b, IndelOut &out
     if (!s.stream) IND_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
     cudaStream_t st = s.stream;
     const int64_t nJ = b.nJobs;
+    for (int k = 0; k < 3; k++)
+        if (b.off[k][nJ] >= INT32_MAX || nJ >= INT32_MAX)
+            return mp_fail(MP_ERR_ARGUMENT, "indel candidates: 2^31 or more tuples in one list");
     std::vector<JobIn> jobs((size_t) nJ);
     for (int64_t j = 0; j < nJ; j++) jobs[(size_t) j] = JobIn{b.refBase[j], b.refRuns[j], b.readBase[j], b.readRuns[j]};
     IND_TRY(upload(s.jobs, jobs.data(), nJ, st));
@@ -428,6 +431,7 @@ mp_status deviceIndelCandidates(mp_engine *e, const IndelBatch &b, IndelOut &out
     }
     winStart[(size_t) nJ] = (int64_t) win.size();
     const int64_t nW = (int64_t) win.size();
+    if (nW + 1 >= INT32_MAX) return mp_fail(MP_ERR_ARGUMENT, "indel candidates: too many tuple windows");
     IND_TRY(upload(s.win, win.data(), nW, st));
     // per read run: its matches in the job's sorted match keys
     IND_TRY(s.mStart.reserve(sizeof(int32_t) * (size_t) std::max<int64_t>(b.nReadRuns, 1)));

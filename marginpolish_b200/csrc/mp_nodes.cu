@@ -238,8 +238,9 @@ mp_status validate(const mp_node_batch *b) {
     const int64_t nTup = nReads > 0 ? b->match_offsets[nReads] : 0;
     if ((nRuns > 0 && (!b->read_chars || !b->read_counts)) || (nTup > 0 && (!b->weight || !b->x || !b->y)))
         return mp_fail(MP_ERR_ARGUMENT, "mp_node_update: missing read or tuple array");
-    if (nTup >= INT32_MAX || nReads >= INT32_MAX)
-        return mp_fail(MP_ERR_ARGUMENT, "mp_node_update: more than 2^31 tuples or reads");
+    const int64_t nNodes = b->n_chunks > 0 ? b->node_offsets[b->n_chunks] : 0;
+    if (nTup >= INT32_MAX || nReads >= INT32_MAX || nNodes >= INT32_MAX)
+        return mp_fail(MP_ERR_ARGUMENT, "mp_node_update: 2^31 or more tuples, reads or nodes");
     return MP_OK;
 }
 

@@ -579,25 +579,33 @@ def measure_realign_pass(engine, model, pm, wl, peak, cpu_seconds, plain_reads=1
     return out
 
 
-def measure_polish_loop(engine, model, pm, wl, max_iterations):
+def measure_polish_loop(engine, model, pm, wl, max_iterations, runs=2):
     """poa_realignAll in consensus mode over a polishing workload: the first realignment, then
-    the consensus iterations, wall seconds with the per-phase split."""
+    the consensus iterations, wall seconds with the per-phase split; the fastest of `runs` runs
+    (the first run on an engine also grows its buffers), with the first run's time beside it."""
     from marginpolish_b200 import PoaSet, PolishParams
-    s = PoaSet.from_polish_model(engine, model, pm, PolishParams(max_iterations=max_iterations), wl.drafts,
-                                 wl.reads, wl.strands, wl.anchors)
-    t0 = time.perf_counter()
-    s.realign()
-    t1 = time.perf_counter()
-    s.iterate()
-    s.estimate_repeat_counts()
-    t2 = time.perf_counter()
-    its = [s.info(c)["iterations"] for c in range(s.n_chunks)]
-    phases = {k: round(v, 3) for k, v in s.phase_seconds().items()}
-    s.close()
-    return {"seconds": t2 - t0, "realign_seconds": t1 - t0, "iterate_seconds": t2 - t1, "phase_seconds": phases,
-            "iterations": its,
-            "chunks": len(wl.drafts), "reads": int(sum(len(r) for r in wl.reads)),
-            "bases": int(sum(r.non_rle_length for lst in wl.reads for r in lst))}
+    best, first = None, None
+    for _ in range(runs):
+        s = PoaSet.from_polish_model(engine, model, pm, PolishParams(max_iterations=max_iterations), wl.drafts,
+                                     wl.reads, wl.strands, wl.anchors)
+        t0 = time.perf_counter()
+        s.realign()
+        t1 = time.perf_counter()
+        s.iterate()
+        s.estimate_repeat_counts()
+        t2 = time.perf_counter()
+        its = [s.info(c)["iterations"] for c in range(s.n_chunks)]
+        phases = {k: round(v, 3) for k, v in s.phase_seconds().items()}
+        s.close()
+        r = {"seconds": t2 - t0, "realign_seconds": t1 - t0, "iterate_seconds": t2 - t1, "phase_seconds": phases,
+             "iterations": its}
+        first = r["seconds"] if first is None else first
+        if best is None or r["seconds"] < best["seconds"]:
+            best = r
+    best.update({"first_run_seconds": first, "runs": runs, "chunks": len(wl.drafts),
+                 "reads": int(sum(len(r) for r in wl.reads)),
+                 "bases": int(sum(r.non_rle_length for lst in wl.reads for r in lst))})
+    return best
 
 
 def measure_scale_configs(engine, model, pm, peak, cpu_seconds, chunks_5mb):

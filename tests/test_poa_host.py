@@ -119,3 +119,24 @@ def test_realign_needs_an_engine(polish_model):
     with pytest.raises(MpError):
         s.consensus(0)  # no graph yet
     s.close()
+
+
+def test_device_steps_flags_and_node_update_arguments(polish_model):
+    """mp_poa_set_device_steps takes only its two step bits; mp_node_update refuses a missing
+    engine or batch before it touches a GPU."""
+    import ctypes
+
+    from marginpolish_b200 import _lib
+    from marginpolish_b200._lib import MpError
+    wl = synth.config_polish(seed=8, n_chunks=1, chunk_len=300, coverage=4, read_len=(200, 280))
+    s = PoaSet(None, None, polish_model.alignment, PolishParams(), wl.drafts, wl.reads, wl.strands, wl.anchors,
+               polish_model.repeat_log10)
+    s.set_device_steps(run_lengths=False, indels=False)
+    s.set_device_steps()
+    lib = _lib.load()
+    assert lib.mp_poa_set_device_steps(s.handle, 4) == _lib.MP_ERR_ARGUMENT
+    s.close()
+    r = _lib.NodeResult()
+    assert lib.mp_node_update(None, None, ctypes.byref(r)) == _lib.MP_ERR_ARGUMENT
+    with pytest.raises(MpError):
+        _lib.check(lib.mp_node_update(None, None, ctypes.byref(r)))

@@ -1305,10 +1305,13 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
     std::vector<uint64_t> ml;
     std::vector<int64_t> nodeBase;
     mp_status mlStatus = MP_OK;
+    std::string mlError;  // the worker thread's error message (messages are per thread)
     std::thread mlThread;
     if (s->useRle && nJobs > 0 && (s->deviceSteps & MP_POA_DEVICE_RUN_LENGTHS)) {
-        mlThread = std::thread([&]() { mlStatus = deviceRepeatCounts(s, chunks, refs, offs[0], w[0], x[0], y[0], ml,
-                                                                     nodeBase); });
+        mlThread = std::thread([&]() {
+            mlStatus = deviceRepeatCounts(s, chunks, refs, offs[0], w[0], x[0], y[0], ml, nodeBase);
+            if (mlStatus != MP_OK) mlError = mp_last_error();
+        });
     }
     // fold each chunk's reads into its graph (chunks in parallel, reads in order)
     std::vector<int64_t> firstJob(s->nChunks, 0);
@@ -1464,7 +1467,7 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
     if (mlThread.joinable()) {
         PhaseTimer tJoin(s->phase[kPhaseJoin]);
         mlThread.join();
-        if (mlStatus != MP_OK) return mlStatus;
+        if (mlStatus != MP_OK) return mp_fail(mlStatus, "run-length estimate: %s", mlError.c_str());
         for (int64_t c : chunks)
             out[c].ml.assign(ml.begin() + nodeBase[c] + 1, ml.begin() + nodeBase[c] + refs[c].length() + 1);
     }

@@ -141,6 +141,11 @@ struct mp_engine {
     mp_pair_scratch pairScratch;       // mp_forward_pairs (under oneShotLock)
     struct mp_node_scratch *nodeScratch = nullptr;    // mp_node_update's device arrays
     struct mp_indel_scratch *indelScratch = nullptr;  // the indel candidates' device arrays
+    // Page-locked tuple arrays of the POA sets' realignments (w, x, y of each list, grow only),
+    // kept by the engine so that later sets do not pin memory again; a realignment holds
+    // poaLock while it uses them.
+    PinBuf poaTuples[3];
+    std::mutex poaLock;
     std::mutex oneShotLock;
 };
 

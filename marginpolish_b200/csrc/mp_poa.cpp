@@ -1104,9 +1104,6 @@ struct mp_poa_set {
     std::vector<std::vector<uint8_t>> quals;  // per read, per run (empty when none given)
     std::vector<BubbleGraph> bubbles;        // per chunk: the last graph mp_poa_set_build_bubbles made
     mp_device_batch *db = nullptr;
-    // page-locked tuple arrays of the last realignment (grow only): the copies run by DMA
-    void *pinned[3] = {nullptr, nullptr, nullptr};
-    size_t pinnedCap[3] = {0, 0, 0};  // tuples
     // Wall seconds spent in each step of the loop since the set was created (kPhase*).
     double phase[kPhaseCount] = {};
     // Steps of a realignment that run on the GPU instead of the host threads
@@ -1116,10 +1113,7 @@ struct mp_poa_set {
     std::vector<int64_t> flatReadOff;
     std::string flatReadChars;
     std::vector<uint32_t> flatReadCounts;
-    ~mp_poa_set() {
-        mp_device_batch_destroy(db);
-        for (void *q : pinned) mp_host_free(q);
-    }
+    ~mp_poa_set() { mp_device_batch_destroy(db); }
 };
 
 namespace {
@@ -1179,6 +1173,8 @@ mp_status deviceRepeatCounts(mp_poa_set *s, const std::vector<int64_t> &chunks, 
 mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const std::vector<Rle> &refs,
                         const std::vector<std::vector<Anchor>> *anchors, std::vector<Poa> &out) {
     if (!s->e || !s->m) return mp_fail(MP_ERR_STATE, "mp_poa: realignment needs an engine and a model");
+    // the engine's page-locked tuple arrays are this realignment's until it returns
+    std::lock_guard<std::mutex> tuplesGuard(s->e->poaLock);
     // symbol repeat counts are clamped below the repeat table's dimension on the cropping path
     // (impl/polisher.c:634-635) and one lower on the path without anchors (:676-679)
     const uint64_t maxRC = s->useRle ? (uint64_t) s->rm.M : 2;
@@ -1278,24 +1274,21 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
         memset(&o, 0, sizeof(o));
         for (int k = 0; k < 3; k++) {
             offs[k].assign(nJobs + 1, 0);
+            // the list's w, x and y arrays, back to back in the engine's page-locked buffer (the
+            // copies run by DMA); the buffer grows by a quarter over the need
             const size_t need = (size_t) std::max<int64_t>(totals[k], 1);
-            if (need > s->pinnedCap[k]) {
-                mp_host_free(s->pinned[k]);
-                s->pinned[k] = nullptr;
-                s->pinnedCap[k] = 0;
-                const size_t cap = need + need / 4;
-                rc = mp_host_alloc(3 * sizeof(int32_t) * cap, &s->pinned[k]);
-                if (rc != MP_OK) return rc;
-                s->pinnedCap[k] = cap;
-            }
-            int32_t *base = static_cast<int32_t *>(s->pinned[k]);
+            PinBuf &pb = s->e->poaTuples[k];
+            rc = pb.reserve(3 * sizeof(int32_t) * need);
+            if (rc != MP_OK) return rc;
+            const size_t cap = pb.bytes / (3 * sizeof(int32_t));
+            int32_t *base = static_cast<int32_t *>(pb.p);
             w[k] = base;
-            x[k] = base + s->pinnedCap[k];
-            y[k] = base + 2 * s->pinnedCap[k];
+            x[k] = base + cap;
+            y[k] = base + 2 * cap;
             o.offsets[k] = offs[k].data();
             o.weight[k] = base;
-            o.x[k] = base + s->pinnedCap[k];
-            o.y[k] = base + 2 * s->pinnedCap[k];
+            o.x[k] = base + cap;
+            o.y[k] = base + 2 * cap;
         }
         rc = mp_device_batch_fetch_into(s->e, s->db, &o);
         if (rc != MP_OK) return rc;

@@ -1109,11 +1109,24 @@ struct mp_poa_set {
     // Steps of a realignment that run on the GPU instead of the host threads
     // (mp_poa_set_device_steps; both forms build the same graphs).
     int32_t deviceSteps = MP_POA_DEVICE_RUN_LENGTHS | MP_POA_DEVICE_INDELS;
+    // symbols and anchors of the last realignment's jobs (reused between realignments)
+    std::vector<uint16_t> jobX, jobY;
+    std::vector<int32_t> jobAnchors;
     // every read's runs in one array each (the device-side steps' input)
     std::vector<int64_t> flatReadOff;
     std::string flatReadChars;
     std::vector<uint32_t> flatReadCounts;
-    ~mp_poa_set() { mp_device_batch_destroy(db); }
+    // Frees the graphs the loop has replaced or rejected, off the loop's path (one batch at a
+    // time: the previous batch's thread is joined before the next starts, and at destruction).
+    std::thread reaper;
+    void reap(std::vector<Poa> &&graphs) {
+        if (reaper.joinable()) reaper.join();
+        reaper = std::thread([g = std::move(graphs)]() mutable { std::vector<Poa>().swap(g); });
+    }
+    ~mp_poa_set() {
+        if (reaper.joinable()) reaper.join();
+        mp_device_batch_destroy(db);
+    }
 };
 
 namespace {
@@ -1204,9 +1217,14 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
         }
     }
     const int64_t nJobs = (int64_t) yo.size() - 1;
-    std::vector<uint16_t> xs((size_t) nx), ys((size_t) yo.back());
+    // the symbol and anchor arrays are the set's, kept between realignments (every entry is
+    // written below), so that later realignments reuse memory already mapped
+    std::vector<uint16_t> &xs = s->jobX, &ys = s->jobY;
+    std::vector<int32_t> &an = s->jobAnchors;
+    xs.resize((size_t) nx);
+    ys.resize((size_t) yo.back());
+    an.resize((size_t) (3 * ao.back()));
     std::vector<int64_t> xb((size_t) nJobs), xe((size_t) nJobs), shift((size_t) nJobs);
-    std::vector<int32_t> an((size_t) (3 * ao.back()));
     std::vector<uint8_t> st((size_t) nJobs);
     forChunks(chunks, [&](int64_t c) {
         const int64_t L = refs[c].length();
@@ -1628,17 +1646,20 @@ mp_status iterate(mp_poa_set *s, bool polishMode) {
         std::vector<int64_t> still;
         std::vector<uint8_t> keep(nC, 0);
         PhaseTimer tRep(s->phase[kPhaseRepeat]);
+        std::vector<Poa> trash(nC);  // graphs no longer needed, freed by the set's reaper thread
         forChunks(go, [&](int64_t c) {
             if (s->useRle) estimateRepeatCounts(next[c], s->reads, s->strand, s->chunkReads[c], s->rm);
             const double sc2 = score(next[c]);
             if (sc2 <= sc[c] && s->iterations[c] > minIter) {  // greedy stop: keep the old graph
-                Poa drop = std::move(next[c]);                // (freed here, in parallel)
+                trash[c] = std::move(next[c]);
                 return;
             }
+            trash[c] = std::move(s->poas[c]);
             s->poas[c] = std::move(next[c]);
             sc[c] = sc2;
             keep[c] = 1;
         });
+        s->reap(std::move(trash));
         for (int64_t c : go)
             if (keep[c] && s->iterations[c] < maxIter) still.push_back(c);
         active.swap(still);

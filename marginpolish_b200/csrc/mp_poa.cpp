@@ -1116,15 +1116,22 @@ struct mp_poa_set {
     std::vector<int64_t> flatReadOff;
     std::string flatReadChars;
     std::vector<uint32_t> flatReadCounts;
-    // Frees the graphs the loop has replaced or rejected, off the loop's path (one batch at a
-    // time: the previous batch's thread is joined before the next starts, and at destruction).
+    // Graphs the loop has replaced or rejected. The next realignment frees them on a thread of
+    // their own while its posterior pass runs on the GPU (the host is idle then; freeing them
+    // beside the read merge would contend with its allocations).
+    std::vector<Poa> trash;
     std::thread reaper;
-    void reap(std::vector<Poa> &&graphs) {
+    void reapStart() {
+        reapJoin();
+        if (trash.empty()) return;
+        reaper = std::thread([g = std::move(trash)]() mutable { std::vector<Poa>().swap(g); });
+        trash.clear();
+    }
+    void reapJoin() {
         if (reaper.joinable()) reaper.join();
-        reaper = std::thread([g = std::move(graphs)]() mutable { std::vector<Poa>().swap(g); });
     }
     ~mp_poa_set() {
-        if (reaper.joinable()) reaper.join();
+        reapJoin();
         mp_device_batch_destroy(db);
     }
 };
@@ -1259,6 +1266,7 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
     const int32_t *w[3] = {nullptr, nullptr, nullptr}, *x[3] = {nullptr, nullptr, nullptr},
                   *y[3] = {nullptr, nullptr, nullptr};
     s->phase[kPhaseJobs] += std::chrono::duration<double>(std::chrono::steady_clock::now() - tJobs).count();
+    s->reapStart();  // earlier graphs are freed while the GPU works
     if (nJobs > 0) {
         PhaseTimer tDev(s->phase[kPhaseDevice]);
         mp_batch b;
@@ -1311,6 +1319,7 @@ mp_status realignChunks(mp_poa_set *s, const std::vector<int64_t> &chunks, const
         rc = mp_device_batch_fetch_into(s->e, s->db, &o);
         if (rc != MP_OK) return rc;
     }
+    s->reapJoin();
     // The run-length estimate of the new graphs runs on the GPU (mp_node_update, from the same
     // match tuples) while the host threads fold the reads into the graphs.
     std::vector<uint64_t> ml;
@@ -1646,7 +1655,7 @@ mp_status iterate(mp_poa_set *s, bool polishMode) {
         std::vector<int64_t> still;
         std::vector<uint8_t> keep(nC, 0);
         PhaseTimer tRep(s->phase[kPhaseRepeat]);
-        std::vector<Poa> trash(nC);  // graphs no longer needed, freed by the set's reaper thread
+        std::vector<Poa> trash(nC);  // graphs no longer needed: freed during the next realignment
         forChunks(go, [&](int64_t c) {
             if (s->useRle) estimateRepeatCounts(next[c], s->reads, s->strand, s->chunkReads[c], s->rm);
             const double sc2 = score(next[c]);
@@ -1659,7 +1668,8 @@ mp_status iterate(mp_poa_set *s, bool polishMode) {
             sc[c] = sc2;
             keep[c] = 1;
         });
-        s->reap(std::move(trash));
+        for (Poa &g : trash)
+            if (!g.nodes.empty()) s->trash.push_back(std::move(g));
         for (int64_t c : go)
             if (keep[c] && s->iterations[c] < maxIter) still.push_back(c);
         active.swap(still);
